@@ -1,0 +1,395 @@
+// ref_harness.C — TEST INFRASTRUCTURE ONLY (the oracle). Never linked into the product.
+//
+// Drives the reference's own, unmodified MOSFET device code (MOSFET1 level 1, BSIM3 level 9,
+// BSIM4 level 14 from src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET{1,_B3,_B4}.C) through the
+// same calls the reference's device manager makes, so the outputs are the reference's outputs:
+//
+//   setup  : Configuration::findConfiguration -> createDevice -> addModel / addInstance
+//            (DeviceMgr::addDeviceModel / addDeviceInstance, N_DEV_DeviceMgr.C:1272, 1446), then the
+//            topology hooks registerLIDs / registerStateLIDs / registerStoreLIDs / jacobianStamp /
+//            registerJacLIDs / setupPointers (N_TOP_CktGraphBasic.C:1092-1142, N_DEV_DeviceMgr.C:3482).
+//   load   : zero F,Q,B,dFdxdVp,dQdxdVp and dFdx,dQdx (N_LOA_NonlinearEquationLoader.C:128-133,
+//            226-227), then Device::updateState, updateSecondaryState, loadDAEVectors, loadDAEMatrices
+//            (N_DEV_DeviceMgr.C:2117-2123, 2424-2429, 2452-2461, 2256-2261).
+//
+// Vector layout: unknown index = node id for external nodes [0, n_nodes), then each instance's
+// internal nodes in instance order; the ground slot is the last index (n_unknowns), like the
+// reference's overlap-with-ground map (N_LAS_Builder.C:416-440). The CSR pattern is supplied by the
+// caller (rows 0..n_unknowns, the last being ground) so that the product's own pattern is the one
+// exercised; in-row offsets are found by searching each row's sorted columns, which is what
+// Indexor::matrixGlobalToLocal does (N_TOP_Indexor.C:171-205).
+
+#include <Xyce_config.h>
+
+#include <cmath>
+#include <cstring>
+#include <cstdio>
+#include <chrono>
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <N_DEV_Configuration.h>
+#include <N_DEV_Device.h>
+#include <N_DEV_DeviceBlock.h>
+#include <N_DEV_DeviceInstance.h>
+#include <N_DEV_DeviceOptions.h>
+#include <N_DEV_ExternData.h>
+#include <N_DEV_MatrixLoadData.h>
+#include <N_DEV_SolverState.h>
+#include <N_DEV_Param.h>
+#include <N_DEV_MOSFET1.h>
+#include <N_DEV_MOSFET_B3.h>
+#include <N_DEV_MOSFET_B4.h>
+#include <N_IO_CmdParse.h>
+#include <N_LAS_Matrix.h>
+#include <N_LAS_Vector.h>
+
+// The command-line parser lives in the reference's IO package, which is not compiled here. The
+// device code only asks it whether debug switches were given; these definitions answer "no".
+namespace Xyce { namespace IO {
+CmdParse::CmdParse() : iargs(0), cargs(0), allocatedCargs_(false), parMgr_(0) {}
+CmdParse::~CmdParse() {}
+bool CmdParse::argExists(const std::string &) const { return false; }
+std::string CmdParse::getArgumentValue(const std::string &) const { return std::string(); }
+}}
+
+namespace XD = Xyce::Device;
+
+extern "C" {
+// Mirrors the reference SolverState / DeviceOptions fields the MOSFET loads read.
+typedef struct xref_flags {
+  int dcop;          // SolverState::dcopFlag
+  int init_tran;     // SolverState::initTranFlag
+  int newton_iter;   // SolverState::newtonIter
+  int init_jct;      // SolverState::initJctFlag
+  int init_fix;      // SolverState::initFixFlag
+  int transient;     // SolverState::transientFlag
+  int tranop;        // SolverState::tranopFlag
+  int acop;          // SolverState::acopFlag
+  int voltlim;       // DeviceOptions::voltageLimiterFlag
+  int input_op;      // SolverState::inputOPFlag
+  double gmin;       // DeviceOptions::gmin
+  double pdt;        // SolverState::pdt
+} xref_flags;
+}
+
+namespace {
+
+struct RefCircuit {
+  Xyce::IO::CmdParse cp;
+  XD::DeviceOptions opts;
+  XD::SolverState ss;
+  XD::MatrixLoadData mld;
+  XD::ExternData ext;
+  XD::Device *dev;
+  std::vector<XD::DeviceInstance *> inst;
+  int level;
+  int n_nodes, n_unknowns, n_sta, n_sto;
+  std::vector<int> int_lid_base, int_count, sta_base, sto_base, n_sta_inst;
+  std::vector<int> inst_lids;  // per instance: 4 external LIDs (ground mapped to n_unknowns)
+  N_LAS_Matrix dFdx, dQdx;
+  N_LAS_Vector flagSol;
+  std::vector<double> nextSol, currSol, lastSol, nextSta, currSta, lastSta, nextSto, currSto, lastSto,
+      staDeriv, f, q, b, dfdxdvp, dqdxdvp, leadF, leadQ;
+  std::string err;
+  RefCircuit() : dev(0), level(0), n_nodes(0), n_unknowns(0), n_sta(0), n_sto(0) {}
+  ~RefCircuit() { delete dev; }
+};
+
+const char *device_letter_for(int level) { (void)level; return "m"; }
+
+void register_level(int level) {
+  static bool b1 = false, b3 = false, b4 = false;
+  if (level == 1 && !b1) { XD::MOSFET1::registerDevice(); b1 = true; }
+  if (level == 9 && !b3) { XD::MOSFET_B3::registerDevice(); b3 = true; }
+  if (level == 14 && !b4) { XD::MOSFET_B4::registerDevice(); b4 = true; }
+}
+
+void bind_extern(RefCircuit &c) {
+  XD::ExternData &e = c.ext;
+  e.nextSolVectorRawPtr = c.nextSol.data();
+  e.currSolVectorRawPtr = c.currSol.data();
+  e.lastSolVectorRawPtr = c.lastSol.data();
+  e.nextStaVectorRawPtr = c.nextSta.data();
+  e.currStaVectorRawPtr = c.currSta.data();
+  e.lastStaVectorRawPtr = c.lastSta.data();
+  e.nextStoVectorRawPtr = c.nextSto.data();
+  e.currStoVectorRawPtr = c.currSto.data();
+  e.lastStoVectorRawPtr = c.lastSto.data();
+  e.nextStaDerivVectorRawPtr = c.staDeriv.data();
+  e.daeFVectorRawPtr = c.f.data();
+  e.daeQVectorRawPtr = c.q.data();
+  e.daeBVectorRawPtr = c.b.data();
+  e.dFdxdVpVectorRawPtr = c.dfdxdvp.data();
+  e.dQdxdVpVectorRawPtr = c.dqdxdvp.data();
+  e.storeLeadCurrQCompRawPtr = c.leadQ.data();
+  e.dFdxMatrixPtr = &c.dFdx;
+  e.dQdxMatrixPtr = &c.dQdx;
+  e.flagSolVectorPtr = &c.flagSol;
+}
+
+void apply_flags(RefCircuit &c, const xref_flags &fl) {
+  c.ss.dcopFlag = fl.dcop != 0;
+  c.ss.initTranFlag = fl.init_tran != 0;
+  c.ss.newtonIter = fl.newton_iter;
+  c.ss.initJctFlag = fl.init_jct != 0;
+  c.ss.initFixFlag = fl.init_fix != 0;
+  c.ss.transientFlag = fl.transient != 0;
+  c.ss.tranopFlag = fl.tranop != 0;
+  c.ss.acopFlag = fl.acop != 0;
+  c.ss.inputOPFlag = fl.input_op != 0;
+  c.ss.pdt = fl.pdt;
+  c.opts.voltageLimiterFlag = fl.voltlim != 0;
+  c.opts.gmin = fl.gmin;
+}
+
+void do_load(RefCircuit &c) {
+  std::fill(c.f.begin(), c.f.end(), 0.0);
+  std::fill(c.q.begin(), c.q.end(), 0.0);
+  std::fill(c.b.begin(), c.b.end(), 0.0);
+  std::fill(c.dfdxdvp.begin(), c.dfdxdvp.end(), 0.0);
+  std::fill(c.dqdxdvp.begin(), c.dqdxdvp.end(), 0.0);
+  c.dFdx.put(0.0);
+  c.dQdx.put(0.0);
+  c.dev->updateState(c.nextSol.data(), c.nextSta.data(), c.nextSto.data());
+  c.dev->updateSecondaryState(c.staDeriv.data(), c.nextSto.data());
+  c.dev->loadDAEVectors(c.nextSol.data(), c.f.data(), c.q.data(), c.b.data(), c.leadF.data(), c.leadQ.data());
+  c.dev->loadDAEMatrices(c.dFdx, c.dQdx);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds the reference device objects for one MOSFET family.
+//   level            1, 9 or 14
+//   n_models         number of .MODEL cards; model m is "nmos" if model_is_pmos[m]==0 else "pmos"
+//   model_nparams[m] number of (name, value) pairs for model m, concatenated in param_names/values
+//   inst_model[i]    model index of instance i; inst_nodes[4*i..] = D, G, S, B node ids (-1 = ground)
+//   inst_param_names / inst_param_values[i*n_inst_params + k]; NaN = not given
+void *xref_create(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
+                  const char **param_names, const double *param_values, int n_inst, const int *inst_model,
+                  const int *inst_nodes, int n_inst_params, const char **inst_param_names,
+                  const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
+  RefCircuit *c = new RefCircuit();
+  try {
+    c->level = level;
+    register_level(level);
+    const XD::Configuration *cfg = XD::Configuration::findConfiguration(device_letter_for(level), level);
+    if (!cfg) throw std::runtime_error("no configuration for level");
+    XD::FactoryBlock fb(c->opts, c->ss, c->mld, c->ext, c->cp);
+    c->dev = cfg->createDevice(fb);
+    int off = 0;
+    for (int m = 0; m < n_models; ++m) {
+      char name[64];
+      snprintf(name, sizeof(name), "xmod%d", m);
+      XD::ModelBlock mb(name, model_is_pmos[m] ? "PMOS" : "NMOS", level);
+      for (int k = 0; k < model_nparams[m]; ++k, ++off)
+        mb.params.push_back(XD::Param(param_names[off], param_values[off], true));
+      c->dev->addModel(mb, fb);
+    }
+    c->n_nodes = n_nodes;
+    c->inst.resize(n_inst);
+    for (int i = 0; i < n_inst; ++i) {
+      char name[64], mname[64];
+      snprintf(name, sizeof(name), "m%d", i);
+      snprintf(mname, sizeof(mname), "xmod%d", inst_model[i]);
+      XD::InstanceBlock ib(name);
+      ib.setModelName(Xyce::Device::ModelName(mname));
+      for (int k = 0; k < n_inst_params; ++k) {
+        double v = inst_param_values[(size_t)i * n_inst_params + k];
+        if (!std::isnan(v)) ib.params.push_back(XD::Param(inst_param_names[k], v, true));
+      }
+      ib.numExtVars = 4;
+      c->inst[i] = c->dev->addInstance(ib, fb);
+      if (!c->inst[i]) throw std::runtime_error("addInstance failed");
+    }
+    // LID assignment: external nodes, then internals in instance order, then ground.
+    int next = n_nodes;
+    c->int_lid_base.resize(n_inst);
+    c->int_count.resize(n_inst);
+    for (int i = 0; i < n_inst; ++i) {
+      c->int_lid_base[i] = next;
+      c->int_count[i] = c->inst[i]->getNumIntVars();
+      next += c->int_count[i];
+    }
+    c->n_unknowns = next;
+    const int gnd = next;
+    c->inst_lids.resize(4 * (size_t)n_inst);
+    int sta = 0, sto = 0;
+    c->sta_base.resize(n_inst);
+    c->sto_base.resize(n_inst);
+    c->n_sta_inst.resize(n_inst);
+    for (int i = 0; i < n_inst; ++i) {
+      XD::DeviceInstance *d = c->inst[i];
+      std::vector<int> ext(d->getNumExtVars()), in(d->getNumIntVars());
+      for (int k = 0; k < (int)ext.size(); ++k) {
+        int node = inst_nodes[4 * (size_t)i + k];
+        ext[k] = node < 0 ? gnd : node;
+        c->inst_lids[4 * (size_t)i + k] = ext[k];
+      }
+      for (int k = 0; k < (int)in.size(); ++k) in[k] = c->int_lid_base[i] + k;
+      d->registerLIDs(in, ext);
+      std::vector<int> st(d->getNumStateVars()), so(d->getNumStoreVars());
+      c->sta_base[i] = sta;
+      c->n_sta_inst[i] = (int)st.size();
+      for (int k = 0; k < (int)st.size(); ++k) st[k] = sta++;
+      c->sto_base[i] = sto;
+      for (int k = 0; k < (int)so.size(); ++k) so[k] = sto++;
+      d->registerStateLIDs(st);
+      d->registerStoreLIDs(so);
+    }
+    c->n_sta = sta;
+    c->n_sto = sto;
+    const size_t nv = (size_t)c->n_unknowns + 1;
+    c->nextSol.assign(nv, 0.0); c->currSol.assign(nv, 0.0); c->lastSol.assign(nv, 0.0);
+    c->f.assign(nv, 0.0); c->q.assign(nv, 0.0); c->b.assign(nv, 0.0);
+    c->dfdxdvp.assign(nv, 0.0); c->dqdxdvp.assign(nv, 0.0);
+    c->leadF.assign(nv, 0.0); c->leadQ.assign(nv, 0.0);
+    c->flagSol = N_LAS_Vector((int)nv);
+    c->flagSol.putScalar(1.0);
+    const size_t ns = std::max(1, sta), no = std::max(1, sto);
+    c->nextSta.assign(ns, 0.0); c->currSta.assign(ns, 0.0); c->lastSta.assign(ns, 0.0);
+    c->staDeriv.assign(ns, 0.0);
+    c->nextSto.assign(no, 0.0); c->currSto.assign(no, 0.0); c->lastSto.assign(no, 0.0);
+    bind_extern(*c);
+  } catch (std::exception &ex) {
+    if (errbuf && errlen > 0) snprintf(errbuf, errlen, "%s", ex.what());
+    delete c;
+    return 0;
+  }
+  return c;
+}
+
+void xref_destroy(void *h) { delete static_cast<RefCircuit *>(h); }
+
+int xref_num_unknowns(void *h) { return static_cast<RefCircuit *>(h)->n_unknowns; }
+int xref_num_state(void *h) { return static_cast<RefCircuit *>(h)->n_sta; }
+int xref_num_store(void *h) { return static_cast<RefCircuit *>(h)->n_sto; }
+int xref_num_internal(void *h, int i) { return static_cast<RefCircuit *>(h)->int_count[i]; }
+int xref_state_base(void *h, int i) { return static_cast<RefCircuit *>(h)->sta_base[i]; }
+int xref_num_state_inst(void *h, int i) { return static_cast<RefCircuit *>(h)->n_sta_inst[i]; }
+int xref_store_base(void *h, int i) { return static_cast<RefCircuit *>(h)->sto_base[i]; }
+
+// Number of (row, col) pairs in instance i's collapsed Jacobian stamp.
+int xref_stamp_count(void *h, int i) {
+  RefCircuit *c = static_cast<RefCircuit *>(h);
+  const std::vector<std::vector<int> > &js = c->inst[i]->jacobianStamp();
+  int n = 0;
+  for (size_t r = 0; r < js.size(); ++r) n += (int)js[r].size();
+  return n;
+}
+
+// The instance's stamp as (row unknown, col unknown) pairs, using the instance's devLIDs order
+// (external then internal, as in registerJacLIDswithDevs).
+int xref_stamp(void *h, int i, int *rows, int *cols) {
+  RefCircuit *c = static_cast<RefCircuit *>(h);
+  XD::DeviceInstance *d = c->inst[i];
+  const std::vector<std::vector<int> > &js = d->jacobianStamp();
+  std::vector<int> lids;
+  for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[4 * (size_t)i + k]);
+  for (int k = 0; k < d->getNumIntVars(); ++k) lids.push_back(c->int_lid_base[i] + k);
+  int n = 0;
+  for (size_t r = 0; r < js.size(); ++r)
+    for (size_t k = 0; k < js[r].size(); ++k) {
+      rows[n] = lids[r];
+      cols[n] = lids[js[r][k]];
+      ++n;
+    }
+  return n;
+}
+
+// Installs the CSR pattern (n_rows = n_unknowns + 1, ground last) and hands every instance its
+// in-row offsets; returns 0, or -1-i if instance i stamps an entry absent from the pattern.
+int xref_set_pattern(void *h, int n_rows, const int *rowptr, const int *colind) {
+  RefCircuit *c = static_cast<RefCircuit *>(h);
+  if (n_rows != c->n_unknowns + 1) return -1000000;
+  std::vector<int> rp(rowptr, rowptr + n_rows + 1);
+  c->dFdx = N_LAS_Matrix(rp);
+  c->dQdx = N_LAS_Matrix(rp);
+  bind_extern(*c);
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    XD::DeviceInstance *d = c->inst[i];
+    const std::vector<std::vector<int> > &js = d->jacobianStamp();
+    std::vector<int> lids;
+    for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[4 * i + k]);
+    for (int k = 0; k < d->getNumIntVars(); ++k) lids.push_back(c->int_lid_base[i] + k);
+    std::vector<std::vector<int> > jl(js.size());
+    for (size_t r = 0; r < js.size(); ++r) {
+      int row = lids[r];
+      const int *b = colind + rowptr[row], *e = colind + rowptr[row + 1];
+      for (size_t k = 0; k < js[r].size(); ++k) {
+        int col = lids[js[r][k]];
+        const int *p = std::lower_bound(b, e, col);
+        if (p == e || *p != col) return -1 - (int)i;
+        jl[r].push_back((int)(p - b));
+      }
+    }
+    d->registerJacLIDs(jl);
+    d->setupPointers();
+  }
+  return 0;
+}
+
+// One full device load. In/out buffers have the harness layout: vectors n_unknowns+1 long,
+// state n_state, store n_store; CSR values as installed by xref_set_pattern. next_sta/next_sto are
+// read (previous Newton iterate) and overwritten; curr_sta may be written on the first transient step.
+int xref_load(void *h, const xref_flags *fl, const double *next_sol, const double *curr_sol,
+              double *next_sta, double *curr_sta, double *next_sto, const double *curr_sto,
+              double *f, double *q, double *dfdxdvp, double *dqdxdvp, double *dfdx_vals,
+              double *dqdx_vals, int repetitions) {
+  RefCircuit *c = static_cast<RefCircuit *>(h);
+  try {
+    apply_flags(*c, *fl);
+    const size_t nv = (size_t)c->n_unknowns + 1;
+    std::copy(next_sol, next_sol + nv, c->nextSol.begin());
+    if (curr_sol) std::copy(curr_sol, curr_sol + nv, c->currSol.begin());
+    if (c->n_sta) {
+      std::copy(next_sta, next_sta + c->n_sta, c->nextSta.begin());
+      std::copy(curr_sta, curr_sta + c->n_sta, c->currSta.begin());
+    }
+    std::copy(next_sto, next_sto + c->n_sto, c->nextSto.begin());
+    std::copy(curr_sto, curr_sto + c->n_sto, c->currSto.begin());
+    std::vector<double> sto_in(c->nextSto);
+    for (int r = 0; r < std::max(1, repetitions); ++r) {
+      if (r) std::copy(sto_in.begin(), sto_in.end(), c->nextSto.begin());
+      do_load(*c);
+    }
+    std::copy(c->f.begin(), c->f.end(), f);
+    std::copy(c->q.begin(), c->q.end(), q);
+    std::copy(c->dfdxdvp.begin(), c->dfdxdvp.end(), dfdxdvp);
+    std::copy(c->dqdxdvp.begin(), c->dqdxdvp.end(), dqdxdvp);
+    std::copy(c->dFdx.values().begin(), c->dFdx.values().end(), dfdx_vals);
+    std::copy(c->dQdx.values().begin(), c->dQdx.values().end(), dqdx_vals);
+    if (c->n_sta) {
+      std::copy(c->nextSta.begin(), c->nextSta.begin() + c->n_sta, next_sta);
+      std::copy(c->currSta.begin(), c->currSta.begin() + c->n_sta, curr_sta);
+    }
+    std::copy(c->nextSto.begin(), c->nextSto.begin() + c->n_sto, next_sto);
+  } catch (std::exception &ex) {
+    c->err = ex.what();
+    return -1;
+  }
+  return 0;
+}
+
+// Times `repetitions` full loads on the current inputs (set by a previous xref_load); returns
+// seconds of wall time for the whole batch. Each repetition restores the store input first.
+double xref_time_loads(void *h, int repetitions) {
+  RefCircuit *c = static_cast<RefCircuit *>(h);
+  std::vector<double> sto_in(c->nextSto), sta_in(c->nextSta);
+  auto t0 = std::chrono::steady_clock::now();
+  for (int r = 0; r < repetitions; ++r) {
+    std::copy(sto_in.begin(), sto_in.end(), c->nextSto.begin());
+    do_load(*c);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  std::copy(sto_in.begin(), sto_in.end(), c->nextSto.begin());
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+const char *xref_last_error(void *h) { return static_cast<RefCircuit *>(h)->err.c_str(); }
+
+}  // extern "C"

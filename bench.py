@@ -1,0 +1,380 @@
+"""BSIM4 device-load throughput on B200 (loads/s, eval + stamp), with roofline and CPU baseline.
+
+One step = one full device load of every BSIM4 instance of the workload at a fixed Newton
+iterate: the caller-side zeroing of F, Q, dF/dx*dVp, dQ/dx*dVp, dF/dx and dQ/dx (as the
+reference's loader does before every load), then update_state + loadDAEVectors +
+loadDAEMatrices through the C ABI. Metric: instances x steps / device time.
+
+Default workload: the scale configuration — a seeded random INV/NAND2/NOR2 netlist of about
+1M BSIM4 MOSFETs with RC wire ladders (~3M R/C), node voltages uniform in 0-1.2 V, transient
+flags (charges computed, limiting on, newton_iter > 0). The per-step working set (staging,
+maps, CSR values) is several hundred MB, larger than the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mos M]
+
+With N > 1 (torchrun), every rank loads its own replica circuit (seed + rank): the path has no
+exchange step ("replicas only"); value = all ranks' instances x steps / max rank time.
+--impl reference times the reference's own CPU load (the oracle library built from the
+reference sources) on the host cores instead, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BSIM4 device loads/s (eval+stamp)"
+UNIT = "loads/s"
+# Algorithmic HBM bytes per instance per load of the evaluation kernel: reads 4 voltages (32),
+# node indices (16), record index (4), 5 store values (40), vgb (8); writes 48 stamp values (384),
+# 12 store (96), 3 state (24), vgb (8).
+EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mos", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--wire-segments", type=int, default=4)
+    ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_workload(n_mos, seed, wire_segments):
+    from xyce_b200 import netlist
+
+    c = netlist.random_logic(n_mos, seed=seed, wire_segments=wire_segments)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    return c, rowptr, colind
+
+
+def family(c):
+    from xyce_b200 import ModelCard
+
+    cards = [ModelCard(False, {}), ModelCard(True, {})]
+    return cards, c.mos_type.astype(np.int32), c.mos_nodes.astype(np.int32), {"L": c.mos_l, "W": c.mos_w}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.strip().split(", ") for l in open(self.path) if l.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(args, omp=False, sample=None, min_seconds=10.0):
+    """Reference CPU load (oracle library = the reference's own device code) on a bounded sample."""
+    from oracle import xyce_ref as xr
+    from tests.parity import OracleRun
+
+    sample = sample or args.cpu_sample
+    c, rowptr, colind = build_workload(sample, args.seed, args.wire_segments)
+    cards, im, nd, params = family(c)
+    orc = OracleRun(c, cards, im, nd, params, rowptr, colind)
+    if omp:
+        # Same circuit through the OpenMP build of the reference (updateState parallel).
+        orc.ref = xr.RefCircuit(14, [(m.pmos, dict(m.params)) for m in cards], im, nd, params, c.n_unknowns, omp=True)
+        orc.ref.set_pattern(*_oracle_pattern(c, nd, rowptr, colind))
+    n = im.shape[0]
+    sol = np.random.default_rng(args.seed).uniform(0.0, 1.2, c.n_unknowns)
+    from xyce_b200 import SolverFlags
+
+    z3, z14 = np.zeros(3 * n), np.zeros(14 * n)
+    r = orc.load(SolverFlags(newton_iter=1, voltlim=0), sol, z3, z3, z14, z14)
+    orc.load(SolverFlags(newton_iter=1), sol, r["next_sta"], z3, r["next_sto"], z14)
+    reps, dt = 1, orc.ref.time_loads(1)
+    while dt < min_seconds and reps < 10000:
+        reps = max(reps * 2, int(reps * min_seconds / max(dt, 1e-3) * 1.1))
+        dt = orc.ref.time_loads(reps)
+    return n * reps / dt, n, reps, dt
+
+
+def _oracle_pattern(c, inst_nodes, rowptr, colind):
+    nu = c.n_unknowns
+    pairs = [np.stack([np.repeat(np.arange(nu), np.diff(rowptr)), colind], 1)]
+    nd = np.where(inst_nodes < 0, nu, inst_nodes).astype(np.int64)
+    pairs.append(np.stack([np.repeat(nd, 4, axis=1).reshape(-1), np.tile(nd, (1, 4)).reshape(-1)], 1))
+    pr = np.concatenate(pairs, 0)
+    key = np.unique(pr[:, 0] * (nu + 1) + pr[:, 1])
+    rows, cols = key // (nu + 1), (key % (nu + 1)).astype(np.int32)
+    orp = np.zeros(nu + 2, dtype=np.int64)
+    np.add.at(orp, rows + 1, 1)
+    return np.cumsum(orp).astype(np.int32), cols
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from oracle import xyce_ref as xr
+
+    if not xr.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle library (reference sources compiled) not built"}))
+        return
+    omp = xr.available(omp=True)
+    cores = host_cores()
+    if omp:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    samples = []
+    for _ in range(args.warmup):
+        cpu_baseline(args, omp=omp, min_seconds=1.0)
+    for _ in range(args.steps):
+        v, n, reps, dt = cpu_baseline(args, omp=omp, min_seconds=2.0)
+        samples.append((v, dt))
+    value = statistics.median([s[0] for s in samples])
+    total = sum(s[1] for s in samples)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"random INV/NAND2/NOR2 logic, BSIM4, sample of {args.cpu_sample} MOSFETs "
+                                   f"(generator of the {args.mos}-MOSFET scale circuit), fixed Newton iterate"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores if omp else 1, "kind": "reference",
+                             "sample": f"{args.cpu_sample} BSIM4 instances x repeated loads, >=2 s per step; "
+                                       f"{'OpenMP build (updateState parallel over instances)' if omp else 'serial build'}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+
+    from xyce_b200 import Bsim4Device, SolverFlags, _native
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev_id = local
+    c, rowptr, colind = build_workload(args.mos, args.seed + rank, args.wire_segments)
+    cards, im, nd, params = family(c)
+    n = im.shape[0]
+    nu, nnz = c.n_unknowns, int(rowptr[-1])
+    dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), nu, device=dev_id)
+    lib = _native.load()
+    launches = lib.xd_launches_per_load(dev._h)
+    stream = torch.cuda.current_stream()
+    f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
+    rng = np.random.default_rng(args.seed + 17 * rank)
+    sol_h = rng.uniform(0.0, 1.2, nu)
+    sol = torch.as_tensor(sol_h, **f64)
+    sta_n, sta_c = torch.zeros(3 * n, **f64), torch.zeros(3 * n, **f64)
+    sto_n, sto_c = torch.zeros(14 * n, **f64), torch.zeros(14 * n, **f64)
+    out = {k: torch.zeros(nu, **f64) for k in ("f", "q", "fx", "qx")}
+    out["jf"], out["jq"] = torch.zeros(nnz, **f64), torch.zeros(nnz, **f64)
+    # Consistent previous iterate: one load at the same voltages without limiting.
+    dev.load(SolverFlags(newton_iter=1, voltlim=0), sol, sta_n, sta_c, sto_n, sto_c, *out.values())
+    flags = SolverFlags(newton_iter=1)
+
+    def step():
+        for v in out.values():
+            v.zero_()
+        dev.load(flags, sol, sta_n, sta_c, sto_n, sto_c, out["f"], out["q"], out["fx"], out["qx"], out["jf"],
+                 out["jq"])
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev_id) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev_id}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * n / (ms_max * 1e-3)
+
+    # Per-kernel device time on the launching stream (eval kernel vs gathers).
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    t_eval, t_vec, t_mat, reps = 0.0, 0.0, 0.0, max(5, args.steps)
+    for _ in range(reps):
+        for v in out.values():
+            v.zero_()
+        evs[0].record(stream)
+        dev.update_state(flags, sol, sta_n, sta_c, sto_n, sto_c)
+        evs[1].record(stream)
+        dev.load_dae_vectors(out["f"], out["q"], out["fx"], out["qx"])
+        evs[2].record(stream)
+        dev.load_dae_matrices(out["jf"], out["jq"])
+        evs[3].record(stream)
+        torch.cuda.synchronize()
+        t_eval += evs[0].elapsed_time(evs[1])
+        t_vec += evs[1].elapsed_time(evs[2])
+        t_mat += evs[2].elapsed_time(evs[3])
+    t_eval, t_vec, t_mat = t_eval / reps, t_vec / reps, t_mat / reps
+
+    # FP64 FMA pipe throughput (project probe) for the evaluation kernel's compute roofline.
+    probe = torch.zeros(148 * 8 * 256, **f64)
+    iters = 2000
+    lib.xd_probe_fp64_fma(probe.data_ptr(), 148 * 8, iters, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    lib.xd_probe_fp64_fma(probe.data_ptr(), 148 * 8, iters, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fp64_peak_tflops = 2.0 * 148 * 8 * 256 * iters * 64 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+    # End to end through the C ABI with host buffers: H2D of the iterate, D2H of every output.
+    pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h_sol = pin(sol)
+    h_sol.copy_(torch.as_tensor(sol_h))
+    h_sto = pin(sto_n)
+    h_sto.copy_(sto_n.cpu())
+    h_out = {k: pin(v) for k, v in out.items()}
+    h_sta, h_sto_out = pin(sta_n), pin(sto_n)
+    h2d = (h_sol.numel() + h_sto.numel()) * 8
+    d2h = sum(v.numel() for v in h_out.values()) * 8 + (h_sta.numel() + h_sto_out.numel()) * 8
+
+    def e2e_step():
+        sol.copy_(h_sol, non_blocking=True)
+        sto_n.copy_(h_sto, non_blocking=True)
+        step()
+        for k, v in out.items():
+            h_out[k].copy_(v, non_blocking=True)
+        h_sta.copy_(sta_n, non_blocking=True)
+        h_sto_out.copy_(sto_n, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev_id}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import xyce_ref as xr
+
+        if xr.available():
+            v, ns, reps_c, dt = cpu_baseline(args)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"{ns} BSIM4 instances of the same generator x {reps_c} full loads ({dt:.1f} s), "
+                             "serial reference build (-O2), fixed Newton iterate"}
+    hbm_peak, peak_src = measured_peaks()
+    eval_achieved = EVAL_BYTES_PER_INST * n / (t_eval * 1e-3) / 1e9
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"scale circuit: seeded random INV/NAND2/NOR2 logic, {n} BSIM4 MOSFETs per GPU, "
+                               f"{c.res_nodes.shape[0]} R + {c.cap_nodes.shape[0]} C wire parasitics, "
+                               f"{nnz} Jacobian nnz, fixed Newton iterate (node voltages U[0,1.2] V)",
+                   "instances_per_gpu": n, "nnz": nnz, "parallelism": f"replicas x{world}",
+                   "l2": "working set > 126 MB L2 (staging + maps + CSR values), no flush"},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "bsim4_eval_kernel", "achieved": eval_achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": eval_achieved / hbm_peak, "traffic": None,
+                     "note": f"peak = {peak_src} HBM copy bandwidth; algorithmic bytes {EVAL_BYTES_PER_INST} B/instance"},
+        "kernels_ms": {"eval": t_eval, "gather_vectors": t_vec, "gather_matrices": t_mat},
+        "fp64": {"probe_peak_tflops": fp64_peak_tflops},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clk.summary(),
+    }
+    if cpu is not None:
+        result["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(result))
+    dev.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

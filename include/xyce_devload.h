@@ -1,0 +1,153 @@
+/*
+ * xyce_devload.h — C ABI of the B200 MOSFET device-load library (libxyce_b200.so).
+ *
+ * The library evaluates MOSFET instances and stamps F, Q, dF/dx, dQ/dx and the limiter
+ * correction vectors into caller-owned device memory. It replaces, for one MOSFET family, the
+ * three calls the reference's device manager makes on every Newton iteration:
+ *
+ *   xd_update_state   <- Device::updateState(solVec, staVec, stoVec)
+ *                        src/DeviceModelPKG/Core/include/N_DEV_Device.h:315,
+ *                        BSIM4 Master::updateState  src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C:16180
+ *   xd_load_vectors   <- Device::loadDAEVectors(solVec, fVec, qVec, bVec, storeLeadF, storeLeadQ)
+ *                        N_DEV_Device.h:361, BSIM4 Master::loadDAEVectors  N_DEV_MOSFET_B4.C:16303
+ *   xd_load_matrices  <- Device::loadDAEMatrices(dFdx, dQdx)
+ *                        N_DEV_Device.h:384, BSIM4 Master::loadDAEMatrices N_DEV_MOSFET_B4.C:16577
+ *
+ * and the set-up the reference performs when a device is added and its Jacobian entries are
+ * registered (DeviceMgr::addDeviceModel / addDeviceInstance, N_DEV_DeviceMgr.C:1272, 1446;
+ * Instance::registerLIDs / registerStateLIDs / registerStoreLIDs / registerJacLIDs / setupPointers,
+ * N_DEV_MOSFET_B4.C:4996-5626; CktGraphBasic::registerJacLIDswithDevs, N_TOP_CktGraphBasic.C:1092):
+ *
+ *   xd_create         <- addDeviceModel + addDeviceInstance + register*LIDs + setupPointers
+ *   xd_destroy        <- DeviceMgr destructor for the family's Device object
+ *
+ * Conventions
+ *   - Every function returns int: 0 = success, < 0 = error (argument, unsupported model feature
+ *     or CUDA error). xd_last_error() describes the last error on the calling thread.
+ *   - Loads follow the reference's contract: the caller zeroes the outputs once per Newton
+ *     iteration (N_LOA_NonlinearEquationLoader.C:128-133, 226-227) and every device adds (+=)
+ *     its contributions, so several families and other devices can share the same outputs.
+ *   - Device pointers (d_*) are caller-owned device memory on the context's CUDA device. All
+ *     work is ordered on the given CUDA stream (a cudaStream_t passed as void*; NULL = legacy
+ *     default stream). Nothing is allocated or freed after xd_create.
+ *   - Vector layout: one entry per unknown, indexed 0 .. n_unknowns-1; ground is not stored and
+ *     reads as 0 V. Matrices are CSR value arrays for the pattern given at xd_create.
+ *   - State/store layout: a family owns a contiguous block of the state (store) vector laid out
+ *     slot-major: entry (slot s, instance i) at [s * n_inst + i]. BSIM4 has 3 state slots
+ *     (qb, qg, qd) and 14 store slots (vbd vbs vgs vds vges vgms vdes vses vdbs vsbs vdbd vged
+ *     vgmd von) — the reference's per-instance registration order (N_DEV_MOSFET_B4.C:5200, 5267).
+ *   - Results are deterministic: no atomics; every output entry is summed in a fixed order.
+ */
+#ifndef XYCE_DEVLOAD_H
+#define XYCE_DEVLOAD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xd_ctx xd_ctx;
+
+/* Solver state the loads read (SolverState / DeviceOptions fields,
+ * src/DeviceModelPKG/Core/include/N_DEV_SolverState.h:93-204, N_DEV_DeviceOptions.h). */
+typedef struct xd_flags {
+  int dcop;        /* dcopFlag: DC operating point                        */
+  int init_tran;   /* initTranFlag: first time step of a transient         */
+  int newton_iter; /* newtonIter: Newton iteration count within the step   */
+  int init_jct;    /* initJctFlag: junction initialisation (first DCOP it) */
+  int init_fix;    /* initFixFlag                                          */
+  int transient;   /* transientFlag                                        */
+  int tranop;      /* tranopFlag: DCOP phase of a transient                */
+  int acop;        /* acopFlag                                             */
+  int voltlim;     /* voltageLimiterFlag (.OPTIONS DEVICE VOLTLIM)         */
+  int input_op;    /* inputOPFlag (not modelled: must be 0)                */
+  double gmin;     /* DeviceOptions::gmin                                  */
+  double pdt;      /* SolverState::pdt (alpha/dt)                          */
+} xd_flags;
+
+/* One MOSFET family (one reference Device object): its .MODEL cards and instances. */
+typedef struct xd_mosfet_family {
+  int level;                             /* 14 or 54 = BSIM4                                  */
+  int n_models;                          /* number of .MODEL cards                            */
+  const int *model_is_pmos;              /* [n_models] 0 = NMOS, 1 = PMOS                     */
+  const int *model_nparams;              /* [n_models] (name, value) pairs per card           */
+  const char *const *model_param_names;  /* concatenated over cards, netlist names            */
+  const double *model_param_values;      /* same order                                        */
+  int n_inst;                            /* number of instances                               */
+  const int *inst_model;                 /* [n_inst] card index                               */
+  const int *inst_nodes;                 /* [4*n_inst] D, G, S, B unknown index; -1 = ground  */
+  int n_inst_params;                     /* instance-line parameter names                     */
+  const char *const *inst_param_names;   /* e.g. "L", "W", "NF", "AD", "DELVTO", "M"          */
+  const double *inst_param_values;       /* [n_inst * n_inst_params]; NaN = not given         */
+  double temp_c;                         /* .OPTIONS DEVICE TEMP (Celsius)                    */
+  double tnom_c;                         /* .OPTIONS DEVICE TNOM (Celsius)                    */
+} xd_mosfet_family;
+
+/* Jacobian sparsity pattern over the unknowns (host memory, read during xd_create only).
+ * Column indices must be sorted within each row and must include every entry the family's
+ * stamps touch (the reference's topology builds the same union of device stamps). */
+typedef struct xd_csr {
+  int n_rows;          /* number of unknowns                 */
+  const int *rowptr;   /* [n_rows + 1]                       */
+  const int *colind;   /* [rowptr[n_rows]]                   */
+} xd_csr;
+
+/* Builds the family on CUDA device `cuda_device`: processes model cards (defaults,
+ * temperature, size binning), uploads per-instance constants, and precomputes the
+ * stamp-to-output gather maps. Fails (< 0) on unsupported model features. */
+int xd_create(const xd_mosfet_family *family, const xd_csr *pattern, int cuda_device, xd_ctx **out);
+
+/* Releases all device memory of the context. */
+int xd_destroy(xd_ctx *ctx);
+
+/* Description of the last error on the calling thread ("" if none). */
+const char *xd_last_error(void);
+
+int xd_num_instances(const xd_ctx *ctx);
+int xd_num_state_slots(const xd_ctx *ctx); /* per instance: 3 for BSIM4  */
+int xd_num_store_slots(const xd_ctx *ctx); /* per instance: 14 for BSIM4 */
+
+/* Evaluates every instance at the solution d_sol. Reads the previous iterate's limited
+ * voltages from d_next_sto (newton_iter > 0) or d_curr_sto (newton_iter == 0), writes the new
+ * store entries into d_next_sto (except vged/vgmd, which the reference does not write) and the
+ * charges into d_next_sta; on the first Newton step of the first transient step it also writes
+ * the charges into d_curr_sta (N_DEV_MOSFET_B4.C:16254-16289). The stamp values are kept in the
+ * context for the following xd_load_vectors / xd_load_matrices calls. */
+int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta,
+                    double *d_curr_sta, double *d_next_sto, const double *d_curr_sto, void *stream);
+
+/* Adds the family's F, Q, dF/dx*dVp and dQ/dx*dVp contributions (last xd_update_state). */
+int xd_load_vectors(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp,
+                    void *stream);
+
+/* Adds the family's dF/dx and dQ/dx contributions into CSR value arrays of the pattern. */
+int xd_load_matrices(xd_ctx *ctx, double *d_dfdx_vals, double *d_dqdx_vals, void *stream);
+
+/* xd_update_state + xd_load_vectors + xd_load_matrices in one call. */
+int xd_load(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta, double *d_curr_sta,
+            double *d_next_sto, const double *d_curr_sto, double *d_f, double *d_q, double *d_dfdxdvp,
+            double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals, void *stream);
+
+/* Test and error-bound support: like the two load calls, but adds |term| instead of term, so the
+ * outputs hold, per entry, the sum of absolute contributions (the scale of the rounding error of
+ * that entry's sum). */
+int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp,
+                double *d_dfdx_vals, double *d_dqdx_vals, void *stream);
+
+/* Copies the per-instance local stamps of the last xd_update_state to host memory:
+ * [48 * n_inst] doubles, slot-major (slot k of instance i at [k * n_inst + i]); slots 0-15 are
+ * the F, Q, dFdxdVp, dQdxdVp terminal entries (D, G, S, B each), 16-31 dF/dx and 32-47 dQ/dx
+ * as 4x4 row-major terminal blocks. Synchronises the stream. */
+int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream);
+
+/* Diagnostics. xd_launches_per_load: kernels one xd_load enqueues (eval + gathers).
+ * xd_probe_fp64_fma: runs `blocks` x 256 threads, each doing `iters` x 64 independent-chain
+ * FP64 FMAs in registers, and writes one checksum per thread into d_out (blocks*256 doubles);
+ * timing it gives the FP64 FMA-pipe throughput the evaluation kernel is measured against. */
+int xd_launches_per_load(const xd_ctx *ctx);
+int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XYCE_DEVLOAD_H */

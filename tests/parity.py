@@ -1,0 +1,110 @@
+"""Shared helpers for parity tests: the same circuit through the oracle and through the C ABI."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from oracle import xyce_ref as xr
+from xyce_b200 import netlist
+from xyce_b200.device import ModelCard, SolverFlags
+
+# Relative tolerance per entry, and the rounding floor as a multiple of the entry's sum of
+# absolute contributions (summation order differs between the two implementations only).
+RTOL = 1e-12
+ABS_SUM_FLOOR = 1e-14
+
+
+def family_inputs(c: netlist.Circuit, cards=None, extra_params=None):
+    """(models, inst_model, inst_nodes, inst_params) for the circuit's MOSFETs (BSIM4)."""
+    if cards is None:
+        cards = [ModelCard(False, {}), ModelCard(True, {})]
+    inst_model = c.mos_type.astype(np.int32)
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float)}
+    if extra_params:
+        params.update(extra_params)
+    return cards, inst_model, c.mos_nodes.astype(np.int32), params
+
+
+def flags_dict(f: SolverFlags) -> dict:
+    return dict(dcop=f.dcop, init_tran=f.init_tran, newton_iter=f.newton_iter, init_jct=f.init_jct,
+                init_fix=f.init_fix, transient=f.transient, tranop=f.tranop, acop=f.acop, voltlim=f.voltlim,
+                input_op=f.input_op, gmin=f.gmin, pdt=f.pdt)
+
+
+class OracleRun:
+    """The reference's own device objects for the circuit's MOSFETs, on the product's pattern."""
+
+    def __init__(self, c: netlist.Circuit, cards, inst_model, inst_nodes, params, rowptr, colind, level=14):
+        self.c = c
+        models = [(m.pmos, dict(m.params)) for m in cards]
+        nu = c.n_unknowns
+        self.ref = xr.RefCircuit(level, models, inst_model, inst_nodes, params, nu)
+        assert self.ref.n_unknowns == nu, "oracle created internal nodes the product does not model"
+        n = inst_model.shape[0]
+        # Oracle pattern: the product's pattern plus the ground row / column entries the stamps hit.
+        g = nu
+        pairs = [np.stack([np.repeat(np.arange(nu), np.diff(rowptr)), colind], 1)]
+        nd = np.where(inst_nodes < 0, g, inst_nodes).astype(np.int64)
+        rr = np.repeat(nd, 4, axis=1).reshape(-1)
+        cc = np.tile(nd, (1, 4)).reshape(-1)
+        pairs.append(np.stack([rr, cc], 1))
+        pr = np.concatenate(pairs, 0)
+        key = np.unique(pr[:, 0] * (nu + 1) + pr[:, 1])
+        rows, cols = key // (nu + 1), (key % (nu + 1)).astype(np.int32)
+        orp = np.zeros(nu + 2, dtype=np.int64)
+        np.add.at(orp, rows + 1, 1)
+        orp = np.cumsum(orp).astype(np.int32)
+        self.ref.set_pattern(orp, cols)
+        # Map each product CSR entry to the oracle CSR entry with the same (row, col).
+        prow = np.repeat(np.arange(nu), np.diff(rowptr))
+        okey = rows * (nu + 1) + cols
+        self.map = np.searchsorted(okey, prow * (nu + 1) + colind)
+        self.n = n
+        self.sta_base = np.array([self.ref.state_base(i) for i in range(n)], dtype=np.int64)
+        self.sto_base = np.array([self.ref.store_base(i) for i in range(n)], dtype=np.int64)
+
+    def to_aos_sto(self, soa):
+        """Product slot-major store block -> oracle per-instance layout."""
+        out = np.zeros(max(1, self.ref.n_store))
+        for s in range(14):
+            out[self.sto_base + s] = soa[s * self.n:(s + 1) * self.n]
+        return out
+
+    def to_aos_sta(self, soa):
+        out = np.zeros(max(1, self.ref.n_state))
+        for s in range(3):
+            out[self.sta_base + s] = soa[s * self.n:(s + 1) * self.n]
+        return out
+
+    def from_aos_sto(self, aos):
+        return np.concatenate([aos[self.sto_base + s] for s in range(14)])
+
+    def from_aos_sta(self, aos):
+        return np.concatenate([aos[self.sta_base + s] for s in range(3)])
+
+    def load(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa):
+        nu = self.c.n_unknowns
+        s = np.zeros(nu + 1)
+        s[:nu] = sol
+        out = self.ref.load(xr.make_flags(**flags_dict(flags)), s, self.to_aos_sta(next_sta_soa),
+                            self.to_aos_sta(curr_sta_soa), self.to_aos_sto(next_sto_soa),
+                            self.to_aos_sto(curr_sto_soa))
+        return dict(f=out.f[:nu], q=out.q[:nu], dfdxdvp=out.dfdxdvp[:nu], dqdxdvp=out.dqdxdvp[:nu],
+                    dfdx=out.dfdx[self.map], dqdx=out.dqdx[self.map], next_sta=self.from_aos_sta(out.next_sta),
+                    curr_sta=self.from_aos_sta(out.curr_sta), next_sto=self.from_aos_sto(out.next_sto))
+
+
+def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR):
+    """Returns (n_bad, worst ratio of |diff| to the allowed error)."""
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    d = np.abs(got - ref)
+    allow = rtol * np.maximum(np.abs(got), np.abs(ref))
+    if abs_sum is not None:
+        allow = allow + floor * np.asarray(abs_sum)
+    allow = np.maximum(allow, 1e-300)
+    ratio = d / allow
+    bad = int(np.count_nonzero(d > allow))
+    worst = float(ratio.max()) if ratio.size else 0.0
+    return bad, worst

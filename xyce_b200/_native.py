@@ -1,0 +1,94 @@
+"""Loader for the package's native library (libxyce_b200.so) and its C ABI (include/xyce_devload.h).
+
+The library is built in-tree by ``xyce_b200.build.build()``. There is no fallback: if the
+library is missing or was built for another architecture, loading fails with an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libxyce_b200.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_cpp = ctypes.POINTER(ctypes.c_char_p)
+
+
+class XdFlags(ctypes.Structure):
+    """Mirror of ``xd_flags`` (SolverState / DeviceOptions fields the loads read)."""
+
+    _fields_ = [
+        ("dcop", ctypes.c_int), ("init_tran", ctypes.c_int), ("newton_iter", ctypes.c_int),
+        ("init_jct", ctypes.c_int), ("init_fix", ctypes.c_int), ("transient", ctypes.c_int),
+        ("tranop", ctypes.c_int), ("acop", ctypes.c_int), ("voltlim", ctypes.c_int),
+        ("input_op", ctypes.c_int), ("gmin", ctypes.c_double), ("pdt", ctypes.c_double),
+    ]
+
+
+class XdMosfetFamily(ctypes.Structure):
+    _fields_ = [
+        ("level", ctypes.c_int), ("n_models", ctypes.c_int), ("model_is_pmos", _ip), ("model_nparams", _ip),
+        ("model_param_names", _cpp), ("model_param_values", _dp), ("n_inst", ctypes.c_int),
+        ("inst_model", _ip), ("inst_nodes", _ip), ("n_inst_params", ctypes.c_int),
+        ("inst_param_names", _cpp), ("inst_param_values", _dp), ("temp_c", ctypes.c_double),
+        ("tnom_c", ctypes.c_double),
+    ]
+
+
+class XdCsr(ctypes.Structure):
+    _fields_ = [("n_rows", ctypes.c_int), ("rowptr", _ip), ("colind", _ip)]
+
+
+# Every symbol the header declares, with its ctypes signature.
+SIGNATURES = {
+    "xd_create": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), ctypes.POINTER(XdCsr), ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_last_error": (ctypes.c_char_p, []),
+    "xd_num_instances": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_num_state_slots": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_num_store_slots": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_update_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags), ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_load_vectors": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4 + [ctypes.c_void_p]),
+    "xd_load_matrices": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_load": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
+    "xd_load_abs": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 7),
+    "xd_copy_stamps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_launches_per_load": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_probe_fp64_fma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+}
+
+_LIB = None
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load():
+    """Loads libxyce_b200.so and binds every C-ABI entry point (raises if it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise NativeError(f"native library not built: {LIB_PATH} (run python -c 'import xyce_b200.build as b; b.build()')")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = _LIB.xd_last_error().decode() if _LIB is not None else ""
+        raise NativeError(f"{what} failed ({rc}): {msg}")

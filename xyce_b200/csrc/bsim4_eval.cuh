@@ -1,0 +1,2060 @@
+// BSIM4 (v4.6.1) per-instance load: voltage limiting, DC and charge model, and the stamp values
+// for F, Q, dF/dx, dQ/dx and the limiter correction vectors, for one instance.
+//
+// One call evaluates one instance entirely in registers (one CUDA thread per instance on the
+// device). It restates, in the reference's order of floating-point operations:
+//   Instance::updateIntermediateVars    N_DEV_MOSFET_B4.C:7744-11918
+//   Instance::setupCapacitors_oldDAE     N_DEV_MOSFET_B4.C:12616-13045 (charge bookkeeping only)
+//   Instance::setupCapacitors_newDAE     N_DEV_MOSFET_B4.C:12357-12608
+//   Master::updateState                  N_DEV_MOSFET_B4.C:16180-16293
+//   Instance::setupFVectorVars           N_DEV_MOSFET_B4.C:13525-13855
+//   Instance::auxChargeCalculations      N_DEV_MOSFET_B4.C:12216-12350
+//   Master::loadDAEVectors / loadDAEMatrices  N_DEV_MOSFET_B4.C:16303-16567, 16577-17268
+// for the configuration the set-up accepts: rgateMod = rbodyMod = trnqsMod = acnqsMod = rdsMod = 0,
+// igcMod = igbMod = 0, capMod = 2, no source/drain resistance nodes, no initial conditions. With
+// no internal nodes the 11 stamp rows collapse onto the 4 terminals D, G, S, B.
+//
+// Local stamp layout (terminal order D=0, G=1, S=2, B=3):
+//   vec[0..3]   F,  vec[4..7] Q,  vec[8..11] dFdxdVp,  vec[12..15] dQdxdVp
+//   jf[r*4+c]   dF_r/dx_c,  jq[r*4+c]  dQ_r/dx_c
+// Within one slot the terms are accumulated in the reference's statement order.
+#pragma once
+
+#include "bsim4_fields.h"
+#include "xd_consts.h"
+
+namespace xb4 {
+
+struct LoadFlags {
+  int dcop, init_tran, newton_iter, init_jct, init_fix, transient, tranop, acop, voltlim, input_op;
+  double gmin, pdt;
+};
+
+// Store slots (registerStoreLIDs order, N_DEV_MOSFET_B4.C:5267-5290) and state slots
+// (registerStateLIDs order, :5200-5230).
+enum StoreSlot { s_vbd, s_vbs, s_vgs, s_vds, s_vges, s_vgms, s_vdes, s_vses, s_vdbs, s_vsbs, s_vdbd, s_vged, s_vgmd, s_von, kNumStore };
+enum StateSlot { t_qb, t_qg, t_qd, kNumState };
+enum { kNumVec = 16, kNumMat = 16, kNumStage = kNumVec + 2 * kNumMat };
+
+struct LoadOut {
+  double vec[kNumVec];
+  double jf[kNumMat];
+  double jq[kNumMat];
+  double sto[kNumStore];  // s_vged and s_vgmd are not written by the load (kept from the input)
+  double sta[kNumState];
+  bool write_curr_sta;    // first Newton step of the first transient step: also write currSta
+  double vgb;             // this load's vgb (the next load's "vgb_orig")
+};
+
+// Field-major record view: field f of this instance's record.
+struct RecPtr {
+  const double *base;
+  int stride;
+  XD_HD double operator()(int f) const {
+#if defined(__CUDA_ARCH__)
+    return __ldg(base + (size_t)f * stride);
+#else
+    return base[(size_t)f * stride];
+#endif
+  }
+};
+
+XD_HD void poly_depletion(double phi, double ngate, double epsgate, double coxe, double Vgs_arg, double &Vgs_eff,
+                          double &dVgs_eff_dVg) {
+  if ((ngate > 1.0e18) && (ngate < 1.0e25) && (Vgs_arg > phi) && (epsgate != 0)) {
+    double T1 = 1.0e6 * xdc::CONSTQ * epsgate * ngate / (coxe * coxe);
+    double T8 = Vgs_arg - phi;
+    double T4 = sqrt(1.0 + 2.0 * T8 / T1);
+    double T2 = 2.0 * T8 / (T4 + 1.0);
+    double T3 = 0.5 * T2 * T2 / T1;
+    double T7 = 1.12 - T3 - 0.05;
+    double T6 = sqrt(T7 * T7 + 0.224);
+    double T5 = 1.12 - 0.5 * (T7 + T6);
+    Vgs_eff = Vgs_arg - T5;
+    dVgs_eff_dVg = 1.0 - (0.5 - 0.5 / T4) * (1.0 + T7 / T6);
+  } else {
+    Vgs_eff = Vgs_arg;
+    dVgs_eff_dVg = 1.0;
+  }
+}
+
+// V[4] = node voltages (D, G, S, B); sto_old = the store values the limiter compares against
+// (currSto on Newton step 0 of a transient step, nextSto otherwise); vgb_orig = the previous load's
+// vgb of this instance (0 before the first load), which the reference uses as the "original" vgb.
+template <class RV>
+XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
+                      LoadOut &o) {
+  using namespace xdc;
+#define P(x) P_(f_##x)
+  const double dtype = P(dtype);
+  const int mobMod = (int)P(mobMod);
+  const int dioMod = (int)P(dioMod);
+  const int tempMod = (int)P(tempMod);
+  const double gmin = fl.gmin;
+  const double nf = P(nf);
+  const double vth0 = P(vth0);
+  const double M = P(mult);
+  const bool OFF = P(off) != 0.0;
+
+  const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
+
+  // Node and branch voltages (:7932-8030), collapsed topology.
+  const double Vd = V[0], Vge = V[1], Vs = V[2], Vb = V[3];
+  const double Vdp = Vd, Vsp = Vs, Vgp = Vge, Vbp = Vb, Vgm = Vge, Vdb = Vb, Vsb = Vb;
+  (void)Vdp; (void)Vgp; (void)Vbp; (void)Vgm; (void)Vdb; (void)Vsb;
+  double vds = dtype * (Vd - Vsp);
+  double vgs = dtype * (Vge - Vsp);
+  double vbs = dtype * (Vb - Vsp);
+  double vges = dtype * (Vge - Vsp);
+  double vgms = dtype * (Vge - Vsp);
+  double vdbs = dtype * (Vb - Vsp);
+  double vsbs = dtype * (Vb - Vsp);
+  double vses = dtype * (Vs - Vsp);
+  double vdes = dtype * (Vd - Vsp);
+  double vbd = vbs - vds;
+  double vdbd = vdbs - vds;
+  double vgd = vgs - vds;
+  double vged = vges - vds;
+  double vgmd = vgms - vds;
+  double vgmb = vgms - vbs;
+  double vbs_jct = vbs;
+  double vbd_jct = vbd;
+  int origFlag = 1;
+  const double vbd_orig = vbd, vbs_orig = vbs, vgs_orig = vgs, vds_orig = vds, vgd_orig = vgd;
+  const double vges_orig = vges, vgms_orig = vgms, vdes_orig = vdes, vses_orig = vses, vdbs_orig = vdbs;
+  const double vsbs_orig = vsbs, vdbd_orig = vdbd, vged_orig = vged, vgmd_orig = vgmd;
+  const double vbs_jct_orig = vbs_jct, vbd_jct_orig = vbd_jct, vgmb_orig = vgmb;
+  // The reference takes vgb_orig from the instance's vgb member before it is recomputed, i.e. the
+  // previous load's value (:8026); in the limiter test below vgb therefore equals vgb_orig.
+  double vgb = vgb_orig;
+
+  // Initial-condition handling (:8051-8097). inputOP with a flag vector is not modelled.
+  if (fl.init_jct && !OFF && fl.voltlim) {
+    vds = 0.1;
+    vdes = 0.11;
+    vses = -0.01;
+    vgs = vges = vgms = dtype * vth0 + 0.1;
+    origFlag = 0;
+    vbs = vdbs = vsbs = 0.0;
+    vbd = vbs - vds;
+    vdbd = vdbs - vds;
+    vgd = vgs - vds;
+    vged = vges - vds;
+    vgmd = vgms - vds;
+  } else if ((fl.init_fix || fl.init_jct) && OFF) {
+    vds = vgs = vbs = vges = vgms = 0.0;
+    vds = vsbs = vdes = vses = 0.0;
+  }
+
+  // Previous-iterate voltages for limiting (:8099-8166).
+  double vbd_old, vbs_old, vgs_old, vds_old, von_local;
+  if (fl.newton_iter == 0 && fl.dcop) {
+    vbd_old = vbd;
+    vbs_old = vbs;
+    vgs_old = vgs;
+    vds_old = vds;
+    von_local = 0.0;
+  } else {
+    vbd_old = sto_old[s_vbd];
+    vbs_old = sto_old[s_vbs];
+    vgs_old = sto_old[s_vgs];
+    vds_old = sto_old[s_vds];
+    von_local = sto_old[s_von];
+  }
+  const double vgd_old = vgs_old - vds_old;
+
+  if (fl.voltlim && !(fl.init_fix && OFF)) {
+    int Check = 0;
+    if (fl.newton_iter >= 0 && !(fl.init_jct)) {
+      if (vds_old >= 0.0) {
+        vgs = fetlim(vgs, vgs_old, von_local);
+        vds = vgs - vgd;
+        vds = limvds(vds, vds_old);
+        vgd = vgs - vds;
+      } else {
+        vgd = fetlim(vgd, vgd_old, von_local);
+        vds = vgs - vgd;
+        vds = -limvds(-vds, -vds_old);
+        vgs = vgd + vds;
+      }
+      if (vds >= 0.0) {
+        vbs = pnjlim(vbs, vbs_old, CONSTvt0, P(vcrit), &Check);
+        vbd = vbs - vds;
+      } else {
+        vbd = pnjlim(vbd, vbd_old, CONSTvt0, P(vcrit), &Check);
+        vbs = vbd + vds;
+      }
+    }
+    (void)Check;
+    if (fabs(vbd_orig - vbd) > kMachPrec || fabs(vbs_orig - vbs) > kMachPrec || fabs(vgs_orig - vgs) > kMachPrec ||
+        fabs(vds_orig - vds) > kMachPrec || fabs(vgd_orig - vgd) > kMachPrec || fabs(vges_orig - vges) > kMachPrec ||
+        fabs(vgms_orig - vgms) > kMachPrec || fabs(vdes_orig - vdes) > kMachPrec ||
+        fabs(vses_orig - vses) > kMachPrec || fabs(vdbs_orig - vdbs) > kMachPrec ||
+        fabs(vsbs_orig - vsbs) > kMachPrec || fabs(vdbd_orig - vdbd) > kMachPrec ||
+        fabs(vbs_jct_orig - vbs_jct) > kMachPrec || fabs(vbd_jct_orig - vbd_jct) > kMachPrec ||
+        fabs(vgmb_orig - vgmb) > kMachPrec || fabs(vgb_orig - vgb) > kMachPrec ||
+        fabs(vged_orig - vged) > kMachPrec || fabs(vgmd_orig - vgmd) > kMachPrec) {
+      origFlag = 0;
+    }
+  }
+  vbd = vbs - vds;
+  vgd = vgs - vds;
+  vgb = vgs - vbs;
+  vged = vges - vds;
+  vgmd = vgms - vds;
+  vgmb = vgms - vbs;
+  vdbd = vdbs - vds;
+  vbs_jct = vbs;
+  vbd_jct = vbd;
+
+  double T0, T1, T2, T3, T4, T5, T6, T7, T8, T9, T10, T11, T12, T13, T14;
+  double dT0_dVg, dT0_dVd, dT0_dVb, dT1_dVg, dT1_dVd, dT1_dVb, dT2_dVg, dT2_dVd, dT2_dVb;
+  double dT3_dVg, dT3_dVd, dT3_dVb, dT4_dVd, dT5_dVg, dT5_dVd, dT5_dVb, dT6_dVg, dT6_dVd, dT6_dVb;
+  double dT8_dVg, dT8_dVd, dT8_dVb, dT9_dVg, dT9_dVd, dT9_dVb, dT10_dVg, dT10_dVd, dT10_dVb;
+  double tmp, tmp1, tmp2, tmp3, tmp4;
+
+  // Source/drain junction diodes (:8420-8660).
+  const double Aseff = P(Aseff), Pseff = P(Pseff), Adeff = P(Adeff), Pdeff = P(Pdeff), weffCJ = P(weffCJ);
+  double gbs, cbs, gbd, cbd;
+  {
+    const double Nvtms = P(vtm) * P(SjctEmissionCoeff);
+    double SourceSatCurrent;
+    if ((Aseff <= 0.0) && (Pseff <= 0.0))
+      SourceSatCurrent = 1.0e-14;
+    else
+      SourceSatCurrent = Aseff * P(SjctTempSatCurDensity) + Pseff * P(SjctSidewallTempSatCurDensity) +
+                         weffCJ * nf * P(SjctGateSidewallTempSatCurDensity);
+    if (SourceSatCurrent <= 0.0) {
+      gbs = gmin;
+      cbs = gbs * vbs_jct;
+    } else {
+      switch (dioMod) {
+        case 0: {
+          double evbs = exp(vbs_jct / Nvtms);
+          T1 = P(xjbvs) * exp(-(P(bvs) + vbs_jct) / Nvtms);
+          gbs = SourceSatCurrent * (evbs + T1) / Nvtms + gmin;
+          cbs = SourceSatCurrent * (evbs + P(XExpBVS) - T1 - 1.0) + gmin * vbs_jct;
+          break;
+        }
+        case 1:
+          T2 = vbs_jct / Nvtms;
+          if (T2 < -CONSTEXP_THRESHOLD) {
+            gbs = gmin;
+            cbs = SourceSatCurrent * (CONSTMIN_EXP - 1.0) + gmin * vbs_jct;
+          } else if (vbs_jct <= P(vjsmFwd)) {
+            double evbs = exp(T2);
+            gbs = SourceSatCurrent * evbs / Nvtms + gmin;
+            cbs = SourceSatCurrent * (evbs - 1.0) + gmin * vbs_jct;
+          } else {
+            T0 = P(IVjsmFwd) / Nvtms;
+            gbs = T0 + gmin;
+            cbs = P(IVjsmFwd) - SourceSatCurrent + T0 * (vbs_jct - P(vjsmFwd)) + gmin * vbs_jct;
+          }
+          break;
+        default: {
+          double evbs, devbs_dvb;
+          if (vbs_jct < P(vjsmRev)) {
+            T0 = vbs_jct / Nvtms;
+            if (T0 < -CONSTEXP_THRESHOLD) {
+              evbs = CONSTMIN_EXP;
+              devbs_dvb = 0.0;
+            } else {
+              evbs = exp(T0);
+              devbs_dvb = evbs / Nvtms;
+            }
+            T1 = evbs - 1.0;
+            T2 = P(IVjsmRev) + P(SslpRev) * (vbs_jct - P(vjsmRev));
+            gbs = devbs_dvb * T2 + T1 * P(SslpRev) + gmin;
+            cbs = T1 * T2 + gmin * vbs_jct;
+          } else if (vbs_jct <= P(vjsmFwd)) {
+            T0 = vbs_jct / Nvtms;
+            if (T0 < -CONSTEXP_THRESHOLD) {
+              evbs = CONSTMIN_EXP;
+              devbs_dvb = 0.0;
+            } else {
+              evbs = exp(T0);
+              devbs_dvb = evbs / Nvtms;
+            }
+            T1 = (P(bvs) + vbs_jct) / Nvtms;
+            if (T1 > CONSTEXP_THRESHOLD) {
+              T2 = CONSTMIN_EXP;
+              T3 = 0.0;
+            } else {
+              T2 = exp(-T1);
+              T3 = -T2 / Nvtms;
+            }
+            gbs = SourceSatCurrent * (devbs_dvb - P(xjbvs) * T3) + gmin;
+            cbs = SourceSatCurrent * (evbs + P(XExpBVS) - 1.0 - P(xjbvs) * T2) + gmin * vbs_jct;
+          } else {
+            gbs = P(SslpFwd) + gmin;
+            cbs = P(IVjsmFwd) + P(SslpFwd) * (vbs_jct - P(vjsmFwd)) + gmin * vbs_jct;
+          }
+          break;
+        }
+      }
+    }
+    const double Nvtmd = P(vtm) * P(DjctEmissionCoeff);
+    double DrainSatCurrent;
+    if ((Adeff <= 0.0) && (Pdeff <= 0.0))
+      DrainSatCurrent = 1.0e-14;
+    else
+      DrainSatCurrent = Adeff * P(DjctTempSatCurDensity) + Pdeff * P(DjctSidewallTempSatCurDensity) +
+                        weffCJ * nf * P(DjctGateSidewallTempSatCurDensity);
+    if (DrainSatCurrent <= 0.0) {
+      gbd = gmin;
+      cbd = gbd * vbd_jct;
+    } else {
+      switch (dioMod) {
+        case 0: {
+          double evbd = exp(vbd_jct / Nvtmd);
+          T1 = P(xjbvd) * exp(-(P(bvd) + vbd_jct) / Nvtmd);
+          gbd = DrainSatCurrent * (evbd + T1) / Nvtmd + gmin;
+          cbd = DrainSatCurrent * (evbd + P(XExpBVD) - T1 - 1.0) + gmin * vbd_jct;
+          break;
+        }
+        case 1:
+          T2 = vbd_jct / Nvtmd;
+          if (T2 < -CONSTEXP_THRESHOLD) {
+            gbd = gmin;
+            cbd = DrainSatCurrent * (CONSTMIN_EXP - 1.0) + gmin * vbd_jct;
+          } else if (vbd_jct <= P(vjdmFwd)) {
+            double evbd = exp(T2);
+            gbd = DrainSatCurrent * evbd / Nvtmd + gmin;
+            cbd = DrainSatCurrent * (evbd - 1.0) + gmin * vbd_jct;
+          } else {
+            T0 = P(IVjdmFwd) / Nvtmd;
+            gbd = T0 + gmin;
+            cbd = P(IVjdmFwd) - DrainSatCurrent + T0 * (vbd_jct - P(vjdmFwd)) + gmin * vbd_jct;
+          }
+          break;
+        default: {
+          double evbd, devbd_dvb;
+          if (vbd_jct < P(vjdmRev)) {
+            T0 = vbd_jct / Nvtmd;
+            if (T0 < -CONSTEXP_THRESHOLD) {
+              evbd = CONSTMIN_EXP;
+              devbd_dvb = 0.0;
+            } else {
+              evbd = exp(T0);
+              devbd_dvb = evbd / Nvtmd;
+            }
+            T1 = evbd - 1.0;
+            T2 = P(IVjdmRev) + P(DslpRev) * (vbd_jct - P(vjdmRev));
+            gbd = devbd_dvb * T2 + T1 * P(DslpRev) + gmin;
+            cbd = T1 * T2 + gmin * vbd_jct;
+          } else if (vbd_jct <= P(vjdmFwd)) {
+            T0 = vbd_jct / Nvtmd;
+            if (T0 < -CONSTEXP_THRESHOLD) {
+              evbd = CONSTMIN_EXP;
+              devbd_dvb = 0.0;
+            } else {
+              evbd = exp(T0);
+              devbd_dvb = evbd / Nvtmd;
+            }
+            T1 = (P(bvd) + vbd_jct) / Nvtmd;
+            if (T1 > CONSTEXP_THRESHOLD) {
+              T2 = CONSTMIN_EXP;
+              T3 = 0.0;
+            } else {
+              T2 = exp(-T1);
+              T3 = -T2 / Nvtmd;
+            }
+            gbd = DrainSatCurrent * (devbd_dvb - P(xjbvd) * T3) + gmin;
+            cbd = DrainSatCurrent * (evbd + P(XExpBVD) - 1.0 - P(xjbvd) * T2) + gmin * vbd_jct;
+          } else {
+            gbd = P(DslpFwd) + gmin;
+            cbd = P(IVjdmFwd) + P(DslpFwd) * (vbd_jct - P(vjdmFwd)) + gmin * vbd_jct;
+          }
+          break;
+        }
+      }
+    }
+  }
+
+  // Trap-assisted tunnelling and recombination for reverse bias (:8661-8760).
+  {
+    const double vtm0 = P(vtm0);
+    const double Nvtmrssws = vtm0 * P(njtsswstemp);
+    const double Nvtmrsswgs = vtm0 * P(njtsswgstemp);
+    const double Nvtmrss = vtm0 * P(njtsstemp);
+    const double Nvtmrsswd = vtm0 * P(njtsswdtemp);
+    const double Nvtmrsswgd = vtm0 * P(njtsswgdtemp);
+    const double Nvtmrsd = vtm0 * P(njtsdtemp);
+    double e1, e2, e3, e4, e5, e6, d1, d2, d3, d4, d5, d6;
+    const double vtss = P(vtss), vtsd = P(vtsd), vtssws = P(vtssws), vtsswd = P(vtsswd), vtsswgs = P(vtsswgs),
+                 vtsswgd = P(vtsswgd);
+    if ((vtss - vbs_jct) < (vtss * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbs_jct / Nvtmrss * T9; dexp(T0, e1, T10); d1 = T10 / Nvtmrss * T9;
+    } else {
+      T9 = 1.0 / (vtss - vbs_jct); T0 = -vbs_jct / Nvtmrss * vtss * T9;
+      dT0_dVb = vtss / Nvtmrss * (T9 + vbs_jct * T9 * T9); dexp(T0, e1, T10); d1 = T10 * dT0_dVb;
+    }
+    if ((vtsd - vbd_jct) < (vtsd * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbd_jct / Nvtmrsd * T9; dexp(T0, e2, T10); d2 = T10 / Nvtmrsd * T9;
+    } else {
+      T9 = 1.0 / (vtsd - vbd_jct); T0 = -vbd_jct / Nvtmrsd * vtsd * T9;
+      dT0_dVb = vtsd / Nvtmrsd * (T9 + vbd_jct * T9 * T9); dexp(T0, e2, T10); d2 = T10 * dT0_dVb;
+    }
+    if ((vtssws - vbs_jct) < (vtssws * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbs_jct / Nvtmrssws * T9; dexp(T0, e3, T10); d3 = T10 / Nvtmrssws * T9;
+    } else {
+      T9 = 1.0 / (vtssws - vbs_jct); T0 = -vbs_jct / Nvtmrssws * vtssws * T9;
+      dT0_dVb = vtssws / Nvtmrssws * (T9 + vbs_jct * T9 * T9); dexp(T0, e3, T10); d3 = T10 * dT0_dVb;
+    }
+    if ((vtsswd - vbd_jct) < (vtsswd * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbd_jct / Nvtmrsswd * T9; dexp(T0, e4, T10); d4 = T10 / Nvtmrsswd * T9;
+    } else {
+      T9 = 1.0 / (vtsswd - vbd_jct); T0 = -vbd_jct / Nvtmrsswd * vtsswd * T9;
+      dT0_dVb = vtsswd / Nvtmrsswd * (T9 + vbd_jct * T9 * T9); dexp(T0, e4, T10); d4 = T10 * dT0_dVb;
+    }
+    if ((vtsswgs - vbs_jct) < (vtsswgs * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbs_jct / Nvtmrsswgs * T9; dexp(T0, e5, T10); d5 = T10 / Nvtmrsswgs * T9;
+    } else {
+      T9 = 1.0 / (vtsswgs - vbs_jct); T0 = -vbs_jct / Nvtmrsswgs * vtsswgs * T9;
+      dT0_dVb = vtsswgs / Nvtmrsswgs * (T9 + vbs_jct * T9 * T9); dexp(T0, e5, T10); d5 = T10 * dT0_dVb;
+    }
+    if ((vtsswgd - vbd_jct) < (vtsswgd * 1e-3)) {
+      T9 = 1.0e3; T0 = -vbd_jct / Nvtmrsswgd * T9; dexp(T0, e6, T10); d6 = T10 / Nvtmrsswgd * T9;
+    } else {
+      T9 = 1.0 / (vtsswgd - vbd_jct); T0 = -vbd_jct / Nvtmrsswgd * vtsswgd * T9;
+      dT0_dVb = vtsswgd / Nvtmrsswgd * (T9 + vbd_jct * T9 * T9); dexp(T0, e6, T10); d6 = T10 * dT0_dVb;
+    }
+    gbs += P(SjctTempRevSatCur) * d1 + P(SswTempRevSatCur) * d3 + P(SswgTempRevSatCur) * d5;
+    cbs -= P(SjctTempRevSatCur) * (e1 - 1.0) + P(SswTempRevSatCur) * (e3 - 1.0) + P(SswgTempRevSatCur) * (e5 - 1.0);
+    gbd += P(DjctTempRevSatCur) * d2 + P(DswTempRevSatCur) * d4 + P(DswgTempRevSatCur) * d6;
+    cbd -= P(DjctTempRevSatCur) * (e2 - 1.0) + P(DswTempRevSatCur) * (e4 - 1.0) + P(DswgTempRevSatCur) * (e6 - 1.0);
+  }
+
+  // Operating mode (:8761-8780).
+  int mode;
+  double Vds, Vgs, Vbs;
+  if (vds >= 0.0) {
+    mode = 1;
+    Vds = vds;
+    Vgs = vgs;
+    Vbs = vbs;
+  } else {
+    mode = -1;
+    Vds = -vds;
+    Vgs = vgd;
+    Vbs = vbd;
+  }
+  (void)Vgs;
+  const double epsrox = P(epsrox_m);
+  const double toxe = P(toxe_m);
+  const double epssub = CONSTEPSSI;
+  (void)epsrox;
+
+  // Effective body bias, threshold voltage (:8819-9030).
+  const double vbsc = P(vbsc);
+  double Vbseff, dVbseff_dVb;
+  T0 = Vbs - vbsc - 0.001;
+  T1 = sqrt(T0 * T0 - 0.004 * vbsc);
+  if (T0 >= 0.0) {
+    Vbseff = vbsc + 0.5 * (T0 + T1);
+    dVbseff_dVb = 0.5 * (1.0 + T0 / T1);
+  } else {
+    T2 = -0.002 / (T1 - T0);
+    Vbseff = vbsc * (1.0 + T2);
+    dVbseff_dVb = T2 * vbsc / T1;
+  }
+  const double phi = P(phi), sqrtPhi_p = P(sqrtPhi);
+  T9 = 0.95 * phi;
+  T0 = T9 - Vbseff - 0.001;
+  T1 = sqrt(T0 * T0 + 0.004 * T9);
+  Vbseff = T9 - 0.5 * (T0 + T1);
+  dVbseff_dVb *= 0.5 * (1.0 + T0 / T1);
+  const double Phis = phi - Vbseff;
+  const double dPhis_dVb = -1.0;
+  const double sqrtPhis = sqrt(Phis);
+  const double dsqrtPhis_dVb = -0.5 / sqrtPhis;
+  const double Xdep = P(Xdep0) * sqrtPhis / sqrtPhi_p;
+  const double dXdep_dVb = (P(Xdep0) / sqrtPhi_p) * dsqrtPhis_dVb;
+  const double Leff = P(leff);
+  const double Vtm = P(vtm);
+  const double Vtm0 = P(vtm0);
+  T3 = sqrt(Xdep);
+  const double V0 = P(vbi) - phi;
+  T0 = P(dvt2) * Vbseff;
+  if (T0 >= -0.5) {
+    T1 = 1.0 + T0;
+    T2 = P(dvt2);
+  } else {
+    T4 = 1.0 / (3.0 + 8.0 * T0);
+    T1 = (1.0 + 3.0 * T0) * T4;
+    T2 = P(dvt2) * T4 * T4;
+  }
+  const double factor1 = P(factor1);
+  const double lt1 = factor1 * T3 * T1;
+  const double dlt1_dVb = factor1 * (0.5 / T3 * T1 * dXdep_dVb + T3 * T2);
+  T0 = P(dvt2w) * Vbseff;
+  if (T0 >= -0.5) {
+    T1 = 1.0 + T0;
+    T2 = P(dvt2w);
+  } else {
+    T4 = 1.0 / (3.0 + 8.0 * T0);
+    T1 = (1.0 + 3.0 * T0) * T4;
+    T2 = P(dvt2w) * T4 * T4;
+  }
+  const double ltw = factor1 * T3 * T1;
+  const double dltw_dVb = factor1 * (0.5 / T3 * T1 * dXdep_dVb + T3 * T2);
+  double Theta0, dTheta0_dVb;
+  T0 = P(dvt1) * Leff / lt1;
+  if (T0 < CONSTEXP_THRESHOLD) {
+    T1 = exp(T0);
+    T2 = T1 - 1.0;
+    T3 = T2 * T2;
+    T4 = T3 + 2.0 * T1 * CONSTMIN_EXP;
+    Theta0 = T1 / T4;
+    dT1_dVb = -T0 * T1 * dlt1_dVb / lt1;
+    dTheta0_dVb = dT1_dVb * (T4 - 2.0 * T1 * (T2 + CONSTMIN_EXP)) / T4 / T4;
+  } else {
+    Theta0 = 1.0 / (CONSTMAX_EXP - 2.0);
+    dTheta0_dVb = 0.0;
+  }
+  const double thetavth = P(dvt0) * Theta0;
+  const double Delt_vth = thetavth * V0;
+  const double dDelt_vth_dVb = P(dvt0) * dTheta0_dVb * V0;
+  T0 = P(dvt1w) * P(weff) * Leff / ltw;
+  if (T0 < CONSTEXP_THRESHOLD) {
+    T1 = exp(T0);
+    T2 = T1 - 1.0;
+    T3 = T2 * T2;
+    T4 = T3 + 2.0 * T1 * CONSTMIN_EXP;
+    T5 = T1 / T4;
+    dT1_dVb = -T0 * T1 * dltw_dVb / ltw;
+    dT5_dVb = dT1_dVb * (T4 - 2.0 * T1 * (T2 + CONSTMIN_EXP)) / T4 / T4;
+  } else {
+    T5 = 1.0 / (CONSTMAX_EXP - 2.0);
+    dT5_dVb = 0.0;
+  }
+  T0 = P(dvt0w) * T5;
+  T2 = T0 * V0;
+  dT2_dVb = P(dvt0w) * dT5_dVb * V0;
+  const double TempRatio = P(temp) / P(tnom) - 1.0;
+  T0 = sqrt(1.0 + P(lpe0) / Leff);
+  const double k1ox = P(k1ox);
+  T1 = k1ox * (T0 - 1.0) * sqrtPhi_p + (P(kt1) + P(kt1l) / Leff + P(kt2) * Vbseff) * TempRatio;
+  const double Vth_NarrowW = toxe * phi / (P(weff) + P(w0));
+  T3 = P(eta0) + P(etab) * Vbseff;
+  if (T3 < 1.0e-4) {
+    T9 = 1.0 / (3.0 - 2.0e4 * T3);
+    T3 = (2.0e-4 - T3) * T9;
+    T4 = T9 * T9;
+  } else {
+    T4 = 1.0;
+  }
+  const double dDIBL_Sft_dVd = T3 * P(theta0vb0);
+  const double DIBL_Sft = dDIBL_Sft_dVd * Vds;
+  const double Lpe_Vb = sqrt(1.0 + P(lpeb) / Leff);
+  const double k2ox = P(k2ox);
+  double Vth = dtype * vth0 + (k1ox * sqrtPhis - P(k1) * sqrtPhi_p) * Lpe_Vb - k2ox * Vbseff - Delt_vth - T2 +
+               (P(k3) + P(k3b) * Vbseff) * Vth_NarrowW + T1 - DIBL_Sft;
+  double dVth_dVb = Lpe_Vb * k1ox * dsqrtPhis_dVb - k2ox - dDelt_vth_dVb - dT2_dVb + P(k3b) * Vth_NarrowW -
+                    P(etab) * Vds * P(theta0vb0) * T4 + P(kt2) * TempRatio;
+  double dVth_dVd = -dDIBL_Sft_dVd;
+  const double coxe = P(coxe);
+  tmp1 = epssub / Xdep;
+  tmp2 = P(nfactor) * tmp1;
+  tmp3 = P(cdsc) + P(cdscb) * Vbseff + P(cdscd) * Vds;
+  tmp4 = (tmp2 + tmp3 * Theta0 + P(cit)) / coxe;
+  double n, dn_dVb, dn_dVd;
+  if (tmp4 >= -0.5) {
+    n = 1.0 + tmp4;
+    dn_dVb = (-tmp2 / Xdep * dXdep_dVb + tmp3 * dTheta0_dVb + P(cdscb) * Theta0) / coxe;
+    dn_dVd = P(cdscd) * Theta0 / coxe;
+  } else {
+    T0 = 1.0 / (3.0 + 8.0 * tmp4);
+    n = (1.0 + 3.0 * tmp4) * T0;
+    T0 *= T0;
+    dn_dVb = (-tmp2 / Xdep * dXdep_dVb + tmp3 * dTheta0_dVb + P(cdscb) * Theta0) / coxe * T0;
+    dn_dVd = P(cdscd) * Theta0 / coxe * T0;
+  }
+  if (P(dvtp0) > 0.0) {
+    T0 = -P(dvtp1) * Vds;
+    if (T0 < -CONSTEXP_THRESHOLD) {
+      T2 = CONSTMIN_EXP;
+      dT2_dVd = 0.0;
+    } else {
+      T2 = exp(T0);
+      dT2_dVd = -P(dvtp1) * T2;
+    }
+    T3 = Leff + P(dvtp0) * (1.0 + T2);
+    dT3_dVd = P(dvtp0) * dT2_dVd;
+    if (tempMod < 2) {
+      T4 = Vtm * log(Leff / T3);
+      dT4_dVd = -Vtm * dT3_dVd / T3;
+    } else {
+      T4 = Vtm0 * log(Leff / T3);
+      dT4_dVd = -Vtm0 * dT3_dVd / T3;
+    }
+    const double dDITS_Sft_dVd = dn_dVd * T4 + n * dT4_dVd;
+    const double dDITS_Sft_dVb = T4 * dn_dVb;
+    Vth -= n * T4;
+    dVth_dVd -= dDITS_Sft_dVd;
+    dVth_dVb -= dDITS_Sft_dVb;
+  }
+  const double von = Vth;
+
+  // Poly-gate depletion (:9033-9060).
+  double vgs_eff, dvgs_eff_dvg, vgd_eff, dvgd_eff_dvg;
+  T0 = P(vfb) + phi;
+  T1 = CONSTEPSSI;
+  poly_depletion(T0, P(ngate), T1, coxe, vgs, vgs_eff, dvgs_eff_dvg);
+  poly_depletion(T0, P(ngate), T1, coxe, vgd, vgd_eff, dvgd_eff_dvg);
+  double Vgs_eff, dVgs_eff_dVg;
+  if (mode > 0) {
+    Vgs_eff = vgs_eff;
+    dVgs_eff_dVg = dvgs_eff_dvg;
+  } else {
+    Vgs_eff = vgd_eff;
+    dVgs_eff_dVg = dvgd_eff_dvg;
+  }
+  const double Vgst = Vgs_eff - Vth;
+
+  // Effective gate overdrive Vgsteff (:9061-9150).
+  const double mstar = P(mstar);
+  T0 = n * Vtm;
+  T1 = mstar * Vgst;
+  T2 = T1 / T0;
+  if (T2 > CONSTEXP_THRESHOLD) {
+    T10 = T1;
+    dT10_dVg = mstar * dVgs_eff_dVg;
+    dT10_dVd = -dVth_dVd * mstar;
+    dT10_dVb = -dVth_dVb * mstar;
+  } else if (T2 < -CONSTEXP_THRESHOLD) {
+    T10 = Vtm * log(1.0 + CONSTMIN_EXP);
+    dT10_dVg = 0.0;
+    dT10_dVd = T10 * dn_dVd;
+    dT10_dVb = T10 * dn_dVb;
+    T10 *= n;
+  } else {
+    const double ExpVgst = exp(T2);
+    T3 = Vtm * log(1.0 + ExpVgst);
+    T10 = n * T3;
+    dT10_dVg = mstar * ExpVgst / (1.0 + ExpVgst);
+    dT10_dVb = T3 * dn_dVb - dT10_dVg * (dVth_dVb + Vgst * dn_dVb / n);
+    dT10_dVd = T3 * dn_dVd - dT10_dVg * (dVth_dVd + Vgst * dn_dVd / n);
+    dT10_dVg *= dVgs_eff_dVg;
+  }
+  T1 = P(voffcbn) - (1.0 - mstar) * Vgst;
+  T2 = T1 / T0;
+  if (T2 < -CONSTEXP_THRESHOLD) {
+    T3 = coxe * CONSTMIN_EXP / P(cdep0);
+    T9 = mstar + T3 * n;
+    dT9_dVg = 0.0;
+    dT9_dVd = dn_dVd * T3;
+    dT9_dVb = dn_dVb * T3;
+  } else if (T2 > CONSTEXP_THRESHOLD) {
+    T3 = coxe * CONSTMAX_EXP / P(cdep0);
+    T9 = mstar + T3 * n;
+    dT9_dVg = 0.0;
+    dT9_dVd = dn_dVd * T3;
+    dT9_dVb = dn_dVb * T3;
+  } else {
+    const double ExpVgst = exp(T2);
+    T3 = coxe / P(cdep0);
+    T4 = T3 * ExpVgst;
+    T5 = T1 * T4 / T0;
+    T9 = mstar + n * T4;
+    dT9_dVg = T3 * (mstar - 1.0) * ExpVgst / Vtm;
+    dT9_dVb = T4 * dn_dVb - dT9_dVg * dVth_dVb - T5 * dn_dVb;
+    dT9_dVd = T4 * dn_dVd - dT9_dVg * dVth_dVd - T5 * dn_dVd;
+    dT9_dVg *= dVgs_eff_dVg;
+  }
+  double Vgsteff = T10 / T9;
+  T11 = T9 * T9;
+  double dVgsteff_dVg = (T9 * dT10_dVg - T10 * dT9_dVg) / T11;
+  double dVgsteff_dVd = (T9 * dT10_dVd - T10 * dT9_dVd) / T11;
+  double dVgsteff_dVb = (T9 * dT10_dVb - T10 * dT9_dVb) / T11;
+
+  // Effective width and source/drain series resistance (:9155-9200).
+  T9 = sqrtPhis - sqrtPhi_p;
+  double Weff = P(weff) - 2.0 * (P(dwg) * Vgsteff + P(dwb) * T9);
+  double dWeff_dVg = -2.0 * P(dwg);
+  double dWeff_dVb = -2.0 * P(dwb) * dsqrtPhis_dVb;
+  if (Weff < 2.0e-8) {
+    T0 = 1.0 / (6.0e-8 - 2.0 * Weff);
+    Weff = 2.0e-8 * (4.0e-8 - Weff) * T0;
+    T0 *= T0 * 4.0e-16;
+    dWeff_dVg *= T0;
+    dWeff_dVb *= T0;
+  }
+  double Rds, dRds_dVg, dRds_dVb;
+  {
+    T0 = 1.0 + P(prwg) * Vgsteff;
+    dT0_dVg = -P(prwg) / T0 / T0;
+    T1 = P(prwb) * T9;
+    dT1_dVb = P(prwb) * dsqrtPhis_dVb;
+    T2 = 1.0 / T0 + T1;
+    T3 = T2 + sqrt(T2 * T2 + 0.01);
+    dT3_dVg = 1.0 + T2 / (T3 - T2);
+    dT3_dVb = dT3_dVg * dT1_dVb;
+    dT3_dVg *= dT0_dVg;
+    T4 = P(rds0) * 0.5;
+    Rds = P(rdswmin) + T3 * T4;
+    dRds_dVg = T4 * dT3_dVg;
+    dRds_dVb = T4 * dT3_dVb;
+  }
+
+  // Bulk charge factor Abulk (:9201-9260).
+  T9 = 0.5 * k1ox * Lpe_Vb / sqrtPhis;
+  T1 = T9 + k2ox - P(k3b) * Vth_NarrowW;
+  dT1_dVb = -T9 / sqrtPhis * dsqrtPhis_dVb;
+  T9 = sqrt(P(xj) * Xdep);
+  tmp1 = Leff + 2.0 * T9;
+  T5 = Leff / tmp1;
+  tmp2 = P(a0) * T5;
+  tmp3 = P(weff) + P(b1);
+  tmp4 = P(b0) / tmp3;
+  T2 = tmp2 + tmp4;
+  dT2_dVb = -T9 / tmp1 / Xdep * dXdep_dVb;
+  T6 = T5 * T5;
+  T7 = T5 * T6;
+  double Abulk0 = 1.0 + T1 * T2;
+  double dAbulk0_dVb = T1 * tmp2 * dT2_dVb + T2 * dT1_dVb;
+  T8 = P(ags) * P(a0) * T7;
+  double dAbulk_dVg = -T1 * T8;
+  double Abulk = Abulk0 + dAbulk_dVg * Vgsteff;
+  double dAbulk_dVb = dAbulk0_dVb - T8 * Vgsteff * (dT1_dVb + 3.0 * T1 * dT2_dVb);
+  if (Abulk0 < 0.1) {
+    T9 = 1.0 / (3.0 - 20.0 * Abulk0);
+    Abulk0 = (0.2 - Abulk0) * T9;
+    dAbulk0_dVb *= T9 * T9;
+  }
+  if (Abulk < 0.1) {
+    T9 = 1.0 / (3.0 - 20.0 * Abulk);
+    Abulk = (0.2 - Abulk) * T9;
+    T10 = T9 * T9;
+    dAbulk_dVb *= T10;
+    dAbulk_dVg *= T10;
+  }
+  T2 = P(keta) * Vbseff;
+  if (T2 >= -0.9) {
+    T0 = 1.0 / (1.0 + T2);
+    dT0_dVb = -P(keta) * T0 * T0;
+  } else {
+    T1 = 1.0 / (0.8 + T2);
+    T0 = (17.0 + 20.0 * T2) * T1;
+    dT0_dVb = -P(keta) * T1 * T1;
+  }
+  dAbulk_dVg *= T0;
+  dAbulk_dVb = dAbulk_dVb * T0 + Abulk * dT0_dVb;
+  dAbulk0_dVb = dAbulk0_dVb * T0 + Abulk0 * dT0_dVb;
+  Abulk *= T0;
+  Abulk0 *= T0;
+
+  // Mobility (:9261-9340).
+  T14 = 0.0;
+  double Denomi, dDenomi_dVg, dDenomi_dVd, dDenomi_dVb;
+  if (mobMod == 0) {
+    T0 = Vgsteff + Vth + Vth - T14;
+    T2 = P(ua) + P(uc) * Vbseff;
+    T3 = T0 / toxe;
+    T12 = sqrt(Vth * Vth + 0.0001);
+    T9 = 1.0 / (Vgsteff + 2 * T12);
+    T10 = T9 * toxe;
+    T8 = P(ud) * T10 * T10 * Vth;
+    T6 = T8 * Vth;
+    T5 = T3 * (T2 + P(ub) * T3) + T6;
+    T7 = -2.0 * T6 * T9;
+    T11 = T7 * Vth / T12;
+    dDenomi_dVg = (T2 + 2.0 * P(ub) * T3) / toxe;
+    T13 = 2.0 * (dDenomi_dVg + T11 + T8);
+    dDenomi_dVd = T13 * dVth_dVd;
+    dDenomi_dVb = T13 * dVth_dVb + P(uc) * T3;
+    dDenomi_dVg += T7;
+  } else if (mobMod == 1) {
+    T0 = Vgsteff + Vth + Vth - T14;
+    T2 = 1.0 + P(uc) * Vbseff;
+    T3 = T0 / toxe;
+    T4 = T3 * (P(ua) + P(ub) * T3);
+    T12 = sqrt(Vth * Vth + 0.0001);
+    T9 = 1.0 / (Vgsteff + 2 * T12);
+    T10 = T9 * toxe;
+    T8 = P(ud) * T10 * T10 * Vth;
+    T6 = T8 * Vth;
+    T5 = T4 * T2 + T6;
+    T7 = -2.0 * T6 * T9;
+    T11 = T7 * Vth / T12;
+    dDenomi_dVg = (P(ua) + 2.0 * P(ub) * T3) * T2 / toxe;
+    T13 = 2.0 * (dDenomi_dVg + T11 + T8);
+    dDenomi_dVd = T13 * dVth_dVd;
+    dDenomi_dVb = T13 * dVth_dVb + P(uc) * T4;
+    dDenomi_dVg += T7;
+  } else {
+    T0 = (Vgsteff + P(vtfbphi1)) / toxe;
+    T1 = exp(P(eu) * log(T0));
+    dT1_dVg = T1 * P(eu) / T0 / toxe;
+    T2 = P(ua) + P(uc) * Vbseff;
+    T3 = T0 / toxe;
+    T12 = sqrt(Vth * Vth + 0.0001);
+    T9 = 1.0 / (Vgsteff + 2 * T12);
+    T10 = T9 * toxe;
+    T8 = P(ud) * T10 * T10 * Vth;
+    T6 = T8 * Vth;
+    T5 = T1 * T2 + T6;
+    T7 = -2.0 * T6 * T9;
+    T11 = T7 * Vth / T12;
+    dDenomi_dVg = T2 * dT1_dVg + T7;
+    T13 = 2.0 * (T11 + T8);
+    dDenomi_dVd = T13 * dVth_dVd;
+    dDenomi_dVb = T13 * dVth_dVb + T1 * P(uc);
+  }
+  if (T5 >= -0.8) {
+    Denomi = 1.0 + T5;
+  } else {
+    T9 = 1.0 / (7.0 + 10.0 * T5);
+    Denomi = (0.6 + T5) * T9;
+    T9 *= T9;
+    dDenomi_dVg *= T9;
+    dDenomi_dVd *= T9;
+    dDenomi_dVb *= T9;
+  }
+  const double ueff = P(u0temp) / Denomi;
+  T9 = -ueff / Denomi;
+  const double dueff_dVg = T9 * dDenomi_dVg;
+  const double dueff_dVd = T9 * dDenomi_dVd;
+  const double dueff_dVb = T9 * dDenomi_dVb;
+
+  // Saturation velocity, Vdsat (:9341-9460).
+  const double vsattemp = P(vsattemp);
+  const double WVCox = Weff * vsattemp * coxe;
+  const double WVCoxRds = WVCox * Rds;
+  const double Esat = 2.0 * vsattemp / ueff;
+  double EsatL = Esat * Leff;
+  T0 = -EsatL / ueff;
+  double dEsatL_dVg = T0 * dueff_dVg;
+  double dEsatL_dVd = T0 * dueff_dVd;
+  double dEsatL_dVb = T0 * dueff_dVb;
+  const double a1 = P(a1);
+  double Lambda, dLambda_dVg;
+  if (a1 == 0.0) {
+    Lambda = P(a2);
+    dLambda_dVg = 0.0;
+  } else if (a1 > 0.0) {
+    T0 = 1.0 - P(a2);
+    T1 = T0 - a1 * Vgsteff - 0.0001;
+    T2 = sqrt(T1 * T1 + 0.0004 * T0);
+    Lambda = P(a2) + T0 - 0.5 * (T1 + T2);
+    dLambda_dVg = 0.5 * a1 * (1.0 + T1 / T2);
+  } else {
+    T1 = P(a2) + a1 * Vgsteff - 0.0001;
+    T2 = sqrt(T1 * T1 + 0.0004 * P(a2));
+    Lambda = 0.5 * (T1 + T2);
+    dLambda_dVg = 0.5 * a1 * (1.0 + T1 / T2);
+  }
+  const double Vgst2Vtm = Vgsteff + 2.0 * Vtm;
+  if (Rds > 0) {
+    tmp2 = dRds_dVg / Rds + dWeff_dVg / Weff;
+    tmp3 = dRds_dVb / Rds + dWeff_dVb / Weff;
+  } else {
+    tmp2 = dWeff_dVg / Weff;
+    tmp3 = dWeff_dVb / Weff;
+  }
+  double Vdsat, dVdsat_dVg, dVdsat_dVd, dVdsat_dVb;
+  if ((Rds == 0.0) && (Lambda == 1.0)) {
+    T0 = 1.0 / (Abulk * EsatL + Vgst2Vtm);
+    tmp1 = 0.0;
+    T1 = T0 * T0;
+    T2 = Vgst2Vtm * T0;
+    T3 = EsatL * Vgst2Vtm;
+    Vdsat = T3 * T0;
+    dT0_dVg = -(Abulk * dEsatL_dVg + EsatL * dAbulk_dVg + 1.0) * T1;
+    dT0_dVd = -(Abulk * dEsatL_dVd) * T1;
+    dT0_dVb = -(Abulk * dEsatL_dVb + dAbulk_dVb * EsatL) * T1;
+    dVdsat_dVg = T3 * dT0_dVg + T2 * dEsatL_dVg + EsatL * T0;
+    dVdsat_dVd = T3 * dT0_dVd + T2 * dEsatL_dVd;
+    dVdsat_dVb = T3 * dT0_dVb + T2 * dEsatL_dVb;
+  } else {
+    tmp1 = dLambda_dVg / (Lambda * Lambda);
+    T9 = Abulk * WVCoxRds;
+    T8 = Abulk * T9;
+    T7 = Vgst2Vtm * T9;
+    T6 = Vgst2Vtm * WVCoxRds;
+    T0 = 2.0 * Abulk * (T9 - 1.0 + 1.0 / Lambda);
+    dT0_dVg = 2.0 * (T8 * tmp2 - Abulk * tmp1 + (2.0 * T9 + 1.0 / Lambda - 1.0) * dAbulk_dVg);
+    dT0_dVb = 2.0 * (T8 * (2.0 / Abulk * dAbulk_dVb + tmp3) + (1.0 / Lambda - 1.0) * dAbulk_dVb);
+    dT0_dVd = 0.0;
+    T1 = Vgst2Vtm * (2.0 / Lambda - 1.0) + Abulk * EsatL + 3.0 * T7;
+    dT1_dVg = (2.0 / Lambda - 1.0) - 2.0 * Vgst2Vtm * tmp1 + Abulk * dEsatL_dVg + EsatL * dAbulk_dVg +
+              3.0 * (T9 + T7 * tmp2 + T6 * dAbulk_dVg);
+    dT1_dVb = Abulk * dEsatL_dVb + EsatL * dAbulk_dVb + 3.0 * (T6 * dAbulk_dVb + T7 * tmp3);
+    dT1_dVd = Abulk * dEsatL_dVd;
+    T2 = Vgst2Vtm * (EsatL + 2.0 * T6);
+    dT2_dVg = EsatL + Vgst2Vtm * dEsatL_dVg + T6 * (4.0 + 2.0 * Vgst2Vtm * tmp2);
+    dT2_dVb = Vgst2Vtm * (dEsatL_dVb + 2.0 * T6 * tmp3);
+    dT2_dVd = Vgst2Vtm * dEsatL_dVd;
+    T3 = sqrt(T1 * T1 - 2.0 * T0 * T2);
+    Vdsat = (T1 - T3) / T0;
+    dVdsat_dVg = (dT1_dVg - (T1 * dT1_dVg - dT0_dVg * T2 - T0 * dT2_dVg) / T3 - Vdsat * dT0_dVg) / T0;
+    dVdsat_dVb = (dT1_dVb - (T1 * dT1_dVb - dT0_dVb * T2 - T0 * dT2_dVb) / T3 - Vdsat * dT0_dVb) / T0;
+    dVdsat_dVd = (dT1_dVd - (T1 * dT1_dVd - T0 * dT2_dVd) / T3) / T0;
+  }
+
+  // Effective Vds (:9461-9500).
+  const double delta = P(delta);
+  T1 = Vdsat - Vds - delta;
+  dT1_dVg = dVdsat_dVg;
+  dT1_dVd = dVdsat_dVd - 1.0;
+  dT1_dVb = dVdsat_dVb;
+  T2 = sqrt(T1 * T1 + 4.0 * delta * Vdsat);
+  T0 = T1 / T2;
+  T9 = 2.0 * delta;
+  T3 = T9 / T2;
+  dT2_dVg = T0 * dT1_dVg + T3 * dVdsat_dVg;
+  dT2_dVd = T0 * dT1_dVd + T3 * dVdsat_dVd;
+  dT2_dVb = T0 * dT1_dVb + T3 * dVdsat_dVb;
+  double Vdseff, dVdseff_dVg, dVdseff_dVd, dVdseff_dVb;
+  if (T1 >= 0.0) {
+    Vdseff = Vdsat - 0.5 * (T1 + T2);
+    dVdseff_dVg = dVdsat_dVg - 0.5 * (dT1_dVg + dT2_dVg);
+    dVdseff_dVd = dVdsat_dVd - 0.5 * (dT1_dVd + dT2_dVd);
+    dVdseff_dVb = dVdsat_dVb - 0.5 * (dT1_dVb + dT2_dVb);
+  } else {
+    T4 = T9 / (T2 - T1);
+    T5 = 1.0 - T4;
+    T6 = Vdsat * T4 / (T2 - T1);
+    Vdseff = Vdsat * T5;
+    dVdseff_dVg = dVdsat_dVg * T5 + T6 * (dT2_dVg - dT1_dVg);
+    dVdseff_dVd = dVdsat_dVd * T5 + T6 * (dT2_dVd - dT1_dVd);
+    dVdseff_dVb = dVdsat_dVb * T5 + T6 * (dT2_dVb - dT1_dVb);
+  }
+  if (Vds == 0.0) {
+    Vdseff = 0.0;
+    dVdseff_dVg = 0.0;
+    dVdseff_dVb = 0.0;
+  }
+  if (Vdseff > Vds) Vdseff = Vds;
+  const double diffVds = Vds - Vdseff;
+
+  // Velocity overshoot (lambda) (:9501-9545).
+  if ((P(lambdaGiven) != 0.0) && (P(lambda_m) > 0.0)) {
+    T1 = Leff * ueff;
+    T2 = P(lambda) / T1;
+    T3 = -T2 / T1 * Leff;
+    dT2_dVd = T3 * dueff_dVd;
+    dT2_dVg = T3 * dueff_dVg;
+    dT2_dVb = T3 * dueff_dVb;
+    T5 = 1.0 / (Esat * P(litl));
+    T4 = -T5 / EsatL;
+    dT5_dVg = dEsatL_dVg * T4;
+    dT5_dVd = dEsatL_dVd * T4;
+    dT5_dVb = dEsatL_dVb * T4;
+    T6 = 1.0 + diffVds * T5;
+    dT6_dVg = dT5_dVg * diffVds - dVdseff_dVg * T5;
+    dT6_dVd = dT5_dVd * diffVds + (1.0 - dVdseff_dVd) * T5;
+    dT6_dVb = dT5_dVb * diffVds - dVdseff_dVb * T5;
+    T7 = 2.0 / (T6 * T6 + 1.0);
+    T8 = 1.0 - T7;
+    T9 = T6 * T7 * T7;
+    dT8_dVg = T9 * dT6_dVg;
+    dT8_dVd = T9 * dT6_dVd;
+    dT8_dVb = T9 * dT6_dVb;
+    T10 = 1.0 + T2 * T8;
+    dT10_dVg = dT2_dVg * T8 + T2 * dT8_dVg;
+    dT10_dVd = dT2_dVd * T8 + T2 * dT8_dVd;
+    dT10_dVb = dT2_dVb * T8 + T2 * dT8_dVb;
+    if (T10 == 1.0) dT10_dVg = dT10_dVd = dT10_dVb = 0.0;
+    dEsatL_dVg *= T10;
+    dEsatL_dVg += EsatL * dT10_dVg;
+    dEsatL_dVd *= T10;
+    dEsatL_dVd += EsatL * dT10_dVd;
+    dEsatL_dVb *= T10;
+    dEsatL_dVb += EsatL * dT10_dVb;
+    EsatL *= T10;
+  }
+
+  // Vasat (:9546-9565).
+  tmp4 = 1.0 - 0.5 * Abulk * Vdsat / Vgst2Vtm;
+  T9 = WVCoxRds * Vgsteff;
+  T8 = T9 / Vgst2Vtm;
+  T0 = EsatL + Vdsat + 2.0 * T9 * tmp4;
+  T7 = 2.0 * WVCoxRds * tmp4;
+  dT0_dVg = dEsatL_dVg + dVdsat_dVg + T7 * (1.0 + tmp2 * Vgsteff) -
+            T8 * (Abulk * dVdsat_dVg - Abulk * Vdsat / Vgst2Vtm + Vdsat * dAbulk_dVg);
+  dT0_dVb = dEsatL_dVb + dVdsat_dVb + T7 * tmp3 * Vgsteff - T8 * (dAbulk_dVb * Vdsat + Abulk * dVdsat_dVb);
+  dT0_dVd = dEsatL_dVd + dVdsat_dVd - T8 * Abulk * dVdsat_dVd;
+  T9 = WVCoxRds * Abulk;
+  T1 = 2.0 / Lambda - 1.0 + T9;
+  dT1_dVg = -2.0 * tmp1 + WVCoxRds * (Abulk * tmp2 + dAbulk_dVg);
+  dT1_dVb = dAbulk_dVb * WVCoxRds + T9 * tmp3;
+  const double Vasat = T0 / T1;
+  const double dVasat_dVg = (dT0_dVg - Vasat * dT1_dVg) / T1;
+  const double dVasat_dVb = (dT0_dVb - Vasat * dT1_dVb) / T1;
+  const double dVasat_dVd = dT0_dVd / T1;
+
+  // Quantum-mechanical effective oxide capacitance and beta (:9566-9590).
+  tmp1 = P(vtfbphi2);
+  tmp2 = 2.0e8 * P(toxp);
+  dT0_dVg = 1.0 / tmp2;
+  T0 = (Vgsteff + tmp1) * dT0_dVg;
+  tmp3 = exp(P(bdos) * 0.7 * log(T0));
+  T1 = 1.0 + tmp3;
+  T2 = P(bdos) * 0.7 * tmp3 / T0;
+  double Tcen = P(ados) * 1.9e-9 / T1;
+  double dTcen_dVg = -Tcen * T2 * dT0_dVg / T1;
+  const double coxp = P(coxp);
+  double Coxeff = epssub * coxp / (epssub + coxp * Tcen);
+  double dCoxeff_dVg = -Coxeff * Coxeff * dTcen_dVg / epssub;
+  const double CoxeffWovL = Coxeff * Weff / Leff;
+  const double beta = ueff * CoxeffWovL;
+  T3 = ueff / Leff;
+  const double dbeta_dVg = CoxeffWovL * dueff_dVg + T3 * (Weff * dCoxeff_dVg + Coxeff * dWeff_dVg);
+  const double dbeta_dVd = CoxeffWovL * dueff_dVd;
+  const double dbeta_dVb = CoxeffWovL * dueff_dVb + T3 * Coxeff * dWeff_dVb;
+  (void)dbeta_dVd; (void)dbeta_dVb;
+
+  // Linear-region current Idl (:9591-9640).
+  const double AbovVgst2Vtm = Abulk / Vgst2Vtm;
+  T0 = 1.0 - 0.5 * Vdseff * AbovVgst2Vtm;
+  dT0_dVg = -0.5 * (Abulk * dVdseff_dVg - Abulk * Vdseff / Vgst2Vtm + Vdseff * dAbulk_dVg) / Vgst2Vtm;
+  dT0_dVd = -0.5 * Abulk * dVdseff_dVd / Vgst2Vtm;
+  dT0_dVb = -0.5 * (Abulk * dVdseff_dVb + dAbulk_dVb * Vdseff) / Vgst2Vtm;
+  const double fgche1 = Vgsteff * T0;
+  const double dfgche1_dVg = Vgsteff * dT0_dVg + T0;
+  const double dfgche1_dVd = Vgsteff * dT0_dVd;
+  const double dfgche1_dVb = Vgsteff * dT0_dVb;
+  T9 = Vdseff / EsatL;
+  const double fgche2 = 1.0 + T9;
+  const double dfgche2_dVg = (dVdseff_dVg - T9 * dEsatL_dVg) / EsatL;
+  const double dfgche2_dVd = (dVdseff_dVd - T9 * dEsatL_dVd) / EsatL;
+  const double dfgche2_dVb = (dVdseff_dVb - T9 * dEsatL_dVb) / EsatL;
+  const double gche = beta * fgche1 / fgche2;
+  const double dgche_dVg = (beta * dfgche1_dVg + fgche1 * dbeta_dVg - gche * dfgche2_dVg) / fgche2;
+  const double dgche_dVd = (beta * dfgche1_dVd + fgche1 * dbeta_dVd - gche * dfgche2_dVd) / fgche2;
+  const double dgche_dVb = (beta * dfgche1_dVb + fgche1 * dbeta_dVb - gche * dfgche2_dVb) / fgche2;
+  T0 = 1.0 + gche * Rds;
+  const double Idl = gche / T0;
+  T1 = (1.0 - Idl * Rds) / T0;
+  T2 = Idl * Idl;
+  const double dIdl_dVg = T1 * dgche_dVg - T2 * dRds_dVg;
+  const double dIdl_dVd = T1 * dgche_dVd;
+  const double dIdl_dVb = T1 * dgche_dVb - T2 * dRds_dVb;
+
+  // Output resistance terms: FP, PvagTerm, CLM, DIBL, DITS, SCBE (:9641-9800).
+  double FP, dFP_dVg;
+  if (P(fprout) <= 0.0) {
+    FP = 1.0;
+    dFP_dVg = 0.0;
+  } else {
+    T9 = P(fprout) * sqrt(Leff) / Vgst2Vtm;
+    FP = 1.0 / (1.0 + T9);
+    dFP_dVg = FP * FP * T9 / Vgst2Vtm;
+  }
+  double PvagTerm, dPvagTerm_dVg, dPvagTerm_dVb, dPvagTerm_dVd;
+  T8 = P(pvag) / EsatL;
+  T9 = T8 * Vgsteff;
+  if (T9 > -0.9) {
+    PvagTerm = 1.0 + T9;
+    dPvagTerm_dVg = T8 * (1.0 - Vgsteff * dEsatL_dVg / EsatL);
+    dPvagTerm_dVb = -T9 * dEsatL_dVb / EsatL;
+    dPvagTerm_dVd = -T9 * dEsatL_dVd / EsatL;
+  } else {
+    T4 = 1.0 / (17.0 + 20.0 * T9);
+    PvagTerm = (0.8 + T9) * T4;
+    T4 *= T4;
+    dPvagTerm_dVg = T8 * (1.0 - Vgsteff * dEsatL_dVg / EsatL) * T4;
+    T9 *= T4 / EsatL;
+    dPvagTerm_dVb = -T9 * dEsatL_dVb;
+    dPvagTerm_dVd = -T9 * dEsatL_dVd;
+  }
+  double Cclm, dCclm_dVg, dCclm_dVd, dCclm_dVb, VACLM, dVACLM_dVg, dVACLM_dVd, dVACLM_dVb;
+  if ((P(pclm) > CONSTMIN_EXP) && (diffVds > 1.0e-10)) {
+    T0 = 1.0 + Rds * Idl;
+    dT0_dVg = dRds_dVg * Idl + Rds * dIdl_dVg;
+    dT0_dVd = Rds * dIdl_dVd;
+    dT0_dVb = dRds_dVb * Idl + Rds * dIdl_dVb;
+    T2 = Vdsat / Esat;
+    T1 = Leff + T2;
+    dT1_dVg = (dVdsat_dVg - T2 * dEsatL_dVg / Leff) / Esat;
+    dT1_dVd = (dVdsat_dVd - T2 * dEsatL_dVd / Leff) / Esat;
+    dT1_dVb = (dVdsat_dVb - T2 * dEsatL_dVb / Leff) / Esat;
+    Cclm = FP * PvagTerm * T0 * T1 / (P(pclm) * P(litl));
+    dCclm_dVg = Cclm * (dFP_dVg / FP + dPvagTerm_dVg / PvagTerm + dT0_dVg / T0 + dT1_dVg / T1);
+    dCclm_dVb = Cclm * (dPvagTerm_dVb / PvagTerm + dT0_dVb / T0 + dT1_dVb / T1);
+    dCclm_dVd = Cclm * (dPvagTerm_dVd / PvagTerm + dT0_dVd / T0 + dT1_dVd / T1);
+    VACLM = Cclm * diffVds;
+    dVACLM_dVg = dCclm_dVg * diffVds - dVdseff_dVg * Cclm;
+    dVACLM_dVb = dCclm_dVb * diffVds - dVdseff_dVb * Cclm;
+    dVACLM_dVd = dCclm_dVd * diffVds + (1.0 - dVdseff_dVd) * Cclm;
+  } else {
+    VACLM = Cclm = CONSTMAX_EXP;
+    dVACLM_dVd = dVACLM_dVg = dVACLM_dVb = 0.0;
+    dCclm_dVd = dCclm_dVg = dCclm_dVb = 0.0;
+  }
+  double VADIBL, dVADIBL_dVg, dVADIBL_dVd, dVADIBL_dVb;
+  if (P(thetaRout) > CONSTMIN_EXP) {
+    T8 = Abulk * Vdsat;
+    T0 = Vgst2Vtm * T8;
+    dT0_dVg = Vgst2Vtm * Abulk * dVdsat_dVg + T8 + Vgst2Vtm * Vdsat * dAbulk_dVg;
+    dT0_dVb = Vgst2Vtm * (dAbulk_dVb * Vdsat + Abulk * dVdsat_dVb);
+    dT0_dVd = Vgst2Vtm * Abulk * dVdsat_dVd;
+    T1 = Vgst2Vtm + T8;
+    dT1_dVg = 1.0 + Abulk * dVdsat_dVg + Vdsat * dAbulk_dVg;
+    dT1_dVb = Abulk * dVdsat_dVb + dAbulk_dVb * Vdsat;
+    dT1_dVd = Abulk * dVdsat_dVd;
+    T9 = T1 * T1;
+    T2 = P(thetaRout);
+    VADIBL = (Vgst2Vtm - T0 / T1) / T2;
+    dVADIBL_dVg = (1.0 - dT0_dVg / T1 + T0 * dT1_dVg / T9) / T2;
+    dVADIBL_dVb = (-dT0_dVb / T1 + T0 * dT1_dVb / T9) / T2;
+    dVADIBL_dVd = (-dT0_dVd / T1 + T0 * dT1_dVd / T9) / T2;
+    T7 = P(pdiblb) * Vbseff;
+    if (T7 >= -0.9) {
+      T3 = 1.0 / (1.0 + T7);
+      VADIBL *= T3;
+      dVADIBL_dVg *= T3;
+      dVADIBL_dVb = (dVADIBL_dVb - VADIBL * P(pdiblb)) * T3;
+      dVADIBL_dVd *= T3;
+    } else {
+      T4 = 1.0 / (0.8 + T7);
+      T3 = (17.0 + 20.0 * T7) * T4;
+      dVADIBL_dVg *= T3;
+      dVADIBL_dVb = dVADIBL_dVb * T3 - VADIBL * P(pdiblb) * T4 * T4;
+      dVADIBL_dVd *= T3;
+      VADIBL *= T3;
+    }
+    dVADIBL_dVg = dVADIBL_dVg * PvagTerm + VADIBL * dPvagTerm_dVg;
+    dVADIBL_dVb = dVADIBL_dVb * PvagTerm + VADIBL * dPvagTerm_dVb;
+    dVADIBL_dVd = dVADIBL_dVd * PvagTerm + VADIBL * dPvagTerm_dVd;
+    VADIBL *= PvagTerm;
+  } else {
+    VADIBL = CONSTMAX_EXP;
+    dVADIBL_dVd = dVADIBL_dVg = dVADIBL_dVb = 0.0;
+  }
+  const double Va = Vasat + VACLM;
+  const double dVa_dVg = dVasat_dVg + dVACLM_dVg;
+  const double dVa_dVb = dVasat_dVb + dVACLM_dVb;
+  const double dVa_dVd = dVasat_dVd + dVACLM_dVd;
+  T0 = P(pditsd) * Vds;
+  if (T0 > CONSTEXP_THRESHOLD) {
+    T1 = CONSTMAX_EXP;
+    dT1_dVd = 0;
+  } else {
+    T1 = exp(T0);
+    dT1_dVd = T1 * P(pditsd);
+  }
+  double VADITS, dVADITS_dVg, dVADITS_dVd;
+  if (P(pdits) > CONSTMIN_EXP) {
+    T2 = 1.0 + P(pditsl) * Leff;
+    VADITS = (1.0 + T2 * T1) / P(pdits);
+    dVADITS_dVg = VADITS * dFP_dVg;
+    dVADITS_dVd = FP * T2 * dT1_dVd / P(pdits);
+    VADITS *= FP;
+  } else {
+    VADITS = CONSTMAX_EXP;
+    dVADITS_dVg = dVADITS_dVd = 0;
+  }
+  double VASCBE, dVASCBE_dVg, dVASCBE_dVd, dVASCBE_dVb;
+  if (P(pscbe2) > 0.0) {
+    if (diffVds > P(pscbe1) * P(litl) / CONSTEXP_THRESHOLD) {
+      T0 = P(pscbe1) * P(litl) / diffVds;
+      VASCBE = Leff * exp(T0) / P(pscbe2);
+      T1 = T0 * VASCBE / diffVds;
+      dVASCBE_dVg = T1 * dVdseff_dVg;
+      dVASCBE_dVd = -T1 * (1.0 - dVdseff_dVd);
+      dVASCBE_dVb = T1 * dVdseff_dVb;
+    } else {
+      VASCBE = CONSTMAX_EXP * Leff / P(pscbe2);
+      dVASCBE_dVg = dVASCBE_dVd = dVASCBE_dVb = 0.0;
+    }
+  } else {
+    VASCBE = CONSTMAX_EXP;
+    dVASCBE_dVg = dVASCBE_dVd = dVASCBE_dVb = 0.0;
+  }
+
+  // Drain current with CLM, DIBL, DITS, SCBE (:9801-9870).
+  T9 = diffVds / VADIBL;
+  T0 = 1.0 + T9;
+  double Idsa = Idl * T0;
+  double dIdsa_dVg = T0 * dIdl_dVg - Idl * (dVdseff_dVg + T9 * dVADIBL_dVg) / VADIBL;
+  double dIdsa_dVd = T0 * dIdl_dVd + Idl * (1.0 - dVdseff_dVd - T9 * dVADIBL_dVd) / VADIBL;
+  double dIdsa_dVb = T0 * dIdl_dVb - Idl * (dVdseff_dVb + T9 * dVADIBL_dVb) / VADIBL;
+  T9 = diffVds / VADITS;
+  T0 = 1.0 + T9;
+  dIdsa_dVg = T0 * dIdsa_dVg - Idsa * (dVdseff_dVg + T9 * dVADITS_dVg) / VADITS;
+  dIdsa_dVd = T0 * dIdsa_dVd + Idsa * (1.0 - dVdseff_dVd - T9 * dVADITS_dVd) / VADITS;
+  dIdsa_dVb = T0 * dIdsa_dVb - Idsa * dVdseff_dVb / VADITS;
+  Idsa *= T0;
+  T0 = log(Va / Vasat);
+  dT0_dVg = dVa_dVg / Va - dVasat_dVg / Vasat;
+  dT0_dVb = dVa_dVb / Va - dVasat_dVb / Vasat;
+  dT0_dVd = dVa_dVd / Va - dVasat_dVd / Vasat;
+  T1 = T0 / Cclm;
+  T9 = 1.0 + T1;
+  dT9_dVg = (dT0_dVg - T1 * dCclm_dVg) / Cclm;
+  dT9_dVb = (dT0_dVb - T1 * dCclm_dVb) / Cclm;
+  dT9_dVd = (dT0_dVd - T1 * dCclm_dVd) / Cclm;
+  dIdsa_dVg = dIdsa_dVg * T9 + Idsa * dT9_dVg;
+  dIdsa_dVb = dIdsa_dVb * T9 + Idsa * dT9_dVb;
+  dIdsa_dVd = dIdsa_dVd * T9 + Idsa * dT9_dVd;
+  Idsa *= T9;
+
+  // Substrate current (:9871-9910).
+  double Isub, Gbd, Gbb, Gbg;
+  tmp = P(alpha0) + P(alpha1) * Leff;
+  if ((tmp <= 0.0) || (P(beta0) <= 0.0)) {
+    Isub = Gbd = Gbb = Gbg = 0.0;
+  } else {
+    T2 = tmp / Leff;
+    if (diffVds > P(beta0) / CONSTEXP_THRESHOLD) {
+      T0 = -P(beta0) / diffVds;
+      T1 = T2 * diffVds * exp(T0);
+      T3 = T1 / diffVds * (T0 - 1.0);
+      dT1_dVg = T3 * dVdseff_dVg;
+      dT1_dVd = T3 * (dVdseff_dVd - 1.0);
+      dT1_dVb = T3 * dVdseff_dVb;
+    } else {
+      T3 = T2 * CONSTMIN_EXP;
+      T1 = T3 * diffVds;
+      dT1_dVg = -T3 * dVdseff_dVg;
+      dT1_dVd = T3 * (1.0 - dVdseff_dVd);
+      dT1_dVb = -T3 * dVdseff_dVb;
+    }
+    T4 = Idsa * Vdseff;
+    Isub = T1 * T4;
+    Gbg = T1 * (dIdsa_dVg * Vdseff + Idsa * dVdseff_dVg) + T4 * dT1_dVg;
+    Gbd = T1 * (dIdsa_dVd * Vdseff + Idsa * dVdseff_dVd) + T4 * dT1_dVd;
+    Gbb = T1 * (dIdsa_dVb * Vdseff + Idsa * dVdseff_dVb) + T4 * dT1_dVb;
+    Gbd += Gbg * dVgsteff_dVd;
+    Gbb += Gbg * dVgsteff_dVb;
+    Gbg *= dVgsteff_dVg;
+    Gbb *= dVbseff_dVb;
+  }
+  double csub = Isub, gbbs = Gbb, gbgs = Gbg, gbds = Gbd;
+
+  // Drain current and conductances (:9911-9990).
+  T9 = diffVds / VASCBE;
+  T0 = 1.0 + T9;
+  const double Ids = Idsa * T0;
+  double Gm = T0 * dIdsa_dVg - Idsa * (dVdseff_dVg + T9 * dVASCBE_dVg) / VASCBE;
+  double Gds = T0 * dIdsa_dVd + Idsa * (1.0 - dVdseff_dVd - T9 * dVASCBE_dVd) / VASCBE;
+  double Gmb = T0 * dIdsa_dVb - Idsa * (dVdseff_dVb + T9 * dVASCBE_dVb) / VASCBE;
+  tmp1 = Gds + Gm * dVgsteff_dVd;
+  tmp2 = Gmb + Gm * dVgsteff_dVb;
+  tmp3 = Gm;
+  Gm = (Ids * dVdseff_dVg + Vdseff * tmp3) * dVgsteff_dVg;
+  Gds = Ids * (dVdseff_dVd + dVdseff_dVg * dVgsteff_dVd) + Vdseff * tmp1;
+  Gmb = (Ids * (dVdseff_dVb + dVdseff_dVg * dVgsteff_dVb) + Vdseff * tmp2) * dVbseff_dVb;
+  double cdrain = Ids * Vdseff;
+  if ((P(vtlGiven) != 0.0) && (P(vtl_m) > 0.0)) {
+    T12 = 1.0 / Leff / CoxeffWovL;
+    T11 = T12 / Vgsteff;
+    T10 = -T11 / Vgsteff;
+    const double vs = cdrain * T11;
+    const double dvs_dVg = Gm * T11 + cdrain * T10 * dVgsteff_dVg;
+    const double dvs_dVd = Gds * T11 + cdrain * T10 * dVgsteff_dVd;
+    const double dvs_dVb = Gmb * T11 + cdrain * T10 * dVgsteff_dVb;
+    T0 = 2 * CONSTMM;
+    T1 = vs / (P(vtl) * P(tfactor));
+    double Fsevl, dFsevl_dVg, dFsevl_dVd, dFsevl_dVb;
+    if (T1 > 0.0) {
+      T2 = 1.0 + exp(T0 * log(T1));
+      T3 = (T2 - 1.0) * T0 / vs;
+      Fsevl = 1.0 / exp(log(T2) / T0);
+      dT2_dVg = T3 * dvs_dVg;
+      dT2_dVd = T3 * dvs_dVd;
+      dT2_dVb = T3 * dvs_dVb;
+      T4 = -1.0 / T0 * Fsevl / T2;
+      dFsevl_dVg = T4 * dT2_dVg;
+      dFsevl_dVd = T4 * dT2_dVd;
+      dFsevl_dVb = T4 * dT2_dVb;
+    } else {
+      Fsevl = 1.0;
+      dFsevl_dVg = 0.0;
+      dFsevl_dVd = 0.0;
+      dFsevl_dVb = 0.0;
+    }
+    Gm *= Fsevl;
+    Gm += cdrain * dFsevl_dVg;
+    Gmb *= Fsevl;
+    Gmb += cdrain * dFsevl_dVb;
+    Gds *= Fsevl;
+    Gds += cdrain * dFsevl_dVd;
+    cdrain *= Fsevl;
+  }
+  double gds = Gds, gm = Gm, gmbs = Gmb;
+
+  // GIDL and GISL (:10063-10180). vgs_eff / vgd_eff here are the poly-depleted gate voltages.
+  T0 = 3.0 * toxe;
+  T1 = (vds - vgs_eff - P(egidl)) / T0;
+  double Igidl, Ggidld, Ggidlg, Ggidlb;
+  if ((P(agidl) <= 0.0) || (P(bgidl) <= 0.0) || (T1 <= 0.0) || (P(cgidl) <= 0.0) || (vbd > 0.0)) {
+    Igidl = Ggidld = Ggidlg = Ggidlb = 0.0;
+  } else {
+    dT1_dVd = 1.0 / T0;
+    dT1_dVg = -dvgs_eff_dvg * dT1_dVd;
+    T2 = P(bgidl) / T1;
+    if (T2 < 100.0) {
+      Igidl = P(agidl) * weffCJ * T1 * exp(-T2);
+      T3 = Igidl * (1.0 + T2) / T1;
+      Ggidld = T3 * dT1_dVd;
+      Ggidlg = T3 * dT1_dVg;
+    } else {
+      Igidl = P(agidl) * weffCJ * 3.720075976e-44;
+      Ggidld = Igidl * dT1_dVd;
+      Ggidlg = Igidl * dT1_dVg;
+      Igidl *= T1;
+    }
+    T4 = vbd * vbd;
+    T5 = -vbd * T4;
+    T6 = P(cgidl) + T5;
+    T7 = T5 / T6;
+    T8 = 3.0 * P(cgidl) * T4 / T6 / T6;
+    Ggidld = Ggidld * T7 + Igidl * T8;
+    Ggidlg = Ggidlg * T7;
+    Ggidlb = -Igidl * T8;
+    Igidl *= T7;
+  }
+  double ggidld = Ggidld, ggidlg = Ggidlg, ggidlb = Ggidlb;
+  T1 = (-vds - vgd_eff - P(egisl)) / T0;
+  double Igisl, Ggisls, Ggislg, Ggislb;
+  if ((P(agisl) <= 0.0) || (P(bgisl) <= 0.0) || (T1 <= 0.0) || (P(cgisl) <= 0.0) || (vbs > 0.0)) {
+    Igisl = Ggisls = Ggislg = Ggislb = 0.0;
+  } else {
+    dT1_dVd = 1.0 / T0;
+    dT1_dVg = -dvgd_eff_dvg * dT1_dVd;
+    T2 = P(bgisl) / T1;
+    if (T2 < 100.0) {
+      Igisl = P(agisl) * weffCJ * T1 * exp(-T2);
+      T3 = Igisl * (1.0 + T2) / T1;
+      Ggisls = T3 * dT1_dVd;
+      Ggislg = T3 * dT1_dVg;
+    } else {
+      Igisl = P(agisl) * weffCJ * 3.720075976e-44;
+      Ggisls = Igisl * dT1_dVd;
+      Ggislg = Igisl * dT1_dVg;
+      Igisl *= T1;
+    }
+    T4 = vbs * vbs;
+    T5 = -vbs * T4;
+    T6 = P(cgisl) + T5;
+    T7 = T5 / T6;
+    T8 = 3.0 * P(cgisl) * T4 / T6 / T6;
+    Ggisls = Ggisls * T7 + Igisl * T8;
+    Ggislg = Ggislg * T7;
+    Ggislb = -Igisl * T8;
+    Igisl *= T7;
+  }
+  double ggisls = Ggisls, ggislg = Ggislg, ggislb = Ggislb;
+  // Gate tunnelling currents are off (igcMod = igbMod = 0).
+
+  // Multi-finger scaling (:10601-10640).
+  if (nf != 1.0) {
+    cdrain *= nf; gds *= nf; gm *= nf; gmbs *= nf;
+    gbbs *= nf; gbgs *= nf; gbds *= nf; csub *= nf;
+    Igidl *= nf; ggidld *= nf; ggidlg *= nf; ggidlb *= nf;
+    Igisl *= nf; ggisls *= nf; ggislg *= nf; ggislb *= nf;
+  }
+
+  // Intrinsic charges, capMod = 2 charge-thickness model (:10707-11620).
+  double qgate = 0, qdrn = 0, qbulk = 0, qsrc = 0;
+  double cggb = 0, cgsb = 0, cgdb = 0, cdgb = 0, cdsb = 0, cddb = 0, cbgb = 0, cbsb = 0, cbdb = 0;
+  if ((P(xpart) < 0) || (!ChargeComputationNeeded)) {
+    // all zero
+  } else {
+    double VbseffCV, dVbseffCV_dVb;
+    if (Vbseff < 0.0) {
+      VbseffCV = Vbseff;
+      dVbseffCV_dVb = 1.0;
+    } else {
+      VbseffCV = phi - Phis;
+      dVbseffCV_dVb = -dPhis_dVb;
+    }
+    const double CoxWL = coxe * P(weffCV) * P(leffCV) * nf;
+    if (P(cvchargeMod) == 0.0) {
+      const double noff = n * P(noff);
+      const double dnoff_dVd = P(noff) * dn_dVd;
+      const double dnoff_dVb = P(noff) * dn_dVb;
+      T0 = Vtm * noff;
+      const double voffcv = P(voffcv);
+      const double VgstNVt = (Vgst - voffcv) / T0;
+      if (VgstNVt > CONSTEXP_THRESHOLD) {
+        Vgsteff = Vgst - voffcv;
+        dVgsteff_dVg = dVgs_eff_dVg;
+        dVgsteff_dVd = -dVth_dVd;
+        dVgsteff_dVb = -dVth_dVb;
+      } else if (VgstNVt < -CONSTEXP_THRESHOLD) {
+        Vgsteff = T0 * log(1.0 + CONSTMIN_EXP);
+        dVgsteff_dVg = 0.0;
+        dVgsteff_dVd = Vgsteff / noff;
+        dVgsteff_dVb = dVgsteff_dVd * dnoff_dVb;
+        dVgsteff_dVd *= dnoff_dVd;
+      } else {
+        const double ExpVgst = exp(VgstNVt);
+        Vgsteff = T0 * log(1.0 + ExpVgst);
+        dVgsteff_dVg = ExpVgst / (1.0 + ExpVgst);
+        dVgsteff_dVd = -dVgsteff_dVg * (dVth_dVd + (Vgst - voffcv) / noff * dnoff_dVd) + Vgsteff / noff * dnoff_dVd;
+        dVgsteff_dVb = -dVgsteff_dVg * (dVth_dVb + (Vgst - voffcv) / noff * dnoff_dVb) + Vgsteff / noff * dnoff_dVb;
+        dVgsteff_dVg *= dVgs_eff_dVg;
+      }
+    } else {
+      const double mstarcv = P(mstarcv);
+      T0 = n * Vtm;
+      T1 = mstarcv * Vgst;
+      T2 = T1 / T0;
+      if (T2 > CONSTEXP_THRESHOLD) {
+        T10 = T1;
+        dT10_dVg = mstarcv * dVgs_eff_dVg;
+        dT10_dVd = -dVth_dVd * mstarcv;
+        dT10_dVb = -dVth_dVb * mstarcv;
+      } else if (T2 < -CONSTEXP_THRESHOLD) {
+        T10 = Vtm * log(1.0 + CONSTMIN_EXP);
+        dT10_dVg = 0.0;
+        dT10_dVd = T10 * dn_dVd;
+        dT10_dVb = T10 * dn_dVb;
+        T10 *= n;
+      } else {
+        const double ExpVgst = exp(T2);
+        T3 = Vtm * log(1.0 + ExpVgst);
+        T10 = n * T3;
+        dT10_dVg = mstarcv * ExpVgst / (1.0 + ExpVgst);
+        dT10_dVb = T3 * dn_dVb - dT10_dVg * (dVth_dVb + Vgst * dn_dVb / n);
+        dT10_dVd = T3 * dn_dVd - dT10_dVg * (dVth_dVd + Vgst * dn_dVd / n);
+        dT10_dVg *= dVgs_eff_dVg;
+      }
+      T1 = P(voffcbncv) - (1.0 - mstarcv) * Vgst;
+      T2 = T1 / T0;
+      if (T2 < -CONSTEXP_THRESHOLD) {
+        T3 = coxe * CONSTMIN_EXP / P(cdep0);
+        T9 = mstarcv + T3 * n;
+        dT9_dVg = 0.0;
+        dT9_dVd = dn_dVd * T3;
+        dT9_dVb = dn_dVb * T3;
+      } else if (T2 > CONSTEXP_THRESHOLD) {
+        T3 = coxe * CONSTMAX_EXP / P(cdep0);
+        T9 = mstarcv + T3 * n;
+        dT9_dVg = 0.0;
+        dT9_dVd = dn_dVd * T3;
+        dT9_dVb = dn_dVb * T3;
+      } else {
+        const double ExpVgst = exp(T2);
+        T3 = coxe / P(cdep0);
+        T4 = T3 * ExpVgst;
+        T5 = T1 * T4 / T0;
+        T9 = mstarcv + n * T4;
+        dT9_dVg = T3 * (mstarcv - 1.0) * ExpVgst / Vtm;
+        dT9_dVb = T4 * dn_dVb - dT9_dVg * dVth_dVb - T5 * dn_dVb;
+        dT9_dVd = T4 * dn_dVd - dT9_dVg * dVth_dVd - T5 * dn_dVd;
+        dT9_dVg *= dVgs_eff_dVg;
+      }
+      Vgsteff = T10 / T9;
+      T11 = T9 * T9;
+      dVgsteff_dVg = (T9 * dT10_dVg - T10 * dT9_dVg) / T11;
+      dVgsteff_dVd = (T9 * dT10_dVd - T10 * dT9_dVd) / T11;
+      dVgsteff_dVb = (T9 * dT10_dVb - T10 * dT9_dVb) / T11;
+    }
+    // capMod == 2
+    const double vfbzb = P(vfbzb);
+    double V3 = vfbzb - Vgs_eff + VbseffCV - CONSTDELTA_3;
+    if (vfbzb <= 0.0)
+      T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * vfbzb);
+    else
+      T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * vfbzb);
+    T1 = 0.5 * (1.0 + V3 / T0);
+    const double Vfbeff = vfbzb - 0.5 * (V3 + T0);
+    const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
+    const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
+    const double Cox = coxp;
+    double Tox = 1.0e8 * P(toxp);
+    T0 = (Vgs_eff - VbseffCV - vfbzb) / Tox;
+    dT0_dVg = dVgs_eff_dVg / Tox;
+    dT0_dVb = -dVbseffCV_dVb / Tox;
+    tmp = T0 * P(acde);
+    const double ldeb = P(ldeb);
+    double dTcen_dVb, dTcen_dVd;
+    if ((-CONSTEXP_THRESHOLD < tmp) && (tmp < CONSTEXP_THRESHOLD)) {
+      Tcen = ldeb * exp(tmp);
+      dTcen_dVg = P(acde) * Tcen;
+      dTcen_dVb = dTcen_dVg * dT0_dVb;
+      dTcen_dVg *= dT0_dVg;
+    } else if (tmp <= -CONSTEXP_THRESHOLD) {
+      Tcen = ldeb * CONSTMIN_EXP;
+      dTcen_dVg = dTcen_dVb = 0.0;
+    } else {
+      Tcen = ldeb * CONSTMAX_EXP;
+      dTcen_dVg = dTcen_dVb = 0.0;
+    }
+    const double LINK = 1.0e-3 * P(toxp);
+    V3 = ldeb - Tcen - LINK;
+    const double V4 = sqrt(V3 * V3 + 4.0 * LINK * ldeb);
+    Tcen = ldeb - 0.5 * (V3 + V4);
+    T1 = 0.5 * (1.0 + V3 / V4);
+    dTcen_dVg *= T1;
+    dTcen_dVb *= T1;
+    double Ccen = epssub / Tcen;
+    T2 = Cox / (Cox + Ccen);
+    Coxeff = T2 * Ccen;
+    T3 = -Ccen / Tcen;
+    dCoxeff_dVg = T2 * T2 * T3;
+    double dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
+    dCoxeff_dVg *= dTcen_dVg;
+    double CoxWLcen = CoxWL * Coxeff / coxe;
+    const double Qac0 = CoxWLcen * (Vfbeff - vfbzb);
+    double QovCox = Qac0 / Coxeff;
+    const double dQac0_dVg = CoxWLcen * dVfbeff_dVg + QovCox * dCoxeff_dVg;
+    const double dQac0_dVb = CoxWLcen * dVfbeff_dVb + QovCox * dCoxeff_dVb;
+    T0 = 0.5 * k1ox;
+    T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
+    if (k1ox == 0.0) {
+      T1 = 0.0;
+      T2 = 0.0;
+    } else if (T3 < 0.0) {
+      T1 = T0 + T3 / k1ox;
+      T2 = CoxWLcen;
+    } else {
+      T1 = sqrt(T0 * T0 + T3);
+      T2 = CoxWLcen * T0 / T1;
+    }
+    const double Qsub0 = CoxWLcen * k1ox * (T1 - T0);
+    QovCox = Qsub0 / Coxeff;
+    const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg) + QovCox * dCoxeff_dVg;
+    const double dQsub0_dVd = -T2 * dVgsteff_dVd;
+    const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb) + QovCox * dCoxeff_dVb;
+    if (k1ox <= 0.0) {
+      Denomi = 0.25 * P(moin) * Vtm;
+      T0 = 0.5 * sqrtPhi_p;
+    } else {
+      Denomi = P(moin) * Vtm * k1ox * k1ox;
+      T0 = k1ox * sqrtPhi_p;
+    }
+    T1 = 2.0 * T0 + Vgsteff;
+    const double DeltaPhi = Vtm * log(1.0 + T1 * Vgsteff / Denomi);
+    const double dDeltaPhi_dVg = 2.0 * Vtm * (T1 - T0) / (Denomi + T1 * Vgsteff);
+    T0 = Vgsteff - DeltaPhi - 0.001;
+    dT0_dVg = 1.0 - dDeltaPhi_dVg;
+    T1 = sqrt(T0 * T0 + Vgsteff * 0.004);
+    const double VgDP = 0.5 * (T0 + T1);
+    const double dVgDP_dVg = 0.5 * (dT0_dVg + (T0 * dT0_dVg + 0.002) / T1);
+    Tox += Tox;
+    T0 = (Vgsteff + P(vtfbphi2)) / Tox;
+    tmp = exp(P(bdos) * 0.7 * log(T0));
+    T1 = 1.0 + tmp;
+    T2 = P(bdos) * 0.7 * tmp / (T0 * Tox);
+    Tcen = P(ados) * 1.9e-9 / T1;
+    dTcen_dVg = -Tcen * T2 / T1;
+    dTcen_dVd = dTcen_dVg * dVgsteff_dVd;
+    dTcen_dVb = dTcen_dVg * dVgsteff_dVb;
+    dTcen_dVg *= dVgsteff_dVg;
+    Ccen = epssub / Tcen;
+    T0 = Cox / (Cox + Ccen);
+    Coxeff = T0 * Ccen;
+    T1 = -Ccen / Tcen;
+    dCoxeff_dVg = T0 * T0 * T1;
+    const double dCoxeff_dVd = dCoxeff_dVg * dTcen_dVd;
+    dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
+    dCoxeff_dVg *= dTcen_dVg;
+    CoxWLcen = CoxWL * Coxeff / coxe;
+    const double AbulkCV = Abulk0 * P(abulkCVfactor);
+    const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+    const double VdsatCV = VgDP / AbulkCV;
+    T0 = VdsatCV - Vds - CONSTDELTA_4;
+    dT0_dVg = dVgDP_dVg / AbulkCV;
+    dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
+    dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
+    dT1_dVd = -T0 / T1;
+    dT1_dVb = dT1_dVg * dT0_dVb;
+    dT1_dVg *= dT0_dVg;
+    double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
+    if (T0 >= 0.0) {
+      VdseffCV = VdsatCV - 0.5 * (T0 + T1);
+      dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
+      dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
+      dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
+    } else {
+      T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
+      T4 = 1.0 - T3;
+      T5 = VdsatCV * T3 / (T1 - T0);
+      VdseffCV = VdsatCV * T4;
+      dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
+      dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
+      dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
+    }
+    if (Vds == 0.0) {
+      VdseffCV = 0.0;
+      dVdseffCV_dVg = 0.0;
+      dVdseffCV_dVb = 0.0;
+    }
+    T0 = AbulkCV * VdseffCV;
+    T1 = VgDP;
+    T2 = 12.0 * (T1 - 0.5 * T0 + 1.0e-20);
+    T3 = T0 / T2;
+    T4 = 1.0 - 12.0 * T3 * T3;
+    T5 = AbulkCV * (6.0 * T0 * (4.0 * T1 - T0) / (T2 * T2) - 0.5);
+    T6 = T5 * VdseffCV / AbulkCV;
+    qgate = CoxWLcen * (T1 - T0 * (0.5 - T3));
+    QovCox = qgate / Coxeff;
+    double Cgg1 = CoxWLcen * (T4 * dVgDP_dVg + T5 * dVdseffCV_dVg);
+    const double Cgd1 = CoxWLcen * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+    const double Cgb1 = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+    Cgg1 = Cgg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    T7 = 1.0 - AbulkCV;
+    T8 = T2 * T2;
+    T9 = 12.0 * T7 * T0 * T0 / (T8 * AbulkCV);
+    T10 = T9 * dVgDP_dVg;
+    T11 = -T7 * T5 / AbulkCV;
+    T12 = -(T9 * T1 / AbulkCV + VdseffCV * (0.5 - T0 / T2));
+    qbulk = CoxWLcen * T7 * (0.5 * VdseffCV - T0 * VdseffCV / T2);
+    QovCox = qbulk / Coxeff;
+    double Cbg1 = CoxWLcen * (T10 + T11 * dVdseffCV_dVg);
+    const double Cbd1 = CoxWLcen * T11 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+    const double Cbb1 = CoxWLcen * (T11 * dVdseffCV_dVb + T12 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+    Cbg1 = Cbg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    double Csg, Csd, Csb;
+    const double xpart = P(xpart);
+    if (xpart > 0.5) {
+      qsrc = -CoxWLcen * (T1 / 2.0 + T0 / 4.0 - 0.5 * T0 * T0 / T2);
+      QovCox = qsrc / Coxeff;
+      T2 += T2;
+      T3 = T2 * T2;
+      T7 = -(0.25 - 12.0 * T0 * (4.0 * T1 - T0) / T3);
+      T4 = -(0.5 + 24.0 * T0 * T0 / T3) * dVgDP_dVg;
+      T5 = T7 * AbulkCV;
+      T6 = T7 * VdseffCV;
+      Csg = CoxWLcen * (T4 + T5 * dVdseffCV_dVg);
+      Csd = CoxWLcen * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+      Csb = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    } else if (xpart < 0.5) {
+      T2 = T2 / 12.0;
+      T3 = 0.5 * CoxWLcen / (T2 * T2);
+      T4 = T1 * (2.0 * T0 * T0 / 3.0 + T1 * (T1 - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
+      qsrc = -T3 * T4;
+      QovCox = qsrc / Coxeff;
+      T8 = 4.0 / 3.0 * T1 * (T1 - T0) + 0.4 * T0 * T0;
+      T5 = -2.0 * qsrc / T2 - T3 * (T1 * (3.0 * T1 - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
+      T6 = AbulkCV * (qsrc / T2 + T3 * T8);
+      T7 = T6 * VdseffCV / AbulkCV;
+      Csg = T5 * dVgDP_dVg + T6 * dVdseffCV_dVg;
+      Csd = Csg * dVgsteff_dVd + T6 * dVdseffCV_dVd + QovCox * dCoxeff_dVd;
+      Csb = Csg * dVgsteff_dVb + T6 * dVdseffCV_dVb + T7 * dAbulkCV_dVb + QovCox * dCoxeff_dVb;
+      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    } else {
+      qsrc = -0.5 * qgate;
+      Csg = -0.5 * Cgg1;
+      Csd = -0.5 * Cgd1;
+      Csb = -0.5 * Cgb1;
+    }
+    qgate += Qac0 + Qsub0 - qbulk;
+    qbulk -= (Qac0 + Qsub0);
+    qdrn = -(qgate + qbulk + qsrc);
+    const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
+    const double Cbd = Cbd1 - dQsub0_dVd;
+    double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
+    const double Cgg = Cgg1 - Cbg;
+    const double Cgd = Cgd1 - Cbd;
+    double Cgb = Cgb1 - Cbb;
+    Cgb *= dVbseff_dVb;
+    Cbb *= dVbseff_dVb;
+    Csb *= dVbseff_dVb;
+    cggb = Cgg;
+    cgsb = -(Cgg + Cgd + Cgb);
+    cgdb = Cgd;
+    cdgb = -(Cgg + Cbg + Csg);
+    cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
+    cddb = -(Cgd + Cbd + Csd);
+    cbgb = Cbg;
+    cbsb = -(Cbg + Cbd + Cbb);
+    cbdb = Cbd;
+  }
+
+  // Junction charges and capacitances (:11661-11810). Outside charge computation the reference
+  // keeps the previous load's junction values; they only feed Q and dQ/dx, which a DC solve does
+  // not use, and are zero here.
+  double qbs = 0.0, qbd = 0.0, capbs = 0.0, capbd = 0.0;
+  if (ChargeComputationNeeded) {
+    const double czbd = P(DunitAreaTempJctCap) * Adeff;
+    const double czbs = P(SunitAreaTempJctCap) * Aseff;
+    const double czbdsw = P(DunitLengthSidewallTempJctCap) * Pdeff;
+    const double czbdswg = P(DunitLengthGateSidewallTempJctCap) * weffCJ * nf;
+    const double czbssw = P(SunitLengthSidewallTempJctCap) * Pseff;
+    const double czbsswg = P(SunitLengthGateSidewallTempJctCap) * weffCJ * nf;
+    const double MJS = P(SbulkJctBotGradingCoeff), MJSWS = P(SbulkJctSideGradingCoeff);
+    const double MJSWGS = P(SbulkJctGateSideGradingCoeff);
+    const double MJD = P(DbulkJctBotGradingCoeff), MJSWD = P(DbulkJctSideGradingCoeff);
+    const double MJSWGD = P(DbulkJctGateSideGradingCoeff);
+    double arg, sarg;
+    if (vbs_jct == 0.0) {
+      qbs = 0.0;
+      capbs = czbs + czbssw + czbsswg;
+    } else if (vbs_jct < 0.0) {
+      if (czbs > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBS);
+        if (MJS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJS * log(arg));
+        qbs = P(PhiBS) * czbs * (1.0 - arg * sarg) / (1.0 - MJS);
+        capbs = czbs * sarg;
+      } else {
+        qbs = 0.0;
+        capbs = 0.0;
+      }
+      if (czbssw > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBSWS);
+        if (MJSWS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWS * log(arg));
+        qbs += P(PhiBSWS) * czbssw * (1.0 - arg * sarg) / (1.0 - MJSWS);
+        capbs += czbssw * sarg;
+      }
+      if (czbsswg > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBSWGS);
+        if (MJSWGS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWGS * log(arg));
+        qbs += P(PhiBSWGS) * czbsswg * (1.0 - arg * sarg) / (1.0 - MJSWGS);
+        capbs += czbsswg * sarg;
+      }
+    } else {
+      T0 = czbs + czbssw + czbsswg;
+      T1 = vbs_jct * (czbs * MJS / P(PhiBS) + czbssw * MJSWS / P(PhiBSWS) + czbsswg * MJSWGS / P(PhiBSWGS));
+      qbs = vbs_jct * (T0 + 0.5 * T1);
+      capbs = T0 + T1;
+    }
+    if (vbd_jct == 0.0) {
+      qbd = 0.0;
+      capbd = czbd + czbdsw + czbdswg;
+    } else if (vbd_jct < 0.0) {
+      if (czbd > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBD);
+        if (MJD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJD * log(arg));
+        qbd = P(PhiBD) * czbd * (1.0 - arg * sarg) / (1.0 - MJD);
+        capbd = czbd * sarg;
+      } else {
+        qbd = 0.0;
+        capbd = 0.0;
+      }
+      if (czbdsw > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBSWD);
+        if (MJSWD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWD * log(arg));
+        qbd += P(PhiBSWD) * czbdsw * (1.0 - arg * sarg) / (1.0 - MJSWD);
+        capbd += czbdsw * sarg;
+      }
+      if (czbdswg > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBSWGD);
+        if (MJSWGD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWGD * log(arg));
+        qbd += P(PhiBSWGD) * czbdswg * (1.0 - arg * sarg) / (1.0 - MJSWGD);
+        capbd += czbdswg * sarg;
+      }
+    } else {
+      T0 = czbd + czbdsw + czbdswg;
+      T1 = vbd_jct * (czbd * MJD / P(PhiBD) + czbdsw * MJSWD / P(PhiBSWD) + czbdswg * MJSWGD / P(PhiBSWGD));
+      qbd = vbd_jct * (T0 + 0.5 * T1);
+      capbd = T0 + T1;
+    }
+  }
+
+  // Overlap capacitances, capMod 1/2 (:11853-11890).
+  const double vgdx = vgd, vgsx = vgs;
+  double cgdo, qgdo, cgso, qgso;
+  {
+    T0 = vgdx + CONSTDELTA_1;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+    T2 = 0.5 * (T0 - T1);
+    T3 = P(weffCV) * P(cgdl);
+    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappad));
+    cgdo = P(cgdo) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+    qgdo = (P(cgdo) + T3) * vgdx - T3 * (T2 + 0.5 * P(ckappad) * (T4 - 1.0));
+    T0 = vgsx + CONSTDELTA_1;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+    T2 = 0.5 * (T0 - T1);
+    T3 = P(weffCV) * P(cgsl);
+    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappas));
+    cgso = P(cgso) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+    qgso = (P(cgso) + T3) * vgsx - T3 * (T2 + 0.5 * P(ckappas) * (T4 - 1.0));
+  }
+  if (nf != 1.0) {
+    cgdo *= nf;
+    cgso *= nf;
+    qgdo *= nf;
+    qgso *= nf;
+  }
+
+  // Overlap and gate-bulk charge bookkeeping (setupCapacitors_oldDAE, trnqsMod = 0, :12624-12760).
+  const double cgbo = P(cgbo);
+  double dxpart, sxpart;
+  if (mode > 0) {
+    qdrn -= qgdo;
+    const double qgb = cgbo * vgb;
+    qgate += qgdo + qgso + qgb;
+    qbulk -= qgb;
+    qsrc = -(qgate + qbulk + qdrn);
+    sxpart = 0.6;
+    dxpart = 0.4;
+  } else {
+    qsrc = qdrn - qgso;
+    const double qgb = cgbo * vgb;
+    qgate += qgdo + qgso + qgb;
+    qbulk -= qgb;
+    qdrn = -(qgate + qbulk + qsrc);
+    sxpart = 0.4;
+    dxpart = 0.6;
+  }
+  (void)qsrc;
+
+  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = rgateMod = rbodyMod = 0).
+  double CAPcggb, CAPcgdb, CAPcgsb, CAPcgbb, CAPcdgb, CAPcsgb, CAPcbgb, CAPcddb, CAPcdsb, CAPcsdb, CAPcssb;
+  double CAPcdbb, CAPcsbb, CAPcbdb, CAPcbsb, CAPcbbb;
+  const double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
+  if (mode > 0) {
+    CAPcggb = (cggb + cgdo + cgso + cgbo);
+    CAPcgdb = (cgdb - cgdo);
+    CAPcgsb = (cgsb - cgso);
+    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+    CAPcdgb = (cdgb - cgdo);
+    CAPcsgb = -(cggb + cbgb + cdgb + cgso);
+    CAPcbgb = (cbgb - cgbo);
+    CAPcddb = (cddb + capbd + cgdo);
+    CAPcdsb = cdsb;
+    CAPcsdb = -(cgdb + cbdb + cddb);
+    CAPcssb = (capbs + cgso - (cgsb + cbsb + cdsb));
+    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+    CAPcbdb = (cbdb - capbd);
+    CAPcbsb = (cbsb - capbs);
+    CAPcbbb = -(CAPcbdb + CAPcbgb + CAPcbsb + CAPcbgmb);
+  } else {
+    CAPcggb = (cggb + cgdo + cgso + cgbo);
+    CAPcgdb = (cgsb - cgdo);
+    CAPcgsb = (cgdb - cgso);
+    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+    CAPcdgb = -(cggb + cbgb + cdgb + cgdo);
+    CAPcsgb = (cdgb - cgso);
+    CAPcbgb = (cbgb - cgbo);
+    CAPcddb = (capbd + cgdo - (cgsb + cbsb + cdsb));
+    CAPcdsb = -(cgdb + cbdb + cddb);
+    CAPcsdb = cdsb;
+    CAPcssb = (cddb + capbs + cgso);
+    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+    CAPcbdb = (cbsb - capbd);
+    CAPcbsb = (cbdb - capbs);
+    CAPcbbb = -(CAPcbgb + CAPcbdb + CAPcbsb + CAPcbgmb);
+  }
+
+  // Master::updateState: store and state (:16195-16242).
+  o.sto[s_vbd] = vbd;
+  o.sto[s_vbs] = vbs;
+  o.sto[s_vgs] = vgs;
+  o.sto[s_vds] = vds;
+  o.sto[s_vges] = vges;
+  o.sto[s_vgms] = vgms;
+  o.sto[s_vdes] = vdes;
+  o.sto[s_vses] = vses;
+  o.sto[s_vdbs] = vdbs;
+  o.sto[s_vsbs] = vsbs;
+  o.sto[s_vdbd] = vdbd;
+  o.sto[s_vged] = 0.0;
+  o.sto[s_vgmd] = 0.0;
+  o.sto[s_von] = von;
+  const double qg = qgate;
+  const double qd = qdrn - qbd;
+  const double qb = qbulk + qbd + qbs;
+  o.sta[t_qg] = qg;
+  o.sta[t_qd] = qd;
+  o.sta[t_qb] = qb;
+  o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
+  o.vgb = vgb;
+
+  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0, no gate current.
+  const double gjbd = gbd, gjbs = gbs;
+  double Gmv, Gmbsv, FwdSum, RevSum, ceqdrn, ceqdrn_Jdxp, ceqbd, ceqbd_Jdxp, ceqbs, ceqbs_Jdxp;
+  double gbbdp, gbbsp, gbdpg, gbdpdp, gbdpb, gbdpsp, gbspg, gbspdp, gbspb, gbspsp;
+  if (mode >= 0) {
+    Gmv = gm;
+    Gmbsv = gmbs;
+    FwdSum = Gmv + Gmbsv;
+    RevSum = 0.0;
+    ceqdrn = dtype * cdrain;
+    ceqdrn_Jdxp = dtype * (-gds * (vds - vds_orig) - Gmv * (vgs - vgs_orig) - Gmbsv * (vbs - vbs_orig));
+    ceqbd = dtype * (csub + Igidl);
+    ceqbd_Jdxp = dtype * (-(gbds + ggidld) * (vds - vds_orig) - (gbgs + ggidlg) * (vgs - vgs_orig) -
+                          (gbbs + ggidlb) * (vbs - vbs_orig));
+    ceqbs = dtype * Igisl;
+    ceqbs_Jdxp = dtype * (+ggisls * (vds - vds_orig) - ggislg * (vgd - vgd_orig) - ggislb * (vbd - vbd_orig));
+    gbbdp = -(gbds);
+    gbbsp = gbds + gbgs + gbbs;
+    gbdpg = gbgs;
+    gbdpdp = gbds;
+    gbdpb = gbbs;
+    gbdpsp = -(gbdpg + gbdpdp + gbdpb);
+    gbspg = 0.0;
+    gbspdp = 0.0;
+    gbspb = 0.0;
+    gbspsp = 0.0;
+  } else {
+    Gmv = -gm;
+    Gmbsv = -gmbs;
+    FwdSum = 0.0;
+    RevSum = -(Gmv + Gmbsv);
+    ceqdrn = -dtype * cdrain;
+    ceqdrn_Jdxp = -dtype * (+gds * (vds - vds_orig) + Gmv * (vgd - vgd_orig) + Gmbsv * (vbd - vbd_orig));
+    ceqbs = dtype * (csub + Igisl);
+    ceqbs_Jdxp = dtype * (+(gbds + ggisls) * (vds - vds_orig) - (gbgs + ggislg) * (vgd - vgd_orig) -
+                          (gbbs + ggislb) * (vbd - vbd_orig));
+    ceqbd = dtype * Igidl;
+    ceqbd_Jdxp = dtype * (-ggidld * (vds - vds_orig) - ggidlg * (vgs - vgs_orig) - ggidlb * (vbs - vbs_orig));
+    gbbsp = -(gbds);
+    gbbdp = gbds + gbgs + gbbs;
+    gbdpg = 0.0;
+    gbdpsp = 0.0;
+    gbdpb = 0.0;
+    gbdpdp = 0.0;
+    gbspg = gbgs;
+    gbspsp = gbds;
+    gbspb = gbbs;
+    gbspdp = -(gbspg + gbspsp + gbspb);
+  }
+  const double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0, ceqgcrg = 0.0;
+  const double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0, ceqgcrg_Jdxp = 0.0;
+  const double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
+  const double gIdtotg = 0.0, gIdtotd = 0.0, gIdtots = 0.0, gIdtotb = 0.0;
+  const double gIbtotg = 0.0, gIbtotd = 0.0, gIbtots = 0.0, gIbtotb = 0.0;
+  const double gIgtotg = 0.0, gIgtotd = 0.0, gIgtots = 0.0, gIgtotb = 0.0;
+  const double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
+  const double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
+  double ceqjs, ceqjs_Jdxp, ceqjd, ceqjd_Jdxp;
+  if (dtype > 0) {
+    ceqjs = (cbs);
+    ceqjs_Jdxp = (-gbs * (vbs_jct - vbs_jct_orig));
+    ceqjd = (cbd);
+    ceqjd_Jdxp = (-gbd * (vbd_jct - vbd_jct_orig));
+  } else {
+    ceqjs = -(cbs);
+    ceqjs_Jdxp = (gbs * (vbs_jct - vbs_jct_orig));
+    ceqjd = -(cbd);
+    ceqjd_Jdxp = (gbd * (vbd_jct - vbd_jct_orig));
+  }
+
+  // Master::loadDAEVectors (:16316-16564). Local order D, G, S, B.
+  const bool lim = fl.voltlim && !origFlag;
+  for (int k = 0; k < kNumVec; ++k) o.vec[k] = 0.0;
+  o.vec[0] += -(ceqjd - ceqbd - ceqdrn + Idtoteq) * M;
+  o.vec[1] -= -(-ceqgcrg + Igtoteq) * M;
+  o.vec[3] += -(ceqbd + ceqbs - ceqjd - ceqjs + Ibtoteq) * M;
+  o.vec[2] += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
+  if (lim) {
+    o.vec[8 + 0] += (ceqjd_Jdxp - ceqbd_Jdxp - ceqdrn_Jdxp + Idtoteq_Jdxp) * M;
+    o.vec[8 + 1] -= (-ceqgcrg_Jdxp + Igtoteq_Jdxp) * M;
+    o.vec[8 + 3] += (ceqbd_Jdxp + ceqbs_Jdxp - ceqjd_Jdxp - ceqjs_Jdxp + Ibtoteq_Jdxp) * M;
+    o.vec[8 + 2] += (ceqdrn_Jdxp - ceqbs_Jdxp + ceqjs_Jdxp + Istoteq_Jdxp) * M;
+  }
+  // auxChargeCalculations (:12216-12350).
+  double Qeqqg_Jdxp = 0.0, Qeqqd_Jdxp = 0.0, Qeqqb_Jdxp = 0.0;
+  if (ChargeComputationNeeded && !origFlag) {
+    Qeqqg_Jdxp = -CAPcggb * (vgb - vgb_orig) + CAPcgdb * (vbd - vbd_orig) + CAPcgsb * (vbs - vbs_orig);
+    Qeqqd_Jdxp = -CAPcdgb * (vgb - vgb_orig) - CAPcdgmb * (vgmb - vgmb_orig) +
+                 (CAPcddb + 0.0) * (vbd - vbd_orig) - 0.0 * (vbd_jct - vbd_jct_orig) + CAPcdsb * (vbs - vbs_orig);
+    Qeqqb_Jdxp = -CAPcbgb * (vgb - vgb_orig) - CAPcbgmb * (vgmb - vgmb_orig) + CAPcbdb * (vbd - vbd_orig) +
+                 CAPcbsb * (vbs - vbs_orig);
+  }
+  const double Qeqqgmid_Jdxp = 0.0, Qeqqgmid = 0.0;
+  double Qeqqg, Qeqqd, Qeqqb;
+  if (dtype > 0) {
+    Qeqqg = qg;
+    Qeqqd = qd;
+    Qeqqb = qb;
+  } else {
+    Qeqqg = -qg;
+    Qeqqd = -qd;
+    Qeqqb = -qb;
+  }
+  o.vec[4 + 0] += -(-Qeqqd) * M;
+  o.vec[4 + 1] -= -(Qeqqg) * M;
+  o.vec[4 + 3] += -(-Qeqqb) * M;
+  o.vec[4 + 2] += -(+Qeqqg + Qeqqb + Qeqqd + Qeqqgmid) * M;
+  if (lim) {
+    o.vec[12 + 0] += (-Qeqqd_Jdxp) * M;
+    o.vec[12 + 1] -= (Qeqqg_Jdxp) * M;
+    o.vec[12 + 3] += (-Qeqqb_Jdxp) * M;
+    o.vec[12 + 2] += (+Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqd_Jdxp + Qeqqgmid_Jdxp) * M;
+  }
+
+  // Master::loadDAEMatrices (:16577-17268). Rows/cols D=0 G=1 S=2 B=3.
+  for (int k = 0; k < kNumMat; ++k) {
+    o.jf[k] = 0.0;
+    o.jq[k] = 0.0;
+  }
+  const double gdpr = P(drainConductance), gspr = P(sourceConductance);
+  const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
+  const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
+  const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
+  const double Tq = 0.0;  // qdef * gtau with no NQS charge
+#define JF(r, c) o.jf[(r)*4 + (c)]
+#define JQ(r, c) o.jq[(r)*4 + (c)]
+  JF(1, 1) += (-ggtg + gIgtotg) * M;
+  JF(1, 0) += (-ggtd + gIgtotd) * M;
+  JF(1, 2) += (-ggts + gIgtots) * M;
+  JF(1, 3) += (-ggtb + gIgtotb) * M;
+  JF(0, 0) += (gdpr + gds + gbd + Tq * ddxpart_dVd - gdtotd + RevSum + gbdpdp + dxpart * ggtd - gIdtotd) * M;
+  JF(0, 0) -= (gdpr + gdtot) * M;
+  JF(0, 1) += (Gmv - gdtotg + gbdpg - gIdtotg + dxpart * ggtg + Tq * ddxpart_dVg) * M;
+  JF(0, 2) -= (gds + gdtots - dxpart * ggts + gIdtots - Tq * ddxpart_dVs + FwdSum - gbdpsp) * M;
+  JF(0, 3) -= (gjbd + gdtotb - Gmbsv - gbdpb + gIdtotb - Tq * ddxpart_dVb - dxpart * ggtb) * M;
+  JF(0, 0) -= (gdpr - gdtotd) * M;
+  JF(0, 0) += (gdpr + gdtot) * M;
+  JF(2, 0) -= (gds + gstotd + RevSum - gbspdp - Tq * dsxpart_dVd - sxpart * ggtd + gIstotd) * M;
+  JF(2, 1) += (-Gmv - gstotg + gbspg + sxpart * ggtg + Tq * dsxpart_dVg - gIstotg) * M;
+  JF(2, 2) += (gspr + gds + gbs + Tq * dsxpart_dVs - gstots + FwdSum + gbspsp + sxpart * ggts - gIstots) * M;
+  JF(2, 2) -= (gspr + gstot) * M;
+  JF(2, 3) -= (gjbs + gstotb + Gmbsv - gbspb - sxpart * ggtb - Tq * dsxpart_dVb + gIstotb) * M;
+  JF(2, 2) -= (gspr - gstots) * M;
+  JF(2, 2) += (gspr + gstot) * M;
+  JF(3, 0) += (-gjbd + gbbdp - gIbtotd) * M;
+  JF(3, 1) += (-gbgs - gIbtotg) * M;
+  JF(3, 2) += (-gjbs + gbbsp - gIbtots) * M;
+  JF(3, 3) += (gjbd + gjbs - gbbs - gIbtotb) * M;
+  JF(0, 0) += (ggidld) * M;
+  JF(0, 1) += (ggidlg) * M;
+  JF(0, 2) -= ((ggidlg + ggidld + ggidlb)) * M;
+  JF(0, 3) += (ggidlb) * M;
+  JF(3, 0) -= (ggidld) * M;
+  JF(3, 1) -= (ggidlg) * M;
+  JF(3, 2) += ((ggidlg + ggidld + ggidlb)) * M;
+  JF(3, 3) -= (ggidlb) * M;
+  JF(2, 0) -= ((ggisls + ggislg + ggislb)) * M;
+  JF(2, 1) += (ggislg) * M;
+  JF(2, 2) += (ggisls) * M;
+  JF(2, 3) += (ggislb) * M;
+  JF(3, 0) += ((ggislg + ggisls + ggislb)) * M;
+  JF(3, 1) -= (ggislg) * M;
+  JF(3, 2) -= (ggisls) * M;
+  JF(3, 3) -= (ggislb) * M;
+  if (!(!fl.dcop && fl.init_tran && fl.newton_iter == 0)) {
+    JQ(1, 1) += (CAPcggb) * M;
+    JQ(1, 0) += (CAPcgdb) * M;
+    JQ(1, 2) += (CAPcgsb) * M;
+    JQ(1, 3) += (CAPcgbb) * M;
+    JQ(0, 0) += (CAPcddb) * M;
+    JQ(0, 1) += (+CAPcdgb) * M;
+    JQ(0, 2) -= (-CAPcdsb) * M;
+    JQ(0, 3) -= (-CAPcdbb) * M;
+    JQ(2, 0) -= (-CAPcsdb) * M;
+    JQ(2, 1) += (CAPcsgb) * M;
+    JQ(2, 2) += (CAPcssb) * M;
+    JQ(2, 3) -= (-CAPcsbb) * M;
+    JQ(3, 0) += (CAPcbdb) * M;
+    JQ(3, 1) += (CAPcbgb) * M;
+    JQ(3, 2) += (CAPcbsb) * M;
+    JQ(3, 3) += (CAPcbbb) * M;
+  }
+#undef JF
+#undef JQ
+#undef P
+}
+
+}  // namespace xb4

@@ -1,0 +1,529 @@
+// B200 device-load library: BSIM4 evaluation kernel, deterministic gather assembly, C ABI.
+//
+// Per Newton iteration (xd_load):
+//   1. bsim4_eval_kernel — one thread per instance. Gathers the 4 terminal voltages, reads the
+//      previous iterate's limited voltages, evaluates the model in FP64 registers and writes
+//      its 48 local stamp values slot-major into the context's staging array (coalesced: one
+//      128-byte line per warp per slot), plus its store/state entries.
+//   2. gather kernels — one output entry per thread (or per block for entries with many
+//      contributions). Each entry sums its contributions in a fixed order (instance order, then
+//      local slot order: the reference's summation order) through a precomputed
+//      stamp-to-output map and adds the sum into the caller's vector / CSR value array. No
+//      atomics: every run produces bit-identical results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/xyce_devload.h"
+#include "bsim4_eval.cuh"
+#include "bsim4_setup.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+  return fail(-3, std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+}
+
+#define XD_CUDA(call)                                     \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+constexpr int kLongThreshold = 64;   // targets with more contributions get a block each
+constexpr int kLongBlock = 256;
+constexpr int kEvalBlock = 128;
+
+// Stamp-to-output gather map for one group of outputs (the four vectors, or the two matrices).
+struct GatherMap {
+  int n_short = 0, n_long = 0;
+  int *d_short_dst = nullptr, *d_short_ptr = nullptr;
+  int *d_long_dst = nullptr, *d_long_ptr = nullptr;
+  int *d_src = nullptr;  // staging index within one output's slot range
+  size_t n_src = 0;
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct xd_ctx {
+  int device = 0;
+  int n = 0;
+  int n_unknowns = 0;
+  int nnz = 0;
+  int n_rec = 0;
+  double *d_tab = nullptr;
+  int *d_rec = nullptr;
+  int4 *d_nodes = nullptr;
+  double *d_vgb = nullptr;
+  double *d_stage = nullptr;
+  GatherMap vmap, mmap;
+};
+
+namespace {
+
+__global__ void __launch_bounds__(kEvalBlock) bsim4_eval_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
+    double *__restrict__ stage, xb4::LoadFlags fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 nd = nodes[i];
+  double V[4];
+  V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
+  V[1] = nd.y >= 0 ? sol[nd.y] : 0.0;
+  V[2] = nd.z >= 0 ? sol[nd.z] : 0.0;
+  V[3] = nd.w >= 0 ? sol[nd.w] : 0.0;
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+  double sto_old[xb4::kNumStore];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = 0.0;
+  sto_old[xb4::s_vbd] = so[(size_t)xb4::s_vbd * n + i];
+  sto_old[xb4::s_vbs] = so[(size_t)xb4::s_vbs * n + i];
+  sto_old[xb4::s_vgs] = so[(size_t)xb4::s_vgs * n + i];
+  sto_old[xb4::s_vds] = so[(size_t)xb4::s_vds * n + i];
+  sto_old[xb4::s_von] = so[(size_t)xb4::s_von * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load(rp, V, sto_old, fl, vgb[i], o);
+#pragma unroll
+  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k)
+    if (k != xb4::s_vged && k != xb4::s_vgmd) next_sto[(size_t)k * n + i] = o.sto[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumState; ++k) next_sta[(size_t)k * n + i] = o.sta[k];
+  if (o.write_curr_sta) {
+#pragma unroll
+    for (int k = 0; k < xb4::kNumState; ++k) curr_sta[(size_t)k * n + i] = o.sta[k];
+  }
+  vgb[i] = o.vgb;
+}
+
+template <int NOUT, bool ABS>
+struct OutSet {
+  double *out[NOUT];
+  size_t base[NOUT];  // staging offset of each output's slot range
+};
+
+template <int NOUT, bool ABS>
+__global__ void gather_short_kernel(int nt, const int *__restrict__ dst, const int *__restrict__ ptr,
+                                    const int *__restrict__ src, const double *__restrict__ stage,
+                                    OutSet<NOUT, ABS> os) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const int b = ptr[t], e = ptr[t + 1];
+  double acc[NOUT];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
+  for (int k = b; k < e; ++k) {
+    const size_t s = (size_t)src[k];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      const double v = stage[os.base[o] + s];
+      acc[o] += ABS ? fabs(v) : v;
+    }
+  }
+  const int d = dst[t];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+    if (os.out[o]) os.out[o][d] += acc[o];
+}
+
+// One block per output entry with many contributions: each thread sums a fixed strided subset in
+// order, then a fixed-shape tree combines the partial sums (deterministic).
+template <int NOUT, bool ABS>
+__global__ void __launch_bounds__(kLongBlock) gather_long_kernel(const int *__restrict__ dst,
+                                                                 const int *__restrict__ ptr,
+                                                                 const int *__restrict__ src,
+                                                                 const double *__restrict__ stage,
+                                                                 OutSet<NOUT, ABS> os) {
+  __shared__ double red[NOUT][kLongBlock];
+  const int t = blockIdx.x;
+  const int b = ptr[t], e = ptr[t + 1];
+  double acc[NOUT];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
+  for (int k = b + threadIdx.x; k < e; k += kLongBlock) {
+    const size_t s = (size_t)src[k];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      const double v = stage[os.base[o] + s];
+      acc[o] += ABS ? fabs(v) : v;
+    }
+  }
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) red[o][threadIdx.x] = acc[o];
+  __syncthreads();
+  for (int w = kLongBlock / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) red[o][threadIdx.x] += red[o][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int d = dst[t];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o)
+      if (os.out[o]) os.out[o][d] += red[o][0];
+  }
+}
+
+template <int NOUT, bool ABS>
+int run_gather(const GatherMap &m, const double *stage, const OutSet<NOUT, ABS> &os, cudaStream_t st) {
+  if (m.n_short > 0) {
+    const int blk = 256;
+    gather_short_kernel<NOUT, ABS><<<(m.n_short + blk - 1) / blk, blk, 0, st>>>(m.n_short, m.d_short_dst,
+                                                                               m.d_short_ptr, m.d_src, stage, os);
+  }
+  if (m.n_long > 0)
+    gather_long_kernel<NOUT, ABS><<<m.n_long, kLongBlock, 0, st>>>(m.d_long_dst, m.d_long_ptr, m.d_src, stage, os);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "gather launch");
+  return 0;
+}
+
+// Builds a gather map from (target, source) pairs listed in summation order.
+// tgt_of[k] = target index or -1 (dropped); the map keeps, per target, sources in list order.
+int build_map(const std::vector<int> &tgt_of, const std::vector<int> &src_of, int n_targets, GatherMap &m) {
+  std::vector<int> count(n_targets, 0);
+  for (int t : tgt_of)
+    if (t >= 0) ++count[t];
+  // Order targets: short ones first, long ones in a separate list; both keep ascending target.
+  std::vector<int> short_dst, long_dst, short_ptr(1, 0), long_ptr(1, 0);
+  std::vector<long long> start(n_targets, -1);
+  size_t n_src = 0;
+  for (int t = 0; t < n_targets; ++t)
+    if (count[t] > 0 && count[t] <= kLongThreshold) {
+      start[t] = (long long)n_src;
+      n_src += count[t];
+      short_dst.push_back(t);
+      short_ptr.push_back((int)n_src);
+    }
+  const size_t long_base = n_src;
+  for (int t = 0; t < n_targets; ++t)
+    if (count[t] > kLongThreshold) {
+      start[t] = (long long)n_src;
+      n_src += count[t];
+      long_dst.push_back(t);
+      long_ptr.push_back((int)n_src);
+    }
+  if (n_src > (size_t)0x7fffffff) return fail(-1, "too many stamp contributions for 32-bit gather indices");
+  std::vector<int> src(n_src);
+  std::vector<long long> fillp(start);
+  for (size_t k = 0; k < tgt_of.size(); ++k) {
+    const int t = tgt_of[k];
+    if (t < 0) continue;
+    src[(size_t)fillp[t]++] = src_of[k];
+  }
+  m.n_short = (int)short_dst.size();
+  m.n_long = (int)long_dst.size();
+  m.n_src = n_src;
+  (void)long_base;
+  auto up = [](int **d, const std::vector<int> &h) -> cudaError_t {
+    if (h.empty()) {
+      *d = nullptr;
+      return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(d, h.size() * sizeof(int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice);
+  };
+  XD_CUDA(up(&m.d_short_dst, short_dst));
+  XD_CUDA(up(&m.d_short_ptr, short_ptr));
+  XD_CUDA(up(&m.d_long_dst, long_dst));
+  XD_CUDA(up(&m.d_long_ptr, long_ptr));
+  XD_CUDA(up(&m.d_src, src));
+  return 0;
+}
+
+void free_map(GatherMap &m) {
+  cudaFree(m.d_short_dst);
+  cudaFree(m.d_short_ptr);
+  cudaFree(m.d_long_dst);
+  cudaFree(m.d_long_ptr);
+  cudaFree(m.d_src);
+  m = GatherMap();
+}
+
+// FP64 FMA throughput probe: 8 independent accumulator chains x 8 FMAs per iteration per thread.
+__global__ void __launch_bounds__(256) fma_probe_kernel(double *out, int iters) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (t + k);
+  const double b = 0.999999999, c = 1e-12;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  out[t] = s;
+}
+
+xb4::LoadFlags to_flags(const xd_flags &f) {
+  xb4::LoadFlags l;
+  l.dcop = f.dcop;
+  l.init_tran = f.init_tran;
+  l.newton_iter = f.newton_iter;
+  l.init_jct = f.init_jct;
+  l.init_fix = f.init_fix;
+  l.transient = f.transient;
+  l.tranop = f.tranop;
+  l.acop = f.acop;
+  l.voltlim = f.voltlim;
+  l.input_op = f.input_op;
+  l.gmin = f.gmin;
+  l.pdt = f.pdt;
+  return l;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *xd_last_error(void) { return g_err.c_str(); }
+
+int xd_num_instances(const xd_ctx *ctx) { return ctx ? ctx->n : -1; }
+int xd_num_state_slots(const xd_ctx *ctx) { return ctx ? (int)xb4::kNumState : -1; }
+int xd_num_store_slots(const xd_ctx *ctx) { return ctx ? (int)xb4::kNumStore : -1; }
+
+int xd_destroy(xd_ctx *ctx) {
+  if (!ctx) return 0;
+  DeviceGuard g(ctx->device);
+  cudaFree(ctx->d_tab);
+  cudaFree(ctx->d_rec);
+  cudaFree(ctx->d_nodes);
+  cudaFree(ctx->d_vgb);
+  cudaFree(ctx->d_stage);
+  free_map(ctx->vmap);
+  free_map(ctx->mmap);
+  delete ctx;
+  return 0;
+}
+
+int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, xd_ctx **out) {
+  g_err.clear();
+  if (!fam || !pat || !out) return fail(-1, "null argument");
+  *out = nullptr;
+  if (fam->level != 14 && fam->level != 54) return fail(-2, "only BSIM4 (level 14/54) is implemented");
+  if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
+  if ((long long)fam->n_inst * xb4::kNumStage >= (1LL << 31)) return fail(-1, "too many instances");
+  if (pat->n_rows < 0 || !pat->rowptr || (pat->rowptr[pat->n_rows] > 0 && !pat->colind))
+    return fail(-1, "bad CSR pattern");
+  const int n = fam->n_inst;
+  const int nu = pat->n_rows;
+  // Model cards and per-record constants.
+  std::vector<xb4::ModelSpec> models(fam->n_models);
+  size_t off = 0;
+  for (int m = 0; m < fam->n_models; ++m) {
+    models[m].pmos = fam->model_is_pmos[m] != 0;
+    for (int k = 0; k < fam->model_nparams[m]; ++k, ++off)
+      models[m].params.push_back({fam->model_param_names[off], fam->model_param_values[off]});
+  }
+  std::vector<std::string> ipn;
+  for (int k = 0; k < fam->n_inst_params; ++k) ipn.push_back(fam->inst_param_names[k]);
+  xb4::SetupOptions opts;
+  opts.temp_c = fam->temp_c;
+  opts.tnom_c = fam->tnom_c;
+  xb4::RecordTable rt;
+  std::string e = xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  if (!e.empty()) return fail(-2, e);
+  // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent).
+  std::vector<int4> nodes(n);
+  for (int i = 0; i < n; ++i) {
+    int v[4];
+    for (int k = 0; k < 4; ++k) {
+      v[k] = fam->inst_nodes[4 * (size_t)i + k];
+      if (v[k] >= nu) return fail(-1, "instance node index beyond the pattern's unknowns");
+      if (v[k] < 0) v[k] = -1;
+    }
+    nodes[i] = make_int4(v[0], v[1], v[2], v[3]);
+  }
+  std::vector<int> vt, vs, mt, ms;
+  vt.reserve((size_t)4 * n);
+  vs.reserve((size_t)4 * n);
+  mt.reserve((size_t)16 * n);
+  ms.reserve((size_t)16 * n);
+  for (int i = 0; i < n; ++i) {
+    const int nd[4] = {nodes[i].x, nodes[i].y, nodes[i].z, nodes[i].w};
+    for (int r = 0; r < 4; ++r) {
+      vt.push_back(nd[r]);
+      vs.push_back(r * n + i);
+    }
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) {
+        int p = -1;
+        if (nd[r] >= 0 && nd[c] >= 0) {
+          const int *b = pat->colind + pat->rowptr[nd[r]], *en = pat->colind + pat->rowptr[nd[r] + 1];
+          const int *q = std::lower_bound(b, en, nd[c]);
+          if (q == en || *q != nd[c]) return fail(-1, "CSR pattern lacks an entry the instance stamps");
+          p = (int)(q - pat->colind);
+        }
+        mt.push_back(p);
+        ms.push_back((r * 4 + c) * n + i);
+      }
+  }
+  int rc = cudaSetDevice(cuda_device);
+  if (rc != cudaSuccess) return cuda_fail((cudaError_t)rc, "cudaSetDevice");
+  xd_ctx *ctx = new xd_ctx();
+  ctx->device = cuda_device;
+  ctx->n = n;
+  ctx->n_unknowns = nu;
+  ctx->nnz = pat->rowptr[nu];
+  ctx->n_rec = rt.n_records;
+  auto cleanup = [&](int code) {
+    xd_destroy(ctx);
+    return code;
+  };
+  cudaError_t ce;
+  if ((ce = cudaMalloc(&ctx->d_tab, std::max<size_t>(1, rt.tab.size()) * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMemcpy(ctx->d_tab, rt.tab.data(), rt.tab.size() * sizeof(double), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (ce = cudaMalloc(&ctx->d_rec, std::max(1, n) * sizeof(int))) != cudaSuccess ||
+      (ce = cudaMemcpy(ctx->d_rec, rt.inst_rec.data(), n * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMalloc(&ctx->d_nodes, std::max(1, n) * sizeof(int4))) != cudaSuccess ||
+      (ce = cudaMemcpy(ctx->d_nodes, nodes.data(), n * sizeof(int4), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMalloc(&ctx->d_vgb, std::max(1, n) * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMemset(ctx->d_vgb, 0, std::max(1, n) * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMalloc(&ctx->d_stage, std::max<size_t>(1, (size_t)xb4::kNumStage * n) * sizeof(double))) !=
+          cudaSuccess ||
+      (ce = cudaMemset(ctx->d_stage, 0, std::max<size_t>(1, (size_t)xb4::kNumStage * n) * sizeof(double))) !=
+          cudaSuccess)
+    return cleanup(cuda_fail(ce, "xd_create allocation"));
+  if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
+  if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
+  *out = ctx;
+  return 0;
+}
+
+int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta, double *d_curr_sta,
+                    double *d_next_sto, const double *d_curr_sto, void *stream) {
+  if (!ctx || !flags) return fail(-1, "null argument");
+  if (ctx->n == 0) return 0;
+  if (!d_sol || !d_next_sta || !d_next_sto || !d_curr_sto || !d_curr_sta) return fail(-1, "null device buffer");
+  if (flags->input_op) return fail(-2, "inputOP loads are not supported");
+  DeviceGuard g(ctx->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int blocks = (ctx->n + kEvalBlock - 1) / kEvalBlock;
+  bsim4_eval_kernel<<<blocks, kEvalBlock, 0, st>>>(ctx->n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, d_sol,
+                                                   d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, ctx->d_vgb,
+                                                   ctx->d_stage, to_flags(*flags));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "bsim4_eval_kernel launch");
+  return 0;
+}
+
+static int load_vectors_impl(xd_ctx *ctx, double *f, double *q, double *fx, double *qx, bool abs_mode, cudaStream_t st) {
+  const size_t n = (size_t)ctx->n;
+  if (abs_mode) {
+    OutSet<4, true> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}};
+    return run_gather(ctx->vmap, ctx->d_stage, os, st);
+  }
+  OutSet<4, false> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}};
+  return run_gather(ctx->vmap, ctx->d_stage, os, st);
+}
+
+static int load_matrices_impl(xd_ctx *ctx, double *jf, double *jq, bool abs_mode, cudaStream_t st) {
+  const size_t n = (size_t)ctx->n;
+  if (abs_mode) {
+    OutSet<2, true> os{{jf, jq}, {16 * n, 32 * n}};
+    return run_gather(ctx->mmap, ctx->d_stage, os, st);
+  }
+  OutSet<2, false> os{{jf, jq}, {16 * n, 32 * n}};
+  return run_gather(ctx->mmap, ctx->d_stage, os, st);
+}
+
+int xd_load_vectors(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, void *stream) {
+  if (!ctx) return fail(-1, "null context");
+  if (ctx->n == 0) return 0;
+  DeviceGuard g(ctx->device);
+  return load_vectors_impl(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, false, (cudaStream_t)stream);
+}
+
+int xd_load_matrices(xd_ctx *ctx, double *d_dfdx_vals, double *d_dqdx_vals, void *stream) {
+  if (!ctx) return fail(-1, "null context");
+  if (ctx->n == 0) return 0;
+  DeviceGuard g(ctx->device);
+  return load_matrices_impl(ctx, d_dfdx_vals, d_dqdx_vals, false, (cudaStream_t)stream);
+}
+
+int xd_load(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta, double *d_curr_sta,
+            double *d_next_sto, const double *d_curr_sto, double *d_f, double *d_q, double *d_dfdxdvp,
+            double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals, void *stream) {
+  int rc = xd_update_state(ctx, flags, d_sol, d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, stream);
+  if (rc) return rc;
+  if ((rc = xd_load_vectors(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, stream))) return rc;
+  return xd_load_matrices(ctx, d_dfdx_vals, d_dqdx_vals, stream);
+}
+
+int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,
+                double *d_dqdx_vals, void *stream) {
+  if (!ctx) return fail(-1, "null context");
+  if (ctx->n == 0) return 0;
+  DeviceGuard g(ctx->device);
+  int rc = load_vectors_impl(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, true, (cudaStream_t)stream);
+  if (rc) return rc;
+  return load_matrices_impl(ctx, d_dfdx_vals, d_dqdx_vals, true, (cudaStream_t)stream);
+}
+
+int xd_launches_per_load(const xd_ctx *ctx) {
+  if (!ctx) return -1;
+  if (ctx->n == 0) return 0;
+  return 1 + (ctx->vmap.n_short > 0) + (ctx->vmap.n_long > 0) + (ctx->mmap.n_short > 0) + (ctx->mmap.n_long > 0);
+}
+
+int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream) {
+  if (!d_out || blocks <= 0 || iters <= 0) return fail(-1, "bad probe arguments");
+  fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d_out, iters);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fma_probe_kernel launch");
+  return 0;
+}
+
+int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream) {
+  if (!ctx || !h_out) return fail(-1, "null argument");
+  DeviceGuard g(ctx->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  XD_CUDA(cudaMemcpyAsync(h_out, ctx->d_stage, (size_t)xb4::kNumStage * ctx->n * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  XD_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+}  // extern "C"

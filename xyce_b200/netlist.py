@@ -1,0 +1,204 @@
+"""Seeded synthetic circuits and the Jacobian pattern they induce.
+
+The reference reads SPICE netlists; the workloads here are generated instead, from a seed:
+
+* ``random_logic``  — a random gate-level digital netlist of BSIM4 MOSFETs in INV / NAND2 / NOR2
+  gates (gate type uniform), fan-out uniform in 1..4, each fan-out branch an RC wire (segment R
+  log-uniform in 10-1000 ohm, C log-uniform in 0.1-10 fF), driven by primary inputs with
+  piecewise-linear sources (50 ps edges). Gates only read nets created before them, so the
+  logic is acyclic.
+* ``inverter_ring`` — an odd-stage CMOS inverter ring with a load capacitor per stage.
+
+The unknowns follow the reference's modified nodal analysis: one unknown per circuit node
+(ground is not an unknown) and one per voltage-source branch current. ``jacobian_pattern``
+forms the union of all device stamps as a CSR pattern with sorted columns, which is what the
+reference's topology builds before devices register their Jacobian offsets
+(src/TopoManagerPKG/src/N_TOP_CktGraphBasic.C:1092-1142).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+NMOS, PMOS = 0, 1
+
+
+@dataclass
+class Circuit:
+    n_nodes: int                          # circuit nodes (unknowns 0 .. n_nodes-1)
+    mos_type: np.ndarray                  # [n_mos] NMOS / PMOS
+    mos_nodes: np.ndarray                 # [n_mos, 4] D, G, S, B (-1 = ground)
+    mos_w: np.ndarray                     # [n_mos] width (m)
+    mos_l: np.ndarray                     # [n_mos] length (m)
+    res_nodes: np.ndarray                 # [n_res, 2]
+    res_value: np.ndarray                 # [n_res] ohm
+    cap_nodes: np.ndarray                 # [n_cap, 2]
+    cap_value: np.ndarray                 # [n_cap] farad
+    vsrc_nodes: np.ndarray                # [n_vsrc, 2] (+, -)
+    vsrc_dc: np.ndarray                   # [n_vsrc] DC value (V)
+    vsrc_pwl: list = field(default_factory=list)  # per source: None or (times, values)
+    vdd: float = 1.2
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_mos(self) -> int:
+        return int(self.mos_type.shape[0])
+
+    @property
+    def n_vsrc(self) -> int:
+        return int(self.vsrc_nodes.shape[0])
+
+    @property
+    def n_unknowns(self) -> int:
+        return self.n_nodes + self.n_vsrc
+
+    def branch_index(self, k: int) -> int:
+        return self.n_nodes + k
+
+
+def _pairs_2term(nodes: np.ndarray) -> np.ndarray:
+    a, b = nodes[:, 0], nodes[:, 1]
+    rows = np.concatenate([a, a, b, b])
+    cols = np.concatenate([a, b, a, b])
+    return np.stack([rows, cols], 1)
+
+
+def jacobian_pattern(c: Circuit):
+    """CSR (rowptr, colind) over the unknowns: union of MOSFET 4x4, R/C 2x2 and V-source stamps."""
+    parts = []
+    m = c.mos_nodes.astype(np.int64)
+    r = np.repeat(m, 4, axis=1)
+    cc = np.tile(m, (1, 4))
+    parts.append(np.stack([r.reshape(-1), cc.reshape(-1)], 1))
+    if c.res_nodes.shape[0]:
+        parts.append(_pairs_2term(c.res_nodes.astype(np.int64)))
+    if c.cap_nodes.shape[0]:
+        parts.append(_pairs_2term(c.cap_nodes.astype(np.int64)))
+    if c.n_vsrc:
+        br = np.arange(c.n_nodes, c.n_nodes + c.n_vsrc, dtype=np.int64)
+        p, n = c.vsrc_nodes[:, 0].astype(np.int64), c.vsrc_nodes[:, 1].astype(np.int64)
+        parts.append(np.stack([np.concatenate([p, br, n, br]), np.concatenate([br, p, br, n])], 1))
+    pr = np.concatenate(parts, 0)
+    pr = pr[(pr[:, 0] >= 0) & (pr[:, 1] >= 0)]
+    nu = c.n_unknowns
+    key = np.unique(pr[:, 0] * nu + pr[:, 1])
+    rows = key // nu
+    cols = (key % nu).astype(np.int32)
+    rowptr = np.zeros(nu + 1, dtype=np.int64)
+    np.add.at(rowptr, rows + 1, 1)
+    rowptr = np.cumsum(rowptr).astype(np.int32)
+    return rowptr, cols
+
+
+def _loguniform(rng, lo, hi, n):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+
+
+def random_logic(n_mos_target: int, seed: int = 0, n_inputs: int = 64, wire_segments: int = 2, vdd: float = 1.2,
+                 wn: float = 1e-6, wp: float = 2e-6, length: float = 0.18e-6, edge: float = 50e-12) -> Circuit:
+    """Random INV/NAND2/NOR2 netlist with about ``n_mos_target`` MOSFETs (see module doc)."""
+    rng = np.random.default_rng(seed)
+    # Gate types: 0 INV (2 MOSFETs, 1 input), 1 NAND2 (4, 2), 2 NOR2 (4, 2); mean 10/3 MOSFETs.
+    n_gates = max(1, int(round(n_mos_target * 3 / 10)))
+    gtype = rng.integers(0, 3, n_gates)
+    n_pins = np.where(gtype == 0, 1, 2)
+    node = 0
+    VDD = node
+    node += 1
+    inputs = np.arange(node, node + n_inputs)
+    node += n_inputs
+    outs = np.arange(node, node + n_gates)
+    node += n_gates
+    mids = np.full(n_gates, -1)
+    nm = gtype != 0
+    mids[nm] = np.arange(node, node + int(nm.sum()))
+    node += int(nm.sum())
+    # Fan-out slots: each net (primary input or gate output) offers U{1..4} branch slots; a gate
+    # pin takes a random open slot of an earlier net (or, if none is open, a random earlier net).
+    net_src = np.concatenate([inputs, outs])
+    fan = rng.integers(1, 5, net_src.shape[0])
+    pin_net = np.empty(int(n_pins.sum()), dtype=np.int64)
+    pool = []
+    pool.extend(np.repeat(np.arange(n_inputs), fan[:n_inputs]).tolist())
+    pin = 0
+    for g in range(n_gates):
+        for _ in range(int(n_pins[g])):
+            if pool:
+                j = int(rng.integers(0, len(pool)))
+                pool[j], pool[-1] = pool[-1], pool[j]
+                pin_net[pin] = pool.pop()
+            else:
+                pin_net[pin] = int(rng.integers(0, n_inputs + g))
+            pin += 1
+        pool.extend([n_inputs + g] * int(fan[n_inputs + g]))
+    stub_nets = np.array(pool, dtype=np.int64)
+    # Each pin (and each unused slot) is reached through an RC ladder of `wire_segments` segments.
+    n_branch = pin_net.shape[0] + stub_nets.shape[0]
+    branch_net = np.concatenate([pin_net, stub_nets])
+    ladder = np.arange(node, node + n_branch * wire_segments).reshape(n_branch, wire_segments)
+    node += n_branch * wire_segments
+    drv = net_src[branch_net]
+    seg_from = np.concatenate([drv[:, None], ladder[:, :-1]], 1)
+    res_nodes = np.stack([seg_from.reshape(-1), ladder.reshape(-1)], 1)
+    res_value = _loguniform(rng, 10.0, 1000.0, res_nodes.shape[0])
+    cap_nodes = np.stack([ladder.reshape(-1), np.full(ladder.size, -1)], 1)
+    cap_value = _loguniform(rng, 0.1e-15, 10e-15, cap_nodes.shape[0])
+    pin_node = ladder[: pin_net.shape[0], -1]
+    # Transistors.
+    typ, nod = [], []
+    first_pin = np.concatenate([[0], np.cumsum(n_pins)[:-1]])
+    for g in range(n_gates):
+        o = outs[g]
+        a = pin_node[first_pin[g]]
+        if gtype[g] == 0:
+            typ += [PMOS, NMOS]
+            nod += [[o, a, VDD, VDD], [o, a, -1, -1]]
+            continue
+        b = pin_node[first_pin[g] + 1]
+        m = mids[g]
+        if gtype[g] == 1:  # NAND2: PMOS in parallel, NMOS in series
+            typ += [PMOS, PMOS, NMOS, NMOS]
+            nod += [[o, a, VDD, VDD], [o, b, VDD, VDD], [o, a, m, -1], [m, b, -1, -1]]
+        else:  # NOR2: PMOS in series, NMOS in parallel
+            typ += [PMOS, PMOS, NMOS, NMOS]
+            nod += [[m, a, VDD, VDD], [o, b, m, VDD], [o, a, -1, -1], [o, b, -1, -1]]
+    mos_type = np.array(typ, dtype=np.int32)
+    mos_nodes = np.array(nod, dtype=np.int32)
+    mos_w = np.where(mos_type == PMOS, wp, wn)
+    mos_l = np.full(mos_type.shape[0], length)
+    # Sources: VDD, and one PWL source per primary input (random bit sequence, 50 ps edges).
+    vsrc_nodes = np.stack([np.concatenate([[VDD], inputs]), np.full(n_inputs + 1, -1)], 1)
+    vsrc_dc = np.concatenate([[vdd], np.zeros(n_inputs)])
+    pwl = [None]
+    period = 1e-9
+    for k in range(n_inputs):
+        bits = rng.integers(0, 2, 12)
+        t, v = [0.0], [vdd * bits[0]]
+        for j in range(1, bits.shape[0]):
+            t0 = j * period * 0.5 + rng.uniform(0, 0.2e-9)
+            t += [t0, t0 + edge]
+            v += [v[-1], vdd * bits[j]]
+        pwl.append((np.array(t), np.array(v)))
+    return Circuit(n_nodes=node, mos_type=mos_type, mos_nodes=mos_nodes, mos_w=mos_w, mos_l=mos_l,
+                   res_nodes=res_nodes.astype(np.int32), res_value=res_value, cap_nodes=cap_nodes.astype(np.int32),
+                   cap_value=cap_value, vsrc_nodes=vsrc_nodes.astype(np.int32), vsrc_dc=vsrc_dc, vsrc_pwl=pwl,
+                   vdd=vdd, meta=dict(kind="random_logic", seed=seed, n_gates=n_gates, n_inputs=n_inputs))
+
+
+def inverter_ring(stages: int = 101, vdd: float = 1.8, wn: float = 1e-6, wp: float = 2e-6, length: float = 0.18e-6,
+                  cload: float = 5e-15) -> Circuit:
+    """Odd-stage CMOS inverter ring with a load capacitor on every stage output."""
+    VDD = 0
+    out = np.arange(1, stages + 1)
+    inp = np.roll(out, 1)
+    typ = np.tile([PMOS, NMOS], stages)
+    nod = np.empty((2 * stages, 4), dtype=np.int32)
+    nod[0::2] = np.stack([out, inp, np.full(stages, VDD), np.full(stages, VDD)], 1)
+    nod[1::2] = np.stack([out, inp, np.full(stages, -1), np.full(stages, -1)], 1)
+    w = np.where(typ == PMOS, wp, wn)
+    return Circuit(n_nodes=stages + 1, mos_type=typ.astype(np.int32), mos_nodes=nod, mos_w=w,
+                   mos_l=np.full(2 * stages, length), res_nodes=np.zeros((0, 2), np.int32), res_value=np.zeros(0),
+                   cap_nodes=np.stack([out, np.full(stages, -1)], 1).astype(np.int32),
+                   cap_value=np.full(stages, cload), vsrc_nodes=np.array([[VDD, -1]], np.int32),
+                   vsrc_dc=np.array([vdd]), vsrc_pwl=[None], vdd=vdd, meta=dict(kind="inverter_ring", stages=stages))

@@ -230,6 +230,10 @@ def main():
     dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), nu, device=dev_id)
     lib = _native.load()
     launches = lib.xd_launches_per_load(dev._h)
+    import ctypes
+
+    blk, minb = ctypes.c_int(), ctypes.c_int()
+    lib.xd_eval_launch_shape(dev._h, ctypes.byref(blk), ctypes.byref(minb))
     stream = torch.cuda.current_stream()
     f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
     rng = np.random.default_rng(args.seed + 17 * rank)
@@ -363,6 +367,7 @@ def main():
                      "unit": "GB/s", "frac": eval_achieved / hbm_peak, "traffic": None,
                      "note": f"peak = {peak_src} HBM copy bandwidth; algorithmic bytes {EVAL_BYTES_PER_INST} B/instance"},
         "kernels_ms": {"eval": t_eval, "gather_vectors": t_vec, "gather_matrices": t_mat},
+        "eval_launch_shape": {"block": blk.value, "min_blocks_per_sm": minb.value},
         "fp64": {"probe_peak_tflops": fp64_peak_tflops},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),

@@ -144,6 +144,9 @@ int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream);
  * FP64 FMAs in registers, and writes one checksum per thread into d_out (blocks*256 doubles);
  * timing it gives the FP64 FMA-pipe throughput the evaluation kernel is measured against. */
 int xd_launches_per_load(const xd_ctx *ctx);
+/* Launch shape (threads per block, minimum resident blocks per SM) that xd_create's autotuner
+ * selected for the evaluation kernel after timing every candidate on the circuit. */
+int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);
 
 #ifdef __cplusplus

@@ -58,6 +58,7 @@ SIGNATURES = {
     "xd_load_abs": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 7),
     "xd_copy_stamps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "xd_launches_per_load": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_eval_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
     "xd_probe_fp64_fma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
 }
 

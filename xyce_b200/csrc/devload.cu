@@ -42,15 +42,17 @@ int cuda_fail(cudaError_t e, const char *where) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
   } while (0)
 
-constexpr int kLongThreshold = 64;   // targets with more contributions get a block each
-constexpr int kLongBlock = 256;
-constexpr int kEvalBlock = 128;
+constexpr int kLongThreshold = 32;   // entries with more contributions take the chunked path
+constexpr int kChunk = 1024;         // contributions per chunk on the chunked path
+constexpr int kChunkBlock = 128;
 
 // Stamp-to-output gather map for one group of outputs (the four vectors, or the two matrices).
 struct GatherMap {
-  int n_short = 0, n_long = 0;
-  int *d_short_dst = nullptr, *d_short_ptr = nullptr;
-  int *d_long_dst = nullptr, *d_long_ptr = nullptr;
+  int n_short = 0, n_long = 0, n_chunks = 0;
+  int *d_short_dst = nullptr, *d_short_ptr = nullptr;  // thread-per-entry path
+  int *d_long_dst = nullptr, *d_long_chunk = nullptr;  // chunked path: entry -> [first chunk, next)
+  int *d_chunk_begin = nullptr;                        // chunk -> [first contribution, next)
+  double *d_partial = nullptr;                         // [NOUT][n_chunks] chunk partial sums
   int *d_src = nullptr;  // staging index within one output's slot range
   size_t n_src = 0;
 };
@@ -82,11 +84,13 @@ struct xd_ctx {
   double *d_vgb = nullptr;
   double *d_stage = nullptr;
   GatherMap vmap, mmap;
+  int eval_variant = 0;
 };
 
 namespace {
 
-__global__ void __launch_bounds__(kEvalBlock) bsim4_eval_kernel(
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
@@ -159,21 +163,24 @@ __global__ void gather_short_kernel(int nt, const int *__restrict__ dst, const i
     if (os.out[o]) os.out[o][d] += acc[o];
 }
 
-// One block per output entry with many contributions: each thread sums a fixed strided subset in
-// order, then a fixed-shape tree combines the partial sums (deterministic).
+// Entries with many contributions (the supply rail's row, for instance) are split into fixed
+// chunks of kChunk consecutive contributions. Pass 1: one block per chunk sums its chunk with a
+// fixed strided split and a fixed-shape tree into a per-chunk partial. Pass 2: one warp per
+// entry combines its chunk partials in a fixed tree and adds the result to the output. Both the
+// split and the trees are fixed by the map, so the result is bit-identical run to run.
 template <int NOUT, bool ABS>
-__global__ void __launch_bounds__(kLongBlock) gather_long_kernel(const int *__restrict__ dst,
-                                                                 const int *__restrict__ ptr,
-                                                                 const int *__restrict__ src,
-                                                                 const double *__restrict__ stage,
-                                                                 OutSet<NOUT, ABS> os) {
-  __shared__ double red[NOUT][kLongBlock];
-  const int t = blockIdx.x;
-  const int b = ptr[t], e = ptr[t + 1];
+__global__ void __launch_bounds__(kChunkBlock) gather_chunk_kernel(const int *__restrict__ chunk_begin,
+                                                                   const int *__restrict__ src,
+                                                                   const double *__restrict__ stage,
+                                                                   double *__restrict__ partial, int n_chunks,
+                                                                   OutSet<NOUT, ABS> os) {
+  __shared__ double red[NOUT][kChunkBlock];
+  const int c = blockIdx.x;
+  const int b = chunk_begin[c], e = chunk_begin[c + 1];
   double acc[NOUT];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
-  for (int k = b + threadIdx.x; k < e; k += kLongBlock) {
+  for (int k = b + threadIdx.x; k < e; k += kChunkBlock) {
     const size_t s = (size_t)src[k];
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(kLongBlock) gather_long_kernel(const int *__re
 #pragma unroll
   for (int o = 0; o < NOUT; ++o) red[o][threadIdx.x] = acc[o];
   __syncthreads();
-  for (int w = kLongBlock / 2; w > 0; w >>= 1) {
+  for (int w = kChunkBlock / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
 #pragma unroll
       for (int o = 0; o < NOUT; ++o) red[o][threadIdx.x] += red[o][threadIdx.x + w];
@@ -192,10 +199,35 @@ __global__ void __launch_bounds__(kLongBlock) gather_long_kernel(const int *__re
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) partial[(size_t)o * n_chunks + c] = red[o][0];
+  }
+}
+
+template <int NOUT, bool ABS>
+__global__ void gather_combine_kernel(int n_long, const int *__restrict__ dst, const int *__restrict__ first_chunk,
+                                      const double *__restrict__ partial, int n_chunks, OutSet<NOUT, ABS> os) {
+  const int t = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (t >= n_long) return;
+  const int b = first_chunk[t], e = first_chunk[t + 1];
+  double acc[NOUT];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
+  for (int k = b + lane; k < e; k += 32) {
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) acc[o] += partial[(size_t)o * n_chunks + k];
+  }
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) acc[o] += __shfl_down_sync(0xffffffffu, acc[o], w);
+  }
+  if (lane == 0) {
     const int d = dst[t];
 #pragma unroll
     for (int o = 0; o < NOUT; ++o)
-      if (os.out[o]) os.out[o][d] += red[o][0];
+      if (os.out[o]) os.out[o][d] += acc[o];
   }
 }
 
@@ -206,8 +238,13 @@ int run_gather(const GatherMap &m, const double *stage, const OutSet<NOUT, ABS> 
     gather_short_kernel<NOUT, ABS><<<(m.n_short + blk - 1) / blk, blk, 0, st>>>(m.n_short, m.d_short_dst,
                                                                                m.d_short_ptr, m.d_src, stage, os);
   }
-  if (m.n_long > 0)
-    gather_long_kernel<NOUT, ABS><<<m.n_long, kLongBlock, 0, st>>>(m.d_long_dst, m.d_long_ptr, m.d_src, stage, os);
+  if (m.n_long > 0) {
+    gather_chunk_kernel<NOUT, ABS><<<m.n_chunks, kChunkBlock, 0, st>>>(m.d_chunk_begin, m.d_src, stage, m.d_partial,
+                                                                       m.n_chunks, os);
+    const int warps = 8;
+    gather_combine_kernel<NOUT, ABS><<<(m.n_long + warps - 1) / warps, 32 * warps, 0, st>>>(
+        m.n_long, m.d_long_dst, m.d_long_chunk, m.d_partial, m.n_chunks, os);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "gather launch");
   return 0;
@@ -220,7 +257,7 @@ int build_map(const std::vector<int> &tgt_of, const std::vector<int> &src_of, in
   for (int t : tgt_of)
     if (t >= 0) ++count[t];
   // Order targets: short ones first, long ones in a separate list; both keep ascending target.
-  std::vector<int> short_dst, long_dst, short_ptr(1, 0), long_ptr(1, 0);
+  std::vector<int> short_dst, long_dst, short_ptr(1, 0);
   std::vector<long long> start(n_targets, -1);
   size_t n_src = 0;
   for (int t = 0; t < n_targets; ++t)
@@ -230,14 +267,16 @@ int build_map(const std::vector<int> &tgt_of, const std::vector<int> &src_of, in
       short_dst.push_back(t);
       short_ptr.push_back((int)n_src);
     }
-  const size_t long_base = n_src;
+  std::vector<int> long_chunk(1, 0), chunk_begin;
   for (int t = 0; t < n_targets; ++t)
     if (count[t] > kLongThreshold) {
       start[t] = (long long)n_src;
+      for (int k = 0; k < count[t]; k += kChunk) chunk_begin.push_back((int)(n_src + k));
       n_src += count[t];
       long_dst.push_back(t);
-      long_ptr.push_back((int)n_src);
+      long_chunk.push_back((int)chunk_begin.size());
     }
+  chunk_begin.push_back((int)n_src);
   if (n_src > (size_t)0x7fffffff) return fail(-1, "too many stamp contributions for 32-bit gather indices");
   std::vector<int> src(n_src);
   std::vector<long long> fillp(start);
@@ -248,8 +287,8 @@ int build_map(const std::vector<int> &tgt_of, const std::vector<int> &src_of, in
   }
   m.n_short = (int)short_dst.size();
   m.n_long = (int)long_dst.size();
+  m.n_chunks = (int)chunk_begin.size() - 1;
   m.n_src = n_src;
-  (void)long_base;
   auto up = [](int **d, const std::vector<int> &h) -> cudaError_t {
     if (h.empty()) {
       *d = nullptr;
@@ -262,7 +301,9 @@ int build_map(const std::vector<int> &tgt_of, const std::vector<int> &src_of, in
   XD_CUDA(up(&m.d_short_dst, short_dst));
   XD_CUDA(up(&m.d_short_ptr, short_ptr));
   XD_CUDA(up(&m.d_long_dst, long_dst));
-  XD_CUDA(up(&m.d_long_ptr, long_ptr));
+  XD_CUDA(up(&m.d_long_chunk, long_chunk));
+  XD_CUDA(up(&m.d_chunk_begin, chunk_begin));
+  if (m.n_chunks > 0) XD_CUDA(cudaMalloc(&m.d_partial, (size_t)4 * m.n_chunks * sizeof(double)));
   XD_CUDA(up(&m.d_src, src));
   return 0;
 }
@@ -271,7 +312,9 @@ void free_map(GatherMap &m) {
   cudaFree(m.d_short_dst);
   cudaFree(m.d_short_ptr);
   cudaFree(m.d_long_dst);
-  cudaFree(m.d_long_ptr);
+  cudaFree(m.d_long_chunk);
+  cudaFree(m.d_chunk_begin);
+  cudaFree(m.d_partial);
   cudaFree(m.d_src);
   m = GatherMap();
 }
@@ -294,6 +337,86 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(double *out, int iters) 
 #pragma unroll
   for (int k = 0; k < 8; ++k) s += a[k];
   out[t] = s;
+}
+
+// Launch shapes of the evaluation kernel. The kernel is register-bound (hundreds of live FP64
+// intermediates); the shapes trade occupancy against spills. xd_create times each on the
+// circuit and keeps the fastest.
+struct EvalVariant {
+  int block, min_blocks;
+};
+constexpr EvalVariant kEvalVariants[] = {{128, 1}, {128, 2}, {128, 3}, {128, 4}, {64, 4}, {256, 2}};
+constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
+
+void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const double *sol, double *next_sta,
+                 double *curr_sta, double *next_sto, const double *curr_sto, double *stage, cudaStream_t st) {
+  const int n = ctx->n;
+  const int blk = kEvalVariants[v].block;
+  const int grid = (n + blk - 1) / blk;
+#define XD_EVAL_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
+                     ctx->d_vgb, stage, fl
+  switch (v) {
+    case 0: bsim4_eval_kernel<128, 1><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 1: bsim4_eval_kernel<128, 2><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 2: bsim4_eval_kernel<128, 3><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 3: bsim4_eval_kernel<128, 4><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 4: bsim4_eval_kernel<64, 4><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    default: bsim4_eval_kernel<256, 2><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+  }
+#undef XD_EVAL_ARGS
+}
+
+// Times every launch shape on the circuit's own instances at a synthetic operating point (node
+// voltages spread over 0..1.2 V, transient flags) in scratch buffers, and returns the fastest.
+int autotune_eval(xd_ctx *ctx, int &best) {
+  best = 0;
+  const int n = ctx->n;
+  if (n < 4096) return 0;
+  double *sol = nullptr, *sta = nullptr, *sto = nullptr;
+  cudaError_t ce;
+  if ((ce = cudaMalloc(&sol, std::max(1, ctx->n_unknowns) * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMalloc(&sta, (size_t)2 * xb4::kNumState * n * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMalloc(&sto, (size_t)2 * xb4::kNumStore * n * sizeof(double))) != cudaSuccess) {
+    cudaFree(sol); cudaFree(sta); cudaFree(sto);
+    return cuda_fail(ce, "autotune allocation");
+  }
+  std::vector<double> h(std::max(1, ctx->n_unknowns));
+  for (size_t k = 0; k < h.size(); ++k) h[k] = 1.2 * (double)((k * 2654435761u) % 1000u) / 999.0;
+  cudaMemcpy(sol, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemset(sta, 0, (size_t)2 * xb4::kNumState * n * sizeof(double));
+  cudaMemset(sto, 0, (size_t)2 * xb4::kNumStore * n * sizeof(double));
+  xb4::LoadFlags fl{};
+  fl.transient = 1; fl.newton_iter = 1; fl.voltlim = 1; fl.gmin = 1e-12;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  for (int v = 0; v < kNumEvalVariants; ++v) {
+    launch_eval(v, ctx, fl, sol, sta, sta + (size_t)xb4::kNumState * n, sto, sto + (size_t)xb4::kNumStore * n,
+                ctx->d_stage, 0);
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < 3; ++r)
+      launch_eval(v, ctx, fl, sol, sta, sta + (size_t)xb4::kNumState * n, sto, sto + (size_t)xb4::kNumStore * n,
+                  ctx->d_stage, 0);
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sol);
+  cudaFree(sta);
+  cudaFree(sto);
+  // The tuning runs advanced the per-instance vgb memory; a fresh context starts from 0.
+  cudaMemset(ctx->d_vgb, 0, (size_t)n * sizeof(double));
+  ce = cudaDeviceSynchronize();
+  if (ce != cudaSuccess) return cuda_fail(ce, "autotune");
+  return 0;
 }
 
 xb4::LoadFlags to_flags(const xd_flags &f) {
@@ -428,6 +551,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
   if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
+  if ((rc = autotune_eval(ctx, ctx->eval_variant)) != 0) return cleanup(rc);
   *out = ctx;
   return 0;
 }
@@ -440,10 +564,8 @@ int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, dou
   if (flags->input_op) return fail(-2, "inputOP loads are not supported");
   DeviceGuard g(ctx->device);
   cudaStream_t st = (cudaStream_t)stream;
-  const int blocks = (ctx->n + kEvalBlock - 1) / kEvalBlock;
-  bsim4_eval_kernel<<<blocks, kEvalBlock, 0, st>>>(ctx->n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, d_sol,
-                                                   d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, ctx->d_vgb,
-                                                   ctx->d_stage, to_flags(*flags));
+  launch_eval(ctx->eval_variant, ctx, to_flags(*flags), d_sol, d_next_sta, d_curr_sta, d_next_sto, d_curr_sto,
+              ctx->d_stage, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "bsim4_eval_kernel launch");
   return 0;
@@ -505,7 +627,15 @@ int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double
 int xd_launches_per_load(const xd_ctx *ctx) {
   if (!ctx) return -1;
   if (ctx->n == 0) return 0;
-  return 1 + (ctx->vmap.n_short > 0) + (ctx->vmap.n_long > 0) + (ctx->mmap.n_short > 0) + (ctx->mmap.n_long > 0);
+  return 1 + (ctx->vmap.n_short > 0) + 2 * (ctx->vmap.n_long > 0) + (ctx->mmap.n_short > 0) +
+         2 * (ctx->mmap.n_long > 0);
+}
+
+int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks) {
+  if (!ctx || !block || !min_blocks) return fail(-1, "null argument");
+  *block = kEvalVariants[ctx->eval_variant].block;
+  *min_blocks = kEvalVariants[ctx->eval_variant].min_blocks;
+  return 0;
 }
 
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream) {

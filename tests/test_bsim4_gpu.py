@@ -67,12 +67,13 @@ def _check_step(step, flags, g, r, n, charges=True, rowptr=None):
     bad, worst = compare("sto", gs, rs)
     assert bad == 0, f"step {step}: store out of tolerance ({worst:.3g}x)"
     if charges:
-        bad, worst = compare("sta", g["next_sta"], r["next_sta"], None, RTOL)
-        # Charges are sums of cancelling terms; compare against the charge magnitude scale.
+        # Charges are sums of cancelling terms: the floor is 1e-14 of the instance's largest charge.
         scale = np.abs(r["next_sta"]).reshape(3, n).max(0)
-        d = np.abs(g["next_sta"] - r["next_sta"]).reshape(3, n)
-        assert np.all(d <= RTOL * np.maximum(np.abs(r["next_sta"].reshape(3, n)), 1e-3 * scale) + 1e-30), \
-            f"step {step}: state out of tolerance"
+        detail = []
+        bad, worst = compare("sta", g["next_sta"].reshape(3, n), r["next_sta"].reshape(3, n),
+                             np.broadcast_to(scale, (3, n)), RTOL, ABS_SUM_FLOOR, detail=detail)
+        report["sta"] = worst
+        assert bad == 0, f"step {step}: state out of tolerance ({worst:.3g}x): {detail}"
         if flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
             assert np.allclose(g["curr_sta"], g["next_sta"], rtol=0, atol=0)
     return report

@@ -149,6 +149,33 @@ int xd_launches_per_load(const xd_ctx *ctx);
 int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);
 
+/* Allocation-free load (no counterpart in the reference: it is for callers of this library).
+ *
+ * Same work and same results as xd_load, but the scratch the load needs between evaluation and
+ * assembly (48 staged values per instance and the chunk partial sums) lives in one fixed array
+ * inside the library — a file-scope __device__ array of XD_STATIC_MAX_INSTANCES * 52 doubles
+ * (6.8 MB) that every GPU loading the library holds until the process exits — instead of the
+ * context's own buffers. The call itself performs no cudaMalloc, cudaFree or other allocation.
+ * It is meant for callers that cannot allocate device memory when they load: a solver that has
+ * handed all device memory to its own pool allocator, or that runs its Newton loop under a
+ * fixed memory budget, still needs the context (xd_create allocates once at set-up) but gets
+ * no per-call or per-context scratch from this entry point.
+ *
+ *   - Families with more than XD_STATIC_MAX_INSTANCES instances are rejected (< 0, see
+ *     xd_last_error); use xd_load for them.
+ *   - The first call on a device resolves the array's device address (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream capture.
+ *   - Every call, from every context on the device, shares the one array and it keeps the last
+ *     call's contents. Calls whose work overlaps on the GPU (different streams, or different
+ *     host threads without ordering) race on it; order them on one stream.
+ *   - Nothing in the array needs to start at zero: each call writes every staged value and
+ *     every partial it later reads. */
+#define XD_STATIC_MAX_INSTANCES 16384
+int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta,
+                           double *d_curr_sta, double *d_next_sto, const double *d_curr_sto, double *d_f,
+                           double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,
+                           double *d_dqdx_vals, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

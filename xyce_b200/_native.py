@@ -59,6 +59,7 @@ SIGNATURES = {
     "xd_copy_stamps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "xd_launches_per_load": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_eval_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
+    "xd_load_static_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
     "xd_probe_fp64_fma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
 }
 

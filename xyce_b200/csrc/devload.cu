@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "../../include/xyce_devload.h"
@@ -654,6 +655,98 @@ int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream) {
                           cudaMemcpyDeviceToHost, st));
   XD_CUDA(cudaStreamSynchronize(st));
   return 0;
+}
+
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free load. Scratch for the staged stamps and the chunk partial sums lives in a
+// file-scope device array instead of context buffers, so xd_load_static_scratch itself never
+// allocates. Capacity: XD_STATIC_MAX_INSTANCES instances (48 staged doubles each) plus
+// 4 * XD_STATIC_MAX_INSTANCES chunk partials — 52 * 16384 doubles = 6.8 MB, held by every GPU
+// that loads the library until the process exits.
+namespace {
+
+constexpr size_t kStaticStage = (size_t)XD_STATIC_MAX_INSTANCES * xb4::kNumStage;
+constexpr size_t kStaticPartial = (size_t)4 * XD_STATIC_MAX_INSTANCES;
+static __device__ __align__(256) double g_static_scratch[kStaticStage + kStaticPartial];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double *g_static_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_static_scratch on the current device (resolved once per device). In host
+// code the symbol names a host-side stand-in, never a device address, so kernels only ever get
+// the address cudaGetSymbolAddress returns.
+int static_scratch_on(int dev, double **out) {
+  if (dev < 0 || dev >= kMaxDevices) return fail(-1, "device ordinal out of range for static scratch");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+    g_static_ptr[dev] = static_cast<double *>(p);
+  }
+  *out = g_static_ptr[dev];
+  return 0;
+}
+
+template <int NOUT>
+int run_gather_static(const GatherMap &m, const double *stage, double *partial, const OutSet<NOUT, false> &os,
+                      cudaStream_t st) {
+  if (m.n_short > 0) {
+    const int blk = 256;
+    gather_short_kernel<NOUT, false><<<(m.n_short + blk - 1) / blk, blk, 0, st>>>(m.n_short, m.d_short_dst,
+                                                                                m.d_short_ptr, m.d_src, stage, os);
+  }
+  if (m.n_long > 0) {
+    gather_chunk_kernel<NOUT, false><<<m.n_chunks, kChunkBlock, 0, st>>>(m.d_chunk_begin, m.d_src, stage, partial,
+                                                                         m.n_chunks, os);
+    const int warps = 8;
+    gather_combine_kernel<NOUT, false><<<(m.n_long + warps - 1) / warps, 32 * warps, 0, st>>>(
+        m.n_long, m.d_long_dst, m.d_long_chunk, partial, m.n_chunks, os);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "gather launch");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta,
+                           double *d_curr_sta, double *d_next_sto, const double *d_curr_sto, double *d_f, double *d_q,
+                           double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals,
+                           void *stream) {
+  if (!ctx || !flags) return fail(-1, "null argument");
+  if (ctx->n > XD_STATIC_MAX_INSTANCES)
+    return fail(-1, "xd_load_static_scratch: " + std::to_string(ctx->n) + " instances exceed the static scratch "
+                    "capacity of " + std::to_string(XD_STATIC_MAX_INSTANCES) + "; use xd_load");
+  if (4 * (size_t)ctx->vmap.n_chunks > kStaticPartial || 2 * (size_t)ctx->mmap.n_chunks > kStaticPartial)
+    return fail(-1, "xd_load_static_scratch: gather partials exceed the static scratch capacity; use xd_load");
+  if (ctx->n == 0) return 0;
+  if (!d_sol || !d_next_sta || !d_next_sto || !d_curr_sto || !d_curr_sta) return fail(-1, "null device buffer");
+  if (flags->input_op) return fail(-2, "inputOP loads are not supported");
+  DeviceGuard g(ctx->device);
+  double *scratch = nullptr;
+  int rc = static_scratch_on(ctx->device, &scratch);
+  if (rc) return rc;
+  double *stage = scratch;
+  double *partial = scratch + kStaticStage;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Every staged slot of every instance is written by the evaluation before the gathers read it,
+  // and every chunk partial is written before it is combined, so nothing needs clearing.
+  launch_eval(ctx->eval_variant, ctx, to_flags(*flags), d_sol, d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, stage,
+              st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "bsim4_eval_kernel launch");
+  const size_t n = (size_t)ctx->n;
+  OutSet<4, false> vs{{d_f, d_q, d_dfdxdvp, d_dqdxdvp}, {0, 4 * n, 8 * n, 12 * n}};
+  if ((rc = run_gather_static(ctx->vmap, stage, partial, vs, st))) return rc;
+  OutSet<2, false> ms{{d_dfdx_vals, d_dqdx_vals}, {16 * n, 32 * n}};
+  return run_gather_static(ctx->mmap, stage, partial, ms, st);
 }
 
 }  // extern "C"

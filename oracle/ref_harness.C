@@ -91,6 +91,8 @@ struct RefCircuit {
   std::vector<int> inst_lids;  // per instance: 4 external LIDs (ground mapped to n_unknowns)
   N_LAS_Matrix dFdx, dQdx;
   N_LAS_Vector flagSol;
+  // Views of the raw solver vectors for devices that index through N_LAS_Vector.
+  N_LAS_Vector vNextSol, vCurrSol, vLastSol, vNextSta, vCurrSta, vLastSta, vNextSto, vCurrSto, vLastSto, vQ;
   std::vector<double> nextSol, currSol, lastSol, nextSta, currSta, lastSta, nextSto, currSto, lastSto,
       staDeriv, f, q, b, dfdxdvp, dqdxdvp, leadF, leadQ;
   std::string err;
@@ -128,6 +130,26 @@ void bind_extern(RefCircuit &c) {
   e.dFdxMatrixPtr = &c.dFdx;
   e.dQdxMatrixPtr = &c.dQdx;
   e.flagSolVectorPtr = &c.flagSol;
+  c.vNextSol = N_LAS_Vector(c.nextSol.data(), (int)c.nextSol.size());
+  c.vCurrSol = N_LAS_Vector(c.currSol.data(), (int)c.currSol.size());
+  c.vLastSol = N_LAS_Vector(c.lastSol.data(), (int)c.lastSol.size());
+  c.vNextSta = N_LAS_Vector(c.nextSta.data(), (int)c.nextSta.size());
+  c.vCurrSta = N_LAS_Vector(c.currSta.data(), (int)c.currSta.size());
+  c.vLastSta = N_LAS_Vector(c.lastSta.data(), (int)c.lastSta.size());
+  c.vNextSto = N_LAS_Vector(c.nextSto.data(), (int)c.nextSto.size());
+  c.vCurrSto = N_LAS_Vector(c.currSto.data(), (int)c.currSto.size());
+  c.vLastSto = N_LAS_Vector(c.lastSto.data(), (int)c.lastSto.size());
+  c.vQ = N_LAS_Vector(c.q.data(), (int)c.q.size());
+  e.nextSolVectorPtr = &c.vNextSol;
+  e.currSolVectorPtr = &c.vCurrSol;
+  e.lastSolVectorPtr = &c.vLastSol;
+  e.nextStaVectorPtr = &c.vNextSta;
+  e.currStaVectorPtr = &c.vCurrSta;
+  e.lastStaVectorPtr = &c.vLastSta;
+  e.nextStoVectorPtr = &c.vNextSto;
+  e.currStoVectorPtr = &c.vCurrSto;
+  e.lastStoVectorPtr = &c.vLastSto;
+  e.daeQVectorPtr = &c.vQ;
 }
 
 void apply_flags(RefCircuit &c, const xref_flags &fl) {

@@ -77,25 +77,27 @@ class OracleRun:
         self.n = n
         self.sta_base = np.array([self.ref.state_base(i) for i in range(n)], dtype=np.int64)
         self.sto_base = np.array([self.ref.store_base(i) for i in range(n)], dtype=np.int64)
+        self.n_sta_slots = self.ref.n_state // max(1, n)
+        self.n_sto_slots = self.ref.n_store // max(1, n)
 
     def to_aos_sto(self, soa):
         """Product slot-major store block -> oracle per-instance layout."""
         out = np.zeros(max(1, self.ref.n_store))
-        for s in range(14):
+        for s in range(self.n_sto_slots):
             out[self.sto_base + s] = soa[s * self.n:(s + 1) * self.n]
         return out
 
     def to_aos_sta(self, soa):
         out = np.zeros(max(1, self.ref.n_state))
-        for s in range(3):
+        for s in range(self.n_sta_slots):
             out[self.sta_base + s] = soa[s * self.n:(s + 1) * self.n]
         return out
 
     def from_aos_sto(self, aos):
-        return np.concatenate([aos[self.sto_base + s] for s in range(14)])
+        return np.concatenate([aos[self.sto_base + s] for s in range(self.n_sto_slots)])
 
     def from_aos_sta(self, aos):
-        return np.concatenate([aos[self.sta_base + s] for s in range(3)])
+        return np.concatenate([aos[self.sta_base + s] for s in range(self.n_sta_slots)])
 
     def load(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa):
         nu = self.c.n_unknowns

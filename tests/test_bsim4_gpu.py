@@ -12,98 +12,14 @@ the scale of the rounding residue left where capacitances cancel analytically.
 import numpy as np
 import pytest
 
-from tests.parity import ABS_SUM_FLOOR, RTOL, OracleRun, compare, family_inputs
+from tests.parity import family_inputs
 from xyce_b200 import Bsim4Device, ModelCard, SolverFlags, netlist
 
 pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-
-def _dev(a):
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
-
-
-class GpuRun:
-    def __init__(self, dev: Bsim4Device, nnz: int, n_unknowns: int):
-        self.dev, self.nnz, self.nu = dev, nnz, n_unknowns
-
-    def load(self, flags, sol, next_sta, curr_sta, next_sto, curr_sto):
-        nu, nnz = self.nu, self.nnz
-        t = dict(sol=_dev(sol), next_sta=_dev(next_sta), curr_sta=_dev(curr_sta), next_sto=_dev(next_sto),
-                 curr_sto=_dev(curr_sto))
-        outs = {k: torch.zeros(nu, dtype=torch.float64, device="cuda") for k in ("f", "q", "dfdxdvp", "dqdxdvp")}
-        outs["dfdx"] = torch.zeros(nnz, dtype=torch.float64, device="cuda")
-        outs["dqdx"] = torch.zeros(nnz, dtype=torch.float64, device="cuda")
-        self.dev.update_state(flags, t["sol"], t["next_sta"], t["curr_sta"], t["next_sto"], t["curr_sto"])
-        self.dev.load_dae_vectors(outs["f"], outs["q"], outs["dfdxdvp"], outs["dqdxdvp"])
-        self.dev.load_dae_matrices(outs["dfdx"], outs["dqdx"])
-        sums = {k: torch.zeros_like(v) for k, v in outs.items()}
-        self.dev.load_abs(sums["f"], sums["q"], sums["dfdxdvp"], sums["dqdxdvp"], sums["dfdx"], sums["dqdx"])
-        torch.cuda.synchronize()
-        res = {k: v.cpu().numpy() for k, v in outs.items()}
-        res["next_sta"] = t["next_sta"].cpu().numpy()
-        res["curr_sta"] = t["curr_sta"].cpu().numpy()
-        res["next_sto"] = t["next_sto"].cpu().numpy()
-        res["abs"] = {k: v.cpu().numpy() for k, v in sums.items()}
-        return res
-
-
-STORE_WRITTEN = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13]
-
-
-def _check_step(step, flags, g, r, n, charges=True, rowptr=None):
-    report = {}
-    keys = ["f", "dfdxdvp", "dfdx"] + (["q", "dqdxdvp", "dqdx"] if charges else [])
-    for k in keys:
-        detail = []
-        bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR,
-                             rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail)
-        report[k] = worst
-        assert bad == 0, (f"step {step} {flags}: {k} has {bad} entries out of tolerance (worst {worst:.3g}x); "
-                          f"(name, index, gpu, ref, allowed): {detail}")
-    gs = g["next_sto"].reshape(14, n)[STORE_WRITTEN]
-    rs = r["next_sto"].reshape(14, n)[STORE_WRITTEN]
-    bad, worst = compare("sto", gs, rs)
-    assert bad == 0, f"step {step}: store out of tolerance ({worst:.3g}x)"
-    if charges:
-        # Charges are sums of cancelling terms: the floor is 1e-14 of the instance's largest charge.
-        scale = np.abs(r["next_sta"]).reshape(3, n).max(0)
-        detail = []
-        bad, worst = compare("sta", g["next_sta"].reshape(3, n), r["next_sta"].reshape(3, n),
-                             np.broadcast_to(scale, (3, n)), RTOL, ABS_SUM_FLOOR, detail=detail)
-        report["sta"] = worst
-        assert bad == 0, f"step {step}: state out of tolerance ({worst:.3g}x): {detail}"
-        if flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
-            assert np.allclose(g["curr_sta"], g["next_sta"], rtol=0, atol=0)
-    return report
-
-
-def _run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, charges_in_dc=False):
-    rowptr, colind = netlist.jacobian_pattern(c)
-    cards, inst_model, inst_nodes, params = family_inputs(c, cards, extra_params)
-    orc = OracleRun(c, cards, inst_model, inst_nodes, params, rowptr, colind)
-    dev = Bsim4Device(cards, inst_model, inst_nodes, params, (rowptr, colind), c.n_unknowns)
-    gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
-    n = inst_model.shape[0]
-    rng = np.random.default_rng(seed)
-    sta_n, sta_c = np.zeros(3 * n), np.zeros(3 * n)
-    sto_n, sto_c = np.zeros(14 * n), np.zeros(14 * n)
-    worst = {}
-    for step, flags in enumerate(seqs):
-        sol = rng.uniform(vrange[0], vrange[1], c.n_unknowns)
-        r = orc.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
-        g = gpu.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
-        charges = bool(flags.transient or flags.tranop or flags.acop) or charges_in_dc
-        rep = _check_step(step, flags, g, r, n, charges, rowptr)
-        for k, v in rep.items():
-            worst[k] = max(worst.get(k, 0.0), v)
-        # Both sides continue from the oracle's state and store.
-        sta_n, sta_c, sto_n = r["next_sta"], r["curr_sta"], r["next_sto"]
-        if flags.newton_iter == 0:
-            sto_c = r["next_sto"].copy()
-    dev.close()
-    return worst
+from tests.gpu_parity import GpuRun, run_sequence as _run_sequence  # noqa: E402
 
 
 TRANSIENT_SEQ = [SolverFlags(newton_iter=1, voltlim=0), SolverFlags(newton_iter=1), SolverFlags(newton_iter=2),

@@ -6,7 +6,9 @@ CUDA kernels behind a C ABI (include/xyce_devload.h), plus the host-side mirror 
 reference's Device interface (``device.Bsim4Device``) and seeded workload generators
 (``netlist``).
 """
-from .device import Bsim4Device, ModelCard, SolverFlags, BSIM4_STATE_SLOTS, BSIM4_STORE_SLOTS  # noqa: F401
+from .device import (Bsim4Device, Mos1Device, MosfetDevice, ModelCard, SolverFlags, BSIM4_STATE_SLOTS,  # noqa: F401
+                     BSIM4_STORE_SLOTS, MOS1_STATE_SLOTS, MOS1_STORE_SLOTS)
 from . import netlist  # noqa: F401
 
-__all__ = ["Bsim4Device", "ModelCard", "SolverFlags", "netlist", "BSIM4_STATE_SLOTS", "BSIM4_STORE_SLOTS"]
+__all__ = ["Bsim4Device", "Mos1Device", "MosfetDevice", "ModelCard", "SolverFlags", "netlist", "BSIM4_STATE_SLOTS",
+           "BSIM4_STORE_SLOTS", "MOS1_STATE_SLOTS", "MOS1_STORE_SLOTS"]

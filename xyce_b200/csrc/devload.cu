@@ -23,6 +23,7 @@
 #include "../../include/xyce_devload.h"
 #include "bsim4_eval.cuh"
 #include "bsim4_setup.h"
+#include "mos1.h"
 
 namespace {
 
@@ -73,7 +74,11 @@ struct DeviceGuard {
 
 }  // namespace
 
+// Model families the library evaluates (the reference's device levels).
+enum Family { kFamilyMos1 = 1, kFamilyBsim4 = 4 };
+
 struct xd_ctx {
+  int family = kFamilyBsim4;
   int device = 0;
   int n = 0;
   int n_unknowns = 0;
@@ -132,6 +137,45 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
     for (int k = 0; k < xb4::kNumState; ++k) curr_sta[(size_t)k * n + i] = o.sta[k];
   }
   vgb[i] = o.vgb;
+}
+
+// MOSFET level 1: one thread per instance; reads the previous time point's Meyer state for
+// back-averaging.
+__global__ void __launch_bounds__(128) mos1_eval_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, double *__restrict__ next_sta, const double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
+    xb4::LoadFlags fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 nd = nodes[i];
+  double V[4];
+  V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
+  V[1] = nd.y >= 0 ? sol[nd.y] : 0.0;
+  V[2] = nd.z >= 0 ? sol[nd.z] : 0.0;
+  V[3] = nd.w >= 0 ? sol[nd.w] : 0.0;
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+  double sto_old[xm1::kNumStore], csto[xm1::kNumStore], csta[xm1::kNumState];
+#pragma unroll
+  for (int k = 0; k < xm1::kNumStore; ++k) {
+    sto_old[k] = so[(size_t)k * n + i];
+    csto[k] = curr_sto[(size_t)k * n + i];
+  }
+#pragma unroll
+  for (int k = 0; k < xm1::kNumState; ++k) csta[k] = curr_sta[(size_t)k * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xm1::LoadOut o;
+  xm1::mos1_load(rp, V, sto_old, csta, csto, fl, o);
+#pragma unroll
+  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+#pragma unroll
+  for (int k = 0; k < xm1::kNumStore; ++k) next_sto[(size_t)k * n + i] = o.sto[k];
+#pragma unroll
+  for (int k = 0; k < xm1::kNumState; ++k) next_sta[(size_t)k * n + i] = o.sta[k];
 }
 
 template <int NOUT, bool ABS>
@@ -352,6 +396,11 @@ constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]
 void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const double *sol, double *next_sta,
                  double *curr_sta, double *next_sto, const double *curr_sto, double *stage, cudaStream_t st) {
   const int n = ctx->n;
+  if (ctx->family == kFamilyMos1) {
+    mos1_eval_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta,
+                                                      curr_sta, next_sto, curr_sto, stage, fl);
+    return;
+  }
   const int blk = kEvalVariants[v].block;
   const int grid = (n + blk - 1) / blk;
 #define XD_EVAL_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
@@ -372,7 +421,7 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
 int autotune_eval(xd_ctx *ctx, int &best) {
   best = 0;
   const int n = ctx->n;
-  if (n < 4096) return 0;
+  if (n < 4096 || ctx->family != kFamilyBsim4) return 0;
   double *sol = nullptr, *sta = nullptr, *sto = nullptr;
   cudaError_t ce;
   if ((ce = cudaMalloc(&sol, std::max(1, ctx->n_unknowns) * sizeof(double))) != cudaSuccess ||
@@ -444,8 +493,14 @@ extern "C" {
 const char *xd_last_error(void) { return g_err.c_str(); }
 
 int xd_num_instances(const xd_ctx *ctx) { return ctx ? ctx->n : -1; }
-int xd_num_state_slots(const xd_ctx *ctx) { return ctx ? (int)xb4::kNumState : -1; }
-int xd_num_store_slots(const xd_ctx *ctx) { return ctx ? (int)xb4::kNumStore : -1; }
+int xd_num_state_slots(const xd_ctx *ctx) {
+  if (!ctx) return -1;
+  return ctx->family == kFamilyMos1 ? (int)xm1::kNumState : (int)xb4::kNumState;
+}
+int xd_num_store_slots(const xd_ctx *ctx) {
+  if (!ctx) return -1;
+  return ctx->family == kFamilyMos1 ? (int)xm1::kNumStore : (int)xb4::kNumStore;
+}
 
 int xd_destroy(xd_ctx *ctx) {
   if (!ctx) return 0;
@@ -465,7 +520,13 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   g_err.clear();
   if (!fam || !pat || !out) return fail(-1, "null argument");
   *out = nullptr;
-  if (fam->level != 14 && fam->level != 54) return fail(-2, "only BSIM4 (level 14/54) is implemented");
+  int family;
+  if (fam->level == 14 || fam->level == 54)
+    family = kFamilyBsim4;
+  else if (fam->level == 1)
+    family = kFamilyMos1;
+  else
+    return fail(-2, "MOSFET level " + std::to_string(fam->level) + " is not implemented (levels 1, 14, 54 are)");
   if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
   if ((long long)fam->n_inst * xb4::kNumStage >= (1LL << 31)) return fail(-1, "too many instances");
   if (pat->n_rows < 0 || !pat->rowptr || (pat->rowptr[pat->n_rows] > 0 && !pat->colind))
@@ -486,7 +547,9 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   opts.temp_c = fam->temp_c;
   opts.tnom_c = fam->tnom_c;
   xb4::RecordTable rt;
-  std::string e = xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  std::string e = family == kFamilyMos1
+                      ? xm1::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+                      : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
   // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent).
   std::vector<int4> nodes(n);
@@ -526,6 +589,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   int rc = cudaSetDevice(cuda_device);
   if (rc != cudaSuccess) return cuda_fail((cudaError_t)rc, "cudaSetDevice");
   xd_ctx *ctx = new xd_ctx();
+  ctx->family = family;
   ctx->device = cuda_device;
   ctx->n = n;
   ctx->n_unknowns = nu;

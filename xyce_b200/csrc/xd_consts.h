@@ -29,6 +29,7 @@ constexpr double CONSTEPSSI = 1.03594e-10;
 constexpr double CONSTEXP_THRESHOLD = 34.0;
 constexpr double CONSTMAX_EXP = 5.834617425e14;
 constexpr double CONSTMIN_EXP = 1.713908431e-15;
+constexpr double CONSTMAX_EXP_ARG = 100.0;
 constexpr double CONSTDELTA_1 = 0.02;
 constexpr double CONSTDELTA_3 = 0.02;
 constexpr double CONSTDELTA_4 = 0.02;

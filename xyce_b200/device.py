@@ -1,9 +1,11 @@
 """Host-side mirror of the reference's MOSFET Device interface, backed by the B200 kernels.
 
-``Bsim4Device`` plays the role of the reference's ``MOSFET_B4::Master`` object inside the
-device manager (src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C:16180-17268): one object
-per MOSFET family, created from .MODEL cards and instance lines, with the three per-iteration
-calls of ``Device`` (src/DeviceModelPKG/Core/include/N_DEV_Device.h:315, 361, 384):
+``MosfetDevice`` plays the role of one of the reference's MOSFET ``Master`` objects inside the
+device manager — ``Bsim4Device`` for ``MOSFET_B4::Master``
+(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C:16180-17268), ``Mos1Device`` for
+``MOSFET1::Master`` (N_DEV_MOSFET1.C:4069-4697): one object per MOSFET family, created from
+.MODEL cards and instance lines, with the three per-iteration calls of ``Device``
+(src/DeviceModelPKG/Core/include/N_DEV_Device.h:315, 361, 384):
 
     update_state(sol, sta, sto)          <- Device::updateState
     load_dae_vectors(f, q, dfdxdvp, dqdxdvp) <- Device::loadDAEVectors
@@ -81,8 +83,8 @@ def _stream_handle(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
-class Bsim4Device:
-    """One BSIM4 family (level 14/54) on one CUDA device.
+class MosfetDevice:
+    """One MOSFET family (one reference Device object) on one CUDA device.
 
     models:       list of ``ModelCard``
     inst_model:   int array [n]      card index per instance
@@ -94,7 +96,9 @@ class Bsim4Device:
     level = 14
 
     def __init__(self, models, inst_model, inst_nodes, inst_params, pattern, n_unknowns, device=0,
-                 temp_c=27.0, tnom_c=27.0):
+                 temp_c=27.0, tnom_c=27.0, level=None):
+        if level is not None:
+            self.level = int(level)
         lib = _native.load()
         self._lib = lib
         self.device = int(device)
@@ -146,8 +150,10 @@ class Bsim4Device:
         _native.check(lib.xd_create(ctypes.byref(fam), ctypes.byref(csr), self.device, ctypes.byref(h)), "xd_create")
         self._h = h
         self.nnz = int(rowptr[-1])
-        self.n_state = lib.xd_num_state_slots(h) * self.n
-        self.n_store = lib.xd_num_store_slots(h) * self.n
+        self.n_state_slots = lib.xd_num_state_slots(h)
+        self.n_store_slots = lib.xd_num_store_slots(h)
+        self.n_state = self.n_state_slots * self.n
+        self.n_store = self.n_store_slots * self.n
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -190,3 +196,19 @@ class Bsim4Device:
         _native.check(self._lib.xd_copy_stamps(self._h, ctypes.c_void_p(out.ctypes.data), _stream_handle(stream)),
                       "xd_copy_stamps")
         return out.reshape(48, self.n)
+
+
+class Bsim4Device(MosfetDevice):
+    """BSIM4 v4.6.1 (levels 14/54): the reference's MOSFET_B4::Master."""
+
+    level = 14
+
+
+class Mos1Device(MosfetDevice):
+    """Level-1 MOSFET (Shichman-Hodges, Meyer capacitances): the reference's MOSFET1::Master."""
+
+    level = 1
+
+
+MOS1_STATE_SLOTS = ("qgs", "qgd", "qgb", "capgs", "capgd", "capgb", "qbd", "qbs")
+MOS1_STORE_SLOTS = ("vbd", "vbs", "vgs", "vds", "von")

@@ -11,7 +11,7 @@ def _dev(a):
 
 
 class GpuRun:
-    def __init__(self, dev: Bsim4Device, nnz: int, n_unknowns: int):
+    def __init__(self, dev: MosfetDevice, nnz: int, n_unknowns: int):
         self.dev, self.nnz, self.nu = dev, nnz, n_unknowns
 
     def load(self, flags, sol, next_sta, curr_sta, next_sto, curr_sto):

@@ -36,7 +36,7 @@ class GpuRun:
 
 
 # Store slots each family writes (BSIM4 leaves vged / vgmd untouched, N_DEV_MOSFET_B4.C:16195-16210).
-STORE_WRITTEN = {14: [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13], 1: [0, 1, 2, 3, 4]}
+STORE_WRITTEN = {14: [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13], 9: [0, 1, 2, 3, 4], 1: [0, 1, 2, 3, 4]}
 
 
 def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=3, n_sto=14):
@@ -61,7 +61,7 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
                              np.broadcast_to(scale, (n_sta, n)), RTOL, ABS_SUM_FLOOR, detail=detail)
         report["sta"] = worst
         assert bad == 0, f"step {step}: state out of tolerance ({worst:.3g}x): {detail}"
-        if level == 14 and flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
+        if level in (9, 14) and flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
             assert np.allclose(g["curr_sta"], g["next_sta"], rtol=0, atol=0)
     return report
 
@@ -69,8 +69,9 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
 def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, charges_in_dc=False, level=14):
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, inst_model, inst_nodes, params = family_inputs(c, cards, extra_params)
-    orc = OracleRun(c, cards, inst_model, inst_nodes, params, rowptr, colind, level=level)
     dev = MosfetDevice(cards, inst_model, inst_nodes, params, (rowptr, colind), c.n_unknowns, level=level)
+    orc = OracleRun(c, cards, inst_model, inst_nodes, params, rowptr, colind, level=level,
+                    n_sta_slots=dev.n_state_slots)
     gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
     n = inst_model.shape[0]
     n_sta, n_sto = dev.n_state_slots, dev.n_store_slots

@@ -30,7 +30,7 @@ def row_scale(rowptr, vals_a, vals_b):
 
 
 def family_inputs(c: netlist.Circuit, cards=None, extra_params=None):
-    """(models, inst_model, inst_nodes, inst_params) for the circuit's MOSFETs (BSIM4)."""
+    """(models, inst_model, inst_nodes, inst_params) for the circuit's MOSFETs."""
     if cards is None:
         cards = [ModelCard(False, {}), ModelCard(True, {})]
     inst_model = c.mos_type.astype(np.int32)
@@ -49,7 +49,8 @@ def flags_dict(f: SolverFlags) -> dict:
 class OracleRun:
     """The reference's own device objects for the circuit's MOSFETs, on the product's pattern."""
 
-    def __init__(self, c: netlist.Circuit, cards, inst_model, inst_nodes, params, rowptr, colind, level=14):
+    def __init__(self, c: netlist.Circuit, cards, inst_model, inst_nodes, params, rowptr, colind, level=14,
+                 n_sta_slots=None):
         self.c = c
         models = [(m.pmos, dict(m.params)) for m in cards]
         nu = c.n_unknowns
@@ -77,7 +78,9 @@ class OracleRun:
         self.n = n
         self.sta_base = np.array([self.ref.state_base(i) for i in range(n)], dtype=np.int64)
         self.sto_base = np.array([self.ref.store_base(i) for i in range(n)], dtype=np.int64)
-        self.n_sta_slots = self.ref.n_state // max(1, n)
+        # The reference may reserve more state entries per instance than the load writes (BSIM3
+        # reserves 12 and writes the first 5 without NQS); the product keeps only the written ones.
+        self.n_sta_slots = self.ref.n_state // max(1, n) if n_sta_slots is None else n_sta_slots
         self.n_sto_slots = self.ref.n_store // max(1, n)
 
     def to_aos_sto(self, soa):

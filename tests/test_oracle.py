@@ -10,8 +10,8 @@ from oracle import xyce_ref as xr
 pytestmark = pytest.mark.skipif(not xr.available(), reason="oracle library not built")
 
 
-def _one_nmos(params=None):
-    ref = xr.RefCircuit(14, [(False, {})], np.array([0]), np.array([[0, 1, -1, -1]]),
+def _one_nmos(params=None, level=14):
+    ref = xr.RefCircuit(level, [(False, {})], np.array([0]), np.array([[0, 1, -1, -1]]),
                         params or {"L": np.array([0.18e-6]), "W": np.array([1e-6])}, 2)
     rows, cols = ref.stamp(0)
     nv = ref.n_unknowns + 1
@@ -59,3 +59,36 @@ def test_finite_difference_jacobian_matches_dfdx():
         fd = (F(s2).f - base.f) / h
         # dfdx entry (row 0, col j) in the 2x2 (+ground) pattern: row 0 columns are [0, 1, 2]
         assert fd[0] == pytest.approx(base.dfdx[j], rel=1e-4, abs=1e-12)
+
+
+def test_bsim3_default_topology_has_no_internal_nodes():
+    ref = _one_nmos(level=9)
+    assert ref.n_unknowns == 2
+    # 12 state entries are reserved per instance (5 used without NQS) and 5 store entries.
+    assert ref.n_state == 12 and ref.n_store == 5
+
+
+@pytest.mark.parametrize("level", [9, 14])
+def test_finite_difference_jacobians_both_families(level):
+    """dF/dx and dQ/dx of the oracle against central differences of F and Q (transient flags)."""
+    ref = _one_nmos(level=level)
+    ns, no = ref.n_state, ref.n_store
+    f0 = xr.make_flags(newton_iter=1, voltlim=0)
+    sol = np.array([0.9, 1.1, 0.0])
+
+    def load(s):
+        return ref.load(f0, s, np.zeros(ns), np.zeros(ns), np.zeros(no), np.zeros(no))
+
+    base = load(sol)
+    h = 1e-6
+    for j in range(2):
+        sp, sm = sol.copy(), sol.copy()
+        sp[j] += h
+        sm[j] -= h
+        lp, lm = load(sp), load(sm)
+        fd_f = (lp.f - lm.f) / (2 * h)
+        fd_q = (lp.q - lm.q) / (2 * h)
+        for r in range(2):
+            k = 3 * r + j  # row r of the 2 x (2 + ground) pattern
+            assert fd_f[r] == pytest.approx(base.dfdx[k], rel=1e-5, abs=1e-12)
+            assert fd_q[r] == pytest.approx(base.dqdx[k], rel=1e-5, abs=1e-22)

@@ -1,0 +1,51 @@
+"""Host-side set-up refuses the model options the B200 load does not implement, before any device
+memory is touched (so these run without a GPU). A refused card must never fall back to another
+implementation: xd_create returns an error and the Python mirror raises."""
+import numpy as np
+import pytest
+
+from xyce_b200 import ModelCard, MosfetDevice, netlist
+from xyce_b200._native import NativeError
+
+
+def _make(level, cards, extra=None):
+    c = netlist.inverter_ring(5)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float)}
+    if extra:
+        params.update({k: np.full(c.n_mos, v) for k, v in extra.items()})
+    return MosfetDevice(cards, c.mos_type, c.mos_nodes, params, (rowptr, colind), c.n_unknowns, level=level)
+
+
+NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
+
+
+@pytest.mark.parametrize("level,cards,extra,match", [
+    (3, NMOS_PMOS, None, "not implemented"),
+    (14, [ModelCard(False, {"RGATEMOD": 1}), ModelCard(True, {})], None, "rgateMod"),
+    (14, [ModelCard(False, {"CAPMOD": 1}), ModelCard(True, {})], None, "capMod"),
+    (14, NMOS_PMOS, {"NRD": 2.0}, "NRD/NRS"),
+    (14, [ModelCard(False, {"NOSUCH": 1.0}), ModelCard(True, {})], None, "unknown BSIM4 model parameter"),
+    (9, [ModelCard(False, {"CAPMOD": 0}), ModelCard(True, {})], None, "capMod"),
+    (9, [ModelCard(False, {"CAPMOD": 1}), ModelCard(True, {})], None, "capMod"),
+    (9, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], None, "series resistance"),
+    (9, NMOS_PMOS, {"NQSMOD": 1}, "nqsMod"),
+    (9, NMOS_PMOS, {"IC1": 0.5}, "initial conditions"),
+    (9, [ModelCard(False, {"NPEAK": 1e17}), ModelCard(True, {})], None, "unknown BSIM3 model parameter NPEAK"),
+    (1, [ModelCard(False, {"RD": 10.0}), ModelCard(True, {})], None, "series resistance"),
+    (1, NMOS_PMOS, {"IC2": 0.5}, "initial conditions"),
+])
+def test_unsupported_option_is_refused(level, cards, extra, match):
+    with pytest.raises(NativeError, match=match):
+        _make(level, cards, extra)
+
+
+def test_mixed_instance_temperatures_are_refused():
+    c = netlist.inverter_ring(5)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    temp = np.where(np.arange(c.n_mos) % 4 < 2, 27.0, 60.0)
+    for level in (9, 14):
+        params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float), "TEMP": temp}
+        # Instances alternate PMOS / NMOS, so each model's instances see both temperatures.
+        with pytest.raises(NativeError, match="share one temperature"):
+            MosfetDevice(NMOS_PMOS, c.mos_type, c.mos_nodes, params, (rowptr, colind), c.n_unknowns, level=level)

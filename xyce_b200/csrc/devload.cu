@@ -23,6 +23,7 @@
 #include "../../include/xyce_devload.h"
 #include "bsim4_eval.cuh"
 #include "bsim4_setup.h"
+#include "bsim3.h"
 #include "mos1.h"
 
 namespace {
@@ -75,7 +76,7 @@ struct DeviceGuard {
 }  // namespace
 
 // Model families the library evaluates (the reference's device levels).
-enum Family { kFamilyMos1 = 1, kFamilyBsim4 = 4 };
+enum Family { kFamilyMos1 = 1, kFamilyBsim3 = 3, kFamilyBsim4 = 4 };
 
 struct xd_ctx {
   int family = kFamilyBsim4;
@@ -387,6 +388,45 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(double *out, int iters) 
 // Launch shapes of the evaluation kernel. The kernel is register-bound (hundreds of live FP64
 // intermediates); the shapes trade occupancy against spills. xd_create times each on the
 // circuit and keeps the fastest.
+// BSIM3: one thread per instance.
+__global__ void __launch_bounds__(128) bsim3_eval_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
+    xb4::LoadFlags fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 nd = nodes[i];
+  double V[4];
+  V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
+  V[1] = nd.y >= 0 ? sol[nd.y] : 0.0;
+  V[2] = nd.z >= 0 ? sol[nd.z] : 0.0;
+  V[3] = nd.w >= 0 ? sol[nd.w] : 0.0;
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+  double sto_old[xb3::kNumStore];
+#pragma unroll
+  for (int k = 0; k < xb3::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb3::LoadOut o;
+  xb3::bsim3_load(rp, V, sto_old, fl, o);
+#pragma unroll
+  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+#pragma unroll
+  for (int k = 0; k < xb3::kNumStore; ++k) next_sto[(size_t)k * n + i] = o.sto[k];
+#pragma unroll
+  for (int k = 0; k < xb3::kNumState; ++k) next_sta[(size_t)k * n + i] = o.sta[k];
+  // Master::updateState also seeds the previous time point's charges on the first step of a
+  // transient (N_DEV_MOSFET_B3.C:9248-9262).
+  if (!fl.dcop && fl.init_tran && fl.newton_iter == 0) {
+#pragma unroll
+    for (int k = 0; k < xb3::kNumState; ++k) curr_sta[(size_t)k * n + i] = o.sta[k];
+  }
+}
+
 struct EvalVariant {
   int block, min_blocks;
 };
@@ -399,6 +439,11 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
   if (ctx->family == kFamilyMos1) {
     mos1_eval_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta,
                                                       curr_sta, next_sto, curr_sto, stage, fl);
+    return;
+  }
+  if (ctx->family == kFamilyBsim3) {
+    bsim3_eval_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
+                                                       next_sta, curr_sta, next_sto, curr_sto, stage, fl);
     return;
   }
   const int blk = kEvalVariants[v].block;
@@ -495,11 +540,15 @@ const char *xd_last_error(void) { return g_err.c_str(); }
 int xd_num_instances(const xd_ctx *ctx) { return ctx ? ctx->n : -1; }
 int xd_num_state_slots(const xd_ctx *ctx) {
   if (!ctx) return -1;
-  return ctx->family == kFamilyMos1 ? (int)xm1::kNumState : (int)xb4::kNumState;
+  return ctx->family == kFamilyMos1 ? (int)xm1::kNumState
+         : ctx->family == kFamilyBsim3 ? (int)xb3::kNumState
+                                       : (int)xb4::kNumState;
 }
 int xd_num_store_slots(const xd_ctx *ctx) {
   if (!ctx) return -1;
-  return ctx->family == kFamilyMos1 ? (int)xm1::kNumStore : (int)xb4::kNumStore;
+  return ctx->family == kFamilyMos1 ? (int)xm1::kNumStore
+         : ctx->family == kFamilyBsim3 ? (int)xb3::kNumStore
+                                       : (int)xb4::kNumStore;
 }
 
 int xd_destroy(xd_ctx *ctx) {
@@ -523,10 +572,13 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   int family;
   if (fam->level == 14 || fam->level == 54)
     family = kFamilyBsim4;
+  else if (fam->level == 9 || fam->level == 49)
+    family = kFamilyBsim3;
   else if (fam->level == 1)
     family = kFamilyMos1;
   else
-    return fail(-2, "MOSFET level " + std::to_string(fam->level) + " is not implemented (levels 1, 14, 54 are)");
+    return fail(-2, "MOSFET level " + std::to_string(fam->level) +
+                        " is not implemented (levels 1, 9, 49, 14, 54 are)");
   if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
   if ((long long)fam->n_inst * xb4::kNumStage >= (1LL << 31)) return fail(-1, "too many instances");
   if (pat->n_rows < 0 || !pat->rowptr || (pat->rowptr[pat->n_rows] > 0 && !pat->colind))
@@ -547,9 +599,10 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   opts.temp_c = fam->temp_c;
   opts.tnom_c = fam->tnom_c;
   xb4::RecordTable rt;
-  std::string e = family == kFamilyMos1
-                      ? xm1::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
-                      : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  std::string e =
+      family == kFamilyMos1    ? xm1::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+      : family == kFamilyBsim3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+                               : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
   // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent).
   std::vector<int4> nodes(n);

@@ -2,7 +2,8 @@
 
 ``MosfetDevice`` plays the role of one of the reference's MOSFET ``Master`` objects inside the
 device manager — ``Bsim4Device`` for ``MOSFET_B4::Master``
-(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C:16180-17268), ``Mos1Device`` for
+(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C:16180-17268), ``Bsim3Device`` for
+``MOSFET_B3::Master`` (N_DEV_MOSFET_B3.C:9199-9900), ``Mos1Device`` for
 ``MOSFET1::Master`` (N_DEV_MOSFET1.C:4069-4697): one object per MOSFET family, created from
 .MODEL cards and instance lines, with the three per-iteration calls of ``Device``
 (src/DeviceModelPKG/Core/include/N_DEV_Device.h:315, 361, 384):
@@ -204,11 +205,19 @@ class Bsim4Device(MosfetDevice):
     level = 14
 
 
+class Bsim3Device(MosfetDevice):
+    """BSIM3 v3.2.2 (levels 9/49): the reference's MOSFET_B3::Master."""
+
+    level = 9
+
+
 class Mos1Device(MosfetDevice):
     """Level-1 MOSFET (Shichman-Hodges, Meyer capacitances): the reference's MOSFET1::Master."""
 
     level = 1
 
 
+BSIM3_STATE_SLOTS = ("qb", "qg", "qd", "qbs", "qbd")
+BSIM3_STORE_SLOTS = ("vbd", "vbs", "vgs", "vds", "von")
 MOS1_STATE_SLOTS = ("qgs", "qgd", "qgb", "capgs", "capgd", "capgb", "qbd", "qbs")
 MOS1_STORE_SLOTS = ("vbd", "vbs", "vgs", "vds", "von")

@@ -52,6 +52,9 @@ def load_library(omp: bool = False):
         ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, _ip, _ip,
         ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     lib.xref_destroy.argtypes = [ctypes.c_void_p]
+    if hasattr(lib, "xref_set_perturbation"):
+        lib.xref_set_perturbation.argtypes = [ctypes.c_int, ctypes.c_ulonglong]
+        lib.xref_set_perturbation.restype = None
     for name in ("xref_num_unknowns", "xref_num_state", "xref_num_store"):
         getattr(lib, name).argtypes = [ctypes.c_void_p]
         getattr(lib, name).restype = ctypes.c_int
@@ -171,7 +174,9 @@ class RefCircuit:
         self.nnz = int(self._rowptr[-1])
 
     def load(self, flags: XrefFlags, next_sol, next_sta, curr_sta, next_sto, curr_sto, curr_sol=None,
-             repetitions=1) -> RefLoad:
+             repetitions=1, perturb_seed=None) -> RefLoad:
+        """One reference load. With ``perturb_seed``, every exp/log/log10/pow result inside the load
+        is moved by one ulp (direction drawn from the seed); see libm_perturb.C."""
         nv = self.n_unknowns + 1
         next_sol = np.ascontiguousarray(next_sol, dtype=np.float64)
         assert next_sol.shape[0] == nv
@@ -184,10 +189,19 @@ class RefCircuit:
         csol = None if curr_sol is None else np.ascontiguousarray(curr_sol, dtype=np.float64)
         out = RefLoad(np.zeros(nv), np.zeros(nv), np.zeros(nv), np.zeros(nv), np.zeros(self.nnz),
                       np.zeros(self.nnz), nsta, csta, nsto)
-        rc = self.lib.xref_load(self.h, ctypes.byref(flags), _dptr(next_sol),
-                                _dptr(csol) if csol is not None else None, _dptr(nsta), _dptr(csta), _dptr(nsto),
-                                _dptr(csto), _dptr(out.f), _dptr(out.q), _dptr(out.dfdxdvp), _dptr(out.dqdxdvp),
-                                _dptr(out.dfdx), _dptr(out.dqdx), int(repetitions))
+        if perturb_seed is not None:
+            if not hasattr(self.lib, "xref_set_perturbation"):
+                raise RuntimeError("this oracle build has no libm perturbation (serial library only)")
+            self.lib.xref_set_perturbation(1, ctypes.c_ulonglong(int(perturb_seed)))
+        try:
+            rc = self.lib.xref_load(self.h, ctypes.byref(flags), _dptr(next_sol),
+                                    _dptr(csol) if csol is not None else None, _dptr(nsta), _dptr(csta),
+                                    _dptr(nsto), _dptr(csto), _dptr(out.f), _dptr(out.q), _dptr(out.dfdxdvp),
+                                    _dptr(out.dqdxdvp),
+                                    _dptr(out.dfdx), _dptr(out.dqdx), int(repetitions))
+        finally:
+            if perturb_seed is not None:
+                self.lib.xref_set_perturbation(0, ctypes.c_ulonglong(0))
         if rc != 0:
             raise RuntimeError(f"oracle load failed: {self.lib.xref_last_error(self.h).decode()}")
         out.next_sta = nsta[: self.n_state]

@@ -45,20 +45,23 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
     for k in keys:
         detail = []
         bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR,
-                             rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail)
+                             rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail,
+                             sens=r["sens"][k] if "sens" in r else None)
         report[k] = worst
         assert bad == 0, (f"step {step} {flags}: {k} has {bad} entries out of tolerance (worst {worst:.3g}x); "
                           f"(name, index, gpu, ref, allowed): {detail}")
     gs = g["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]]
     rs = r["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]]
-    bad, worst = compare("sto", gs, rs)
+    ss = r["sens"]["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]] if "sens" in r else None
+    bad, worst = compare("sto", gs, rs, sens=ss)
     assert bad == 0, f"step {step}: store out of tolerance ({worst:.3g}x)"
     if charges:
         # Charges are sums of cancelling terms: the floor is 1e-14 of the instance's largest charge.
         scale = np.abs(r["next_sta"]).reshape(n_sta, n).max(0)
         detail = []
         bad, worst = compare("sta", g["next_sta"].reshape(n_sta, n), r["next_sta"].reshape(n_sta, n),
-                             np.broadcast_to(scale, (n_sta, n)), RTOL, ABS_SUM_FLOOR, detail=detail)
+                             np.broadcast_to(scale, (n_sta, n)), RTOL, ABS_SUM_FLOOR, detail=detail,
+                             sens=r["sens"]["next_sta"].reshape(n_sta, n) if "sens" in r else None)
         report["sta"] = worst
         assert bad == 0, f"step {step}: state out of tolerance ({worst:.3g}x): {detail}"
         if level in (9, 14) and flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
@@ -82,7 +85,7 @@ def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, c
     worst = {}
     for step, flags in enumerate(seqs):
         sol = rng.uniform(vrange[0], vrange[1], c.n_unknowns)
-        r = orc.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
+        r = orc.load_with_sensitivity(flags, sol, sta_n, sta_c, sto_n, sto_c)
         g = gpu.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
         charges = bool(flags.transient or flags.tranop or flags.acop) or charges_in_dc
         rep = check_step(step, flags, g, r, n, charges, rowptr, level, n_sta, n_sto)

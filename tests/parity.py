@@ -18,6 +18,16 @@ from xyce_b200.device import ModelCard, SolverFlags
 RTOL = 1e-12
 ABS_SUM_FLOOR = 1e-14
 ROW_FLOOR = 1e-14
+# Conditioning: the oracle can rerun a load with every exp / log / log10 / pow result moved by one
+# ulp (oracle/libm_perturb.C). The largest change of an entry over SENS_SEEDS such runs measures
+# how much that entry depends on the last bit of the elementary functions; the GPU's functions and
+# the host C library's may differ by an ulp, so each entry's tolerance also admits SENS_FACTOR
+# times that change. Well-conditioned entries move by ~1e-16 relative and keep the 1e-12 bound;
+# the ones this opens up are values formed by cancellation (the drain-bulk transconductance of a
+# device deep in cut-off, for instance), which no implementation with a different libm can pin.
+SENS_FACTOR = 4.0
+SENS_SEEDS = (101, 202)
+OUTPUT_KEYS = ("f", "q", "dfdxdvp", "dqdxdvp", "dfdx", "dqdx", "next_sta", "next_sto")
 
 
 def row_scale(rowptr, vals_a, vals_b):
@@ -102,21 +112,34 @@ class OracleRun:
     def from_aos_sta(self, aos):
         return np.concatenate([aos[self.sta_base + s] for s in range(self.n_sta_slots)])
 
-    def load(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa):
+    def load(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa,
+             perturb_seed=None):
         nu = self.c.n_unknowns
         s = np.zeros(nu + 1)
         s[:nu] = sol
         out = self.ref.load(xr.make_flags(**flags_dict(flags)), s, self.to_aos_sta(next_sta_soa),
                             self.to_aos_sta(curr_sta_soa), self.to_aos_sto(next_sto_soa),
-                            self.to_aos_sto(curr_sto_soa))
+                            self.to_aos_sto(curr_sto_soa), perturb_seed=perturb_seed)
         return dict(f=out.f[:nu], q=out.q[:nu], dfdxdvp=out.dfdxdvp[:nu], dqdxdvp=out.dqdxdvp[:nu],
                     dfdx=out.dfdx[self.map], dqdx=out.dqdx[self.map], next_sta=self.from_aos_sta(out.next_sta),
                     curr_sta=self.from_aos_sta(out.curr_sta), next_sto=self.from_aos_sto(out.next_sto))
 
+    def load_with_sensitivity(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa,
+                              curr_sto_soa):
+        """The load, plus r["sens"][key]: per entry, the largest change over the one-ulp-perturbed
+        reruns. The perturbed runs go first so that the device objects' carried state (BSIM4
+        keeps the previous load's vgb) ends as the unperturbed load leaves it."""
+        pert = [self.load(flags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa, perturb_seed=sd)
+                for sd in SENS_SEEDS]
+        r = self.load(flags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa)
+        r["sens"] = {k: np.max([np.abs(p[k] - r[k]) for p in pert], axis=0) for k in OUTPUT_KEYS}
+        return r
 
-def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None):
+
+def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None, sens=None):
     """Returns (n_bad, worst ratio of |diff| to the allowed error). With rowptr (CSR values), adds
-    the row-scaled floor. If `detail` is a list, the worst offenders are appended to it."""
+    the row-scaled floor; with sens (the oracle's one-ulp sensitivity of each entry), adds
+    SENS_FACTOR times it. If `detail` is a list, the worst offenders are appended to it."""
     got = np.asarray(got)
     ref = np.asarray(ref)
     d = np.abs(got - ref)
@@ -125,6 +148,8 @@ def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr
         allow = allow + floor * np.asarray(abs_sum)
     if rowptr is not None:
         allow = allow + ROW_FLOOR * row_scale(rowptr, got, ref)
+    if sens is not None:
+        allow = allow + SENS_FACTOR * np.asarray(sens).reshape(allow.shape)
     allow = np.maximum(allow, 1e-300)
     ratio = d / allow
     bad = int(np.count_nonzero(d > allow))

@@ -127,6 +127,17 @@ int xd_load(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_n
             double *d_next_sto, const double *d_curr_sto, double *d_f, double *d_q, double *d_dfdxdvp,
             double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals, void *stream);
 
+/* Like xd_load, but stores (=) the family's sum into every vector entry and CSR value the family
+ * stamps, instead of adding to it; entries the family does not stamp are not touched. For a
+ * caller that keeps one set of output buffers per device family (zeroed once when allocated),
+ * this removes the zeroing pass the reference's loader makes before every load
+ * (N_LOA_NonlinearEquationLoader.C:128-133, 226-227). No counterpart in the reference: its
+ * devices only accumulate. */
+int xd_load_assign(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta,
+                   double *d_curr_sta, double *d_next_sto, const double *d_curr_sto, double *d_f,
+                   double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,
+                   double *d_dqdx_vals, void *stream);
+
 /* Test and error-bound support: like the two load calls, but adds |term| instead of term, so the
  * outputs hold, per entry, the sum of absolute contributions (the scale of the rounding error of
  * that entry's sum). */

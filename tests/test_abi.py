@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports every symbol include/xyce_devload.h declares (no GPU calls)."""
+"""The C-ABI library loads and exports every symbol the headers in include/ declare (no GPU calls)."""
 import os
 import re
 
@@ -10,9 +10,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_symbols():
-    text = open(os.path.join(ROOT, "include", "xyce_devload.h")).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(xd_[a-z0-9_]+)\s*\(", text)))
+    syms = set()
+    inc = os.path.join(ROOT, "include")
+    for name in sorted(os.listdir(inc)):
+        if name.endswith(".h"):
+            text = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, name)).read(), flags=re.S)
+            syms |= set(re.findall(r"\b(xd_[a-z0-9_]+)\s*\(", text))
+    return sorted(syms)
 
 
 def test_header_declares_the_entry_points():

@@ -1,4 +1,5 @@
-"""Loader for the package's native library (libxyce_b200.so) and its C ABI (include/xyce_devload.h).
+"""Loader for the package's native library (libxyce_b200.so) and its C ABI (include/xyce_devload.h,
+include/xyce_tia.h).
 
 The library is built in-tree by ``xyce_b200.build.build()``. There is no fallback: if the
 library is missing or was built for another architecture, loading fails with an error.
@@ -41,6 +42,13 @@ class XdCsr(ctypes.Structure):
     _fields_ = [("n_rows", ctypes.c_int), ("rowptr", _ip), ("colind", _ip)]
 
 
+class XdTiaCoef(ctypes.Structure):
+    """Mirror of ``xd_tia_coef``."""
+
+    _fields_ = [("mode", ctypes.c_int), ("qscale", ctypes.c_double), ("fscale", ctypes.c_double),
+                ("inv_h", ctypes.c_double), ("hist_scale", ctypes.c_double), ("gshunt", ctypes.c_double)]
+
+
 # Every symbol the header declares, with its ctypes signature.
 SIGNATURES = {
     "xd_create": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), ctypes.POINTER(XdCsr), ctypes.c_int,
@@ -61,6 +69,10 @@ SIGNATURES = {
     "xd_eval_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
     "xd_load_static_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
     "xd_probe_fp64_fma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "xd_load_assign": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
+    "xd_tia_create": (ctypes.c_int, [ctypes.POINTER(XdCsr), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_tia_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
 }
 
 _LIB = None

@@ -183,6 +183,7 @@ template <int NOUT, bool ABS>
 struct OutSet {
   double *out[NOUT];
   size_t base[NOUT];  // staging offset of each output's slot range
+  int assign = 0;     // 1: store the family's sum (=) instead of adding it (+=)
 };
 
 template <int NOUT, bool ABS>
@@ -206,7 +207,12 @@ __global__ void gather_short_kernel(int nt, const int *__restrict__ dst, const i
   const int d = dst[t];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o)
-    if (os.out[o]) os.out[o][d] += acc[o];
+    if (os.out[o]) {
+      if (os.assign)
+        os.out[o][d] = acc[o];
+      else
+        os.out[o][d] += acc[o];
+    }
 }
 
 // Entries with many contributions (the supply rail's row, for instance) are split into fixed
@@ -273,7 +279,12 @@ __global__ void gather_combine_kernel(int n_long, const int *__restrict__ dst, c
     const int d = dst[t];
 #pragma unroll
     for (int o = 0; o < NOUT; ++o)
-      if (os.out[o]) os.out[o][d] += acc[o];
+      if (os.out[o]) {
+        if (os.assign)
+          os.out[o][d] = acc[o];
+        else
+          os.out[o][d] += acc[o];
+      }
   }
 }
 
@@ -533,6 +544,9 @@ xb4::LoadFlags to_flags(const xd_flags &f) {
 
 }  // namespace
 
+// Error reporting for the library's other translation units (xd_last_error reads it).
+int xd_internal_fail(int code, const std::string &msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char *xd_last_error(void) { return g_err.c_str(); }
@@ -689,23 +703,24 @@ int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, dou
   return 0;
 }
 
-static int load_vectors_impl(xd_ctx *ctx, double *f, double *q, double *fx, double *qx, bool abs_mode, cudaStream_t st) {
+static int load_vectors_impl(xd_ctx *ctx, double *f, double *q, double *fx, double *qx, bool abs_mode, cudaStream_t st,
+                             int assign = 0) {
   const size_t n = (size_t)ctx->n;
   if (abs_mode) {
     OutSet<4, true> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}};
     return run_gather(ctx->vmap, ctx->d_stage, os, st);
   }
-  OutSet<4, false> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}};
+  OutSet<4, false> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}, assign};
   return run_gather(ctx->vmap, ctx->d_stage, os, st);
 }
 
-static int load_matrices_impl(xd_ctx *ctx, double *jf, double *jq, bool abs_mode, cudaStream_t st) {
+static int load_matrices_impl(xd_ctx *ctx, double *jf, double *jq, bool abs_mode, cudaStream_t st, int assign = 0) {
   const size_t n = (size_t)ctx->n;
   if (abs_mode) {
     OutSet<2, true> os{{jf, jq}, {16 * n, 32 * n}};
     return run_gather(ctx->mmap, ctx->d_stage, os, st);
   }
-  OutSet<2, false> os{{jf, jq}, {16 * n, 32 * n}};
+  OutSet<2, false> os{{jf, jq}, {16 * n, 32 * n}, assign};
   return run_gather(ctx->mmap, ctx->d_stage, os, st);
 }
 
@@ -730,6 +745,17 @@ int xd_load(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_n
   if (rc) return rc;
   if ((rc = xd_load_vectors(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, stream))) return rc;
   return xd_load_matrices(ctx, d_dfdx_vals, d_dqdx_vals, stream);
+}
+
+int xd_load_assign(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta, double *d_curr_sta,
+                   double *d_next_sto, const double *d_curr_sto, double *d_f, double *d_q, double *d_dfdxdvp,
+                   double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals, void *stream) {
+  int rc = xd_update_state(ctx, flags, d_sol, d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, stream);
+  if (rc) return rc;
+  if (ctx->n == 0) return 0;
+  DeviceGuard g(ctx->device);
+  if ((rc = load_vectors_impl(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, false, (cudaStream_t)stream, 1))) return rc;
+  return load_matrices_impl(ctx, d_dfdx_vals, d_dqdx_vals, false, (cudaStream_t)stream, 1);
 }
 
 int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,

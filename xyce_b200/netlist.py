@@ -186,6 +186,20 @@ def random_logic(n_mos_target: int, seed: int = 0, n_inputs: int = 64, wire_segm
                    vdd=vdd, meta=dict(kind="random_logic", seed=seed, n_gates=n_gates, n_inputs=n_inputs))
 
 
+# Model cards for the BSIM3 ring-oscillator workload (W/L = 1u/0.18u, PMOS W = 2u, VDD = 1.8 V).
+# An empty BSIM3 card makes the threshold ~2 V at L = 0.18u (VTH0 is then derived from VFB = -1
+# and a body factor K1 ~ 1.9 computed from the default doping and 15 nm oxide), above the supply,
+# so the ring would never switch. These project-chosen round values keep every other parameter at
+# its card default and give thresholds near 0.6 V and on-currents of a few hundred uA.
+RING_BSIM3_NMOS = {"TOX": 4e-9, "VTH0": 0.45, "K1": 0.55, "K2": 0.0, "U0": 400.0, "VSAT": 1e5}
+RING_BSIM3_PMOS = {"TOX": 4e-9, "VTH0": -0.45, "K1": 0.55, "K2": 0.0, "U0": 120.0, "VSAT": 8e4}
+
+
+def ring_bsim3_cards():
+    from .device import ModelCard
+    return [ModelCard(False, dict(RING_BSIM3_NMOS)), ModelCard(True, dict(RING_BSIM3_PMOS))]
+
+
 def inverter_ring(stages: int = 101, vdd: float = 1.8, wn: float = 1e-6, wp: float = 2e-6, length: float = 0.18e-6,
                   cload: float = 5e-15) -> Circuit:
     """Odd-stage CMOS inverter ring with a load capacitor on every stage output."""

@@ -1,0 +1,432 @@
+"""Transient analysis on the B200 device loads: the callers either side of the hot path.
+
+Restates, for the circuits this package generates (MOSFETs of one family, resistors, capacitors,
+DC and piecewise-linear voltage sources), the reference's transient driver:
+
+* linear devices — resistor, capacitor and independent voltage source loads
+  (src/DeviceModelPKG/OpenModels/src/N_DEV_Resistor.C:1075-1161, N_DEV_Capacitor.C:1821-2002,
+  N_DEV_Vsrc.C:941-1028); their dF/dx and dQ/dx do not depend on the solution, so they are
+  assembled once as CSR value arrays, and source values enter through b(t). PWL sources follow
+  PWLinData::updateSource (src/DeviceModelPKG/Core/src/N_DEV_SourceData.C:1371-1480).
+* the one-step integrator (N_TIA_OneStep.C: backward Euler on the first step after the operating
+  point, trapezoid after it), its Jacobian J = (1/h) dQ/dx + f dF/dx and residual with the
+  devices' voltage-limiter corrections (N_TIA_OneStep.C:272-336, 470-497) — formed on the GPU by
+  ``xd_tia_combine``.
+* the damped-Newton loop with its convergence test (N_NLS_DampedNewton.C:485-600, 1792-1900) and
+  the parameters the reference uses for DC operating points and for transient steps
+  (N_NLS_NLParams.C:90-160).
+
+Every device load and the combine run as CUDA kernels on device-resident buffers; the host only
+sees two scalars per Newton iteration (the residual's max norm and the update's weighted norm).
+The linear system is solved by a dense LU on the GPU for small circuits and by a host sparse LU
+(SuperLU through scipy) for large ones: the linear solve is outside the device-load path.
+
+Step control is fixed-step (the largest step the analysis allows), halving on Newton failure.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time as _time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from .device import MosfetDevice, SolverFlags
+
+
+@dataclass
+class NewtonParams:
+    """N_NLS_NLParams defaults: DC operating point, and the transient overrides (:120-131)."""
+
+    max_iter: int = 200
+    rhs_tol: float = 1e-6
+    delta_x_tol: float = 1.0
+    abs_tol: float = 1e-12
+    rel_tol: float = 1e-3
+    update_weights_each_iter: bool = True
+
+    @staticmethod
+    def dc() -> "NewtonParams":
+        return NewtonParams()
+
+    @staticmethod
+    def transient() -> "NewtonParams":
+        return NewtonParams(max_iter=20, rhs_tol=1e-2, delta_x_tol=0.33, abs_tol=1e-6, rel_tol=1e-2,
+                            update_weights_each_iter=False)
+
+
+def pwl_value(times, values, t: float) -> float:
+    """PWLinData::updateSource without delay or repeat: linear between points, zero-valued start at
+    t = 0 when the first point is later, the last value after the last point."""
+    n = len(times)
+    if t > times[n - 1]:
+        return float(values[n - 1])
+    loc = n - 1
+    for i in range(n):
+        if t < times[i]:
+            loc = i
+            break
+    if loc == 0:
+        t1, v1 = 0.0, 0.0
+    else:
+        t1, v1 = float(times[loc - 1]), float(values[loc - 1])
+    t2, v2 = float(times[loc]), float(values[loc])
+    if t1 == t2:
+        return v2
+    length = t2 - t1
+    return (t2 - t) * v1 / length + (-t1 + t) * v2 / length
+
+
+class LinearDevices:
+    """Resistors, capacitors and voltage sources of a circuit as constant CSR stamps."""
+
+    def __init__(self, c, rowptr, colind):
+        self.c = c
+        nu = c.n_unknowns
+        nnz = int(rowptr[-1])
+        rows = np.repeat(np.arange(nu), np.diff(rowptr))
+        key = rows.astype(np.int64) * nu + colind
+
+        def pos(r, cc):
+            k = np.searchsorted(key, np.asarray(r, np.int64) * nu + np.asarray(cc, np.int64))
+            assert np.all(key[k] == np.asarray(r, np.int64) * nu + cc), "pattern lacks a linear-device entry"
+            return k
+
+        self.lin_f = np.zeros(nnz)
+        self.lin_q = np.zeros(nnz)
+
+        def add2(vals, nodes, g):
+            a, b = nodes[:, 0], nodes[:, 1]
+            for r, cc, s in ((a, a, 1.0), (a, b, -1.0), (b, a, -1.0), (b, b, 1.0)):
+                m = (r >= 0) & (cc >= 0)
+                np.add.at(vals, pos(r[m], cc[m]), s * g[m])
+
+        if c.res_nodes.shape[0]:
+            add2(self.lin_f, c.res_nodes.astype(np.int64), 1.0 / c.res_value)
+        if c.cap_nodes.shape[0]:
+            add2(self.lin_q, c.cap_nodes.astype(np.int64), c.cap_value.astype(float))
+        self.branch = np.arange(c.n_nodes, c.n_nodes + c.n_vsrc)
+        if c.n_vsrc:
+            p, n = c.vsrc_nodes[:, 0].astype(np.int64), c.vsrc_nodes[:, 1].astype(np.int64)
+            for r, cc, s in ((p, self.branch, 1.0), (n, self.branch, -1.0), (self.branch, p, 1.0),
+                             (self.branch, n, -1.0)):
+                m = (r >= 0) & (cc >= 0)
+                np.add.at(self.lin_f, pos(r[m], cc[m]), s)
+
+    def source_values(self, t: float | None) -> np.ndarray:
+        """Source values at time t (None: the DC values)."""
+        c = self.c
+        v = np.array(c.vsrc_dc, dtype=float)
+        if t is not None:
+            for k, p in enumerate(c.vsrc_pwl):
+                if p is not None:
+                    v[k] = pwl_value(p[0], p[1], t)
+        return v
+
+
+@dataclass
+class StepStats:
+    newton_iters: list = field(default_factory=list)
+    times: list = field(default_factory=list)
+    failed_steps: int = 0
+    wall_s: float = 0.0
+    loads: int = 0
+
+
+class TransientBase:
+    """Operating point and fixed-step transient of a circuit: the integrator and Newton loop.
+
+    Subclasses supply the two per-iterate steps, ``_load(flags)`` (every device's F, Q, dF/dx,
+    dQ/dx at self.x) and ``_combine(mode, h, order, qn0, fhist)`` (Newton matrix, residual, Q and F
+    totals); the buffers are torch tensors on ``dev``.
+    ``solver``: "dense" (LU on ``dev``, small circuits), "splu" (host sparse LU) or "auto".
+    """
+
+    def __init__(self, c, n_state, n_store, rowptr, colind, dev, solver="auto", gmin=1e-12):
+        import torch
+
+        self.torch = torch
+        self.c = c
+        self.nu = c.n_unknowns
+        self.nnz = int(rowptr[-1])
+        self.rowptr = np.ascontiguousarray(rowptr, np.int32)
+        self.colind = np.ascontiguousarray(colind, np.int32)
+        self.dev = dev
+        self.gmin = gmin
+        self.gshunt = 0.0  # node-to-ground conductance during gmin stepping
+        self.limiting = True  # device voltage limiting, with its corrections in the Newton residual
+        self.lin = LinearDevices(c, self.rowptr, self.colind)
+        z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
+        self.next_sta, self.curr_sta = z(n_state), z(n_state)
+        self.next_sto, self.curr_sto = z(n_store), z(n_store)
+        self.jac, self.rhs, self.qtot, self.ftot = z(self.nnz), z(self.nu), z(self.nu), z(self.nu)
+        self.b = z(self.nu)
+        self.x = z(self.nu)
+        self._branch = torch.as_tensor(self.lin.branch, device=self.dev)
+        if solver == "auto":
+            solver = "dense" if self.nu <= 4096 else "splu"
+        self.solver = solver
+        if solver == "dense":
+            rows = np.repeat(np.arange(self.nu), np.diff(self.rowptr))
+            self._flat = torch.as_tensor(rows.astype(np.int64) * self.nu + self.colind, device=self.dev)
+            self._dense = torch.zeros(self.nu * self.nu, dtype=torch.float64, device=self.dev)
+        self.stats = StepStats()
+
+    def _set_sources(self, t):
+        vals = self.lin.source_values(t)
+        self.b.zero_()
+        if len(vals):
+            self.b[self._branch] = self.torch.as_tensor(vals, dtype=self.torch.float64, device=self.dev)
+
+    def _load(self, flags: SolverFlags):
+        raise NotImplementedError
+
+    def _combine(self, mode, h=None, order=1, qn0=None, fhist=None):
+        raise NotImplementedError
+
+    def _sync(self):
+        pass
+
+    def _solve(self):
+        torch = self.torch
+        if self.solver == "dense":
+            self._dense.zero_()
+            self._dense[self._flat] = self.jac
+            return torch.linalg.solve(self._dense.view(self.nu, self.nu), self.rhs)
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+        J = sp.csr_matrix((self.jac.cpu().numpy(), self.colind, self.rowptr), shape=(self.nu, self.nu))
+        dx = spl.splu(J.tocsc()).solve(self.rhs.cpu().numpy())
+        return torch.as_tensor(dx, device=self.dev)
+
+    def _newton(self, prm: NewtonParams, flags_for_iter, mode, h=None, order=1, qn0=None, fhist=None):
+        """Newton iterations from self.x; returns the number of updates or -1 (no convergence).
+
+        As in DampedNewton::solve, the residual is re-evaluated at each updated iterate and the
+        convergence test (:1792-1830) takes its max norm together with the weighted RMS norm of the
+        update just made, weights rel_tol * max(|x_ref|, |x|) + abs_tol (:325-350) with x_ref the
+        iterate the solve started from; a transient solve fixes the weights at its start. So the
+        last load of a converged solve is at the converged point, and Q and F there are current.
+        """
+        torch = self.torch
+        x_ref = self.x.clone()
+        w = prm.rel_tol * x_ref.abs() + prm.abs_tol
+        self._load(flags_for_iter(0))
+        self._combine(mode, h, order, qn0, fhist)
+        for it in range(1, prm.max_iter + 1):
+            dx = self._solve()
+            self.x += dx
+            if prm.update_weights_each_iter:
+                w = prm.rel_tol * torch.maximum(x_ref.abs(), self.x.abs()) + prm.abs_tol
+            wrms = float(torch.sqrt(torch.mean((dx / w) ** 2)))
+            self._load(flags_for_iter(it))
+            self._combine(mode, h, order, qn0, fhist)
+            max_rhs = float(self.rhs.abs().max())
+            if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
+                return -1
+            if max_rhs <= prm.rhs_tol and wrms <= prm.delta_x_tol:
+                return it
+        return -1
+
+    def _history_here(self):
+        """Q and F at the current point (after a load there) into q_tot / f_tot."""
+        zero = self.torch.zeros_like(self.x)
+        self._combine(1, 1.0, 1, zero, None)
+
+    # -- analyses -----------------------------------------------------------------------------------
+    def dcop(self, params: NewtonParams | None = None, x0=None, t0: float = 0.0) -> int:
+        """Operating point at time t0 (sources at their transient values, as the reference does
+        for the operating point of a transient), with charges computed (tranop); leaves Q(t0) and
+        F(t0) in q_tot / f_tot and the device history rotated. Plain Newton first; if it fails,
+        gmin stepping: a shunt conductance from every unknown to ground, lowered a decade at a
+        time from 1e-2 S, each stage starting from the previous one's solution, then removed.
+        Returns the total number of Newton updates."""
+        prm = params or NewtonParams.dc()
+        start = self.torch.zeros_like(self.x)
+        if x0 is not None:
+            start.copy_(self.torch.as_tensor(x0, dtype=self.torch.float64))
+        self._set_sources(t0)
+
+        def flags(it, first=True):
+            return SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=it,
+                               init_jct=1 if (it == 0 and first) else 0, gmin=self.gmin,
+                               voltlim=int(self.limiting))
+
+        self.x.copy_(start)
+        self.gshunt = 0.0
+        total = self._newton(prm, flags, mode=0)
+        if total < 0:
+            total = 0
+            self.x.copy_(start)
+            self.next_sta.zero_()
+            self.next_sto.zero_()
+            self.curr_sta.zero_()
+            self.curr_sto.zero_()
+            first = True
+            for g in [10.0 ** (-k) for k in range(2, 13)] + [0.0]:
+                self.gshunt = g
+                n_it = self._newton(prm, lambda it, first=first: flags(it, first), mode=0)
+                if n_it < 0:
+                    self.gshunt = 0.0
+                    raise RuntimeError(f"operating point did not converge (gmin stepping at {g:g} S)")
+                total += n_it
+                first = False
+                self.curr_sto.copy_(self.next_sto)
+            self.gshunt = 0.0
+        self._history_here()
+        self._accept_point()
+        return total
+
+    def _accept_point(self):
+        """The accepted point's device history becomes the current one."""
+        self.curr_sta.copy_(self.next_sta)
+        self.curr_sto.copy_(self.next_sto)
+
+    def set_initial_state(self, x, t0: float = 0.0):
+        """Starts the transient from x (an operating point with a kick, say): one load at x gives
+        Q(t0), F(t0) and the device history."""
+        self.x.copy_(self.torch.as_tensor(x, dtype=self.torch.float64))
+        self._set_sources(t0)
+        self._load(SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=1, gmin=self.gmin,
+                               voltlim=int(self.limiting)))
+        self._history_here()
+        self._accept_point()
+
+    def run(self, tstop: float, hmax: float, params: NewtonParams | None = None, record=None, warm_start=None,
+            min_step: float = 1e-18):
+        """Fixed-step transient from the current state to tstop. ``record``: unknown indices whose
+        waveforms are returned. ``warm_start(t, h, x_n, x_nm1)``: optional initial Newton iterate.
+        Returns (times, waveforms [n_points, len(record)])."""
+        torch = self.torch
+        prm = params or NewtonParams.transient()
+        rec = np.arange(self.nu) if record is None else np.asarray(record)
+        rec_t = torch.as_tensor(rec, device=self.dev)
+        t = 0.0
+        h = hmax
+        qn0 = self.qtot.clone()
+        fhist = self.ftot.clone()
+        x_n = self.x.clone()
+        x_nm1 = None
+        times, waves = [0.0], [self.x[rec_t].cpu().numpy()]
+        first = True
+        t_start = _time.perf_counter()
+        while t < tstop * (1 - 1e-12):
+            h = min(h, tstop - t)
+            order = 1 if first else 2
+            self._set_sources(t + h)
+            if warm_start is not None:
+                self.x.copy_(warm_start(t, h, x_n, x_nm1))
+            else:
+                self.x.copy_(x_n)
+
+            def flags(it, first=first, h=h):
+                return SolverFlags(transient=1, newton_iter=it, init_tran=1 if first else 0, pdt=1.0 / h,
+                                   gmin=self.gmin, voltlim=int(self.limiting))
+
+            n_it = self._newton(prm, flags, mode=1, h=h, order=order, qn0=qn0, fhist=fhist)
+            if n_it < 0:
+                self.stats.failed_steps += 1
+                # Restore the device history of the last accepted point and retry with half the step.
+                self.next_sta.copy_(self.curr_sta)
+                self.next_sto.copy_(self.curr_sto)
+                h *= 0.5
+                if h < min_step:
+                    raise RuntimeError(f"time step too small at t = {t:.6g}")
+                continue
+            t += h
+            first = False
+            # Accept: the last load was at the converged point, so q_tot / f_tot are Q and F there.
+            qn0.copy_(self.qtot)
+            fhist.copy_(self.ftot)
+            self._accept_point()
+            x_nm1, x_n = x_n, self.x.clone()
+            self.stats.newton_iters.append(n_it)
+            self.stats.times.append(t)
+            times.append(t)
+            waves.append(self.x[rec_t].cpu().numpy())
+            h = min(hmax, h * 2.0)
+        self._sync()
+        self.stats.wall_s += _time.perf_counter() - t_start
+        return np.array(times), np.stack(waves)
+
+
+class GpuTransient(TransientBase):
+    """The transient on one CUDA device: MOSFET loads by ``xd_load_assign`` and the combine with
+    the linear devices by ``xd_tia_combine``, on device-resident buffers.
+
+    ``family``: the circuit's MOSFETs as one ``MosfetDevice`` built on the pattern (rowptr, colind).
+    """
+
+    def __init__(self, c, family: MosfetDevice, rowptr, colind, device=0, solver="auto", gmin=1e-12):
+        import torch
+
+        super().__init__(c, family.n_state, family.n_store, rowptr, colind, torch.device("cuda", device), solver,
+                         gmin)
+        self.fam = family
+        lib = _native.load()
+        self._lib = lib
+        csr = _native.XdCsr(self.nu, self.rowptr.ctypes.data_as(_native._ip), self.colind.ctypes.data_as(_native._ip))
+        h = ctypes.c_void_p()
+        _native.check(lib.xd_tia_create(ctypes.byref(csr), int(device), ctypes.byref(h)), "xd_tia_create")
+        self._tia = h
+        T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=self.dev).contiguous()
+        z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
+        self.lin_f, self.lin_q = T(self.lin.lin_f), T(self.lin.lin_q)
+        # Family outputs (stored by xd_load_assign; entries the family does not stamp stay zero).
+        self.f, self.q, self.fx, self.qx = z(self.nu), z(self.nu), z(self.nu), z(self.nu)
+        self.jf, self.jq = z(self.nnz), z(self.nnz)
+
+    def close(self):
+        if getattr(self, "_tia", None) is not None and self._tia.value:
+            self._lib.xd_tia_destroy(self._tia)
+            self._tia = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ptr(self, t):
+        return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+    def _stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _sync(self):
+        self.torch.cuda.synchronize(self.dev)
+
+    def _load(self, flags: SolverFlags):
+        c = flags.to_c()
+        p = self._ptr
+        _native.check(self._lib.xd_load_assign(self.fam._h, ctypes.byref(c), p(self.x), p(self.next_sta),
+                                               p(self.curr_sta), p(self.next_sto), p(self.curr_sto), p(self.f),
+                                               p(self.q), p(self.fx), p(self.qx), p(self.jf), p(self.jq),
+                                               self._stream()), "xd_load_assign")
+        self.stats.loads += 1
+
+    def _combine(self, mode, h=None, order=1, qn0=None, fhist=None):
+        coef = tia_coef(mode, h, order, self.gshunt)
+        p = self._ptr
+        _native.check(self._lib.xd_tia_combine(self._tia, ctypes.byref(coef), p(self.x), p(self.jf), p(self.jq),
+                                               p(self.lin_f), p(self.lin_q), p(self.f), p(self.q),
+                                               p(self.fx) if self.limiting else None,
+                                               p(self.qx) if self.limiting else None, p(self.b),
+                                               p(qn0), p(fhist), p(self.jac), p(self.rhs), p(self.qtot),
+                                               p(self.ftot), self._stream()), "xd_tia_combine")
+
+
+def tia_coef(mode, h=None, order=1, gshunt=0.0) -> _native.XdTiaCoef:
+    """Coefficients of the one-step method: backward Euler (order 1) or trapezoid (order 2)."""
+    coef = _native.XdTiaCoef()
+    coef.mode = mode
+    coef.gshunt = gshunt
+    if mode:
+        coef.qscale = coef.inv_h = 1.0 / h
+        coef.fscale = 0.5 if order == 2 else 1.0
+        coef.hist_scale = 0.5 if order == 2 else 0.0
+    else:
+        coef.qscale, coef.fscale, coef.inv_h, coef.hist_scale = 0.0, 1.0, 0.0, 0.0
+    return coef

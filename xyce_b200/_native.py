@@ -49,7 +49,22 @@ class XdTiaCoef(ctypes.Structure):
                 ("inv_h", ctypes.c_double), ("hist_scale", ctypes.c_double), ("gshunt", ctypes.c_double)]
 
 
-# Every symbol the header declares, with its ctypes signature.
+class XdGemmArgs(ctypes.Structure):
+    """Mirror of ``xd_gemm_args`` (include/xyce_surrogate.h)."""
+
+    _fields_ = [("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("M", ctypes.c_int), ("N", ctypes.c_int),
+                ("K", ctypes.c_int), ("lda", ctypes.c_int), ("ldb", ctypes.c_int), ("ldc", ctypes.c_int),
+                ("ldt", ctypes.c_int), ("tile_n", ctypes.c_int), ("epilogue", ctypes.c_int),
+                ("C32", ctypes.c_void_p), ("bias", ctypes.c_void_p), ("Z", ctypes.c_void_p), ("H", ctypes.c_void_p),
+                ("HT", ctypes.c_void_p), ("Zin", ctypes.c_void_p), ("err", ctypes.c_void_p)]
+
+
+class XdAdamArgs(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("bias_corr1", ctypes.c_float), ("bias_corr2", ctypes.c_float)]
+
+
+# Every symbol the headers declare, with its ctypes signature.
 SIGNATURES = {
     "xd_create": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), ctypes.POINTER(XdCsr), ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_void_p)]),
@@ -73,6 +88,18 @@ SIGNATURES = {
     "xd_tia_create": (ctypes.c_int, [ctypes.POINTER(XdCsr), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "xd_tia_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
+    "xd_gemm_bf16": (ctypes.c_int, [ctypes.POINTER(XdGemmArgs), ctypes.c_int, ctypes.c_void_p]),
+    "xd_mse_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_void_p]),
+    "xd_bias_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p]),
+    "xd_splitk_sum": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_column_sum": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "xd_adam": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.POINTER(XdAdamArgs), ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
 }
 
 _LIB = None

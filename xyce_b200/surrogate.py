@@ -1,0 +1,259 @@
+"""Learned surrogate of the MOSFET current/charge map: an MLP trained and run on the tensor cores.
+
+Network (one per device type): 5 inputs (Vgs, Vds, Vbs, log W, log L; each scaled to about
+[-1, 1]) -> 4 hidden layers of 128 SiLU units -> 10 outputs, the drain current Id, the gate,
+drain and bulk charges Qg, Qd, Qb, and the bias derivatives gm = dId/dVgs, gds = dId/dVds,
+gmb = dId/dVbs, Cgg = dQg/dVgs, Cgd = dQg/dVds, Cgb = dQg/dVbs. Outputs are learned in a
+compressed scale, y = asinh(x / s) per output, so that relative accuracy holds across the many
+decades a MOSFET current spans.
+
+Weights are BF16 for the matrix products (FP32 master copies and Adam moments), accumulation is
+FP32. Every product runs in ``xd_gemm_bf16`` (tcgen05 tensor cores, include/xyce_surrogate.h) with
+the bias / SiLU / SiLU-derivative work fused into its epilogue; the loss gradient, bias gradients,
+split-K reductions and the Adam update are the library's own kernels as well. torch only owns the
+buffers and orders the calls on a stream.
+
+Shapes are padded for the tensor cores: inputs to 16 columns (K of the first layer), outputs to 16
+(N of the last), the batch to a multiple of 128.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+N_IN, N_HID, N_LAYERS, N_OUT = 5, 128, 4, 10
+PAD_IN, PAD_OUT = 16, 16
+OUTPUT_NAMES = ("Id", "Qg", "Qd", "Qb", "gm", "gds", "gmb", "Cgg", "Cgd", "Cgb")
+# Scale of each output inside asinh(x / s): about the smallest magnitude that still matters.
+OUTPUT_SCALE = np.array([1e-9, 1e-18, 1e-18, 1e-18, 1e-8, 1e-8, 1e-8, 1e-17, 1e-17, 1e-17])
+VMAX = 1.2
+LOG_W = (math.log(0.1e-6), math.log(10e-6))
+LOG_L = (math.log(30e-9), math.log(500e-9))
+
+
+def features(vgs, vds, vbs, w, l):
+    """Scaled network inputs [n, 5] from biases (V) and geometry (m)."""
+    def sc(x, lo, hi):
+        return (2.0 * (x - lo) / (hi - lo)) - 1.0
+    return np.stack([np.asarray(vgs) / VMAX, np.asarray(vds) / VMAX, np.asarray(vbs) / VMAX,
+                     sc(np.log(w), *LOG_W), sc(np.log(l), *LOG_L)], 1)
+
+
+def encode_targets(y):
+    return np.arcsinh(np.asarray(y) / OUTPUT_SCALE)
+
+
+def decode_outputs(z):
+    return np.sinh(np.asarray(z)) * OUTPUT_SCALE
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class _Lib:
+    def __init__(self, torch, device):
+        self.lib = _native.load()
+        self.torch = torch
+        self.dev = device
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def gemm(self, A, B, M, N, K, lda, ldb, epilogue, tile_n, *, C32=None, ldc=0, bias=None, Z=None, H=None, HT=None,
+             ldt=0, Zin=None, splits=1):
+        g = _native.XdGemmArgs()
+        g.A, g.B = A.data_ptr(), B.data_ptr()
+        g.M, g.N, g.K, g.lda, g.ldb, g.ldc, g.ldt = M, N, K, lda, ldb, ldc, ldt
+        g.tile_n, g.epilogue = tile_n, epilogue
+        for name, t in (("C32", C32), ("bias", bias), ("Z", Z), ("H", H), ("HT", HT), ("Zin", Zin)):
+            setattr(g, name, None if t is None else t.data_ptr())
+        g.err = self.err.data_ptr()
+        rc = self.lib.xd_gemm_bf16(ctypes.byref(g), int(splits), self.stream())
+        if rc < 0:
+            _native.check(rc, "xd_gemm_bf16")
+        return rc
+
+    def check_err(self):
+        if int(self.err.item()) != 0:
+            raise _native.NativeError("a tensor-core kernel's internal wait expired")
+
+
+EPI_F32, EPI_BIAS_F32, EPI_BIAS_SILU, EPI_SILU_BACK = 0, 1, 2, 3
+
+
+@dataclass
+class AdamConfig:
+    lr: float = 2e-3
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+
+
+class SurrogateMLP:
+    """One 5 -> 128^4 -> 10 SiLU network on a CUDA device, trained with the library's kernels."""
+
+    def __init__(self, device=0, seed=0, max_batch=65536):
+        import torch
+
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.k = _Lib(torch, self.dev)
+        g = torch.Generator().manual_seed(seed)
+        dims = [(N_HID, N_IN)] + [(N_HID, N_HID)] * (N_LAYERS - 1) + [(N_OUT, N_HID)]
+        pads = [(N_HID, PAD_IN)] + [(N_HID, N_HID)] * (N_LAYERS - 1) + [(PAD_OUT, N_HID)]
+        f32 = dict(dtype=torch.float32, device=self.dev)
+        self.W, self.b, self.mW, self.vW, self.mb, self.vb = [], [], [], [], [], []
+        self.W16, self.W16T = [], []
+        for (o, i), (po, pi) in zip(dims, pads):
+            w = torch.zeros(po, pi, dtype=torch.float32)
+            w[:o, :i] = (torch.rand(o, i, generator=g) * 2 - 1) * math.sqrt(6.0 / (i + o))
+            self.W.append(w.to(self.dev))
+            self.b.append(torch.zeros(po, **f32))
+            self.mW.append(torch.zeros(po, pi, **f32))
+            self.vW.append(torch.zeros(po, pi, **f32))
+            self.mb.append(torch.zeros(po, **f32))
+            self.vb.append(torch.zeros(po, **f32))
+            self.W16.append(self.W[-1].to(torch.bfloat16).contiguous())
+            self.W16T.append(self.W[-1].t().contiguous().to(torch.bfloat16))
+        self.dims, self.pads = dims, pads
+        self.step_count = 0
+        self._alloc(max_batch)
+
+    def _alloc(self, B):
+        torch = self.torch
+        B = (B + 127) // 128 * 128
+        self.max_batch = B
+        bf = dict(dtype=torch.bfloat16, device=self.dev)
+        f32 = dict(dtype=torch.float32, device=self.dev)
+        self.X16 = torch.zeros(B, PAD_IN, **bf)
+        self.XT16 = torch.zeros(PAD_IN, B, **bf)
+        self.Z = [torch.zeros(B, N_HID, **bf) for _ in range(N_LAYERS)]
+        self.H = [torch.zeros(B, N_HID, **bf) for _ in range(N_LAYERS)]
+        self.HT = [torch.zeros(N_HID, B, **bf) for _ in range(N_LAYERS)]
+        self.Y = torch.zeros(B, PAD_OUT, **f32)
+        self.dZ = [torch.zeros(B, N_HID, **bf) for _ in range(N_LAYERS)]
+        self.dZT = [torch.zeros(N_HID, B, **bf) for _ in range(N_LAYERS)]
+        self.dY16 = torch.zeros(B, PAD_OUT, **bf)
+        self.dYT16 = torch.zeros(PAD_OUT, B, **bf)
+        self.sq = torch.zeros(B, **f32)
+        self.T = torch.zeros(B, N_OUT, **f32)
+        self.splits = 64
+        self.part = torch.zeros(self.splits * N_HID * N_HID, **f32)
+        self.gW = [torch.zeros_like(w) for w in self.W]
+        self.gb = [torch.zeros_like(b) for b in self.b]
+
+    # -- forward / backward -------------------------------------------------------------------------
+    def _load_inputs(self, X):
+        torch = self.torch
+        n = X.shape[0]
+        Bp = (n + 127) // 128 * 128
+        if Bp > self.max_batch:
+            self._alloc(Bp)
+        x = torch.as_tensor(X, dtype=torch.float32, device=self.dev)
+        self.X16.zero_()
+        self.X16[:n, :N_IN] = x.to(torch.bfloat16)
+        self.XT16.zero_()
+        self.XT16[:N_IN, :n] = x.t().to(torch.bfloat16)
+        return n, Bp
+
+    def forward(self, X):
+        """Network outputs (scaled space) for inputs X [n, 5]; returns a float32 tensor [n, 10]."""
+        n, Bp = self._load_inputs(X)
+        self._forward(Bp)
+        return self.Y[:n, :N_OUT]
+
+    def _forward(self, Bp):
+        k = self.k
+        A, lda = self.X16, PAD_IN
+        for l in range(N_LAYERS):
+            k.gemm(A, self.W16[l], Bp, N_HID, lda, lda, lda, EPI_BIAS_SILU, 128, bias=self.b[l], Z=self.Z[l],
+                   H=self.H[l], HT=self.HT[l], ldc=N_HID, ldt=self.max_batch)
+            A, lda = self.H[l], N_HID
+        k.gemm(A, self.W16[N_LAYERS], Bp, PAD_OUT, N_HID, N_HID, N_HID, EPI_BIAS_F32, 16, C32=self.Y,
+               bias=self.b[N_LAYERS], ldc=PAD_OUT)
+
+    def _weight_grad(self, dZT, inT, n_out_rows, n_in, Bp, out):
+        """out [n_out_rows x n_in] = dZT [rows x Bp] . inT [n_in x Bp]^T, split over the batch."""
+        k = self.k
+        tile_n = 16 if n_in <= 16 else 128
+        splits = max(1, min(self.splits, Bp // 128))
+        used = k.gemm(dZT, inT, n_out_rows, n_in, Bp, self.max_batch, self.max_batch, EPI_F32, tile_n, C32=self.part,
+                      ldc=n_in, splits=splits)
+        _native.check(k.lib.xd_splitk_sum(n_out_rows * n_in, used, _p(self.part), _p(out), k.stream()),
+                      "xd_splitk_sum")
+
+    def backward(self, n, Bp):
+        """Gradients of the mean squared error (scaled space) w.r.t. every parameter, after a
+        forward pass on a batch whose targets are in self.T[:n]."""
+        k = self.k
+        L = N_LAYERS
+        scale = 2.0 / (n * N_OUT)
+        _native.check(k.lib.xd_mse_grad(n, N_OUT, PAD_OUT, _p(self.Y), _p(self.T), ctypes.c_float(scale),
+                                        _p(self.dY16), _p(self.dYT16), self.max_batch, _p(self.sq), k.stream()),
+                      "xd_mse_grad")
+        if Bp > n:
+            self.dY16[n:Bp].zero_()
+            self.dYT16[:, n:Bp].zero_()
+        # Output layer.
+        self._weight_grad(self.dYT16, self.HT[L - 1], PAD_OUT, N_HID, Bp, self.gW[L])
+        _native.check(k.lib.xd_bias_grad(Bp, PAD_OUT, _p(self.dYT16), self.max_batch, _p(self.gb[L]), k.stream()),
+                      "xd_bias_grad")
+        k.gemm(self.dY16, self.W16T[L], Bp, N_HID, PAD_OUT, PAD_OUT, PAD_OUT, EPI_SILU_BACK, 128, Zin=self.Z[L - 1],
+               H=self.dZ[L - 1], HT=self.dZT[L - 1], ldc=N_HID, ldt=self.max_batch)
+        # Hidden layers L-1 .. 1 (weights W[l], l >= 1).
+        for l in range(L - 1, 0, -1):
+            self._weight_grad(self.dZT[l], self.HT[l - 1], N_HID, N_HID, Bp, self.gW[l])
+            _native.check(k.lib.xd_bias_grad(Bp, N_HID, _p(self.dZT[l]), self.max_batch, _p(self.gb[l]), k.stream()),
+                          "xd_bias_grad")
+            k.gemm(self.dZ[l], self.W16T[l], Bp, N_HID, N_HID, N_HID, N_HID, EPI_SILU_BACK, 128, Zin=self.Z[l - 1],
+                   H=self.dZ[l - 1], HT=self.dZT[l - 1], ldc=N_HID, ldt=self.max_batch)
+        # First layer.
+        self._weight_grad(self.dZT[0], self.XT16, N_HID, PAD_IN, Bp, self.gW[0])
+        _native.check(k.lib.xd_bias_grad(Bp, N_HID, _p(self.dZT[0]), self.max_batch, _p(self.gb[0]), k.stream()),
+                      "xd_bias_grad")
+
+    def adam_step(self, cfg: AdamConfig):
+        k = self.k
+        self.step_count += 1
+        t = self.step_count
+        a = _native.XdAdamArgs(cfg.lr, cfg.beta1, cfg.beta2, cfg.eps, 1 - cfg.beta1 ** t, 1 - cfg.beta2 ** t)
+        for l in range(N_LAYERS + 1):
+            ro, ri = self.pads[l]
+            _native.check(k.lib.xd_adam(ro, ri, _p(self.W[l]), _p(self.gW[l]), _p(self.mW[l]), _p(self.vW[l]),
+                                        ctypes.byref(a), _p(self.W16[l]), _p(self.W16T[l]), ri, ro, k.stream()),
+                          "xd_adam")
+            _native.check(k.lib.xd_adam(1, ro, _p(self.b[l]), _p(self.gb[l]), _p(self.mb[l]), _p(self.vb[l]),
+                                        ctypes.byref(a), None, None, 0, 0, k.stream()), "xd_adam")
+        # Keep the padding of the first and last layers exactly zero.
+        self.W[0][:, N_IN:].zero_()
+        self.W16[0][:, N_IN:].zero_()
+        self.W16T[0][N_IN:, :].zero_()
+        self.W[N_LAYERS][N_OUT:, :].zero_()
+        self.W16[N_LAYERS][N_OUT:, :].zero_()
+        self.W16T[N_LAYERS][:, N_OUT:].zero_()
+        self.b[N_LAYERS][N_OUT:].zero_()
+
+    def train_step(self, X, T, cfg: AdamConfig):
+        """One Adam step on a batch (X [n, 5], T [n, 10] in scaled space); returns the loss tensor."""
+        torch = self.torch
+        n, Bp = self._load_inputs(X)
+        self.T[:n] = torch.as_tensor(T, dtype=torch.float32, device=self.dev)
+        self._forward(Bp)
+        self.backward(n, Bp)
+        self.adam_step(cfg)
+        return self.sq[:n].mean() / N_OUT
+
+    def parameters_numpy(self):
+        """(W, b) per layer as float64 arrays, unpadded, of the BF16 weights the kernels use and the
+        FP32 biases."""
+        out = []
+        for l, (o, i) in enumerate(self.dims):
+            out.append((self.W16[l].float()[:o, :i].double().cpu().numpy(), self.b[l][:o].double().cpu().numpy()))
+        return out

@@ -138,6 +138,14 @@ int xd_load_assign(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, doub
                    double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,
                    double *d_dqdx_vals, void *stream);
 
+/* Assembles vector stamps computed outside the library (by the learned surrogate, for instance):
+ * d_stage16 holds 16 x n_inst doubles in the layout of the first 16 slots of xd_copy_stamps (F, Q,
+ * dFdxdVp, dQdxdVp at D, G, S, B), summed into the four vectors through the family's gather map
+ * with the same order and determinism as xd_load_vectors; assign != 0 stores instead of adding.
+ * No counterpart in the reference. */
+int xd_load_vectors_staged(xd_ctx *ctx, const double *d_stage16, double *d_f, double *d_q, double *d_dfdxdvp,
+                           double *d_dqdxdvp, int assign, void *stream);
+
 /* Test and error-bound support: like the two load calls, but adds |term| instead of term, so the
  * outputs hold, per entry, the sum of absolute contributions (the scale of the rounding error of
  * that entry's sum). */

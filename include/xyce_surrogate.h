@@ -42,6 +42,16 @@ typedef struct xd_gemm_args {
  * K slices actually used (>= 1) or < 0. */
 int xd_gemm_bf16(const xd_gemm_args *args, int splits, void *stream);
 
+/* First layer in FP32 (CUDA cores), so that the inputs keep full precision: for each of the M
+ * rows of x [M x ldx] (n_in <= 8 used columns) and each hidden unit u < n_hid (<= 1024),
+ * z = w1[u] . x + b1[u] (w1 row stride ldw); Z, H = silu(z) BF16 [M x n_hid], HT [n_hid x ldt]. */
+int xd_mlp_input_layer(int M, int n_in, int n_hid, const float *d_x, int ldx, const float *d_w1, int ldw,
+                       const float *d_b1, void *d_z, void *d_h, void *d_ht, int ldt, void *stream);
+
+/* Its weight gradient: gw[u][i] = sum_{r < M} dzt[u][r] x[r][i] (FP32, fixed tree). */
+int xd_mlp_input_grad(int M, int n_in, int n_hid, const void *d_dzt, int ldt, const float *d_x, int ldx,
+                      float *d_gw, int ldw, void *stream);
+
 /* d = scale * (y - target) for the first n_out of ld columns (0 in the padding), as BF16 in
  * d_dz [M x ld] and transposed in d_dzt [ld x ldt]; per-sample squared error into d_sq (or null). */
 int xd_mse_grad(int M, int n_out, int ld, const float *d_y, const float *d_target, float scale, void *d_dz,
@@ -55,6 +65,20 @@ int xd_splitk_sum(int n, int splits, const float *d_part, float *d_out, void *st
 
 /* out[c] = sum_{r < rows} in[r * ld + c] (FP32, fixed tree). */
 int xd_column_sum(int rows, int cols, const float *d_in, int ld, float *d_out, void *stream);
+
+/* Surrogate inputs of circuit instances idx[k] (k < n): from the solution d_sol and the
+ * instances' terminal unknowns d_nodes4 [n_inst x 4] (D, G, S, B; -1 = ground), x[k] =
+ * ((VG - VS) / vmax, (VD - VS) / vmax, (VB - VS) / vmax, geom2[2i], geom2[2i + 1]) (FP32, row
+ * stride ldx >= 5); geom2 holds each instance's scaled log W and log L. */
+int xd_surrogate_features(int n, const int *d_idx, const int *d_nodes4, const double *d_sol, const float *d_geom2,
+                          float vmax, float *d_x, int ldx, void *stream);
+
+/* Decodes outputs y[k] (row stride ldy; value = sinh(y) * out_scale[j] for j = Id, Qg, Qd, Qb)
+ * of instances idx[k] and writes their terminal currents and charges into a staged array
+ * [16 x n_inst] in the exact load's slot layout (F at D, G, S, B; Q at D, G, S, B; limiter slots
+ * zero), ready for xd_load_vectors_staged. */
+int xd_surrogate_stage(int n, const int *d_idx, const float *d_y, int ldy, const float *d_out_scale, int n_inst,
+                       double *d_stage, void *stream);
 
 typedef struct xd_adam_args {
   float lr, beta1, beta2, eps, bias_corr1, bias_corr2; /* bias_corr = 1 - beta^t */

@@ -77,7 +77,7 @@ def test_network_gradients_match_cpu_reference():
     n = 1000
     X = rng.uniform(-1, 1, (n, S.N_IN))
     T = rng.standard_normal((n, S.N_OUT))
-    Xq = _np(_bf(X))  # the inputs as the kernels see them
+    Xq = X.astype(np.float32).astype(np.float64)  # the inputs as the kernels see them (FP32)
     Bp = 1024
     net._load_inputs(X)
     net.T[:n] = torch.as_tensor(T, dtype=torch.float32, device="cuda")

@@ -758,6 +758,17 @@ int xd_load_assign(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, doub
   return load_matrices_impl(ctx, d_dfdx_vals, d_dqdx_vals, false, (cudaStream_t)stream, 1);
 }
 
+int xd_load_vectors_staged(xd_ctx *ctx, const double *d_stage16, double *d_f, double *d_q, double *d_dfdxdvp,
+                           double *d_dqdxdvp, int assign, void *stream) {
+  if (!ctx) return fail(-1, "null context");
+  if (ctx->n == 0) return 0;
+  if (!d_stage16) return fail(-1, "null staged array");
+  DeviceGuard g(ctx->device);
+  const size_t n = (size_t)ctx->n;
+  OutSet<4, false> os{{d_f, d_q, d_dfdxdvp, d_dqdxdvp}, {0, 4 * n, 8 * n, 12 * n}, assign ? 1 : 0};
+  return run_gather(ctx->vmap, d_stage16, os, (cudaStream_t)stream);
+}
+
 int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals,
                 double *d_dqdx_vals, void *stream) {
   if (!ctx) return fail(-1, "null context");

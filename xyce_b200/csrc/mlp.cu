@@ -381,6 +381,99 @@ __global__ void adam_kernel(int rows, int cols, float *__restrict__ p, const flo
   if (p16t) p16t[(size_t)c * ld16t + r] = __float2bfloat16(pi);
 }
 
+// First layer in FP32 on the CUDA cores: the network inputs (biases in volts, log-geometry) keep
+// full precision, which BF16 (8-bit mantissa, ~4 mV at 1 V) would not give them. One thread per
+// (sample, hidden unit): z = W1[u] . x + b1[u]; writes Z, H = silu(z) (BF16) and H transposed.
+__global__ void input_layer_kernel(int M, int n_in, int n_hid, const float *__restrict__ x, int ldx,
+                                   const float *__restrict__ w1, int ldw, const float *__restrict__ b1,
+                                   __nv_bfloat16 *__restrict__ Z, __nv_bfloat16 *__restrict__ H,
+                                   __nv_bfloat16 *__restrict__ HT, int ldt) {
+  const int u = threadIdx.x;  // hidden unit
+  const int row = blockIdx.x;
+  if (u >= n_hid || row >= M) return;
+  float z = b1[u];
+  for (int i = 0; i < n_in; ++i) z += w1[u * ldw + i] * x[(size_t)row * ldx + i];
+  const float h = silu(z);
+  Z[(size_t)row * n_hid + u] = __float2bfloat16(z);
+  H[(size_t)row * n_hid + u] = __float2bfloat16(h);
+  if (HT) HT[(size_t)u * ldt + row] = __float2bfloat16(h);
+}
+
+// First-layer weight gradient in FP32: gw[u][i] = sum_r dzt[u][r] * x[r][i] for i < n_in, one
+// block per hidden unit, fixed reduction tree.
+__global__ void input_grad_kernel(int M, int n_in, const __nv_bfloat16 *__restrict__ dzt, int ldt,
+                                  const float *__restrict__ x, int ldx, float *__restrict__ gw, int ldw) {
+  __shared__ float red[8][256];
+  const int u = blockIdx.x;
+  float acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i] = 0.0f;
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    const float d = __bfloat162float(dzt[(size_t)u * ldt + r]);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (i < n_in) acc[i] += d * x[(size_t)r * ldx + i];
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) red[i][threadIdx.x] = acc[i];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < n_in) gw[u * ldw + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Surrogate inputs for circuit instances idx[k]: terminal voltages from the solution (ground ->
+// 0), differences to the source, scaled by 1 / vmax, then the instance's scaled log W and log L.
+__global__ void surrogate_features_kernel(int n, const int *__restrict__ idx, const int *__restrict__ nodes4,
+                                          const double *__restrict__ sol, const float *__restrict__ geom2,
+                                          float inv_vmax, float *__restrict__ x, int ldx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = idx[k];
+  double v[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int nd = nodes4[4 * i + t];
+    v[t] = nd >= 0 ? sol[nd] : 0.0;
+  }
+  x[(size_t)k * ldx + 0] = (float)((v[1] - v[2]) * inv_vmax);  // Vgs
+  x[(size_t)k * ldx + 1] = (float)((v[0] - v[2]) * inv_vmax);  // Vds
+  x[(size_t)k * ldx + 2] = (float)((v[3] - v[2]) * inv_vmax);  // Vbs
+  x[(size_t)k * ldx + 3] = geom2[2 * i];
+  x[(size_t)k * ldx + 4] = geom2[2 * i + 1];
+}
+
+// Decodes the surrogate's outputs y = asinh(value / scale) for instances idx[k] and stages the
+// terminal currents and charges in the exact load's slot layout (slot-major, 16 x n_inst):
+// F = (Id, 0, -Id, 0) at (D, G, S, B), Q = (Qd, Qg, -(Qg + Qd + Qb), Qb), limiter slots zero.
+__global__ void surrogate_stage_kernel(int n, const int *__restrict__ idx, const float *__restrict__ y, int ldy,
+                                       const float *__restrict__ out_scale, int n_inst, double *__restrict__ stage) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = idx[k];
+  const float *yr = y + (size_t)k * ldy;
+  const double id = sinh((double)yr[0]) * out_scale[0];
+  const double qg = sinh((double)yr[1]) * out_scale[1];
+  const double qd = sinh((double)yr[2]) * out_scale[2];
+  const double qb = sinh((double)yr[3]) * out_scale[3];
+  const size_t N = (size_t)n_inst;
+  stage[0 * N + i] = id;
+  stage[1 * N + i] = 0.0;
+  stage[2 * N + i] = -id;
+  stage[3 * N + i] = 0.0;
+  stage[4 * N + i] = qd;
+  stage[5 * N + i] = qg;
+  stage[6 * N + i] = -(qg + qd + qb);
+  stage[7 * N + i] = qb;
+#pragma unroll
+  for (int s = 8; s < 16; ++s) stage[s * N + i] = 0.0;
+}
+
 int cuda_err(cudaError_t e, const char *where) {
   return xd_internal_fail(-3, std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
 }
@@ -413,6 +506,49 @@ int xd_gemm_bf16(const xd_gemm_args *g, int splits, void *stream) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "gemm_bf16_tc_kernel launch");
   return used;
+}
+
+int xd_mlp_input_layer(int M, int n_in, int n_hid, const float *d_x, int ldx, const float *d_w1, int ldw,
+                       const float *d_b1, void *d_z, void *d_h, void *d_ht, int ldt, void *stream) {
+  if (M <= 0 || n_in <= 0 || n_in > 8 || n_hid <= 0 || n_hid > 1024 || !d_x || !d_w1 || !d_b1 || !d_z || !d_h)
+    return xd_internal_fail(-1, "bad input-layer arguments");
+  input_layer_kernel<<<M, n_hid, 0, (cudaStream_t)stream>>>(M, n_in, n_hid, d_x, ldx, d_w1, ldw, d_b1,
+                                                            (__nv_bfloat16 *)d_z, (__nv_bfloat16 *)d_h,
+                                                            (__nv_bfloat16 *)d_ht, ldt);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_err(e, "input_layer_kernel");
+}
+
+int xd_mlp_input_grad(int M, int n_in, int n_hid, const void *d_dzt, int ldt, const float *d_x, int ldx,
+                      float *d_gw, int ldw, void *stream) {
+  if (M <= 0 || n_in <= 0 || n_in > 8 || n_hid <= 0 || !d_dzt || !d_x || !d_gw)
+    return xd_internal_fail(-1, "bad input-grad arguments");
+  input_grad_kernel<<<n_hid, 256, 0, (cudaStream_t)stream>>>(M, n_in, (const __nv_bfloat16 *)d_dzt, ldt, d_x, ldx,
+                                                             d_gw, ldw);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_err(e, "input_grad_kernel");
+}
+
+int xd_surrogate_features(int n, const int *d_idx, const int *d_nodes4, const double *d_sol, const float *d_geom2,
+                          float vmax, float *d_x, int ldx, void *stream) {
+  if (n < 0 || (n > 0 && (!d_idx || !d_nodes4 || !d_sol || !d_geom2 || !d_x)) || ldx < 5 || vmax <= 0.0f)
+    return xd_internal_fail(-1, "bad surrogate-feature arguments");
+  if (n == 0) return 0;
+  surrogate_features_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(n, d_idx, d_nodes4, d_sol, d_geom2,
+                                                                               1.0f / vmax, d_x, ldx);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_err(e, "surrogate_features_kernel");
+}
+
+int xd_surrogate_stage(int n, const int *d_idx, const float *d_y, int ldy, const float *d_out_scale, int n_inst,
+                       double *d_stage, void *stream) {
+  if (n < 0 || (n > 0 && (!d_idx || !d_y || !d_out_scale || !d_stage)) || ldy < 4 || n_inst < n)
+    return xd_internal_fail(-1, "bad surrogate-stage arguments");
+  if (n == 0) return 0;
+  surrogate_stage_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(n, d_idx, d_y, ldy, d_out_scale, n_inst,
+                                                                            d_stage);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_err(e, "surrogate_stage_kernel");
 }
 
 int xd_mse_grad(int M, int n_out, int ld, const float *d_y, const float *d_target, float scale, void *d_dz,

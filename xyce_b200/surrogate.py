@@ -7,10 +7,13 @@ gmb = dId/dVbs, Cgg = dQg/dVgs, Cgd = dQg/dVds, Cgb = dQg/dVbs. Outputs are lear
 compressed scale, y = asinh(x / s) per output, so that relative accuracy holds across the many
 decades a MOSFET current spans.
 
-Weights are BF16 for the matrix products (FP32 master copies and Adam moments), accumulation is
-FP32. Every product runs in ``xd_gemm_bf16`` (tcgen05 tensor cores, include/xyce_surrogate.h) with
-the bias / SiLU / SiLU-derivative work fused into its epilogue; the loss gradient, bias gradients,
-split-K reductions and the Adam update are the library's own kernels as well. torch only owns the
+Weights of the 128-wide layers are BF16 for the matrix products (FP32 master copies and Adam
+moments), accumulation is FP32; those products run in ``xd_gemm_bf16`` (tcgen05 tensor cores,
+include/xyce_surrogate.h) with the bias / SiLU / SiLU-derivative work fused into the epilogue. The
+first layer (5 -> 128, 0.5% of the FLOPs) runs in FP32 on the CUDA cores so that the bias inputs
+keep full precision (BF16 would round 1 V to ~4 mV, a 10% step of a subthreshold current). The
+loss gradient, bias gradients, split-K reductions and the Adam update are the library's own
+kernels as well. torch only owns the
 buffers and orders the calls on a stream.
 
 Shapes are padded for the tensor cores: inputs to 16 columns (K of the first layer), outputs to 16
@@ -132,8 +135,7 @@ class SurrogateMLP:
         self.max_batch = B
         bf = dict(dtype=torch.bfloat16, device=self.dev)
         f32 = dict(dtype=torch.float32, device=self.dev)
-        self.X16 = torch.zeros(B, PAD_IN, **bf)
-        self.XT16 = torch.zeros(PAD_IN, B, **bf)
+        self.X32 = torch.zeros(B, PAD_IN, **f32)
         self.Z = [torch.zeros(B, N_HID, **bf) for _ in range(N_LAYERS)]
         self.H = [torch.zeros(B, N_HID, **bf) for _ in range(N_LAYERS)]
         self.HT = [torch.zeros(N_HID, B, **bf) for _ in range(N_LAYERS)]
@@ -157,10 +159,9 @@ class SurrogateMLP:
         if Bp > self.max_batch:
             self._alloc(Bp)
         x = torch.as_tensor(X, dtype=torch.float32, device=self.dev)
-        self.X16.zero_()
-        self.X16[:n, :N_IN] = x.to(torch.bfloat16)
-        self.XT16.zero_()
-        self.XT16[:N_IN, :n] = x.t().to(torch.bfloat16)
+        self.X32[:n, :N_IN] = x
+        if Bp > n:
+            self.X32[n:Bp].zero_()
         return n, Bp
 
     def forward(self, X):
@@ -171,8 +172,11 @@ class SurrogateMLP:
 
     def _forward(self, Bp):
         k = self.k
-        A, lda = self.X16, PAD_IN
-        for l in range(N_LAYERS):
+        _native.check(k.lib.xd_mlp_input_layer(Bp, N_IN, N_HID, _p(self.X32), PAD_IN, _p(self.W[0]), PAD_IN,
+                                               _p(self.b[0]), _p(self.Z[0]), _p(self.H[0]), _p(self.HT[0]),
+                                               self.max_batch, k.stream()), "xd_mlp_input_layer")
+        A, lda = self.H[0], N_HID
+        for l in range(1, N_LAYERS):
             k.gemm(A, self.W16[l], Bp, N_HID, lda, lda, lda, EPI_BIAS_SILU, 128, bias=self.b[l], Z=self.Z[l],
                    H=self.H[l], HT=self.HT[l], ldc=N_HID, ldt=self.max_batch)
             A, lda = self.H[l], N_HID
@@ -214,8 +218,9 @@ class SurrogateMLP:
                           "xd_bias_grad")
             k.gemm(self.dZ[l], self.W16T[l], Bp, N_HID, N_HID, N_HID, N_HID, EPI_SILU_BACK, 128, Zin=self.Z[l - 1],
                    H=self.dZ[l - 1], HT=self.dZT[l - 1], ldc=N_HID, ldt=self.max_batch)
-        # First layer.
-        self._weight_grad(self.dZT[0], self.XT16, N_HID, PAD_IN, Bp, self.gW[0])
+        # First layer (FP32 on the CUDA cores).
+        _native.check(k.lib.xd_mlp_input_grad(Bp, N_IN, N_HID, _p(self.dZT[0]), self.max_batch, _p(self.X32), PAD_IN,
+                                              _p(self.gW[0]), PAD_IN, k.stream()), "xd_mlp_input_grad")
         _native.check(k.lib.xd_bias_grad(Bp, N_HID, _p(self.dZT[0]), self.max_batch, _p(self.gb[0]), k.stream()),
                       "xd_bias_grad")
 
@@ -251,9 +256,169 @@ class SurrogateMLP:
         return self.sq[:n].mean() / N_OUT
 
     def parameters_numpy(self):
-        """(W, b) per layer as float64 arrays, unpadded, of the BF16 weights the kernels use and the
-        FP32 biases."""
+        """(W, b) per layer as float64 arrays, unpadded: the FP32 first layer, the BF16 weights the
+        tensor-core layers use, and the FP32 biases."""
         out = []
         for l, (o, i) in enumerate(self.dims):
-            out.append((self.W16[l].float()[:o, :i].double().cpu().numpy(), self.b[l][:o].double().cpu().numpy()))
+            w = self.W[0] if l == 0 else self.W16[l].float()
+            out.append((w[:o, :i].double().cpu().numpy(), self.b[l][:o].double().cpu().numpy()))
         return out
+
+
+# ---- training data from the FP64 BSIM4 kernel, and the two-network surrogate ---------------------
+
+# Staged-slot indices (xd_copy_stamps layout) of the ten targets, per instance with the source
+# grounded: F at D; Q at G, D, B; dF_D/dV_G, dF_D/dV_D, dF_D/dV_B; dQ_G/dV_G, dQ_G/dV_D, dQ_G/dV_B.
+_TARGET_SLOTS = (0, 4 + 1, 4 + 0, 4 + 3, 16 + 1, 16 + 0, 16 + 3, 32 + 5, 32 + 4, 32 + 7)
+
+
+def bsim4_samples(n, pmos, seed=0, card=None, n_geom=1024, device=0, chunk=1 << 20):
+    """n samples of the FP64 BSIM4 load (this package's kernel) at biases uniform in |V| <= 1.2 V
+    and geometries uniform in L 30-500 nm, W 0.1-10 um (n_geom distinct (L, W) pairs, each
+    instance drawing one). Returns (features [n, 5] float32, targets [n, 10] float64)."""
+    import torch
+
+    from .device import Bsim4Device, ModelCard, SolverFlags
+
+    rng = np.random.default_rng(seed)
+    gl = rng.uniform(30e-9, 500e-9, n_geom)
+    gw = rng.uniform(0.1e-6, 10e-6, n_geom)
+    Xs, Ys = [], []
+    done = 0
+    dev = None
+    while done < n:
+        m = min(chunk, n - done)
+        if dev is None or dev.n != m:
+            if dev is not None:
+                dev.close()
+            geo = rng.integers(0, n_geom, m)
+            nodes = np.stack([3 * np.arange(m), 3 * np.arange(m) + 1, -np.ones(m, np.int64), 3 * np.arange(m) + 2], 1)
+            rowptr = np.arange(0, 9 * m + 1, 3, dtype=np.int32)
+            colind = (np.repeat(3 * np.arange(m), 9) + np.tile([0, 1, 2], 3 * m)).astype(np.int32)
+            dev = Bsim4Device([card or ModelCard(pmos, {})], np.zeros(m, np.int32), nodes,
+                              {"L": gl[geo], "W": gw[geo]}, (rowptr, colind), 3 * m, device=device)
+            geo_l, geo_w = gl[geo], gw[geo]
+        v = rng.uniform(-VMAX, VMAX, (m, 3))  # Vds, Vgs, Vbs with the source at ground
+        sol = torch.as_tensor(v.reshape(-1), dtype=torch.float64, device=f"cuda:{device}")
+        z = lambda k: torch.zeros(k, dtype=torch.float64, device=f"cuda:{device}")
+        nsta, nsto = z(dev.n_state), z(dev.n_store)
+        f, q, fx, qx = z(3 * m), z(3 * m), z(3 * m), z(3 * m)
+        jf, jq = z(dev.nnz), z(dev.nnz)
+        dev.load(SolverFlags(newton_iter=1, voltlim=0), sol, nsta, z(dev.n_state), nsto, z(dev.n_store), f, q, fx, qx,
+                 jf, jq)
+        st = dev.copy_stamps()
+        Ys.append(st[list(_TARGET_SLOTS)].T.copy())
+        Xs.append(features(v[:, 1], v[:, 0], v[:, 2], geo_w, geo_l).astype(np.float32))
+        done += m
+    if dev is not None:
+        dev.close()
+    return np.concatenate(Xs), np.concatenate(Ys)
+
+
+def error_report(pred, ref):
+    """Per output, over the samples whose reference magnitude is at least 1% of the output's RMS:
+    median and 95th percentile of the relative error |pred - ref| / |ref|, and the fraction of all
+    samples in that set."""
+    out = {}
+    for k, name in enumerate(OUTPUT_NAMES):
+        rms = np.sqrt(np.mean(ref[:, k] ** 2)) or 1.0
+        sel = np.abs(ref[:, k]) >= 0.01 * rms
+        e = np.abs(pred[sel, k] - ref[sel, k]) / np.abs(ref[sel, k])
+        out[name] = {"rel_median": float(np.median(e)), "rel_p95": float(np.quantile(e, 0.95)),
+                     "fraction": float(sel.mean())}
+    return out
+
+
+class BsimSurrogate:
+    """The NMOS and PMOS networks of the BSIM4 surrogate, trained on FP64 kernel samples."""
+
+    def __init__(self, device=0, seed=0):
+        self.device = device
+        self.nets = {False: SurrogateMLP(device, seed=seed), True: SurrogateMLP(device, seed=seed + 1)}
+        self.history = {False: [], True: []}
+
+    def train(self, n_samples=10_000_000, epochs=8, batch=16384, lr=3e-3, lr_end=5e-5, seed=0, log=None):
+        """Trains each type on n_samples FP64 samples; returns the held-out error report per type."""
+        import torch
+
+        reports = {}
+        for pmos in (False, True):
+            X, Y = bsim4_samples(n_samples + 200_000, pmos, seed=seed + (7 if pmos else 0), device=self.device)
+            Xv, Yv = X[-200_000:], Y[-200_000:]
+            X, Y = X[:-200_000], Y[:-200_000]
+            T = encode_targets(Y).astype(np.float32)
+            net = self.nets[pmos]
+            Xd = torch.as_tensor(X, device=net.dev)
+            Td = torch.as_tensor(T, device=net.dev)
+            steps = epochs * (len(X) // batch)
+            g = torch.Generator(device=net.dev).manual_seed(seed)
+            s = 0
+            for ep in range(epochs):
+                perm = torch.randperm(len(X), device=net.dev, generator=g)
+                for i in range(len(X) // batch):
+                    idx = perm[i * batch:(i + 1) * batch]
+                    cur = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * s / max(1, steps)))
+                    loss = net.train_step(Xd[idx], Td[idx], AdamConfig(lr=cur))
+                    s += 1
+                    if i % 200 == 0:
+                        self.history[pmos].append((s, float(loss)))
+                        if log:
+                            log(f"{'pmos' if pmos else 'nmos'} epoch {ep} step {s}/{steps} loss {float(loss):.4g}")
+            net.k.check_err()
+            pred = self.predict_physical(pmos, Xv)
+            reports["pmos" if pmos else "nmos"] = error_report(pred, Yv)
+        return reports
+
+    def predict_physical(self, pmos, X, batch=262144):
+        out = []
+        net = self.nets[pmos]
+        for i in range(0, len(X), batch):
+            out.append(net.forward(X[i:i + batch]).double().cpu().numpy())
+        return decode_outputs(np.concatenate(out))
+
+
+class SurrogateLoads:
+    """Vector loads (F, Q) of a circuit's BSIM4 family from the trained surrogate, on the GPU:
+    inputs built from the solution by ``xd_surrogate_features``, both networks' forward passes,
+    outputs decoded and staged by ``xd_surrogate_stage`` and assembled through the family's own
+    gather map by ``xd_load_vectors_staged`` (stored, not added)."""
+
+    def __init__(self, sur: BsimSurrogate, family, mos_type, mos_nodes, w, l):
+        import torch
+
+        self.torch = torch
+        self.sur = sur
+        self.fam = family
+        self.dev = sur.nets[False].dev
+        self.lib = _native.load()
+        n = len(mos_type)
+        self.n = n
+        T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.dev)
+        self.nodes4 = T(np.asarray(mos_nodes, np.int32).reshape(-1), torch.int32)
+        f = features(np.zeros(n), np.zeros(n), np.zeros(n), np.asarray(w, float), np.asarray(l, float))
+        self.geom2 = T(f[:, 3:5].astype(np.float32).reshape(-1), torch.float32)
+        self.idx = {p: T(np.nonzero(np.asarray(mos_type) == (1 if p else 0))[0].astype(np.int32), torch.int32)
+                    for p in (False, True)}
+        self.out_scale = T(OUTPUT_SCALE.astype(np.float32), torch.float32)
+        self.stage = torch.zeros(16 * n, dtype=torch.float64, device=self.dev)
+        for p in (False, True):
+            m = int(self.idx[p].shape[0])
+            net = sur.nets[p]
+            if m > net.max_batch:
+                net._alloc(m)
+
+    def load(self, x, f, q, fx, qx, stream):
+        for p in (False, True):
+            m = int(self.idx[p].shape[0])
+            if m == 0:
+                continue
+            net = self.sur.nets[p]
+            Bp = (m + 127) // 128 * 128
+            _native.check(self.lib.xd_surrogate_features(m, _p(self.idx[p]), _p(self.nodes4), _p(x), _p(self.geom2),
+                                                         ctypes.c_float(VMAX), _p(net.X32), PAD_IN, stream),
+                          "xd_surrogate_features")
+            net._forward(Bp)
+            _native.check(self.lib.xd_surrogate_stage(m, _p(self.idx[p]), _p(net.Y), PAD_OUT, _p(self.out_scale),
+                                                      self.n, _p(self.stage), stream), "xd_surrogate_stage")
+        _native.check(self.lib.xd_load_vectors_staged(self.fam._h, _p(self.stage), _p(f), _p(q), _p(fx), _p(qx), 1,
+                                                      stream), "xd_load_vectors_staged")

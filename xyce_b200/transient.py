@@ -133,6 +133,10 @@ class StepStats:
     failed_steps: int = 0
     wall_s: float = 0.0
     loads: int = 0
+    factorizations: int = 0
+    surrogate_loads: int = 0
+    chord_iters: list = field(default_factory=list)
+    surrogate_error: list = field(default_factory=list)
 
 
 class TransientBase:
@@ -189,16 +193,58 @@ class TransientBase:
     def _sync(self):
         pass
 
+    # -- learned warm start ------------------------------------------------------------------------
+    surrogate = None  # set to an object with load(x, f, q, fx, qx, stream) to enable the warm start
+    chord_max = 3
+    chord_tol = 1e-4
+
+    def _surrogate_load(self):
+        raise NotImplementedError
+
+    def _surrogate_warm_start(self, h, order, qn0, fhist):
+        """Chord iterations on the surrogate's device loads: residual from the surrogate's currents
+        and charges (linear devices exact), matrix = the last exact factorization. Moves self.x
+        towards the solution before the exact FP64 Newton iterations take over; the exact loads
+        always make the final, converged evaluation."""
+        lim = self.limiting
+        self.limiting = False  # the surrogate has no limiter corrections
+        n_it = 0
+        try:
+            for _ in range(self.chord_max):
+                self._surrogate_load()
+                self._combine(1, h, order, qn0, fhist)
+                dx = self._solve_factored()
+                self.x += dx
+                n_it += 1
+                if float(dx.abs().max()) <= self.chord_tol:
+                    break
+        finally:
+            self.limiting = lim
+        self.stats.chord_iters.append(n_it)
+        self.stats.surrogate_loads += n_it
+
     def _solve(self):
+        """Factors the current Newton matrix (kept for chord iterations) and solves with rhs."""
         torch = self.torch
         if self.solver == "dense":
             self._dense.zero_()
             self._dense[self._flat] = self.jac
-            return torch.linalg.solve(self._dense.view(self.nu, self.nu), self.rhs)
-        import scipy.sparse as sp
-        import scipy.sparse.linalg as spl
-        J = sp.csr_matrix((self.jac.cpu().numpy(), self.colind, self.rowptr), shape=(self.nu, self.nu))
-        dx = spl.splu(J.tocsc()).solve(self.rhs.cpu().numpy())
+            self._lu = torch.linalg.lu_factor(self._dense.view(self.nu, self.nu))
+        else:
+            import scipy.sparse as sp
+            import scipy.sparse.linalg as spl
+            J = sp.csr_matrix((self.jac.cpu().numpy(), self.colind, self.rowptr), shape=(self.nu, self.nu))
+            self._lu = spl.splu(J.tocsc())
+        self.stats.factorizations += 1
+        return self._solve_factored()
+
+    def _solve_factored(self):
+        """Solves with the last factorization (a chord step when the matrix has moved on)."""
+        torch = self.torch
+        if self.solver == "dense":
+            LU, piv = self._lu
+            return torch.linalg.lu_solve(LU, piv, self.rhs.view(-1, 1)).view(-1)
+        dx = self._lu.solve(self.rhs.cpu().numpy())
         return torch.as_tensor(dx, device=self.dev)
 
     def _newton(self, prm: NewtonParams, flags_for_iter, mode, h=None, order=1, qn0=None, fhist=None):
@@ -320,6 +366,8 @@ class TransientBase:
                 self.x.copy_(warm_start(t, h, x_n, x_nm1))
             else:
                 self.x.copy_(x_n)
+            if self.surrogate is not None and not first and getattr(self, "_lu", None) is not None:
+                self._surrogate_warm_start(h, order, qn0, fhist)
 
             def flags(it, first=first, h=h):
                 return SolverFlags(transient=1, newton_iter=it, init_tran=1 if first else 0, pdt=1.0 / h,
@@ -406,6 +454,9 @@ class GpuTransient(TransientBase):
                                                p(self.q), p(self.fx), p(self.qx), p(self.jf), p(self.jq),
                                                self._stream()), "xd_load_assign")
         self.stats.loads += 1
+
+    def _surrogate_load(self):
+        self.surrogate.load(self.x, self.f, self.q, self.fx, self.qx, self._stream())
 
     def _combine(self, mode, h=None, order=1, qn0=None, fhist=None):
         coef = tia_coef(mode, h, order, self.gshunt)

@@ -111,3 +111,37 @@ def test_training_reduces_loss():
     torch.cuda.synchronize()
     net.k.check_err()
     assert losses[-1] < 0.05 * losses[0], (losses[0], losses[-1])
+
+
+def test_bsim4_surrogate_trains_on_fp64_samples_and_warm_start_keeps_exact_answer():
+    """FP64 kernel samples -> tensor-core training -> held-out error vs FP64; then a transient of a
+    BSIM4 gate netlist with and without the surrogate warm start: the exact FP64 loads make the
+    converged evaluations, so the waveforms agree to the Newton tolerance."""
+    from tests.parity import family_inputs
+    from xyce_b200 import MosfetDevice, netlist
+    from xyce_b200.transient import GpuTransient, NewtonParams
+
+    sur = S.BsimSurrogate(seed=0)
+    rep = sur.train(n_samples=400_000, epochs=3, batch=16384)
+    for typ in ("nmos", "pmos"):
+        assert rep[typ]["Id"]["rel_median"] < 0.5, rep[typ]["Id"]
+    c = netlist.random_logic(300, seed=3, n_inputs=8)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, None)
+    tight = NewtonParams(max_iter=40, rhs_tol=1e-9, delta_x_tol=1e-3, abs_tol=1e-9, rel_tol=1e-6,
+                         update_weights_each_iter=False)
+    waves = []
+    for warm in (False, True):
+        fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
+        g = GpuTransient(c, fam, rowptr, colind)
+        g.predictor = "linear"
+        if warm:
+            g.surrogate = S.SurrogateLoads(sur, fam, c.mos_type, c.mos_nodes, c.mos_w, c.mos_l)
+        g.dcop()
+        _, w = g.run(0.3e-9, 10e-12, params=tight, record=np.arange(c.n_nodes))
+        if warm:
+            assert g.stats.surrogate_loads > 0
+        waves.append(w)
+        g.close()
+        fam.close()
+    assert np.abs(waves[0] - waves[1]).max() < 1e-9

@@ -32,8 +32,10 @@ from . import _native
 N_IN, N_HID, N_LAYERS, N_OUT = 5, 128, 4, 10
 PAD_IN, PAD_OUT = 16, 16
 OUTPUT_NAMES = ("Id", "Qg", "Qd", "Qb", "gm", "gds", "gmb", "Cgg", "Cgd", "Cgb")
-# Scale of each output inside asinh(x / s): about the smallest magnitude that still matters.
-OUTPUT_SCALE = np.array([1e-9, 1e-18, 1e-18, 1e-18, 1e-8, 1e-8, 1e-8, 1e-17, 1e-17, 1e-17])
+# Scale of each output inside asinh(x / s). Near the operating magnitudes rather than at the
+# smallest values: with a tiny scale the encoded value swings by ~20 within millivolts of a sign
+# change (Id at Vds = 0, the charges), a near-discontinuity the network cannot fit.
+OUTPUT_SCALE = np.array([1e-6, 1e-16, 1e-16, 1e-16, 1e-6, 1e-6, 1e-6, 1e-16, 1e-16, 1e-16])
 VMAX = 1.2
 LOG_W = (math.log(0.1e-6), math.log(10e-6))
 LOG_L = (math.log(30e-9), math.log(500e-9))
@@ -47,8 +49,14 @@ def features(vgs, vds, vbs, w, l):
                      sc(np.log(w), *LOG_W), sc(np.log(l), *LOG_L)], 1)
 
 
+# Encoded targets are clipped to +-ENC_CLIP: beyond it (|Id| > ~0.24 A, reached only by
+# forward-biased junctions deep in the sampling box) the exact value is of no use to a warm start,
+# and unclipped exponential tails would dominate the squared error.
+ENC_CLIP = 20.0
+
+
 def encode_targets(y):
-    return np.arcsinh(np.asarray(y) / OUTPUT_SCALE)
+    return np.clip(np.arcsinh(np.asarray(y) / OUTPUT_SCALE), -ENC_CLIP, ENC_CLIP)
 
 
 def decode_outputs(z):

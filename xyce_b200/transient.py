@@ -197,29 +197,69 @@ class TransientBase:
     surrogate = None  # set to an object with load(x, f, q, fx, qx, stream) to enable the warm start
     chord_max = 3
     chord_tol = 1e-4
+    chord_step_cap = 0.5  # volts
+    chord_monotone = True  # stop the chord iterations when the surrogate residual grows
+    predictor = "none"  # Newton start: "none" (the last point) or "linear" (extrapolation of the last two)
 
     def _surrogate_load(self):
         raise NotImplementedError
 
-    def _surrogate_warm_start(self, h, order, qn0, fhist):
-        """Chord iterations on the surrogate's device loads: residual from the surrogate's currents
-        and charges (linear devices exact), matrix = the last exact factorization. Moves self.x
-        towards the solution before the exact FP64 Newton iterations take over; the exact loads
-        always make the final, converged evaluation."""
+    def _anchor(self, f_sn, q_sn):
+        """f <- f_anchor + (f - f_sn), likewise q: anchored surrogate vectors."""
+        self.f.sub_(f_sn).add_(self.f_anchor)
+        self.q.sub_(q_sn).add_(self.q_anchor)
+
+    def _save_anchor(self):
+        """Exact MOSFET F and Q at the accepted point (the last load was there)."""
+        if self.surrogate is not None:
+            self.f_anchor = self.f.clone()
+            self.q_anchor = self.q.clone()
+
+    def _surrogate_warm_start(self, h, order, qn0, fhist, x_n):
+        """Chord iterations on anchored surrogate loads: the MOSFETs' F and Q at an iterate x are
+        the exact FP64 values at the last accepted point x_n plus the surrogate's change from x_n
+        to x, so the surrogate's level errors cancel and only its slope errors remain; the linear
+        devices are exact and the matrix is the last exact factorization. This moves self.x towards
+        the solution before the exact FP64 Newton iterations take over; the exact loads always make
+        the final, converged evaluation."""
         lim = self.limiting
         self.limiting = False  # the surrogate has no limiter corrections
         n_it = 0
+        x_start = self.x.clone()
+        self.x.copy_(x_n)
+        self._surrogate_load()
+        f_sn, q_sn = self.f.clone(), self.q.clone()
+        self.x.copy_(x_start)
+        best_x, best_r = self.x.clone(), math.inf
         try:
-            for _ in range(self.chord_max):
+            for _ in range(self.chord_max + 1):
                 self._surrogate_load()
+                self._anchor(f_sn, q_sn)
                 self._combine(1, h, order, qn0, fhist)
+                r = float(self.rhs.abs().max())
+                if not math.isfinite(r) or (self.chord_monotone and r >= best_r):
+                    break  # the surrogate residual stopped falling: keep the best iterate
+                if r < best_r or not self.chord_monotone:
+                    best_x.copy_(self.x)
+                    best_r = min(r, best_r)
+                if n_it == self.chord_max:
+                    break
                 dx = self._solve_factored()
+                step = float(dx.abs().max())
+                if not math.isfinite(step):
+                    break
+                if step > self.chord_step_cap:
+                    dx *= self.chord_step_cap / step
                 self.x += dx
                 n_it += 1
-                if float(dx.abs().max()) <= self.chord_tol:
+                if step <= self.chord_tol:
+                    best_x.copy_(self.x)
                     break
         finally:
             self.limiting = lim
+            self.x.copy_(best_x)
+            self.f.copy_(self.f_anchor)
+            self.q.copy_(self.q_anchor)
         self.stats.chord_iters.append(n_it)
         self.stats.surrogate_loads += n_it
 
@@ -229,7 +269,8 @@ class TransientBase:
         if self.solver == "dense":
             self._dense.zero_()
             self._dense[self._flat] = self.jac
-            self._lu = torch.linalg.lu_factor(self._dense.view(self.nu, self.nu))
+            LU, piv, _ = torch.linalg.lu_factor_ex(self._dense.view(self.nu, self.nu))
+            self._lu = (LU, piv)  # a singular matrix gives a non-finite step: a Newton failure
         else:
             import scipy.sparse as sp
             import scipy.sparse.linalg as spl
@@ -329,6 +370,7 @@ class TransientBase:
         """The accepted point's device history becomes the current one."""
         self.curr_sta.copy_(self.next_sta)
         self.curr_sto.copy_(self.next_sto)
+        self._save_anchor()
 
     def set_initial_state(self, x, t0: float = 0.0):
         """Starts the transient from x (an operating point with a kick, say): one load at x gives
@@ -355,6 +397,7 @@ class TransientBase:
         fhist = self.ftot.clone()
         x_n = self.x.clone()
         x_nm1 = None
+        h_prev = hmax
         times, waves = [0.0], [self.x[rec_t].cpu().numpy()]
         first = True
         t_start = _time.perf_counter()
@@ -364,10 +407,12 @@ class TransientBase:
             self._set_sources(t + h)
             if warm_start is not None:
                 self.x.copy_(warm_start(t, h, x_n, x_nm1))
+            elif x_nm1 is not None and self.predictor == "linear":
+                self.x.copy_(x_n + (x_n - x_nm1) * (h / h_prev))
             else:
                 self.x.copy_(x_n)
             if self.surrogate is not None and not first and getattr(self, "_lu", None) is not None:
-                self._surrogate_warm_start(h, order, qn0, fhist)
+                self._surrogate_warm_start(h, order, qn0, fhist, x_n)
 
             def flags(it, first=first, h=h):
                 return SolverFlags(transient=1, newton_iter=it, init_tran=1 if first else 0, pdt=1.0 / h,
@@ -390,6 +435,7 @@ class TransientBase:
             fhist.copy_(self.ftot)
             self._accept_point()
             x_nm1, x_n = x_n, self.x.clone()
+            h_prev = h
             self.stats.newton_iters.append(n_it)
             self.stats.times.append(t)
             times.append(t)

@@ -39,6 +39,89 @@ UNIT = "loads/s"
 # node indices (16), record index (4), 5 store values (40), vgb (8); writes 48 stamp values (384),
 # 12 store (96), 3 state (24), vgb (8).
 EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
+# DRAM bytes per instance of one evaluation launch (dram__bytes_read.sum + dram__bytes_write.sum
+# of an ncu capture at 199,832 instances of the same generator, 90 + 333 B; traffic grows with
+# the instance count), for roofline.traffic.
+EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 333
+
+
+def transient_section(args):
+    """Transient wall time per run, GPU path vs the oracle's loads through the same driver, and
+    the learned warm start against the plain GPU path (Newton iterations per step)."""
+    import torch
+
+    from tests.parity import family_inputs
+    from tests.transient_oracle import OracleTransient
+    from xyce_b200 import Bsim3Device, MosfetDevice, netlist, surrogate as S
+    from xyce_b200.transient import GpuTransient, NewtonParams
+
+    out = {}
+    # BSIM3 ring oscillator: operating point, 0.1 V kick on node 1, 0-20 ns at 10 ps steps.
+    c = netlist.inverter_ring(101, vdd=1.8)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards = netlist.ring_bsim3_cards()
+    fam = Bsim3Device(cards, c.mos_type, c.mos_nodes, {"L": c.mos_l, "W": c.mos_w}, (rowptr, colind),
+                      c.n_unknowns)
+    runs = {}
+    for name, mk in (("gpu", lambda: GpuTransient(c, fam, rowptr, colind)),
+                     ("cpu_oracle", lambda: OracleTransient(c, cards, rowptr, colind, level=9))):
+        tr = mk()
+        tr.dcop()
+        x0 = tr.x.clone()
+        x0[1] += 0.1
+        tr.set_initial_state(x0)
+        if name == "gpu":
+            torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, w = tr.run(20e-9, 10e-12, params=NewtonParams.transient(), record=[1, 51])
+        if name == "gpu":
+            torch.cuda.synchronize()
+        runs[name] = (time.perf_counter() - t0, tr.stats, w)
+    g_s, g_st, g_w = runs["gpu"]
+    c_s, c_st, _ = runs["cpu_oracle"]
+    out["ring_bsim3"] = {
+        "workload": "101-stage BSIM3 ring oscillator, W/L 1u/0.18u (PMOS 2u), VDD 1.8 V, 5 fF/stage, operating "
+                    "point + 0.1 V kick on node 1, 0-20 ns, 10 ps steps, reference transient Newton tolerances",
+        "gpu_s_per_run": g_s, "cpu_oracle_s_per_run": c_s, "cpu_cores": 1,
+        "gpu_newton_iters_per_step": float(np.mean(g_st.newton_iters)),
+        "cpu_newton_iters_per_step": float(np.mean(c_st.newton_iters)), "steps": len(g_st.newton_iters),
+        "node1_swing_v": [float(g_w[:, 0].min()), float(g_w[:, 0].max())]}
+    fam.close()
+    # Learned warm start on a BSIM4 gate netlist.
+    t0 = time.perf_counter()
+    sur = S.BsimSurrogate(seed=0)
+    rep = sur.train(n_samples=args.surrogate_samples // 2, epochs=8)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    c = netlist.random_logic(1200, seed=7, n_inputs=16)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, None)
+    res, waves = {}, {}
+    for mode in ("plain", "warm_start"):
+        fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
+        g = GpuTransient(c, fam, rowptr, colind)
+        g.predictor = "linear"
+        if mode == "warm_start":
+            g.surrogate = S.SurrogateLoads(sur, fam, c.mos_type, c.mos_nodes, c.mos_w, c.mos_l)
+        g.dcop()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, waves[mode] = g.run(1e-9, 10e-12, params=NewtonParams.transient(), record=np.arange(c.n_nodes))
+        torch.cuda.synchronize()
+        res[mode] = {"s_per_run": time.perf_counter() - t0,
+                     "exact_newton_iters_per_step": float(np.mean(g.stats.newton_iters)),
+                     "factorizations": g.stats.factorizations, "surrogate_loads": g.stats.surrogate_loads}
+        g.close()
+        fam.close()
+    out["warm_start_bsim4_gates"] = {
+        "workload": f"seeded INV/NAND2/NOR2 netlist, {c.n_mos} BSIM4 MOSFETs, RC wires, 16 PWL inputs, "
+                    f"{c.n_unknowns} unknowns, 0-1 ns at 10 ps, linear predictor on both paths",
+        "plain": res["plain"], "warm_start": res["warm_start"],
+        "max_waveform_difference_v": float(np.abs(waves["plain"] - waves["warm_start"]).max()),
+        "surrogate": {"train_s": train_s, "samples": 2 * (args.surrogate_samples // 2),
+                      "heldout_rel_error_median_p95": {t: {k: [round(v["rel_median"], 4), round(v["rel_p95"], 4)]
+                                                           for k, v in r.items()} for t, r in rep.items()}}}
+    return out
 
 
 def parse():
@@ -52,6 +135,8 @@ def parse():
     ap.add_argument("--wire-segments", type=int, default=4)
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-transient", action="store_true")
+    ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     return ap.parse_args()
 
 
@@ -364,8 +449,11 @@ def main():
                    "l2": "working set > 126 MB L2 (staging + maps + CSR values), no flush"},
         "gpu_launches": launches * args.steps,
         "roofline": {"bound": "hbm", "kernel": "bsim4_eval_kernel", "achieved": eval_achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": eval_achieved / hbm_peak, "traffic": None,
-                     "note": f"peak = {peak_src} HBM copy bandwidth; algorithmic bytes {EVAL_BYTES_PER_INST} B/instance"},
+                     "unit": "GB/s", "frac": eval_achieved / hbm_peak,
+                     "traffic": EVAL_DRAM_BYTES_PER_INST_NCU * n,
+                     "note": f"peak = {peak_src} HBM copy bandwidth; algorithmic bytes {EVAL_BYTES_PER_INST} B/instance; "
+                             f"traffic = ncu DRAM bytes per instance ({EVAL_DRAM_BYTES_PER_INST_NCU} B at 199,832 "
+                             "instances, profiles/bsim4_eval_kernel_scale.md) x instances"},
         "kernels_ms": {"eval": t_eval, "gather_vectors": t_vec, "gather_matrices": t_mat},
         "eval_launch_shape": {"block": blk.value, "min_blocks_per_sm": minb.value},
         "fp64": {"probe_peak_tflops": fp64_peak_tflops},
@@ -374,6 +462,11 @@ def main():
     }
     if cpu is not None:
         result["cpu_baseline"] = cpu
+    if rank == 0 and world == 1 and not args.no_transient:
+        from oracle import xyce_ref as xr
+
+        if xr.available():
+            result["transient"] = transient_section(args)
     if rank == 0:
         print(json.dumps(result))
     dev.close()

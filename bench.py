@@ -45,6 +45,68 @@ EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
 EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 333
 
 
+def batched_section(args, dev_id):
+    """The batched Monte-Carlo sweep: 256 circuits (sizes log-uniform 1k-20k MOSFETs, per-circuit
+    DELVTO ~ N(0, 30 mV) and TOXE x U[0.98, 1.02]) merged into one block-diagonal system, every
+    device load one evaluation launch over all circuits; timed as direct calls and as replays of
+    a CUDA graph that captured the load (output zeroing + update_state + both gathers)."""
+    import ctypes
+
+    import torch
+
+    from xyce_b200 import MosfetDevice, SolverFlags, _native, netlist
+
+    b = netlist.batched_sweep(256, 1000, 20000, seed=args.seed)
+    c = b.circuit
+    rowptr, colind = netlist.jacobian_pattern(c)
+    dev = MosfetDevice(b.cards, b.inst_model, c.mos_nodes, b.inst_params, (rowptr, colind), c.n_unknowns,
+                       device=dev_id, level=14)
+    n, nu, nnz = c.n_mos, c.n_unknowns, int(rowptr[-1])
+    f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
+    sol = torch.as_tensor(np.random.default_rng(args.seed).uniform(0, 1.2, nu), **f64)
+    sta_n, sta_c = torch.zeros(3 * n, **f64), torch.zeros(3 * n, **f64)
+    sto_n, sto_c = torch.zeros(14 * n, **f64), torch.zeros(14 * n, **f64)
+    out = [torch.zeros(nu, **f64) for _ in range(4)] + [torch.zeros(nnz, **f64) for _ in range(2)]
+    dev.load(SolverFlags(newton_iter=1, voltlim=0), sol, sta_n, sta_c, sto_n, sto_c, *out)
+    flags = SolverFlags(newton_iter=1)
+
+    def step():
+        for v in out:
+            v.zero_()
+        dev.load(flags, sol, sta_n, sta_c, sto_n, sto_c, *out)
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        step()
+    res = {}
+    for mode in ("direct", "cuda_graph"):
+        for _ in range(3):
+            graph.replay() if mode == "cuda_graph" else step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            graph.replay() if mode == "cuda_graph" else step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[mode] = {"ms_per_load": ms, "loads_per_s": n / (ms * 1e-3)}
+    blk, minb = ctypes.c_int(), ctypes.c_int()
+    _native.load().xd_eval_launch_shape(dev._h, ctypes.byref(blk), ctypes.byref(minb))
+    dev.close()
+    return {"workload": f"256 seeded gate netlists (sizes log-uniform 1k-20k, {n} BSIM4 MOSFETs in all, {nu} "
+                        f"unknowns, {nnz} nnz), per-circuit DELVTO ~ N(0, 30 mV) and TOXE x U[0.98, 1.02] "
+                        f"(512 model cards), one evaluation launch per load",
+            "circuits": int(len(b.sizes)), "mosfets": n, **res,
+            "eval_launch_shape": {"block": blk.value, "min_blocks_per_sm": minb.value}}
+
+
 def transient_section(args):
     """Transient wall time per run, GPU path vs the oracle's loads through the same driver, and
     the learned warm start against the plain GPU path (Newton iterations per step)."""
@@ -136,6 +198,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-transient", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     return ap.parse_args()
 
@@ -392,33 +455,48 @@ def main():
     torch.cuda.synchronize()
     fp64_peak_tflops = 2.0 * 148 * 8 * 256 * iters * 64 / (e0.elapsed_time(e1) * 1e-3) / 1e12
 
-    # End to end through the C ABI with host buffers: H2D of the iterate, D2H of every output.
+    # End to end through the C ABI with host buffers: every step copies its iterate and store in
+    # from pinned host memory and every output (F, Q, both limiter vectors, both CSR value arrays,
+    # state, store) back out. Two buffer sets and two streams pipeline consecutive steps: step
+    # k's load runs while step k-1's results travel back over PCIe.
     pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-    h_sol = pin(sol)
-    h_sol.copy_(torch.as_tensor(sol_h))
-    h_sto = pin(sto_n)
-    h_sto.copy_(sto_n.cpu())
-    h_out = {k: pin(v) for k, v in out.items()}
-    h_sta, h_sto_out = pin(sta_n), pin(sto_n)
-    h2d = (h_sol.numel() + h_sto.numel()) * 8
-    d2h = sum(v.numel() for v in h_out.values()) * 8 + (h_sta.numel() + h_sto_out.numel()) * 8
+    s_comp, s_copy = torch.cuda.Stream(), torch.cuda.Stream()
+    sets = []
+    for _ in range(2):
+        d = {"sol": torch.empty_like(sol), "sta_n": torch.zeros_like(sta_n), "sto_n": torch.zeros_like(sto_n)}
+        d.update({k: torch.zeros_like(v) for k, v in out.items()})
+        h = {k: pin(v) for k, v in d.items() if k not in ("sol",)}
+        h_in = {"sol": pin(sol), "sto_n": pin(sto_n)}
+        h_in["sol"].copy_(torch.as_tensor(sol_h))
+        h_in["sto_n"].copy_(sto_n.cpu())
+        sets.append((d, h, h_in, torch.cuda.Event(), torch.cuda.Event()))
+    h2d = (sol.numel() + sto_n.numel()) * 8
+    d2h = sum(v.numel() for v in out.values()) * 8 + (sta_n.numel() + sto_n.numel()) * 8
 
-    def e2e_step():
-        sol.copy_(h_sol, non_blocking=True)
-        sto_n.copy_(h_sto, non_blocking=True)
-        step()
-        for k, v in out.items():
-            h_out[k].copy_(v, non_blocking=True)
-        h_sta.copy_(sta_n, non_blocking=True)
-        h_sto_out.copy_(sto_n, non_blocking=True)
+    def e2e_step(k):
+        d, h, h_in, computed, copied = sets[k % 2]
+        s_comp.wait_event(copied)
+        with torch.cuda.stream(s_comp):
+            d["sol"].copy_(h_in["sol"], non_blocking=True)
+            d["sto_n"].copy_(h_in["sto_n"], non_blocking=True)
+            for key in ("f", "q", "fx", "qx", "jf", "jq"):
+                d[key].zero_()
+            dev.load(flags, d["sol"], d["sta_n"], sta_c, d["sto_n"], sto_c, d["f"], d["q"], d["fx"], d["qx"], d["jf"],
+                     d["jq"], stream=s_comp)
+            computed.record(s_comp)
+        s_copy.wait_event(computed)
+        with torch.cuda.stream(s_copy):
+            for key in ("f", "q", "fx", "qx", "jf", "jq", "sta_n", "sto_n"):
+                h[key].copy_(d[key], non_blocking=True)
+            copied.record(s_copy)
 
-    for _ in range(3):
-        e2e_step()
+    for k in range(4):
+        e2e_step(k)
     torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
+    e0.record(s_comp)
+    for k in range(args.steps):
+        e2e_step(k)
+    e1.record(s_copy)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     if dist is not None:
@@ -462,6 +540,8 @@ def main():
     }
     if cpu is not None:
         result["cpu_baseline"] = cpu
+    if rank == 0 and world == 1 and not args.no_batched:
+        result["batched"] = batched_section(args, dev_id)
     if rank == 0 and world == 1 and not args.no_transient:
         from oracle import xyce_ref as xr
 

@@ -216,3 +216,65 @@ def inverter_ring(stages: int = 101, vdd: float = 1.8, wn: float = 1e-6, wp: flo
                    cap_nodes=np.stack([out, np.full(stages, -1)], 1).astype(np.int32),
                    cap_value=np.full(stages, cload), vsrc_nodes=np.array([[VDD, -1]], np.int32),
                    vsrc_dc=np.array([vdd]), vsrc_pwl=[None], vdd=vdd, meta=dict(kind="inverter_ring", stages=stages))
+
+
+@dataclass
+class Batch:
+    """Several circuits merged into one block-diagonal system (one family, one launch)."""
+
+    circuit: Circuit              # merged circuit (unknowns of circuit k are contiguous)
+    cards: list                   # model cards: 2 per circuit (NMOS, PMOS)
+    inst_model: np.ndarray        # card index per MOSFET
+    inst_params: dict             # instance-line parameters (L, W, DELVTO)
+    node_offset: np.ndarray       # [n_circuits + 1] first node of each circuit
+    mos_offset: np.ndarray        # [n_circuits + 1] first MOSFET of each circuit
+    sizes: np.ndarray             # MOSFETs per circuit
+    delvto: np.ndarray            # per-circuit threshold shift (V)
+    toxe_factor: np.ndarray       # per-circuit oxide-thickness factor
+
+
+def batched_sweep(n_circuits: int = 256, min_mos: int = 1000, max_mos: int = 20000, seed: int = 0,
+                  sigma_vth: float = 0.030, toxe_spread: float = 0.02, toxe_nominal: float = 3.0e-9,
+                  wire_segments: int = 2) -> Batch:
+    """A Monte-Carlo sweep: n_circuits random gate netlists (``random_logic``, sizes log-uniform in
+    [min_mos, max_mos]), each with its own threshold shift ~ N(0, sigma_vth) (instance DELVTO on
+    all its MOSFETs) and oxide thickness TOXE x U[1 - spread, 1 + spread] (its own NMOS/PMOS model
+    cards), merged into one block-diagonal circuit whose unknowns keep each circuit contiguous.
+    Node unknowns of every circuit come first, then every circuit's source branches."""
+    from .device import ModelCard
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(min_mos), np.log(max_mos), n_circuits)).astype(int)
+    delvto = rng.normal(0.0, sigma_vth, n_circuits)
+    toxe = rng.uniform(1 - toxe_spread, 1 + toxe_spread, n_circuits)
+    parts = [random_logic(int(m), seed=seed * 100003 + k + 1, wire_segments=wire_segments) for k, m in enumerate(sizes)]
+    node_off = np.zeros(n_circuits + 1, dtype=np.int64)
+    mos_off = np.zeros(n_circuits + 1, dtype=np.int64)
+    for k, p in enumerate(parts):
+        node_off[k + 1] = node_off[k] + p.n_nodes
+        mos_off[k + 1] = mos_off[k] + p.n_mos
+
+    def shift(a, off):
+        a = np.asarray(a, dtype=np.int64)
+        return np.where(a >= 0, a + off, -1)
+
+    mos_nodes = np.concatenate([shift(p.mos_nodes, node_off[k]) for k, p in enumerate(parts)]).astype(np.int32)
+    res_nodes = np.concatenate([shift(p.res_nodes, node_off[k]) for k, p in enumerate(parts)]).astype(np.int32)
+    cap_nodes = np.concatenate([shift(p.cap_nodes, node_off[k]) for k, p in enumerate(parts)]).astype(np.int32)
+    vsrc_nodes = np.concatenate([shift(p.vsrc_nodes, node_off[k]) for k, p in enumerate(parts)]).astype(np.int32)
+    merged = Circuit(n_nodes=int(node_off[-1]), mos_type=np.concatenate([p.mos_type for p in parts]),
+                     mos_nodes=mos_nodes, mos_w=np.concatenate([p.mos_w for p in parts]),
+                     mos_l=np.concatenate([p.mos_l for p in parts]), res_nodes=res_nodes,
+                     res_value=np.concatenate([p.res_value for p in parts]), cap_nodes=cap_nodes,
+                     cap_value=np.concatenate([p.cap_value for p in parts]), vsrc_nodes=vsrc_nodes,
+                     vsrc_dc=np.concatenate([p.vsrc_dc for p in parts]),
+                     vsrc_pwl=[w for p in parts for w in p.vsrc_pwl], vdd=parts[0].vdd,
+                     meta=dict(kind="batched_sweep", n_circuits=n_circuits, seed=seed))
+    cards = []
+    for k in range(n_circuits):
+        cards.append(ModelCard(False, {"TOXE": toxe_nominal * toxe[k]}))
+        cards.append(ModelCard(True, {"TOXE": toxe_nominal * toxe[k]}))
+    circ = np.repeat(np.arange(n_circuits), np.diff(mos_off))
+    inst_model = (2 * circ + merged.mos_type).astype(np.int32)
+    params = {"L": merged.mos_l.astype(float), "W": merged.mos_w.astype(float), "DELVTO": delvto[circ]}
+    return Batch(merged, cards, inst_model, params, node_off, mos_off, sizes, delvto, toxe)

@@ -122,9 +122,9 @@ def test_bsim4_surrogate_trains_on_fp64_samples_and_warm_start_keeps_exact_answe
     from xyce_b200.transient import GpuTransient, NewtonParams
 
     sur = S.BsimSurrogate(seed=0)
-    rep = sur.train(n_samples=400_000, epochs=3, batch=16384)
+    rep = sur.train(n_samples=2_000_000, epochs=4, batch=16384)
     for typ in ("nmos", "pmos"):
-        assert rep[typ]["Id"]["rel_median"] < 0.5, rep[typ]["Id"]
+        assert rep[typ]["Id"]["rel_median"] < 0.35, rep[typ]["Id"]
     c = netlist.random_logic(300, seed=3, n_inputs=8)
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, im, nd, params = family_inputs(c, None)

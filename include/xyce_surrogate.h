@@ -52,6 +52,24 @@ int xd_mlp_input_layer(int M, int n_in, int n_hid, const float *d_x, int ldx, co
 int xd_mlp_input_grad(int M, int n_in, int n_hid, const void *d_dzt, int ldt, const float *d_x, int ldx,
                       float *d_gw, int ldw, void *stream);
 
+/* The whole surrogate network for inference in one persistent kernel: weights staged once per CTA
+ * in shared memory, each 128-sample tile through the FP32 first layer (CUDA cores), three 128-wide
+ * BF16 layers and the 16-wide output layer on the tcgen05 tensor cores (accumulator in tensor
+ * memory, bias + SiLU epilogues writing the next operand back to shared memory). Reads x [n x ldx]
+ * (n_in columns), writes y [n x ldy] (ldy >= 16; 16 outputs, padding included). max_ctas <= 0
+ * means one CTA per SM. */
+typedef struct xd_mlp_net {
+  int n_in;            /* inputs, <= 8 */
+  const float *w1;     /* FP32 [128 x ldw1] */
+  int ldw1;
+  const void *w[3];    /* BF16 [128 x 128], hidden layers 2..4, row-major [out][in] */
+  const void *w5;      /* BF16 [16 x 128], output layer (rows past the outputs zero) */
+  const float *b[5];   /* FP32 biases: 128, 128, 128, 128, 16 */
+} xd_mlp_net;
+
+int xd_mlp_forward(const xd_mlp_net *net, int n, const float *d_x, int ldx, float *d_y, int ldy, int *d_err,
+                   int max_ctas, void *stream);
+
 /* d = scale * (y - target) for the first n_out of ld columns (0 in the padding), as BF16 in
  * d_dz [M x ld] and transposed in d_dzt [ld x ldt]; per-sample squared error into d_sq (or null). */
 int xd_mse_grad(int M, int n_out, int ld, const float *d_y, const float *d_target, float scale, void *d_dz,

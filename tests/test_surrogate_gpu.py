@@ -145,3 +145,22 @@ def test_bsim4_surrogate_trains_on_fp64_samples_and_warm_start_keeps_exact_answe
         g.close()
         fam.close()
     assert np.abs(waves[0] - waves[1]).max() < 1e-9
+
+
+def test_fused_forward_matches_layer_by_layer():
+    """The one-launch fused inference kernel against the layer-by-layer GEMM path, on a trained-ish
+    network (a few Adam steps so the weights are not the initial ones)."""
+    rng = np.random.default_rng(8)
+    net = S.SurrogateMLP(seed=4, max_batch=70000)
+    for _ in range(5):
+        X = rng.uniform(-1, 1, (4096, S.N_IN))
+        net.train_step(X, np.tanh(X @ rng.standard_normal((S.N_IN, S.N_OUT))), S.AdamConfig(lr=1e-2))
+    n = 66_000  # not a multiple of the 128-row tile
+    X = rng.uniform(-1, 1, (n, S.N_IN))
+    ref = net.forward(X).clone()
+    net._load_inputs(X)
+    net.Y.zero_()
+    got = net.forward_fused(n)
+    torch.cuda.synchronize()
+    net.k.check_err()
+    assert torch.allclose(got, ref, rtol=1e-5, atol=1e-5), (got - ref).abs().max()

@@ -59,6 +59,13 @@ class XdGemmArgs(ctypes.Structure):
                 ("HT", ctypes.c_void_p), ("Zin", ctypes.c_void_p), ("err", ctypes.c_void_p)]
 
 
+class XdMlpNet(ctypes.Structure):
+    """Mirror of ``xd_mlp_net``."""
+
+    _fields_ = [("n_in", ctypes.c_int), ("w1", ctypes.c_void_p), ("ldw1", ctypes.c_int), ("w", ctypes.c_void_p * 3),
+                ("w5", ctypes.c_void_p), ("b", ctypes.c_void_p * 5)]
+
+
 class XdAdamArgs(ctypes.Structure):
     _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
                 ("bias_corr1", ctypes.c_float), ("bias_corr2", ctypes.c_float)]
@@ -102,6 +109,8 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "xd_load_vectors_staged": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5 + [ctypes.c_int,
                                                                                         ctypes.c_void_p]),
+    "xd_mlp_forward": (ctypes.c_int, [ctypes.POINTER(XdMlpNet), ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "xd_mse_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_void_p]),

@@ -474,6 +474,150 @@ __global__ void surrogate_stage_kernel(int n, const int *__restrict__ idx, const
   for (int s = 8; s < 16; ++s) stage[s * N + i] = 0.0;
 }
 
+// ---- fused inference: the whole 5 -> 128 -> 128 -> 128 -> 128 -> 16 network in one kernel -----
+
+constexpr int kFusedThreads = 256;  // 8 warps: two per tensor-memory lane quarter
+constexpr int kHid = 128;
+constexpr int kOutPad = 16;
+// Shared-memory layout of a 128-row x 128-K BF16 operand: 8 x 8 core matrices, K-adjacent ones
+// 128 B apart, 8-row groups 2048 B apart.
+__device__ __forceinline__ uint32_t off128(int r, int kc) {
+  return (uint32_t)((r >> 3) * 2048 + kc * 128 + (r & 7) * 16);
+}
+
+struct FusedSmem {
+  unsigned char w[3][kHid * kHid * 2];   // hidden layers 2..4, [out][in] K-major
+  unsigned char w5[kOutPad * kHid * 2];  // output layer, 16 x 128
+  unsigned char act[kHid * kHid * 2];    // activation tile (A operand), 128 x 128
+  float w1[kHid * 8];                    // first layer, FP32, 128 x n_in (n_in <= 8)
+  float b[4 * kHid + kOutPad];           // biases of layers 1..5
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(kFusedThreads, 1) mlp_forward_fused_kernel(xd_mlp_net net, int n, const float *x,
+                                                                            int ldx, float *y, int ldy, int *err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  FusedSmem &S = *reinterpret_cast<FusedSmem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // Stage the weights once per CTA.
+  for (int l = 0; l < 3; ++l) {
+    const __nv_bfloat16 *W = static_cast<const __nv_bfloat16 *>(net.w[l]);
+    for (int i = tid; i < kHid * 16; i += kFusedThreads) {
+      const int r = i >> 4, kc = i & 15;
+      *reinterpret_cast<uint4 *>(S.w[l] + off128(r, kc)) =
+          *reinterpret_cast<const uint4 *>(W + (size_t)r * kHid + kc * 8);
+    }
+  }
+  {
+    const __nv_bfloat16 *W = static_cast<const __nv_bfloat16 *>(net.w5);
+    for (int i = tid; i < kOutPad * 16; i += kFusedThreads) {
+      const int r = i >> 4, kc = i & 15;
+      *reinterpret_cast<uint4 *>(S.w5 + off128(r, kc)) = *reinterpret_cast<const uint4 *>(W + (size_t)r * kHid + kc * 8);
+    }
+  }
+  for (int i = tid; i < kHid * net.n_in; i += kFusedThreads) S.w1[(i / net.n_in) * 8 + i % net.n_in] =
+      net.w1[(i / net.n_in) * net.ldw1 + i % net.n_in];
+  for (int i = tid; i < 4 * kHid + kOutPad; i += kFusedThreads) {
+    const int l = i / kHid, u = i % kHid;
+    S.b[i] = (l < 4) ? net.b[l][u] : net.b[4][i - 4 * kHid];
+  }
+  if (warp == 0) tmem_alloc(&S.tmem, kHid);
+  if (tid == 0) {
+    mbar_init(&S.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t idesc_h = instr_desc_bf16(kTileM, kHid);
+  const uint32_t idesc_o = instr_desc_bf16(kTileM, kOutPad);
+  const uint32_t act_a = smem_u32(S.act);
+  const int quarter = warp & 3;           // tensor-memory lanes 32q .. 32q + 31
+  const int half = warp >> 2;             // columns [64 half, 64 half + 64)
+  const int row = quarter * 32 + lane;    // the tile row this thread owns in the epilogues
+  const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int tiles = (n + kTileM - 1) / kTileM;
+  for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const int g = tile * kTileM + row;
+    // Layer 1 on the CUDA cores (FP32): this thread's 64 hidden units of its row.
+    {
+      float xi[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) xi[i] = (i < net.n_in && g < n) ? x[(size_t)g * ldx + i] : 0.0f;
+      for (int c8 = 0; c8 < 8; ++c8) {
+        __align__(16) __nv_bfloat16 h8[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int u = half * 64 + c8 * 8 + j;
+          float z = S.b[u];
+          for (int i = 0; i < net.n_in; ++i) z += S.w1[u * 8 + i] * xi[i];
+          h8[j] = __float2bfloat16(g < n ? silu(z) : 0.0f);
+        }
+        *reinterpret_cast<uint4 *>(S.act + off128(row, half * 8 + c8)) = *reinterpret_cast<uint4 *>(h8);
+      }
+    }
+    // Layers 2..5 on the tensor cores.
+    for (int l = 0; l < 4 && ok; ++l) {
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      const bool last = (l == 3);
+      if (tid == 0) {
+        const uint32_t wb = last ? smem_u32(S.w5) : smem_u32(S.w[l]);
+        for (int s = 0; s < 8; ++s)
+          mma_bf16(tmem, smem_desc(act_a + s * 256, 128, 2048), smem_desc(wb + s * 256, 128, 2048),
+                   last ? idesc_o : idesc_h, s > 0 ? 1u : 0u);
+        mma_commit(&S.bar);
+      }
+      ok = __syncthreads_and(mbar_wait(&S.bar, phase)) != 0;
+      phase ^= 1u;
+      tc_fence_after();
+      if (!ok) break;
+      if (!last) {
+        // Epilogue: bias + SiLU, written back as the next layer's operand.
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 32) {
+          float v[32];
+          tmem_ld32(lane_base + half * 64 + c0, v);
+#pragma unroll
+          for (int c8 = 0; c8 < 4; ++c8) {
+            __align__(16) __nv_bfloat16 h8[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int u = half * 64 + c0 + c8 * 8 + j;
+              h8[j] = __float2bfloat16(silu(v[c8 * 8 + j] + S.b[(l + 1) * kHid + u]));
+            }
+            *reinterpret_cast<uint4 *>(S.act + off128(row, (half * 64 + c0) / 8 + c8)) =
+                *reinterpret_cast<uint4 *>(h8);
+          }
+        }
+      } else if (half == 0) {
+        float v[16];
+        tmem_ld16(lane_base, v);
+        if (g < n) {
+#pragma unroll
+          for (int j = 0; j < kOutPad; ++j) y[(size_t)g * ldy + j] = v[j] + S.b[4 * kHid + j];
+        }
+      }
+      tc_fence_before();
+    }
+    __syncthreads();
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    mbar_wait(&S.bar, phase ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_free(tmem, kHid);
+}
+
 int cuda_err(cudaError_t e, const char *where) {
   return xd_internal_fail(-3, std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
 }
@@ -549,6 +693,33 @@ int xd_surrogate_stage(int n, const int *d_idx, const float *d_y, int ldy, const
                                                                             d_stage);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : cuda_err(e, "surrogate_stage_kernel");
+}
+
+int xd_mlp_forward(const xd_mlp_net *net, int n, const float *d_x, int ldx, float *d_y, int ldy, int *d_err,
+                   int max_ctas, void *stream) {
+  if (!net || !net->w1 || !net->w5 || !d_x || !d_y || !d_err || n < 0 || net->n_in < 1 || net->n_in > 8 ||
+      ldy < kOutPad)
+    return xd_internal_fail(-1, "bad fused-forward arguments");
+  for (int l = 0; l < 3; ++l)
+    if (!net->w[l]) return xd_internal_fail(-1, "bad fused-forward weights");
+  for (int l = 0; l < 5; ++l)
+    if (!net->b[l]) return xd_internal_fail(-1, "bad fused-forward biases");
+  if ((reinterpret_cast<uintptr_t>(net->w[0]) | reinterpret_cast<uintptr_t>(net->w[1]) |
+       reinterpret_cast<uintptr_t>(net->w[2]) | reinterpret_cast<uintptr_t>(net->w5)) & 15)
+    return xd_internal_fail(-1, "fused-forward weights must be 16-byte aligned");
+  if (n == 0) return 0;
+  const int tiles = (n + kTileM - 1) / kTileM;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid = tiles < sms ? tiles : sms;
+  if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+  const size_t smem = sizeof(FusedSmem);
+  cudaError_t e = cudaFuncSetAttribute(mlp_forward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_err(e, "cudaFuncSetAttribute(mlp_forward_fused_kernel)");
+  mlp_forward_fused_kernel<<<grid, kFusedThreads, smem, (cudaStream_t)stream>>>(*net, n, d_x, ldx, d_y, ldy, d_err);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : cuda_err(e, "mlp_forward_fused_kernel");
 }
 
 int xd_mse_grad(int M, int n_out, int ld, const float *d_y, const float *d_target, float scale, void *d_dz,

@@ -178,6 +178,21 @@ class SurrogateMLP:
         self._forward(Bp)
         return self.Y[:n, :N_OUT]
 
+    def forward_fused(self, n):
+        """Inference on the first n rows of self.X32 by the fused kernel (xd_mlp_forward): one
+        persistent launch for the whole network; outputs (scaled space) in self.Y[:n]."""
+        k = self.k
+        net = _native.XdMlpNet()
+        net.n_in, net.w1, net.ldw1 = N_IN, self.W[0].data_ptr(), PAD_IN
+        for l in range(3):
+            net.w[l] = self.W16[l + 1].data_ptr()
+        net.w5 = self.W16[N_LAYERS].data_ptr()
+        for l in range(5):
+            net.b[l] = self.b[l].data_ptr()
+        _native.check(k.lib.xd_mlp_forward(ctypes.byref(net), int(n), _p(self.X32), PAD_IN, _p(self.Y), PAD_OUT,
+                                           _p(k.err), 0, k.stream()), "xd_mlp_forward")
+        return self.Y[:n, :N_OUT]
+
     def _forward(self, Bp):
         k = self.k
         _native.check(k.lib.xd_mlp_input_layer(Bp, N_IN, N_HID, _p(self.X32), PAD_IN, _p(self.W[0]), PAD_IN,
@@ -381,7 +396,8 @@ class BsimSurrogate:
         out = []
         net = self.nets[pmos]
         for i in range(0, len(X), batch):
-            out.append(net.forward(X[i:i + batch]).double().cpu().numpy())
+            n, _ = net._load_inputs(X[i:i + batch])
+            out.append(net.forward_fused(n).double().cpu().numpy())
         return decode_outputs(np.concatenate(out))
 
 
@@ -421,11 +437,10 @@ class SurrogateLoads:
             if m == 0:
                 continue
             net = self.sur.nets[p]
-            Bp = (m + 127) // 128 * 128
             _native.check(self.lib.xd_surrogate_features(m, _p(self.idx[p]), _p(self.nodes4), _p(x), _p(self.geom2),
                                                          ctypes.c_float(VMAX), _p(net.X32), PAD_IN, stream),
                           "xd_surrogate_features")
-            net._forward(Bp)
+            net.forward_fused(m)
             _native.check(self.lib.xd_surrogate_stage(m, _p(self.idx[p]), _p(net.Y), PAD_OUT, _p(self.out_scale),
                                                       self.n, _p(self.stage), stream), "xd_surrogate_stage")
         _native.check(self.lib.xd_load_vectors_staged(self.fam._h, _p(self.stage), _p(f), _p(q), _p(fx), _p(qx), 1,

@@ -1,0 +1,41 @@
+/* xyce_rf.h — GPU sparse LU refactorization for the transient driver's Newton matrices.
+ *
+ * Stands in for the reference's direct solve (KLU through Amesos, src/LinearAlgebraServicesPKG/
+ * src/N_LAS_AmesosSolver.C:160, 305) where the matrix values are already on the GPU: one host
+ * factorization P A Q = L U fixes the pivot order and the fill pattern, every later matrix with
+ * A's pattern is refactored and solved on the device. Calls run on the CUDA legacy default stream
+ * (the refactorization library has no stream argument); order them after the producer of the
+ * values on that stream. Status: 0 ok, < 0 error (xd_last_error()).
+ */
+#ifndef XYCE_RF_H
+#define XYCE_RF_H
+
+#include "xyce_devload.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xd_rf xd_rf;
+
+/* Host inputs, all CSR 0-based, n x n: A's pattern and values, the factors L (unit lower, the
+ * unit diagonal stored) and U (upper) of P A Q = L U, and P, Q as arrays: (P A Q)[i][j] =
+ * A[P[i]][Q[j]]. */
+int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, const double *vals_a, int nnz_l,
+                 const int *rowptr_l, const int *colind_l, const double *vals_l, int nnz_u, const int *rowptr_u,
+                 const int *colind_u, const double *vals_u, const int *p, const int *q, int cuda_device,
+                 xd_rf **out);
+
+/* Refactors with new values of A (device, in A's pattern), keeping the pivot order. */
+int xd_rf_refactor(xd_rf *rf, const double *d_vals_a);
+
+/* Solves A x = b in place: d_x holds b on entry and x on return (device, length n). */
+int xd_rf_solve(xd_rf *rf, double *d_x);
+
+int xd_rf_destroy(xd_rf *rf);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XYCE_RF_H */

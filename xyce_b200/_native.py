@@ -1,5 +1,5 @@
 """Loader for the package's native library (libxyce_b200.so) and its C ABI (include/xyce_devload.h,
-include/xyce_tia.h).
+include/xyce_tia.h, include/xyce_surrogate.h, include/xyce_rf.h).
 
 The library is built in-tree by ``xyce_b200.build.build()``. There is no fallback: if the
 library is missing or was built for another architecture, loading fails with an error.
@@ -111,6 +111,12 @@ SIGNATURES = {
                                                                                         ctypes.c_void_p]),
     "xd_mlp_forward": (ctypes.c_int, [ctypes.POINTER(XdMlpNet), ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "xd_rf_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _ip, _ip, _dp,
+                                    ctypes.c_int, _ip, _ip, _dp, _ip, _ip, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_rf_refactor": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_rf_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_rf_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_mse_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_void_p]),

@@ -1,0 +1,156 @@
+// GPU sparse LU refactorization for the Newton matrices of a transient (include/xyce_rf.h).
+//
+// Every Newton matrix of a circuit has the same sparsity pattern, so after one numeric
+// factorization P A Q = L U on the host (its pivot order and fill pattern), every later matrix is
+// refactored and solved on the GPU with that pattern (cuSOLVER's refactorization library), and
+// the values never leave the device. This is the library linear solve of the transient driver,
+// not part of the device-load path.
+#include <cuda_runtime.h>
+#include <cusolverRf.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/xyce_rf.h"
+
+int xd_internal_fail(int code, const std::string &msg);
+
+struct xd_rf {
+  int device = 0;
+  int n = 0, nnz_a = 0;
+  int *d_rowptr = nullptr, *d_colind = nullptr, *d_p = nullptr, *d_q = nullptr;
+  double *d_temp = nullptr;
+  cusolverRfHandle_t h = nullptr;
+};
+
+namespace {
+
+int rf_fail(cusolverStatus_t st, const char *where) {
+  return xd_internal_fail(-4, std::string("cuSOLVER refactorization error ") + std::to_string((int)st) + " in " +
+                                  where);
+}
+
+int cu_fail(cudaError_t e, const char *where) {
+  return xd_internal_fail(-3, std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+}
+
+void release(xd_rf *r) {
+  if (!r) return;
+  if (r->h) cusolverRfDestroy(r->h);
+  cudaFree(r->d_rowptr);
+  cudaFree(r->d_colind);
+  cudaFree(r->d_p);
+  cudaFree(r->d_q);
+  cudaFree(r->d_temp);
+  delete r;
+}
+
+bool csr_ok(int n, int nnz, const int *rp, const int *ci) {
+  if (!rp || (nnz > 0 && !ci) || rp[0] != 0 || rp[n] != nnz) return false;
+  for (int r = 0; r < n; ++r)
+    if (rp[r + 1] < rp[r]) return false;
+  for (int k = 0; k < nnz; ++k)
+    if (ci[k] < 0 || ci[k] >= n) return false;
+  return true;
+}
+
+bool perm_ok(int n, const int *p) {
+  if (!p) return false;
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; ++i) {
+    if (p[i] < 0 || p[i] >= n || seen[p[i]]) return false;
+    seen[p[i]] = 1;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, const double *vals_a, int nnz_l,
+                 const int *rowptr_l, const int *colind_l, const double *vals_l, int nnz_u, const int *rowptr_u,
+                 const int *colind_u, const double *vals_u, const int *p, const int *q, int cuda_device,
+                 xd_rf **out) {
+  if (!out || n <= 0 || !vals_a || !vals_l || !vals_u) return xd_internal_fail(-1, "bad refactorization arguments");
+  *out = nullptr;
+  if (!csr_ok(n, nnz_a, rowptr_a, colind_a) || !csr_ok(n, nnz_l, rowptr_l, colind_l) ||
+      !csr_ok(n, nnz_u, rowptr_u, colind_u))
+    return xd_internal_fail(-1, "bad CSR input to the refactorization set-up");
+  if (!perm_ok(n, p) || !perm_ok(n, q)) return xd_internal_fail(-1, "P and Q must be permutations of 0..n-1");
+  cudaError_t e = cudaSetDevice(cuda_device);
+  if (e != cudaSuccess) return cu_fail(e, "cudaSetDevice");
+  xd_rf *r = new xd_rf();
+  r->device = cuda_device;
+  r->n = n;
+  r->nnz_a = nnz_a;
+  if ((e = cudaMalloc(&r->d_rowptr, sizeof(int) * (n + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&r->d_colind, sizeof(int) * (nnz_a > 0 ? nnz_a : 1))) != cudaSuccess ||
+      (e = cudaMalloc(&r->d_p, sizeof(int) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&r->d_q, sizeof(int) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&r->d_temp, sizeof(double) * n)) != cudaSuccess ||
+      (e = cudaMemcpy(r->d_rowptr, rowptr_a, sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(r->d_colind, colind_a, sizeof(int) * nnz_a, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(r->d_p, p, sizeof(int) * n, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(r->d_q, q, sizeof(int) * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    release(r);
+    return cu_fail(e, "xd_rf_create upload");
+  }
+  cusolverStatus_t st;
+  if ((st = cusolverRfCreate(&r->h)) != CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfCreate");
+  }
+  if ((st = cusolverRfSetMatrixFormat(r->h, CUSOLVERRF_MATRIX_FORMAT_CSR, CUSOLVERRF_UNIT_DIAGONAL_STORED_L)) !=
+          CUSOLVER_STATUS_SUCCESS ||
+      (st = cusolverRfSetResetValuesFastMode(r->h, CUSOLVERRF_RESET_VALUES_FAST_MODE_ON)) != CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRf configuration");
+  }
+  // The set-up reads host copies; the library's signature is not const-qualified.
+  std::vector<int> ra(rowptr_a, rowptr_a + n + 1), ca(colind_a, colind_a + nnz_a);
+  std::vector<int> rl(rowptr_l, rowptr_l + n + 1), cl(colind_l, colind_l + nnz_l);
+  std::vector<int> ru(rowptr_u, rowptr_u + n + 1), cu(colind_u, colind_u + nnz_u);
+  std::vector<double> va(vals_a, vals_a + nnz_a), vl(vals_l, vals_l + nnz_l), vu(vals_u, vals_u + nnz_u);
+  std::vector<int> hp(p, p + n), hq(q, q + n);
+  if ((st = cusolverRfSetupHost(n, nnz_a, ra.data(), ca.data(), va.data(), nnz_l, rl.data(), cl.data(), vl.data(),
+                                nnz_u, ru.data(), cu.data(), vu.data(), hp.data(), hq.data(), r->h)) !=
+      CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfSetupHost");
+  }
+  if ((st = cusolverRfAnalyze(r->h)) != CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfAnalyze");
+  }
+  *out = r;
+  return 0;
+}
+
+int xd_rf_refactor(xd_rf *r, const double *d_vals_a) {
+  if (!r || !d_vals_a) return xd_internal_fail(-1, "null refactorization argument");
+  cudaSetDevice(r->device);
+  cusolverStatus_t st = cusolverRfResetValues(r->n, r->nnz_a, r->d_rowptr, r->d_colind, const_cast<double *>(d_vals_a),
+                                              r->d_p, r->d_q, r->h);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfResetValues");
+  st = cusolverRfRefactor(r->h);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfRefactor");
+  return 0;
+}
+
+int xd_rf_solve(xd_rf *r, double *d_x) {
+  if (!r || !d_x) return xd_internal_fail(-1, "null refactorization argument");
+  cudaSetDevice(r->device);
+  cusolverStatus_t st = cusolverRfSolve(r->h, r->d_p, r->d_q, 1, r->d_temp, r->n, d_x, r->n);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfSolve");
+  return 0;
+}
+
+int xd_rf_destroy(xd_rf *r) {
+  if (!r) return 0;
+  cudaSetDevice(r->device);
+  release(r);
+  return 0;
+}
+
+}  // extern "C"

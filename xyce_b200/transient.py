@@ -18,8 +18,10 @@ DC and piecewise-linear voltage sources), the reference's transient driver:
 
 Every device load and the combine run as CUDA kernels on device-resident buffers; the host only
 sees two scalars per Newton iteration (the residual's max norm and the update's weighted norm).
-The linear system is solved by a dense LU on the GPU for small circuits and by a host sparse LU
-(SuperLU through scipy) for large ones: the linear solve is outside the device-load path.
+The linear system is solved by a dense LU on the GPU for small circuits, by GPU sparse
+refactorization (one host factorization fixes pivots and fill, ``xd_rf_*`` refactors every later
+matrix on the device) or by a host sparse LU (SuperLU through scipy): the linear solve is outside
+the device-load path.
 
 Step control is fixed-step (the largest step the analysis allows), halving on Newton failure.
 """
@@ -134,6 +136,7 @@ class StepStats:
     wall_s: float = 0.0
     loads: int = 0
     factorizations: int = 0
+    host_factorizations: int = 0
     surrogate_loads: int = 0
     chord_iters: list = field(default_factory=list)
     surrogate_error: list = field(default_factory=list)
@@ -145,7 +148,8 @@ class TransientBase:
     Subclasses supply the two per-iterate steps, ``_load(flags)`` (every device's F, Q, dF/dx,
     dQ/dx at self.x) and ``_combine(mode, h, order, qn0, fhist)`` (Newton matrix, residual, Q and F
     totals); the buffers are torch tensors on ``dev``.
-    ``solver``: "dense" (LU on ``dev``, small circuits), "splu" (host sparse LU) or "auto".
+    ``solver``: "dense" (LU on ``dev``, small circuits), "rf" (GPU sparse refactorization, device
+    backends), "splu" (host sparse LU) or "auto".
     """
 
     def __init__(self, c, n_state, n_store, rowptr, colind, dev, solver="auto", gmin=1e-12):
@@ -266,6 +270,8 @@ class TransientBase:
     def _solve(self):
         """Factors the current Newton matrix (kept for chord iterations) and solves with rhs."""
         torch = self.torch
+        if self.solver == "rf":
+            return self._solve_rf()
         if self.solver == "dense":
             self._dense.zero_()
             self._dense[self._flat] = self.jac
@@ -279,9 +285,16 @@ class TransientBase:
         self.stats.factorizations += 1
         return self._solve_factored()
 
+    def _solve_rf(self):
+        raise NotImplementedError("the GPU refactorization needs a device backend")
+
     def _solve_factored(self):
         """Solves with the last factorization (a chord step when the matrix has moved on)."""
         torch = self.torch
+        if self.solver == "rf":
+            x = self.rhs.clone()
+            _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
+            return x
         if self.solver == "dense":
             LU, piv = self._lu
             return torch.linalg.lu_solve(LU, piv, self.rhs.view(-1, 1)).view(-1)
@@ -476,6 +489,63 @@ class GpuTransient(TransientBase):
         if getattr(self, "_tia", None) is not None and self._tia.value:
             self._lib.xd_tia_destroy(self._tia)
             self._tia = None
+        if getattr(self, "_rf", None) is not None and self._rf.value:
+            self._lib.xd_rf_destroy(self._rf)
+            self._rf = None
+
+    def _rf_setup(self):
+        """Host factorization of the current matrix (pivot order, fill) and the GPU refactorization
+        set-up from it: P A Q = L U with (P A Q)[i][j] = A[P[i]][Q[j]]."""
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+
+        if getattr(self, "_rf", None) is not None and self._rf.value:
+            self._lib.xd_rf_destroy(self._rf)
+            self._rf = None
+        vals = self.jac.cpu().numpy()
+        A = sp.csr_matrix((vals, self.colind, self.rowptr), shape=(self.nu, self.nu))
+        lu = spl.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A")
+        P = np.argsort(lu.perm_r).astype(np.int32)
+        Q = np.argsort(lu.perm_c).astype(np.int32)
+        L = lu.L.tocsr()
+        U = lu.U.tocsr()
+        L.sort_indices()
+        U.sort_indices()
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        arrs = [i32(self.rowptr), i32(self.colind), f64(vals), i32(L.indptr), i32(L.indices), f64(L.data),
+                i32(U.indptr), i32(U.indices), f64(U.data), P, Q]
+        self._rf_keep = arrs
+        ip = lambda a: a.ctypes.data_as(_native._ip)
+        dp = lambda a: a.ctypes.data_as(_native._dp)
+        h = ctypes.c_void_p()
+        _native.check(self._lib.xd_rf_create(self.nu, self.nnz, ip(arrs[0]), ip(arrs[1]), dp(arrs[2]), int(L.nnz),
+                                             ip(arrs[3]), ip(arrs[4]), dp(arrs[5]), int(U.nnz), ip(arrs[6]),
+                                             ip(arrs[7]), dp(arrs[8]), ip(P), ip(Q), self.dev.index or 0,
+                                             ctypes.byref(h)), "xd_rf_create")
+        self._rf = h
+        self.stats.host_factorizations += 1
+
+    def _solve_rf(self):
+        torch = self.torch
+        if getattr(self, "_rf", None) is None or not self._rf.value:
+            self._rf_setup()
+        else:
+            torch.cuda.current_stream(self.dev).synchronize()  # values complete before the library reads them
+            _native.check(self._lib.xd_rf_refactor(self._rf, ctypes.c_void_p(self.jac.data_ptr())), "xd_rf_refactor")
+        self.stats.factorizations += 1
+        self._lu = True
+        x = self.rhs.clone()
+        torch.cuda.current_stream(self.dev).synchronize()
+        _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
+        torch.cuda.synchronize(self.dev)
+        if not bool(torch.isfinite(x).all()):
+            # The kept pivot order failed on this matrix: factor it afresh on the host.
+            self._rf_setup()
+            x = self.rhs.clone()
+            _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
+            torch.cuda.synchronize(self.dev)
+        return x
 
     def __del__(self):
         try:

@@ -123,6 +123,11 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
     release(r);
     return rf_fail(st, "cusolverRfAnalyze");
   }
+  // The analysis is symbolic; the numeric factors come from a refactorization of A's values.
+  if ((st = cusolverRfRefactor(r->h)) != CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfRefactor");
+  }
   *out = r;
   return 0;
 }

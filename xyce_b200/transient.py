@@ -532,7 +532,11 @@ class GpuTransient(TransientBase):
             self._rf_setup()
         else:
             torch.cuda.current_stream(self.dev).synchronize()  # values complete before the library reads them
-            _native.check(self._lib.xd_rf_refactor(self._rf, ctypes.c_void_p(self.jac.data_ptr())), "xd_rf_refactor")
+            rc = self._lib.xd_rf_refactor(self._rf, ctypes.c_void_p(self.jac.data_ptr()))
+            if rc != 0:
+                # A zero pivot in the kept pivot order (the matrices of a DC solve and of a time step
+                # differ in which entries dominate): factor this matrix afresh on the host.
+                self._rf_setup()
         self.stats.factorizations += 1
         self._lu = True
         x = self.rhs.clone()

@@ -539,17 +539,46 @@ class GpuTransient(TransientBase):
                 self._rf_setup()
         self.stats.factorizations += 1
         self._lu = True
-        x = self.rhs.clone()
+        x = self._rf_solve_refined(self.rhs)
+        if x is None:
+            # The kept pivot order does not suit this matrix: factor it afresh on the host.
+            self._rf_setup()
+            x = self._rf_solve_refined(self.rhs)
+            if x is None:
+                x = torch.full_like(self.rhs, float("nan"))
+        return x
+
+    def _rf_matrix(self):
+        torch = self.torch
+        if getattr(self, "_rf_crow", None) is None:
+            self._rf_crow = torch.as_tensor(self.rowptr.astype(np.int64), device=self.dev)
+            self._rf_col = torch.as_tensor(self.colind.astype(np.int64), device=self.dev)
+        return torch.sparse_csr_tensor(self._rf_crow, self._rf_col, self.jac, size=(self.nu, self.nu))
+
+    def _rf_solve_refined(self, b, tol=1e-10, max_refine=2):
+        """Solve with the current factors, then iterative refinement (r = b - J x, x += J^-1 r) up
+        to max_refine times; None if the relative residual stays above tol."""
+        torch = self.torch
+        J = self._rf_matrix()
+        x = b.clone()
         torch.cuda.current_stream(self.dev).synchronize()
         _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
         torch.cuda.synchronize(self.dev)
-        if not bool(torch.isfinite(x).all()):
-            # The kept pivot order failed on this matrix: factor it afresh on the host.
-            self._rf_setup()
-            x = self.rhs.clone()
-            _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
+        bn = float(b.abs().max()) or 1.0
+        for k in range(max_refine + 1):
+            if not bool(torch.isfinite(x).all()):
+                return None
+            r = b - J @ x
+            if float(r.abs().max()) <= tol * bn:
+                return x
+            if k == max_refine:
+                return None
+            d = r.contiguous()
+            torch.cuda.current_stream(self.dev).synchronize()
+            _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(d.data_ptr())), "xd_rf_solve")
             torch.cuda.synchronize(self.dev)
-        return x
+            x = x + d
+        return None
 
     def __del__(self):
         try:

@@ -48,10 +48,13 @@ def test_transient_with_gpu_refactorization_matches_dense():
     c = netlist.random_logic(800, seed=7, n_inputs=8)
     tight = NewtonParams(max_iter=40, rhs_tol=1e-9, delta_x_tol=1e-3, abs_tol=1e-9, rel_tol=1e-6,
                          update_weights_each_iter=False)
+    # The default operating-point tolerances admit millivolt differences between two Newton paths
+    # (deltaXTol 1 on relTol 1e-3 weights); tightened, both solvers land on the same point.
+    tight_dc = NewtonParams(rhs_tol=1e-12, delta_x_tol=1e-3, abs_tol=1e-12, rel_tol=1e-6)
     waves = []
     for solver in ("dense", "rf"):
         g, fam = _pair(c, solver)
-        g.dcop()
+        g.dcop(tight_dc)
         _, w = g.run(0.5e-9, 10e-12, params=tight, record=np.arange(c.n_nodes))
         waves.append(w)
         if solver == "rf":

@@ -503,7 +503,12 @@ class GpuTransient(TransientBase):
             self._lib.xd_rf_destroy(self._rf)
             self._rf = None
         vals = self.jac.cpu().numpy()
-        A = sp.csr_matrix((vals, self.colind, self.rowptr), shape=(self.nu, self.nu))
+        # SuperLU drops entries that are exactly zero, but the refactorization needs L + U to hold
+        # every position of the pattern (a DC matrix has zeros where later matrices have
+        # capacitances): factor with a placeholder far below every pivot in those positions.
+        scale = float(np.abs(vals).max()) or 1.0
+        sym = np.where(vals == 0.0, scale * 1e-30, vals)
+        A = sp.csr_matrix((sym, self.colind, self.rowptr), shape=(self.nu, self.nu))
         lu = spl.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A")
         P = np.argsort(lu.perm_r).astype(np.int32)
         Q = np.argsort(lu.perm_c).astype(np.int32)
@@ -543,36 +548,42 @@ class GpuTransient(TransientBase):
         if x is None:
             # The kept pivot order does not suit this matrix: factor it afresh on the host.
             self._rf_setup()
-            x = self._rf_solve_refined(self.rhs)
+            x = self._rf_solve_refined(self.rhs, accept=True)
             if x is None:
                 x = torch.full_like(self.rhs, float("nan"))
         return x
 
-    def _rf_matrix(self):
+    def _rf_matrices(self):
         torch = self.torch
         if getattr(self, "_rf_crow", None) is None:
             self._rf_crow = torch.as_tensor(self.rowptr.astype(np.int64), device=self.dev)
             self._rf_col = torch.as_tensor(self.colind.astype(np.int64), device=self.dev)
-        return torch.sparse_csr_tensor(self._rf_crow, self._rf_col, self.jac, size=(self.nu, self.nu))
+        mk = lambda v: torch.sparse_csr_tensor(self._rf_crow, self._rf_col, v, size=(self.nu, self.nu),
+                                               check_invariants=False)
+        return mk(self.jac), mk(self.jac.abs())
 
-    def _rf_solve_refined(self, b, tol=1e-10, max_refine=2):
-        """Solve with the current factors, then iterative refinement (r = b - J x, x += J^-1 r) up
-        to max_refine times; None if the relative residual stays above tol."""
+    def _rf_solve_refined(self, b, tol=1e-10, max_refine=3, accept=False):
+        """Solve with the current factors, then iterative refinement (r = b - J x, x += J^-1 r) until
+        the componentwise backward error max_i |r_i| / (|J| |x| + |b|)_i is at most tol (a stable
+        factorization gives a few ulps after one refinement step), at most max_refine times. Returns
+        None when the error stays above tol, or the last iterate when accept is set."""
         torch = self.torch
-        J = self._rf_matrix()
+        J, Ja = self._rf_matrices()
         x = b.clone()
         torch.cuda.current_stream(self.dev).synchronize()
         _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
         torch.cuda.synchronize(self.dev)
-        bn = float(b.abs().max()) or 1.0
+        ab = b.abs()
         for k in range(max_refine + 1):
             if not bool(torch.isfinite(x).all()):
                 return None
             r = b - J @ x
-            if float(r.abs().max()) <= tol * bn:
+            den = Ja @ x.abs() + ab
+            err = torch.where(r == 0, torch.zeros_like(r), r.abs() / den.clamp_min(1e-300))
+            if float(err.max()) <= tol:
                 return x
             if k == max_refine:
-                return None
+                return x if accept else None
             d = r.contiguous()
             torch.cuda.current_stream(self.dev).synchronize()
             _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(d.data_ptr())), "xd_rf_solve")

@@ -20,13 +20,18 @@ typedef struct xd_rf xd_rf;
 
 /* Host inputs, all CSR 0-based, n x n: A's pattern and values, the factors L (unit lower, the
  * unit diagonal stored) and U (upper) of P A Q = L U, and P, Q as arrays: (P A Q)[i][j] =
- * A[P[i]][Q[j]]. */
+ * A[P[i]][Q[j]]. The patterns of L and U must cover every position of P A Q's pattern and its
+ * fill, including positions whose value is zero in this A (a host factorization that drops
+ * numerical zeros must be given placeholders there), because later values may fill them. */
 int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, const double *vals_a, int nnz_l,
                  const int *rowptr_l, const int *colind_l, const double *vals_l, int nnz_u, const int *rowptr_u,
                  const int *colind_u, const double *vals_u, const int *p, const int *q, int cuda_device,
                  xd_rf **out);
 
-/* Refactors with new values of A (device, in A's pattern), keeping the pivot order. */
+/* Refactors with new values of A (device, in A's pattern), keeping the pivot order. A zero pivot
+ * in that order is an error (< 0); a small one is not detected here, so a caller that cannot
+ * bound the growth checks the solution's residual (the transient driver refines and, failing
+ * that, makes a new host factorization). */
 int xd_rf_refactor(xd_rf *rf, const double *d_vals_a);
 
 /* Solves A x = b in place: d_x holds b on entry and x on return (device, length n). */

@@ -44,6 +44,19 @@ EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
 # of an ncu capture at 199,832 instances of the same generator, 90 + 333 B; traffic grows with
 # the instance count), for roofline.traffic.
 EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 333
+# FP64 operations per instance of one evaluation (ncu thread-instruction counters of the same
+# capture: 2,621 DFMA (2 flops each) + 844 DMUL + 511 DADD per instance), for the evaluation
+# kernel's compute roofline against the FP64 FMA-pipe probe.
+EVAL_FP64_FLOPS_PER_INST = 2 * 2621 + 844 + 511
+
+
+def eval_shape(lib, h):
+    """The evaluation kernel's launch shape that the autotuner picked for a context."""
+    import ctypes
+
+    blk, minb = ctypes.c_int(), ctypes.c_int()
+    lib.xd_eval_variant_info(lib.xd_get_eval_variant(h), ctypes.byref(blk), ctypes.byref(minb))
+    return {"block": blk.value, "min_blocks_per_sm": minb.value}
 
 
 def batched_section(args, dev_id):
@@ -98,14 +111,13 @@ def batched_section(args, dev_id):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         res[mode] = {"ms_per_load": ms, "loads_per_s": n / (ms * 1e-3)}
-    blk, minb = ctypes.c_int(), ctypes.c_int()
-    _native.load().xd_eval_launch_shape(dev._h, ctypes.byref(blk), ctypes.byref(minb))
+    shape = eval_shape(_native.load(), dev._h)
     dev.close()
     return {"workload": f"256 seeded gate netlists (sizes log-uniform 1k-20k, {n} BSIM4 MOSFETs in all, {nu} "
                         f"unknowns, {nnz} nnz), per-circuit DELVTO ~ N(0, 30 mV) and TOXE x U[0.98, 1.02] "
                         f"(512 model cards), one evaluation launch per load",
             "circuits": int(len(b.sizes)), "mosfets": n, **res,
-            "eval_launch_shape": {"block": blk.value, "min_blocks_per_sm": minb.value}}
+            "eval_launch_shape": shape}
 
 
 def transient_section(args):
@@ -381,8 +393,7 @@ def main():
     launches = lib.xd_launches_per_load(dev._h)
     import ctypes
 
-    blk, minb = ctypes.c_int(), ctypes.c_int()
-    lib.xd_eval_launch_shape(dev._h, ctypes.byref(blk), ctypes.byref(minb))
+    shape = eval_shape(lib, dev._h)
     stream = torch.cuda.current_stream()
     f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
     rng = np.random.default_rng(args.seed + 17 * rank)
@@ -539,8 +550,10 @@ def main():
                              f"traffic = ncu DRAM bytes per instance ({EVAL_DRAM_BYTES_PER_INST_NCU} B at 199,832 "
                              "instances, profiles/bsim4_eval_kernel_scale.md) x instances"},
         "kernels_ms": {"eval": t_eval, "gather_vectors": t_vec, "gather_matrices": t_mat},
-        "eval_launch_shape": {"block": blk.value, "min_blocks_per_sm": minb.value},
-        "fp64": {"probe_peak_tflops": fp64_peak_tflops},
+        "eval_launch_shape": shape,
+        "fp64": {"probe_peak_tflops": fp64_peak_tflops, "flops_per_instance": EVAL_FP64_FLOPS_PER_INST,
+                 "eval_achieved_tflops": EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12,
+                 "eval_frac": EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12 / fp64_peak_tflops},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
     }

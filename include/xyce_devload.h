@@ -166,6 +166,13 @@ int xd_launches_per_load(const xd_ctx *ctx);
 /* Launch shape (threads per block, minimum resident blocks per SM) that xd_create's autotuner
  * selected for the evaluation kernel after timing every candidate on the circuit. */
 int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks);
+/* The autotuner's candidates: xd_num_eval_variants() of them; xd_eval_variant_info gives the
+ * launch shape of candidate v; xd_get_eval_variant / xd_set_eval_variant read and override the
+ * context's choice (every candidate computes identical results; tests force each in turn). */
+int xd_num_eval_variants(void);
+int xd_eval_variant_info(int v, int *block, int *min_blocks);
+int xd_get_eval_variant(const xd_ctx *ctx);
+int xd_set_eval_variant(xd_ctx *ctx, int v);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);
 
 /* Allocation-free load (no counterpart in the reference: it is for callers of this library).

@@ -69,10 +69,13 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
     return report
 
 
-def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, charges_in_dc=False, level=14):
+def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, charges_in_dc=False, level=14,
+                 eval_variant=None):
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, inst_model, inst_nodes, params = family_inputs(c, cards, extra_params)
     dev = MosfetDevice(cards, inst_model, inst_nodes, params, (rowptr, colind), c.n_unknowns, level=level)
+    if eval_variant is not None:
+        assert dev._lib.xd_set_eval_variant(dev._h, eval_variant) == 0
     orc = OracleRun(c, cards, inst_model, inst_nodes, params, rowptr, colind, level=level,
                     n_sta_slots=dev.n_state_slots)
     gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)

@@ -60,6 +60,46 @@ def test_parity_model_card_variants():
     print("worst error / tolerance:", worst)
 
 
+def _num_variants():
+    from xyce_b200 import _native
+    return _native.load().xd_num_eval_variants()
+
+
+@pytest.mark.parametrize("v", range(6))
+def test_parity_every_eval_launch_variant(v):
+    """The autotuner may pick any launch shape of the evaluation kernel; each is held to the
+    oracle, with an instance count that leaves a partial last block."""
+    if v >= _num_variants():
+        pytest.skip("no such variant")
+    c = netlist.random_logic(1500, seed=21)
+    worst = _run_sequence(c, None, TRANSIENT_SEQ[:3] + DC_SEQ[:2], eval_variant=v)
+    print("variant", v, "worst error / tolerance:", worst)
+
+
+def test_eval_launch_variants_bitwise_identical():
+    c = netlist.random_logic(5000, seed=4)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c)
+    n = im.shape[0]
+    sol = np.random.default_rng(1).uniform(0, 1.2, c.n_unknowns)
+    sto = np.random.default_rng(2).uniform(-0.2, 1.2, 14 * n)
+    z3 = np.zeros(3 * n)
+    ref = None
+    for v in range(_num_variants()):
+        dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
+        assert dev._lib.xd_set_eval_variant(dev._h, v) == 0
+        gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
+        out = gpu.load(SolverFlags(newton_iter=1), sol, z3, z3, sto.copy(), sto.copy())
+        dev.close()
+        if ref is None:
+            ref = out
+            continue
+        for k in ref:
+            if k == "abs":
+                continue
+            assert np.array_equal(ref[k], out[k], equal_nan=True), (v, k)
+
+
 def test_parity_inverter_ring_bsim4():
     c = netlist.inverter_ring(101, vdd=1.8)
     worst = _run_sequence(c, None, TRANSIENT_SEQ, vrange=(0.0, 1.8))

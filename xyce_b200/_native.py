@@ -89,6 +89,10 @@ SIGNATURES = {
     "xd_copy_stamps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "xd_launches_per_load": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_eval_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
+    "xd_num_eval_variants": (ctypes.c_int, []),
+    "xd_eval_variant_info": (ctypes.c_int, [ctypes.c_int, _ip, _ip]),
+    "xd_get_eval_variant": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_set_eval_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "xd_load_static_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
     "xd_probe_fp64_fma": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "xd_load_assign": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),

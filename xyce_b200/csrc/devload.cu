@@ -793,6 +793,23 @@ int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks) {
   return 0;
 }
 
+int xd_num_eval_variants(void) { return kNumEvalVariants; }
+
+int xd_eval_variant_info(int v, int *block, int *min_blocks) {
+  if (v < 0 || v >= kNumEvalVariants || !block || !min_blocks) return fail(-1, "bad variant query");
+  *block = kEvalVariants[v].block;
+  *min_blocks = kEvalVariants[v].min_blocks;
+  return 0;
+}
+
+int xd_get_eval_variant(const xd_ctx *ctx) { return ctx ? ctx->eval_variant : -1; }
+
+int xd_set_eval_variant(xd_ctx *ctx, int v) {
+  if (!ctx || v < 0 || v >= kNumEvalVariants) return fail(-1, "bad evaluation variant");
+  ctx->eval_variant = v;
+  return 0;
+}
+
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream) {
   if (!d_out || blocks <= 0 || iters <= 0) return fail(-1, "bad probe arguments");
   fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d_out, iters);

@@ -10,8 +10,9 @@
  * stamps do not depend on the solution (resistors N_DEV_Resistor.C:1075-1161, capacitors
  * N_DEV_Capacitor.C:1821-2002, independent voltage sources N_DEV_Vsrc.C:941-1028): their dF/dx and
  * dQ/dx are constant CSR value arrays, their F and Q are those matrices times x, and the source
- * values enter through a vector b(t) (F = ... - b). An optional shunt conductance on every unknown
- * supports gmin stepping, the operating-point continuation of the reference's nonlinear solver.
+ * values enter through a vector b(t) (F = ... - b). An optional shunt conductance on every node row
+ * supports gmin stepping, the operating-point continuation of the reference's nonlinear solver
+ * (N_NLS_NOX_AugmentLinSys_GStepping.C:142-197 augments the voltage nodes).
  *
  * Buffers are caller-owned device pointers; calls are stream-ordered and capturable. Status: 0 =
  * ok, < 0 = error (xd_last_error()).
@@ -37,7 +38,8 @@ typedef struct xd_tia xd_tia;
 typedef struct xd_tia_coef {
   int mode;
   double qscale, fscale, inv_h, hist_scale;
-  double gshunt; /* conductance from every unknown to ground (gmin stepping); 0 for none */
+  double gshunt; /* conductance to ground on every row whose diagonal is in the pattern, i.e. the
+                   node rows, not a voltage source's branch row (gmin stepping); 0 for none */
 } xd_tia_coef;
 
 /* Uploads the CSR pattern (rows = unknowns). */
@@ -46,7 +48,7 @@ int xd_tia_destroy(xd_tia *t);
 
 /* Per row i, in one pass over the row's entries k:
  *   jac[k]   = qscale (dqdx[k] + lin_dqdx[k]) + fscale (dfdx[k] + lin_dfdx[k] + gshunt [k diagonal])
- *   F_i      = f[i] + sum_k lin_dfdx[k] x[col k] + gshunt x[i] - b[i]
+ *   F_i      = f[i] + sum_k lin_dfdx[k] x[col k] + gshunt x[i] [row i has its diagonal] - b[i]
  *   Q_i      = q[i] + sum_k lin_dqdx[k] x[col k]
  *   rhs[i]   as above (limiter corrections dfdxdvp / dqdxdvp, when non-null, added last);
  *   f_tot[i] = F_i and q_tot[i] = Q_i when those pointers are non-null.
@@ -59,6 +61,22 @@ int xd_tia_combine(xd_tia *t, const xd_tia_coef *coef, const double *d_x, const 
                    const double *d_f, const double *d_q, const double *d_dfdxdvp, const double *d_dqdxdvp,
                    const double *d_b, const double *d_qn0, const double *d_fhist, double *d_jac,
                    double *d_rhs, double *d_q_tot, double *d_f_tot, void *stream);
+
+/* Small dense direct solve of the Newton system J x = rhs (J in the pattern's CSR values), for
+ * circuits of at most XD_DENSE_MAX_N unknowns; stands in for the reference's direct solve (KLU
+ * through Amesos, src/LinearAlgebraServicesPKG/src/N_LAS_AmesosSolver.C:160, 305) where the
+ * system is small enough for one SM's shared memory. Gaussian elimination with partial pivoting
+ * (the first row of largest magnitude in the column; rows swapped whole, LAPACK's convention),
+ * then back substitution. d_lu (n * n doubles, row-major: U on and above the diagonal, the unit
+ * lower factor's multipliers below) and d_piv (n ints: row k was swapped with row piv[k] at step
+ * k) receive the factors when non-null; d_info (may be null) receives 0, or k + 1 for the first
+ * column k without a nonzero pivot (the solution is then not finite). One kernel launch. */
+#define XD_DENSE_MAX_N 160
+int xd_tia_dense_solve(xd_tia *t, const double *d_jac, const double *d_rhs, double *d_lu, int *d_piv, double *d_x,
+                       int *d_info, void *stream);
+/* Solves with factors kept from xd_tia_dense_solve (a chord step). */
+int xd_tia_dense_resolve(xd_tia *t, const double *d_lu, const int *d_piv, const double *d_rhs, double *d_x,
+                         void *stream);
 
 #ifdef __cplusplus
 }

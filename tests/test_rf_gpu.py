@@ -63,3 +63,34 @@ def test_transient_with_gpu_refactorization_matches_dense():
         g.close()
         fam.close()
     assert np.abs(waves[0] - waves[1]).max() < 1e-8
+
+
+def test_placed_netlist_transient_refactorization_matches_oracle():
+    """A placed (locality-wired) BSIM4 gate netlist: operating point from the logic-level starting
+    iterate, then 0.3 ns on the GPU refactorization path, against the same driver on the oracle's
+    loads with a host LU; waveforms within reltol 1e-3 / abstol 1e-12."""
+    from tests.transient_oracle import OracleTransient
+
+    c = netlist.random_logic(2500, seed=4, n_inputs=16, locality=64)
+    tight = NewtonParams(max_iter=40, rhs_tol=1e-9, delta_x_tol=1e-3, abs_tol=1e-9, rel_tol=1e-6,
+                         update_weights_each_iter=False)
+    tight_dc = NewtonParams(rhs_tol=1e-12, delta_x_tol=1e-3, abs_tol=1e-12, rel_tol=1e-6)
+    rec = np.arange(0, c.n_nodes, max(1, c.n_nodes // 50))
+    x0 = netlist.logic_initial_guess(c)
+    g, fam = _pair(c, "rf")
+    rowptr, colind = netlist.jacobian_pattern(c)
+    o = OracleTransient(c, None, rowptr, colind, level=14, solver="splu")
+    waves = []
+    for s in (g, o):
+        s.dcop(tight_dc, x0=x0)
+        waves.append(s.run(0.3e-9, 10e-12, params=tight, record=rec))
+    (tg, wg), (to, wo) = waves
+    assert np.array_equal(tg, to)
+    bound = 1e-3 * np.abs(wo).max(axis=0, keepdims=True) + 1e-12
+    worst = float((np.abs(wg - wo) / bound).max())
+    assert worst <= 1.0, worst
+    assert g.stats.host_factorizations < g.stats.factorizations // 4, g.stats
+    print("placed netlist: worst error / bound", worst, "host factorizations", g.stats.host_factorizations,
+          "of", g.stats.factorizations)
+    g.close()
+    fam.close()

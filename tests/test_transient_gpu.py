@@ -53,12 +53,18 @@ def test_combine_kernel_matches_numpy():
     for buf in (g.f, g.q, g.jf, g.jq, g.b):
         buf.copy_(T(rng.standard_normal(buf.shape[0])))
     qn0, fh = T(rng.standard_normal(nu)), T(rng.standard_normal(nu))
-    for mode, h, order in ((0, None, 1), (1, 1e-11, 1), (1, 3e-12, 2)):
+    rows = np.repeat(np.arange(nu), np.diff(g.rowptr))
+    diag = (rows == g.colind).astype(float)
+    has_diag = np.zeros(nu)
+    has_diag[rows[rows == g.colind]] = 1.0
+    assert has_diag[:c.n_nodes].all() and not has_diag[c.n_nodes:].any()  # branch rows have no diagonal
+    for mode, h, order, gsh in ((0, None, 1, 0.0), (1, 1e-11, 1, 0.0), (1, 3e-12, 2, 0.0), (0, None, 1, 1e-3)):
+        g.gshunt = gsh
         g._combine(mode, h, order, qn0, fh)
         x = g.x.cpu().numpy()
         A_f = o.Af
-        jf = g.jf.cpu().numpy() + g.lin.lin_f
-        F = g.f.cpu().numpy() + A_f @ x - g.b.cpu().numpy()
+        jf = g.jf.cpu().numpy() + g.lin.lin_f + gsh * diag
+        F = g.f.cpu().numpy() + A_f @ x + gsh * has_diag * x - g.b.cpu().numpy()
         if mode == 0:
             jac, rhs = jf, -F
         else:
@@ -71,6 +77,7 @@ def test_combine_kernel_matches_numpy():
         assert np.allclose(g.jac.cpu().numpy(), jac, rtol=1e-13, atol=1e-30), mode
         assert np.allclose(g.rhs.cpu().numpy(), rhs, rtol=1e-12, atol=1e-18 * np.abs(rhs).max()), mode
         assert np.allclose(g.ftot.cpu().numpy(), F, rtol=1e-12, atol=1e-18 * np.abs(F).max()), mode
+    g.gshunt = 0.0
     g.close()
 
 
@@ -110,3 +117,83 @@ def test_gate_netlist_bsim4_waveforms_match_oracle():
     worst = _check_waves(tg, wg, to, wo)
     print("gates: worst waveform error / bound", worst, "GPU Newton its/step", np.mean(g.stats.newton_iters))
     g.close()
+
+
+def test_graph_replayed_newton_matches_eager_bitwise():
+    """Each Newton iteration replayed as a CUDA graph computes exactly what the eager iteration
+    does: same iteration counts, bit-identical waveforms (ring from the operating point plus a
+    kick, reference transient tolerances, so the run includes step-size and order changes)."""
+    c = netlist.inverter_ring(101, vdd=1.8)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, netlist.ring_bsim3_cards())
+    out = []
+    for graphs in (False, True):
+        fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=9)
+        g = GpuTransient(c, fam, rowptr, colind, graphs=graphs)
+        assert g.graphs == graphs
+        g.dcop()
+        x0 = g.x.clone()
+        x0[1] += 0.1
+        g.set_initial_state(x0)
+        t, w = g.run(2e-9, 10e-12, record=np.arange(c.n_unknowns))
+        out.append((t, w, list(g.stats.newton_iters), g.stats.wall_s))
+        g.close()
+        fam.close()
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    print(f"ring 2 ns: eager {out[0][3]:.3f} s, graphs {out[1][3]:.3f} s")
+
+
+def test_small_dense_solve_matches_numpy():
+    """The one-SM dense solve (include/xyce_tia.h) against numpy on circuit-like sparse matrices
+    (row pivoting needed: zero diagonals of source branch rows), a dense matrix, the size limit,
+    a singular matrix (info set, solution not finite), and solves with kept factors."""
+    from xyce_b200 import _native
+
+    lib = _native.load()
+    rng = np.random.default_rng(3)
+    T = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    for n, density in ((1, 1.0), (7, 0.5), (33, 0.1), (103, 0.03), (160, 0.02), (150, 1.0)):
+        A = np.where(rng.random((n, n)) < density, rng.standard_normal((n, n)), 0.0)
+        A[np.arange(n), np.arange(n)] += np.where(rng.random(n) < 0.2, 0.0, 3.0)  # some zero diagonals
+        A[np.arange(n), (np.arange(n) + 1) % n] += 1.0  # keeps it nonsingular with zero diagonals
+        rows, cols = np.nonzero(np.ones((n, n)) if density == 1.0 else (A != 0) | np.eye(n, dtype=bool))
+        rowptr = np.zeros(n + 1, np.int32)
+        np.add.at(rowptr, rows + 1, 1)
+        rowptr = np.cumsum(rowptr).astype(np.int32)
+        colind = cols.astype(np.int32)
+        csr = _native.XdCsr(n, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
+        h = ctypes.c_void_p()
+        assert lib.xd_tia_create(ctypes.byref(csr), 0, ctypes.byref(h)) == 0
+        vals, b = T(A[rows, cols]), T(rng.standard_normal(n))
+        lu, piv, x, info = T(np.zeros(n * n)), T(np.zeros(n), torch.int32), T(np.zeros(n)), T([7], torch.int32)
+        assert lib.xd_tia_dense_solve(h, p(vals), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+        torch.cuda.synchronize()
+        ref = np.linalg.solve(A, b.cpu().numpy())
+        err = np.abs(x.cpu().numpy() - ref).max() / np.abs(ref).max()
+        assert int(info.item()) == 0 and err < 1e-10, (n, err)
+        b2 = T(rng.standard_normal(n))
+        x2 = T(np.zeros(n))
+        assert lib.xd_tia_dense_resolve(h, p(lu), p(piv), p(b2), p(x2), None) == 0
+        torch.cuda.synchronize()
+        ref2 = np.linalg.solve(A, b2.cpu().numpy())
+        assert np.abs(x2.cpu().numpy() - ref2).max() / np.abs(ref2).max() < 1e-10, n
+        if n == 33:
+            A0 = A.copy()
+            A0[:, 5] = 0.0  # singular: column 5 has no pivot
+            assert lib.xd_tia_dense_solve(h, p(T(A0[rows, cols])), p(b), None, None, p(x), p(info), None) == 0
+            torch.cuda.synchronize()
+            assert int(info.item()) > 0 and not np.isfinite(x.cpu().numpy()).all()
+        lib.xd_tia_destroy(h)
+    # Beyond the size limit the call is refused.
+    n = _native.XD_DENSE_MAX_N + 1
+    rowptr = np.arange(n + 1, dtype=np.int32)
+    colind = np.arange(n, dtype=np.int32)
+    csr = _native.XdCsr(n, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
+    h = ctypes.c_void_p()
+    assert lib.xd_tia_create(ctypes.byref(csr), 0, ctypes.byref(h)) == 0
+    v = T(np.ones(n))
+    assert lib.xd_tia_dense_solve(h, p(v), p(v), None, None, p(v), None, None) < 0
+    lib.xd_tia_destroy(h)

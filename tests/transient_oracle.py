@@ -28,6 +28,8 @@ class OracleTransient(TransientBase):
         self._r = None
         rows = np.repeat(np.arange(nu), np.diff(self.rowptr))
         self._diag = (rows == self.colind).astype(float)
+        self._has_diag = np.zeros(nu)
+        self._has_diag[rows[rows == self.colind]] = 1.0  # the shunt's rows: node rows, not branch rows
 
     def _load(self, flags: SolverFlags):
         r = self.orc.load(flags, self.x.numpy(), self.next_sta.numpy(), self.curr_sta.numpy(), self.next_sto.numpy(),
@@ -45,7 +47,7 @@ class OracleTransient(TransientBase):
         F = r["f"] + self.Af @ x
         if self.gshunt:
             jf = jf + self.gshunt * self._diag
-            F = F + self.gshunt * x
+            F = F + self.gshunt * self._has_diag * x
         F = F - self.b.numpy()
         self.ftot.copy_(torch.as_tensor(F))
         if mode == 0:

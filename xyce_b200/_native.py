@@ -72,6 +72,8 @@ class XdAdamArgs(ctypes.Structure):
 
 
 # Every symbol the headers declare, with its ctypes signature.
+XD_DENSE_MAX_N = 160  # include/xyce_tia.h
+
 SIGNATURES = {
     "xd_create": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), ctypes.POINTER(XdCsr), ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_void_p)]),
@@ -99,6 +101,8 @@ SIGNATURES = {
     "xd_tia_create": (ctypes.c_int, [ctypes.POINTER(XdCsr), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "xd_tia_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
+    "xd_tia_dense_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
+    "xd_tia_dense_resolve": (ctypes.c_int, [ctypes.c_void_p] * 6),
     "xd_gemm_bf16": (ctypes.c_int, [ctypes.POINTER(XdGemmArgs), ctypes.c_int, ctypes.c_void_p]),
     "xd_mlp_input_layer": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

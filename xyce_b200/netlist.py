@@ -96,8 +96,14 @@ def _loguniform(rng, lo, hi, n):
 
 
 def random_logic(n_mos_target: int, seed: int = 0, n_inputs: int = 64, wire_segments: int = 2, vdd: float = 1.2,
-                 wn: float = 1e-6, wp: float = 2e-6, length: float = 0.18e-6, edge: float = 50e-12) -> Circuit:
-    """Random INV/NAND2/NOR2 netlist with about ``n_mos_target`` MOSFETs (see module doc)."""
+                 wn: float = 1e-6, wp: float = 2e-6, length: float = 0.18e-6, edge: float = 50e-12,
+                 locality: int = 0) -> Circuit:
+    """Random INV/NAND2/NOR2 netlist with about ``n_mos_target`` MOSFETs (see module doc).
+
+    ``locality`` = 0: a gate pin takes any open fan-out slot of an earlier net (the wiring is an
+    expander graph: a direct factorization of its matrix fills in almost completely). K > 0: a pin
+    takes one of the K most recently opened slots, as in a placed netlist where a gate drives
+    nearby gates; the fan-out distribution is unchanged."""
     rng = np.random.default_rng(seed)
     # Gate types: 0 INV (2 MOSFETs, 1 input), 1 NAND2 (4, 2), 2 NOR2 (4, 2); mean 10/3 MOSFETs.
     n_gates = max(1, int(round(n_mos_target * 3 / 10)))
@@ -125,7 +131,7 @@ def random_logic(n_mos_target: int, seed: int = 0, n_inputs: int = 64, wire_segm
     for g in range(n_gates):
         for _ in range(int(n_pins[g])):
             if pool:
-                j = int(rng.integers(0, len(pool)))
+                j = int(rng.integers(max(0, len(pool) - locality) if locality > 0 else 0, len(pool)))
                 pool[j], pool[-1] = pool[-1], pool[j]
                 pin_net[pin] = pool.pop()
             else:
@@ -183,7 +189,57 @@ def random_logic(n_mos_target: int, seed: int = 0, n_inputs: int = 64, wire_segm
     return Circuit(n_nodes=node, mos_type=mos_type, mos_nodes=mos_nodes, mos_w=mos_w, mos_l=mos_l,
                    res_nodes=res_nodes.astype(np.int32), res_value=res_value, cap_nodes=cap_nodes.astype(np.int32),
                    cap_value=cap_value, vsrc_nodes=vsrc_nodes.astype(np.int32), vsrc_dc=vsrc_dc, vsrc_pwl=pwl,
-                   vdd=vdd, meta=dict(kind="random_logic", seed=seed, n_gates=n_gates, n_inputs=n_inputs))
+                   vdd=vdd, meta=dict(kind="random_logic", seed=seed, n_gates=n_gates, n_inputs=n_inputs,
+                                      logic=dict(gtype=gtype, outs=outs, mids=mids, inputs=inputs, net_src=net_src,
+                                                 pin_net=pin_net, first_pin=first_pin, n_pins=n_pins,
+                                                 branch_net=branch_net, ladder=ladder, vdd_node=VDD)))
+
+
+def logic_initial_guess(c: Circuit, t: float = 0.0) -> np.ndarray:
+    """Node voltages of a random_logic netlist at the logic levels its inputs set at time t: the
+    primary inputs' source values propagated through the gates in order (every gate reads earlier
+    nets only), each wire ladder at its driving net's voltage, series-stack middle nodes at the
+    rail their conducting transistor ties them to. A starting iterate for the operating point's
+    Newton solve, as a .NODESET gives one; the solve itself settles the analogue values."""
+    lg = c.meta["logic"]
+    x = np.zeros(c.n_unknowns)
+    vdd = c.vdd
+    x[lg["vdd_node"]] = vdd
+    n_in = lg["inputs"].shape[0]
+    net_v = np.zeros(lg["net_src"].shape[0])
+    for k in range(n_in):
+        times, vals = c.vsrc_pwl[1 + k]
+        net_v[k] = _pwl_at(times, vals, t)
+    hi = lambda v: v > 0.5 * vdd
+    gtype, first, pin_net = lg["gtype"], lg["first_pin"], lg["pin_net"]
+    mids = lg["mids"]
+    for g in range(gtype.shape[0]):
+        a = hi(net_v[pin_net[first[g]]])
+        if gtype[g] == 0:
+            out = not a
+        else:
+            b = hi(net_v[pin_net[first[g] + 1]])
+            if gtype[g] == 1:  # NAND2: middle node between the series NMOS
+                out = not (a and b)
+                x[mids[g]] = 0.0 if b else (vdd if a else 0.0)
+            else:  # NOR2: middle node between the series PMOS
+                out = not (a or b)
+                x[mids[g]] = vdd if not a else (vdd if out else 0.0)
+        net_v[n_in + g] = vdd if out else 0.0
+        x[lg["outs"][g]] = net_v[n_in + g]
+    x[lg["inputs"]] = net_v[:n_in]
+    x[lg["ladder"]] = net_v[lg["branch_net"]][:, None]
+    return x
+
+
+def _pwl_at(times, values, t):
+    if t <= times[0]:
+        return float(values[0]) if times[0] == 0.0 else 0.0
+    if t >= times[-1]:
+        return float(values[-1])
+    k = int(np.searchsorted(times, t, side="right"))
+    t0, t1, v0, v1 = times[k - 1], times[k], values[k - 1], values[k]
+    return float(v0 + (v1 - v0) * (t - t0) / (t1 - t0))
 
 
 # Model cards for the BSIM3 ring-oscillator workload (W/L = 1u/0.18u, PMOS W = 2u, VDD = 1.8 V).

@@ -281,7 +281,13 @@ class TransientBase:
             import scipy.sparse as sp
             import scipy.sparse.linalg as spl
             J = sp.csr_matrix((self.jac.cpu().numpy(), self.colind, self.rowptr), shape=(self.nu, self.nu))
-            self._lu = spl.splu(J.tocsc())
+            self.stats.factorizations += 1
+            try:
+                self._lu = spl.splu(J.tocsc())
+            except RuntimeError:  # exactly singular: a Newton failure, as with the dense factorization
+                self._lu = None
+                return torch.full_like(self.rhs, float("nan"))
+            return self._solve_factored()
         self.stats.factorizations += 1
         return self._solve_factored()
 
@@ -339,45 +345,73 @@ class TransientBase:
     def dcop(self, params: NewtonParams | None = None, x0=None, t0: float = 0.0) -> int:
         """Operating point at time t0 (sources at their transient values, as the reference does
         for the operating point of a transient), with charges computed (tranop); leaves Q(t0) and
-        F(t0) in q_tot / f_tot and the device history rotated. Plain Newton first; if it fails,
-        gmin stepping: a shunt conductance from every unknown to ground, lowered a decade at a
-        time from 1e-2 S, each stage starting from the previous one's solution, then removed.
-        Returns the total number of Newton updates."""
+        F(t0) in q_tot / f_tot and the device history rotated. Newton from x0 (zero if not given)
+        first; if it fails,
+        gmin stepping as the reference's continuation does it (N_NLS_NOX_Interface.C:1351-1380,
+        N_NLS_NOX_AugmentLinSys_GStepping.C:125-131): a shunt conductance 10^p - 10^-4 from every
+        unknown to ground, p stepped from 4 to -4 by natural continuation with an adaptive step
+        (first step -2, halved on a failed stage, grown by the LOCA rule with aggressiveness 0.01;
+        at most 400 stages of at most 20 Newton iterations), each stage starting from the last
+        converged one. Returns the total number of Newton updates."""
         prm = params or NewtonParams.dc()
         start = self.torch.zeros_like(self.x)
         if x0 is not None:
             start.copy_(self.torch.as_tensor(x0, dtype=self.torch.float64))
         self._set_sources(t0)
 
+        # The first load of a solve from zero initialises the junction voltages (the models ignore
+        # the iterate there); a supplied starting iterate (x0, as a .NODESET gives) is evaluated
+        # from the first load on.
         def flags(it, first=True):
             return SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=it,
-                               init_jct=1 if (it == 0 and first) else 0, gmin=self.gmin,
+                               init_jct=1 if (it == 0 and first and x0 is None) else 0, gmin=self.gmin,
                                voltlim=int(self.limiting))
 
         self.x.copy_(start)
         self.gshunt = 0.0
         total = self._newton(prm, flags, mode=0)
         if total < 0:
-            total = 0
-            self.x.copy_(start)
-            self.next_sta.zero_()
-            self.next_sto.zero_()
-            self.curr_sta.zero_()
-            self.curr_sto.zero_()
-            first = True
-            for g in [10.0 ** (-k) for k in range(2, 13)] + [0.0]:
-                self.gshunt = g
-                n_it = self._newton(prm, lambda it, first=first: flags(it, first), mode=0)
-                if n_it < 0:
-                    self.gshunt = 0.0
-                    raise RuntimeError(f"operating point did not converge (gmin stepping at {g:g} S)")
-                total += n_it
-                first = False
-                self.curr_sto.copy_(self.next_sto)
-            self.gshunt = 0.0
+            total = self._gmin_stepping(prm, start, flags)
+        self.gshunt = 0.0
         self._history_here()
         self._accept_point()
         return total
+
+    def _gmin_stepping(self, prm: NewtonParams, start, flags) -> int:
+        p, p_end, step = 4.0, -4.0, -2.0
+        max_stages, stage_iters, aggressiveness, min_step = 400, 20, 0.01, 1e-6
+        stage_prm = NewtonParams(max_iter=min(stage_iters, prm.max_iter), rhs_tol=prm.rhs_tol,
+                                 delta_x_tol=prm.delta_x_tol, abs_tol=prm.abs_tol, rel_tol=prm.rel_tol,
+                                 update_weights_each_iter=prm.update_weights_each_iter)
+        self.x.copy_(start)
+        for t in (self.next_sta, self.next_sto, self.curr_sta, self.curr_sto):
+            t.zero_()
+        total, first, saved = 0, True, None
+        p_try = p
+        for _ in range(max_stages):
+            self.gshunt = 10.0 ** p_try - 10.0 ** p_end
+            n_it = self._newton(stage_prm, lambda it, first=first: flags(it, first), mode=0)
+            if n_it >= 0:
+                total += n_it
+                first = False
+                self.curr_sto.copy_(self.next_sto)
+                saved = [t.clone() for t in (self.x, self.next_sta, self.next_sto, self.curr_sto)]
+                p = p_try
+                if p <= p_end:
+                    return total
+                frac = (stage_iters - n_it) / (stage_iters - 1)
+                step *= 1.0 + aggressiveness * max(frac, 0.0) ** 2
+            else:
+                if saved is None:
+                    break  # the heavily shunted start itself failed
+                for t, v in zip((self.x, self.next_sta, self.next_sto, self.curr_sto), saved):
+                    t.copy_(v)
+                step *= 0.5
+                if abs(step) < min_step:
+                    break
+            p_try = max(p + step, p_end)
+        self.gshunt = 0.0
+        raise RuntimeError(f"operating point did not converge (gmin stepping stopped at 10^{p_try:.3g} S)")
 
     def _accept_point(self):
         """The accepted point's device history becomes the current one."""
@@ -466,12 +500,18 @@ class GpuTransient(TransientBase):
     ``family``: the circuit's MOSFETs as one ``MosfetDevice`` built on the pattern (rowptr, colind).
     """
 
-    def __init__(self, c, family: MosfetDevice, rowptr, colind, device=0, solver="auto", gmin=1e-12):
+    def __init__(self, c, family: MosfetDevice, rowptr, colind, device=0, solver="auto", gmin=1e-12,
+                 graphs=True):
         import torch
 
         super().__init__(c, family.n_state, family.n_store, rowptr, colind, torch.device("cuda", device), solver,
                          gmin)
         self.fam = family
+        # With the dense solve, each Newton iteration (factor, solve, update, norms, device loads,
+        # combine) replays as one CUDA graph, one per distinct (flags, step, method) combination.
+        self.graphs = bool(graphs) and self.solver == "dense"
+        self._graphs = {}
+        self._graph_pool = None
         lib = _native.load()
         self._lib = lib
         csr = _native.XdCsr(self.nu, self.rowptr.ctypes.data_as(_native._ip), self.colind.ctypes.data_as(_native._ip))
@@ -481,11 +521,18 @@ class GpuTransient(TransientBase):
         T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=self.dev).contiguous()
         z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
         self.lin_f, self.lin_q = T(self.lin.lin_f), T(self.lin.lin_q)
+        # Circuits of at most XD_DENSE_MAX_N unknowns take the library's one-SM dense solve.
+        self._small = self.solver == "dense" and self.nu <= _native.XD_DENSE_MAX_N
+        if self._small:
+            self._lu_d = z(self.nu * self.nu)
+            self._piv_d = torch.zeros(self.nu, dtype=torch.int32, device=self.dev)
+            self._dx_d = z(self.nu)
         # Family outputs (stored by xd_load_assign; entries the family does not stamp stay zero).
         self.f, self.q, self.fx, self.qx = z(self.nu), z(self.nu), z(self.nu), z(self.nu)
         self.jf, self.jq = z(self.nnz), z(self.nnz)
 
     def close(self):
+        self._graphs = {}
         if getattr(self, "_tia", None) is not None and self._tia.value:
             self._lib.xd_tia_destroy(self._tia)
             self._tia = None
@@ -509,7 +556,12 @@ class GpuTransient(TransientBase):
         scale = float(np.abs(vals).max()) or 1.0
         sym = np.where(vals == 0.0, scale * 1e-30, vals)
         A = sp.csr_matrix((sym, self.colind, self.rowptr), shape=(self.nu, self.nu))
-        lu = spl.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A")
+        # Fill-reducing order on A + A^T with threshold pivoting that prefers the diagonal (a row
+        # swap only when the diagonal is below 0.1 of the column's largest entry), as circuit
+        # solvers such as KLU factor: strict partial pivoting destroys the order's sparsity on
+        # MNA matrices (66M instead of 2M nonzeros at 200k unknowns).
+        lu = spl.splu(A.tocsc(), permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.1,
+                      options=dict(SymmetricMode=True))
         P = np.argsort(lu.perm_r).astype(np.int32)
         Q = np.argsort(lu.perm_c).astype(np.int32)
         L = lu.L.tocsr()
@@ -531,27 +583,44 @@ class GpuTransient(TransientBase):
         self._rf = h
         self.stats.host_factorizations += 1
 
+    def _rf_try_setup(self):
+        """_rf_setup, with a singular matrix (the library's zero pivot, or the host factorization's)
+        reported as False, like a failed dense factorization, so that Newton fails the step."""
+        try:
+            self._rf_setup()
+            return True
+        except (_native.NativeError, RuntimeError):
+            if getattr(self, "_rf", None) is not None and self._rf.value:
+                self._lib.xd_rf_destroy(self._rf)
+            self._rf = None
+            return False
+
     def _solve_rf(self):
         torch = self.torch
+        self.stats.factorizations += 1
+        self._lu = True
+        nan = lambda: torch.full_like(self.rhs, float("nan"))
+        fresh = False
         if getattr(self, "_rf", None) is None or not self._rf.value:
-            self._rf_setup()
+            if not self._rf_try_setup():
+                return nan()
+            fresh = True
         else:
             torch.cuda.current_stream(self.dev).synchronize()  # values complete before the library reads them
             rc = self._lib.xd_rf_refactor(self._rf, ctypes.c_void_p(self.jac.data_ptr()))
             if rc != 0:
                 # A zero pivot in the kept pivot order (the matrices of a DC solve and of a time step
                 # differ in which entries dominate): factor this matrix afresh on the host.
-                self._rf_setup()
-        self.stats.factorizations += 1
-        self._lu = True
-        x = self._rf_solve_refined(self.rhs)
-        if x is None:
+                if not self._rf_try_setup():
+                    return nan()
+                fresh = True
+        x = self._rf_solve_refined(self.rhs, accept=fresh)
+        if x is None and not fresh:
             # The kept pivot order does not suit this matrix: factor it afresh on the host.
-            self._rf_setup()
+            if not self._rf_try_setup():
+                return nan()
             x = self._rf_solve_refined(self.rhs, accept=True)
-            if x is None:
-                x = torch.full_like(self.rhs, float("nan"))
-        return x
+        return nan() if x is None else x
 
     def _rf_matrices(self):
         torch = self.torch
@@ -600,6 +669,109 @@ class GpuTransient(TransientBase):
     def _ptr(self, t):
         return None if t is None else ctypes.c_void_p(t.data_ptr())
 
+    # -- graph-replayed Newton iterations (dense solve) ---------------------------------------------
+    def _iteration_body(self, prm, flags1, mode, h, order, qn0, fhist):
+        """One Newton update and the evaluation at the new iterate, as _newton does it eagerly:
+        factor and solve, x += dx, the weighted update norm, the device loads and the combine at
+        the new x, and the residual's max norm; the two norms land in the pinned host buffer."""
+        torch = self.torch
+        if self._small:
+            self._dense_solve(self._dx_d)
+            dx, LU, piv = self._dx_d, None, None
+        else:
+            self._dense.zero_()
+            self._dense[self._flat] = self.jac
+            LU, piv, _ = torch.linalg.lu_factor_ex(self._dense.view(self.nu, self.nu))
+            dx = torch.linalg.lu_solve(LU, piv, self.rhs.view(-1, 1)).view(-1)
+        self.x += dx
+        if prm.update_weights_each_iter:
+            self._g_w.copy_(prm.rel_tol * torch.maximum(self._g_xref.abs(), self.x.abs()) + prm.abs_tol)
+        wrms = torch.sqrt(torch.mean((dx / self._g_w) ** 2))
+        self._load_raw(flags1)
+        self._combine(mode, h, order, qn0, fhist)
+        self._g_norms.copy_(torch.stack([wrms, self.rhs.abs().max()]))
+        self._g_host.copy_(self._g_norms, non_blocking=True)
+        return "small" if self._small else (LU, piv)
+
+    def _graph_for(self, prm, flags1, mode, h, order, qn0, fhist):
+        torch = self.torch
+        key = (mode, h, order, self.gshunt, self.limiting, prm.rel_tol, prm.abs_tol, prm.update_weights_each_iter,
+               tuple(sorted(vars(flags1).items())), self._ptr(qn0).value if qn0 is not None else 0,
+               self._ptr(fhist).value if fhist is not None else 0)
+        g = self._graphs.get(key)
+        if g is not None:
+            return g
+        if not hasattr(self, "_g_host"):
+            z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
+            self._g_xref, self._g_w, self._g_norms = z(self.nu), z(self.nu), z(2)
+            self._g_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+            if not self._small:
+                # Library handles and workspaces come into being outside any capture.
+                eye = torch.eye(self.nu, dtype=torch.float64, device=self.dev)
+                torch.linalg.lu_solve(*torch.linalg.lu_factor_ex(eye)[:2], eye[:, :1])
+            self._graph_pool = torch.cuda.graph_pool_handle()
+            torch.cuda.synchronize(self.dev)
+        # Capture from a copy of the state: capturing runs nothing, but the buffers are restored to
+        # be safe against any eager work a library does while it is captured.
+        keep = [t.clone() for t in (self.x, self.next_sta, self.next_sto, self.jac, self.rhs)]
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, pool=self._graph_pool):
+            lu = self._iteration_body(prm, flags1, mode, h, order, qn0, fhist)
+        for t, k in zip((self.x, self.next_sta, self.next_sto, self.jac, self.rhs), keep):
+            t.copy_(k)
+        self._graphs[key] = (graph, lu)
+        return self._graphs[key]
+
+    def _newton(self, prm: NewtonParams, flags_for_iter, mode, h=None, order=1, qn0=None, fhist=None):
+        if not self.graphs:
+            return super()._newton(prm, flags_for_iter, mode, h, order, qn0, fhist)
+        f1, f2 = flags_for_iter(1), flags_for_iter(2)
+        f2.newton_iter = 1
+        if f1 != f2:  # the iterations' flags differ beyond newton_iter >= 1: no single graph
+            return super()._newton(prm, flags_for_iter, mode, h, order, qn0, fhist)
+        torch = self.torch
+        graph, lu = self._graph_for(prm, f1, mode, h, order, qn0, fhist)
+        self._g_xref.copy_(self.x)
+        self._g_w.copy_(prm.rel_tol * self._g_xref.abs() + prm.abs_tol)
+        self._load(flags_for_iter(0))
+        self._combine(mode, h, order, qn0, fhist)
+        stream = torch.cuda.current_stream(self.dev)
+        for it in range(1, prm.max_iter + 1):
+            graph.replay()
+            self._lu = lu
+            self.stats.factorizations += 1
+            self.stats.loads += 1
+            stream.synchronize()
+            wrms, max_rhs = float(self._g_host[0]), float(self._g_host[1])
+            if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
+                return -1
+            if max_rhs <= prm.rhs_tol and wrms <= prm.delta_x_tol:
+                return it
+        return -1
+
+    def _dense_solve(self, out):
+        p = self._ptr
+        _native.check(self._lib.xd_tia_dense_solve(self._tia, p(self.jac), p(self.rhs), p(self._lu_d),
+                                                   p(self._piv_d), p(out), None, self._stream()),
+                      "xd_tia_dense_solve")
+
+    def _solve(self):
+        if not self._small:
+            return super()._solve()
+        self._dense_solve(self._dx_d)
+        self._lu = "small"
+        self.stats.factorizations += 1
+        return self._dx_d.clone()
+
+    def _solve_factored(self):
+        if not self._small:
+            return super()._solve_factored()
+        out = self.torch.empty_like(self.rhs)
+        p = self._ptr
+        _native.check(self._lib.xd_tia_dense_resolve(self._tia, p(self._lu_d), p(self._piv_d), p(self.rhs), p(out),
+                                                     self._stream()), "xd_tia_dense_resolve")
+        return out
+
     def _stream(self):
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
 
@@ -607,13 +779,16 @@ class GpuTransient(TransientBase):
         self.torch.cuda.synchronize(self.dev)
 
     def _load(self, flags: SolverFlags):
+        self._load_raw(flags)
+        self.stats.loads += 1
+
+    def _load_raw(self, flags: SolverFlags):
         c = flags.to_c()
         p = self._ptr
         _native.check(self._lib.xd_load_assign(self.fam._h, ctypes.byref(c), p(self.x), p(self.next_sta),
                                                p(self.curr_sta), p(self.next_sto), p(self.curr_sto), p(self.f),
                                                p(self.q), p(self.fx), p(self.qx), p(self.jf), p(self.jq),
                                                self._stream()), "xd_load_assign")
-        self.stats.loads += 1
 
     def _surrogate_load(self):
         self.surrogate.load(self.x, self.f, self.q, self.fx, self.qx, self._stream())

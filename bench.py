@@ -120,6 +120,78 @@ def batched_section(args, dev_id):
             "eval_launch_shape": shape}
 
 
+def placed_transient(args):
+    """The 100k-MOSFET gate netlist (placed wiring: a pin takes one of the 64 most recently opened
+    fan-out slots) through a transient on the GPU: device loads, combine and the cuSOLVER
+    refactorization of every Newton matrix on the device, one host factorization at the start.
+    Operating point from the logic-level starting iterate, then 0 - placed_ns at 10 ps steps with
+    the reference's transient Newton tolerances."""
+    import ctypes
+
+    import torch
+
+    from tests.parity import family_inputs
+    from xyce_b200 import MosfetDevice, SolverFlags, netlist
+    from xyce_b200.transient import GpuTransient, NewtonParams
+
+    c = netlist.random_logic(args.placed_mos, seed=args.seed, n_inputs=64, locality=64)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, None)
+    fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
+    g = GpuTransient(c, fam, rowptr, colind, solver="rf")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dc_its = g.dcop(x0=netlist.logic_initial_guess(c))
+    torch.cuda.synchronize()
+    dc_s = time.perf_counter() - t0
+    st = g.stats
+    f0, h0, l0 = st.factorizations, st.host_factorizations, st.loads
+    t0 = time.perf_counter()
+    _, w = g.run(args.placed_ns * 1e-9, 10e-12, params=NewtonParams.transient(),
+                 record=np.arange(0, c.n_nodes, 997))
+    torch.cuda.synchronize()
+    run_s = time.perf_counter() - t0
+    its = int(sum(st.newton_iters))
+    # Per-iteration parts, timed alone on the final state: device load + combine, refactor, solve.
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    fl = SolverFlags(newton_iter=1, pdt=1e11, gmin=g.gmin)
+    zero = torch.zeros_like(g.x)
+    ev[0].record()
+    for _ in range(5):
+        g._load_raw(fl)
+        g._combine(1, 1e-11, 2, zero, zero)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ref_ms = []
+    for _ in range(3):
+        t = time.perf_counter()
+        g._lib.xd_rf_refactor(g._rf, ctypes.c_void_p(g.jac.data_ptr()))
+        torch.cuda.synchronize()
+        ref_ms.append((time.perf_counter() - t) * 1e3)
+    x = g.rhs.clone()
+    t = time.perf_counter()
+    for _ in range(3):
+        g._lib.xd_rf_solve(g._rf, ctypes.c_void_p(x.data_ptr()))
+    torch.cuda.synchronize()
+    solve_ms = (time.perf_counter() - t) * 1e3 / 3
+    res = {"workload": f"seeded INV/NAND2/NOR2 netlist with placed wiring (fan-out U{{1..4}}, a pin takes one of "
+                       f"the 64 most recent open slots), {c.n_mos} BSIM4 MOSFETs, {c.res_nodes.shape[0]} R + "
+                       f"{c.cap_nodes.shape[0]} C wire parasitics, 64 PWL inputs, {c.n_unknowns} unknowns, "
+                       f"{g.nnz} nnz; operating point, then 0-{args.placed_ns:g} ns at 10 ps steps, reference "
+                       f"transient Newton tolerances",
+           "operating_point_s": dc_s, "operating_point_newton_iters": int(dc_its),
+           "gpu_s_per_run": run_s, "steps": len(st.newton_iters), "failed_steps": st.failed_steps,
+           "newton_iters_per_step": float(np.mean(st.newton_iters)),
+           "ms_per_newton_iteration": run_s * 1e3 / max(1, its),
+           "matrices": st.factorizations - f0, "host_factorizations": st.host_factorizations - h0,
+           "per_iteration_ms": {"device_loads_and_combine": ev[0].elapsed_time(ev[1]) / 5,
+                                "refactorization": min(ref_ms), "triangular_solves": solve_ms},
+           "swing_v": [float(w.min()), float(w.max())]}
+    g.close()
+    fam.close()
+    return res
+
+
 def transient_section(args):
     """Transient wall time per run, GPU path vs the oracle's loads through the same driver, and
     the learned warm start against the plain GPU path (Newton iterations per step)."""
@@ -188,6 +260,8 @@ def transient_section(args):
                      "factorizations": g.stats.factorizations, "surrogate_loads": g.stats.surrogate_loads}
         g.close()
         fam.close()
+    if args.placed_mos > 0:
+        out["placed_netlist"] = placed_transient(args)
     out["warm_start_bsim4_gates"] = {
         "workload": f"seeded INV/NAND2/NOR2 netlist, {c.n_mos} BSIM4 MOSFETs, RC wires, 16 PWL inputs, "
                     f"{c.n_unknowns} unknowns, 0-1 ns at 10 ps, linear predictor on both paths",
@@ -213,6 +287,8 @@ def parse():
     ap.add_argument("--no-transient", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
+    ap.add_argument("--placed-mos", type=int, default=100_000, help="MOSFETs of the placed-netlist transient (0: skip)")
+    ap.add_argument("--placed-ns", type=float, default=1.0, help="length of the placed-netlist transient (ns)")
     return ap.parse_args()
 
 

@@ -70,3 +70,47 @@ def test_cuda_graph_replay_matches_direct_load():
     for a, d in zip(out, direct):
         assert torch.equal(a, d)
     dev.close()
+
+
+def test_batched_sweep_transient_waveforms_match_per_circuit_oracle_runs():
+    """The merged sweep through one transient on the GPU (one evaluation launch per load for all
+    circuits, refactorization path), against separate oracle runs of single circuits of the sweep
+    (their own TOXE cards and DELVTO): every compared circuit's node waveforms within reltol 1e-3 /
+    abstol 1e-12. Newton tolerances are tight, so the merged system's shared convergence test
+    cannot show in the waveforms."""
+    from tests.parity import family_inputs
+    from tests.transient_oracle import OracleTransient
+    from xyce_b200 import ModelCard
+    from xyce_b200.transient import GpuTransient, NewtonParams
+
+    seed, n_c, lo, hi = 3, 8, 200, 1500
+    b = netlist.batched_sweep(n_c, lo, hi, seed=seed)
+    c = b.circuit
+    rowptr, colind = netlist.jacobian_pattern(c)
+    tight = NewtonParams(max_iter=40, rhs_tol=1e-9, delta_x_tol=1e-3, abs_tol=1e-9, rel_tol=1e-6,
+                         update_weights_each_iter=False)
+    tight_dc = NewtonParams(rhs_tol=1e-12, delta_x_tol=1e-3, abs_tol=1e-12, rel_tol=1e-6)
+    fam = MosfetDevice(b.cards, b.inst_model, c.mos_nodes, b.inst_params, (rowptr, colind), c.n_unknowns, level=14)
+    g = GpuTransient(c, fam, rowptr, colind, solver="rf")
+    g.dcop(tight_dc)
+    tg, wg = g.run(0.8e-9, 10e-12, params=tight, record=np.arange(c.n_nodes))
+    g.close()
+    fam.close()
+    worst = {}
+    for k in (0, 3, 7):
+        ck = netlist.random_logic(int(b.sizes[k]), seed=seed * 100003 + k + 1, wire_segments=2)
+        assert ck.n_nodes == b.node_offset[k + 1] - b.node_offset[k]
+        cards = [ModelCard(False, {"TOXE": 3.0e-9 * b.toxe_factor[k]}),
+                 ModelCard(True, {"TOXE": 3.0e-9 * b.toxe_factor[k]})]
+        extra = {"DELVTO": np.full(ck.n_mos, b.delvto[k])}
+        rp, ci = netlist.jacobian_pattern(ck)
+        o = OracleTransient(ck, cards, rp, ci, level=14, extra_params=extra)
+        o.dcop(tight_dc)
+        to, wo = o.run(0.8e-9, 10e-12, params=tight, record=np.arange(ck.n_nodes))
+        assert np.array_equal(tg, to)
+        mine = wg[:, b.node_offset[k]:b.node_offset[k + 1]]
+        bound = 1e-3 * np.abs(wo).max(axis=0, keepdims=True) + 1e-12
+        worst[k] = float((np.abs(mine - wo) / bound).max())
+        assert worst[k] <= 1.0, (k, worst[k])
+        assert (wo.max(0) - wo.min(0)).max() > 0.5  # inputs switch inside the window
+    print("batched sweep: worst waveform error / bound per circuit", worst)

@@ -100,6 +100,19 @@ def test_eval_launch_variants_bitwise_identical():
             assert np.array_equal(ref[k], out[k], equal_nan=True), (v, k)
 
 
+@pytest.mark.parametrize("capmod,xpart,cvc", [(0, 0.0, 0), (0, 0.5, 0), (0, 1.0, 0), (1, 0.0, 0), (1, 0.5, 1),
+                                               (1, 1.0, 0)])
+def test_parity_capmod_0_and_1(capmod, xpart, cvc):
+    """The simple (capMod 0) and the non-charge-thickness (capMod 1) charge models, every charge
+    partition, both threshold forms of the C-V gate overdrive (cvchargeMod), biases that reach
+    accumulation, depletion, the linear and the saturation regions."""
+    c = netlist.random_logic(1500, seed=31)
+    cards = [ModelCard(False, {"CAPMOD": capmod, "XPART": xpart, "CVCHARGEMOD": cvc}),
+             ModelCard(True, {"CAPMOD": capmod, "XPART": xpart, "CVCHARGEMOD": cvc, "VFBCV": -0.8})]
+    worst = _run_sequence(c, cards, TRANSIENT_SEQ[:4] + DC_SEQ[2:3], vrange=(-0.4, 1.6), seed=capmod + 7)
+    print("capMod", capmod, "xpart", xpart, "worst error / tolerance:", worst)
+
+
 def test_parity_inverter_ring_bsim4():
     c = netlist.inverter_ring(101, vdd=1.8)
     worst = _run_sequence(c, None, TRANSIENT_SEQ, vrange=(0.0, 1.8))

@@ -11,7 +11,7 @@
 //   Instance::auxChargeCalculations      N_DEV_MOSFET_B4.C:12216-12350
 //   Master::loadDAEVectors / loadDAEMatrices  N_DEV_MOSFET_B4.C:16303-16567, 16577-17268
 // for the configuration the set-up accepts: rgateMod = rbodyMod = trnqsMod = acnqsMod = rdsMod = 0,
-// igcMod = igbMod = 0, capMod = 2, no source/drain resistance nodes, no initial conditions. With
+// igcMod = igbMod = 0, capMod = 0, 1 or 2, no source/drain resistance nodes, no initial conditions. With
 // no internal nodes the 11 stamp rows collapse onto the 4 terminals D, G, S, B.
 //
 // Local stamp layout (terminal order D=0, G=1, S=2, B=3):
@@ -90,6 +90,7 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   const int mobMod = (int)P(mobMod);
   const int dioMod = (int)P(dioMod);
   const int tempMod = (int)P(tempMod);
+  const int capMod = (int)P(capMod);
   const double gmin = fl.gmin;
   const double nf = P(nf);
   const double vth0 = P(vth0);
@@ -1348,11 +1349,186 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     Igisl *= nf; ggisls *= nf; ggislg *= nf; ggislb *= nf;
   }
 
-  // Intrinsic charges, capMod = 2 charge-thickness model (:10707-11620).
+  // Intrinsic charges (:10707-11620): capMod 0, 1 or 2 (charge-thickness model).
   double qgate = 0, qdrn = 0, qbulk = 0, qsrc = 0;
   double cggb = 0, cgsb = 0, cgdb = 0, cdgb = 0, cdsb = 0, cddb = 0, cbgb = 0, cbsb = 0, cbdb = 0;
   if ((P(xpart) < 0) || (!ChargeComputationNeeded)) {
     // all zero
+  } else if (capMod == 0) {
+    // capMod = 0 (:10718-11012): a simple charge model with its own flat band (VFBCV) and
+    // threshold; the reference reassigns Vbseff, Vth, Vgst and Vdsat here, which nothing after
+    // the charge section reads, so they are local.
+    double Vbs0, dVbs0_dVb;
+    if (Vbseff < 0.0) {
+      Vbs0 = Vbs;
+      dVbs0_dVb = 1.0;
+    } else {
+      Vbs0 = phi - Phis;
+      dVbs0_dVb = -dPhis_dVb;
+    }
+    const double Vfb0 = P(vfbcv);
+    const double k1ox0 = P(k1ox);
+    const double Vth0 = Vfb0 + phi + k1ox0 * sqrtPhis;
+    const double Vgst0 = Vgs_eff - Vth0;
+    const double dVth0_dVb = k1ox0 * dsqrtPhis_dVb;
+    const double CoxWL = coxe * P(weffCV) * P(leffCV) * nf;
+    const double Arg1 = Vgs_eff - Vbs0 - Vfb0;
+    if (Arg1 <= 0.0) {  // accumulation
+      qgate = CoxWL * Arg1;
+      qbulk = -qgate;
+      qdrn = 0.0;
+      cggb = CoxWL * dVgs_eff_dVg;
+      cgdb = 0.0;
+      cgsb = CoxWL * (dVbs0_dVb - dVgs_eff_dVg);
+      cdgb = 0.0;
+      cddb = 0.0;
+      cdsb = 0.0;
+      cbgb = -CoxWL * dVgs_eff_dVg;
+      cbdb = 0.0;
+      cbsb = -cgsb;
+    } else if (Vgst0 <= 0.0) {  // depletion
+      T1 = 0.5 * k1ox0;
+      T2 = sqrt(T1 * T1 + Arg1);
+      qgate = CoxWL * k1ox0 * (T2 - T1);
+      qbulk = -qgate;
+      qdrn = 0.0;
+      T0 = CoxWL * T1 / T2;
+      cggb = T0 * dVgs_eff_dVg;
+      cgdb = 0.0;
+      cgsb = T0 * (dVbs0_dVb - dVgs_eff_dVg);
+      cdgb = 0.0;
+      cddb = 0.0;
+      cdsb = 0.0;
+      cbgb = -cggb;
+      cbdb = 0.0;
+      cbsb = -cgsb;
+    } else {  // inversion
+      const double One_Third_CoxWL = CoxWL / 3.0;
+      const double Two_Third_CoxWL = 2.0 * One_Third_CoxWL;
+      const double AbulkCV = Abulk0 * P(abulkCVfactor);
+      const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+      const double Vdsat0 = Vgst0 / AbulkCV;
+      const double dVdsat_dVg = dVgs_eff_dVg / AbulkCV;
+      const double dVdsat_dVb = -(Vdsat0 * dAbulkCV_dVb + dVth0_dVb) / AbulkCV;
+      const double xpart = P(xpart);
+      const bool sat = (xpart > 0.5) ? (Vdsat0 <= Vds) : (Vds >= Vdsat0);
+      if (sat) {
+        T1 = Vdsat0 / 3.0;
+        qgate = CoxWL * (Vgs_eff - Vfb0 - phi - T1);
+        T2 = -Two_Third_CoxWL * Vgst0;
+        qbulk = -(qgate + T2);
+        // drain share of the inversion charge: 0 (0/100), 0.4 (40/60), 0.5 (50/50)
+        qdrn = (xpart > 0.5) ? 0.0 : ((xpart < 0.5) ? 0.4 * T2 : 0.5 * T2);
+        cggb = One_Third_CoxWL * (3.0 - dVdsat_dVg) * dVgs_eff_dVg;
+        T2 = -One_Third_CoxWL * dVdsat_dVb;
+        cgsb = -(cggb + T2);
+        cgdb = 0.0;
+        if (xpart > 0.5) {
+          cdgb = 0.0;
+          cddb = 0.0;
+          cdsb = 0.0;
+        } else if (xpart < 0.5) {
+          T3 = 0.4 * Two_Third_CoxWL;
+          cdgb = -T3 * dVgs_eff_dVg;
+          cddb = 0.0;
+          T4 = T3 * dVth0_dVb;
+          cdsb = -(T4 + cdgb);
+        } else {
+          cdgb = -One_Third_CoxWL * dVgs_eff_dVg;
+          cddb = 0.0;
+          T4 = One_Third_CoxWL * dVth0_dVb;
+          cdsb = -(T4 + cdgb);
+        }
+        cbgb = -(cggb - Two_Third_CoxWL * dVgs_eff_dVg);
+        T3 = -(T2 + Two_Third_CoxWL * dVth0_dVb);
+        cbsb = -(cbgb + T3);
+        cbdb = 0.0;
+      } else {  // linear region
+        const double Alphaz = Vgst0 / Vdsat0;
+        T1 = 2.0 * Vdsat0 - Vds;
+        T2 = Vds / (3.0 * T1);
+        T3 = T2 * Vds;
+        T9 = 0.25 * CoxWL;
+        T4 = T9 * Alphaz;
+        if (xpart > 0.5) {
+          T7 = 2.0 * Vds - T1 - 3.0 * T3;
+          T8 = T3 - T1 - 2.0 * Vds;
+        }
+        qgate = CoxWL * (Vgs_eff - Vfb0 - phi - 0.5 * (Vds - T3));
+        if (xpart > 0.5) {
+          T10 = T4 * T8;
+          qdrn = T4 * T7;
+          qbulk = -(qgate + qdrn + T10);
+        }
+        T5 = T3 / T1;
+        cggb = CoxWL * (1.0 - T5 * dVdsat_dVg) * dVgs_eff_dVg;
+        if (xpart > 0.5) {
+          T11 = -CoxWL * T5 * dVdsat_dVb;
+          cgdb = CoxWL * (T2 - 0.5 + 0.5 * T5);
+          cgsb = -(cggb + T11 + cgdb);
+        } else {
+          tmp = -CoxWL * T5 * dVdsat_dVb;
+          cgdb = CoxWL * (T2 - 0.5 + 0.5 * T5);
+          cgsb = -(cggb + cgdb + tmp);
+        }
+        T6 = 1.0 / Vdsat0;
+        const double dAlphaz_dVg = T6 * (1.0 - Alphaz * dVdsat_dVg);
+        const double dAlphaz_dVb = -T6 * (dVth0_dVb + Alphaz * dVdsat_dVb);
+        if (xpart > 0.5) {  // 0/100
+          T7 = T9 * T7;
+          T8 = T9 * T8;
+          T9 = 2.0 * T4 * (1.0 - 3.0 * T5);
+          cdgb = (T7 * dAlphaz_dVg - T9 * dVdsat_dVg) * dVgs_eff_dVg;
+          T12 = T7 * dAlphaz_dVb - T9 * dVdsat_dVb;
+          cddb = T4 * (3.0 - 6.0 * T2 - 3.0 * T5);
+          cdsb = -(cdgb + T12 + cddb);
+          T9 = 2.0 * T4 * (1.0 + T5);
+          T10 = (T8 * dAlphaz_dVg - T9 * dVdsat_dVg) * dVgs_eff_dVg;
+          T11 = T8 * dAlphaz_dVb - T9 * dVdsat_dVb;
+          T12 = T4 * (2.0 * T2 + T5 - 1.0);
+          T0 = -(T10 + T11 + T12);
+          cbgb = -(cggb + cdgb + T10);
+          cbdb = -(cgdb + cddb + T12);
+          cbsb = -(cgsb + cdsb + T0);
+        } else if (xpart < 0.5) {  // 40/60
+          T6 = 8.0 * Vdsat0 * Vdsat0 - 6.0 * Vdsat0 * Vds + 1.2 * Vds * Vds;
+          T8 = T2 / T1;
+          T7 = Vds - T1 - T8 * T6;
+          qdrn = T4 * T7;
+          T7 *= T9;
+          tmp = T8 / T1;
+          tmp1 = T4 * (2.0 - 4.0 * tmp * T6 + T8 * (16.0 * Vdsat0 - 6.0 * Vds));
+          cdgb = (T7 * dAlphaz_dVg - tmp1 * dVdsat_dVg) * dVgs_eff_dVg;
+          T10 = T7 * dAlphaz_dVb - tmp1 * dVdsat_dVb;
+          cddb = T4 * (2.0 - (1.0 / (3.0 * T1 * T1) + 2.0 * tmp) * T6 + T8 * (6.0 * Vdsat0 - 2.4 * Vds));
+          cdsb = -(cdgb + T10 + cddb);
+          T7 = 2.0 * (T1 + T3);
+          qbulk = -(qgate - T4 * T7);
+          T7 *= T9;
+          T0 = 4.0 * T4 * (1.0 - T5);
+          T12 = (-T7 * dAlphaz_dVg - cdgb - T0 * dVdsat_dVg) * dVgs_eff_dVg;
+          T11 = -T7 * dAlphaz_dVb - T10 - T0 * dVdsat_dVb;
+          T10 = -4.0 * T4 * (T2 - 0.5 + 0.5 * T5) - cddb;
+          tmp = -(T10 + T11 + T12);
+          cbgb = -(cggb + cdgb + T12);
+          cbdb = -(cgdb + cddb + T10);
+          cbsb = -(cgsb + cdsb + tmp);
+        } else {  // 50/50
+          T7 = T1 + T3;
+          qdrn = -T4 * T7;
+          qbulk = -(qgate + qdrn + qdrn);
+          T7 *= T9;
+          T0 = T4 * (2.0 * T5 - 2.0);
+          cdgb = (T0 * dVdsat_dVg - T7 * dAlphaz_dVg) * dVgs_eff_dVg;
+          T12 = T0 * dVdsat_dVb - T7 * dAlphaz_dVb;
+          cddb = T4 * (1.0 - 2.0 * T2 - T5);
+          cdsb = -(cdgb + T12 + cddb);
+          cbgb = -(cggb + 2.0 * cdgb);
+          cbdb = -(cgdb + 2.0 * cddb);
+          cbsb = -(cgsb + 2.0 * cdsb);
+        }
+      }
+    }
   } else {
     double VbseffCV, dVbseffCV_dVb;
     if (Vbseff < 0.0) {
@@ -1445,6 +1621,145 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
       dVgsteff_dVd = (T9 * dT10_dVd - T10 * dT9_dVd) / T11;
       dVgsteff_dVb = (T9 * dT10_dVb - T10 * dT9_dVb) / T11;
     }
+    if (capMod == 1) {
+      // capMod = 1 (:11139-11319): accumulation and depletion charges Qac0 / Qsub0 with the
+      // zero-bias flat band, the inversion charge without the charge-thickness correction.
+      const double Vfb1 = P(vfbzb);
+      double V3 = Vfb1 - Vgs_eff + VbseffCV - CONSTDELTA_3;
+      if (Vfb1 <= 0.0)
+        T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * Vfb1);
+      else
+        T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * Vfb1);
+      T1 = 0.5 * (1.0 + V3 / T0);
+      const double Vfbeff = Vfb1 - 0.5 * (V3 + T0);
+      const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
+      const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
+      const double Qac0 = CoxWL * (Vfbeff - Vfb1);
+      const double dQac0_dVg = CoxWL * dVfbeff_dVg;
+      const double dQac0_dVb = CoxWL * dVfbeff_dVb;
+      const double k1ox1 = P(k1ox);
+      T0 = 0.5 * k1ox1;
+      T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
+      if (k1ox1 == 0.0) {
+        T1 = 0.0;
+        T2 = 0.0;
+      } else if (T3 < 0.0) {
+        T1 = T0 + T3 / k1ox1;
+        T2 = CoxWL;
+      } else {
+        T1 = sqrt(T0 * T0 + T3);
+        T2 = CoxWL * T0 / T1;
+      }
+      const double Qsub0 = CoxWL * k1ox1 * (T1 - T0);
+      const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg);
+      const double dQsub0_dVd = -T2 * dVgsteff_dVd;
+      const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb);
+      const double AbulkCV = Abulk0 * P(abulkCVfactor);
+      const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+      const double VdsatCV = Vgsteff / AbulkCV;
+      T0 = VdsatCV - Vds - CONSTDELTA_4;
+      dT0_dVg = 1.0 / AbulkCV;
+      dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
+      T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
+      dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
+      dT1_dVd = -T0 / T1;
+      dT1_dVb = dT1_dVg * dT0_dVb;
+      dT1_dVg *= dT0_dVg;
+      double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
+      if (T0 >= 0.0) {
+        VdseffCV = VdsatCV - 0.5 * (T0 + T1);
+        dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
+        dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
+        dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
+      } else {
+        T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
+        T4 = 1.0 - T3;
+        T5 = VdsatCV * T3 / (T1 - T0);
+        VdseffCV = VdsatCV * T4;
+        dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
+        dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
+        dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
+      }
+      if (Vds == 0.0) {  // the reference leaves dVdseffCV_dVd as computed
+        VdseffCV = 0.0;
+        dVdseffCV_dVg = 0.0;
+        dVdseffCV_dVb = 0.0;
+      }
+      T0 = AbulkCV * VdseffCV;
+      T1 = 12.0 * (Vgsteff - 0.5 * T0 + 1.0e-20);
+      T2 = VdseffCV / T1;
+      T3 = T0 * T2;
+      T4 = (1.0 - 12.0 * T2 * T2 * AbulkCV);
+      T5 = (6.0 * T0 * (4.0 * Vgsteff - T0) / (T1 * T1) - 0.5);
+      T6 = 12.0 * T2 * T2 * Vgsteff;
+      qgate = CoxWL * (Vgsteff - 0.5 * VdseffCV + T3);
+      double Cgg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+      const double Cgd1 = CoxWL * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd;
+      const double Cgb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb;
+      Cgg1 *= dVgsteff_dVg;
+      T7 = 1.0 - AbulkCV;
+      qbulk = CoxWL * T7 * (0.5 * VdseffCV - T3);
+      T4 = -T7 * (T4 - 1.0);
+      T5 = -T7 * T5;
+      T6 = -(T7 * T6 + (0.5 * VdseffCV - T3));
+      double Cbg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+      const double Cbd1 = CoxWL * T5 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd;
+      const double Cbb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb;
+      Cbg1 *= dVgsteff_dVg;
+      double Csg, Csd, Csb;
+      const double xpart = P(xpart);
+      if (xpart > 0.5) {  // 0/100
+        T1 = T1 + T1;
+        qsrc = -CoxWL * (0.5 * Vgsteff + 0.25 * T0 - T0 * T0 / T1);
+        T7 = (4.0 * Vgsteff - T0) / (T1 * T1);
+        T4 = -(0.5 + 24.0 * T0 * T0 / (T1 * T1));
+        T5 = -(0.25 * AbulkCV - 12.0 * AbulkCV * T0 * T7);
+        T6 = -(0.25 * VdseffCV - 12.0 * T0 * VdseffCV * T7);
+        Csg = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+        Csd = CoxWL * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
+        Csb = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
+        Csg *= dVgsteff_dVg;
+      } else if (xpart < 0.5) {  // 40/60
+        T1 = T1 / 12.0;
+        T2 = 0.5 * CoxWL / (T1 * T1);
+        T3 = Vgsteff * (2.0 * T0 * T0 / 3.0 + Vgsteff * (Vgsteff - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
+        qsrc = -T2 * T3;
+        T7 = 4.0 / 3.0 * Vgsteff * (Vgsteff - T0) + 0.4 * T0 * T0;
+        T4 = -2.0 * qsrc / T1 - T2 * (Vgsteff * (3.0 * Vgsteff - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
+        T5 = (qsrc / T1 + T2 * T7) * AbulkCV;
+        T6 = (qsrc / T1 * VdseffCV + T2 * T7 * VdseffCV);
+        Csg = (T4 + T5 * dVdseffCV_dVg);
+        Csd = T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
+        Csb = (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
+        Csg *= dVgsteff_dVg;
+      } else {  // 50/50
+        qsrc = -0.5 * (qgate + qbulk);
+        Csg = -0.5 * (Cgg1 + Cbg1);
+        Csb = -0.5 * (Cgb1 + Cbb1);
+        Csd = -0.5 * (Cgd1 + Cbd1);
+      }
+      qgate += Qac0 + Qsub0;
+      qbulk -= (Qac0 + Qsub0);
+      qdrn = -(qgate + qbulk + qsrc);
+      const double Cgg = dQac0_dVg + dQsub0_dVg + Cgg1;
+      const double Cgd = dQsub0_dVd + Cgd1;
+      double Cgb = dQac0_dVb + dQsub0_dVb + Cgb1;
+      const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
+      const double Cbd = Cbd1 - dQsub0_dVd;
+      double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
+      Cgb *= dVbseff_dVb;
+      Cbb *= dVbseff_dVb;
+      Csb *= dVbseff_dVb;
+      cggb = Cgg;
+      cgsb = -(Cgg + Cgd + Cgb);
+      cgdb = Cgd;
+      cdgb = -(Cgg + Cbg + Csg);
+      cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
+      cddb = -(Cgd + Cbd + Csd);
+      cbgb = Cbg;
+      cbsb = -(Cbg + Cbd + Cbb);
+      cbdb = Cbd;
+    } else {
     // capMod == 2
     const double vfbzb = P(vfbzb);
     double V3 = vfbzb - Vgs_eff + VbseffCV - CONSTDELTA_3;
@@ -1658,6 +1973,7 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     cbgb = Cbg;
     cbsb = -(Cbg + Cbd + Cbb);
     cbdb = Cbd;
+    }
   }
 
   // Junction charges and capacitances (:11661-11810). Outside charge computation the reference
@@ -1758,10 +2074,15 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     }
   }
 
-  // Overlap capacitances, capMod 1/2 (:11853-11890).
+  // Overlap capacitances (:11846-11890): constant for capMod 0, bias-dependent for 1 and 2.
   const double vgdx = vgd, vgsx = vgs;
   double cgdo, qgdo, cgso, qgso;
-  {
+  if (capMod == 0) {
+    cgdo = P(cgdo);
+    qgdo = P(cgdo) * vgdx;
+    cgso = P(cgso);
+    qgso = P(cgso) * vgsx;
+  } else {
     T0 = vgdx + CONSTDELTA_1;
     T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
     T2 = 0.5 * (T0 - T1);

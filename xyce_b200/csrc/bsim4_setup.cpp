@@ -242,7 +242,7 @@ std::string process_model(const ModelSpec &spec, const SetupOptions &opts, Card 
   if (m.rgateMod != 0) return "BSIM4 rgateMod != 0 is not supported";
   if (m.rbodyMod != 0) return "BSIM4 rbodyMod != 0 is not supported";
   if (m.trnqsMod != 0 || m.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
-  if (m.capMod != 2) return "BSIM4 capMod != 2 is not supported";
+  if (m.capMod < 0 || m.capMod > 2) return "BSIM4 capMod must be 0, 1 or 2";
   if (m.dioMod < 0 || m.dioMod > 2) return "BSIM4 dioMod must be 0, 1 or 2";
   if (m.mobMod < 0 || m.mobMod > 2) return "BSIM4 mobMod must be 0, 1 or 2";
   if (m.tnoiMod != 0) return "BSIM4 tnoiMod != 0 is not supported";
@@ -993,7 +993,7 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   R(vtl) = p.vtl; R(tfactor) = p.tfactor; R(xrcrg1) = p.xrcrg1; R(xrcrg2) = p.xrcrg2; R(vfbsd) = p.vfbsd;
   R(egidl) = p.egidl; R(agidl) = p.agidl; R(bgidl) = p.bgidl; R(cgidl) = p.cgidl; R(weffCJ) = p.weffCJ;
   R(egisl) = p.egisl; R(agisl) = p.agisl; R(bgisl) = p.bgisl; R(cgisl) = p.cgisl;
-  R(abulkCVfactor) = p.abulkCVfactor; R(weffCV) = p.weffCV; R(leffCV) = p.leffCV; R(noff) = p.noff;
+  R(vfbcv) = p.vfbcv; R(abulkCVfactor) = p.abulkCVfactor; R(weffCV) = p.weffCV; R(leffCV) = p.leffCV; R(noff) = p.noff;
   R(voffcv) = p.voffcv; R(mstarcv) = p.mstarcv; R(voffcbncv) = p.voffcbncv; R(acde) = p.acde; R(ldeb) = p.ldeb;
   R(moin) = p.moin; R(cgbo) = p.cgbo; R(cgdo) = p.cgdo; R(cgso) = p.cgso; R(cgdl) = p.cgdl; R(cgsl) = p.cgsl;
   R(ckappad) = p.ckappad; R(ckappas) = p.ckappas;

@@ -2,7 +2,7 @@
 import numpy as np
 import torch
 
-from tests.parity import ABS_SUM_FLOOR, RTOL, OracleRun, compare, family_inputs
+from tests.parity import ABS_SUM_FLOOR, RTOL, OracleRun, compare, family_inputs, row_max
 from xyce_b200 import MosfetDevice, netlist
 
 
@@ -39,14 +39,18 @@ class GpuRun:
 STORE_WRITTEN = {14: [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13], 9: [0, 1, 2, 3, 4], 1: [0, 1, 2, 3, 4]}
 
 
-def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=3, n_sto=14):
+def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=3, n_sto=14, vspan=None):
     report = {}
     keys = ["f", "dfdxdvp", "dfdx"] + (["q", "dqdxdvp", "dqdx"] if charges else [])
     for k in keys:
         detail = []
+        vec_scale = None
+        if vspan is not None and rowptr is not None and k in ("dfdxdvp", "dqdxdvp"):
+            m = "dfdx" if k == "dfdxdvp" else "dqdx"
+            vec_scale = vspan * np.maximum(row_max(rowptr, r[m]), row_max(rowptr, g[m]))
         bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR,
                              rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail,
-                             sens=r["sens"][k] if "sens" in r else None)
+                             sens=r["sens"][k] if "sens" in r else None, vec_scale=vec_scale)
         report[k] = worst
         assert bad == 0, (f"step {step} {flags}: {k} has {bad} entries out of tolerance (worst {worst:.3g}x); "
                           f"(name, index, gpu, ref, allowed): {detail}")
@@ -91,7 +95,7 @@ def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, c
         r = orc.load_with_sensitivity(flags, sol, sta_n, sta_c, sto_n, sto_c)
         g = gpu.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
         charges = bool(flags.transient or flags.tranop or flags.acop) or charges_in_dc
-        rep = check_step(step, flags, g, r, n, charges, rowptr, level, n_sta, n_sto)
+        rep = check_step(step, flags, g, r, n, charges, rowptr, level, n_sta, n_sto, vspan=vrange[1] - vrange[0])
         for k, v in rep.items():
             worst[k] = max(worst.get(k, 0.0), v)
         # Both sides continue from the oracle's state and store; a step that ends a time point

@@ -14,7 +14,10 @@ from xyce_b200.device import ModelCard, SolverFlags
 # different orders) and, for Jacobian entries, R is the largest magnitude in the entry's row: an
 # entry that is itself the rounding residue of cancelling capacitances (charge conservation makes
 # some dQ/dx sums vanish analytically) carries noise of the order of eps times the row's scale,
-# which fused multiply-add on the GPU rounds differently from the CPU.
+# which any difference in the last bit of a capacitance changes. The limiter vectors dF/dx*dVp and
+# dQ/dx*dVp are Jacobian rows times voltage steps, formed per instance as sums of terms that can
+# cancel (the source entry is minus the gate, bulk and drain ones), so for them R is the matching
+# Jacobian row's largest magnitude times V, the span of the node voltages (the largest step).
 RTOL = 1e-12
 ABS_SUM_FLOOR = 1e-14
 ROW_FLOOR = 1e-14
@@ -37,6 +40,14 @@ def row_scale(rowptr, vals_a, vals_b):
     rmax = np.zeros(len(rowptr) - 1)
     np.maximum.at(rmax, rows, m)
     return rmax[rows]
+
+
+def row_max(rowptr, vals):
+    """Per-row max |value| of CSR values (0 for an empty row)."""
+    rows = np.repeat(np.arange(len(rowptr) - 1), np.diff(rowptr))
+    rmax = np.zeros(len(rowptr) - 1)
+    np.maximum.at(rmax, rows, np.abs(vals))
+    return rmax
 
 
 def family_inputs(c: netlist.Circuit, cards=None, extra_params=None):
@@ -136,10 +147,12 @@ class OracleRun:
         return r
 
 
-def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None, sens=None):
+def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None, sens=None,
+            vec_scale=None):
     """Returns (n_bad, worst ratio of |diff| to the allowed error). With rowptr (CSR values), adds
-    the row-scaled floor; with sens (the oracle's one-ulp sensitivity of each entry), adds
-    SENS_FACTOR times it. If `detail` is a list, the worst offenders are appended to it."""
+    the row-scaled floor; with vec_scale (per-entry R of a limiter vector), ROW_FLOOR times it;
+    with sens (the oracle's one-ulp sensitivity of each entry), adds SENS_FACTOR times it. If
+    `detail` is a list, the worst offenders are appended to it."""
     got = np.asarray(got)
     ref = np.asarray(ref)
     d = np.abs(got - ref)
@@ -148,6 +161,8 @@ def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr
         allow = allow + floor * np.asarray(abs_sum)
     if rowptr is not None:
         allow = allow + ROW_FLOOR * row_scale(rowptr, got, ref)
+    if vec_scale is not None:
+        allow = allow + ROW_FLOOR * np.asarray(vec_scale)
     if sens is not None:
         allow = allow + SENS_FACTOR * np.asarray(sens).reshape(allow.shape)
     allow = np.maximum(allow, 1e-300)

@@ -31,7 +31,7 @@ def test_batched_sweep_parity_against_oracle():
         sol = rng.uniform(0.0, 1.2, c.n_unknowns)
         r = orc.load_with_sensitivity(fl, sol, sta, sta, sto, sto)
         g = gpu.load(fl, sol, sta, sta, sto, sto)
-        check_step(step, fl, g, r, n, True, rowptr, 14, 3, 14)
+        check_step(step, fl, g, r, n, True, rowptr, 14, 3, 14, vspan=1.2)
         sta, sto = r["next_sta"], r["next_sto"]
     dev.close()
 

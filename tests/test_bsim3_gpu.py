@@ -57,6 +57,18 @@ def test_bsim3_parity_card_variants(k):
     print("worst error / tolerance:", worst)
 
 
+@pytest.mark.parametrize("capmod,xpart", [(0, 0.0), (0, 0.5), (0, 1.0), (1, 0.0), (1, 0.5), (1, 1.0)])
+def test_bsim3_parity_capmod_0_and_1(capmod, xpart):
+    """The simple charge model (capMod 0, its own flat band VFBCV) and capMod 1 with its piecewise
+    overlap capacitances (CGDL / CGSL), every charge partition, over accumulation to saturation."""
+    c = netlist.random_logic(2000, seed=61 + capmod, vdd=1.8, length=0.18e-6)
+    cards = [ModelCard(False, {"CAPMOD": capmod, "XPART": xpart, "CGDL": 2e-10, "CGSL": 2e-10}),
+             ModelCard(True, {"CAPMOD": capmod, "XPART": xpart, "VFBCV": -0.7, "CGDL": 1e-10, "CGSL": 3e-10})]
+    worst = run_sequence(c, cards, SEQ, vrange=(-0.5, 2.2), extra_params=_junction_params(c.n_mos, capmod),
+                         level=9)
+    print("capMod", capmod, "xpart", xpart, "worst error / tolerance:", worst)
+
+
 def test_bsim3_load_is_deterministic():
     c = netlist.random_logic(20000, seed=2, vdd=1.8, length=0.18e-6)
     rowptr, colind = netlist.jacobian_pattern(c)

@@ -26,8 +26,7 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
     (14, [ModelCard(False, {"CAPMOD": 3}), ModelCard(True, {})], None, "capMod must be 0, 1 or 2"),
     (14, NMOS_PMOS, {"NRD": 2.0}, "NRD/NRS"),
     (14, [ModelCard(False, {"NOSUCH": 1.0}), ModelCard(True, {})], None, "unknown BSIM4 model parameter"),
-    (9, [ModelCard(False, {"CAPMOD": 0}), ModelCard(True, {})], None, "capMod"),
-    (9, [ModelCard(False, {"CAPMOD": 1}), ModelCard(True, {})], None, "capMod"),
+    (9, [ModelCard(False, {"CAPMOD": 4}), ModelCard(True, {})], None, "capMod"),
     (9, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], None, "series resistance"),
     (9, NMOS_PMOS, {"NQSMOD": 1}, "nqsMod"),
     (9, NMOS_PMOS, {"IC1": 0.5}, "initial conditions"),

@@ -9,7 +9,7 @@
 //   auxChargeCalculations                    N_DEV_MOSFET_B3.C:7447-7542
 //   Master::updateState                      N_DEV_MOSFET_B3.C:9199-9270
 //   Master::loadDAEVectors / loadDAEMatrices N_DEV_MOSFET_B3.C:9276-9613, 9624-9900
-// for nqsMod = 0, capMod 2 or 3, no drain/source series resistance (RSH * NRD = RSH * NRS = 0,
+// for nqsMod = 0, capMod 0, 1, 2 or 3, no drain/source series resistance (RSH * NRD = RSH * NRS = 0,
 // so D' = D and S' = S) and no instance initial conditions: the 4-terminal collapsed stamp, in
 // the same staged layout as the BSIM4 load.
 #pragma once
@@ -20,6 +20,7 @@
 #include "bsim4_eval.cuh"  // LoadFlags, RecPtr, staged layout constants
 #include "bsim4_setup.h"   // ModelSpec, SetupOptions, RecordTable
 #include "xd_consts.h"
+#include "mos_cv.h"
 
 #define XB3_FIELDS(F)                                                                               \
   /* model-level */                                                                                 \
@@ -35,7 +36,7 @@
   F(voff) F(cdep0) F(dwg) F(dwb) F(rds0) F(prwg) F(prwb) F(xj) F(a0) F(ags) F(b0) F(b1) F(keta) F(ua) \
   F(ub) F(uc) F(u0temp) F(vsattemp) F(a1) F(a2) F(delta) F(pclm) F(litl) F(thetaRout) F(pdiblb)      \
   F(pvag) F(pscbe1) F(pscbe2) F(alpha0) F(alpha1) F(beta0) F(weffCV) F(leffCV) F(noff) F(voffcv)     \
-  F(vfbzb) F(abulkCVfactor) F(acde) F(ldeb) F(moin) F(cgdo) F(cgso) F(cgbo) F(cgdl) F(cgsl) F(ckappa)
+  F(vfbzb) F(vfbcv) F(abulkCVfactor) F(acde) F(ldeb) F(moin) F(cgdo) F(cgso) F(cgbo) F(cgdl) F(cgsl) F(ckappa)
 
 namespace xb3 {
 
@@ -793,12 +794,23 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
   }
   const double cdrain = Ids, gds = Gds, gm = Gm, gmbs = Gmb, gbbs = Gbb, gbgs = Gbg, gbds = Gbd, csub = Isub;
 
-  // Intrinsic charges, capMod 2 / 3 (:6280-6930).
+  // Intrinsic charges (:5964-6930): capMod 0 (shared simple model), 1, 2, 3 (charge thickness).
   double qgate = 0.0, qdrn = 0.0, qsrc = 0.0, qbulk = 0.0;
   double cggb = 0.0, cgsb = 0.0, cgdb = 0.0, cdgb = 0.0, cdsb = 0.0, cddb = 0.0, cbgb = 0.0, cbsb = 0.0,
          cbdb = 0.0;
   const double xpart = P(xpart);
-  if (!((xpart < 0) || (!ChargeComputationNeeded))) {
+  if (((xpart < 0) || (!ChargeComputationNeeded))) {
+    // no charges
+  } else if ((int)P(capMod) == 0) {
+    // capMod = 0 (:5975-6240), the simple charge model BSIM4 shares.
+    xdc::CvCharges cv;
+    xdc::cv_simple(Vbseff, Vbs, phi, Phis, dPhis_dVb, sqrtPhis, dsqrtPhis_dVb, P(vfbcv), P(k1ox), Vgs_eff,
+                   dVgs_eff_dVg, cox * P(weffCV) * P(leffCV), Abulk0, dAbulk0_dVb, P(abulkCVfactor), Vds, xpart,
+                   true, cv);
+    qgate = cv.qgate, qbulk = cv.qbulk, qdrn = cv.qdrn;
+    cggb = cv.cggb, cgsb = cv.cgsb, cgdb = cv.cgdb, cdgb = cv.cdgb, cdsb = cv.cdsb, cddb = cv.cddb;
+    cbgb = cv.cbgb, cbsb = cv.cbsb, cbdb = cv.cbdb;
+  } else {
     double VbseffCV, dVbseffCV_dVb;
     if (Vbseff < 0.0) {
       VbseffCV = Vbseff;
@@ -840,7 +852,119 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
         dVdseffCV_dVd, dVdseffCV_dVb;
     const double vfbzb = P(vfbzb);
     const double k1ox = P(k1ox);
-    if ((int)P(capMod) == 2) {
+    if ((int)P(capMod) == 1) {
+      // capMod = 1 (:6330-6490): depletion charge from the zero-bias flat band, inversion charge
+      // of the saturation or the linear region.
+      const double Arg1 = Vgs_eff - VbseffCV - vfbzb - Vgsteff;
+      if (Arg1 <= 0.0) {
+        qgate = CoxWL * Arg1;
+        Cgg = CoxWL * (dVgs_eff_dVg - dVgsteff_dVg);
+        Cgd = -CoxWL * dVgsteff_dVd;
+        Cgb = -CoxWL * (dVbseffCV_dVb + dVgsteff_dVb);
+      } else {
+        T0 = 0.5 * k1ox;
+        T1 = sqrt(T0 * T0 + Arg1);
+        T2 = CoxWL * T0 / T1;
+        qgate = CoxWL * k1ox * (T1 - T0);
+        Cgg = T2 * (dVgs_eff_dVg - dVgsteff_dVg);
+        Cgd = -T2 * dVgsteff_dVd;
+        Cgb = -T2 * (dVbseffCV_dVb + dVgsteff_dVb);
+      }
+      qbulk = -qgate;
+      Cbg = -Cgg;
+      Cbd = -Cgd;
+      Cbb = -Cgb;
+      const double One_Third_CoxWL = CoxWL / 3.0;
+      const double Two_Third_CoxWL = 2.0 * One_Third_CoxWL;
+      AbulkCV = Abulk0 * P(abulkCVfactor);
+      dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+      VdsatCV = Vgsteff / AbulkCV;
+      if (VdsatCV < Vds) {
+        const double dVdsatCV_dVg = 1.0 / AbulkCV;
+        const double dVdsatCV_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
+        T0 = Vgsteff - VdsatCV / 3.0;
+        dT0_dVg = 1.0 - dVdsatCV_dVg / 3.0;
+        dT0_dVb = -dVdsatCV_dVb / 3.0;
+        qgate += CoxWL * T0;
+        Cgg1 = CoxWL * dT0_dVg;
+        Cgb1 = CoxWL * dT0_dVb + Cgg1 * dVgsteff_dVb;
+        Cgd1 = Cgg1 * dVgsteff_dVd;
+        Cgg1 *= dVgsteff_dVg;
+        Cgg += Cgg1;
+        Cgb += Cgb1;
+        Cgd += Cgd1;
+        T0 = VdsatCV - Vgsteff;
+        dT0_dVg = dVdsatCV_dVg - 1.0;
+        dT0_dVb = dVdsatCV_dVb;
+        qbulk += One_Third_CoxWL * T0;
+        Cbg1 = One_Third_CoxWL * dT0_dVg;
+        Cbb1 = One_Third_CoxWL * dT0_dVb + Cbg1 * dVgsteff_dVb;
+        Cbd1 = Cbg1 * dVgsteff_dVd;
+        Cbg1 *= dVgsteff_dVg;
+        Cbg += Cbg1;
+        Cbb += Cbb1;
+        Cbd += Cbd1;
+        if (xpart > 0.5)
+          T0 = -Two_Third_CoxWL;
+        else if (xpart < 0.5)
+          T0 = -0.4 * CoxWL;
+        else
+          T0 = -One_Third_CoxWL;
+        qsrc = T0 * Vgsteff;
+        Csg = T0 * dVgsteff_dVg;
+        Csb = T0 * dVgsteff_dVb;
+        Csd = T0 * dVgsteff_dVd;
+      } else {
+        T0 = AbulkCV * Vds;
+        T1 = 12.0 * (Vgsteff - 0.5 * T0 + 1.e-20);
+        T2 = Vds / T1;
+        T3 = T0 * T2;
+        dT3_dVg = -12.0 * T2 * T2 * AbulkCV;
+        dT3_dVd = 6.0 * T0 * (4.0 * Vgsteff - T0) / T1 / T1 - 0.5;
+        dT3_dVb = 12.0 * T2 * T2 * dAbulkCV_dVb * Vgsteff;
+        qgate += CoxWL * (Vgsteff - 0.5 * Vds + T3);
+        Cgg1 = CoxWL * (1.0 + dT3_dVg);
+        Cgb1 = CoxWL * dT3_dVb + Cgg1 * dVgsteff_dVb;
+        Cgd1 = CoxWL * dT3_dVd + Cgg1 * dVgsteff_dVd;
+        Cgg1 *= dVgsteff_dVg;
+        Cgg += Cgg1;
+        Cgb += Cgb1;
+        Cgd += Cgd1;
+        qbulk += CoxWL * (1.0 - AbulkCV) * (0.5 * Vds - T3);
+        Cbg1 = -CoxWL * ((1.0 - AbulkCV) * dT3_dVg);
+        Cbb1 = -CoxWL * ((1.0 - AbulkCV) * dT3_dVb + (0.5 * Vds - T3) * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb;
+        Cbd1 = -CoxWL * (1.0 - AbulkCV) * dT3_dVd + Cbg1 * dVgsteff_dVd;
+        Cbg1 *= dVgsteff_dVg;
+        Cbg += Cbg1;
+        Cbb += Cbb1;
+        Cbd += Cbd1;
+        if (xpart > 0.5) {  // 0/100
+          T1 = T1 + T1;
+          qsrc = -CoxWL * (0.5 * Vgsteff + 0.25 * T0 - T0 * T0 / T1);
+          Csg = -CoxWL * (0.5 + 24.0 * T0 * Vds / T1 / T1 * AbulkCV);
+          Csb = -CoxWL * (0.25 * Vds * dAbulkCV_dVb - 12.0 * T0 * Vds / T1 / T1 * (4.0 * Vgsteff - T0) * dAbulkCV_dVb) +
+                Csg * dVgsteff_dVb;
+          Csd = -CoxWL * (0.25 * AbulkCV - 12.0 * AbulkCV * T0 / T1 / T1 * (4.0 * Vgsteff - T0)) + Csg * dVgsteff_dVd;
+          Csg *= dVgsteff_dVg;
+        } else if (xpart < 0.5) {  // 40/60
+          T1 = T1 / 12.0;
+          T2 = 0.5 * CoxWL / (T1 * T1);
+          T3 = Vgsteff * (2.0 * T0 * T0 / 3.0 + Vgsteff * (Vgsteff - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
+          qsrc = -T2 * T3;
+          T4 = 4.0 / 3.0 * Vgsteff * (Vgsteff - T0) + 0.4 * T0 * T0;
+          Csg = -2.0 * qsrc / T1 - T2 * (Vgsteff * (3.0 * Vgsteff - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
+          Csb = (qsrc / T1 * Vds + T2 * T4 * Vds) * dAbulkCV_dVb + Csg * dVgsteff_dVb;
+          Csd = (qsrc / T1 + T2 * T4) * AbulkCV + Csg * dVgsteff_dVd;
+          Csg *= dVgsteff_dVg;
+        } else {  // 50/50
+          qsrc = -0.5 * (qgate + qbulk);
+          Csg = -0.5 * (Cgg1 + Cbg1);
+          Csb = -0.5 * (Cgb1 + Cbb1);
+          Csd = -0.5 * (Cgd1 + Cbd1);
+        }
+      }
+      qdrn = -(qgate + qbulk + qsrc);
+    } else if ((int)P(capMod) == 2) {
       const double Vfb = vfbzb;
       V3 = Vfb - Vgs_eff + VbseffCV - CONSTDELTA_3;
       if (Vfb <= 0.0) {
@@ -1251,22 +1375,47 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
       qbd = vbd * (T0 + 0.5 * T1);
       capbd = T0 + T1;
     }
-    // Overlap capacitances, capMod 2 / 3 branch (:7180-7205).
+    // Overlap capacitances (:7134-7205): constant (capMod 0), piecewise (1), smooth (2 / 3).
     const double weffCV = P(weffCV), ckappa = P(ckappa);
-    T0 = vgd + CONSTDELTA_1;
-    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
-    T2 = 0.5 * (T0 - T1);
-    T3 = weffCV * P(cgdl);
-    T4 = sqrt(1.0 - 4.0 * T2 / ckappa);
-    const double cgdo = P(cgdo) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
-    const double qgdo = (P(cgdo) + T3) * vgd - T3 * (T2 + 0.5 * ckappa * (T4 - 1.0));
-    T0 = vgs + CONSTDELTA_1;
-    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
-    T2 = 0.5 * (T0 - T1);
-    T3 = weffCV * P(cgsl);
-    T4 = sqrt(1.0 - 4.0 * T2 / ckappa);
-    const double cgso = P(cgso) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
-    const double qgso = (P(cgso) + T3) * vgs - T3 * (T2 + 0.5 * ckappa * (T4 - 1.0));
+    double cgdo, qgdo, cgso, qgso;
+    if ((int)P(capMod) == 0) {
+      cgdo = P(cgdo);
+      qgdo = P(cgdo) * vgd;
+      cgso = P(cgso);
+      qgso = P(cgso) * vgs;
+    } else if ((int)P(capMod) == 1) {
+      if (vgd < 0.0) {
+        T1 = sqrt(1.0 - 4.0 * vgd / ckappa);
+        cgdo = P(cgdo) + weffCV * P(cgdl) / T1;
+        qgdo = P(cgdo) * vgd - weffCV * 0.5 * P(cgdl) * ckappa * (T1 - 1.0);
+      } else {
+        cgdo = P(cgdo) + weffCV * P(cgdl);
+        qgdo = (weffCV * P(cgdl) + P(cgdo)) * vgd;
+      }
+      if (vgs < 0.0) {
+        T1 = sqrt(1.0 - 4.0 * vgs / ckappa);
+        cgso = P(cgso) + weffCV * P(cgsl) / T1;
+        qgso = P(cgso) * vgs - weffCV * 0.5 * P(cgsl) * ckappa * (T1 - 1.0);
+      } else {
+        cgso = P(cgso) + weffCV * P(cgsl);
+        qgso = (weffCV * P(cgsl) + P(cgso)) * vgs;
+      }
+    } else {
+      T0 = vgd + CONSTDELTA_1;
+      T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+      T2 = 0.5 * (T0 - T1);
+      T3 = weffCV * P(cgdl);
+      T4 = sqrt(1.0 - 4.0 * T2 / ckappa);
+      cgdo = P(cgdo) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+      qgdo = (P(cgdo) + T3) * vgd - T3 * (T2 + 0.5 * ckappa * (T4 - 1.0));
+      T0 = vgs + CONSTDELTA_1;
+      T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+      T2 = 0.5 * (T0 - T1);
+      T3 = weffCV * P(cgsl);
+      T4 = sqrt(1.0 - 4.0 * T2 / ckappa);
+      cgso = P(cgso) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+      qgso = (P(cgso) + T3) * vgs - T3 * (T2 + 0.5 * ckappa * (T4 - 1.0));
+    }
     // setupCapacitors_oldDAE (charge bookkeeping only, nqsMod = 0).
     const double cgbo = P(cgbo);
     const double qgd = qgdo, qgs = qgso, qgb = cgbo * vgb;

@@ -116,8 +116,8 @@ std::string process_model(const xb4::ModelSpec &spec, const xb4::SetupOptions &o
   if (!m.g("UC")) m.uc = (m.mobMod == 3) ? -0.0465 : -0.0465e-9;
   if (!m.g("UC1")) m.uc1 = (m.mobMod == 3) ? -0.056 : -0.056e-9;
   if (!m.g("U0")) m.u0 = (m.dtype == CONSTNMOS) ? 0.067 : 0.025;
-  if (m.capMod != 2 && m.capMod != 3)
-    return "BSIM3 capMod " + std::to_string((int)m.capMod) + " is not supported (capMod 2 and 3 are)";
+  if (m.capMod < 0 || m.capMod > 3)
+    return "BSIM3 capMod " + std::to_string((int)m.capMod) + " is not supported (capMod 0 to 3 are)";
   // Model::processParams.
   m.cox = 3.453133e-11 / m.tox;
   if (!m.g("TOXM")) m.toxm = m.tox;
@@ -443,7 +443,7 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const xb4::S
   S(k1) S(k3) S(k3b) S(nfactor) S(cdsc) S(cdscb) S(cdscd) S(cit) S(vfb) S(ngate) S(voff) S(cdep0) S(dwg)
   S(dwb) S(rds0) S(prwg) S(prwb) S(xj) S(a0) S(ags) S(b0) S(b1) S(keta) S(ua) S(ub) S(uc) S(u0temp)
   S(vsattemp) S(a1) S(a2) S(delta) S(pclm) S(litl) S(thetaRout) S(pdiblb) S(pvag) S(pscbe1) S(pscbe2)
-  S(alpha0) S(alpha1) S(beta0) S(weffCV) S(leffCV) S(noff) S(voffcv) S(vfbzb) S(abulkCVfactor) S(acde)
+  S(alpha0) S(alpha1) S(beta0) S(weffCV) S(leffCV) S(noff) S(voffcv) S(vfbzb) S(vfbcv) S(abulkCVfactor) S(acde)
   S(ldeb) S(moin) S(cgdo) S(cgso) S(cgbo) S(cgdl) S(cgsl) S(ckappa)
 #undef S
 #undef R

@@ -22,6 +22,7 @@
 
 #include "bsim4_fields.h"
 #include "xd_consts.h"
+#include "mos_cv.h"
 
 namespace xb4 {
 
@@ -1355,180 +1356,14 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   if ((P(xpart) < 0) || (!ChargeComputationNeeded)) {
     // all zero
   } else if (capMod == 0) {
-    // capMod = 0 (:10718-11012): a simple charge model with its own flat band (VFBCV) and
-    // threshold; the reference reassigns Vbseff, Vth, Vgst and Vdsat here, which nothing after
-    // the charge section reads, so they are local.
-    double Vbs0, dVbs0_dVb;
-    if (Vbseff < 0.0) {
-      Vbs0 = Vbs;
-      dVbs0_dVb = 1.0;
-    } else {
-      Vbs0 = phi - Phis;
-      dVbs0_dVb = -dPhis_dVb;
-    }
-    const double Vfb0 = P(vfbcv);
-    const double k1ox0 = P(k1ox);
-    const double Vth0 = Vfb0 + phi + k1ox0 * sqrtPhis;
-    const double Vgst0 = Vgs_eff - Vth0;
-    const double dVth0_dVb = k1ox0 * dsqrtPhis_dVb;
-    const double CoxWL = coxe * P(weffCV) * P(leffCV) * nf;
-    const double Arg1 = Vgs_eff - Vbs0 - Vfb0;
-    if (Arg1 <= 0.0) {  // accumulation
-      qgate = CoxWL * Arg1;
-      qbulk = -qgate;
-      qdrn = 0.0;
-      cggb = CoxWL * dVgs_eff_dVg;
-      cgdb = 0.0;
-      cgsb = CoxWL * (dVbs0_dVb - dVgs_eff_dVg);
-      cdgb = 0.0;
-      cddb = 0.0;
-      cdsb = 0.0;
-      cbgb = -CoxWL * dVgs_eff_dVg;
-      cbdb = 0.0;
-      cbsb = -cgsb;
-    } else if (Vgst0 <= 0.0) {  // depletion
-      T1 = 0.5 * k1ox0;
-      T2 = sqrt(T1 * T1 + Arg1);
-      qgate = CoxWL * k1ox0 * (T2 - T1);
-      qbulk = -qgate;
-      qdrn = 0.0;
-      T0 = CoxWL * T1 / T2;
-      cggb = T0 * dVgs_eff_dVg;
-      cgdb = 0.0;
-      cgsb = T0 * (dVbs0_dVb - dVgs_eff_dVg);
-      cdgb = 0.0;
-      cddb = 0.0;
-      cdsb = 0.0;
-      cbgb = -cggb;
-      cbdb = 0.0;
-      cbsb = -cgsb;
-    } else {  // inversion
-      const double One_Third_CoxWL = CoxWL / 3.0;
-      const double Two_Third_CoxWL = 2.0 * One_Third_CoxWL;
-      const double AbulkCV = Abulk0 * P(abulkCVfactor);
-      const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
-      const double Vdsat0 = Vgst0 / AbulkCV;
-      const double dVdsat_dVg = dVgs_eff_dVg / AbulkCV;
-      const double dVdsat_dVb = -(Vdsat0 * dAbulkCV_dVb + dVth0_dVb) / AbulkCV;
-      const double xpart = P(xpart);
-      const bool sat = (xpart > 0.5) ? (Vdsat0 <= Vds) : (Vds >= Vdsat0);
-      if (sat) {
-        T1 = Vdsat0 / 3.0;
-        qgate = CoxWL * (Vgs_eff - Vfb0 - phi - T1);
-        T2 = -Two_Third_CoxWL * Vgst0;
-        qbulk = -(qgate + T2);
-        // drain share of the inversion charge: 0 (0/100), 0.4 (40/60), 0.5 (50/50)
-        qdrn = (xpart > 0.5) ? 0.0 : ((xpart < 0.5) ? 0.4 * T2 : 0.5 * T2);
-        cggb = One_Third_CoxWL * (3.0 - dVdsat_dVg) * dVgs_eff_dVg;
-        T2 = -One_Third_CoxWL * dVdsat_dVb;
-        cgsb = -(cggb + T2);
-        cgdb = 0.0;
-        if (xpart > 0.5) {
-          cdgb = 0.0;
-          cddb = 0.0;
-          cdsb = 0.0;
-        } else if (xpart < 0.5) {
-          T3 = 0.4 * Two_Third_CoxWL;
-          cdgb = -T3 * dVgs_eff_dVg;
-          cddb = 0.0;
-          T4 = T3 * dVth0_dVb;
-          cdsb = -(T4 + cdgb);
-        } else {
-          cdgb = -One_Third_CoxWL * dVgs_eff_dVg;
-          cddb = 0.0;
-          T4 = One_Third_CoxWL * dVth0_dVb;
-          cdsb = -(T4 + cdgb);
-        }
-        cbgb = -(cggb - Two_Third_CoxWL * dVgs_eff_dVg);
-        T3 = -(T2 + Two_Third_CoxWL * dVth0_dVb);
-        cbsb = -(cbgb + T3);
-        cbdb = 0.0;
-      } else {  // linear region
-        const double Alphaz = Vgst0 / Vdsat0;
-        T1 = 2.0 * Vdsat0 - Vds;
-        T2 = Vds / (3.0 * T1);
-        T3 = T2 * Vds;
-        T9 = 0.25 * CoxWL;
-        T4 = T9 * Alphaz;
-        if (xpart > 0.5) {
-          T7 = 2.0 * Vds - T1 - 3.0 * T3;
-          T8 = T3 - T1 - 2.0 * Vds;
-        }
-        qgate = CoxWL * (Vgs_eff - Vfb0 - phi - 0.5 * (Vds - T3));
-        if (xpart > 0.5) {
-          T10 = T4 * T8;
-          qdrn = T4 * T7;
-          qbulk = -(qgate + qdrn + T10);
-        }
-        T5 = T3 / T1;
-        cggb = CoxWL * (1.0 - T5 * dVdsat_dVg) * dVgs_eff_dVg;
-        if (xpart > 0.5) {
-          T11 = -CoxWL * T5 * dVdsat_dVb;
-          cgdb = CoxWL * (T2 - 0.5 + 0.5 * T5);
-          cgsb = -(cggb + T11 + cgdb);
-        } else {
-          tmp = -CoxWL * T5 * dVdsat_dVb;
-          cgdb = CoxWL * (T2 - 0.5 + 0.5 * T5);
-          cgsb = -(cggb + cgdb + tmp);
-        }
-        T6 = 1.0 / Vdsat0;
-        const double dAlphaz_dVg = T6 * (1.0 - Alphaz * dVdsat_dVg);
-        const double dAlphaz_dVb = -T6 * (dVth0_dVb + Alphaz * dVdsat_dVb);
-        if (xpart > 0.5) {  // 0/100
-          T7 = T9 * T7;
-          T8 = T9 * T8;
-          T9 = 2.0 * T4 * (1.0 - 3.0 * T5);
-          cdgb = (T7 * dAlphaz_dVg - T9 * dVdsat_dVg) * dVgs_eff_dVg;
-          T12 = T7 * dAlphaz_dVb - T9 * dVdsat_dVb;
-          cddb = T4 * (3.0 - 6.0 * T2 - 3.0 * T5);
-          cdsb = -(cdgb + T12 + cddb);
-          T9 = 2.0 * T4 * (1.0 + T5);
-          T10 = (T8 * dAlphaz_dVg - T9 * dVdsat_dVg) * dVgs_eff_dVg;
-          T11 = T8 * dAlphaz_dVb - T9 * dVdsat_dVb;
-          T12 = T4 * (2.0 * T2 + T5 - 1.0);
-          T0 = -(T10 + T11 + T12);
-          cbgb = -(cggb + cdgb + T10);
-          cbdb = -(cgdb + cddb + T12);
-          cbsb = -(cgsb + cdsb + T0);
-        } else if (xpart < 0.5) {  // 40/60
-          T6 = 8.0 * Vdsat0 * Vdsat0 - 6.0 * Vdsat0 * Vds + 1.2 * Vds * Vds;
-          T8 = T2 / T1;
-          T7 = Vds - T1 - T8 * T6;
-          qdrn = T4 * T7;
-          T7 *= T9;
-          tmp = T8 / T1;
-          tmp1 = T4 * (2.0 - 4.0 * tmp * T6 + T8 * (16.0 * Vdsat0 - 6.0 * Vds));
-          cdgb = (T7 * dAlphaz_dVg - tmp1 * dVdsat_dVg) * dVgs_eff_dVg;
-          T10 = T7 * dAlphaz_dVb - tmp1 * dVdsat_dVb;
-          cddb = T4 * (2.0 - (1.0 / (3.0 * T1 * T1) + 2.0 * tmp) * T6 + T8 * (6.0 * Vdsat0 - 2.4 * Vds));
-          cdsb = -(cdgb + T10 + cddb);
-          T7 = 2.0 * (T1 + T3);
-          qbulk = -(qgate - T4 * T7);
-          T7 *= T9;
-          T0 = 4.0 * T4 * (1.0 - T5);
-          T12 = (-T7 * dAlphaz_dVg - cdgb - T0 * dVdsat_dVg) * dVgs_eff_dVg;
-          T11 = -T7 * dAlphaz_dVb - T10 - T0 * dVdsat_dVb;
-          T10 = -4.0 * T4 * (T2 - 0.5 + 0.5 * T5) - cddb;
-          tmp = -(T10 + T11 + T12);
-          cbgb = -(cggb + cdgb + T12);
-          cbdb = -(cgdb + cddb + T10);
-          cbsb = -(cgsb + cdsb + tmp);
-        } else {  // 50/50
-          T7 = T1 + T3;
-          qdrn = -T4 * T7;
-          qbulk = -(qgate + qdrn + qdrn);
-          T7 *= T9;
-          T0 = T4 * (2.0 * T5 - 2.0);
-          cdgb = (T0 * dVdsat_dVg - T7 * dAlphaz_dVg) * dVgs_eff_dVg;
-          T12 = T0 * dVdsat_dVb - T7 * dAlphaz_dVb;
-          cddb = T4 * (1.0 - 2.0 * T2 - T5);
-          cdsb = -(cdgb + T12 + cddb);
-          cbgb = -(cggb + 2.0 * cdgb);
-          cbdb = -(cgdb + 2.0 * cddb);
-          cbsb = -(cgsb + 2.0 * cdsb);
-        }
-      }
-    }
+    // capMod = 0 (:10718-11012), the simple charge model BSIM3 shares.
+    xdc::CvCharges cv;
+    xdc::cv_simple(Vbseff, Vbs, phi, Phis, dPhis_dVb, sqrtPhis, dsqrtPhis_dVb, P(vfbcv), P(k1ox), Vgs_eff,
+                   dVgs_eff_dVg, coxe * P(weffCV) * P(leffCV) * nf, Abulk0, dAbulk0_dVb, P(abulkCVfactor), Vds,
+                   P(xpart), false, cv);
+    qgate = cv.qgate, qbulk = cv.qbulk, qdrn = cv.qdrn;
+    cggb = cv.cggb, cgsb = cv.cgsb, cgdb = cv.cgdb, cdgb = cv.cdgb, cdsb = cv.cdsb, cddb = cv.cddb;
+    cbgb = cv.cbgb, cbsb = cv.cbsb, cbdb = cv.cbdb;
   } else {
     double VbseffCV, dVbseffCV_dVb;
     if (Vbseff < 0.0) {

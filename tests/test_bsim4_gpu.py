@@ -65,7 +65,7 @@ def _num_variants():
     return _native.load().xd_num_eval_variants()
 
 
-@pytest.mark.parametrize("v", range(6))
+@pytest.mark.parametrize("v", range(8))
 def test_parity_every_eval_launch_variant(v):
     """The autotuner may pick any launch shape of the evaluation kernel; each is held to the
     oracle, with an instance count that leaves a partial last block."""
@@ -111,6 +111,39 @@ def test_parity_capmod_0_and_1(capmod, xpart, cvc):
              ModelCard(True, {"CAPMOD": capmod, "XPART": xpart, "CVCHARGEMOD": cvc, "VFBCV": -0.8})]
     worst = _run_sequence(c, cards, TRANSIENT_SEQ[:4] + DC_SEQ[2:3], vrange=(-0.4, 1.6), seed=capmod + 7)
     print("capMod", capmod, "xpart", xpart, "worst error / tolerance:", worst)
+
+
+@pytest.mark.parametrize("igc,igb,cards_extra", [
+    (1, 0, {}), (2, 0, {"PIGCD": 1.5}), (0, 1, {}), (2, 1, {"TOXE": 1.4e-9, "NF": 2.0, "AIGSD": 0.012}),
+])
+def test_parity_gate_tunnelling(igc, igb, cards_extra):
+    """Gate tunnelling currents: gate to channel partitioned to source and drain (igcMod 1, with the
+    bias-dependent partition, and 2 with a given PIGCD), gate to source / drain overlap, gate to
+    bulk in accumulation and inversion (igbMod 1), thin oxide so the currents matter, multi-finger
+    scaling; both operating modes (the random iterate puts drain below source on many devices)."""
+    c = netlist.random_logic(1500, seed=41 + igc + 2 * igb)
+    common = {"IGCMOD": igc, "IGBMOD": igb, "TOXE": cards_extra.get("TOXE", 1.8e-9)}
+    common.update({k: v for k, v in cards_extra.items() if k not in ("TOXE", "NF")})
+    cards = [ModelCard(False, dict(common)), ModelCard(True, dict(common))]
+    extra = {"NF": np.full(c.n_mos, cards_extra["NF"])} if "NF" in cards_extra else None
+    worst = _run_sequence(c, cards, TRANSIENT_SEQ[:4] + DC_SEQ[:2], extra_params=extra, vrange=(-0.6, 1.8),
+                          seed=igc + igb)
+    print("igcMod", igc, "igbMod", igb, "worst error / tolerance:", worst)
+
+
+def test_gate_tunnelling_family_refuses_variants_without_it():
+    from xyce_b200 import _native
+
+    c = netlist.random_logic(200, seed=3)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, [ModelCard(False, {"IGCMOD": 1}), ModelCard(True, {})])
+    dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
+    lib = _native.load()
+    ok = []
+    for v in range(lib.xd_num_eval_variants()):
+        ok.append(lib.xd_set_eval_variant(dev._h, v) == 0)
+    dev.close()
+    assert ok == [False] * 6 + [True] * 2
 
 
 def test_parity_inverter_ring_bsim4():

@@ -24,6 +24,8 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
     (3, NMOS_PMOS, None, "not implemented"),
     (14, [ModelCard(False, {"RGATEMOD": 1}), ModelCard(True, {})], None, "rgateMod"),
     (14, [ModelCard(False, {"CAPMOD": 3}), ModelCard(True, {})], None, "capMod must be 0, 1 or 2"),
+    (14, [ModelCard(False, {"IGCMOD": 3}), ModelCard(True, {})], None, "igcMod must be 0, 1 or 2"),
+    (14, [ModelCard(False, {}), ModelCard(True, {"IGBMOD": 2})], None, "igbMod must be 0 or 1"),
     (14, NMOS_PMOS, {"NRD": 2.0}, "NRD/NRS"),
     (14, [ModelCard(False, {"NOSUCH": 1.0}), ModelCard(True, {})], None, "unknown BSIM4 model parameter"),
     (9, [ModelCard(False, {"CAPMOD": 4}), ModelCard(True, {})], None, "capMod"),

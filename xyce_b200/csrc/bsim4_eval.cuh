@@ -11,7 +11,7 @@
 //   Instance::auxChargeCalculations      N_DEV_MOSFET_B4.C:12216-12350
 //   Master::loadDAEVectors / loadDAEMatrices  N_DEV_MOSFET_B4.C:16303-16567, 16577-17268
 // for the configuration the set-up accepts: rgateMod = rbodyMod = trnqsMod = acnqsMod = rdsMod = 0,
-// igcMod = igbMod = 0, capMod = 0, 1 or 2, no source/drain resistance nodes, no initial conditions. With
+// igcMod 0/1/2, igbMod 0/1, capMod 0/1/2, no source/drain resistance nodes, no initial conditions. With
 // no internal nodes the 11 stamp rows collapse onto the 4 terminals D, G, S, B.
 //
 // Local stamp layout (terminal order D=0, G=1, S=2, B=3):
@@ -82,7 +82,10 @@ XD_HD void poly_depletion(double phi, double ngate, double epsgate, double coxe,
 // V[4] = node voltages (D, G, S, B); sto_old = the store values the limiter compares against
 // (currSto on Newton step 0 of a transient step, nextSto otherwise); vgb_orig = the previous load's
 // vgb of this instance (0 before the first load), which the reference uses as the "original" vgb.
-template <class RV>
+// IGC = false compiles the load without the gate tunnelling currents (igcMod = igbMod = 0 whatever
+// the record says): the default kernel keeps its register allocation; families whose cards
+// enable tunnelling run the IGC = true instantiation.
+template <bool IGC = false, class RV>
 XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
                       LoadOut &o) {
   using namespace xdc;
@@ -1340,7 +1343,324 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     Igisl *= T7;
   }
   double ggisls = Ggisls, ggislg = Ggislg, ggislb = Ggislb;
-  // Gate tunnelling currents are off (igcMod = igbMod = 0).
+  // Gate tunnelling currents (:10183-10600): gate to channel (igcMod, partitioned between source
+  // and drain), gate to source / drain overlap (with igcMod) and gate to bulk (igbMod).
+  const int igcMod = IGC ? (int)P(igcMod) : 0, igbMod = IGC ? (int)P(igbMod) : 0;
+  double Igcs = 0.0, gIgcsg = 0.0, gIgcsd = 0.0, gIgcsb = 0.0;
+  double Igcd = 0.0, gIgcdg = 0.0, gIgcdd = 0.0, gIgcdb = 0.0;
+  double Igs = 0.0, gIgsg = 0.0, gIgss = 0.0, Igd = 0.0, gIgdg = 0.0, gIgdd = 0.0;
+  double Igb = 0.0, gIgbg = 0.0, gIgbd = 0.0, gIgbb = 0.0;
+  if (igcMod != 0 || igbMod != 0) {
+    double Vfb_g = P(vfbzb);
+    double Voxacc = 0.0, dVoxacc_dVg = 0.0, dVoxacc_dVb = 0.0;
+    double Voxdepinv = 0.0, dVoxdepinv_dVg = 0.0, dVoxdepinv_dVd = 0.0, dVoxdepinv_dVb = 0.0;
+    {
+      const double V3 = Vfb_g - Vgs_eff + Vbseff - CONSTDELTA_3;
+      if (Vfb_g <= 0.0)
+        T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * Vfb_g);
+      else
+        T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * Vfb_g);
+      T1 = 0.5 * (1.0 + V3 / T0);
+      const double Vfbeff = Vfb_g - 0.5 * (V3 + T0);
+      const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
+      const double dVfbeff_dVb = -T1;
+      Voxacc = Vfb_g - Vfbeff;
+      dVoxacc_dVg = -dVfbeff_dVg;
+      dVoxacc_dVb = -dVfbeff_dVb;
+      if (Voxacc < 0.0) {
+        Voxacc = dVoxacc_dVg = dVoxacc_dVb = 0.0;
+      }
+      const double k1ox = P(k1ox);
+      T0 = 0.5 * k1ox;
+      T3 = Vgs_eff - Vfbeff - Vbseff - Vgsteff;
+      if (k1ox == 0.0) {
+        Voxdepinv = dVoxdepinv_dVg = dVoxdepinv_dVd = dVoxdepinv_dVb = 0.0;
+      } else if (T3 < 0.0) {
+        Voxdepinv = -T3;
+        dVoxdepinv_dVg = -dVgs_eff_dVg + dVfbeff_dVg + dVgsteff_dVg;
+        dVoxdepinv_dVd = dVgsteff_dVd;
+        dVoxdepinv_dVb = dVfbeff_dVb + 1.0 + dVgsteff_dVb;
+      } else {
+        T1 = sqrt(T0 * T0 + T3);
+        T2 = T0 / T1;
+        Voxdepinv = k1ox * (T1 - T0);
+        dVoxdepinv_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg);
+        dVoxdepinv_dVd = -T2 * dVgsteff_dVd;
+        dVoxdepinv_dVb = -T2 * (dVfbeff_dVb + 1.0 + dVgsteff_dVb);
+      }
+      Voxdepinv += Vgsteff;
+      dVoxdepinv_dVg += dVgsteff_dVg;
+      dVoxdepinv_dVd += dVgsteff_dVd;
+      dVoxdepinv_dVb += dVgsteff_dVb;
+    }
+    const double vtmg = (tempMod < 2) ? Vtm : Vtm0;
+    double Vaux = 0.0, dVaux_dVg = 0.0, dVaux_dVd = 0.0, dVaux_dVb = 0.0, VxNVt = 0.0;
+    if (igcMod) {
+      T0 = vtmg * P(nigc);
+      if (igcMod == 1) {
+        VxNVt = (Vgs_eff - dtype * vth0) / T0;
+        if (VxNVt > CONSTEXP_THRESHOLD) {
+          Vaux = Vgs_eff - dtype * vth0;
+          dVaux_dVg = dVgs_eff_dVg;
+          dVaux_dVd = 0.0;
+          dVaux_dVb = 0.0;
+        }
+      } else {
+        VxNVt = (Vgs_eff - von) / T0;
+        if (VxNVt > CONSTEXP_THRESHOLD) {
+          Vaux = Vgs_eff - von;
+          dVaux_dVg = dVgs_eff_dVg;
+          dVaux_dVd = -dVth_dVd;
+          dVaux_dVb = -dVth_dVb;
+        }
+      }
+      if (VxNVt < -CONSTEXP_THRESHOLD) {
+        Vaux = T0 * log(1.0 + CONSTMIN_EXP);
+        dVaux_dVg = dVaux_dVd = dVaux_dVb = 0.0;
+      } else if ((VxNVt >= -CONSTEXP_THRESHOLD) && (VxNVt <= CONSTEXP_THRESHOLD)) {
+        const double ExpVxNVt = exp(VxNVt);
+        Vaux = T0 * log(1.0 + ExpVxNVt);
+        dVaux_dVg = ExpVxNVt / (1.0 + ExpVxNVt);
+        if (igcMod == 1) {
+          dVaux_dVd = 0.0;
+          dVaux_dVb = 0.0;
+        } else {
+          dVaux_dVd = -dVgs_eff_dVg * dVth_dVd;
+          dVaux_dVb = -dVgs_eff_dVg * dVth_dVb;
+        }
+        dVaux_dVg *= dVgs_eff_dVg;
+      }
+      T2 = Vgs_eff * Vaux;
+      dT2_dVg = dVgs_eff_dVg * Vaux + Vgs_eff * dVaux_dVg;
+      dT2_dVd = Vgs_eff * dVaux_dVd;
+      dT2_dVb = Vgs_eff * dVaux_dVb;
+      T11 = P(Aechvb);
+      T12 = P(Bechvb);
+      T3 = P(aigc) * P(cigc) - P(bigc);
+      T4 = P(bigc) * P(cigc);
+      T5 = T12 * (P(aigc) + T3 * Voxdepinv - T4 * Voxdepinv * Voxdepinv);
+      if (T5 > CONSTEXP_THRESHOLD) {
+        T6 = CONSTMAX_EXP;
+        dT6_dVg = dT6_dVd = dT6_dVb = 0.0;
+      } else if (T5 < -CONSTEXP_THRESHOLD) {
+        T6 = CONSTMIN_EXP;
+        dT6_dVg = dT6_dVd = dT6_dVb = 0.0;
+      } else {
+        T6 = exp(T5);
+        dT6_dVg = T6 * T12 * (T3 - 2.0 * T4 * Voxdepinv);
+        dT6_dVd = dT6_dVg * dVoxdepinv_dVd;
+        dT6_dVb = dT6_dVg * dVoxdepinv_dVb;
+        dT6_dVg *= dVoxdepinv_dVg;
+      }
+      const double Igc = T11 * T2 * T6;
+      const double dIgc_dVg = T11 * (T2 * dT6_dVg + T6 * dT2_dVg);
+      const double dIgc_dVd = T11 * (T2 * dT6_dVd + T6 * dT2_dVd);
+      const double dIgc_dVb = T11 * (T2 * dT6_dVb + T6 * dT2_dVb);
+      double Pigcd, dPigcd_dVg, dPigcd_dVd, dPigcd_dVb;
+      if (P(pigcdGiven) != 0.0) {
+        Pigcd = P(pigcd);
+        dPigcd_dVg = dPigcd_dVd = dPigcd_dVb = 0.0;
+      } else {
+        T11 = P(Bechvb) * toxe;
+        T12 = Vgsteff + 1.0e-20;
+        T13 = T11 / T12 / T12;
+        T14 = -T13 / T12;
+        Pigcd = T13 * (1.0 - 0.5 * Vdseff / T12);
+        dPigcd_dVg = T14 * (2.0 + 0.5 * (dVdseff_dVg - 3.0 * Vdseff / T12));
+        dPigcd_dVd = 0.5 * T14 * dVdseff_dVd;
+        dPigcd_dVb = 0.5 * T14 * dVdseff_dVb;
+      }
+      T7 = -Pigcd * Vdseff;
+      double dT7_dVg = -Vdseff * dPigcd_dVg - Pigcd * dVdseff_dVg;
+      double dT7_dVd = -Vdseff * dPigcd_dVd - Pigcd * dVdseff_dVd + dT7_dVg * dVgsteff_dVd;
+      double dT7_dVb = -Vdseff * dPigcd_dVb - Pigcd * dVdseff_dVb + dT7_dVg * dVgsteff_dVb;
+      dT7_dVg *= dVgsteff_dVg;
+      dT7_dVb *= dVbseff_dVb;
+      T8 = T7 * T7 + 2.0e-4;
+      dT8_dVg = 2.0 * T7;
+      dT8_dVd = dT8_dVg * dT7_dVd;
+      dT8_dVb = dT8_dVg * dT7_dVb;
+      dT8_dVg *= dT7_dVg;
+      if (T7 > CONSTEXP_THRESHOLD) {
+        T9 = CONSTMAX_EXP;
+        dT9_dVg = dT9_dVd = dT9_dVb = 0.0;
+      } else if (T7 < -CONSTEXP_THRESHOLD) {
+        T9 = CONSTMIN_EXP;
+        dT9_dVg = dT9_dVd = dT9_dVb = 0.0;
+      } else {
+        T9 = exp(T7);
+        dT9_dVg = T9 * dT7_dVg;
+        dT9_dVd = T9 * dT7_dVd;
+        dT9_dVb = T9 * dT7_dVb;
+      }
+      T0 = T8 * T8;
+      T1 = T9 - 1.0 + 1.0e-4;
+      T10 = (T1 - T7) / T8;
+      dT10_dVg = (dT9_dVg - dT7_dVg - T10 * dT8_dVg) / T8;
+      dT10_dVd = (dT9_dVd - dT7_dVd - T10 * dT8_dVd) / T8;
+      dT10_dVb = (dT9_dVb - dT7_dVb - T10 * dT8_dVb) / T8;
+      Igcs = Igc * T10;
+      const double dIgcs_dVg = dIgc_dVg * T10 + Igc * dT10_dVg;
+      const double dIgcs_dVd = dIgc_dVd * T10 + Igc * dT10_dVd;
+      const double dIgcs_dVb = dIgc_dVb * T10 + Igc * dT10_dVb;
+      T1 = T9 - 1.0 - 1.0e-4;
+      T10 = (T7 * T9 - T1) / T8;
+      dT10_dVg = (dT7_dVg * T9 + (T7 - 1.0) * dT9_dVg - T10 * dT8_dVg) / T8;
+      dT10_dVd = (dT7_dVd * T9 + (T7 - 1.0) * dT9_dVd - T10 * dT8_dVd) / T8;
+      dT10_dVb = (dT7_dVb * T9 + (T7 - 1.0) * dT9_dVb - T10 * dT8_dVb) / T8;
+      Igcd = Igc * T10;
+      const double dIgcd_dVg = dIgc_dVg * T10 + Igc * dT10_dVg;
+      const double dIgcd_dVd = dIgc_dVd * T10 + Igc * dT10_dVd;
+      const double dIgcd_dVb = dIgc_dVb * T10 + Igc * dT10_dVb;
+      gIgcsg = dIgcs_dVg;
+      gIgcsd = dIgcs_dVd;
+      gIgcsb = dIgcs_dVb * dVbseff_dVb;
+      gIgcdg = dIgcd_dVg;
+      gIgcdd = dIgcd_dVd;
+      gIgcdb = dIgcd_dVb * dVbseff_dVb;
+      // Gate to source and drain overlap tunnelling, on the terminal (not mode-ordered) voltages.
+      const double vfbsd_t = P(vfbsd) + P(vfbsdoff);
+      T0 = vgs - vfbsd_t;
+      double vgx_eff = sqrt(T0 * T0 + 1.0e-4);
+      double dvgx_eff_dvg = T0 / vgx_eff;
+      T2 = vgs * vgx_eff;
+      dT2_dVg = vgs * dvgx_eff_dvg + vgx_eff;
+      T11 = P(AechvbEdgeS);
+      T12 = P(BechvbEdge);
+      T3 = P(aigs) * P(cigs) - P(bigs);
+      T4 = P(bigs) * P(cigs);
+      T5 = T12 * (P(aigs) + T3 * vgx_eff - T4 * vgx_eff * vgx_eff);
+      if (T5 > CONSTEXP_THRESHOLD) {
+        T6 = CONSTMAX_EXP;
+        dT6_dVg = 0.0;
+      } else if (T5 < -CONSTEXP_THRESHOLD) {
+        T6 = CONSTMIN_EXP;
+        dT6_dVg = 0.0;
+      } else {
+        T6 = exp(T5);
+        dT6_dVg = T6 * T12 * (T3 - 2.0 * T4 * vgx_eff) * dvgx_eff_dvg;
+      }
+      Igs = T11 * T2 * T6;
+      const double dIgs_dVg = T11 * (T2 * dT6_dVg + T6 * dT2_dVg);
+      const double dIgs_dVs = -dIgs_dVg;
+      T0 = vgd - vfbsd_t;
+      vgx_eff = sqrt(T0 * T0 + 1.0e-4);
+      dvgx_eff_dvg = T0 / vgx_eff;
+      T2 = vgd * vgx_eff;
+      dT2_dVg = vgd * dvgx_eff_dvg + vgx_eff;
+      T11 = P(AechvbEdgeD);
+      T3 = P(aigd) * P(cigd) - P(bigd);
+      T4 = P(bigd) * P(cigd);
+      T5 = T12 * (P(aigd) + T3 * vgx_eff - T4 * vgx_eff * vgx_eff);
+      if (T5 > CONSTEXP_THRESHOLD) {
+        T6 = CONSTMAX_EXP;
+        dT6_dVg = 0.0;
+      } else if (T5 < -CONSTEXP_THRESHOLD) {
+        T6 = CONSTMIN_EXP;
+        dT6_dVg = 0.0;
+      } else {
+        T6 = exp(T5);
+        dT6_dVg = T6 * T12 * (T3 - 2.0 * T4 * vgx_eff) * dvgx_eff_dvg;
+      }
+      Igd = T11 * T2 * T6;
+      const double dIgd_dVg = T11 * (T2 * dT6_dVg + T6 * dT2_dVg);
+      const double dIgd_dVd = -dIgd_dVg;
+      gIgsg = dIgs_dVg;
+      gIgss = dIgs_dVs;
+      gIgdg = dIgd_dVg;
+      gIgdd = dIgd_dVd;
+    }
+    if (igbMod) {
+      T0 = vtmg * P(nigbacc);
+      T1 = -Vgs_eff + Vbseff + Vfb_g;
+      VxNVt = T1 / T0;
+      if (VxNVt > CONSTEXP_THRESHOLD) {
+        Vaux = T1;
+        dVaux_dVg = -dVgs_eff_dVg;
+        dVaux_dVb = 1.0;
+      } else if (VxNVt < -CONSTEXP_THRESHOLD) {
+        Vaux = T0 * log(1.0 + CONSTMIN_EXP);
+        dVaux_dVg = dVaux_dVb = 0.0;
+      } else {
+        const double ExpVxNVt = exp(VxNVt);
+        Vaux = T0 * log(1.0 + ExpVxNVt);
+        dVaux_dVb = ExpVxNVt / (1.0 + ExpVxNVt);
+        dVaux_dVg = -dVaux_dVb * dVgs_eff_dVg;
+      }
+      T2 = (Vgs_eff - Vbseff) * Vaux;
+      dT2_dVg = dVgs_eff_dVg * Vaux + (Vgs_eff - Vbseff) * dVaux_dVg;
+      dT2_dVb = -Vaux + (Vgs_eff - Vbseff) * dVaux_dVb;
+      T11 = 4.97232e-7 * P(weff) * P(leff) * P(ToxRatio);
+      T12 = -7.45669e11 * toxe;
+      T3 = P(aigbacc) * P(cigbacc) - P(bigbacc);
+      T4 = P(bigbacc) * P(cigbacc);
+      T5 = T12 * (P(aigbacc) + T3 * Voxacc - T4 * Voxacc * Voxacc);
+      if (T5 > CONSTEXP_THRESHOLD) {
+        T6 = CONSTMAX_EXP;
+        dT6_dVg = dT6_dVb = 0.0;
+      } else if (T5 < -CONSTEXP_THRESHOLD) {
+        T6 = CONSTMIN_EXP;
+        dT6_dVg = dT6_dVb = 0.0;
+      } else {
+        T6 = exp(T5);
+        dT6_dVg = T6 * T12 * (T3 - 2.0 * T4 * Voxacc);
+        dT6_dVb = dT6_dVg * dVoxacc_dVb;
+        dT6_dVg *= dVoxacc_dVg;
+      }
+      const double Igbacc = T11 * T2 * T6;
+      const double dIgbacc_dVg = T11 * (T2 * dT6_dVg + T6 * dT2_dVg);
+      const double dIgbacc_dVb = T11 * (T2 * dT6_dVb + T6 * dT2_dVb);
+      T0 = vtmg * P(nigbinv);
+      T1 = Voxdepinv - P(eigbinv);
+      VxNVt = T1 / T0;
+      if (VxNVt > CONSTEXP_THRESHOLD) {
+        Vaux = T1;
+        dVaux_dVg = dVoxdepinv_dVg;
+        dVaux_dVd = dVoxdepinv_dVd;
+        dVaux_dVb = dVoxdepinv_dVb;
+      } else if (VxNVt < -CONSTEXP_THRESHOLD) {
+        Vaux = T0 * log(1.0 + CONSTMIN_EXP);
+        dVaux_dVg = dVaux_dVd = dVaux_dVb = 0.0;
+      } else {
+        const double ExpVxNVt = exp(VxNVt);
+        Vaux = T0 * log(1.0 + ExpVxNVt);
+        dVaux_dVg = ExpVxNVt / (1.0 + ExpVxNVt);
+        dVaux_dVd = dVaux_dVg * dVoxdepinv_dVd;
+        dVaux_dVb = dVaux_dVg * dVoxdepinv_dVb;
+        dVaux_dVg *= dVoxdepinv_dVg;
+      }
+      T2 = (Vgs_eff - Vbseff) * Vaux;
+      dT2_dVg = dVgs_eff_dVg * Vaux + (Vgs_eff - Vbseff) * dVaux_dVg;
+      dT2_dVd = (Vgs_eff - Vbseff) * dVaux_dVd;
+      dT2_dVb = -Vaux + (Vgs_eff - Vbseff) * dVaux_dVb;
+      T11 *= 0.75610;
+      T12 *= 1.31724;
+      T3 = P(aigbinv) * P(cigbinv) - P(bigbinv);
+      T4 = P(bigbinv) * P(cigbinv);
+      T5 = T12 * (P(aigbinv) + T3 * Voxdepinv - T4 * Voxdepinv * Voxdepinv);
+      if (T5 > CONSTEXP_THRESHOLD) {
+        T6 = CONSTMAX_EXP;
+        dT6_dVg = dT6_dVd = dT6_dVb = 0.0;
+      } else if (T5 < -CONSTEXP_THRESHOLD) {
+        T6 = CONSTMIN_EXP;
+        dT6_dVg = dT6_dVd = dT6_dVb = 0.0;
+      } else {
+        T6 = exp(T5);
+        dT6_dVg = T6 * T12 * (T3 - 2.0 * T4 * Voxdepinv);
+        dT6_dVd = dT6_dVg * dVoxdepinv_dVd;
+        dT6_dVb = dT6_dVg * dVoxdepinv_dVb;
+        dT6_dVg *= dVoxdepinv_dVg;
+      }
+      const double Igbinv = T11 * T2 * T6;
+      const double dIgbinv_dVg = T11 * (T2 * dT6_dVg + T6 * dT2_dVg);
+      const double dIgbinv_dVd = T11 * (T2 * dT6_dVd + T6 * dT2_dVd);
+      const double dIgbinv_dVb = T11 * (T2 * dT6_dVb + T6 * dT2_dVb);
+      Igb = Igbinv + Igbacc;
+      gIgbg = dIgbinv_dVg + dIgbacc_dVg;
+      gIgbd = dIgbinv_dVd;
+      gIgbb = (dIgbinv_dVb + dIgbacc_dVb) * dVbseff_dVb;
+    }
+  }
 
   // Multi-finger scaling (:10601-10640).
   if (nf != 1.0) {
@@ -1348,7 +1668,15 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     gbbs *= nf; gbgs *= nf; gbds *= nf; csub *= nf;
     Igidl *= nf; ggidld *= nf; ggidlg *= nf; ggidlb *= nf;
     Igisl *= nf; ggisls *= nf; ggislg *= nf; ggislb *= nf;
+    Igcs *= nf; gIgcsg *= nf; gIgcsd *= nf; gIgcsb *= nf;
+    Igcd *= nf; gIgcdg *= nf; gIgcdd *= nf; gIgcdb *= nf;
+    Igs *= nf; gIgsg *= nf; gIgss *= nf;
+    Igd *= nf; gIgdg *= nf; gIgdd *= nf;
+    Igb *= nf; gIgbg *= nf; gIgbd *= nf; gIgbb *= nf;
   }
+  const double gIgbs = -(gIgbg + gIgbd + gIgbb);
+  const double gIgcss = -(gIgcsg + gIgcsd + gIgcsb);
+  const double gIgcds = -(gIgcdg + gIgcdd + gIgcdb);
 
   // Intrinsic charges (:10707-11620): capMod 0, 1 or 2 (charge-thickness model).
   double qgate = 0, qdrn = 0, qbulk = 0, qsrc = 0;
@@ -2026,7 +2354,7 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
   o.vgb = vgb;
 
-  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0, no gate current.
+  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0.
   const double gjbd = gbd, gjbs = gbs;
   double Gmv, Gmbsv, FwdSum, RevSum, ceqdrn, ceqdrn_Jdxp, ceqbd, ceqbd_Jdxp, ceqbs, ceqbs_Jdxp;
   double gbbdp, gbbsp, gbdpg, gbdpdp, gbdpb, gbdpsp, gbspg, gbspdp, gbspb, gbspsp;
@@ -2075,12 +2403,72 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     gbspb = gbbs;
     gbspdp = -(gbspg + gbspsp + gbspb);
   }
-  const double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0, ceqgcrg = 0.0;
-  const double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0, ceqgcrg_Jdxp = 0.0;
-  const double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
-  const double gIdtotg = 0.0, gIdtotd = 0.0, gIdtots = 0.0, gIdtotb = 0.0;
-  const double gIbtotg = 0.0, gIbtotd = 0.0, gIbtots = 0.0, gIbtotb = 0.0;
-  const double gIgtotg = 0.0, gIgtotd = 0.0, gIgtots = 0.0, gIgtotb = 0.0;
+  // Gate-current totals (:13112-13170, mode >= 0; :13243-13300, mode < 0).
+  const double ceqgcrg = 0.0, ceqgcrg_Jdxp = 0.0;
+  double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0;
+  double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0;
+  double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
+  double gIdtotg = 0.0, gIdtotd = 0.0, gIdtots = 0.0, gIdtotb = 0.0;
+  double gIbtotg = 0.0, gIbtotd = 0.0, gIbtots = 0.0, gIbtotb = 0.0;
+  double gIgtotg = 0.0, gIgtotd = 0.0, gIgtots = 0.0, gIgtotb = 0.0;
+  if (mode >= 0) {
+    if (igcMod) {
+      gIstotg = gIgsg + gIgcsg;
+      gIstotd = gIgcsd;
+      gIstots = gIgss + gIgcss;
+      gIstotb = gIgcsb;
+      Istoteq = dtype * (Igs + Igcs);
+      Istoteq_Jdxp = dtype * (-gIstotg * (vgs - vgs_orig) - gIgcsd * (vds - vds_orig) - gIgcsb * (vbs - vbs_orig));
+      gIdtotg = gIgdg + gIgcdg;
+      gIdtotd = gIgdd + gIgcdd;
+      gIdtots = gIgcds;
+      gIdtotb = gIgcdb;
+      Idtoteq = dtype * (Igd + Igcd);
+      Idtoteq_Jdxp = dtype * (-gIgdg * (vgd - vgd_orig) - gIgcdg * (vgs - vgs_orig) - gIgcdd * (vds - vds_orig) -
+                              gIgcdb * (vbs - vbs_orig));
+    }
+    if (igbMod) {
+      gIbtotg = gIgbg;
+      gIbtotd = gIgbd;
+      gIbtots = gIgbs;
+      gIbtotb = gIgbb;
+      Ibtoteq = dtype * Igb;
+      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgs - vgs_orig) - gIgbd * (vds - vds_orig) - gIgbb * (vbs - vbs_orig));
+    }
+  } else {
+    if (igcMod) {
+      gIstotg = gIgsg + gIgcdg;
+      gIstotd = gIgcds;
+      gIstots = gIgss + gIgcdd;
+      gIstotb = gIgcdb;
+      Istoteq = dtype * (Igs + Igcd);
+      Istoteq_Jdxp = dtype * (-gIgsg * (vgs - vgs_orig) - gIgcdg * (vgd - vgd_orig) + gIgcdd * (vds - vds_orig) -
+                              gIgcdb * (vbd - vbd_orig));
+      gIdtotg = gIgdg + gIgcsg;
+      gIdtotd = gIgdd + gIgcss;
+      gIdtots = gIgcsd;
+      gIdtotb = gIgcsb;
+      Idtoteq = dtype * (Igd + Igcs);
+      Idtoteq_Jdxp = dtype * (-(gIgdg + gIgcsg) * (vgd - vgd_orig) + gIgcsd * (vds - vds_orig) -
+                              gIgcsb * (vbd - vbd_orig));
+    }
+    if (igbMod) {
+      gIbtotg = gIgbg;
+      gIbtotd = gIgbs;
+      gIbtots = gIgbd;
+      gIbtotb = gIgbb;
+      Ibtoteq = dtype * Igb;
+      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgd - vgd_orig) + gIgbd * (vds - vds_orig) - gIgbb * (vbd - vbd_orig));
+    }
+  }
+  if (igcMod != 0 || igbMod != 0) {
+    gIgtotg = gIstotg + gIdtotg + gIbtotg;
+    gIgtotd = gIstotd + gIdtotd + gIbtotd;
+    gIgtots = gIstots + gIdtots + gIbtots;
+    gIgtotb = gIstotb + gIdtotb + gIbtotb;
+    Igtoteq = Istoteq + Idtoteq + Ibtoteq;
+    Igtoteq_Jdxp = Istoteq_Jdxp + Idtoteq_Jdxp + Ibtoteq_Jdxp;
+  }
   const double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
   const double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
   double ceqjs, ceqjs_Jdxp, ceqjd, ceqjd_Jdxp;

@@ -35,7 +35,10 @@
   F(alpha1) F(beta0) F(vtl) F(tfactor) F(xrcrg1) F(xrcrg2) F(vfbsd) F(egidl) F(agidl) F(bgidl)    \
   F(cgidl) F(weffCJ) F(egisl) F(agisl) F(bgisl) F(cgisl) F(abulkCVfactor) F(weffCV) F(leffCV)     \
   F(noff) F(voffcv) F(mstarcv) F(voffcbncv) F(acde) F(ldeb) F(moin) F(cgbo) F(cgdo) F(cgso)       \
-  F(cgdl) F(cgsl) F(ckappad) F(ckappas) F(vfbcv)                                                 \
+  F(cgdl) F(cgsl) F(ckappad) F(ckappas) F(vfbcv) F(Aechvb) F(Bechvb) F(AechvbEdgeS) F(AechvbEdgeD)  \
+  F(BechvbEdge) F(ToxRatio) F(aigc) F(bigc) F(cigc) F(nigc) F(pigcd) F(pigcdGiven) F(vfbsdoff)      \
+  F(aigs) F(bigs) F(cigs) F(aigd) F(bigd) F(cigd) F(nigbacc) F(aigbacc) F(bigbacc) F(cigbacc)       \
+  F(nigbinv) F(eigbinv) F(aigbinv) F(bigbinv) F(cigbinv)                                           \
   /* instance-level */                                                                           \
   F(vth0) F(eta0) F(k2ox) F(vfb) F(vbsc) F(u0temp) F(vsattemp) F(vtfbphi1) F(vtfbphi2) F(vfbzb)   \
   F(nf) F(mult) F(Aseff) F(Pseff) F(Adeff) F(Pdeff) F(XExpBVS) F(XExpBVD) F(vjsmFwd) F(vjsmRev)   \

@@ -238,7 +238,8 @@ std::string process_model(const ModelSpec &spec, const SetupOptions &opts, Card 
   // Features outside the load kernel's scope are refused here rather than mis-evaluated.
   if (m.mtrlMod != 0) return "BSIM4 mtrlMod != 0 is not supported";
   if (m.rdsMod != 0) return "BSIM4 rdsMod != 0 is not supported";
-  if (m.igcMod != 0 || m.igbMod != 0) return "BSIM4 gate tunnelling (igcMod/igbMod != 0) is not supported";
+  if (m.igcMod < 0 || m.igcMod > 2) return "BSIM4 igcMod must be 0, 1 or 2";
+  if (m.igbMod < 0 || m.igbMod > 1) return "BSIM4 igbMod must be 0 or 1";
   if (m.rgateMod != 0) return "BSIM4 rgateMod != 0 is not supported";
   if (m.rbodyMod != 0) return "BSIM4 rbodyMod != 0 is not supported";
   if (m.trnqsMod != 0 || m.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
@@ -993,7 +994,14 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   R(vtl) = p.vtl; R(tfactor) = p.tfactor; R(xrcrg1) = p.xrcrg1; R(xrcrg2) = p.xrcrg2; R(vfbsd) = p.vfbsd;
   R(egidl) = p.egidl; R(agidl) = p.agidl; R(bgidl) = p.bgidl; R(cgidl) = p.cgidl; R(weffCJ) = p.weffCJ;
   R(egisl) = p.egisl; R(agisl) = p.agisl; R(bgisl) = p.bgisl; R(cgisl) = p.cgisl;
-  R(vfbcv) = p.vfbcv; R(abulkCVfactor) = p.abulkCVfactor; R(weffCV) = p.weffCV; R(leffCV) = p.leffCV; R(noff) = p.noff;
+  R(vfbcv) = p.vfbcv; R(Aechvb) = p.Aechvb; R(Bechvb) = p.Bechvb; R(AechvbEdgeS) = p.AechvbEdgeS;
+  R(AechvbEdgeD) = p.AechvbEdgeD; R(BechvbEdge) = p.BechvbEdge; R(ToxRatio) = p.ToxRatio; R(aigc) = p.aigc;
+  R(bigc) = p.bigc; R(cigc) = p.cigc; R(nigc) = p.nigc; R(pigcd) = p.pigcd; R(pigcdGiven) = m.g("PIGCD") ? 1 : 0;
+  R(vfbsdoff) = p.vfbsdoff; R(aigs) = p.aigs; R(bigs) = p.bigs; R(cigs) = p.cigs; R(aigd) = p.aigd; R(bigd) = p.bigd;
+  R(cigd) = p.cigd; R(nigbacc) = p.nigbacc; R(aigbacc) = p.aigbacc; R(bigbacc) = p.bigbacc; R(cigbacc) = p.cigbacc;
+  R(nigbinv) = p.nigbinv; R(eigbinv) = p.eigbinv; R(aigbinv) = p.aigbinv; R(bigbinv) = p.bigbinv;
+  R(cigbinv) = p.cigbinv;
+  R(abulkCVfactor) = p.abulkCVfactor; R(weffCV) = p.weffCV; R(leffCV) = p.leffCV; R(noff) = p.noff;
   R(voffcv) = p.voffcv; R(mstarcv) = p.mstarcv; R(voffcbncv) = p.voffcbncv; R(acde) = p.acde; R(ldeb) = p.ldeb;
   R(moin) = p.moin; R(cgbo) = p.cgbo; R(cgdo) = p.cgdo; R(cgso) = p.cgso; R(cgdl) = p.cgdl; R(cgsl) = p.cgsl;
   R(ckappad) = p.ckappad; R(ckappas) = p.ckappas;

@@ -50,6 +50,25 @@ EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 333
 EVAL_FP64_FLOPS_PER_INST = 2 * 2621 + 844 + 511
 
 
+def replica_totals(dist, n, ms, device):
+    """Whole-job figures of the replicas: the instances all ranks loaded (each rank's circuit is its
+    own seeded replica, so the counts differ slightly) and the slowest rank's time per step."""
+    if dist is None:
+        return n, ms
+    import torch
+
+    t_n = torch.tensor([float(n)], dtype=torch.float64, device=device)
+    t_ms = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t_n, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+    return int(round(float(t_n.item()))), float(t_ms.item())
+
+
+def replica_seed(seed, rank):
+    """The seed of rank `rank`'s replica circuit."""
+    return seed + rank
+
+
 def eval_shape(lib, h):
     """The evaluation kernel's launch shape that the autotuner picked for a context."""
     import ctypes
@@ -460,7 +479,7 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev_id = local
-    c, rowptr, colind = build_workload(args.mos, args.seed + rank, args.wire_segments)
+    c, rowptr, colind = build_workload(args.mos, replica_seed(args.seed, rank), args.wire_segments)
     cards, im, nd, params = family(c)
     n = im.shape[0]
     nu, nnz = c.n_unknowns, int(rowptr[-1])
@@ -510,12 +529,8 @@ def main():
     if dist is not None:
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev_id}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * n / (ms_max * 1e-3)
+    n_all, ms_max = replica_totals(dist, n, ms, f"cuda:{dev_id}")
+    value = n_all / (ms_max * 1e-3)
 
     # Per-kernel device time on the launching stream (eval kernel vs gathers).
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -592,11 +607,8 @@ def main():
     e1.record(s_copy)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev_id}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n / (e2e_ms * 1e-3)
+    _, e2e_ms = replica_totals(dist, n, e2e_ms, f"cuda:{dev_id}")
+    e2e_value = n_all / (e2e_ms * 1e-3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -124,7 +124,7 @@ def test_parity_gate_tunnelling(igc, igb, cards_extra):
     c = netlist.random_logic(1500, seed=41 + igc + 2 * igb)
     common = {"IGCMOD": igc, "IGBMOD": igb, "TOXE": cards_extra.get("TOXE", 1.8e-9)}
     common.update({k: v for k, v in cards_extra.items() if k not in ("TOXE", "NF")})
-    cards = [ModelCard(False, dict(common)), ModelCard(True, dict(common))]
+    cards = [ModelCard(False, dict(common, TNOIMOD=1)), ModelCard(True, dict(common))]
     extra = {"NF": np.full(c.n_mos, cards_extra["NF"])} if "NF" in cards_extra else None
     worst = _run_sequence(c, cards, TRANSIENT_SEQ[:4] + DC_SEQ[:2], extra_params=extra, vrange=(-0.6, 1.8),
                           seed=igc + igb)

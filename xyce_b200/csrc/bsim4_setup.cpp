@@ -246,7 +246,9 @@ std::string process_model(const ModelSpec &spec, const SetupOptions &opts, Card 
   if (m.capMod < 0 || m.capMod > 2) return "BSIM4 capMod must be 0, 1 or 2";
   if (m.dioMod < 0 || m.dioMod > 2) return "BSIM4 dioMod must be 0, 1 or 2";
   if (m.mobMod < 0 || m.mobMod > 2) return "BSIM4 mobMod must be 0, 1 or 2";
-  if (m.tnoiMod != 0) return "BSIM4 tnoiMod != 0 is not supported";
+  // tnoiMod selects the thermal-noise model: outside a noise analysis it adds no nodes
+  // (N_DEV_MOSFET_B4.C:3687) and feeds only the noise charge (:10674), so every value loads alike.
+  if (m.tnoiMod < 0 || m.tnoiMod > 1) return "BSIM4 tnoiMod must be 0 or 1";
   return std::string();
 }
 

@@ -168,9 +168,10 @@ int xd_launches_per_load(const xd_ctx *ctx);
 int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks);
 /* The autotuner's candidates: xd_num_eval_variants() of them; xd_eval_variant_info gives the
  * launch shape of candidate v; xd_get_eval_variant / xd_set_eval_variant read and override the
- * context's choice (every candidate computes identical results; tests force each in turn). Some
- * candidates are compiled with the BSIM4 gate tunnelling currents; a family whose cards set
- * igcMod or igbMod only runs those, and xd_set_eval_variant refuses the others for it. */
+ * context's choice (every candidate computes identical results; tests force each in turn). The
+ * common candidates are compiled for BSIM4 capMod 2 without gate tunnelling; a family whose cards
+ * use capMod 0/1 or igcMod/igbMod runs only the full ones, and xd_set_eval_variant refuses the
+ * others for it. */
 int xd_num_eval_variants(void);
 int xd_eval_variant_info(int v, int *block, int *min_blocks);
 int xd_get_eval_variant(const xd_ctx *ctx);

@@ -82,10 +82,11 @@ XD_HD void poly_depletion(double phi, double ngate, double epsgate, double coxe,
 // V[4] = node voltages (D, G, S, B); sto_old = the store values the limiter compares against
 // (currSto on Newton step 0 of a transient step, nextSto otherwise); vgb_orig = the previous load's
 // vgb of this instance (0 before the first load), which the reference uses as the "original" vgb.
-// IGC = false compiles the load without the gate tunnelling currents (igcMod = igbMod = 0 whatever
-// the record says): the default kernel keeps its register allocation; families whose cards
-// enable tunnelling run the IGC = true instantiation.
-template <bool IGC = false, class RV>
+// FULL = false compiles the load for the common card only — capMod 2, no gate tunnelling
+// (igcMod = igbMod = 0) — whatever the record says, so the default kernel carries none of the
+// other branches in its registers or its code; families whose cards use capMod 0/1 or the
+// tunnelling currents run the FULL = true instantiation.
+template <bool FULL = false, class RV>
 XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
                       LoadOut &o) {
   using namespace xdc;
@@ -94,7 +95,7 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   const int mobMod = (int)P(mobMod);
   const int dioMod = (int)P(dioMod);
   const int tempMod = (int)P(tempMod);
-  const int capMod = (int)P(capMod);
+  const int capMod = FULL ? (int)P(capMod) : 2;
   const double gmin = fl.gmin;
   const double nf = P(nf);
   const double vth0 = P(vth0);
@@ -1345,7 +1346,7 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   double ggisls = Ggisls, ggislg = Ggislg, ggislb = Ggislb;
   // Gate tunnelling currents (:10183-10600): gate to channel (igcMod, partitioned between source
   // and drain), gate to source / drain overlap (with igcMod) and gate to bulk (igbMod).
-  const int igcMod = IGC ? (int)P(igcMod) : 0, igbMod = IGC ? (int)P(igbMod) : 0;
+  const int igcMod = FULL ? (int)P(igcMod) : 0, igbMod = FULL ? (int)P(igbMod) : 0;
   double Igcs = 0.0, gIgcsg = 0.0, gIgcsd = 0.0, gIgcsb = 0.0;
   double Igcd = 0.0, gIgcdg = 0.0, gIgcdd = 0.0, gIgcdb = 0.0;
   double Igs = 0.0, gIgsg = 0.0, gIgss = 0.0, Igd = 0.0, gIgdg = 0.0, gIgdd = 0.0;

@@ -92,12 +92,12 @@ struct xd_ctx {
   double *d_stage = nullptr;
   GatherMap vmap, mmap;
   int eval_variant = 0;
-  bool gate_tunnel = false;  // some BSIM4 record has igcMod or igbMod set
+  bool needs_full = false;  // some BSIM4 record uses capMod 0/1 or the gate tunnelling currents
 };
 
 namespace {
 
-template <int BLOCK, int MINB, bool IGC>
+template <int BLOCK, int MINB, bool FULL>
 __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
   sto_old[xb4::s_von] = so[(size_t)xb4::s_von * n + i];
   xb4::RecPtr rp{tab + rec[i], nrec};
   xb4::LoadOut o;
-  xb4::bsim4_load<IGC>(rp, V, sto_old, fl, vgb[i], o);
+  xb4::bsim4_load<FULL>(rp, V, sto_old, fl, vgb[i], o);
 #pragma unroll
   for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
 #pragma unroll
@@ -441,14 +441,14 @@ __global__ void __launch_bounds__(128) bsim3_eval_kernel(
 
 struct EvalVariant {
   int block, min_blocks;
-  bool igc;  // compiled with the gate tunnelling currents
+  bool full;  // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
 };
 constexpr EvalVariant kEvalVariants[] = {{128, 1, false}, {128, 2, false}, {128, 3, false}, {128, 4, false},
                                          {64, 4, false},  {256, 2, false}, {128, 2, true},  {128, 3, true}};
-constexpr int kFirstIgcVariant = 6;
-// A variant computes a context's loads exactly if it has the tunnelling currents or the context's
-// cards do not use them.
-bool variant_fits(const xd_ctx *ctx, int v) { return kEvalVariants[v].igc || !ctx->gate_tunnel; }
+constexpr int kFirstFullVariant = 6;
+// A variant computes a context's loads exactly if it is a full one or the context's cards use
+// only the common options.
+bool variant_fits(const xd_ctx *ctx, int v) { return kEvalVariants[v].full || !ctx->needs_full; }
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
 
 void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const double *sol, double *next_sta,
@@ -484,7 +484,7 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
 // Times every launch shape on the circuit's own instances at a synthetic operating point (node
 // voltages spread over 0..1.2 V, transient flags) in scratch buffers, and returns the fastest.
 int autotune_eval(xd_ctx *ctx, int &best) {
-  best = ctx->gate_tunnel ? kFirstIgcVariant : 0;
+  best = ctx->needs_full ? kFirstFullVariant : 0;
   const int n = ctx->n;
   if (n < 4096 || ctx->family != kFamilyBsim4) return 0;
   double *sol = nullptr, *sta = nullptr, *sto = nullptr;
@@ -675,8 +675,9 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   if (family == kFamilyBsim4)
     for (int r = 0; r < rt.n_records; ++r)
       if (rt.tab[(size_t)xb4::f_igcMod * rt.n_records + r] != 0.0 ||
-          rt.tab[(size_t)xb4::f_igbMod * rt.n_records + r] != 0.0)
-        ctx->gate_tunnel = true;
+          rt.tab[(size_t)xb4::f_igbMod * rt.n_records + r] != 0.0 ||
+          rt.tab[(size_t)xb4::f_capMod * rt.n_records + r] != 2.0)
+        ctx->needs_full = true;
   auto cleanup = [&](int code) {
     xd_destroy(ctx);
     return code;
@@ -822,7 +823,8 @@ int xd_get_eval_variant(const xd_ctx *ctx) { return ctx ? ctx->eval_variant : -1
 int xd_set_eval_variant(xd_ctx *ctx, int v) {
   if (!ctx || v < 0 || v >= kNumEvalVariants) return fail(-1, "bad evaluation variant");
   if (!variant_fits(ctx, v))
-    return fail(-1, "this evaluation variant has no gate tunnelling currents, which the family's cards use");
+    return fail(-1, "this evaluation variant is compiled for capMod 2 without gate tunnelling, which the family's "
+                    "cards need");
   ctx->eval_variant = v;
   return 0;
 }

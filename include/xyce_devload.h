@@ -80,6 +80,9 @@ typedef struct xd_mosfet_family {
   const double *inst_param_values;       /* [n_inst * n_inst_params]; NaN = not given         */
   double temp_c;                         /* .OPTIONS DEVICE TEMP (Celsius)                    */
   double tnom_c;                         /* .OPTIONS DEVICE TNOM (Celsius)                    */
+  const int *inst_internal;              /* [2*n_inst] internal drain, source unknown (D', S')
+                                            or -1 where the node collapses onto D / S; null if
+                                            no instance has one (see xd_internal_nodes)        */
 } xd_mosfet_family;
 
 /* Jacobian sparsity pattern over the unknowns (host memory, read during xd_create only).
@@ -95,6 +98,13 @@ typedef struct xd_csr {
  * temperature, size binning), uploads per-instance constants, and precomputes the
  * stamp-to-output gather maps. Fails (< 0) on unsupported model features. */
 int xd_create(const xd_mosfet_family *family, const xd_csr *pattern, int cuda_device, xd_ctx **out);
+
+/* Topology query before xd_create, as the reference's instances report their internal variables
+ * (N_DEV_MOSFET_B4.C:3684-3760, registerLIDs :4996-5060): flags[2i] / flags[2i+1] = 1 when
+ * instance i has an internal drain / source node (BSIM4, rdsMod = 0: sheet resistance RSH with
+ * NRD / NRS > 0). The caller allocates those unknowns (the reference numbers them after the
+ * external ones, in instance order, drain first) and passes them in inst_internal. Host-only. */
+int xd_internal_nodes(const xd_mosfet_family *family, int *flags);
 
 /* Releases all device memory of the context. */
 int xd_destroy(xd_ctx *ctx);
@@ -155,7 +165,10 @@ int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double
 /* Copies the per-instance local stamps of the last xd_update_state to host memory:
  * [48 * n_inst] doubles, slot-major (slot k of instance i at [k * n_inst + i]); slots 0-15 are
  * the F, Q, dFdxdVp, dQdxdVp terminal entries (D, G, S, B each), 16-31 dF/dx and 32-47 dQ/dx
- * as 4x4 row-major terminal blocks. Synchronises the stream. */
+ * as 4x4 row-major terminal blocks. A family with internal drain / source nodes has the wide
+ * layout, [68 * n_inst]: each vector takes 6 rows (D', G, S', B, then the external D and S,
+ * F only), dF/dx and dQ/dx take 22 slots each (the 4x4 block on D', G, S', B, then (D', D),
+ * (D, D'), (D, D), (S', S), (S, S'), (S, S)). Synchronises the stream. */
 int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream);
 
 /* Diagnostics. xd_launches_per_load: kernels one xd_load enqueues (eval + gathers).

@@ -77,7 +77,8 @@ def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, c
                  eval_variant=None):
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, inst_model, inst_nodes, params = family_inputs(c, cards, extra_params)
-    dev = MosfetDevice(cards, inst_model, inst_nodes, params, (rowptr, colind), c.n_unknowns, level=level)
+    dev = MosfetDevice(cards, inst_model, inst_nodes, params, (rowptr, colind), c.n_unknowns, level=level,
+                       inst_internal=c.mos_internal)
     if eval_variant is not None:
         assert dev._lib.xd_set_eval_variant(dev._h, eval_variant) == 0
     orc = OracleRun(c, cards, inst_model, inst_nodes, params, rowptr, colind, level=level,

@@ -75,8 +75,9 @@ class OracleRun:
         self.c = c
         models = [(m.pmos, dict(m.params)) for m in cards]
         nu = c.n_unknowns
-        self.ref = xr.RefCircuit(level, models, inst_model, inst_nodes, params, nu)
-        assert self.ref.n_unknowns == nu, "oracle created internal nodes the product does not model"
+        # The reference numbers its internal nodes after the external unknowns, in instance order.
+        self.ref = xr.RefCircuit(level, models, inst_model, inst_nodes, params, nu - c.n_internal)
+        assert self.ref.n_unknowns == nu, "the oracle's internal nodes differ from the circuit's"
         n = inst_model.shape[0]
         # Oracle pattern: the product's pattern plus the ground row / column entries the stamps hit.
         g = nu
@@ -85,6 +86,11 @@ class OracleRun:
         rr = np.repeat(nd, 4, axis=1).reshape(-1)
         cc = np.tile(nd, (1, 4)).reshape(-1)
         pairs.append(np.stack([rr, cc], 1))
+        if c.n_internal:
+            # With internal nodes the reference's stamps reach beyond the terminal block: add them.
+            for i in range(n):
+                sr, sc = self.ref.stamp(i)
+                pairs.append(np.stack([np.asarray(sr, np.int64), np.asarray(sc, np.int64)], 1))
         pr = np.concatenate(pairs, 0)
         key = np.unique(pr[:, 0] * (nu + 1) + pr[:, 1])
         rows, cols = key // (nu + 1), (key % (nu + 1)).astype(np.int32)

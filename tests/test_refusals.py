@@ -26,7 +26,9 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
     (14, [ModelCard(False, {"CAPMOD": 3}), ModelCard(True, {})], None, "capMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {"IGCMOD": 3}), ModelCard(True, {})], None, "igcMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {}), ModelCard(True, {"IGBMOD": 2})], None, "igbMod must be 0 or 1"),
-    (14, NMOS_PMOS, {"NRD": 2.0}, "NRD/NRS"),
+    (14, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], {"RGEOMOD": 1}, "rgeoMod"),
+    (14, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {"RSH": 5.0})], {"NRD": 2.0, "NRS": 1.5},
+     "inst_internal"),
     (14, [ModelCard(False, {"NOSUCH": 1.0}), ModelCard(True, {})], None, "unknown BSIM4 model parameter"),
     (9, [ModelCard(False, {"CAPMOD": 4}), ModelCard(True, {})], None, "capMod"),
     (9, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], None, "series resistance"),
@@ -50,3 +52,25 @@ def test_mixed_instance_temperatures_are_refused():
         # Instances alternate PMOS / NMOS, so each model's instances see both temperatures.
         with pytest.raises(NativeError, match="share one temperature"):
             MosfetDevice(NMOS_PMOS, c.mos_type, c.mos_nodes, params, (rowptr, colind), c.n_unknowns, level=level)
+
+
+def test_internal_node_query_follows_sheet_resistance():
+    """RSH with NRD / NRS > 0 gives an instance internal drain / source nodes; without RSH, or
+    with zero squares, the node collapses (the reference's createNode rule)."""
+    from xyce_b200.device import internal_nodes
+
+    c = netlist.inverter_ring(5)
+    n = c.n_mos
+    cards = [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})]
+    nrd = np.where(np.arange(n) % 3 == 0, 2.0, np.where(np.arange(n) % 3 == 1, 0.0, np.nan))
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float), "NRD": nrd, "NRS": np.full(n, 1.0)}
+    flags = internal_nodes(cards, c.mos_type, c.mos_nodes, params)
+    nmos = c.mos_type == 0
+    assert (flags[:, 0] == (nmos & (np.arange(n) % 3 == 0))).all()
+    assert (flags[:, 1] == nmos).all()
+    c2 = netlist.with_internal_nodes(c, flags)
+    assert c2.n_unknowns == c.n_unknowns + int(flags.sum())
+    got = c2.mos_internal[flags]
+    assert (np.sort(got) == np.arange(c.n_unknowns, c2.n_unknowns)).all()
+    rowptr, colind = netlist.jacobian_pattern(c2)
+    assert rowptr.shape[0] == c2.n_unknowns + 1

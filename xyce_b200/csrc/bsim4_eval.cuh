@@ -36,11 +36,18 @@ struct LoadFlags {
 enum StoreSlot { s_vbd, s_vbs, s_vgs, s_vds, s_vges, s_vgms, s_vdes, s_vses, s_vdbs, s_vsbs, s_vdbd, s_vged, s_vgmd, s_von, kNumStore };
 enum StateSlot { t_qb, t_qg, t_qd, kNumState };
 enum { kNumVec = 16, kNumMat = 16, kNumStage = kNumVec + 2 * kNumMat };
+// Series-resistance layout (internal drain / source nodes): the four vectors get rows 4 and 5 for
+// the external drain and source, the matrices six more slots for the resistor couplings.
+enum { kSerVecRows = 6, kSerMat = kNumMat + 6, kSerStage = 4 * kSerVecRows + 2 * kSerMat };
 
 struct LoadOut {
   double vec[kNumVec];
   double jf[kNumMat];
   double jq[kNumMat];
+  // With internal nodes: F at the external drain and source, and dF/dx at (D', D), (D, D'),
+  // (D, D), (S', S), (S, S'), (S, S); rows 0 and 2 of vec/jf/jq are then D' and S'.
+  double vecx[2];
+  double jfx[6];
   double sto[kNumStore];  // s_vged and s_vgmd are not written by the load (kept from the input)
   double sta[kNumState];
   bool write_curr_sta;    // first Newton step of the first transient step: also write currSta
@@ -86,9 +93,11 @@ XD_HD void poly_depletion(double phi, double ngate, double epsgate, double coxe,
 // (igcMod = igbMod = 0) — whatever the record says, so the default kernel carries none of the
 // other branches in its registers or its code; families whose cards use capMod 0/1 or the
 // tunnelling currents run the FULL = true instantiation.
-template <bool FULL = false, class RV>
+// SERIES = true: V holds (D', G, S', B) and Vx the external (D, S); the linear drain and source
+// resistances (rdsMod = 0, sheet resistance) load into vecx / jfx.
+template <bool FULL = false, bool SERIES = false, class RV>
 XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
-                      LoadOut &o) {
+                      LoadOut &o, const double *Vx = nullptr) {
   using namespace xdc;
 #define P(x) P_(f_##x)
   const double dtype = P(dtype);
@@ -105,10 +114,13 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
 
   // Node and branch voltages (:7932-8030), collapsed topology.
-  const double Vd = V[0], Vge = V[1], Vs = V[2], Vb = V[3];
-  const double Vdp = Vd, Vsp = Vs, Vgp = Vge, Vbp = Vb, Vgm = Vge, Vdb = Vb, Vsb = Vb;
-  (void)Vdp; (void)Vgp; (void)Vbp; (void)Vgm; (void)Vdb; (void)Vsb;
-  double vds = dtype * (Vd - Vsp);
+  const double Vdp = V[0], Vge = V[1], Vsp = V[2], Vb = V[3];
+  const double Vd = SERIES ? Vx[0] : Vdp, Vs = SERIES ? Vx[1] : Vsp;
+  const double Vgp = Vge, Vbp = Vb, Vgm = Vge, Vdb = Vb, Vsb = Vb;
+  (void)Vgp; (void)Vbp; (void)Vgm; (void)Vdb; (void)Vsb;
+  const double Vddp = Vd - Vdp, Vssp = Vs - Vsp;
+  (void)Vddp; (void)Vssp;
+  double vds = dtype * (Vdp - Vsp);
   double vgs = dtype * (Vge - Vsp);
   double vbs = dtype * (Vb - Vsp);
   double vges = dtype * (Vge - Vsp);
@@ -2492,6 +2504,21 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   o.vec[1] -= -(-ceqgcrg + Igtoteq) * M;
   o.vec[3] += -(ceqbd + ceqbs - ceqjd - ceqjs + Ibtoteq) * M;
   o.vec[2] += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
+  if (SERIES) {
+    // Linear terminal resistor currents (:11901-11904, 16360-16370), where the node exists.
+    o.vecx[0] = 0.0;
+    o.vecx[1] = 0.0;
+    if (P(dExists) != 0.0) {
+      const double Idrain = P(drainConductance) * Vddp;
+      o.vecx[0] += -(-Idrain) * M;
+      o.vec[0] += -(Idrain)*M;
+    }
+    if (P(sExists) != 0.0) {
+      const double Isource = P(sourceConductance) * Vssp;
+      o.vecx[1] += -(-Isource) * M;
+      o.vec[2] += -(+Isource) * M;
+    }
+  }
   if (lim) {
     o.vec[8 + 0] += (ceqjd_Jdxp - ceqbd_Jdxp - ceqdrn_Jdxp + Idtoteq_Jdxp) * M;
     o.vec[8 + 1] -= (-ceqgcrg_Jdxp + Igtoteq_Jdxp) * M;
@@ -2546,19 +2573,26 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   JF(1, 2) += (-ggts + gIgtots) * M;
   JF(1, 3) += (-ggtb + gIgtotb) * M;
   JF(0, 0) += (gdpr + gds + gbd + Tq * ddxpart_dVd - gdtotd + RevSum + gbdpdp + dxpart * ggtd - gIdtotd) * M;
-  JF(0, 0) -= (gdpr + gdtot) * M;
+  if (SERIES) {
+    for (int k = 0; k < 6; ++k) o.jfx[k] = 0.0;
+  }
+  // The resistor couplings (D', D), (D, D'), (D, D) and the source's: their own slots with internal
+  // nodes, the collapsed (D, D) / (S, S) entry otherwise.
+#define JRES(k, r) (*(SERIES ? &o.jfx[k] : &JF(r, r)))
+  JRES(0, 0) -= (gdpr + gdtot) * M;
   JF(0, 1) += (Gmv - gdtotg + gbdpg - gIdtotg + dxpart * ggtg + Tq * ddxpart_dVg) * M;
   JF(0, 2) -= (gds + gdtots - dxpart * ggts + gIdtots - Tq * ddxpart_dVs + FwdSum - gbdpsp) * M;
   JF(0, 3) -= (gjbd + gdtotb - Gmbsv - gbdpb + gIdtotb - Tq * ddxpart_dVb - dxpart * ggtb) * M;
-  JF(0, 0) -= (gdpr - gdtotd) * M;
-  JF(0, 0) += (gdpr + gdtot) * M;
+  JRES(1, 0) -= (gdpr - gdtotd) * M;
+  JRES(2, 0) += (gdpr + gdtot) * M;
   JF(2, 0) -= (gds + gstotd + RevSum - gbspdp - Tq * dsxpart_dVd - sxpart * ggtd + gIstotd) * M;
   JF(2, 1) += (-Gmv - gstotg + gbspg + sxpart * ggtg + Tq * dsxpart_dVg - gIstotg) * M;
   JF(2, 2) += (gspr + gds + gbs + Tq * dsxpart_dVs - gstots + FwdSum + gbspsp + sxpart * ggts - gIstots) * M;
-  JF(2, 2) -= (gspr + gstot) * M;
+  JRES(3, 2) -= (gspr + gstot) * M;
   JF(2, 3) -= (gjbs + gstotb + Gmbsv - gbspb - sxpart * ggtb - Tq * dsxpart_dVb + gIstotb) * M;
-  JF(2, 2) -= (gspr - gstots) * M;
-  JF(2, 2) += (gspr + gstot) * M;
+  JRES(4, 2) -= (gspr - gstots) * M;
+  JRES(5, 2) += (gspr + gstot) * M;
+#undef JRES
   JF(3, 0) += (-gjbd + gbbdp - gIbtotd) * M;
   JF(3, 1) += (-gbgs - gIbtotg) * M;
   JF(3, 2) += (-gjbs + gbbsp - gIbtots) * M;

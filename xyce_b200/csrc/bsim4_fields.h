@@ -45,7 +45,7 @@
   F(vjdmFwd) F(vjdmRev) F(IVjsmFwd) F(IVjsmRev) F(IVjdmFwd) F(IVjdmRev) F(SslpFwd) F(SslpRev)     \
   F(DslpFwd) F(DslpRev) F(SjctTempRevSatCur) F(SswTempRevSatCur) F(SswgTempRevSatCur)            \
   F(DjctTempRevSatCur) F(DswTempRevSatCur) F(DswgTempRevSatCur) F(drainConductance)              \
-  F(sourceConductance) F(grgeltd) F(temp) F(off)
+  F(sourceConductance) F(grgeltd) F(temp) F(off) F(dExists) F(sExists)
 
 namespace xb4 {
 enum Field {

@@ -708,8 +708,8 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   if (!ip.g("ACNQSMOD")) ip.acnqsMod = m.acnqsMod;
   if (ip.rbodyMod != 0 || ip.rgateMod != 0 || ip.trnqsMod != 0 || ip.acnqsMod != 0)
     return "BSIM4 instance rbodyMod/rgateMod/trnqsMod/acnqsMod != 0 is not supported";
-  if (ip.g("NRD") || ip.g("NRS"))
-    return "BSIM4 NRD/NRS (source/drain sheet-resistance nodes) are not supported";
+  if (ip.rgeoMod != 0 && m.sheetResistance > 0.0)
+    return "BSIM4 rgeoMod != 0 with RSH > 0 (geometry-derived source/drain resistance) is not supported";
   if (ip.g("IC1") || ip.g("IC2") || ip.g("IC3")) return "BSIM4 instance initial conditions are not supported";
   const double temp = ip.temp;
   if (!ms.temp_done) {
@@ -840,8 +840,20 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
     Adeff = ip.drainArea;
   else
     pa_eff_geo(nf, geoMod, minSD, p.weffCJ, DMCGeff, DMCIeff, DMDGeff, dumPs, dumPd, dumAs, Adeff);
-  const double sourceConductance = 0.0;  // rdsMod == 0 and NRS not given
-  const double drainConductance = 0.0;
+  // Source / drain series resistance, rdsMod = 0 (:7378-7447): sheet resistance times the given
+  // number of squares; a zero product is replaced by 1e3 S. The internal node exists when the
+  // sheet resistance and the squares are both positive (:3684-3745).
+  double sourceConductance = 0.0, drainConductance = 0.0;
+  if (ip.g("NRS")) {
+    sourceConductance = m.sheetResistance * ip.sourceSquares;
+    sourceConductance = (sourceConductance > 0.0) ? 1.0 / sourceConductance : 1.0e3;
+  }
+  if (ip.g("NRD")) {
+    drainConductance = m.sheetResistance * ip.drainSquares;
+    drainConductance = (drainConductance > 0.0) ? 1.0 / drainConductance : 1.0e3;
+  }
+  const bool dExists = m.sheetResistance > 0.0 && ip.g("NRD") && ip.drainSquares > 0.0;
+  const bool sExists = m.sheetResistance > 0.0 && ip.g("NRS") && ip.sourceSquares > 0.0;
   double XExpBVS = 0, XExpBVD = 0, vjsmFwd = 0, vjsmRev = 0, vjdmFwd = 0, vjdmRev = 0;
   double IVjsmFwd = 0, IVjsmRev = 0, IVjdmFwd = 0, IVjdmRev = 0, SslpFwd = 0, SslpRev = 0, DslpFwd = 0, DslpRev = 0;
   const double Nvtms = ms.vtm * m.SjctEmissionCoeff;
@@ -1017,6 +1029,7 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   R(SswgTempRevSatCur) = SswgTempRevSatCur; R(DjctTempRevSatCur) = DjctTempRevSatCur;
   R(DswTempRevSatCur) = DswTempRevSatCur; R(DswgTempRevSatCur) = DswgTempRevSatCur;
   R(drainConductance) = drainConductance; R(sourceConductance) = sourceConductance; R(grgeltd) = grgeltd;
+  R(dExists) = dExists ? 1.0 : 0.0; R(sExists) = sExists ? 1.0 : 0.0;
   R(temp) = temp; R(off) = ip.off;
 #undef R
   return std::string();

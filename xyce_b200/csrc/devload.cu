@@ -93,16 +93,24 @@ struct xd_ctx {
   GatherMap vmap, mmap;
   int eval_variant = 0;
   bool needs_full = false;  // some BSIM4 record uses capMod 0/1 or the gate tunnelling currents
+  // Internal drain / source nodes (series resistance): d_ext holds each instance's external drain
+  // and source, d_nodes its intrinsic (D', G, S', B); the staging layout widens to 6 vector rows
+  // and 22 matrix slots.
+  bool series = false;
+  int2 *d_ext = nullptr;
+  int vec_rows = 4, mat_slots = xb4::kNumMat, stage_slots = xb4::kNumStage;
 };
 
 namespace {
 
-template <int BLOCK, int MINB, bool FULL>
+// SERIES: the family has internal drain / source nodes; ext holds the external drain and source
+// of each instance and the staging layout is the wide one (6 vector rows, 22 matrix slots).
+template <int BLOCK, int MINB, bool FULL, bool SERIES>
 __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
-    double *__restrict__ stage, xb4::LoadFlags fl) {
+    double *__restrict__ stage, xb4::LoadFlags fl, const int2 *__restrict__ ext) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 nd = nodes[i];
@@ -122,13 +130,35 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
   sto_old[xb4::s_von] = so[(size_t)xb4::s_von * n + i];
   xb4::RecPtr rp{tab + rec[i], nrec};
   xb4::LoadOut o;
-  xb4::bsim4_load<FULL>(rp, V, sto_old, fl, vgb[i], o);
+  if (SERIES) {
+    const int2 ex = ext[i];
+    double Vx[2];
+    Vx[0] = ex.x >= 0 ? sol[ex.x] : 0.0;
+    Vx[1] = ex.y >= 0 ? sol[ex.y] : 0.0;
+    xb4::bsim4_load<FULL, true>(rp, V, sto_old, fl, vgb[i], o, Vx);
+    // Wide layout: vector v, row r at (v * 6 + r); rows 4 and 5 (external D, S) carry F only.
 #pragma unroll
-  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+      for (int r = 0; r < 4; ++r) stage[(size_t)(v * xb4::kSerVecRows + r) * n + i] = o.vec[v * 4 + r];
+    stage[(size_t)4 * n + i] = o.vecx[0];
+    stage[(size_t)5 * n + i] = o.vecx[1];
+    const size_t mf = 4 * xb4::kSerVecRows, mq = mf + xb4::kSerMat;
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mf + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) stage[(mf + xb4::kNumMat + k) * n + i] = o.jfx[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mq + k) * n + i] = o.jq[k];
+  } else {
+    xb4::bsim4_load<FULL, false>(rp, V, sto_old, fl, vgb[i], o);
+#pragma unroll
+    for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+  }
 #pragma unroll
   for (int k = 0; k < xb4::kNumStore; ++k)
     if (k != xb4::s_vged && k != xb4::s_vgmd) next_sto[(size_t)k * n + i] = o.sto[k];
@@ -441,14 +471,19 @@ __global__ void __launch_bounds__(128) bsim3_eval_kernel(
 
 struct EvalVariant {
   int block, min_blocks;
-  bool full;  // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
+  bool full;    // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
+  bool series;  // internal drain / source nodes, wide staging layout
 };
-constexpr EvalVariant kEvalVariants[] = {{128, 1, false}, {128, 2, false}, {128, 3, false}, {128, 4, false},
-                                         {64, 4, false},  {256, 2, false}, {128, 2, true},  {128, 3, true}};
-constexpr int kFirstFullVariant = 6;
-// A variant computes a context's loads exactly if it is a full one or the context's cards use
-// only the common options.
-bool variant_fits(const xd_ctx *ctx, int v) { return kEvalVariants[v].full || !ctx->needs_full; }
+constexpr EvalVariant kEvalVariants[] = {
+    {128, 1, false, false}, {128, 2, false, false}, {128, 3, false, false}, {128, 4, false, false},
+    {64, 4, false, false},  {256, 2, false, false}, {128, 2, true, false},  {128, 3, true, false},
+    {128, 2, true, true},   {128, 3, true, true}};
+constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8;
+// A variant computes a context's loads exactly if its staging layout is the context's and it is a
+// full one or the context's cards use only the common options.
+bool variant_fits(const xd_ctx *ctx, int v) {
+  return kEvalVariants[v].series == ctx->series && (kEvalVariants[v].full || !ctx->needs_full);
+}
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
 
 void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const double *sol, double *next_sta,
@@ -467,16 +502,18 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
   const int blk = kEvalVariants[v].block;
   const int grid = (n + blk - 1) / blk;
 #define XD_EVAL_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
-                     ctx->d_vgb, stage, fl
+                     ctx->d_vgb, stage, fl, ctx->d_ext
   switch (v) {
-    case 0: bsim4_eval_kernel<128, 1, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 1: bsim4_eval_kernel<128, 2, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 2: bsim4_eval_kernel<128, 3, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 3: bsim4_eval_kernel<128, 4, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 4: bsim4_eval_kernel<64, 4, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 5: bsim4_eval_kernel<256, 2, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    case 6: bsim4_eval_kernel<128, 2, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    default: bsim4_eval_kernel<128, 3, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 0: bsim4_eval_kernel<128, 1, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 1: bsim4_eval_kernel<128, 2, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 2: bsim4_eval_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 3: bsim4_eval_kernel<128, 4, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 4: bsim4_eval_kernel<64, 4, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 5: bsim4_eval_kernel<256, 2, false, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 6: bsim4_eval_kernel<128, 2, true, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 7: bsim4_eval_kernel<128, 3, true, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 8: bsim4_eval_kernel<128, 2, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    default: bsim4_eval_kernel<128, 3, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
   }
 #undef XD_EVAL_ARGS
 }
@@ -484,7 +521,7 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
 // Times every launch shape on the circuit's own instances at a synthetic operating point (node
 // voltages spread over 0..1.2 V, transient flags) in scratch buffers, and returns the fastest.
 int autotune_eval(xd_ctx *ctx, int &best) {
-  best = ctx->needs_full ? kFirstFullVariant : 0;
+  best = ctx->series ? kFirstSeriesVariant : (ctx->needs_full ? kFirstFullVariant : 0);
   const int n = ctx->n;
   if (n < 4096 || ctx->family != kFamilyBsim4) return 0;
   double *sol = nullptr, *sta = nullptr, *sto = nullptr;
@@ -561,6 +598,36 @@ extern "C" {
 
 const char *xd_last_error(void) { return g_err.c_str(); }
 
+int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
+  g_err.clear();
+  if (!fam || !flags) return fail(-1, "null argument");
+  if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
+  const int n = fam->n_inst;
+  for (int k = 0; k < 2 * n; ++k) flags[k] = 0;
+  if (!(fam->level == 14 || fam->level == 54)) return 0;  // only BSIM4 series resistance is modelled
+  std::vector<xb4::ModelSpec> models(fam->n_models);
+  size_t off = 0;
+  for (int m = 0; m < fam->n_models; ++m) {
+    models[m].pmos = fam->model_is_pmos[m] != 0;
+    for (int k = 0; k < fam->model_nparams[m]; ++k, ++off)
+      models[m].params.push_back({fam->model_param_names[off], fam->model_param_values[off]});
+  }
+  std::vector<std::string> ipn;
+  for (int k = 0; k < fam->n_inst_params; ++k) ipn.push_back(fam->inst_param_names[k]);
+  xb4::SetupOptions opts;
+  opts.temp_c = fam->temp_c;
+  opts.tnom_c = fam->tnom_c;
+  xb4::RecordTable rt;
+  const std::string e = xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  if (!e.empty()) return fail(-2, e);
+  for (int i = 0; i < n; ++i) {
+    const int r = rt.inst_rec[i];
+    flags[2 * i] = rt.tab[(size_t)xb4::f_dExists * rt.n_records + r] != 0.0;
+    flags[2 * i + 1] = rt.tab[(size_t)xb4::f_sExists * rt.n_records + r] != 0.0;
+  }
+  return 0;
+}
+
 int xd_num_instances(const xd_ctx *ctx) { return ctx ? ctx->n : -1; }
 int xd_num_state_slots(const xd_ctx *ctx) {
   if (!ctx) return -1;
@@ -583,6 +650,7 @@ int xd_destroy(xd_ctx *ctx) {
   cudaFree(ctx->d_nodes);
   cudaFree(ctx->d_vgb);
   cudaFree(ctx->d_stage);
+  cudaFree(ctx->d_ext);
   free_map(ctx->vmap);
   free_map(ctx->mmap);
   delete ctx;
@@ -604,7 +672,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     return fail(-2, "MOSFET level " + std::to_string(fam->level) +
                         " is not implemented (levels 1, 9, 49, 14, 54 are)");
   if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
-  if ((long long)fam->n_inst * xb4::kNumStage >= (1LL << 31)) return fail(-1, "too many instances");
+  if ((long long)fam->n_inst * xb4::kSerStage >= (1LL << 31)) return fail(-1, "too many instances");
   if (pat->n_rows < 0 || !pat->rowptr || (pat->rowptr[pat->n_rows] > 0 && !pat->colind))
     return fail(-1, "bad CSR pattern");
   const int n = fam->n_inst;
@@ -628,8 +696,23 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       : family == kFamilyBsim3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
                                : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
-  // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent).
+  // Internal drain / source nodes (BSIM4 sheet resistance): which instances have them.
+  std::vector<unsigned char> dint(n, 0), sint(n, 0);
+  bool series = false;
+  if (family == kFamilyBsim4)
+    for (int i = 0; i < n; ++i) {
+      const int r = rt.inst_rec[i];
+      dint[i] = rt.tab[(size_t)xb4::f_dExists * rt.n_records + r] != 0.0;
+      sint[i] = rt.tab[(size_t)xb4::f_sExists * rt.n_records + r] != 0.0;
+      series = series || dint[i] || sint[i];
+    }
+  if (series && !fam->inst_internal)
+    return fail(-1, "instances have internal drain/source nodes (RSH with NRD/NRS): pass their unknowns in "
+                    "inst_internal (xd_internal_nodes lists which instances have them)");
+  // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent). With internal nodes
+  // the intrinsic device sits on (D', G, S', B) and ext keeps the external drain and source.
   std::vector<int4> nodes(n);
+  std::vector<int2> ext(series ? n : 0);
   for (int i = 0; i < n; ++i) {
     int v[4];
     for (int k = 0; k < 4; ++k) {
@@ -637,31 +720,71 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       if (v[k] >= nu) return fail(-1, "instance node index beyond the pattern's unknowns");
       if (v[k] < 0) v[k] = -1;
     }
+    if (fam->inst_internal) {
+      for (int k = 0; k < 2; ++k) {
+        const int u = fam->inst_internal[2 * (size_t)i + k];
+        const bool has = k == 0 ? dint[i] : sint[i];
+        if (has && (u < 0 || u >= nu))
+          return fail(-1, "instance " + std::to_string(i) + " needs an internal " + (k == 0 ? "drain" : "source") +
+                              " node inside the pattern's unknowns");
+        if (!has && u >= 0)
+          return fail(-1, "instance " + std::to_string(i) + " has no internal " + (k == 0 ? "drain" : "source") +
+                              " node (RSH and NRD/NRS not both positive)");
+      }
+    }
+    if (series) {
+      ext[i] = make_int2(v[0], v[2]);
+      if (dint[i]) v[0] = fam->inst_internal[2 * (size_t)i];
+      if (sint[i]) v[2] = fam->inst_internal[2 * (size_t)i + 1];
+    }
     nodes[i] = make_int4(v[0], v[1], v[2], v[3]);
   }
+  auto csr_pos = [&](int r, int c, int &p) -> bool {
+    p = -1;
+    if (r < 0 || c < 0) return true;
+    const int *b = pat->colind + pat->rowptr[r], *en = pat->colind + pat->rowptr[r + 1];
+    const int *q = std::lower_bound(b, en, c);
+    if (q == en || *q != c) return false;
+    p = (int)(q - pat->colind);
+    return true;
+  };
+  const int vrows = series ? xb4::kSerVecRows : 4;
   std::vector<int> vt, vs, mt, ms;
-  vt.reserve((size_t)4 * n);
-  vs.reserve((size_t)4 * n);
-  mt.reserve((size_t)16 * n);
-  ms.reserve((size_t)16 * n);
+  vt.reserve((size_t)vrows * n);
+  vs.reserve((size_t)vrows * n);
+  mt.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
+  ms.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
   for (int i = 0; i < n; ++i) {
     const int nd[4] = {nodes[i].x, nodes[i].y, nodes[i].z, nodes[i].w};
     for (int r = 0; r < 4; ++r) {
       vt.push_back(nd[r]);
       vs.push_back(r * n + i);
     }
+    if (series) {
+      vt.push_back(ext[i].x);
+      vs.push_back(4 * n + i);
+      vt.push_back(ext[i].y);
+      vs.push_back(5 * n + i);
+    }
     for (int r = 0; r < 4; ++r)
       for (int c = 0; c < 4; ++c) {
-        int p = -1;
-        if (nd[r] >= 0 && nd[c] >= 0) {
-          const int *b = pat->colind + pat->rowptr[nd[r]], *en = pat->colind + pat->rowptr[nd[r] + 1];
-          const int *q = std::lower_bound(b, en, nd[c]);
-          if (q == en || *q != nd[c]) return fail(-1, "CSR pattern lacks an entry the instance stamps");
-          p = (int)(q - pat->colind);
-        }
+        int p;
+        if (!csr_pos(nd[r], nd[c], p)) return fail(-1, "CSR pattern lacks an entry the instance stamps");
         mt.push_back(p);
         ms.push_back((r * 4 + c) * n + i);
       }
+    if (series) {
+      // (D', D), (D, D'), (D, D), (S', S), (S, S'), (S, S): the order of LoadOut::jfx.
+      const int rc[6][2] = {{nd[0], ext[i].x}, {ext[i].x, nd[0]}, {ext[i].x, ext[i].x},
+                            {nd[2], ext[i].y}, {ext[i].y, nd[2]}, {ext[i].y, ext[i].y}};
+      for (int k = 0; k < 6; ++k) {
+        int p;
+        if (!csr_pos(rc[k][0], rc[k][1], p))
+          return fail(-1, "CSR pattern lacks a series-resistance entry the instance stamps");
+        mt.push_back(p);
+        ms.push_back((xb4::kNumMat + k) * n + i);
+      }
+    }
   }
   int rc = cudaSetDevice(cuda_device);
   if (rc != cudaSuccess) return cuda_fail((cudaError_t)rc, "cudaSetDevice");
@@ -672,6 +795,12 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   ctx->n_unknowns = nu;
   ctx->nnz = pat->rowptr[nu];
   ctx->n_rec = rt.n_records;
+  ctx->series = series;
+  if (series) {
+    ctx->vec_rows = xb4::kSerVecRows;
+    ctx->mat_slots = xb4::kSerMat;
+    ctx->stage_slots = xb4::kSerStage;
+  }
   if (family == kFamilyBsim4)
     for (int r = 0; r < rt.n_records; ++r)
       if (rt.tab[(size_t)xb4::f_igcMod * rt.n_records + r] != 0.0 ||
@@ -692,10 +821,13 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       (ce = cudaMemcpy(ctx->d_nodes, nodes.data(), n * sizeof(int4), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (ce = cudaMalloc(&ctx->d_vgb, std::max(1, n) * sizeof(double))) != cudaSuccess ||
       (ce = cudaMemset(ctx->d_vgb, 0, std::max(1, n) * sizeof(double))) != cudaSuccess ||
-      (ce = cudaMalloc(&ctx->d_stage, std::max<size_t>(1, (size_t)xb4::kNumStage * n) * sizeof(double))) !=
+      (ce = cudaMalloc(&ctx->d_stage, std::max<size_t>(1, (size_t)ctx->stage_slots * n) * sizeof(double))) !=
           cudaSuccess ||
-      (ce = cudaMemset(ctx->d_stage, 0, std::max<size_t>(1, (size_t)xb4::kNumStage * n) * sizeof(double))) !=
+      (ce = cudaMemset(ctx->d_stage, 0, std::max<size_t>(1, (size_t)ctx->stage_slots * n) * sizeof(double))) !=
           cudaSuccess)
+    return cleanup(cuda_fail(ce, "xd_create allocation"));
+  if (series && ((ce = cudaMalloc(&ctx->d_ext, std::max(1, n) * sizeof(int2))) != cudaSuccess ||
+                 (ce = cudaMemcpy(ctx->d_ext, ext.data(), n * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess))
     return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
   if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
@@ -721,22 +853,22 @@ int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, dou
 
 static int load_vectors_impl(xd_ctx *ctx, double *f, double *q, double *fx, double *qx, bool abs_mode, cudaStream_t st,
                              int assign = 0) {
-  const size_t n = (size_t)ctx->n;
+  const size_t n = (size_t)ctx->n, r = (size_t)ctx->vec_rows;
   if (abs_mode) {
-    OutSet<4, true> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}};
+    OutSet<4, true> os{{f, q, fx, qx}, {0, r * n, 2 * r * n, 3 * r * n}};
     return run_gather(ctx->vmap, ctx->d_stage, os, st);
   }
-  OutSet<4, false> os{{f, q, fx, qx}, {0, 4 * n, 8 * n, 12 * n}, assign};
+  OutSet<4, false> os{{f, q, fx, qx}, {0, r * n, 2 * r * n, 3 * r * n}, assign};
   return run_gather(ctx->vmap, ctx->d_stage, os, st);
 }
 
 static int load_matrices_impl(xd_ctx *ctx, double *jf, double *jq, bool abs_mode, cudaStream_t st, int assign = 0) {
-  const size_t n = (size_t)ctx->n;
+  const size_t n = (size_t)ctx->n, b = 4 * (size_t)ctx->vec_rows * n, m = (size_t)ctx->mat_slots * n;
   if (abs_mode) {
-    OutSet<2, true> os{{jf, jq}, {16 * n, 32 * n}};
+    OutSet<2, true> os{{jf, jq}, {b, b + m}};
     return run_gather(ctx->mmap, ctx->d_stage, os, st);
   }
-  OutSet<2, false> os{{jf, jq}, {16 * n, 32 * n}, assign};
+  OutSet<2, false> os{{jf, jq}, {b, b + m}, assign};
   return run_gather(ctx->mmap, ctx->d_stage, os, st);
 }
 
@@ -779,6 +911,7 @@ int xd_load_vectors_staged(xd_ctx *ctx, const double *d_stage16, double *d_f, do
   if (!ctx) return fail(-1, "null context");
   if (ctx->n == 0) return 0;
   if (!d_stage16) return fail(-1, "null staged array");
+  if (ctx->series) return fail(-1, "staged vectors take the 4-terminal layout; this family has internal nodes");
   DeviceGuard g(ctx->device);
   const size_t n = (size_t)ctx->n;
   OutSet<4, false> os{{d_f, d_q, d_dfdxdvp, d_dqdxdvp}, {0, 4 * n, 8 * n, 12 * n}, assign ? 1 : 0};
@@ -841,7 +974,7 @@ int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream) {
   if (!ctx || !h_out) return fail(-1, "null argument");
   DeviceGuard g(ctx->device);
   cudaStream_t st = (cudaStream_t)stream;
-  XD_CUDA(cudaMemcpyAsync(h_out, ctx->d_stage, (size_t)xb4::kNumStage * ctx->n * sizeof(double),
+  XD_CUDA(cudaMemcpyAsync(h_out, ctx->d_stage, (size_t)ctx->stage_slots * ctx->n * sizeof(double),
                           cudaMemcpyDeviceToHost, st));
   XD_CUDA(cudaStreamSynchronize(st));
   return 0;
@@ -911,6 +1044,9 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
                            double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals,
                            void *stream) {
   if (!ctx || !flags) return fail(-1, "null argument");
+  if (ctx->series)
+    return fail(-1, "xd_load_static_scratch: the static scratch holds the 4-terminal layout; this family has "
+                    "internal drain/source nodes");
   if (ctx->n > XD_STATIC_MAX_INSTANCES)
     return fail(-1, "xd_load_static_scratch: " + std::to_string(ctx->n) + " instances exceed the static scratch "
                     "capacity of " + std::to_string(XD_STATIC_MAX_INSTANCES) + "; use xd_load");

@@ -84,63 +84,89 @@ def _stream_handle(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
+def _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, tnom_c, inst_internal=None):
+    """The ``xd_mosfet_family`` struct of a family, with the arrays it points into (keep them alive)."""
+    inst_model = np.ascontiguousarray(inst_model, dtype=np.int32)
+    n = int(inst_model.shape[0])
+    nodes = np.ascontiguousarray(np.asarray(inst_nodes, dtype=np.int32).reshape(-1))
+    if nodes.shape[0] != 4 * n:
+        raise _native.NativeError("inst_nodes must have shape [n, 4]")
+    is_pmos = np.array([1 if m.pmos else 0 for m in models], dtype=np.int32)
+    nparams = np.array([len(m.params) for m in models], dtype=np.int32)
+    names, values = [], []
+    for m in models:
+        for k, v in m.params.items():
+            names.append(str(k).encode())
+            values.append(float(v))
+    cnames = (ctypes.c_char_p * max(1, len(names)))(*names)
+    vals = np.ascontiguousarray(values if values else [0.0], dtype=np.float64)
+    pnames = list(inst_params.keys())
+    cpnames = (ctypes.c_char_p * max(1, len(pnames)))(*[p.encode() for p in pnames])
+    pv = np.full((n, max(1, len(pnames))), math.nan)
+    for k, p in enumerate(pnames):
+        pv[:, k] = np.asarray(inst_params[p], dtype=np.float64)
+    pv = np.ascontiguousarray(pv)
+    keep = [inst_model, nodes, is_pmos, nparams, vals, pv, cnames, cpnames]
+    fam = _native.XdMosfetFamily()
+    fam.level = int(level)
+    fam.n_models = len(models)
+    fam.model_is_pmos = is_pmos.ctypes.data_as(_native._ip)
+    fam.model_nparams = nparams.ctypes.data_as(_native._ip)
+    fam.model_param_names = cnames
+    fam.model_param_values = vals.ctypes.data_as(_native._dp)
+    fam.n_inst = n
+    fam.inst_model = inst_model.ctypes.data_as(_native._ip)
+    fam.inst_nodes = nodes.ctypes.data_as(_native._ip)
+    fam.n_inst_params = len(pnames)
+    fam.inst_param_names = cpnames
+    fam.inst_param_values = pv.ctypes.data_as(_native._dp)
+    fam.temp_c = float(temp_c)
+    fam.tnom_c = float(tnom_c)
+    if inst_internal is not None:
+        internal = np.ascontiguousarray(np.asarray(inst_internal, dtype=np.int32).reshape(-1))
+        if internal.shape[0] != 2 * n:
+            raise _native.NativeError("inst_internal must have shape [n, 2]")
+        keep.append(internal)
+        fam.inst_internal = internal.ctypes.data_as(_native._ip)
+    return fam, keep
+
+
+def internal_nodes(models, inst_model, inst_nodes, inst_params, level=14, temp_c=27.0, tnom_c=27.0):
+    """Which instances have an internal drain / source node ([n, 2] bool): the topology query the
+    reference's instances answer before their unknowns are numbered (``xd_internal_nodes``)."""
+    fam, keep = _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, tnom_c)
+    n = int(np.asarray(inst_model).shape[0])
+    flags = np.zeros(2 * n, dtype=np.int32)
+    lib = _native.load()
+    _native.check(lib.xd_internal_nodes(ctypes.byref(fam), flags.ctypes.data_as(_native._ip)), "xd_internal_nodes")
+    return flags.reshape(n, 2).astype(bool)
+
+
 class MosfetDevice:
     """One MOSFET family (one reference Device object) on one CUDA device.
 
-    models:       list of ``ModelCard``
-    inst_model:   int array [n]      card index per instance
-    inst_nodes:   int array [n, 4]   D, G, S, B unknown indices (-1 = ground)
-    inst_params:  dict name -> float array [n] (NaN = not given), e.g. L, W, NF, AD, DELVTO, M
-    pattern:      (rowptr, colind) CSR pattern of the Jacobian over the unknowns
+    models:        list of ``ModelCard``
+    inst_model:    int array [n]      card index per instance
+    inst_nodes:    int array [n, 4]   D, G, S, B unknown indices (-1 = ground)
+    inst_params:   dict name -> float array [n] (NaN = not given), e.g. L, W, NF, AD, DELVTO, M
+    pattern:       (rowptr, colind) CSR pattern of the Jacobian over the unknowns
+    inst_internal: int array [n, 2] internal drain / source unknowns (-1 = none), required when
+                   ``internal_nodes`` reports some
     """
 
     level = 14
 
     def __init__(self, models, inst_model, inst_nodes, inst_params, pattern, n_unknowns, device=0,
-                 temp_c=27.0, tnom_c=27.0, level=None):
+                 temp_c=27.0, tnom_c=27.0, level=None, inst_internal=None):
         if level is not None:
             self.level = int(level)
         lib = _native.load()
         self._lib = lib
         self.device = int(device)
-        inst_model = np.ascontiguousarray(inst_model, dtype=np.int32)
-        self.n = int(inst_model.shape[0])
+        self.n = int(np.asarray(inst_model).shape[0])
         self.n_unknowns = int(n_unknowns)
-        nodes = np.ascontiguousarray(np.asarray(inst_nodes, dtype=np.int32).reshape(-1))
-        if nodes.shape[0] != 4 * self.n:
-            raise _native.NativeError("inst_nodes must have shape [n, 4]")
-        is_pmos = np.array([1 if m.pmos else 0 for m in models], dtype=np.int32)
-        nparams = np.array([len(m.params) for m in models], dtype=np.int32)
-        names, values = [], []
-        for m in models:
-            for k, v in m.params.items():
-                names.append(str(k).encode())
-                values.append(float(v))
-        keep = []
-        self._names = (ctypes.c_char_p * max(1, len(names)))(*names)
-        vals = np.ascontiguousarray(values if values else [0.0], dtype=np.float64)
-        pnames = list(inst_params.keys())
-        self._pnames = (ctypes.c_char_p * max(1, len(pnames)))(*[p.encode() for p in pnames])
-        pv = np.full((self.n, max(1, len(pnames))), math.nan)
-        for k, p in enumerate(pnames):
-            pv[:, k] = np.asarray(inst_params[p], dtype=np.float64)
-        pv = np.ascontiguousarray(pv)
-        keep += [inst_model, nodes, is_pmos, nparams, vals, pv]
-        fam = _native.XdMosfetFamily()
-        fam.level = self.level
-        fam.n_models = len(models)
-        fam.model_is_pmos = is_pmos.ctypes.data_as(_native._ip)
-        fam.model_nparams = nparams.ctypes.data_as(_native._ip)
-        fam.model_param_names = self._names
-        fam.model_param_values = vals.ctypes.data_as(_native._dp)
-        fam.n_inst = self.n
-        fam.inst_model = inst_model.ctypes.data_as(_native._ip)
-        fam.inst_nodes = nodes.ctypes.data_as(_native._ip)
-        fam.n_inst_params = len(pnames)
-        fam.inst_param_names = self._pnames
-        fam.inst_param_values = pv.ctypes.data_as(_native._dp)
-        fam.temp_c = float(temp_c)
-        fam.tnom_c = float(tnom_c)
+        fam, keep = _family_struct(models, inst_model, inst_nodes, inst_params, self.level, temp_c, tnom_c,
+                                   inst_internal)
         rowptr = np.ascontiguousarray(pattern[0], dtype=np.int32)
         colind = np.ascontiguousarray(pattern[1], dtype=np.int32)
         if rowptr.shape[0] != self.n_unknowns + 1:
@@ -149,6 +175,7 @@ class MosfetDevice:
         csr = _native.XdCsr(self.n_unknowns, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
         h = ctypes.c_void_p()
         _native.check(lib.xd_create(ctypes.byref(fam), ctypes.byref(csr), self.device, ctypes.byref(h)), "xd_create")
+        self._keep = keep
         self._h = h
         self.nnz = int(rowptr[-1])
         self.n_state_slots = lib.xd_num_state_slots(h)

@@ -40,6 +40,11 @@ class Circuit:
     vsrc_pwl: list = field(default_factory=list)  # per source: None or (times, values)
     vdd: float = 1.2
     meta: dict = field(default_factory=dict)
+    # Internal drain / source nodes of the MOSFETs (series resistance): [n_mos, 2] unknown indices,
+    # -1 where the node collapses onto the terminal. They come after the nodes and the source
+    # branches, in instance order, drain first (the reference's numbering of internal variables).
+    mos_internal: np.ndarray | None = None
+    n_internal: int = 0
 
     @property
     def n_mos(self) -> int:
@@ -51,7 +56,16 @@ class Circuit:
 
     @property
     def n_unknowns(self) -> int:
-        return self.n_nodes + self.n_vsrc
+        return self.n_nodes + self.n_vsrc + self.n_internal
+
+    def mos_intrinsic_nodes(self) -> np.ndarray:
+        """[n_mos, 4] (D', G, S', B): the intrinsic device's nodes (D / S where no internal node)."""
+        m = self.mos_nodes.copy()
+        if self.mos_internal is not None:
+            for k, col in ((0, 0), (1, 2)):
+                has = self.mos_internal[:, k] >= 0
+                m[has, col] = self.mos_internal[has, k]
+        return m
 
     def branch_index(self, k: int) -> int:
         return self.n_nodes + k
@@ -67,10 +81,16 @@ def _pairs_2term(nodes: np.ndarray) -> np.ndarray:
 def jacobian_pattern(c: Circuit):
     """CSR (rowptr, colind) over the unknowns: union of MOSFET 4x4, R/C 2x2 and V-source stamps."""
     parts = []
-    m = c.mos_nodes.astype(np.int64)
+    m = c.mos_intrinsic_nodes().astype(np.int64)
     r = np.repeat(m, 4, axis=1)
     cc = np.tile(m, (1, 4))
     parts.append(np.stack([r.reshape(-1), cc.reshape(-1)], 1))
+    if c.mos_internal is not None:
+        # Series resistances: (D', D), (D, D'), (D, D) and the source's.
+        for k, col in ((0, 0), (1, 2)):
+            has = c.mos_internal[:, k] >= 0
+            a, b = c.mos_internal[has, k].astype(np.int64), c.mos_nodes[has, col].astype(np.int64)
+            parts.append(np.stack([np.concatenate([a, b, b]), np.concatenate([b, a, b])], 1))
     if c.res_nodes.shape[0]:
         parts.append(_pairs_2term(c.res_nodes.astype(np.int64)))
     if c.cap_nodes.shape[0]:
@@ -89,6 +109,19 @@ def jacobian_pattern(c: Circuit):
     np.add.at(rowptr, rows + 1, 1)
     rowptr = np.cumsum(rowptr).astype(np.int32)
     return rowptr, cols
+
+
+def with_internal_nodes(c: Circuit, flags) -> Circuit:
+    """The circuit with an internal drain / source unknown for every True in flags ([n_mos, 2], from
+    ``device.internal_nodes``), numbered after all other unknowns in instance order, drain first."""
+    import dataclasses
+
+    flags = np.asarray(flags, dtype=bool).reshape(-1, 2)
+    internal = np.full(flags.shape, -1, dtype=np.int64)
+    base = c.n_nodes + c.n_vsrc
+    order = np.flatnonzero(flags.reshape(-1))
+    internal.reshape(-1)[order] = base + np.arange(order.shape[0])
+    return dataclasses.replace(c, mos_internal=internal, n_internal=int(order.shape[0]))
 
 
 def _loguniform(rng, lo, hi, n):

@@ -69,6 +69,26 @@ def test_bsim3_parity_capmod_0_and_1(capmod, xpart):
     print("capMod", capmod, "xpart", xpart, "worst error / tolerance:", worst)
 
 
+def test_bsim3_parity_series_resistance_internal_nodes():
+    """Drain / source sheet resistance (RSH x NRD / NRS, the squares default to 1): internal D' / S'
+    nodes numbered as the reference numbers them, some instances with zero source squares (no
+    source node)."""
+    from xyce_b200.device import internal_nodes
+    from tests.parity import family_inputs
+
+    c = netlist.random_logic(2000, seed=71, vdd=1.8, length=0.18e-6)
+    n = c.n_mos
+    rng = np.random.default_rng(9)
+    cards = [ModelCard(False, {"RSH": 30.0}), ModelCard(True, {"RSH": 45.0})]
+    extra = {"NRD": rng.uniform(0.5, 3.0, n), "NRS": np.where(rng.random(n) < 0.3, 0.0, rng.uniform(0.5, 3.0, n))}
+    cards_, im, nd, params = family_inputs(c, cards, extra)
+    flags = internal_nodes(cards_, im, nd, params, level=9)
+    assert flags.any() and not flags.all()
+    c2 = netlist.with_internal_nodes(c, flags)
+    worst = run_sequence(c2, cards, SEQ, vrange=(-0.3, 2.1), extra_params=extra, level=9)
+    print("BSIM3 series:", int(flags.sum()), "internal nodes; worst error / tolerance:", worst)
+
+
 def test_bsim3_load_is_deterministic():
     c = netlist.random_logic(20000, seed=2, vdd=1.8, length=0.18e-6)
     rowptr, colind = netlist.jacobian_pattern(c)

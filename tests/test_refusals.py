@@ -31,7 +31,7 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
      "inst_internal"),
     (14, [ModelCard(False, {"NOSUCH": 1.0}), ModelCard(True, {})], None, "unknown BSIM4 model parameter"),
     (9, [ModelCard(False, {"CAPMOD": 4}), ModelCard(True, {})], None, "capMod"),
-    (9, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], None, "series resistance"),
+    (9, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], None, "inst_internal"),
     (9, NMOS_PMOS, {"NQSMOD": 1}, "nqsMod"),
     (9, NMOS_PMOS, {"IC1": 0.5}, "initial conditions"),
     (9, [ModelCard(False, {"NPEAK": 1e17}), ModelCard(True, {})], None, "unknown BSIM3 model parameter NPEAK"),
@@ -74,3 +74,19 @@ def test_internal_node_query_follows_sheet_resistance():
     assert (np.sort(got) == np.arange(c.n_unknowns, c2.n_unknowns)).all()
     rowptr, colind = netlist.jacobian_pattern(c2)
     assert rowptr.shape[0] == c2.n_unknowns + 1
+
+
+def test_internal_node_query_bsim3():
+    """BSIM3 gives an instance internal nodes whenever RSH times the squares (1 by default) is
+    positive (N_DEV_MOSFET_B3.C:1849-1865)."""
+    from xyce_b200.device import internal_nodes
+
+    c = netlist.inverter_ring(5)
+    n = c.n_mos
+    cards = [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})]
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float),
+              "NRS": np.where(np.arange(n) % 2 == 0, 0.0, 2.0)}
+    flags = internal_nodes(cards, c.mos_type, c.mos_nodes, params, level=9)
+    nmos = c.mos_type == 0
+    assert (flags[:, 0] == nmos).all()
+    assert (flags[:, 1] == (nmos & (np.arange(n) % 2 == 1))).all()

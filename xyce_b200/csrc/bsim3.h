@@ -9,9 +9,9 @@
 //   auxChargeCalculations                    N_DEV_MOSFET_B3.C:7447-7542
 //   Master::updateState                      N_DEV_MOSFET_B3.C:9199-9270
 //   Master::loadDAEVectors / loadDAEMatrices N_DEV_MOSFET_B3.C:9276-9613, 9624-9900
-// for nqsMod = 0, capMod 0, 1, 2 or 3, no drain/source series resistance (RSH * NRD = RSH * NRS = 0,
-// so D' = D and S' = S) and no instance initial conditions: the 4-terminal collapsed stamp, in
-// the same staged layout as the BSIM4 load.
+// for nqsMod = 0, capMod 0, 1, 2 or 3 and no instance initial conditions: the 4-terminal stamp in
+// the BSIM4 load's staged layout, or with drain / source sheet resistance (RSH * NRD, RSH * NRS)
+// the stamp on (D', G, S', B) plus the resistor couplings in the wide layout.
 #pragma once
 
 #include <string>
@@ -28,7 +28,7 @@
   /* temperature and instance */                                                                    \
   F(vtm) F(TempRatio) F(Nvtm) F(SourceSatCurrent) F(DrainSatCurrent) F(vjsm) F(IsEvjsm) F(vjdm)       \
   F(IsEvjdm) F(czbd) F(czbs) F(czbdsw) F(czbdswg) F(czbssw) F(czbsswg) F(PhiBTemp) F(PhiBSWTemp)    \
-  F(PhiBSWGTemp) F(MJ) F(MJSW) F(MJSWG) F(mult) F(off)                                              \
+  F(PhiBSWGTemp) F(MJ) F(MJSW) F(MJSWG) F(mult) F(off) F(drainConductance) F(sourceConductance)   \
   /* size-binned and size-derived */                                                                \
   F(vbsc) F(phi) F(phis3) F(sqrtPhi) F(Xdep0) F(vbi) F(dvt2) F(dvt2w) F(dvt1) F(dvt0) F(dvt1w)       \
   F(dvt0w) F(weff) F(leff) F(nlx) F(k1ox) F(k2ox) F(kt1) F(kt1l) F(kt2) F(w0) F(eta0) F(etab)        \
@@ -63,13 +63,19 @@ struct LoadOut {
   double jq[xb4::kNumMat];
   double sto[kNumStore];
   double sta[kNumState];
+  // With internal nodes (the BSIM4 wide layout): F at the external drain and source, dF/dx at
+  // (D', D), (D, D'), (D, D), (S', S), (S, S'), (S, S).
+  double vecx[2];
+  double jfx[6];
 };
 
 // One BSIM3 instance. V = terminal voltages (D, G, S, B); sto_old = limiter history (currSto on
 // Newton step 0, nextSto otherwise).
-template <class RV>
+// SERIES = true: V holds (D', G, S', B) and Vx the external (D, S); the sheet-resistance
+// resistors (N_DEV_MOSFET_B3.C:1849-1861, 7235-7236) load into vecx / jfx.
+template <bool SERIES = false, class RV>
 XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, const xb4::LoadFlags &fl,
-                      LoadOut &o) {
+                      LoadOut &o, const double *Vx = nullptr) {
   using namespace xdc;
 #define P(x) P_(f_##x)
   const double dtype = P(dtype);
@@ -79,8 +85,10 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
   const bool ChargeComputationNeeded = fl.tranop || fl.acop || fl.transient;
 
   // Node and branch voltages (:4690-4760).
-  const double Vd = V[0], Vg = V[1], Vs = V[2], Vb = V[3];
-  const double Vsp = Vs, Vdp = Vd;
+  const double Vdp = V[0], Vg = V[1], Vsp = V[2], Vb = V[3];
+  const double Vd = SERIES ? Vx[0] : Vdp, Vs = SERIES ? Vx[1] : Vsp;
+  const double Vddp = Vd - Vdp, Vssp = Vs - Vsp;
+  (void)Vddp; (void)Vssp;
   const double Vbsp = Vb - Vsp;
   const double Vgsp = Vg - Vsp;
   const double Vdpsp = Vdp - Vsp;
@@ -1525,9 +1533,22 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
     ceqbs -= (cbs);
     ceqbd -= (cbd);
   }
-  o.vec[3] += (ceqbs + ceqbd) * M;
-  o.vec[0] += (-(ceqbd - cdreq)) * M;
-  o.vec[2] += (-(cdreq + ceqbs)) * M;
+  if (SERIES) {
+    // Resistor currents at the external nodes (:9355-9362); the primes take -Idrain / -Isource.
+    const double gdr = P(drainConductance), gsr = P(sourceConductance);
+    const double Idrain = gdr * Vddp, Isource = gsr * Vssp;
+    o.vecx[0] = 0.0;
+    o.vecx[1] = 0.0;
+    if (gdr != 0.0) o.vecx[0] += Idrain * M;
+    if (gsr != 0.0) o.vecx[1] += Isource * M;
+    o.vec[3] += (ceqbs + ceqbd) * M;
+    o.vec[0] += (-(ceqbd - cdreq) - Idrain) * M;
+    o.vec[2] += (-(cdreq + ceqbs) - Isource) * M;
+  } else {
+    o.vec[3] += (ceqbs + ceqbd) * M;
+    o.vec[0] += (-(ceqbd - cdreq)) * M;
+    o.vec[2] += (-(cdreq + ceqbs)) * M;
+  }
   if (fl.voltlim && !origFlag) {
     double cdreq_Jdxp, ceqbd_Jdxp, ceqbs_Jdxp = 0.0;
     if (mode >= 0) {
@@ -1592,18 +1613,42 @@ XD_HD void bsim3_load(const RV &P_, const double V[4], const double *sto_old, co
   }
 #define JF(r, c) o.jf[(r)*4 + (c)]
 #define JQ(r, c) o.jq[(r)*4 + (c)]
-  JF(3, 1) += (-gbgs) * M;
-  JF(3, 3) += (gbd + gbs - gbbs) * M;
-  JF(3, 0) += (-gbd + gbbdp) * M;
-  JF(3, 2) += (-gbs + gbbsp) * M;
-  JF(0, 3) -= (gbd - Gmbs - gbdpb) * M;
-  JF(0, 1) += (Gmv + gbdpg) * M;
-  JF(0, 0) += (gds + gbd + RevSum + gbdpdp) * M;
-  JF(0, 2) -= (gds + FwdSum - gbdpsp) * M;
-  JF(2, 1) += (-Gmv + gbspg) * M;
-  JF(2, 3) -= (gbs + Gmbs - gbspb) * M;
-  JF(2, 0) -= (gds + RevSum - gbspdp) * M;
-  JF(2, 2) += (gds + gbs + FwdSum + gbspsp) * M;
+  if (SERIES) {
+    // The sheet-resistance couplings, in the reference's statement order (:9631-9647, 9705, 9739).
+    const double gdr = P(drainConductance), gsr = P(sourceConductance);
+    for (int k = 0; k < 6; ++k) o.jfx[k] = 0.0;
+    o.jfx[2] += gdr * M;
+    o.jfx[1] -= gdr * M;
+    o.jfx[5] += gsr * M;
+    o.jfx[4] -= gsr * M;
+    JF(3, 1) += (-gbgs) * M;
+    JF(3, 3) += (gbd + gbs - gbbs) * M;
+    JF(3, 0) += (-gbd + gbbdp) * M;
+    JF(3, 2) += (-gbs + gbbsp) * M;
+    o.jfx[0] -= gdr * M;
+    JF(0, 3) -= (gbd - Gmbs - gbdpb) * M;
+    JF(0, 1) += (Gmv + gbdpg) * M;
+    JF(0, 0) += (gdr + gds + gbd + RevSum + gbdpdp) * M;
+    JF(0, 2) -= (gds + FwdSum - gbdpsp) * M;
+    JF(2, 1) += (-Gmv + gbspg) * M;
+    JF(2, 3) -= (gbs + Gmbs - gbspb) * M;
+    o.jfx[3] -= gsr * M;
+    JF(2, 0) -= (gds + RevSum - gbspdp) * M;
+    JF(2, 2) += (gsr + gds + gbs + FwdSum + gbspsp) * M;
+  } else {
+    JF(3, 1) += (-gbgs) * M;
+    JF(3, 3) += (gbd + gbs - gbbs) * M;
+    JF(3, 0) += (-gbd + gbbdp) * M;
+    JF(3, 2) += (-gbs + gbbsp) * M;
+    JF(0, 3) -= (gbd - Gmbs - gbdpb) * M;
+    JF(0, 1) += (Gmv + gbdpg) * M;
+    JF(0, 0) += (gds + gbd + RevSum + gbdpdp) * M;
+    JF(0, 2) -= (gds + FwdSum - gbdpsp) * M;
+    JF(2, 1) += (-Gmv + gbspg) * M;
+    JF(2, 3) -= (gbs + Gmbs - gbspb) * M;
+    JF(2, 0) -= (gds + RevSum - gbspdp) * M;
+    JF(2, 2) += (gds + gbs + FwdSum + gbspsp) * M;
+  }
   if (!(!fl.dcop && fl.init_tran && fl.newton_iter == 0)) {
     JQ(1, 1) += (CAPcggb)*M;
     JQ(1, 3) -= (CAPcggb + CAPcgdb + CAPcgsb) * M;

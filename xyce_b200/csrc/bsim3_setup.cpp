@@ -323,9 +323,12 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const xb4::S
   if (!ip.g("AS")) ip.sourceArea = 0.0;
   if (ip.nqsMod != 0) return "BSIM3 nqsMod != 0 is not supported";
   if (ip.g("IC1") || ip.g("IC2") || ip.g("IC3")) return "BSIM3 instance initial conditions are not supported";
-  // Instance::processParams: series resistance from the sheet resistance.
-  if (m.sheetResistance * ip.drainSquares > 0.0 || m.sheetResistance * ip.sourceSquares > 0.0)
-    return "BSIM3 drain/source series resistance (RSH * NRD, RSH * NRS > 0) is not supported";
+  // Instance::processParams (:1849-1861): series conductances from the sheet resistance; a
+  // nonzero one gives the instance its internal drain / source node (:1863-1865).
+  double drainConductance = m.sheetResistance * ip.drainSquares;
+  drainConductance = (drainConductance > 0.0) ? 1.0 / drainConductance : 0.0;
+  double sourceConductance = m.sheetResistance * ip.sourceSquares;
+  sourceConductance = (sourceConductance > 0.0) ? 1.0 / sourceConductance : 0.0;
   const double temp = ip.temp;
   if (!ms.temp_done) {
     ms.temp_done = true;
@@ -437,6 +440,8 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const xb4::S
   R(MJSWG) = m.bulkJctGateSideGradingCoeff;
   R(mult) = ip.mult;
   R(off) = ip.off;
+  R(drainConductance) = drainConductance;
+  R(sourceConductance) = sourceConductance;
 #define S(x) R(x) = p.x;
   S(vbsc) S(phi) S(phis3) S(sqrtPhi) S(Xdep0) S(vbi) S(dvt2) S(dvt2w) S(dvt1) S(dvt0) S(dvt1w) S(dvt0w)
   S(weff) S(leff) S(nlx) S(k1ox) S(k2ox) S(kt1) S(kt1l) S(kt2) S(w0) S(eta0) S(etab) S(theta0vb0) S(vth0)

@@ -430,12 +430,14 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(double *out, int iters) 
 // Launch shapes of the evaluation kernel. The kernel is register-bound (hundreds of live FP64
 // intermediates); the shapes trade occupancy against spills. xd_create times each on the
 // circuit and keeps the fastest.
-// BSIM3: one thread per instance.
+// BSIM3: one thread per instance. SERIES: internal drain / source nodes (ext = external D, S),
+// wide staging layout, as for BSIM4.
+template <bool SERIES>
 __global__ void __launch_bounds__(128) bsim3_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
-    xb4::LoadFlags fl) {
+    xb4::LoadFlags fl, const int2 *__restrict__ ext) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 nd = nodes[i];
@@ -450,13 +452,34 @@ __global__ void __launch_bounds__(128) bsim3_eval_kernel(
   for (int k = 0; k < xb3::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
   xb4::RecPtr rp{tab + rec[i], nrec};
   xb3::LoadOut o;
-  xb3::bsim3_load(rp, V, sto_old, fl, o);
+  if (SERIES) {
+    const int2 ex = ext[i];
+    double Vx[2];
+    Vx[0] = ex.x >= 0 ? sol[ex.x] : 0.0;
+    Vx[1] = ex.y >= 0 ? sol[ex.y] : 0.0;
+    xb3::bsim3_load<true>(rp, V, sto_old, fl, o, Vx);
 #pragma unroll
-  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+      for (int r = 0; r < 4; ++r) stage[(size_t)(v * xb4::kSerVecRows + r) * n + i] = o.vec[v * 4 + r];
+    stage[(size_t)4 * n + i] = o.vecx[0];
+    stage[(size_t)5 * n + i] = o.vecx[1];
+    const size_t mf = 4 * xb4::kSerVecRows, mq = mf + xb4::kSerMat;
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mf + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) stage[(mf + xb4::kNumMat + k) * n + i] = o.jfx[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mq + k) * n + i] = o.jq[k];
+  } else {
+    xb3::bsim3_load<false>(rp, V, sto_old, fl, o);
+#pragma unroll
+    for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+  }
 #pragma unroll
   for (int k = 0; k < xb3::kNumStore; ++k) next_sto[(size_t)k * n + i] = o.sto[k];
 #pragma unroll
@@ -495,8 +518,14 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
     return;
   }
   if (ctx->family == kFamilyBsim3) {
-    bsim3_eval_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
-                                                       next_sta, curr_sta, next_sto, curr_sto, stage, fl);
+    if (ctx->series)
+      bsim3_eval_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes,
+                                                               sol, next_sta, curr_sta, next_sto, curr_sto, stage, fl,
+                                                               ctx->d_ext);
+    else
+      bsim3_eval_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes,
+                                                                sol, next_sta, curr_sta, next_sto, curr_sto, stage,
+                                                                fl, nullptr);
     return;
   }
   const int blk = kEvalVariants[v].block;
@@ -516,6 +545,23 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
     default: bsim4_eval_kernel<128, 3, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
   }
 #undef XD_EVAL_ARGS
+}
+
+// Internal drain / source nodes per instance: BSIM4 where the sheet resistance and the squares are
+// positive (record flags), BSIM3 where the series conductance is nonzero.
+void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned char> &dint,
+                    std::vector<unsigned char> &sint) {
+  const size_t nr = (size_t)rt.n_records;
+  for (size_t i = 0; i < rt.inst_rec.size(); ++i) {
+    const size_t r = (size_t)rt.inst_rec[i];
+    if (family == kFamilyBsim4) {
+      dint[i] = rt.tab[(size_t)xb4::f_dExists * nr + r] != 0.0;
+      sint[i] = rt.tab[(size_t)xb4::f_sExists * nr + r] != 0.0;
+    } else if (family == kFamilyBsim3) {
+      dint[i] = rt.tab[(size_t)xb3::f_drainConductance * nr + r] != 0.0;
+      sint[i] = rt.tab[(size_t)xb3::f_sourceConductance * nr + r] != 0.0;
+    }
+  }
 }
 
 // Times every launch shape on the circuit's own instances at a synthetic operating point (node
@@ -604,7 +650,8 @@ int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
   if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
   const int n = fam->n_inst;
   for (int k = 0; k < 2 * n; ++k) flags[k] = 0;
-  if (!(fam->level == 14 || fam->level == 54)) return 0;  // only BSIM4 series resistance is modelled
+  const bool b4 = fam->level == 14 || fam->level == 54, b3 = fam->level == 9 || fam->level == 49;
+  if (!b4 && !b3) return 0;  // MOSFET1 series resistance is not modelled
   std::vector<xb4::ModelSpec> models(fam->n_models);
   size_t off = 0;
   for (int m = 0; m < fam->n_models; ++m) {
@@ -618,12 +665,15 @@ int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
   opts.temp_c = fam->temp_c;
   opts.tnom_c = fam->tnom_c;
   xb4::RecordTable rt;
-  const std::string e = xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  const std::string e =
+      b4 ? xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+         : xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
+  std::vector<unsigned char> dint(n, 0), sint(n, 0);
+  internal_flags(b4 ? kFamilyBsim4 : kFamilyBsim3, rt, dint, sint);
   for (int i = 0; i < n; ++i) {
-    const int r = rt.inst_rec[i];
-    flags[2 * i] = rt.tab[(size_t)xb4::f_dExists * rt.n_records + r] != 0.0;
-    flags[2 * i + 1] = rt.tab[(size_t)xb4::f_sExists * rt.n_records + r] != 0.0;
+    flags[2 * i] = dint[i];
+    flags[2 * i + 1] = sint[i];
   }
   return 0;
 }
@@ -699,13 +749,8 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   // Internal drain / source nodes (BSIM4 sheet resistance): which instances have them.
   std::vector<unsigned char> dint(n, 0), sint(n, 0);
   bool series = false;
-  if (family == kFamilyBsim4)
-    for (int i = 0; i < n; ++i) {
-      const int r = rt.inst_rec[i];
-      dint[i] = rt.tab[(size_t)xb4::f_dExists * rt.n_records + r] != 0.0;
-      sint[i] = rt.tab[(size_t)xb4::f_sExists * rt.n_records + r] != 0.0;
-      series = series || dint[i] || sint[i];
-    }
+  internal_flags(family, rt, dint, sint);
+  for (int i = 0; i < n; ++i) series = series || dint[i] || sint[i];
   if (series && !fam->inst_internal)
     return fail(-1, "instances have internal drain/source nodes (RSH with NRD/NRS): pass their unknowns in "
                     "inst_internal (xd_internal_nodes lists which instances have them)");

@@ -100,10 +100,11 @@ typedef struct xd_csr {
 int xd_create(const xd_mosfet_family *family, const xd_csr *pattern, int cuda_device, xd_ctx **out);
 
 /* Topology query before xd_create, as the reference's instances report their internal variables
- * (N_DEV_MOSFET_B4.C:3684-3760, registerLIDs :4996-5060; N_DEV_MOSFET_B3.C:1849-1865):
+ * (N_DEV_MOSFET_B4.C:3684-3760, registerLIDs :4996-5060; N_DEV_MOSFET_B3.C:1849-1865;
+ * N_DEV_MOSFET1.C:1180-1253):
  * flags[2i] / flags[2i+1] = 1 when instance i has an internal drain / source node (BSIM4 with
  * rdsMod = 0: sheet resistance RSH with NRD / NRS > 0; BSIM3: RSH times NRD / NRS, 1 square by
- * default, > 0; MOSFET1: none). The caller allocates those unknowns (the reference numbers them after the
+ * default, nonzero; MOSFET1: RD / RS nonzero, else RSH times NRD / NRS nonzero). The caller allocates those unknowns (the reference numbers them after the
  * external ones, in instance order, drain first) and passes them in inst_internal. Host-only. */
 int xd_internal_nodes(const xd_mosfet_family *family, int *flags);
 

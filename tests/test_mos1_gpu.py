@@ -35,3 +35,24 @@ def test_mos1_parity_default_cards_ring():
     worst = run_sequence(c, [ModelCard(False, {}), ModelCard(True, {})], SEQ, vrange=(0.0, 1.8), level=1,
                          charges_in_dc=True)
     print("worst error / tolerance:", worst)
+
+
+def test_mos1_parity_series_resistance_internal_nodes():
+    """Drain / source series resistance: NMOS with RD (which wins over the sheet resistance) and
+    RSH x NRS, PMOS with RS alone (its drain collapses onto the terminal); the internal D' / S'
+    nodes are numbered as the reference numbers them (N_DEV_MOSFET1.C:1180-1220, 1248-1253)."""
+    from xyce_b200.device import internal_nodes
+    from tests.parity import family_inputs
+
+    c = netlist.random_logic(2000, seed=23)
+    n = c.n_mos
+    rng = np.random.default_rng(6)
+    cards = [ModelCard(False, dict(CARDS[0].params, RD=20.0, RSH=30.0)), ModelCard(True, dict(CARDS[1].params, RS=15.0))]
+    extra = {"NRD": rng.uniform(0.5, 3.0, n), "NRS": rng.uniform(0.5, 3.0, n)}
+    cards_, im, nd, params = family_inputs(c, cards, extra)
+    flags = internal_nodes(cards_, im, nd, params, level=1)
+    nmos = c.mos_type == 0
+    assert (flags[:, 0] == nmos).all() and flags[:, 1].all()
+    c2 = netlist.with_internal_nodes(c, flags)
+    worst = run_sequence(c2, cards, SEQ, vrange=(-0.5, 2.5), extra_params=extra, level=1, charges_in_dc=True)
+    print("MOSFET1 series:", int(flags.sum()), "internal nodes; worst error / tolerance:", worst)

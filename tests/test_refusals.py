@@ -35,7 +35,8 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
     (9, NMOS_PMOS, {"NQSMOD": 1}, "nqsMod"),
     (9, NMOS_PMOS, {"IC1": 0.5}, "initial conditions"),
     (9, [ModelCard(False, {"NPEAK": 1e17}), ModelCard(True, {})], None, "unknown BSIM3 model parameter NPEAK"),
-    (1, [ModelCard(False, {"RD": 10.0}), ModelCard(True, {})], None, "series resistance"),
+    (1, [ModelCard(False, {"RD": 10.0}), ModelCard(True, {})], None, "inst_internal"),
+    (1, [ModelCard(False, {"RSH": 10.0}), ModelCard(True, {})], {"NRD": 0.0}, "infinite series conductance"),
     (1, NMOS_PMOS, {"IC2": 0.5}, "initial conditions"),
 ])
 def test_unsupported_option_is_refused(level, cards, extra, match):
@@ -90,3 +91,20 @@ def test_internal_node_query_bsim3():
     nmos = c.mos_type == 0
     assert (flags[:, 0] == nmos).all()
     assert (flags[:, 1] == (nmos & (np.arange(n) % 2 == 1))).all()
+
+
+def test_internal_node_query_mos1():
+    """MOSFET1: RD / RS give the node whatever the squares; otherwise RSH x NRD / NRS (1 by
+    default) does; with neither the node collapses (N_DEV_MOSFET1.C:1180-1220)."""
+    from xyce_b200.device import internal_nodes
+
+    c = netlist.inverter_ring(5)
+    n = c.n_mos
+    cards = [ModelCard(False, {"RD": 10.0}), ModelCard(True, {"RSH": 20.0})]
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float), "NRS": np.full(n, 2.0)}
+    flags = internal_nodes(cards, c.mos_type, c.mos_nodes, params, level=1)
+    nmos = c.mos_type == 0
+    assert (flags[:, 0] == True).all()  # noqa: E712
+    assert (flags[:, 1] == ~nmos).all()
+    none = internal_nodes(NMOS_PMOS, c.mos_type, c.mos_nodes, params, level=1)
+    assert not none.any()

@@ -172,12 +172,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
 }
 
 // MOSFET level 1: one thread per instance; reads the previous time point's Meyer state for
-// back-averaging.
+// back-averaging. SERIES: the nodes are (D', G, S', B), ext the external (D, S), and the staging
+// is the wide layout.
+template <bool SERIES>
 __global__ void __launch_bounds__(128) mos1_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, const double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
-    xb4::LoadFlags fl) {
+    xb4::LoadFlags fl, const int2 *__restrict__ ext) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 nd = nodes[i];
@@ -197,13 +199,34 @@ __global__ void __launch_bounds__(128) mos1_eval_kernel(
   for (int k = 0; k < xm1::kNumState; ++k) csta[k] = curr_sta[(size_t)k * n + i];
   xb4::RecPtr rp{tab + rec[i], nrec};
   xm1::LoadOut o;
-  xm1::mos1_load(rp, V, sto_old, csta, csto, fl, o);
+  if (SERIES) {
+    const int2 ex = ext[i];
+    double Vx[2];
+    Vx[0] = ex.x >= 0 ? sol[ex.x] : 0.0;
+    Vx[1] = ex.y >= 0 ? sol[ex.y] : 0.0;
+    xm1::mos1_load<true>(rp, V, sto_old, csta, csto, fl, o, Vx);
 #pragma unroll
-  for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+      for (int r = 0; r < 4; ++r) stage[(size_t)(v * xb4::kSerVecRows + r) * n + i] = o.vec[v * 4 + r];
+    stage[(size_t)4 * n + i] = o.vecx[0];
+    stage[(size_t)5 * n + i] = o.vecx[1];
+    const size_t mf = 4 * xb4::kSerVecRows, mq = mf + xb4::kSerMat;
 #pragma unroll
-  for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mf + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) stage[(mf + xb4::kNumMat + k) * n + i] = o.jfx[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(mq + k) * n + i] = o.jq[k];
+  } else {
+    xm1::mos1_load<false>(rp, V, sto_old, csta, csto, fl, o);
+#pragma unroll
+    for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + k) * n + i] = o.jf[k];
+#pragma unroll
+    for (int k = 0; k < xb4::kNumMat; ++k) stage[(size_t)(xb4::kNumVec + xb4::kNumMat + k) * n + i] = o.jq[k];
+  }
 #pragma unroll
   for (int k = 0; k < xm1::kNumStore; ++k) next_sto[(size_t)k * n + i] = o.sto[k];
 #pragma unroll
@@ -513,8 +536,14 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
                  double *curr_sta, double *next_sto, const double *curr_sto, double *stage, cudaStream_t st) {
   const int n = ctx->n;
   if (ctx->family == kFamilyMos1) {
-    mos1_eval_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta,
-                                                      curr_sta, next_sto, curr_sto, stage, fl);
+    if (ctx->series)
+      mos1_eval_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
+                                                              next_sta, curr_sta, next_sto, curr_sto, stage, fl,
+                                                              ctx->d_ext);
+    else
+      mos1_eval_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
+                                                               next_sta, curr_sta, next_sto, curr_sto, stage, fl,
+                                                               nullptr);
     return;
   }
   if (ctx->family == kFamilyBsim3) {
@@ -548,7 +577,7 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
 }
 
 // Internal drain / source nodes per instance: BSIM4 where the sheet resistance and the squares are
-// positive (record flags), BSIM3 where the series conductance is nonzero.
+// positive (record flags), BSIM3 and MOSFET1 where the series conductance is nonzero.
 void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned char> &dint,
                     std::vector<unsigned char> &sint) {
   const size_t nr = (size_t)rt.n_records;
@@ -560,6 +589,9 @@ void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned
     } else if (family == kFamilyBsim3) {
       dint[i] = rt.tab[(size_t)xb3::f_drainConductance * nr + r] != 0.0;
       sint[i] = rt.tab[(size_t)xb3::f_sourceConductance * nr + r] != 0.0;
+    } else {
+      dint[i] = rt.tab[(size_t)xm1::f_drainConductance * nr + r] != 0.0;
+      sint[i] = rt.tab[(size_t)xm1::f_sourceConductance * nr + r] != 0.0;
     }
   }
 }
@@ -651,7 +683,7 @@ int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
   const int n = fam->n_inst;
   for (int k = 0; k < 2 * n; ++k) flags[k] = 0;
   const bool b4 = fam->level == 14 || fam->level == 54, b3 = fam->level == 9 || fam->level == 49;
-  if (!b4 && !b3) return 0;  // MOSFET1 series resistance is not modelled
+  if (!b4 && !b3 && fam->level != 1) return fail(-1, "unsupported MOSFET level");
   std::vector<xb4::ModelSpec> models(fam->n_models);
   size_t off = 0;
   for (int m = 0; m < fam->n_models; ++m) {
@@ -666,11 +698,12 @@ int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
   opts.tnom_c = fam->tnom_c;
   xb4::RecordTable rt;
   const std::string e =
-      b4 ? xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
-         : xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+      b4   ? xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+      : b3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
+           : xm1::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
   std::vector<unsigned char> dint(n, 0), sint(n, 0);
-  internal_flags(b4 ? kFamilyBsim4 : kFamilyBsim3, rt, dint, sint);
+  internal_flags(b4 ? kFamilyBsim4 : (b3 ? kFamilyBsim3 : kFamilyMos1), rt, dint, sint);
   for (int i = 0; i < n; ++i) {
     flags[2 * i] = dint[i];
     flags[2 * i + 1] = sint[i];
@@ -746,13 +779,13 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       : family == kFamilyBsim3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
                                : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
-  // Internal drain / source nodes (BSIM4 sheet resistance): which instances have them.
+  // Internal drain / source nodes (series resistance): which instances have them.
   std::vector<unsigned char> dint(n, 0), sint(n, 0);
   bool series = false;
   internal_flags(family, rt, dint, sint);
   for (int i = 0; i < n; ++i) series = series || dint[i] || sint[i];
   if (series && !fam->inst_internal)
-    return fail(-1, "instances have internal drain/source nodes (RSH with NRD/NRS): pass their unknowns in "
+    return fail(-1, "instances have internal drain/source nodes (series resistance): pass their unknowns in "
                     "inst_internal (xd_internal_nodes lists which instances have them)");
   // Node indices and gather maps (registerLIDs / registerJacLIDs equivalent). With internal nodes
   // the intrinsic device sits on (D', G, S', B) and ext keeps the external drain and source.

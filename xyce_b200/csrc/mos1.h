@@ -8,9 +8,11 @@
 //   DeviceSupport::qmeyer                    src/DeviceModelPKG/Core/src/N_DEV_DeviceSupport.C:545-632
 //   Master::updateState                      N_DEV_MOSFET1.C:4069-4160
 //   Master::loadDAEVectors / loadDAEMatrices N_DEV_MOSFET1.C:4168-4396, 4407-4697
-// for the reference's default Meyer back-averaging (NEWMEYER off), without drain/source series
-// resistance nodes (RD = RS = 0 and no sheet resistance) and without instance initial
-// conditions, i.e. the 4-terminal collapsed stamp, the same staged layout as the BSIM4 load.
+// for the reference's default Meyer back-averaging (NEWMEYER off) and without instance initial
+// conditions. Without drain/source series resistance (RD = RS = 0, no sheet resistance) the
+// drain and source primes collapse onto the terminals: the 4-terminal stamp, the same staged
+// layout as the BSIM4 load. With it (SERIES = true) the primes are internal nodes and the
+// resistors load into the BSIM4 wide layout (vecx / jfx).
 #pragma once
 
 #include <string>
@@ -24,7 +26,7 @@
   F(dtype) F(gamma) F(lambda) F(mj) F(mjsw) F(vt) F(tPhi) F(tVbi) F(tVto) F(sourceVcrit) F(drainVcrit) \
   F(Beta) F(DrainSatCur) F(SourceSatCur) F(Cbd) F(Cbdsw) F(Cbs) F(Cbssw) F(tDepCap) F(tBulkPot)       \
   F(f2d) F(f3d) F(f4d) F(f2s) F(f3s) F(f4s) F(GateSourceOverlapCap) F(GateDrainOverlapCap)            \
-  F(GateBulkOverlapCap) F(OxideCap) F(mult) F(off)
+  F(GateBulkOverlapCap) F(OxideCap) F(mult) F(off) F(drainConductance) F(sourceConductance)
 
 namespace xm1 {
 
@@ -50,6 +52,10 @@ struct LoadOut {
   double jq[xb4::kNumMat];
   double sto[kNumStore];
   double sta[kNumState];
+  // With internal nodes: F at the external drain and source, dF/dx at (D', D), (D, D'), (D, D),
+  // (S', S), (S, S'), (S, S).
+  double vecx[2];
+  double jfx[6];
 };
 
 // Meyer gate capacitances (DeviceSupport::qmeyer).
@@ -89,9 +95,11 @@ XD_HD void qmeyer(double vgs, double vgd, double vgb, double von, double vdsat, 
 // One MOSFET1 instance. V = terminal voltages (D, G, S, B); sto_old = limiter history (currSto on
 // Newton step 0, nextSto otherwise); curr_sta / curr_sto = the previous accepted time point's state
 // and store, read for Meyer back-averaging.
-template <class RV>
+// SERIES = true: V holds (D', G, S', B) and Vx the external (D, S); the drain/source resistors
+// (N_DEV_MOSFET1.C:1180-1220, 3302-3303) load into vecx / jfx.
+template <bool SERIES = false, class RV>
 XD_HD void mos1_load(const RV &P_, const double V[4], const double *sto_old, const double *curr_sta,
-                     const double *curr_sto, const xb4::LoadFlags &fl, LoadOut &o) {
+                     const double *curr_sto, const xb4::LoadFlags &fl, LoadOut &o, const double *Vx = nullptr) {
   using namespace xdc;
 #define P(x) P_(f_##x)
   const double dtype = P(dtype);
@@ -101,8 +109,8 @@ XD_HD void mos1_load(const RV &P_, const double V[4], const double *sto_old, con
   const double vt = P(vt);
   const double DrainSatCur = P(DrainSatCur), SourceSatCur = P(SourceSatCur);
   const double Beta = P(Beta);
-  const double Vd = V[0], Vg = V[1], Vs = V[2], Vb = V[3];
-  const double Vdp = Vd, Vsp = Vs;
+  const double Vdp = V[0], Vg = V[1], Vsp = V[2], Vb = V[3];
+  const double Vd = SERIES ? Vx[0] : Vdp, Vs = SERIES ? Vx[1] : Vsp;
   const double Vbsp = Vb - Vsp;
   const double Vgsp = Vg - Vsp;
   const double Vdpsp = Vdp - Vsp;
@@ -348,13 +356,20 @@ XD_HD void mos1_load(const RV &P_, const double V[4], const double *sto_old, con
   o.sta[t_qbd] = qbd;
   o.sta[t_qbs] = qbs;
 
-  // Master::loadDAEVectors (:4168-4396). Local terminal order D=0, G=1, S=2, B=3; the drain and
-  // source primes coincide with D and S.
+  // Master::loadDAEVectors (:4168-4396). Local order D'=0, G=1, S'=2, B=3 (the primes coincide
+  // with D and S without series resistance).
   for (int k = 0; k < xb4::kNumVec; ++k) o.vec[k] = 0.0;
   const double ceqbs = dtype * (cbs), ceqbd = dtype * (cbd), ceqgb = 0.0, ceqgs = 0.0, ceqgd = 0.0;
-  const double Idrain = 0.0, Isource = 0.0;
+  const double gdr = SERIES ? P(drainConductance) : 0.0, gsr = SERIES ? P(sourceConductance) : 0.0;
+  const double Idrain = SERIES ? gdr * (Vd - Vdp) : 0.0, Isource = SERIES ? gsr * (Vs - Vsp) : 0.0;
+  if (SERIES) {
+    o.vecx[0] = 0.0;
+    o.vecx[1] = 0.0;
+    if (gdr != 0.0) o.vecx[0] += Idrain * M;
+  }
   double coef = (ceqgs + ceqgd + ceqgb);
   o.vec[1] += coef * M;
+  if (SERIES && gsr != 0.0) o.vecx[1] += Isource * M;
   coef = ceqbs + ceqbd - ceqgb;
   o.vec[3] += coef * M;
   coef = -Idrain - (ceqbd - cdreq + ceqgd);
@@ -400,26 +415,49 @@ XD_HD void mos1_load(const RV &P_, const double V[4], const double *sto_old, con
     o.jf[k] = 0.0;
     o.jq[k] = 0.0;
   }
-  const double drainConductance = 0.0, sourceConductance = 0.0;
 #define JF(r, c) o.jf[(r)*4 + (c)]
 #define JQ(r, c) o.jq[(r)*4 + (c)]
-  JF(0, 0) += drainConductance * M;
-  JF(0, 0) -= drainConductance * M;
-  JF(2, 2) += sourceConductance * M;
-  JF(2, 2) -= sourceConductance * M;
-  JF(3, 3) += (gbs + gbd) * M;
-  JF(3, 0) -= gbd * M;
-  JF(3, 2) -= gbs * M;
-  JF(0, 0) -= drainConductance * M;
-  JF(0, 1) += (Gm) * M;
-  JF(0, 3) += (-gbd + Gmbs) * M;
-  JF(0, 0) += (drainConductance + gds + gbd + revsum) * M;
-  JF(0, 2) += (-gds - nrmsum) * M;
-  JF(2, 1) -= (Gm) * M;
-  JF(2, 2) -= sourceConductance * M;
-  JF(2, 3) -= (gbs + Gmbs) * M;
-  JF(2, 0) -= (gds + revsum) * M;
-  JF(2, 2) += (sourceConductance + gds + gbs + nrmsum) * M;
+  if (SERIES) {
+    // The resistor couplings in the reference's statement order (:4449-4452, 4482-4485, 4541,
+    // 4578).
+    for (int k = 0; k < 6; ++k) o.jfx[k] = 0.0;
+    o.jfx[2] += gdr * M;
+    o.jfx[1] -= gdr * M;
+    o.jfx[5] += gsr * M;
+    o.jfx[4] -= gsr * M;
+    JF(3, 3) += (gbs + gbd) * M;
+    JF(3, 0) -= gbd * M;
+    JF(3, 2) -= gbs * M;
+    o.jfx[0] -= gdr * M;
+    JF(0, 1) += (Gm) * M;
+    JF(0, 3) += (-gbd + Gmbs) * M;
+    JF(0, 0) += (gdr + gds + gbd + revsum) * M;
+    JF(0, 2) += (-gds - nrmsum) * M;
+    JF(2, 1) -= (Gm) * M;
+    o.jfx[3] -= gsr * M;
+    JF(2, 3) -= (gbs + Gmbs) * M;
+    JF(2, 0) -= (gds + revsum) * M;
+    JF(2, 2) += (gsr + gds + gbs + nrmsum) * M;
+  } else {
+    const double drainConductance = 0.0, sourceConductance = 0.0;
+    JF(0, 0) += drainConductance * M;
+    JF(0, 0) -= drainConductance * M;
+    JF(2, 2) += sourceConductance * M;
+    JF(2, 2) -= sourceConductance * M;
+    JF(3, 3) += (gbs + gbd) * M;
+    JF(3, 0) -= gbd * M;
+    JF(3, 2) -= gbs * M;
+    JF(0, 0) -= drainConductance * M;
+    JF(0, 1) += (Gm) * M;
+    JF(0, 3) += (-gbd + Gmbs) * M;
+    JF(0, 0) += (drainConductance + gds + gbd + revsum) * M;
+    JF(0, 2) += (-gds - nrmsum) * M;
+    JF(2, 1) -= (Gm) * M;
+    JF(2, 2) -= sourceConductance * M;
+    JF(2, 3) -= (gbs + Gmbs) * M;
+    JF(2, 0) -= (gds + revsum) * M;
+    JF(2, 2) += (sourceConductance + gds + gbs + nrmsum) * M;
+  }
   JQ(1, 1) += (gcgd + gcgs + gcgb) * M;
   JQ(1, 3) -= gcgb * M;
   JQ(1, 0) -= gcgd * M;

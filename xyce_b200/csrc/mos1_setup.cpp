@@ -110,8 +110,6 @@ std::string process_model(const xb4::ModelSpec &spec, const xb4::SetupOptions &o
       }
     }
   }
-  if (m.drainResistance != 0 || m.sourceResistance != 0 || (m.g("RSH") && m.sheetResistance != 0))
-    return "MOSFET level 1 drain/source series resistance (internal nodes) is not supported";
   return std::string();
 }
 
@@ -223,6 +221,19 @@ std::string instance_record(const Card &m, InstParams ip, const xb4::SetupOption
     SourceSatCur = tSatCurDens * ip.sourceArea;
   }
   const double Beta = tTransconductance * ip.w / EffectiveLength;
+  // Series resistance (:1180-1220): RD / RS win over the sheet resistance; a conductance that is
+  // nonzero gives the instance an internal node.
+  double drainConductance = 0, sourceConductance = 0;
+  if (m.drainResistance != 0)
+    drainConductance = 1 / m.drainResistance;
+  else if (m.g("RSH") && m.sheetResistance != 0)
+    drainConductance = 1 / (m.sheetResistance * ip.drainSquares);
+  if (m.sourceResistance != 0)
+    sourceConductance = 1 / m.sourceResistance;
+  else if (m.g("RSH") && m.sheetResistance != 0)
+    sourceConductance = 1 / (m.sheetResistance * ip.sourceSquares);
+  if (!std::isfinite(drainConductance) || !std::isfinite(sourceConductance))
+    return "MOSFET level 1: RSH with NRD or NRS = 0 gives an infinite series conductance";
   rec.assign(kNumFields, 0.0);
 #define R(f) rec[f_##f]
   R(dtype) = m.dtype; R(gamma) = m.gamma; R(lambda) = m.lambda; R(mj) = MJ; R(mjsw) = MJSW; R(vt) = vt;
@@ -231,7 +242,8 @@ std::string instance_record(const Card &m, InstParams ip, const xb4::SetupOption
   R(Cbs) = czbs; R(Cbssw) = czbssw; R(tDepCap) = tDepCap; R(tBulkPot) = tBulkPot; R(f2d) = f2d; R(f3d) = f3d;
   R(f4d) = f4d; R(f2s) = f2s; R(f3s) = f3s; R(f4s) = f4s; R(GateSourceOverlapCap) = GateSourceOverlapCap;
   R(GateDrainOverlapCap) = GateDrainOverlapCap; R(GateBulkOverlapCap) = GateBulkOverlapCap; R(OxideCap) = OxideCap;
-  R(mult) = ip.mult; R(off) = ip.off;
+  R(mult) = ip.mult; R(off) = ip.off; R(drainConductance) = drainConductance;
+  R(sourceConductance) = sourceConductance;
 #undef R
   return std::string();
 }

@@ -74,8 +74,9 @@ def eval_shape(lib, h):
     import ctypes
 
     blk, minb = ctypes.c_int(), ctypes.c_int()
-    lib.xd_eval_variant_info(lib.xd_get_eval_variant(h), ctypes.byref(blk), ctypes.byref(minb))
-    return {"block": blk.value, "min_blocks_per_sm": minb.value}
+    v = lib.xd_get_eval_variant(h)
+    lib.xd_eval_variant_info(v, ctypes.byref(blk), ctypes.byref(minb))
+    return {"block": blk.value, "min_blocks_per_sm": minb.value, "persistent": lib.xd_eval_variant_persistent(v) == 1}
 
 
 def batched_section(args, dev_id):

@@ -189,6 +189,9 @@ int xd_eval_launch_shape(const xd_ctx *ctx, int *block, int *min_blocks);
  * others for it. */
 int xd_num_eval_variants(void);
 int xd_eval_variant_info(int v, int *block, int *min_blocks);
+/* 1 when candidate v is a persistent shape (one wave of resident blocks walking the instances with
+ * a grid stride), 0 when it launches one block per `block` instances, < 0 for a bad v. */
+int xd_eval_variant_persistent(int v);
 int xd_get_eval_variant(const xd_ctx *ctx);
 int xd_set_eval_variant(xd_ctx *ctx, int v);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);

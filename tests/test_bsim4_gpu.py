@@ -65,7 +65,7 @@ def _num_variants():
     return _native.load().xd_num_eval_variants()
 
 
-@pytest.mark.parametrize("v", range(8))
+@pytest.mark.parametrize("v", [0, 1, 2, 3, 4, 5, 6, 7, 10, 11])
 def test_parity_every_eval_launch_variant(v):
     """The autotuner may pick any launch shape of the evaluation kernel; each is held to the
     oracle, with an instance count that leaves a partial last block."""
@@ -145,7 +145,8 @@ def test_gate_tunnelling_family_refuses_variants_without_it():
     for v in range(lib.xd_num_eval_variants()):
         ok.append(lib.xd_set_eval_variant(dev._h, v) == 0)
     dev.close()
-    assert ok == [False] * 6 + [True] * 2 + [False] * 2  # the last two are for internal nodes
+    # 6, 7 and 11 are the full ones; 8, 9 are for internal nodes; 10 is a persistent common one.
+    assert ok == [False] * 6 + [True] * 2 + [False] * 2 + [False] + [True]
 
 
 @pytest.mark.parametrize("variant", ["all", "mixed"])
@@ -206,3 +207,32 @@ def test_unsupported_card_is_refused():
     from xyce_b200._native import NativeError
     with pytest.raises(NativeError, match="rgateMod"):
         Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
+
+
+def test_persistent_eval_variants_walk_every_instance():
+    """The persistent launch shapes run one wave of resident blocks over more instances than the
+    wave holds (a grid-stride loop with a partial last stride); their loads equal the one-block-
+    per-128-instances shape bit for bit."""
+    from xyce_b200 import _native
+
+    lib = _native.load()
+    c = netlist.random_logic(100000, seed=8)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c)
+    n = im.shape[0]
+    assert n > 148 * 4 * 128
+    sol = np.random.default_rng(3).uniform(0, 1.2, c.n_unknowns)
+    sto = np.random.default_rng(4).uniform(-0.2, 1.2, 14 * n)
+    z3 = np.zeros(3 * n)
+    outs = {}
+    for v in [2] + [v for v in range(lib.xd_num_eval_variants()) if lib.xd_eval_variant_persistent(v) == 1]:
+        dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
+        assert dev._lib.xd_set_eval_variant(dev._h, v) == 0
+        gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
+        outs[v] = gpu.load(SolverFlags(newton_iter=1), sol, z3, z3, sto.copy(), sto.copy())
+        dev.close()
+    assert len(outs) == 3
+    for v, out in outs.items():
+        for k in out:
+            if k != "abs":
+                assert np.array_equal(out[k], outs[2][k], equal_nan=True), (v, k)

@@ -99,20 +99,20 @@ struct xd_ctx {
   bool series = false;
   int2 *d_ext = nullptr;
   int vec_rows = 4, mat_slots = xb4::kNumMat, stage_slots = xb4::kNumStage;
+  int resident_blocks[16] = {};  // per persistent launch shape: blocks resident on the whole device
 };
 
 namespace {
 
-// SERIES: the family has internal drain / source nodes; ext holds the external drain and source
-// of each instance and the staging layout is the wide one (6 vector rows, 22 matrix slots).
-template <int BLOCK, int MINB, bool FULL, bool SERIES>
-__global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
-    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
-    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
-    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
-    double *__restrict__ stage, xb4::LoadFlags fl, const int2 *__restrict__ ext) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// One instance's evaluation and staging. SERIES: the family has internal drain / source nodes; ext
+// holds the external drain and source of each instance and the staging layout is the wide one
+// (6 vector rows, 22 matrix slots).
+template <bool FULL, bool SERIES>
+__device__ __forceinline__ void bsim4_eval_one(
+    int i, int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec,
+    const int4 *__restrict__ nodes, const double *__restrict__ sol, double *__restrict__ next_sta,
+    double *__restrict__ curr_sta, double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    double *__restrict__ vgb, double *__restrict__ stage, const xb4::LoadFlags &fl, const int2 *__restrict__ ext) {
   const int4 nd = nodes[i];
   double V[4];
   V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
@@ -169,6 +169,29 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
     for (int k = 0; k < xb4::kNumState; ++k) curr_sta[(size_t)k * n + i] = o.sta[k];
   }
   vgb[i] = o.vgb;
+}
+
+// One thread per instance. PERSIST: the grid is one wave of resident blocks that walks the
+// instances with a grid stride, so the warps resident on an SM start together and run through the
+// model's long straight-line code at about the same point, sharing its instruction-cache lines
+// (a grid of one block per 128 instances refills an SM as blocks finish, which leaves the resident
+// blocks a fraction of the code apart).
+template <int BLOCK, int MINB, bool FULL, bool SERIES, bool PERSIST = false>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
+    double *__restrict__ stage, xb4::LoadFlags fl, const int2 *__restrict__ ext) {
+  if (PERSIST) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      bsim4_eval_one<FULL, SERIES>(i, n, tab, nrec, rec, nodes, sol, next_sta, curr_sta, next_sto, curr_sto, vgb,
+                                   stage, fl, ext);
+  } else {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+      bsim4_eval_one<FULL, SERIES>(i, n, tab, nrec, rec, nodes, sol, next_sta, curr_sta, next_sto, curr_sto, vgb,
+                                   stage, fl, ext);
+  }
 }
 
 // MOSFET level 1: one thread per instance; reads the previous time point's Meyer state for
@@ -517,13 +540,15 @@ __global__ void __launch_bounds__(128) bsim3_eval_kernel(
 
 struct EvalVariant {
   int block, min_blocks;
-  bool full;    // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
-  bool series;  // internal drain / source nodes, wide staging layout
+  bool full;     // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
+  bool series;   // internal drain / source nodes, wide staging layout
+  bool persist;  // one wave of resident blocks with a grid-stride loop
 };
 constexpr EvalVariant kEvalVariants[] = {
-    {128, 1, false, false}, {128, 2, false, false}, {128, 3, false, false}, {128, 4, false, false},
-    {64, 4, false, false},  {256, 2, false, false}, {128, 2, true, false},  {128, 3, true, false},
-    {128, 2, true, true},   {128, 3, true, true}};
+    {128, 1, false, false, false}, {128, 2, false, false, false}, {128, 3, false, false, false},
+    {128, 4, false, false, false}, {64, 4, false, false, false},  {256, 2, false, false, false},
+    {128, 2, true, false, false},  {128, 3, true, false, false},  {128, 2, true, true, false},
+    {128, 3, true, true, false},   {128, 3, false, false, true},  {128, 3, true, false, true}};
 constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8;
 // A variant computes a context's loads exactly if its staging layout is the context's and it is a
 // full one or the context's cards use only the common options.
@@ -531,6 +556,33 @@ bool variant_fits(const xd_ctx *ctx, int v) {
   return kEvalVariants[v].series == ctx->series && (kEvalVariants[v].full || !ctx->needs_full);
 }
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
+static_assert(kNumEvalVariants <= 16, "resident_blocks holds 16 launch shapes");
+
+// The persistent launch shapes' kernels (for the occupancy query).
+const void *persistent_eval_kernel(int v) {
+  switch (v) {
+    case 10: return (const void *)bsim4_eval_kernel<128, 3, false, false, true>;
+    case 11: return (const void *)bsim4_eval_kernel<128, 3, true, false, true>;
+    default: return nullptr;
+  }
+}
+
+// One wave of each persistent shape: resident blocks per SM (the occupancy calculator) x SMs.
+int size_persistent_grids(xd_ctx *ctx) {
+  int sms = 0;
+  cudaError_t ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  if (ce != cudaSuccess) return cuda_fail(ce, "multiprocessor count query");
+  for (int v = 0; v < kNumEvalVariants; ++v) {
+    if (!kEvalVariants[v].persist) continue;
+    int per_sm = 0;
+    const void *fn = persistent_eval_kernel(v);
+    if (!fn) return fail(-3, "persistent launch shape without a kernel");
+    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kEvalVariants[v].block, 0);
+    if (ce != cudaSuccess) return cuda_fail(ce, "occupancy query");
+    ctx->resident_blocks[v] = std::max(1, per_sm) * std::max(1, sms);
+  }
+  return 0;
+}
 
 void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const double *sol, double *next_sta,
                  double *curr_sta, double *next_sto, const double *curr_sto, double *stage, cudaStream_t st) {
@@ -558,7 +610,8 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
     return;
   }
   const int blk = kEvalVariants[v].block;
-  const int grid = (n + blk - 1) / blk;
+  int grid = (n + blk - 1) / blk;
+  if (kEvalVariants[v].persist) grid = std::max(1, std::min(grid, ctx->resident_blocks[v]));
 #define XD_EVAL_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
                      ctx->d_vgb, stage, fl, ctx->d_ext
   switch (v) {
@@ -571,7 +624,9 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
     case 6: bsim4_eval_kernel<128, 2, true, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
     case 7: bsim4_eval_kernel<128, 3, true, false><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
     case 8: bsim4_eval_kernel<128, 2, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    default: bsim4_eval_kernel<128, 3, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 9: bsim4_eval_kernel<128, 3, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 10: bsim4_eval_kernel<128, 3, false, false, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    default: bsim4_eval_kernel<128, 3, true, false, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
   }
 #undef XD_EVAL_ARGS
 }
@@ -909,6 +964,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
   if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
+  if ((rc = size_persistent_grids(ctx)) != 0) return cleanup(rc);
   if ((rc = autotune_eval(ctx, ctx->eval_variant)) != 0) return cleanup(rc);
   *out = ctx;
   return 0;
@@ -1027,6 +1083,11 @@ int xd_eval_variant_info(int v, int *block, int *min_blocks) {
   *block = kEvalVariants[v].block;
   *min_blocks = kEvalVariants[v].min_blocks;
   return 0;
+}
+
+int xd_eval_variant_persistent(int v) {
+  if (v < 0 || v >= kNumEvalVariants) return fail(-1, "bad variant query");
+  return kEvalVariants[v].persist ? 1 : 0;
 }
 
 int xd_get_eval_variant(const xd_ctx *ctx) { return ctx ? ctx->eval_variant : -1; }

@@ -34,8 +34,17 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
  * that, makes a new host factorization). */
 int xd_rf_refactor(xd_rf *rf, const double *d_vals_a);
 
-/* Solves A x = b in place: d_x holds b on entry and x on return (device, length n). */
+/* Solves A x = b in place: d_x holds b on entry and x on return (device, length n). The forward
+ * and back substitutions are the library's own kernels (one thread block walking the factors'
+ * dependency levels, deterministic sums), ordered on the legacy default stream. */
 int xd_rf_solve(xd_rf *rf, double *d_x);
+
+/* The same solve through the refactorization library's own triangular solve (for comparison). */
+int xd_rf_solve_library(xd_rf *rf, double *d_x);
+
+/* Dependency levels of the lower and upper factors: the number of sequential steps of each
+ * substitution, which bounds the solve's latency. */
+int xd_rf_levels(const xd_rf *rf, int *levels_l, int *levels_u);
 
 int xd_rf_destroy(xd_rf *rf);
 

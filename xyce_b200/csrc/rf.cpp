@@ -4,7 +4,8 @@
 // factorization P A Q = L U on the host (its pivot order and fill pattern), every later matrix is
 // refactored and solved on the GPU with that pattern (cuSOLVER's refactorization library), and
 // the values never leave the device. This is the library linear solve of the transient driver,
-// not part of the device-load path.
+// not part of the device-load path. The refactorization is cuSOLVER's; the triangular solves are
+// the library's own kernels (sptrsv.cu) on cuSOLVER's bundled factors.
 #include <cuda_runtime.h>
 #include <cusolverRf.h>
 
@@ -12,6 +13,7 @@
 #include <vector>
 
 #include "../../include/xyce_rf.h"
+#include "sptrsv.h"
 
 int xd_internal_fail(int code, const std::string &msg);
 
@@ -21,6 +23,7 @@ struct xd_rf {
   int *d_rowptr = nullptr, *d_colind = nullptr, *d_p = nullptr, *d_q = nullptr;
   double *d_temp = nullptr;
   cusolverRfHandle_t h = nullptr;
+  XdSptrsv tri;
 };
 
 namespace {
@@ -37,6 +40,7 @@ int cu_fail(cudaError_t e, const char *where) {
 void release(xd_rf *r) {
   if (!r) return;
   if (r->h) cusolverRfDestroy(r->h);
+  xd_sptrsv_free(&r->tri);
   cudaFree(r->d_rowptr);
   cudaFree(r->d_colind);
   cudaFree(r->d_p);
@@ -107,6 +111,15 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
     release(r);
     return rf_fail(st, "cusolverRf configuration");
   }
+  // Refactorization algorithm 2 and triangular-solve algorithm 3 (both must precede the analysis):
+  // on the 200k-unknown placed netlist (2M factor entries, ~2,900 dependency levels in each of L
+  // and U) they take 14.9 and 18.8 ms on a B200 against 48.3 and 72.2 ms for the defaults (0, 1),
+  // with the same backward error (5e-14).
+  if ((st = cusolverRfSetAlgs(r->h, CUSOLVERRF_FACTORIZATION_ALG2, CUSOLVERRF_TRIANGULAR_SOLVE_ALG3)) !=
+      CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfSetAlgs");
+  }
   // The set-up reads host copies; the library's signature is not const-qualified.
   std::vector<int> ra(rowptr_a, rowptr_a + n + 1), ca(colind_a, colind_a + nnz_a);
   std::vector<int> rl(rowptr_l, rowptr_l + n + 1), cl(colind_l, colind_l + nnz_l);
@@ -128,6 +141,17 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
     release(r);
     return rf_fail(st, "cusolverRfRefactor");
   }
+  int nnz_m = 0, *mp = nullptr, *mi = nullptr;
+  double *mx = nullptr;
+  if ((st = cusolverRfAccessBundledFactorsDevice(r->h, &nnz_m, &mp, &mi, &mx)) != CUSOLVER_STATUS_SUCCESS) {
+    release(r);
+    return rf_fail(st, "cusolverRfAccessBundledFactorsDevice");
+  }
+  int rc = xd_sptrsv_init(&r->tri, n, nnz_m, mp, mi, p, q);
+  if (rc != 0) {
+    release(r);
+    return rc;
+  }
   *out = r;
   return 0;
 }
@@ -144,6 +168,23 @@ int xd_rf_refactor(xd_rf *r, const double *d_vals_a) {
 }
 
 int xd_rf_solve(xd_rf *r, double *d_x) {
+  if (!r || !d_x) return xd_internal_fail(-1, "null refactorization argument");
+  cudaSetDevice(r->device);
+  int nnz_m = 0, *mp = nullptr, *mi = nullptr;
+  double *mx = nullptr;
+  cusolverStatus_t st = cusolverRfAccessBundledFactorsDevice(r->h, &nnz_m, &mp, &mi, &mx);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfAccessBundledFactorsDevice");
+  return xd_sptrsv_solve(&r->tri, mx, d_x, 0);
+}
+
+int xd_rf_levels(const xd_rf *r, int *levels_l, int *levels_u) {
+  if (!r || !levels_l || !levels_u) return xd_internal_fail(-1, "null refactorization argument");
+  *levels_l = r->tri.nlev[0];
+  *levels_u = r->tri.nlev[1];
+  return 0;
+}
+
+int xd_rf_solve_library(xd_rf *r, double *d_x) {
   if (!r || !d_x) return xd_internal_fail(-1, "null refactorization argument");
   cudaSetDevice(r->device);
   cusolverStatus_t st = cusolverRfSolve(r->h, r->d_p, r->d_q, 1, r->d_temp, r->n, d_x, r->n);

@@ -223,6 +223,9 @@ def transient_section(args):
     from xyce_b200.transient import GpuTransient, NewtonParams
 
     out = {}
+    if args.placed_only:
+        out["placed_netlist"] = placed_transient(args)
+        return out
     # BSIM3 ring oscillator: operating point, 0.1 V kick on node 1, 0-20 ns at 10 ps steps.
     c = netlist.inverter_ring(101, vdd=1.8)
     rowptr, colind = netlist.jacobian_pattern(c)
@@ -309,6 +312,8 @@ def parse():
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     ap.add_argument("--placed-mos", type=int, default=100_000, help="MOSFETs of the placed-netlist transient (0: skip)")
     ap.add_argument("--placed-ns", type=float, default=1.0, help="length of the placed-netlist transient (ns)")
+    ap.add_argument("--placed-only", action="store_true",
+                    help="transient section: only the placed-netlist transient (for profiling its solve)")
     return ap.parse_args()
 
 

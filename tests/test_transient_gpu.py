@@ -197,3 +197,67 @@ def test_small_dense_solve_matches_numpy():
     v = T(np.ones(n))
     assert lib.xd_tia_dense_solve(h, p(v), p(v), None, None, p(v), None, None) < 0
     lib.xd_tia_destroy(h)
+
+
+def test_static_pivot_small_solve_matches_numpy_and_falls_back():
+    """The static-pivot solve (xd_slu_*): pivot order and fill from one matrix, later matrices of
+    the same pattern solved without a pivot search, against numpy; factors kept for a chord solve;
+    a matrix whose pivot fails the 1e-3 threshold test stops it (info = step + 1) and the pivoting
+    solve queued behind it gives the right answer."""
+    from xyce_b200 import _native
+
+    lib = _native.load()
+    rng = np.random.default_rng(11)
+    T = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    for n, density in ((7, 0.5), (33, 0.1), (103, 0.03), (160, 0.02)):
+        A = np.where(rng.random((n, n)) < density, rng.standard_normal((n, n)), 0.0)
+        A[np.arange(n), np.arange(n)] += np.where(rng.random(n) < 0.2, 0.0, 3.0)
+        A[np.arange(n), (np.arange(n) + 1) % n] += 1.0
+        A[0, 0] = 2.0  # column 0 holds at least two entries (this and row n - 1's), for the fallback case
+        mask = (A != 0) | np.eye(n, dtype=bool)
+        rows, cols = np.nonzero(mask)
+        rowptr = np.zeros(n + 1, np.int32)
+        np.add.at(rowptr, rows + 1, 1)
+        rowptr = np.cumsum(rowptr).astype(np.int32)
+        colind = cols.astype(np.int32)
+        csr = _native.XdCsr(n, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
+        tia, slu = ctypes.c_void_p(), ctypes.c_void_p()
+        assert lib.xd_tia_create(ctypes.byref(csr), 0, ctypes.byref(tia)) == 0
+        v0 = np.ascontiguousarray(A[rows, cols])
+        assert lib.xd_slu_create(n, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip),
+                                 v0.ctypes.data_as(_native._dp), 1e-3, 0, ctypes.byref(slu)) == 0
+        lu, piv, x, info = T(np.zeros(n * n)), T(np.zeros(n), torch.int32), T(np.zeros(n)), T([7], torch.int32)
+        for k in range(3):
+            Ak = np.where(mask, A * (1 + 0.05 * rng.standard_normal((n, n))), 0.0)
+            b = T(rng.standard_normal(n))
+            assert lib.xd_slu_solve(slu, p(T(Ak[rows, cols])), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+            torch.cuda.synchronize()
+            assert int(info.item()) == 0, (n, k)
+            ref = np.linalg.solve(Ak, b.cpu().numpy())
+            assert np.abs(x.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-10, (n, k)
+            b2, x2 = T(rng.standard_normal(n)), T(np.zeros(n))
+            assert lib.xd_tia_dense_resolve(tia, p(lu), p(piv), p(b2), p(x2), None) == 0
+            torch.cuda.synchronize()
+            ref2 = np.linalg.solve(Ak, b2.cpu().numpy())
+            assert np.abs(x2.cpu().numpy() - ref2).max() / np.abs(ref2).max() < 1e-10, (n, k)
+        # The first step's pivot row made tiny: the static order fails at step 0, the fallback solves.
+        A1 = A.copy()
+        A1[np.argmax(np.abs(A[:, 0])), 0] = 1e-9
+        b = T(rng.standard_normal(n))
+        vals1 = T(A1[rows, cols])
+        assert lib.xd_slu_solve(slu, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+        torch.cuda.synchronize()
+        assert int(info.item()) == 1, n
+        assert lib.xd_tia_dense_solve_fallback(tia, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+        torch.cuda.synchronize()
+        assert int(info.item()) == 0
+        ref = np.linalg.solve(A1, b.cpu().numpy())
+        assert np.abs(x.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-9, n
+        # With info 0 on entry the fallback does nothing.
+        x.fill_(123.0)
+        assert lib.xd_tia_dense_solve_fallback(tia, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+        torch.cuda.synchronize()
+        assert float(x[0].item()) == 123.0
+        lib.xd_slu_destroy(slu)
+        lib.xd_tia_destroy(tia)

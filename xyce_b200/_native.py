@@ -105,6 +105,11 @@ SIGNATURES = {
     "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
     "xd_tia_dense_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
     "xd_tia_dense_resolve": (ctypes.c_int, [ctypes.c_void_p] * 6),
+    "xd_tia_dense_solve_fallback": (ctypes.c_int, [ctypes.c_void_p] * 8),
+    "xd_slu_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_slu_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
+    "xd_slu_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_gemm_bf16": (ctypes.c_int, [ctypes.POINTER(XdGemmArgs), ctypes.c_int, ctypes.c_void_p]),
     "xd_mlp_input_layer": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

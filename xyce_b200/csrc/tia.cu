@@ -10,7 +10,11 @@
 // linear devices' F and Q use a fixed shuffle tree, so the results do not vary between runs.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/xyce_tia.h"
 
@@ -22,6 +26,15 @@ struct xd_tia {
   int nnz = 0;
   int *d_rowptr = nullptr;
   int *d_colind = nullptr;
+};
+
+struct xd_slu {
+  int device = 0;
+  int n = 0;
+  double tol = 1e-3;
+  int *d_buf = nullptr;  // all index arrays, one allocation
+  int off[12] = {};      // offsets in d_buf: rowptr, colind, pos, lptr, lidx, uptr, uidx, cptr, cidx, pivseq
+  int nsched = 0;        // entries of lptr .. cidx
 };
 
 namespace {
@@ -198,10 +211,12 @@ __device__ __forceinline__ void dense_forward_backward(int n, int lda, double *A
   }
 }
 
+// gate (may be null): solve only when *gate is nonzero (a static-pivot solve before it failed).
 __global__ void __launch_bounds__(kDenseThreads) dense_factor_solve_kernel(
     int n, const int *__restrict__ rowptr, const int *__restrict__ colind, const double *__restrict__ vals,
     const double *__restrict__ rhs, double *__restrict__ lu, int *__restrict__ piv, double *__restrict__ x,
-    int *__restrict__ info) {
+    int *info, const int *gate) {
+  if (gate && *gate == 0) return;
   extern __shared__ double A[];
   __shared__ int spiv[XD_DENSE_MAX_N];
   __shared__ double sinv[XD_DENSE_MAX_N];
@@ -269,6 +284,98 @@ __global__ void __launch_bounds__(32) dense_resolve_kernel(int n, const double *
 }
 
 size_t dense_smem_bytes(int n) { return sizeof(double) * (size_t)n * (size_t)(n + 1); }
+
+// Static-pivot refactorization of a small system (n <= XD_DENSE_MAX_N). The row order and the
+// fill pattern come from one host factorization with partial pivoting (xd_slu_create); each
+// Newton matrix is then eliminated in that order over the pattern alone: step k scales the
+// multipliers of the rows that have an entry in column k and updates only the (row, column) pairs
+// of the pattern, the right-hand side carried along as column n. A pivot smaller than tol times an
+// entry below it (the threshold test of circuit solvers such as KLU) stops the solve with info =
+// k + 1, and the pivoting kernel redoes it (xd_tia_dense_solve_fallback). One warp, shared memory,
+// __syncwarp between steps: a few hundred cycles a step where the pivot search costs thousands.
+struct SluArgs {
+  int n;
+  double tol;
+  const int *rowptr, *colind;  // the system's CSR pattern
+  const int *pos;              // [n] position of each row in the pivot order
+  const int *lptr, *lidx;      // per step k: rows below k with an entry in column k
+  const int *uptr, *uidx;      // per step k: columns right of k with an entry in row k
+  const int *cptr, *cidx;      // per column k: rows above k with an entry in column k (back substitution)
+  const int *pivseq;           // the order as LAPACK row swaps (row k swapped with pivseq[k] at step k)
+  int nsched;                  // entries of the six schedule arrays (lptr .. cidx) copied to shared memory
+                               // (0: too many beside the matrix, read from global memory)
+  const int *sched;            // lptr, lidx, uptr, uidx, cptr, cidx back to back
+};
+
+__global__ void __launch_bounds__(32) slu_kernel(SluArgs a, const double *__restrict__ vals,
+                                                 const double *__restrict__ rhs, double *__restrict__ lu,
+                                                 int *__restrict__ piv, double *__restrict__ x, int *info) {
+  extern __shared__ double M[];
+  __shared__ double sinv[XD_DENSE_MAX_N];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x, n = a.n, lda = n + 1;
+  // The schedule moves to shared memory first (each launch starts with cold caches; read from
+  // global memory, every step would wait on a chain of dependent loads).
+  int *ss = reinterpret_cast<int *>(M + (size_t)n * lda);
+  for (int idx = lane; idx < a.nsched; idx += 32) ss[idx] = a.sched[idx];
+  for (int idx = lane; idx < n * lda; idx += 32) M[idx] = 0.0;
+  __syncwarp();
+  if (a.nsched > 0) {
+    a.lidx = ss + (a.lidx - a.sched);
+    a.uptr = ss + (a.uptr - a.sched);
+    a.uidx = ss + (a.uidx - a.sched);
+    a.cptr = ss + (a.cptr - a.sched);
+    a.cidx = ss + (a.cidx - a.sched);
+    a.lptr = ss;
+  }
+  for (int r = lane; r < n; r += 32) {
+    double *row = M + a.pos[r] * lda;
+    for (int k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) row[a.colind[k]] = vals[k];
+    row[n] = rhs[r];
+  }
+  __syncwarp();
+  for (int k = 0; k < n; ++k) {
+    const double pv = M[k * lda + k];
+    const int lb = a.lptr[k], le = a.lptr[k + 1], ub = a.uptr[k], nu = a.uptr[k + 1] - ub + 1;
+    bool ok = fabs(pv) > 0.0;
+    for (int t = lb + lane; t < le; t += 32) ok = ok && (fabs(M[a.lidx[t] * lda + k]) * a.tol <= fabs(pv));
+    if (!__all_sync(full, ok)) {
+      if (lane == 0) *info = k + 1;
+      return;
+    }
+    const double inv = 1.0 / pv;
+    if (lane == 0) sinv[k] = inv;
+    for (int t = lb + lane; t < le; t += 32) M[a.lidx[t] * lda + k] *= inv;
+    __syncwarp();
+    const int tot = (le - lb) * nu;
+    for (int t = lane; t < tot; t += 32) {
+      const int q = t / nu, c = t - q * nu;
+      const int i = a.lidx[lb + q], j = c < nu - 1 ? a.uidx[ub + c] : n;
+      M[i * lda + j] = M[i * lda + j] - M[i * lda + k] * M[k * lda + j];
+    }
+    __syncwarp();
+  }
+  // Back substitution on U, column by column; column n becomes x.
+  for (int k = n - 1; k >= 0; --k) {
+    if (lane == 0) M[k * lda + n] = M[k * lda + n] * sinv[k];
+    __syncwarp();
+    const double xk = M[k * lda + n];
+    for (int t = a.cptr[k] + lane; t < a.cptr[k + 1]; t += 32) {
+      const int i = a.cidx[t];
+      M[i * lda + n] = M[i * lda + n] - M[i * lda + k] * xk;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) x[i] = M[i * lda + n];
+  if (lu) {
+    for (int idx = lane; idx < n * n; idx += 32) {
+      const int r = idx / n, c = idx - r * n;
+      lu[idx] = M[r * lda + c];
+    }
+    for (int k = lane; k < n; k += 32) piv[k] = a.pivseq[k];
+  }
+  if (lane == 0) *info = 0;
+}
 
 struct Guard {
   int prev = -1;
@@ -371,7 +478,7 @@ int xd_tia_dense_solve(xd_tia *t, const double *d_jac, const double *d_rhs, doub
   if (!d_jac || !d_rhs || !d_x) return xd_internal_fail(-1, "null device buffer");
   Guard g(t->device);
   dense_factor_solve_kernel<<<1, kDenseThreads, dense_smem_bytes(t->n_rows), (cudaStream_t)stream>>>(
-      t->n_rows, t->d_rowptr, t->d_colind, d_jac, d_rhs, d_lu, d_piv, d_x, d_info);
+      t->n_rows, t->d_rowptr, t->d_colind, d_jac, d_rhs, d_lu, d_piv, d_x, d_info, nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "dense_factor_solve_kernel launch");
   return 0;
@@ -388,6 +495,149 @@ int xd_tia_dense_resolve(xd_tia *t, const double *d_lu, const int *d_piv, const 
   dense_resolve_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(t->n_rows, d_lu, d_piv, d_rhs, d_x);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "dense_resolve_kernel launch");
+  return 0;
+}
+
+int xd_tia_dense_solve_fallback(xd_tia *t, const double *d_jac, const double *d_rhs, double *d_lu, int *d_piv,
+                                double *d_x, int *d_info, void *stream) {
+  if (!t || !d_info) return xd_internal_fail(-1, "null argument");
+  if (t->n_rows == 0) return 0;
+  if (t->n_rows > XD_DENSE_MAX_N)
+    return xd_internal_fail(-1, "the dense solve takes at most " + std::to_string(XD_DENSE_MAX_N) + " unknowns");
+  if (!d_jac || !d_rhs || !d_x) return xd_internal_fail(-1, "null device buffer");
+  Guard g(t->device);
+  dense_factor_solve_kernel<<<1, kDenseThreads, dense_smem_bytes(t->n_rows), (cudaStream_t)stream>>>(
+      t->n_rows, t->d_rowptr, t->d_colind, d_jac, d_rhs, d_lu, d_piv, d_x, d_info, d_info);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "dense_factor_solve_kernel launch");
+  return 0;
+}
+
+int xd_slu_create(int n, const int *rowptr, const int *colind, const double *vals, double tol, int cuda_device,
+                  xd_slu **out) {
+  if (!out || !rowptr || n <= 0 || n > XD_DENSE_MAX_N || !(tol > 0.0 && tol <= 1.0))
+    return xd_internal_fail(-1, "bad static-pivot solve arguments (n must be 1.." + std::to_string(XD_DENSE_MAX_N) +
+                                    ", 0 < tol <= 1)");
+  *out = nullptr;
+  const int nnz = rowptr[n];
+  if (rowptr[0] != 0 || nnz < 0 || (nnz > 0 && (!colind || !vals))) return xd_internal_fail(-1, "bad CSR pattern");
+  for (int r = 0; r < n; ++r)
+    if (rowptr[r + 1] < rowptr[r]) return xd_internal_fail(-1, "bad CSR pattern");
+  for (int k = 0; k < nnz; ++k)
+    if (colind[k] < 0 || colind[k] >= n) return xd_internal_fail(-1, "bad CSR pattern");
+  // Host factorization with partial pivoting (first row of largest magnitude), tracking the
+  // pattern: the row order and the fill of every later matrix with this pattern.
+  std::vector<double> A((size_t)n * n, 0.0);
+  std::vector<char> S((size_t)n * n, 0);
+  for (int r = 0; r < n; ++r)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+      A[(size_t)r * n + colind[k]] = vals[k];
+      S[(size_t)r * n + colind[k]] = 1;
+    }
+  std::vector<int> rowof(n);
+  for (int i = 0; i < n; ++i) rowof[i] = i;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = std::fabs(A[(size_t)k * n + k]);
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(A[(size_t)i * n + k]) > best) {
+        best = std::fabs(A[(size_t)i * n + k]);
+        p = i;
+      }
+    if (!(best > 0.0)) return xd_internal_fail(-2, "the matrix for the static pivot order is singular");
+    if (p != k) {
+      for (int j = 0; j < n; ++j) {
+        std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
+        std::swap(S[(size_t)k * n + j], S[(size_t)p * n + j]);
+      }
+      std::swap(rowof[k], rowof[p]);
+    }
+    for (int i = k + 1; i < n; ++i) {
+      if (!S[(size_t)i * n + k]) continue;
+      const double l = A[(size_t)i * n + k] / A[(size_t)k * n + k];
+      for (int j = k + 1; j < n; ++j)
+        if (S[(size_t)k * n + j]) {
+          A[(size_t)i * n + j] -= l * A[(size_t)k * n + j];
+          S[(size_t)i * n + j] = 1;
+        }
+    }
+  }
+  std::vector<int> pos(n), lptr(n + 1, 0), lidx, uptr(n + 1, 0), uidx, cptr(n + 1, 0), cidx, pivseq(n);
+  for (int i = 0; i < n; ++i) pos[rowof[i]] = i;
+  for (int k = 0; k < n; ++k) {
+    for (int i = k + 1; i < n; ++i)
+      if (S[(size_t)i * n + k]) lidx.push_back(i);
+    lptr[k + 1] = (int)lidx.size();
+    for (int j = k + 1; j < n; ++j)
+      if (S[(size_t)k * n + j]) uidx.push_back(j);
+    uptr[k + 1] = (int)uidx.size();
+    for (int i = 0; i < k; ++i)
+      if (S[(size_t)i * n + k]) cidx.push_back(i);
+    cptr[k + 1] = (int)cidx.size();
+  }
+  std::vector<int> cur(n);  // original row at each position while applying the swaps
+  for (int i = 0; i < n; ++i) cur[i] = i;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    while (cur[p] != rowof[k]) ++p;
+    std::swap(cur[k], cur[p]);
+    pivseq[k] = p;
+  }
+  const std::vector<int> *parts[10] = {nullptr, nullptr, &pos, &lptr, &lidx, &uptr, &uidx, &cptr, &cidx, &pivseq};
+  std::vector<int> rp(rowptr, rowptr + n + 1), ci(colind, colind + nnz);
+  parts[0] = &rp;
+  parts[1] = &ci;
+  // Parts 3..8 (the schedule) are contiguous in that order; the kernel copies them to shared
+  // memory behind the matrix when they fit there.
+  size_t nsched = 0;
+  for (int q = 3; q <= 8; ++q) nsched += parts[q]->size();
+  if (dense_smem_bytes(n) + sizeof(int) * nsched + sizeof(double) * XD_DENSE_MAX_N > 227 * 1024) nsched = 0;
+  xd_slu *h = new xd_slu();
+  h->device = cuda_device;
+  h->n = n;
+  h->tol = tol;
+  h->nsched = (int)nsched;
+  std::vector<int> all;
+  for (int q = 0; q < 10; ++q) {
+    h->off[q] = (int)all.size();
+    all.insert(all.end(), parts[q]->begin(), parts[q]->end());
+  }
+  Guard g(cuda_device);
+  cudaError_t e;
+  if ((e = cudaMalloc(&h->d_buf, sizeof(int) * std::max<size_t>(1, all.size()))) != cudaSuccess ||
+      (e = cudaMemcpy(h->d_buf, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (dense_smem_bytes(n) + sizeof(int) * nsched > 48 * 1024 &&
+       (e = cudaFuncSetAttribute(slu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(dense_smem_bytes(n) + sizeof(int) * nsched))) != cudaSuccess)) {
+    cudaFree(h->d_buf);
+    delete h;
+    return cuda_err(e, "xd_slu_create");
+  }
+  *out = h;
+  return 0;
+}
+
+int xd_slu_solve(xd_slu *s, const double *d_vals, const double *d_rhs, double *d_lu, int *d_piv, double *d_x,
+                 int *d_info, void *stream) {
+  if (!s || !d_vals || !d_rhs || !d_x || !d_info || ((d_lu == nullptr) != (d_piv == nullptr)))
+    return xd_internal_fail(-1, "null argument");
+  Guard g(s->device);
+  const int *b = s->d_buf;
+  SluArgs a{s->n,           s->tol,           b + s->off[0], b + s->off[1], b + s->off[2], b + s->off[3],
+            b + s->off[4], b + s->off[5],    b + s->off[6], b + s->off[7], b + s->off[8], b + s->off[9],
+            s->nsched,     b + s->off[3]};
+  slu_kernel<<<1, 32, dense_smem_bytes(s->n) + sizeof(int) * s->nsched, (cudaStream_t)stream>>>(
+      a, d_vals, d_rhs, d_lu, d_piv, d_x, d_info);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "slu_kernel launch");
+  return 0;
+}
+
+int xd_slu_destroy(xd_slu *s) {
+  if (!s) return 0;
+  Guard g(s->device);
+  cudaFree(s->d_buf);
+  delete s;
   return 0;
 }
 

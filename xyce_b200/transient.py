@@ -138,6 +138,7 @@ class StepStats:
     factorizations: int = 0
     host_factorizations: int = 0
     surrogate_loads: int = 0
+    static_pivot_fallbacks: int = 0
     chord_iters: list = field(default_factory=list)
     surrogate_error: list = field(default_factory=list)
 
@@ -501,7 +502,7 @@ class GpuTransient(TransientBase):
     """
 
     def __init__(self, c, family: MosfetDevice, rowptr, colind, device=0, solver="auto", gmin=1e-12,
-                 graphs=True):
+                 graphs=True, static_pivot=True):
         import torch
 
         super().__init__(c, family.n_state, family.n_store, rowptr, colind, torch.device("cuda", device), solver,
@@ -527,12 +528,23 @@ class GpuTransient(TransientBase):
             self._lu_d = z(self.nu * self.nu)
             self._piv_d = torch.zeros(self.nu, dtype=torch.int32, device=self.dev)
             self._dx_d = z(self.nu)
+        # Small systems: static-pivot refactorization (xd_slu_*) with the pivoting solve queued
+        # behind it for the matrices whose pivots fail its threshold test; the order is taken from
+        # a host factorization of the first matrix and taken again after a fallback.
+        self.static_pivot = bool(static_pivot) and self._small
+        self._slu = None
+        self._slu_stale = False
+        self._info_d = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self._fallback_d = torch.zeros(1, dtype=torch.int32, device=self.dev)
         # Family outputs (stored by xd_load_assign; entries the family does not stamp stay zero).
         self.f, self.q, self.fx, self.qx = z(self.nu), z(self.nu), z(self.nu), z(self.nu)
         self.jf, self.jq = z(self.nnz), z(self.nnz)
 
     def close(self):
         self._graphs = {}
+        if getattr(self, "_slu", None) is not None and self._slu.value:
+            self._lib.xd_slu_destroy(self._slu)
+            self._slu = None
         if getattr(self, "_tia", None) is not None and self._tia.value:
             self._lib.xd_tia_destroy(self._tia)
             self._tia = None
@@ -689,12 +701,15 @@ class GpuTransient(TransientBase):
         wrms = torch.sqrt(torch.mean((dx / self._g_w) ** 2))
         self._load_raw(flags1)
         self._combine(mode, h, order, qn0, fhist)
-        self._g_norms.copy_(torch.stack([wrms, self.rhs.abs().max()]))
+        self._g_norms.copy_(torch.stack([wrms, self.rhs.abs().max(), self._fallback_d[0].to(torch.float64)]))
         self._g_host.copy_(self._g_norms, non_blocking=True)
         return "small" if self._small else (LU, piv)
 
     def _graph_for(self, prm, flags1, mode, h, order, qn0, fhist):
         torch = self.torch
+        # The static-pivot set-up reads the current matrix on the host (never while capturing); a new
+        # order drops the graphs that launch the old one's kernels.
+        self._slu_ready()
         key = (mode, h, order, self.gshunt, self.limiting, prm.rel_tol, prm.abs_tol, prm.update_weights_each_iter,
                tuple(sorted(vars(flags1).items())), self._ptr(qn0).value if qn0 is not None else 0,
                self._ptr(fhist).value if fhist is not None else 0)
@@ -703,8 +718,8 @@ class GpuTransient(TransientBase):
             return g
         if not hasattr(self, "_g_host"):
             z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
-            self._g_xref, self._g_w, self._g_norms = z(self.nu), z(self.nu), z(2)
-            self._g_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+            self._g_xref, self._g_w, self._g_norms = z(self.nu), z(self.nu), z(3)
+            self._g_host = torch.zeros(3, dtype=torch.float64, pin_memory=True)
             if not self._small:
                 # Library handles and workspaces come into being outside any capture.
                 eye = torch.eye(self.nu, dtype=torch.float64, device=self.dev)
@@ -723,6 +738,7 @@ class GpuTransient(TransientBase):
         return self._graphs[key]
 
     def _newton(self, prm: NewtonParams, flags_for_iter, mode, h=None, order=1, qn0=None, fhist=None):
+        self._first_solve = True
         if not self.graphs:
             return super()._newton(prm, flags_for_iter, mode, h, order, qn0, fhist)
         f1, f2 = flags_for_iter(1), flags_for_iter(2)
@@ -730,11 +746,11 @@ class GpuTransient(TransientBase):
         if f1 != f2:  # the iterations' flags differ beyond newton_iter >= 1: no single graph
             return super()._newton(prm, flags_for_iter, mode, h, order, qn0, fhist)
         torch = self.torch
-        graph, lu = self._graph_for(prm, f1, mode, h, order, qn0, fhist)
-        self._g_xref.copy_(self.x)
-        self._g_w.copy_(prm.rel_tol * self._g_xref.abs() + prm.abs_tol)
         self._load(flags_for_iter(0))
         self._combine(mode, h, order, qn0, fhist)
+        graph, lu = self._graph_for(prm, f1, mode, h, order, qn0, fhist)  # loads and combine leave x as it was
+        self._g_xref.copy_(self.x)
+        self._g_w.copy_(prm.rel_tol * self._g_xref.abs() + prm.abs_tol)
         stream = torch.cuda.current_stream(self.dev)
         for it in range(1, prm.max_iter + 1):
             graph.replay()
@@ -743,14 +759,53 @@ class GpuTransient(TransientBase):
             self.stats.loads += 1
             stream.synchronize()
             wrms, max_rhs = float(self._g_host[0]), float(self._g_host[1])
+            if self._g_host[2] != 0:
+                self._note_fallback()
             if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
                 return -1
             if max_rhs <= prm.rhs_tol and wrms <= prm.delta_x_tol:
                 return it
         return -1
 
+    def _slu_ready(self, renew=True):
+        """The static-pivot solve's order and pattern, taken from the current matrix when there is
+        none, or (renew) again when one failed a pivot since; False when the matrix is singular (that
+        solve then uses the pivoting kernel alone). Orders are renewed only at the first solve of a
+        Newton solve, in the eager and the graph-replayed iterations alike, so that both use the
+        same orders. Host work: never called while a graph is captured."""
+        if not self.static_pivot:
+            return False
+        if self._slu is not None and not (self._slu_stale and renew):
+            return True
+        if self._slu is not None:
+            self._lib.xd_slu_destroy(self._slu)
+            self._slu = None
+            self._graphs = {}  # they launch the old order's kernels
+        vals = np.ascontiguousarray(self.jac.cpu().numpy())
+        h = ctypes.c_void_p()
+        rc = self._lib.xd_slu_create(self.nu, self.rowptr.ctypes.data_as(_native._ip),
+                                     self.colind.ctypes.data_as(_native._ip), vals.ctypes.data_as(_native._dp),
+                                     1e-3, self.dev.index or 0, ctypes.byref(h))
+        self._slu_stale = False
+        if rc != 0:
+            return False
+        self._slu = h
+        return True
+
+    def _note_fallback(self):
+        self.stats.static_pivot_fallbacks += 1
+        self._slu_stale = True
+
     def _dense_solve(self, out):
         p = self._ptr
+        if self._slu is not None:
+            _native.check(self._lib.xd_slu_solve(self._slu, p(self.jac), p(self.rhs), p(self._lu_d), p(self._piv_d),
+                                                 p(out), p(self._info_d), self._stream()), "xd_slu_solve")
+            self._fallback_d.copy_(self._info_d)
+            _native.check(self._lib.xd_tia_dense_solve_fallback(self._tia, p(self.jac), p(self.rhs), p(self._lu_d),
+                                                                p(self._piv_d), p(out), p(self._info_d),
+                                                                self._stream()), "xd_tia_dense_solve_fallback")
+            return
         _native.check(self._lib.xd_tia_dense_solve(self._tia, p(self.jac), p(self.rhs), p(self._lu_d),
                                                    p(self._piv_d), p(out), None, self._stream()),
                       "xd_tia_dense_solve")
@@ -758,7 +813,11 @@ class GpuTransient(TransientBase):
     def _solve(self):
         if not self._small:
             return super()._solve()
+        self._slu_ready(renew=getattr(self, "_first_solve", True))
+        self._first_solve = False
         self._dense_solve(self._dx_d)
+        if self._slu is not None and int(self._fallback_d.item()) != 0:
+            self._note_fallback()
         self._lu = "small"
         self.stats.factorizations += 1
         return self._dx_d.clone()

@@ -82,6 +82,16 @@ int xd_tia_dense_resolve(xd_tia *t, const double *d_lu, const int *d_piv, const 
 int xd_tia_dense_solve_fallback(xd_tia *t, const double *d_jac, const double *d_rhs, double *d_lu, int *d_piv,
                                 double *d_x, int *d_info, void *stream);
 
+/* Newton's bookkeeping on the device (N_NLS_DampedNewton.C:325-350, 1792-1830), one block each:
+ * xd_tia_newton_update adds the update d_dx to d_x, refreshes the weights d_w = rel_tol *
+ * max(|d_xref|, |d_x|) + abs_tol when update_weights is set, and writes the update's weighted RMS
+ * norm sqrt(mean((dx / w)^2)) to d_norms[0]; xd_tia_residual_norm writes max |d_rhs| to d_norms[1]
+ * (NaN when an entry is not finite) and *d_flag (0 when d_flag is null) to d_norms[2]. Fixed
+ * reduction order: the same inputs give the same norms. */
+int xd_tia_newton_update(xd_tia *t, double *d_x, const double *d_dx, const double *d_xref, double *d_w,
+                         double rel_tol, double abs_tol, int update_weights, double *d_norms, void *stream);
+int xd_tia_residual_norm(xd_tia *t, const double *d_rhs, const int *d_flag, double *d_norms, void *stream);
+
 /* Static-pivot solve of small systems (n <= XD_DENSE_MAX_N) whose matrices share one pattern, as
  * the Newton matrices of a transient do: xd_slu_create factors one matrix on the host with partial
  * pivoting and keeps its row order and fill pattern; xd_slu_solve eliminates each later matrix in

@@ -106,6 +106,9 @@ SIGNATURES = {
     "xd_tia_dense_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
     "xd_tia_dense_resolve": (ctypes.c_int, [ctypes.c_void_p] * 6),
     "xd_tia_dense_solve_fallback": (ctypes.c_int, [ctypes.c_void_p] * 8),
+    "xd_tia_newton_update": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                                    ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_tia_residual_norm": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "xd_slu_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_void_p)]),
     "xd_slu_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),

@@ -285,6 +285,80 @@ __global__ void __launch_bounds__(32) dense_resolve_kernel(int n, const double *
 
 size_t dense_smem_bytes(int n) { return sizeof(double) * (size_t)n * (size_t)(n + 1); }
 
+// Newton's bookkeeping between a solve and the next load, one block: x += dx; the update weights
+// (when refreshed) rel * max(|x_ref|, |x|) + abs; norms[0] = sqrt(mean((dx / w)^2)), the weighted
+// RMS norm of the update (N_NLS_DampedNewton.C's convergence test, :325-350, 1792-1830). Then,
+// after the load, norms[1] = max |rhs| (not finite if any entry is not) and norms[2] = *flag.
+// Sums and maxima use a fixed reduction tree: the same inputs give the same norms.
+constexpr int kNormThreads = 1024;
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+  if (warp == 0) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kNormThreads) newton_update_kernel(int n, double *__restrict__ x,
+                                                                     const double *__restrict__ dx,
+                                                                     const double *__restrict__ xref,
+                                                                     double *__restrict__ w, double rel, double abs_,
+                                                                     int update_w, double *__restrict__ norms) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += kNormThreads) {
+    const double xi = x[i] + dx[i];
+    x[i] = xi;
+    double wi;
+    if (update_w) {
+      wi = rel * fmax(fabs(xref[i]), fabs(xi)) + abs_;
+      w[i] = wi;
+    } else {
+      wi = w[i];
+    }
+    const double q = dx[i] / wi;
+    s += q * q;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) norms[0] = sqrt(s / (double)n);
+}
+
+__global__ void __launch_bounds__(kNormThreads) residual_norm_kernel(int n, const double *__restrict__ rhs,
+                                                                     const int *__restrict__ flag,
+                                                                     double *__restrict__ norms) {
+  __shared__ double red[32];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += kNormThreads) {
+    const double a = fabs(rhs[i]);
+    if (!isfinite(a)) bad = 1;
+    m = fmax(m, a);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if (lane == 0) red[warp] = m;
+  __syncthreads();
+  if (warp == 0) {
+    m = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) {
+      norms[1] = bad ? __longlong_as_double(0x7ff8000000000000LL) : m;
+      norms[2] = flag ? (double)*flag : 0.0;
+    }
+  }
+}
+
 // Static-pivot refactorization of a small system (n <= XD_DENSE_MAX_N). The row order and the
 // fill pattern come from one host factorization with partial pivoting (xd_slu_create); each
 // Newton matrix is then eliminated in that order over the pattern alone: step k scales the
@@ -510,6 +584,28 @@ int xd_tia_dense_solve_fallback(xd_tia *t, const double *d_jac, const double *d_
       t->n_rows, t->d_rowptr, t->d_colind, d_jac, d_rhs, d_lu, d_piv, d_x, d_info, d_info);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "dense_factor_solve_kernel launch");
+  return 0;
+}
+
+int xd_tia_newton_update(xd_tia *t, double *d_x, const double *d_dx, const double *d_xref, double *d_w, double rel_tol,
+                         double abs_tol, int update_weights, double *d_norms, void *stream) {
+  if (!t || !d_x || !d_dx || !d_w || !d_norms || (update_weights && !d_xref)) return xd_internal_fail(-1, "null argument");
+  if (t->n_rows == 0) return 0;
+  Guard g(t->device);
+  newton_update_kernel<<<1, kNormThreads, 0, (cudaStream_t)stream>>>(t->n_rows, d_x, d_dx, d_xref, d_w, rel_tol, abs_tol,
+                                                                     update_weights, d_norms);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "newton_update_kernel launch");
+  return 0;
+}
+
+int xd_tia_residual_norm(xd_tia *t, const double *d_rhs, const int *d_flag, double *d_norms, void *stream) {
+  if (!t || !d_rhs || !d_norms) return xd_internal_fail(-1, "null argument");
+  if (t->n_rows == 0) return 0;
+  Guard g(t->device);
+  residual_norm_kernel<<<1, kNormThreads, 0, (cudaStream_t)stream>>>(t->n_rows, d_rhs, d_flag, d_norms);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "residual_norm_kernel launch");
   return 0;
 }
 

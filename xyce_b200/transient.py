@@ -324,18 +324,27 @@ class TransientBase:
         self._combine(mode, h, order, qn0, fhist)
         for it in range(1, prm.max_iter + 1):
             dx = self._solve()
-            self.x += dx
-            if prm.update_weights_each_iter:
-                w = prm.rel_tol * torch.maximum(x_ref.abs(), self.x.abs()) + prm.abs_tol
-            wrms = float(torch.sqrt(torch.mean((dx / w) ** 2)))
+            w, wrms = self._update(dx, x_ref, w, prm)
             self._load(flags_for_iter(it))
             self._combine(mode, h, order, qn0, fhist)
-            max_rhs = float(self.rhs.abs().max())
+            max_rhs = self._residual_max()
             if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
                 return -1
             if max_rhs <= prm.rhs_tol and wrms <= prm.delta_x_tol:
                 return it
         return -1
+
+    def _update(self, dx, x_ref, w, prm):
+        """x += dx; the weights (refreshed when the parameters say so) and the update's weighted
+        RMS norm."""
+        torch = self.torch
+        self.x += dx
+        if prm.update_weights_each_iter:
+            w = prm.rel_tol * torch.maximum(x_ref.abs(), self.x.abs()) + prm.abs_tol
+        return w, float(torch.sqrt(torch.mean((dx / w) ** 2)))
+
+    def _residual_max(self):
+        return float(self.rhs.abs().max())
 
     def _history_here(self):
         """Q and F at the current point (after a load there) into q_tot / f_tot."""
@@ -536,6 +545,7 @@ class GpuTransient(TransientBase):
         self._slu_stale = False
         self._info_d = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self._fallback_d = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self._e_norms = z(3)  # the eager iterations' norms (the graph-replayed ones use their own)
         # Family outputs (stored by xd_load_assign; entries the family does not stamp stay zero).
         self.f, self.q, self.fx, self.qx = z(self.nu), z(self.nu), z(self.nu), z(self.nu)
         self.jf, self.jq = z(self.nnz), z(self.nnz)
@@ -695,13 +705,10 @@ class GpuTransient(TransientBase):
             self._dense[self._flat] = self.jac
             LU, piv, _ = torch.linalg.lu_factor_ex(self._dense.view(self.nu, self.nu))
             dx = torch.linalg.lu_solve(LU, piv, self.rhs.view(-1, 1)).view(-1)
-        self.x += dx
-        if prm.update_weights_each_iter:
-            self._g_w.copy_(prm.rel_tol * torch.maximum(self._g_xref.abs(), self.x.abs()) + prm.abs_tol)
-        wrms = torch.sqrt(torch.mean((dx / self._g_w) ** 2))
+        self._device_update(dx, self._g_xref, self._g_w, prm, self._g_norms)
         self._load_raw(flags1)
         self._combine(mode, h, order, qn0, fhist)
-        self._g_norms.copy_(torch.stack([wrms, self.rhs.abs().max(), self._fallback_d[0].to(torch.float64)]))
+        self._device_residual_norm(self._g_norms)
         self._g_host.copy_(self._g_norms, non_blocking=True)
         return "small" if self._small else (LU, piv)
 
@@ -766,6 +773,30 @@ class GpuTransient(TransientBase):
             if max_rhs <= prm.rhs_tol and wrms <= prm.delta_x_tol:
                 return it
         return -1
+
+    def _device_update(self, dx, x_ref, w, prm, norms):
+        p = self._ptr
+        _native.check(self._lib.xd_tia_newton_update(self._tia, p(self.x), p(dx.contiguous()), p(x_ref), p(w),
+                                                     prm.rel_tol, prm.abs_tol, int(prm.update_weights_each_iter),
+                                                     p(norms), self._stream()), "xd_tia_newton_update")
+
+    def _device_residual_norm(self, norms):
+        p = self._ptr
+        _native.check(self._lib.xd_tia_residual_norm(self._tia, p(self.rhs), p(self._fallback_d), p(norms),
+                                                     self._stream()), "xd_tia_residual_norm")
+
+    def _update(self, dx, x_ref, w, prm):
+        if not self.graphs and not self._small:
+            return super()._update(dx, x_ref, w, prm)
+        w = w.clone()  # written in place when the weights are refreshed
+        self._device_update(dx, x_ref, w, prm, self._e_norms)
+        return w, float(self._e_norms[0].item())
+
+    def _residual_max(self):
+        if not self.graphs and not self._small:
+            return super()._residual_max()
+        self._device_residual_norm(self._e_norms)
+        return float(self._e_norms[1].item())
 
     def _slu_ready(self, renew=True):
         """The static-pivot solve's order and pattern, taken from the current matrix when there is

@@ -41,9 +41,9 @@ UNIT = "loads/s"
 # 12 store (96), 3 state (24), vgb (8).
 EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
 # DRAM bytes per instance of one evaluation launch (dram__bytes_read.sum + dram__bytes_write.sum
-# of an ncu capture at 199,832 instances of the same generator, 90 + 333 B; traffic grows with
+# of an ncu capture at 199,832 instances of the same generator, 90 + 326 B; traffic grows with
 # the instance count), for roofline.traffic.
-EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 333
+EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 326
 # FP64 operations per instance of one evaluation (ncu thread-instruction counters of the same
 # capture: 2,621 DFMA (2 flops each) + 844 DMUL + 511 DADD per instance), for the evaluation
 # kernel's compute roofline against the FP64 FMA-pipe probe.
@@ -194,6 +194,15 @@ def placed_transient(args):
         g._lib.xd_rf_solve(g._rf, ctypes.c_void_p(x.data_ptr()))
     torch.cuda.synchronize()
     solve_ms = (time.perf_counter() - t) * 1e3 / 3
+    x = g.rhs.clone()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(3):
+        g._lib.xd_rf_solve_library(g._rf, ctypes.c_void_p(x.data_ptr()))
+    torch.cuda.synchronize()
+    solve_lib_ms = (time.perf_counter() - t) * 1e3 / 3
+    lev_l, lev_u = ctypes.c_int(), ctypes.c_int()
+    g._lib.xd_rf_levels(g._rf, ctypes.byref(lev_l), ctypes.byref(lev_u))
     res = {"workload": f"seeded INV/NAND2/NOR2 netlist with placed wiring (fan-out U{{1..4}}, a pin takes one of "
                        f"the 64 most recent open slots), {c.n_mos} BSIM4 MOSFETs, {c.res_nodes.shape[0]} R + "
                        f"{c.cap_nodes.shape[0]} C wire parasitics, 64 PWL inputs, {c.n_unknowns} unknowns, "
@@ -205,7 +214,9 @@ def placed_transient(args):
            "ms_per_newton_iteration": run_s * 1e3 / max(1, its),
            "matrices": st.factorizations - f0, "host_factorizations": st.host_factorizations - h0,
            "per_iteration_ms": {"device_loads_and_combine": ev[0].elapsed_time(ev[1]) / 5,
-                                "refactorization": min(ref_ms), "triangular_solves": solve_ms},
+                                "refactorization": min(ref_ms), "triangular_solves": solve_ms,
+                                "triangular_solves_cusolver": solve_lib_ms},
+           "factor_levels": [lev_l.value, lev_u.value],
            "swing_v": [float(w.min()), float(w.max())]}
     g.close()
     fam.close()

@@ -514,6 +514,11 @@ class GpuTransient(TransientBase):
                  graphs=True, static_pivot=True):
         import torch
 
+        if solver == "auto":
+            # Up to XD_DENSE_MAX_N unknowns the one-SM solves; above, the sparse refactorization
+            # (on the 1,228-MOSFET gate netlist, 2,534 unknowns, 0.22 s for 1 ns against 1.65 s with
+            # a dense LU of every Newton matrix).
+            solver = "dense" if c.n_unknowns <= _native.XD_DENSE_MAX_N else "rf"
         super().__init__(c, family.n_state, family.n_store, rowptr, colind, torch.device("cuda", device), solver,
                          gmin)
         self.fam = family

@@ -108,3 +108,35 @@ def test_internal_node_query_mos1():
     assert (flags[:, 1] == ~nmos).all()
     none = internal_nodes(NMOS_PMOS, c.mos_type, c.mos_nodes, params, level=1)
     assert not none.any()
+
+
+def test_static_pivot_setup_refuses_bad_systems():
+    """xd_slu_create checks its arguments and factors on the host before touching a GPU: sizes
+    outside 1..XD_DENSE_MAX_N, a bad threshold, a malformed pattern and a singular matrix are
+    refused with an error."""
+    import ctypes
+
+    from xyce_b200 import _native
+
+    lib = _native.load()
+
+    def create(n, rowptr, colind, vals, tol=1e-3):
+        rp = np.ascontiguousarray(rowptr, np.int32)
+        ci = np.ascontiguousarray(colind, np.int32)
+        v = np.ascontiguousarray(vals, np.float64)
+        h = ctypes.c_void_p()
+        rc = lib.xd_slu_create(n, rp.ctypes.data_as(_native._ip), ci.ctypes.data_as(_native._ip),
+                               v.ctypes.data_as(_native._dp), tol, 0, ctypes.byref(h))
+        return rc, lib.xd_last_error().decode()
+
+    eye = lambda n: (np.arange(n + 1), np.arange(n), np.ones(n))
+    n = _native.XD_DENSE_MAX_N + 1
+    rc, msg = create(n, *eye(n))
+    assert rc < 0 and "n must be" in msg
+    rc, msg = create(4, *eye(4), tol=0.0)
+    assert rc < 0 and "tol" in msg
+    rc, msg = create(2, [0, 1, 2], [0, 5], [1.0, 1.0])
+    assert rc < 0 and "CSR" in msg
+    # Two identical rows: singular.
+    rc, msg = create(2, [0, 2, 4], [0, 1, 0, 1], [1.0, 2.0, 1.0, 2.0])
+    assert rc == -2 and "singular" in msg

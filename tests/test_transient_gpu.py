@@ -261,3 +261,45 @@ def test_static_pivot_small_solve_matches_numpy_and_falls_back():
         assert float(x[0].item()) == 123.0
         lib.xd_slu_destroy(slu)
         lib.xd_tia_destroy(tia)
+
+
+def test_newton_update_and_residual_norm_kernels():
+    """xd_tia_newton_update / xd_tia_residual_norm against numpy: the update, refreshed and kept
+    weights, the weighted RMS norm, the residual's max norm, a non-finite residual reported as NaN
+    and the flag passed through."""
+    from xyce_b200 import _native
+
+    lib = _native.load()
+    rng = np.random.default_rng(5)
+    T = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    for n in (1, 103, 5000):
+        rowptr = np.arange(n + 1, dtype=np.int32)
+        colind = np.arange(n, dtype=np.int32)
+        csr = _native.XdCsr(n, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
+        h = ctypes.c_void_p()
+        assert lib.xd_tia_create(ctypes.byref(csr), 0, ctypes.byref(h)) == 0
+        x, dx, xref = rng.standard_normal(n), rng.standard_normal(n) * 1e-3, rng.standard_normal(n)
+        w0 = 1e-3 * np.abs(xref) + 1e-6
+        for upd in (0, 1):
+            dx_, xref_ = T(dx), T(xref)
+            xd, wd, norms = T(x), T(w0), T(np.zeros(3))
+            assert lib.xd_tia_newton_update(h, p(xd), p(dx_), p(xref_), p(wd), 1e-3, 1e-6, upd, p(norms), None) == 0
+            torch.cuda.synchronize()
+            xn = x + dx
+            wn = 1e-3 * np.maximum(np.abs(xref), np.abs(xn)) + 1e-6 if upd else w0
+            assert np.array_equal(xd.cpu().numpy(), xn)
+            assert np.array_equal(wd.cpu().numpy(), wn)
+            ref = np.sqrt(np.mean((dx / wn) ** 2))
+            assert abs(float(norms[0]) - ref) <= 1e-13 * ref
+        rhs = rng.standard_normal(n)
+        flag = T([3], torch.int32)
+        norms = T(np.zeros(3))
+        assert lib.xd_tia_residual_norm(h, p(T(rhs)), p(flag), p(norms), None) == 0
+        torch.cuda.synchronize()
+        assert float(norms[1]) == np.abs(rhs).max() and float(norms[2]) == 3.0
+        rhs[n // 2] = np.nan
+        assert lib.xd_tia_residual_norm(h, p(T(rhs)), None, p(norms), None) == 0
+        torch.cuda.synchronize()
+        assert np.isnan(float(norms[1])) and float(norms[2]) == 0.0
+        lib.xd_tia_destroy(h)

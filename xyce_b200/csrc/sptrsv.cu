@@ -37,13 +37,13 @@ namespace {
 // levels of short rows are solved a thread per row, so they do not need many.
 constexpr int kThreads = XD_SPTRSV_THREADS;
 constexpr int kWarps = kThreads / 32;
-constexpr int kAhead = 3;               // levels staged ahead of the one being solved
+constexpr int kAhead = 2;               // levels staged ahead of the one being solved
 constexpr int kSlots = kAhead + 1;      // staging slots (a level uses slot level % kSlots)
 constexpr int kSlotRows = 256;          // rows per staged level
 constexpr int kSlotEnts = 2048;         // entries per staged level
 constexpr int kWindow = 1 << 11;        // solved values kept in shared memory
 constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are summed by the whole block
-constexpr int kThreadRowEnts = 8;       // levels averaging at most this many entries a row: a thread a row
+constexpr int kThreadRowEnts = 4;       // levels averaging at most this many entries a row: a thread a row
 
 constexpr int kEntsPerThread = kSlotEnts / kThreads;
 static_assert(kSlotEnts % kThreads == 0, "a staged level's entries split evenly over the threads");

@@ -1,22 +1,24 @@
 // Forward and back substitution with the refactorization's factors (P A Q = L U, bundled by the
 // refactorization library as one CSR matrix M = L - I + U in the permuted index space).
 //
-// Circuit factors are deep and narrow: the 200k-unknown placed netlist's L and U have ~2,900
-// dependency levels each, a few dozen rows per level, 2M entries in all. The solve is bound by the
-// latency of a level, not by its arithmetic (4M flops) or bytes (24 MB), so each triangle runs in
-// ONE thread block that walks the levels with a block barrier between them (a few hundred cycles;
-// level-by-level launches or grid-wide waits cost microseconds). What keeps a level short is that
-// nothing on its critical path waits for global memory:
+// Circuit factors are deep and narrow: the 200k-unknown placed netlist's L and U have 2,300-4,100
+// dependency levels each, a few dozen rows per level (plus one level of ~85k independent rows in
+// L), 2M entries in all. The solve is bound by the latency of a level, not by its arithmetic (4M
+// flops) or bytes (24 MB), so each triangle runs in ONE thread block that walks the levels with a
+// block barrier between them (level-by-level launches, or grid-wide waits on per-row flags, cost
+// microseconds a level). What keeps a level short is that its rows read shared memory only:
 //   * the set-up renumbers each triangle's rows in level order and lays out, per level, the rows'
 //     entry ranges, the entries (column as a level-order position, value) and the right-hand side
 //     contiguously; a gather kernel refreshes the values and the right-hand side before each solve;
 //   * the block streams the next kAhead levels into shared memory with asynchronous copies
-//     (cp.async, one commit group per level) while it computes the current one;
+//     (cp.async, one commit group per level) while it computes the current one, together with the
+//     solved values their entries read that are already final (positions before the current level);
 //   * the last kWindow solved values stay in shared memory (slot = position mod kWindow; a value
 //     read during level l comes from there when its position is within kWindow of the level's
-//     end, so no row of level l can have reused the slot), older ones are read from global memory.
-// Levels with more rows or entries than a staging slot holds are read from global memory directly.
-// Every sum is reduced in a fixed order, so results do not depend on the timing.
+//     end, so no row of level l can have reused the slot), others are read from global memory.
+// Levels of short rows are solved a thread per row, others a warp per row; levels with more rows
+// or entries than a staging slot holds are read from global memory directly. Every sum is reduced
+// in a fixed order, so results do not depend on the timing.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -79,6 +79,52 @@ def eval_shape(lib, h):
     return {"block": blk.value, "min_blocks_per_sm": minb.value, "persistent": lib.xd_eval_variant_persistent(v) == 1}
 
 
+def other_families(c, rowptr, colind, sol, dev_id, args):
+    """Load throughput of the BSIM3 (level 9) and MOSFET1 (level 1) families on the same circuit and
+    iterate as the BSIM4 step (xd_load_assign, transient flags, limiting on), CUDA events around
+    10 steps after 3 warm-up steps. BSIM3 takes the ring oscillator's cards, MOSFET1 the defaults."""
+    import ctypes
+
+    import torch
+
+    from xyce_b200 import ModelCard, MosfetDevice, SolverFlags, _native, netlist
+
+    lib = _native.load()
+    out = {}
+    nu, nnz = c.n_unknowns, int(rowptr[-1])
+    f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
+    for name, level, cards in (("bsim3", 9, netlist.ring_bsim3_cards()),
+                               ("mosfet1", 1, [ModelCard(False, {}), ModelCard(True, {})])):
+        fam = MosfetDevice(cards, c.mos_type, c.mos_nodes, {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float)},
+                           (rowptr, colind), nu, device=dev_id, level=level)
+        sta = [torch.zeros(fam.n_state, **f64) for _ in range(2)]
+        sto = [torch.zeros(fam.n_store, **f64) for _ in range(2)]
+        bufs = [torch.zeros(nu, **f64) for _ in range(4)] + [torch.zeros(nnz, **f64) for _ in range(2)]
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        fam.load(SolverFlags(newton_iter=1, voltlim=0), sol, sta[0], sta[1], sto[0], sto[1], *bufs)
+
+        def step():
+            fl = SolverFlags(newton_iter=1).to_c()
+            _native.check(lib.xd_load_assign(fam._h, ctypes.byref(fl), p(sol), p(sta[0]), p(sta[1]), p(sto[0]),
+                                             p(sto[1]), *[p(b) for b in bufs],
+                                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                          "xd_load_assign")
+
+        for _ in range(3):
+            step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(10):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[name] = {"ms_per_step": ms, "loads_per_s": c.n_mos / (ms * 1e-3)}
+        fam.close()
+    return out
+
+
 def batched_section(args, dev_id):
     """The batched Monte-Carlo sweep: 256 circuits (sizes log-uniform 1k-20k MOSFETs, per-circuit
     DELVTO ~ N(0, 30 mV) and TOXE x U[0.98, 1.02]) merged into one block-diagonal system, every
@@ -665,6 +711,7 @@ def main():
     if cpu is not None:
         result["cpu_baseline"] = cpu
     if rank == 0 and world == 1 and not args.no_batched:
+        result["other_families"] = other_families(c, rowptr, colind, sol, dev_id, args)
         result["batched"] = batched_section(args, dev_id)
     if rank == 0 and world == 1 and not args.no_transient:
         from oracle import xyce_ref as xr

@@ -311,6 +311,8 @@ def transient_section(args):
                     "point + 0.1 V kick on node 1, 0-20 ns, 10 ps steps, reference transient Newton tolerances",
         "gpu_s_per_run": g_s, "cpu_oracle_s_per_run": c_s, "cpu_cores": 1,
         "gpu_newton_iters_per_step": float(np.mean(g_st.newton_iters)),
+        "gpu_ms_per_newton_iteration": g_s * 1e3 / max(1, int(sum(g_st.newton_iters))),
+        "gpu_static_pivot_fallbacks": g_st.static_pivot_fallbacks,
         "cpu_newton_iters_per_step": float(np.mean(c_st.newton_iters)), "steps": len(g_st.newton_iters),
         "node1_swing_v": [float(g_w[:, 0].min()), float(g_w[:, 0].max())]}
     fam.close()

@@ -93,19 +93,22 @@ int xd_tia_newton_update(xd_tia *t, double *d_x, const double *d_dx, const doubl
 int xd_tia_residual_norm(xd_tia *t, const double *d_rhs, const int *d_flag, double *d_norms, void *stream);
 
 /* Static-pivot solve of small systems (n <= XD_DENSE_MAX_N) whose matrices share one pattern, as
- * the Newton matrices of a transient do: xd_slu_create factors one matrix on the host with partial
- * pivoting and keeps its row order and fill pattern; xd_slu_solve eliminates each later matrix in
- * that order over the pattern alone (no pivot search), on one warp. A pivot smaller than tol times
- * an entry below it (the threshold test of circuit solvers; 1e-3 as KLU's default) stops the solve
- * with *d_info = k + 1 for step k and leaves d_x unwritten; xd_tia_dense_solve_fallback queued after
- * it then solves that system with partial pivoting, so the pair is one stream-ordered, capturable
- * solve. On success *d_info = 0, d_x holds the solution and, when d_lu / d_piv are given, the
- * factors in xd_tia_dense_solve's layout (for xd_tia_dense_resolve). */
+ * the Newton matrices of a transient do: xd_slu_create orders the unknowns by minimum degree of
+ * A + A^T (rows and columns alike), factors one matrix on the host in that order with row pivoting
+ * that keeps the diagonal unless it is below 0.1 of its column's largest entry, and keeps the
+ * orders and the fill pattern; xd_slu_solve eliminates each later matrix in those orders over the
+ * pattern alone (no pivot search), on one warp. A pivot smaller than tol times an entry below it
+ * (the threshold test of circuit solvers; 1e-3 as KLU's default) stops the solve with *d_info =
+ * k + 1 for step k and leaves d_x unwritten; xd_tia_dense_solve_fallback queued after it then
+ * solves that system with partial pivoting, so the pair is one stream-ordered, capturable solve.
+ * On success *d_info = 0, d_x holds the solution and, when d_lu is given (n * n doubles), the
+ * factors in the static orders, for xd_slu_resolve (a chord step). */
 typedef struct xd_slu xd_slu;
 int xd_slu_create(int n, const int *rowptr, const int *colind, const double *vals, double tol, int cuda_device,
                   xd_slu **out);
-int xd_slu_solve(xd_slu *s, const double *d_vals, const double *d_rhs, double *d_lu, int *d_piv, double *d_x,
-                 int *d_info, void *stream);
+int xd_slu_solve(xd_slu *s, const double *d_vals, const double *d_rhs, double *d_lu, double *d_x, int *d_info,
+                 void *stream);
+int xd_slu_resolve(xd_slu *s, const double *d_lu, const double *d_rhs, double *d_x, void *stream);
 int xd_slu_destroy(xd_slu *s);
 
 #ifdef __cplusplus

@@ -200,10 +200,10 @@ def test_small_dense_solve_matches_numpy():
 
 
 def test_static_pivot_small_solve_matches_numpy_and_falls_back():
-    """The static-pivot solve (xd_slu_*): pivot order and fill from one matrix, later matrices of
-    the same pattern solved without a pivot search, against numpy; factors kept for a chord solve;
-    a matrix whose pivot fails the 1e-3 threshold test stops it (info = step + 1) and the pivoting
-    solve queued behind it gives the right answer."""
+    """The static-pivot solve (xd_slu_*): orders and fill from one matrix, later matrices of the
+    same pattern solved without a pivot search, against numpy; factors kept for a chord solve
+    (xd_slu_resolve); a matrix whose pivots fail the 1e-3 threshold test stops it (info = step + 1)
+    and the pivoting solve queued behind it gives the right answer."""
     from xyce_b200 import _native
 
     lib = _native.load()
@@ -231,29 +231,37 @@ def test_static_pivot_small_solve_matches_numpy_and_falls_back():
         for k in range(3):
             Ak = np.where(mask, A * (1 + 0.05 * rng.standard_normal((n, n))), 0.0)
             b = T(rng.standard_normal(n))
-            assert lib.xd_slu_solve(slu, p(T(Ak[rows, cols])), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+            assert lib.xd_slu_solve(slu, p(T(Ak[rows, cols])), p(b), p(lu), p(x), p(info), None) == 0
             torch.cuda.synchronize()
             assert int(info.item()) == 0, (n, k)
             ref = np.linalg.solve(Ak, b.cpu().numpy())
             assert np.abs(x.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-10, (n, k)
             b2, x2 = T(rng.standard_normal(n)), T(np.zeros(n))
-            assert lib.xd_tia_dense_resolve(tia, p(lu), p(piv), p(b2), p(x2), None) == 0
+            assert lib.xd_slu_resolve(slu, p(lu), p(b2), p(x2), None) == 0
             torch.cuda.synchronize()
             ref2 = np.linalg.solve(Ak, b2.cpu().numpy())
             assert np.abs(x2.cpu().numpy() - ref2).max() / np.abs(ref2).max() < 1e-10, (n, k)
-        # The first step's pivot row made tiny: the static order fails at step 0, the fallback solves.
-        A1 = A.copy()
-        A1[np.argmax(np.abs(A[:, 0])), 0] = 1e-9
-        b = T(rng.standard_normal(n))
-        vals1 = T(A1[rows, cols])
-        assert lib.xd_slu_solve(slu, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
-        torch.cuda.synchronize()
-        assert int(info.item()) == 1, n
-        assert lib.xd_tia_dense_solve_fallback(tia, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
-        torch.cuda.synchronize()
-        assert int(info.item()) == 0
-        ref = np.linalg.solve(A1, b.cpu().numpy())
-        assert np.abs(x.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-9, n
+        # Entries rescaled by 10^U(-6, 6): some static pivot fails its threshold test (info > 0) and the
+        # pivoting solve queued behind it answers; every attempt's answer is checked.
+        failed = 0
+        for attempt in range(20):
+            A1 = np.where(mask, A * 10.0 ** rng.uniform(-6, 6, (n, n)), 0.0)
+            b = T(rng.standard_normal(n))
+            vals1 = T(A1[rows, cols])
+            assert lib.xd_slu_solve(slu, p(vals1), p(b), p(lu), p(x), p(info), None) == 0
+            assert lib.xd_tia_dense_solve_fallback(tia, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0
+            torch.cuda.synchronize()
+            xs, bs = x.cpu().numpy(), b.cpu().numpy()
+            berr = np.abs(A1 @ xs - bs).max() / (np.abs(A1).max() * np.abs(xs).max() + np.abs(bs).max())
+            assert berr < 1e-13, (n, attempt, berr)  # backward error: A1 may be badly conditioned
+            fb = T([0], torch.int32)
+            assert lib.xd_slu_solve(slu, p(vals1), p(b), None, p(x), p(fb), None) == 0
+            torch.cuda.synchronize()
+            failed += int(fb.item()) > 0
+            if failed:
+                break
+        assert failed, n
+        info.fill_(0)
         # With info 0 on entry the fallback does nothing.
         x.fill_(123.0)
         assert lib.xd_tia_dense_solve_fallback(tia, p(vals1), p(b), p(lu), p(piv), p(x), p(info), None) == 0

@@ -111,7 +111,8 @@ SIGNATURES = {
     "xd_tia_residual_norm": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "xd_slu_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_void_p)]),
-    "xd_slu_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
+    "xd_slu_solve": (ctypes.c_int, [ctypes.c_void_p] * 7),
+    "xd_slu_resolve": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "xd_slu_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_gemm_bf16": (ctypes.c_int, [ctypes.POINTER(XdGemmArgs), ctypes.c_int, ctypes.c_void_p]),
     "xd_mlp_input_layer": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,

@@ -33,7 +33,7 @@ struct xd_slu {
   int n = 0;
   double tol = 1e-3;
   int *d_buf = nullptr;  // all index arrays, one allocation
-  int off[12] = {};      // offsets in d_buf: rowptr, colind, pos, lptr, lidx, uptr, uidx, cptr, cidx, pivseq
+  int off[12] = {};      // offsets in d_buf: rowptr, colind, pos, lptr, lidx, uptr, uidx, cptr, cidx, cpos, cperm
   int nsched = 0;        // entries of lptr .. cidx
 };
 
@@ -359,8 +359,11 @@ __global__ void __launch_bounds__(kNormThreads) residual_norm_kernel(int n, cons
   }
 }
 
-// Static-pivot refactorization of a small system (n <= XD_DENSE_MAX_N). The row order and the
-// fill pattern come from one host factorization with partial pivoting (xd_slu_create); each
+// Static-pivot refactorization of a small system (n <= XD_DENSE_MAX_N). The orders and the fill
+// pattern come from one host factorization (xd_slu_create): a minimum-degree order of A + A^T
+// applied to rows and columns (a supply node's dense row and column go last instead of filling the
+// whole matrix: the ring oscillator's LU has 704 entries instead of 103^2), then row pivoting that
+// keeps the diagonal unless it is below 0.1 of its column's largest entry; each
 // Newton matrix is then eliminated in that order over the pattern alone: step k scales the
 // multipliers of the rows that have an entry in column k and updates only the (row, column) pairs
 // of the pattern, the right-hand side carried along as column n. A pivot smaller than tol times an
@@ -375,7 +378,8 @@ struct SluArgs {
   const int *lptr, *lidx;      // per step k: rows below k with an entry in column k
   const int *uptr, *uidx;      // per step k: columns right of k with an entry in row k
   const int *cptr, *cidx;      // per column k: rows above k with an entry in column k (back substitution)
-  const int *pivseq;           // the order as LAPACK row swaps (row k swapped with pivseq[k] at step k)
+  const int *cpos;             // [n] position of each column (unknown) in the elimination order
+  const int *cperm;            // [n] the unknown at each column position
   int nsched;                  // entries of the six schedule arrays (lptr .. cidx) copied to shared memory
                                // (0: too many beside the matrix, read from global memory)
   const int *sched;            // lptr, lidx, uptr, uidx, cptr, cidx back to back
@@ -383,7 +387,7 @@ struct SluArgs {
 
 __global__ void __launch_bounds__(32) slu_kernel(SluArgs a, const double *__restrict__ vals,
                                                  const double *__restrict__ rhs, double *__restrict__ lu,
-                                                 int *__restrict__ piv, double *__restrict__ x, int *info) {
+                                                 double *__restrict__ x, int *info) {
   extern __shared__ double M[];
   __shared__ double sinv[XD_DENSE_MAX_N];
   const unsigned full = 0xffffffffu;
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(32) slu_kernel(SluArgs a, const double *__rest
   }
   for (int r = lane; r < n; r += 32) {
     double *row = M + a.pos[r] * lda;
-    for (int k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) row[a.colind[k]] = vals[k];
+    for (int k = a.rowptr[r]; k < a.rowptr[r + 1]; ++k) row[a.cpos[a.colind[k]]] = vals[k];
     row[n] = rhs[r];
   }
   __syncwarp();
@@ -440,15 +444,44 @@ __global__ void __launch_bounds__(32) slu_kernel(SluArgs a, const double *__rest
     }
     __syncwarp();
   }
-  for (int i = lane; i < n; i += 32) x[i] = M[i * lda + n];
+  for (int j = lane; j < n; j += 32) x[a.cperm[j]] = M[j * lda + n];
   if (lu) {
     for (int idx = lane; idx < n * n; idx += 32) {
       const int r = idx / n, c = idx - r * n;
       lu[idx] = M[r * lda + c];
     }
-    for (int k = lane; k < n; k += 32) piv[k] = a.pivseq[k];
   }
   if (lane == 0) *info = 0;
+}
+
+// Solve with factors kept from slu_kernel (in its row and column orders): forward substitution
+// over the unit lower factor's pattern, back substitution over the upper one's, then the
+// unknowns back to their own order. One warp.
+__global__ void __launch_bounds__(32) slu_resolve_kernel(SluArgs a, const double *__restrict__ lu,
+                                                         const double *__restrict__ rhs, double *__restrict__ x) {
+  __shared__ double y[XD_DENSE_MAX_N];
+  const int lane = threadIdx.x, n = a.n;
+  for (int r = lane; r < n; r += 32) y[a.pos[r]] = rhs[r];
+  __syncwarp();
+  for (int k = 0; k < n; ++k) {
+    const double yk = y[k];
+    for (int t = a.lptr[k] + lane; t < a.lptr[k + 1]; t += 32) {
+      const int i = a.lidx[t];
+      y[i] = y[i] - lu[(size_t)i * n + k] * yk;
+    }
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    if (lane == 0) y[k] = y[k] * (1.0 / lu[(size_t)k * n + k]);
+    __syncwarp();
+    const double xk = y[k];
+    for (int t = a.cptr[k] + lane; t < a.cptr[k + 1]; t += 32) {
+      const int i = a.cidx[t];
+      y[i] = y[i] - lu[(size_t)i * n + k] * xk;
+    }
+    __syncwarp();
+  }
+  for (int j = lane; j < n; j += 32) x[a.cperm[j]] = y[j];
 }
 
 struct Guard {
@@ -621,17 +654,47 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
     if (rowptr[r + 1] < rowptr[r]) return xd_internal_fail(-1, "bad CSR pattern");
   for (int k = 0; k < nnz; ++k)
     if (colind[k] < 0 || colind[k] >= n) return xd_internal_fail(-1, "bad CSR pattern");
-  // Host factorization with partial pivoting (first row of largest magnitude), tracking the
-  // pattern: the row order and the fill of every later matrix with this pattern.
+  // Minimum-degree order of A + A^T (greedy; ties to the lowest index), applied to rows and
+  // columns: cperm[j] = the unknown eliminated j-th.
+  std::vector<char> G((size_t)n * n, 0), alive(n, 1);
+  for (int r = 0; r < n; ++r)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
+      if (colind[k] != r) G[(size_t)r * n + colind[k]] = G[(size_t)colind[k] * n + r] = 1;
+  std::vector<int> cperm(n), cpos(n);
+  for (int step = 0; step < n; ++step) {
+    int v = -1, best = n + 1;
+    for (int i = 0; i < n; ++i) {
+      if (!alive[i]) continue;
+      int d = 0;
+      for (int j = 0; j < n; ++j) d += (alive[j] && G[(size_t)i * n + j]) ? 1 : 0;
+      if (d < best) {
+        best = d;
+        v = i;
+      }
+    }
+    cperm[step] = v;
+    alive[v] = 0;
+    std::vector<int> nb;
+    for (int j = 0; j < n; ++j)
+      if (alive[j] && G[(size_t)v * n + j]) nb.push_back(j);
+    for (int p : nb)
+      for (int q : nb)
+        if (p != q) G[(size_t)p * n + q] = 1;
+  }
+  for (int j = 0; j < n; ++j) cpos[cperm[j]] = j;
+  // Host factorization in that order, tracking the pattern: row pivoting that keeps the diagonal
+  // unless it is below 0.1 of the column's largest entry (then the first largest), as circuit
+  // solvers pivot; the row order and the fill of every later matrix with this pattern.
   std::vector<double> A((size_t)n * n, 0.0);
   std::vector<char> S((size_t)n * n, 0);
   for (int r = 0; r < n; ++r)
     for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) {
-      A[(size_t)r * n + colind[k]] = vals[k];
-      S[(size_t)r * n + colind[k]] = 1;
+      const size_t at = (size_t)cpos[r] * n + cpos[colind[k]];
+      A[at] = vals[k];
+      S[at] = 1;
     }
-  std::vector<int> rowof(n);
-  for (int i = 0; i < n; ++i) rowof[i] = i;
+  std::vector<int> rowof(n);  // original row at each row position
+  for (int i = 0; i < n; ++i) rowof[i] = cperm[i];
   for (int k = 0; k < n; ++k) {
     int p = k;
     double best = std::fabs(A[(size_t)k * n + k]);
@@ -641,6 +704,7 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
         p = i;
       }
     if (!(best > 0.0)) return xd_internal_fail(-2, "the matrix for the static pivot order is singular");
+    if (std::fabs(A[(size_t)k * n + k]) >= 0.1 * best) p = k;
     if (p != k) {
       for (int j = 0; j < n; ++j) {
         std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
@@ -658,7 +722,7 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
         }
     }
   }
-  std::vector<int> pos(n), lptr(n + 1, 0), lidx, uptr(n + 1, 0), uidx, cptr(n + 1, 0), cidx, pivseq(n);
+  std::vector<int> pos(n), lptr(n + 1, 0), lidx, uptr(n + 1, 0), uidx, cptr(n + 1, 0), cidx;
   for (int i = 0; i < n; ++i) pos[rowof[i]] = i;
   for (int k = 0; k < n; ++k) {
     for (int i = k + 1; i < n; ++i)
@@ -671,15 +735,7 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
       if (S[(size_t)i * n + k]) cidx.push_back(i);
     cptr[k + 1] = (int)cidx.size();
   }
-  std::vector<int> cur(n);  // original row at each position while applying the swaps
-  for (int i = 0; i < n; ++i) cur[i] = i;
-  for (int k = 0; k < n; ++k) {
-    int p = k;
-    while (cur[p] != rowof[k]) ++p;
-    std::swap(cur[k], cur[p]);
-    pivseq[k] = p;
-  }
-  const std::vector<int> *parts[10] = {nullptr, nullptr, &pos, &lptr, &lidx, &uptr, &uidx, &cptr, &cidx, &pivseq};
+  const std::vector<int> *parts[11] = {nullptr, nullptr, &pos, &lptr, &lidx, &uptr, &uidx, &cptr, &cidx, &cpos, &cperm};
   std::vector<int> rp(rowptr, rowptr + n + 1), ci(colind, colind + nnz);
   parts[0] = &rp;
   parts[1] = &ci;
@@ -694,7 +750,7 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
   h->tol = tol;
   h->nsched = (int)nsched;
   std::vector<int> all;
-  for (int q = 0; q < 10; ++q) {
+  for (int q = 0; q < 11; ++q) {
     h->off[q] = (int)all.size();
     all.insert(all.end(), parts[q]->begin(), parts[q]->end());
   }
@@ -713,19 +769,30 @@ int xd_slu_create(int n, const int *rowptr, const int *colind, const double *val
   return 0;
 }
 
-int xd_slu_solve(xd_slu *s, const double *d_vals, const double *d_rhs, double *d_lu, int *d_piv, double *d_x,
-                 int *d_info, void *stream) {
-  if (!s || !d_vals || !d_rhs || !d_x || !d_info || ((d_lu == nullptr) != (d_piv == nullptr)))
-    return xd_internal_fail(-1, "null argument");
-  Guard g(s->device);
+static SluArgs slu_args(const xd_slu *s) {
   const int *b = s->d_buf;
-  SluArgs a{s->n,           s->tol,           b + s->off[0], b + s->off[1], b + s->off[2], b + s->off[3],
-            b + s->off[4], b + s->off[5],    b + s->off[6], b + s->off[7], b + s->off[8], b + s->off[9],
-            s->nsched,     b + s->off[3]};
+  return SluArgs{s->n,           s->tol,           b + s->off[0], b + s->off[1], b + s->off[2], b + s->off[3],
+                 b + s->off[4], b + s->off[5],    b + s->off[6], b + s->off[7], b + s->off[8], b + s->off[9],
+                 b + s->off[10], s->nsched,        b + s->off[3]};
+}
+
+int xd_slu_solve(xd_slu *s, const double *d_vals, const double *d_rhs, double *d_lu, double *d_x, int *d_info,
+                 void *stream) {
+  if (!s || !d_vals || !d_rhs || !d_x || !d_info) return xd_internal_fail(-1, "null argument");
+  Guard g(s->device);
   slu_kernel<<<1, 32, dense_smem_bytes(s->n) + sizeof(int) * s->nsched, (cudaStream_t)stream>>>(
-      a, d_vals, d_rhs, d_lu, d_piv, d_x, d_info);
+      slu_args(s), d_vals, d_rhs, d_lu, d_x, d_info);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "slu_kernel launch");
+  return 0;
+}
+
+int xd_slu_resolve(xd_slu *s, const double *d_lu, const double *d_rhs, double *d_x, void *stream) {
+  if (!s || !d_lu || !d_rhs || !d_x) return xd_internal_fail(-1, "null argument");
+  Guard g(s->device);
+  slu_resolve_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slu_args(s), d_lu, d_rhs, d_x);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "slu_resolve_kernel launch");
   return 0;
 }
 

@@ -771,6 +771,7 @@ class GpuTransient(TransientBase):
             self.stats.loads += 1
             stream.synchronize()
             wrms, max_rhs = float(self._g_host[0]), float(self._g_host[1])
+            self._lu_from_slu = self._slu is not None and self._g_host[2] == 0
             if self._g_host[2] != 0:
                 self._note_fallback()
             if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
@@ -816,6 +817,7 @@ class GpuTransient(TransientBase):
         if self._slu is not None:
             self._lib.xd_slu_destroy(self._slu)
             self._slu = None
+            self._lu_from_slu = False
             self._graphs = {}  # they launch the old order's kernels
         vals = np.ascontiguousarray(self.jac.cpu().numpy())
         h = ctypes.c_void_p()
@@ -835,8 +837,8 @@ class GpuTransient(TransientBase):
     def _dense_solve(self, out):
         p = self._ptr
         if self._slu is not None:
-            _native.check(self._lib.xd_slu_solve(self._slu, p(self.jac), p(self.rhs), p(self._lu_d), p(self._piv_d),
-                                                 p(out), p(self._info_d), self._stream()), "xd_slu_solve")
+            _native.check(self._lib.xd_slu_solve(self._slu, p(self.jac), p(self.rhs), p(self._lu_d), p(out),
+                                                 p(self._info_d), self._stream()), "xd_slu_solve")
             self._fallback_d.copy_(self._info_d)
             _native.check(self._lib.xd_tia_dense_solve_fallback(self._tia, p(self.jac), p(self.rhs), p(self._lu_d),
                                                                 p(self._piv_d), p(out), p(self._info_d),
@@ -852,8 +854,11 @@ class GpuTransient(TransientBase):
         self._slu_ready(renew=getattr(self, "_first_solve", True))
         self._first_solve = False
         self._dense_solve(self._dx_d)
-        if self._slu is not None and int(self._fallback_d.item()) != 0:
-            self._note_fallback()
+        if self._slu is not None:
+            fell_back = int(self._fallback_d.item()) != 0
+            self._lu_from_slu = not fell_back  # which kernel's factors _lu_d holds
+            if fell_back:
+                self._note_fallback()
         self._lu = "small"
         self.stats.factorizations += 1
         return self._dx_d.clone()
@@ -863,6 +868,10 @@ class GpuTransient(TransientBase):
             return super()._solve_factored()
         out = self.torch.empty_like(self.rhs)
         p = self._ptr
+        if self._slu is not None and getattr(self, "_lu_from_slu", False):
+            _native.check(self._lib.xd_slu_resolve(self._slu, p(self._lu_d), p(self.rhs), p(out), self._stream()),
+                          "xd_slu_resolve")
+            return out
         _native.check(self._lib.xd_tia_dense_resolve(self._tia, p(self._lu_d), p(self._piv_d), p(self.rhs), p(out),
                                                      self._stream()), "xd_tia_dense_resolve")
         return out

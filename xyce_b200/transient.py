@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import warnings
 import time as _time
 from dataclasses import dataclass, field
 
@@ -656,7 +657,9 @@ class GpuTransient(TransientBase):
             self._rf_col = torch.as_tensor(self.colind.astype(np.int64), device=self.dev)
         mk = lambda v: torch.sparse_csr_tensor(self._rf_crow, self._rf_col, v, size=(self.nu, self.nu),
                                                check_invariants=False)
-        return mk(self.jac), mk(self.jac.abs())
+        with warnings.catch_warnings():  # torch marks its sparse CSR support as beta
+            warnings.simplefilter("ignore", UserWarning)
+            return mk(self.jac), mk(self.jac.abs())
 
     def _rf_solve_refined(self, b, tol=1e-10, max_refine=3, accept=False):
         """Solve with the current factors, then iterative refinement (r = b - J x, x += J^-1 r) until

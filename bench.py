@@ -196,13 +196,12 @@ def placed_transient(args):
 
     import torch
 
-    from tests.parity import family_inputs
     from xyce_b200 import MosfetDevice, SolverFlags, netlist
     from xyce_b200.transient import GpuTransient, NewtonParams
 
     c = netlist.random_logic(args.placed_mos, seed=args.seed, n_inputs=64, locality=64)
     rowptr, colind = netlist.jacobian_pattern(c)
-    cards, im, nd, params = family_inputs(c, None)
+    cards, im, nd, params = netlist.mosfet_family(c, None)
     fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
     g = GpuTransient(c, fam, rowptr, colind, solver="rf")
     torch.cuda.synchronize()
@@ -274,7 +273,6 @@ def transient_section(args):
     the learned warm start against the plain GPU path (Newton iterations per step)."""
     import torch
 
-    from tests.parity import family_inputs
     from tests.transient_oracle import OracleTransient
     from xyce_b200 import Bsim3Device, MosfetDevice, netlist, surrogate as S
     from xyce_b200.transient import GpuTransient, NewtonParams
@@ -324,7 +322,7 @@ def transient_section(args):
     train_s = time.perf_counter() - t0
     c = netlist.random_logic(1200, seed=7, n_inputs=16)
     rowptr, colind = netlist.jacobian_pattern(c)
-    cards, im, nd, params = family_inputs(c, None)
+    cards, im, nd, params = netlist.mosfet_family(c, None)
     res, waves = {}, {}
     for mode in ("plain", "warm_start"):
         fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
@@ -445,7 +443,8 @@ class ClockSampler:
 
 
 def cpu_baseline(args, omp=False, sample=None, min_seconds=10.0):
-    """Reference CPU load (oracle library = the reference's own device code) on a bounded sample."""
+    """Reference CPU load (oracle library = the reference's own device code) on a bounded sample.
+    Serial: the plain build (no libm interposer) when present; omp: the OpenMP build."""
     from oracle import xyce_ref as xr
     from tests.parity import OracleRun
 
@@ -453,9 +452,11 @@ def cpu_baseline(args, omp=False, sample=None, min_seconds=10.0):
     c, rowptr, colind = build_workload(sample, args.seed, args.wire_segments)
     cards, im, nd, params = family(c)
     orc = OracleRun(c, cards, im, nd, params, rowptr, colind)
-    if omp:
-        # Same circuit through the OpenMP build of the reference (updateState parallel).
-        orc.ref = xr.RefCircuit(14, [(m.pmos, dict(m.params)) for m in cards], im, nd, params, c.n_unknowns, omp=True)
+    plain = not omp and xr.available(plain=True)
+    if omp or plain:
+        # Same circuit through the OpenMP build (updateState parallel) or the plain serial build.
+        orc.ref = xr.RefCircuit(14, [(m.pmos, dict(m.params)) for m in cards], im, nd, params, c.n_unknowns, omp=omp,
+                                plain=plain)
         orc.ref.set_pattern(*_oracle_pattern(c, nd, rowptr, colind))
     n = im.shape[0]
     sol = np.random.default_rng(args.seed).uniform(0.0, 1.2, c.n_unknowns)
@@ -468,7 +469,7 @@ def cpu_baseline(args, omp=False, sample=None, min_seconds=10.0):
     while dt < min_seconds and reps < 10000:
         reps = max(reps * 2, int(reps * min_seconds / max(dt, 1e-3) * 1.1))
         dt = orc.ref.time_loads(reps)
-    return n * reps / dt, n, reps, dt
+    return n * reps / dt, n, reps, dt, ("openmp" if omp else ("serial" if plain else "serial, libm interposer"))
 
 
 def _oracle_pattern(c, inst_nodes, rowptr, colind):
@@ -507,7 +508,7 @@ def run_reference(args, rank):
     for _ in range(args.warmup):
         cpu_baseline(args, omp=omp, min_seconds=1.0)
     for _ in range(args.steps):
-        v, n, reps, dt = cpu_baseline(args, omp=omp, min_seconds=2.0)
+        v, n, reps, dt, _ = cpu_baseline(args, omp=omp, min_seconds=2.0)
         samples.append((v, dt))
     value = statistics.median([s[0] for s in samples])
     total = sum(s[1] for s in samples)
@@ -680,12 +681,13 @@ def main():
         from oracle import xyce_ref as xr
 
         if xr.available():
-            v, ns, reps_c, dt = cpu_baseline(args)
+            v, ns, reps_c, dt, build = cpu_baseline(args)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"{ns} BSIM4 instances of the same generator x {reps_c} full loads ({dt:.1f} s), "
-                             "serial reference build (-O2), fixed Newton iterate"}
+                             f"reference build -O2 ({build}), fixed Newton iterate"}
     hbm_peak, peak_src = measured_peaks()
     eval_achieved = EVAL_BYTES_PER_INST * n / (t_eval * 1e-3) / 1e9
+    fp64_achieved = EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -696,12 +698,16 @@ def main():
                    "instances_per_gpu": n, "nnz": nnz, "parallelism": f"replicas x{world}",
                    "l2": "working set > 126 MB L2 (staging + maps + CSR values), no flush"},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "bsim4_eval_kernel", "achieved": eval_achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": eval_achieved / hbm_peak,
+        "roofline": {"bound": "fp64", "kernel": "bsim4_eval_kernel", "achieved": fp64_achieved,
+                     "peak": fp64_peak_tflops, "unit": "TFLOP/s", "frac": fp64_achieved / fp64_peak_tflops,
                      "traffic": EVAL_DRAM_BYTES_PER_INST_NCU * n,
-                     "note": f"peak = {peak_src} HBM copy bandwidth; algorithmic bytes {EVAL_BYTES_PER_INST} B/instance; "
-                             f"traffic = ncu DRAM bytes per instance ({EVAL_DRAM_BYTES_PER_INST_NCU} B at 199,832 "
-                             "instances, profiles/bsim4_eval_kernel_scale.md) x instances"},
+                     "note": f"binding bound: the FP64 pipe ({EVAL_FP64_FLOPS_PER_INST} FP64 flops per instance, "
+                             "executed-instruction count); peak = the FP64 FMA probe timed in this run "
+                             "(the measured-peaks file has no FP64 figure); traffic = ncu DRAM bytes per "
+                             f"instance ({EVAL_DRAM_BYTES_PER_INST_NCU} B) x instances",
+                     "hbm": {"achieved": eval_achieved, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": eval_achieved / hbm_peak, "peak_source": peak_src,
+                             "algorithmic_bytes_per_instance": EVAL_BYTES_PER_INST}},
         "kernels_ms": {"eval": t_eval, "gather_vectors": t_vec, "gather_matrices": t_mat},
         "eval_launch_shape": shape,
         "fp64": {"probe_peak_tflops": fp64_peak_tflops, "flops_per_instance": EVAL_FP64_FLOPS_PER_INST,

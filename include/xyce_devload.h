@@ -216,7 +216,15 @@ int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);
  *     call's contents. Calls whose work overlaps on the GPU (different streams, or different
  *     host threads without ordering) race on it; order them on one stream.
  *   - Nothing in the array needs to start at zero: each call writes every staged value and
- *     every partial it later reads. */
+ *     every partial it later reads.
+ *   - The staged stamps of a static load stay in the array, not in the context: after it,
+ *     xd_load_vectors, xd_load_matrices, xd_load_abs and xd_copy_stamps on the same context
+ *     return an error until the next xd_update_state (or xd_load) refills the context's own.
+ *   - The array's device address is kept per device for the life of the process, so the call
+ *     assumes the device's primary context is not reset (cudaDeviceReset) while the library is
+ *     loaded.
+ *   - Families with internal drain / source nodes (series resistance) are rejected: their
+ *     staging layout is wider than the array's. */
 #define XD_STATIC_MAX_INSTANCES 16384
 int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, double *d_next_sta,
                            double *d_curr_sta, double *d_next_sto, const double *d_curr_sto, double *d_f,

@@ -19,6 +19,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libxyce_ref.so")
 LIB_OMP_PATH = os.path.join(_HERE, "_ref", "libxyce_ref_omp.so")
+# Serial build without the libm interposer (oracle/libm_perturb.C): the CPU baseline's timing.
+LIB_PLAIN_PATH = os.path.join(_HERE, "_ref", "libxyce_ref_plain.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -36,12 +38,16 @@ class XrefFlags(ctypes.Structure):
 _LIBS: dict = {}
 
 
-def available(omp: bool = False) -> bool:
-    return os.path.exists(LIB_OMP_PATH if omp else LIB_PATH)
+def _path(omp: bool, plain: bool) -> str:
+    return LIB_OMP_PATH if omp else (LIB_PLAIN_PATH if plain else LIB_PATH)
 
 
-def load_library(omp: bool = False):
-    path = LIB_OMP_PATH if omp else LIB_PATH
+def available(omp: bool = False, plain: bool = False) -> bool:
+    return os.path.exists(_path(omp, plain))
+
+
+def load_library(omp: bool = False, plain: bool = False):
+    path = _path(omp, plain)
     if path in _LIBS:
         return _LIBS[path]
     if not os.path.exists(path):
@@ -106,8 +112,8 @@ class RefCircuit:
     inst_params: {NAME: float array [n]} (NaN = not given).
     """
 
-    def __init__(self, level, models, inst_model, inst_nodes, inst_params, n_nodes, omp=False):
-        self.lib = load_library(omp)
+    def __init__(self, level, models, inst_model, inst_nodes, inst_params, n_nodes, omp=False, plain=False):
+        self.lib = load_library(omp, plain)
         self.level = level
         is_pmos = np.array([1 if m[0] else 0 for m in models], dtype=np.int32)
         nparams = np.array([len(m[1]) for m in models], dtype=np.int32)

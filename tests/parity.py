@@ -50,15 +50,8 @@ def row_max(rowptr, vals):
     return rmax
 
 
-def family_inputs(c: netlist.Circuit, cards=None, extra_params=None):
-    """(models, inst_model, inst_nodes, inst_params) for the circuit's MOSFETs."""
-    if cards is None:
-        cards = [ModelCard(False, {}), ModelCard(True, {})]
-    inst_model = c.mos_type.astype(np.int32)
-    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float)}
-    if extra_params:
-        params.update(extra_params)
-    return cards, inst_model, c.mos_nodes.astype(np.int32), params
+# (cards, inst_model, inst_nodes, inst_params) of a circuit's MOSFETs.
+family_inputs = netlist.mosfet_family
 
 
 def flags_dict(f: SolverFlags) -> dict:
@@ -151,6 +144,16 @@ class OracleRun:
         r = self.load(flags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa)
         r["sens"] = {k: np.max([np.abs(p[k] - r[k]) for p in pert], axis=0) for k in OUTPUT_KEYS}
         return r
+
+
+def strict_split(got, ref, rtol=RTOL):
+    """(entries, entries within the plain bound |a - b| <= rtol * max(|a|, |b|), indices of the
+    others): how many entries needed one of the floors of compare() to pass."""
+    got = np.asarray(got).reshape(-1)
+    ref = np.asarray(ref).reshape(-1)
+    d = np.abs(got - ref)
+    ok = d <= rtol * np.maximum(np.abs(got), np.abs(ref))
+    return int(ok.size), int(np.count_nonzero(ok)), np.flatnonzero(~ok)
 
 
 def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None, sens=None,

@@ -100,6 +100,10 @@ struct xd_ctx {
   int2 *d_ext = nullptr;
   int vec_rows = 4, mat_slots = xb4::kNumMat, stage_slots = xb4::kNumStage;
   int resident_blocks[16] = {};  // per persistent launch shape: blocks resident on the whole device
+  // The last evaluation was xd_load_static_scratch: its staged stamps are in the library's static
+  // array, so d_stage does not hold them and the calls that read d_stage refuse until the next
+  // xd_update_state.
+  bool stage_static = false;
 };
 
 namespace {
@@ -982,6 +986,15 @@ int xd_update_state(xd_ctx *ctx, const xd_flags *flags, const double *d_sol, dou
               ctx->d_stage, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "bsim4_eval_kernel launch");
+  ctx->stage_static = false;
+  return 0;
+}
+
+// The calls that read the context's staged stamps (d_stage) refuse after a static-scratch load.
+static int check_stage_current(const xd_ctx *ctx) {
+  if (ctx->stage_static)
+    return fail(-1, "the last evaluation of this context was xd_load_static_scratch, whose staged stamps are in "
+                    "the library's static array, not in the context; call xd_update_state first");
   return 0;
 }
 
@@ -1009,6 +1022,7 @@ static int load_matrices_impl(xd_ctx *ctx, double *jf, double *jq, bool abs_mode
 int xd_load_vectors(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double *d_dqdxdvp, void *stream) {
   if (!ctx) return fail(-1, "null context");
   if (ctx->n == 0) return 0;
+  if (int rc = check_stage_current(ctx)) return rc;
   DeviceGuard g(ctx->device);
   return load_vectors_impl(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, false, (cudaStream_t)stream);
 }
@@ -1016,6 +1030,7 @@ int xd_load_vectors(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, do
 int xd_load_matrices(xd_ctx *ctx, double *d_dfdx_vals, double *d_dqdx_vals, void *stream) {
   if (!ctx) return fail(-1, "null context");
   if (ctx->n == 0) return 0;
+  if (int rc = check_stage_current(ctx)) return rc;
   DeviceGuard g(ctx->device);
   return load_matrices_impl(ctx, d_dfdx_vals, d_dqdx_vals, false, (cudaStream_t)stream);
 }
@@ -1056,6 +1071,7 @@ int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double
                 double *d_dqdx_vals, void *stream) {
   if (!ctx) return fail(-1, "null context");
   if (ctx->n == 0) return 0;
+  if (int rc = check_stage_current(ctx)) return rc;
   DeviceGuard g(ctx->device);
   int rc = load_vectors_impl(ctx, d_f, d_q, d_dfdxdvp, d_dqdxdvp, true, (cudaStream_t)stream);
   if (rc) return rc;
@@ -1111,6 +1127,7 @@ int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream) {
 
 int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream) {
   if (!ctx || !h_out) return fail(-1, "null argument");
+  if (int rc = check_stage_current(ctx)) return rc;
   DeviceGuard g(ctx->device);
   cudaStream_t st = (cudaStream_t)stream;
   XD_CUDA(cudaMemcpyAsync(h_out, ctx->d_stage, (size_t)ctx->stage_slots * ctx->n * sizeof(double),
@@ -1211,7 +1228,9 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
   OutSet<4, false> vs{{d_f, d_q, d_dfdxdvp, d_dqdxdvp}, {0, 4 * n, 8 * n, 12 * n}};
   if ((rc = run_gather_static(ctx->vmap, stage, partial, vs, st))) return rc;
   OutSet<2, false> ms{{d_dfdx_vals, d_dqdx_vals}, {16 * n, 32 * n}};
-  return run_gather_static(ctx->mmap, stage, partial, ms, st);
+  if ((rc = run_gather_static(ctx->mmap, stage, partial, ms, st))) return rc;
+  ctx->stage_static = true;
+  return 0;
 }
 
 }  // extern "C"

@@ -284,6 +284,21 @@ RING_BSIM3_NMOS = {"TOX": 4e-9, "VTH0": 0.45, "K1": 0.55, "K2": 0.0, "U0": 400.0
 RING_BSIM3_PMOS = {"TOX": 4e-9, "VTH0": -0.45, "K1": 0.55, "K2": 0.0, "U0": 120.0, "VSAT": 8e4}
 
 
+def mosfet_family(c: Circuit, cards=None, extra_params=None):
+    """(cards, inst_model, inst_nodes, inst_params) of the circuit's MOSFETs for ``MosfetDevice``:
+    one NMOS and one PMOS card (default parameters unless ``cards`` is given), each instance's
+    card by its type, its D, G, S, B unknowns, and L / W plus ``extra_params`` per instance."""
+    from .device import ModelCard
+
+    if cards is None:
+        cards = [ModelCard(False, {}), ModelCard(True, {})]
+    inst_model = c.mos_type.astype(np.int32)
+    params = {"L": c.mos_l.astype(float), "W": c.mos_w.astype(float)}
+    if extra_params:
+        params.update(extra_params)
+    return cards, inst_model, c.mos_nodes.astype(np.int32), params
+
+
 def ring_bsim3_cards():
     from .device import ModelCard
     return [ModelCard(False, dict(RING_BSIM3_NMOS)), ModelCard(True, dict(RING_BSIM3_PMOS))]

@@ -192,6 +192,12 @@ int xd_eval_variant_info(int v, int *block, int *min_blocks);
 /* 1 when candidate v is a persistent shape (one wave of resident blocks walking the instances with
  * a grid stride), 0 when it launches one block per `block` instances, < 0 for a bad v. */
 int xd_eval_variant_persistent(int v);
+/* 1 when candidate v splits the evaluation into two kernels — the DC part (limiting, junction
+ * diodes, drain current, GIDL / GISL, gate tunnelling) and then charges, capacitances and stamps —
+ * which hand per-instance state over through a buffer the context allocates at xd_create; each
+ * kernel is smaller than the fused one (fewer registers, a smaller instruction footprint). Its
+ * results are bit-identical to the fused candidates'. 0 otherwise, < 0 for a bad v. */
+int xd_eval_variant_split(int v);
 int xd_get_eval_variant(const xd_ctx *ctx);
 int xd_set_eval_variant(xd_ctx *ctx, int v);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);

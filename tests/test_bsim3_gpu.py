@@ -103,3 +103,53 @@ def test_bsim3_load_is_deterministic():
     for key in ("f", "q", "dfdxdvp", "dqdxdvp", "dfdx", "dqdx", "next_sta", "next_sto"):
         assert np.array_equal(a[key], b[key]), key
     dev.close()
+
+
+def _family_variants(level):
+    from xyce_b200 import _native
+    from xyce_b200.device import MosfetDevice
+
+    lib = _native.load()
+    c = netlist.random_logic(200, seed=3)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c, netlist.ring_bsim3_cards() if level == 9 else None)
+    dev = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=level)
+    vs = [v for v in range(lib.xd_num_eval_variants()) if lib.xd_set_eval_variant(dev._h, v) == 0]
+    dev.close()
+    return vs
+
+
+@pytest.mark.parametrize("level", [9, 1])
+def test_launch_shape_candidates_parity_and_bitwise(level):
+    """BSIM3 and MOSFET1 have their own launch-shape candidates, which the autotuner times per
+    circuit. Each is held to the oracle, with a partial last block, and all give the same loads
+    bit for bit."""
+    variants = _family_variants(level)
+    assert len(variants) >= 4
+    c = netlist.random_logic(1500, seed=22)
+    cards = netlist.ring_bsim3_cards() if level == 9 else [ModelCard(False, {}), ModelCard(True, {})]
+    seq = SEQ[:2] + SEQ[3:6]
+    for v in variants:
+        worst = run_sequence(c, cards, seq, vrange=(-0.3, 1.8), level=level, eval_variant=v, charges_in_dc=level == 1)
+        print("level", level, "variant", v, "worst error / tolerance:", worst)
+    from xyce_b200.device import MosfetDevice
+
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards_, im, nd, params = family_inputs(c, cards)
+    n = im.shape[0]
+    rng = np.random.default_rng(5)
+    sol = rng.uniform(-0.3, 1.8, c.n_unknowns)
+    ref = None
+    for v in variants:
+        dev = MosfetDevice(cards_, im, nd, params, (rowptr, colind), c.n_unknowns, level=level)
+        assert dev._lib.xd_set_eval_variant(dev._h, v) == 0
+        z_sta, z_sto = np.zeros(dev.n_state), np.zeros(dev.n_store)
+        out = GpuRun(dev, int(rowptr[-1]), c.n_unknowns).load(SolverFlags(newton_iter=1), sol, z_sta, z_sta, z_sto,
+                                                              z_sto)
+        dev.close()
+        if ref is None:
+            ref = out
+            continue
+        for k in out:
+            if k != "abs":
+                assert np.array_equal(out[k], ref[k], equal_nan=True), (level, v, k)

@@ -65,7 +65,7 @@ def _num_variants():
     return _native.load().xd_num_eval_variants()
 
 
-@pytest.mark.parametrize("v", [0, 1, 2, 3, 4, 5, 6, 7, 10, 11])
+@pytest.mark.parametrize("v", [0, 1, 2, 3, 4, 5, 6, 7, 10, 11, 12, 13, 14, 15])
 def test_parity_every_eval_launch_variant(v):
     """The autotuner may pick any launch shape of the evaluation kernel; each is held to the
     oracle, with an instance count that leaves a partial last block."""
@@ -145,8 +145,9 @@ def test_gate_tunnelling_family_refuses_variants_without_it():
     for v in range(lib.xd_num_eval_variants()):
         ok.append(lib.xd_set_eval_variant(dev._h, v) == 0)
     dev.close()
-    # 6, 7 and 11 are the full ones; 8, 9 are for internal nodes; 10 is a persistent common one.
-    assert ok == [False] * 6 + [True] * 2 + [False] * 2 + [False] + [True]
+    # 6, 7 and 11 are the full ones; 8, 9 are for internal nodes; 10 is a persistent common one;
+    # 12-15 split the common evaluation into two kernels; 16-23 are for BSIM3 and MOSFET1.
+    assert ok == [False] * 6 + [True] * 2 + [False] * 2 + [False] + [True] + [False] * 4 + [False] * 8
 
 
 @pytest.mark.parametrize("variant", ["all", "mixed"])
@@ -236,3 +237,43 @@ def test_persistent_eval_variants_walk_every_instance():
         for k in out:
             if k != "abs":
                 assert np.array_equal(out[k], outs[2][k], equal_nan=True), (v, k)
+
+
+def test_split_evaluation_equals_fused_bitwise():
+    """The split launch shapes (DC part, then charges and stamps, handing per-instance state over
+    through the context's buffer) give the fused evaluation's results bit for bit over a flag
+    sequence that takes every path of the hand-off: limiting off and on, the first step of a
+    transient (current state written too), junction initialisation and a DC load; the carried vgb
+    of each load feeds the next."""
+    from xyce_b200 import _native
+
+    lib = _native.load()
+    c = netlist.random_logic(20000, seed=12)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards, im, nd, params = family_inputs(c)
+    n = im.shape[0]
+    seq = [SolverFlags(newton_iter=1, voltlim=0), SolverFlags(newton_iter=0, init_tran=1),
+           SolverFlags(newton_iter=2), SolverFlags(dcop=1, transient=0, newton_iter=0, init_jct=1),
+           SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=1)]
+    rng = np.random.default_rng(9)
+    sols = [rng.uniform(-0.3, 1.5, c.n_unknowns) for _ in seq]
+    split = [v for v in range(lib.xd_num_eval_variants()) if lib.xd_eval_variant_split(v) == 1]
+    assert split
+    outs = {}
+    for v in [10] + split:
+        dev = Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
+        assert dev._lib.xd_set_eval_variant(dev._h, v) == 0
+        gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
+        sta_n, sta_c, sto_n, sto_c = np.zeros(3 * n), np.zeros(3 * n), np.zeros(14 * n), np.zeros(14 * n)
+        res = []
+        for flags, sol in zip(seq, sols):
+            g = gpu.load(flags, sol, sta_n, sta_c, sto_n, sto_c)
+            res.append(g)
+            sta_n, sta_c, sto_n = g["next_sta"], g["curr_sta"], g["next_sto"]
+        outs[v] = res
+        dev.close()
+    for v in split:
+        for step, (a, b) in enumerate(zip(outs[10], outs[v])):
+            for k in a:
+                if k != "abs":
+                    assert np.array_equal(a[k], b[k], equal_nan=True), (v, step, k)

@@ -95,24 +95,46 @@ XD_HD void poly_depletion(double phi, double ngate, double epsgate, double coxe,
 // tunnelling currents run the FULL = true instantiation.
 // SERIES = true: V holds (D', G, S', B) and Vx the external (D, S); the linear drain and source
 // resistances (rdsMod = 0, sheet resistance) load into vecx / jfx.
-template <bool FULL = false, bool SERIES = false, class RV>
-XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
-                      LoadOut &o, const double *Vx = nullptr) {
-  using namespace xdc;
+
+// Hand-off state between the two parts of the evaluation when they run as separate kernels: the
+// DC part (limiting, junction diodes, drain current, GIDL / GISL, gate tunnelling) stores these per
+// instance, and the charge-and-stamp part (charges, capacitances, store / state, stamps) reads them.
+// Parameters and node voltages are not in it: the second part reads them again; everything it
+// derives from them (branch voltages from the limited vds / vgs / vbs, Phis from Vbseff, ...) it
+// recomputes with the same operations, so the split evaluation is bit-identical to the fused one.
+enum MidSlot {
+  m_vds, m_vgs, m_vbs, m_orig, m_von, m_gbs, m_cbs, m_gbd, m_cbd, m_cdrain, m_gds, m_gm, m_gmbs, m_csub,
+  m_gbbs, m_gbgs, m_gbds, m_Igidl, m_ggidld, m_ggidlg, m_ggidlb, m_Igisl, m_ggisls, m_ggislg, m_ggislb,
+  m_Abulk0, m_dAbulk0_dVb, m_Vbseff, m_dVbseff_dVb, m_Vgs_eff, m_dVgs_eff_dVg, m_Vgst, m_dVth_dVb, m_dVth_dVd,
+  m_n, m_dn_dVb, m_dn_dVd,
+  kNumMid,
+  // Gate tunnelling currents (the full evaluation variants only).
+  m_Igs = kNumMid, m_gIgsg, m_gIgss, m_Igd, m_gIgdg, m_gIgdd, m_Igcs, m_gIgcsg, m_gIgcsd, m_gIgcsb, m_Igcd,
+  m_gIgcdg, m_gIgcdd, m_gIgcdb, m_Igb, m_gIgbg, m_gIgbd, m_gIgbb,
+  kNumMidFull
+};
+struct Mid {
+  double v[kNumMidFull];
+};
+
 #define P(x) P_(f_##x)
+
+// Node and branch voltages of one instance and their unlimited ("orig") copies, with the
+// initial-condition overrides applied (:7932-8097).
+struct Bias {
+  double Vd, Vs, Vdp, Vsp, Vddp, Vssp;
+  double vds, vgs, vbs, vges, vgms, vdbs, vsbs, vses, vdes, vbd, vdbd, vgd, vged, vgmd, vgmb, vbs_jct, vbd_jct;
+  double vbd_orig, vbs_orig, vgs_orig, vds_orig, vgd_orig, vges_orig, vgms_orig, vdes_orig, vses_orig, vdbs_orig;
+  double vsbs_orig, vdbd_orig, vged_orig, vgmd_orig, vbs_jct_orig, vbd_jct_orig, vgmb_orig;
+  int origFlag;
+};
+
+template <bool SERIES, class RV>
+XD_HD void bsim4_bias(const RV &P_, const double V[4], const LoadFlags &fl, const double *Vx, Bias &b) {
+  using namespace xdc;
   const double dtype = P(dtype);
-  const int mobMod = (int)P(mobMod);
-  const int dioMod = (int)P(dioMod);
-  const int tempMod = (int)P(tempMod);
-  const int capMod = FULL ? (int)P(capMod) : 2;
-  const double gmin = fl.gmin;
-  const double nf = P(nf);
   const double vth0 = P(vth0);
-  const double M = P(mult);
   const bool OFF = P(off) != 0.0;
-
-  const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
-
   // Node and branch voltages (:7932-8030), collapsed topology.
   const double Vdp = V[0], Vge = V[1], Vsp = V[2], Vb = V[3];
   const double Vd = SERIES ? Vx[0] : Vdp, Vs = SERIES ? Vx[1] : Vsp;
@@ -142,9 +164,6 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   const double vges_orig = vges, vgms_orig = vgms, vdes_orig = vdes, vses_orig = vses, vdbs_orig = vdbs;
   const double vsbs_orig = vsbs, vdbd_orig = vdbd, vged_orig = vged, vgmd_orig = vgmd;
   const double vbs_jct_orig = vbs_jct, vbd_jct_orig = vbd_jct, vgmb_orig = vgmb;
-  // The reference takes vgb_orig from the instance's vgb member before it is recomputed, i.e. the
-  // previous load's value (:8026); in the limiter test below vgb therefore equals vgb_orig.
-  double vgb = vgb_orig;
 
   // Initial-condition handling (:8051-8097). inputOP with a flag vector is not modelled.
   if (fl.init_jct && !OFF && fl.voltlim) {
@@ -163,7 +182,1104 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     vds = vgs = vbs = vges = vgms = 0.0;
     vds = vsbs = vdes = vses = 0.0;
   }
+  b.Vd = Vd; b.Vs = Vs; b.Vdp = Vdp; b.Vsp = Vsp; b.Vddp = Vddp; b.Vssp = Vssp;
+  b.vds = vds; b.vgs = vgs; b.vbs = vbs; b.vges = vges; b.vgms = vgms; b.vdbs = vdbs; b.vsbs = vsbs;
+  b.vses = vses; b.vdes = vdes; b.vbd = vbd; b.vdbd = vdbd; b.vgd = vgd; b.vged = vged; b.vgmd = vgmd;
+  b.vgmb = vgmb; b.vbs_jct = vbs_jct; b.vbd_jct = vbd_jct;
+  b.vbd_orig = vbd_orig; b.vbs_orig = vbs_orig; b.vgs_orig = vgs_orig; b.vds_orig = vds_orig;
+  b.vgd_orig = vgd_orig; b.vges_orig = vges_orig; b.vgms_orig = vgms_orig; b.vdes_orig = vdes_orig;
+  b.vses_orig = vses_orig; b.vdbs_orig = vdbs_orig; b.vsbs_orig = vsbs_orig; b.vdbd_orig = vdbd_orig;
+  b.vged_orig = vged_orig; b.vgmd_orig = vgmd_orig; b.vbs_jct_orig = vbs_jct_orig;
+  b.vbd_jct_orig = vbd_jct_orig; b.vgmb_orig = vgmb_orig;
+  b.origFlag = origFlag;
+}
 
+// Charge-and-stamp part of the evaluation: charges and capacitances, store and state, the F / Q /
+// limiter-vector stamps and the dF/dx, dQ/dx stamps (:10707-13855, 16195-17268), from the DC part's
+// hand-off state m.
+template <bool FULL = false, bool SERIES = false, class RV>
+XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, double vgb_orig, const Mid &m,
+                        LoadOut &o, const double *Vx) {
+  using namespace xdc;
+  const double dtype = P(dtype);
+  const int capMod = FULL ? (int)P(capMod) : 2;
+  const int igcMod = FULL ? (int)P(igcMod) : 0, igbMod = FULL ? (int)P(igbMod) : 0;
+  const double nf = P(nf);
+  const double M = P(mult);
+  const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
+  Bias bias;
+  bsim4_bias<SERIES>(P_, V, fl, Vx, bias);
+  const double Vddp = bias.Vddp, Vssp = bias.Vssp;
+  (void)Vddp; (void)Vssp;
+  double vds = bias.vds, vgs = bias.vgs, vbs = bias.vbs, vges = bias.vges, vgms = bias.vgms, vdbs = bias.vdbs;
+  double vsbs = bias.vsbs, vses = bias.vses, vdes = bias.vdes, vbd = bias.vbd, vdbd = bias.vdbd, vgd = bias.vgd;
+  double vged = bias.vged, vgmd = bias.vgmd, vgmb = bias.vgmb, vbs_jct = bias.vbs_jct, vbd_jct = bias.vbd_jct;
+  const double vbd_orig = bias.vbd_orig, vbs_orig = bias.vbs_orig, vgs_orig = bias.vgs_orig;
+  const double vds_orig = bias.vds_orig, vgd_orig = bias.vgd_orig, vges_orig = bias.vges_orig;
+  const double vgms_orig = bias.vgms_orig, vdes_orig = bias.vdes_orig, vses_orig = bias.vses_orig;
+  const double vdbs_orig = bias.vdbs_orig, vsbs_orig = bias.vsbs_orig, vdbd_orig = bias.vdbd_orig;
+  const double vged_orig = bias.vged_orig, vgmd_orig = bias.vgmd_orig, vbs_jct_orig = bias.vbs_jct_orig;
+  const double vbd_jct_orig = bias.vbd_jct_orig, vgmb_orig = bias.vgmb_orig;
+  (void)vdes_orig; (void)vses_orig; (void)vdbs_orig; (void)vsbs_orig; (void)vdbd_orig; (void)vged_orig;
+  (void)vgmd_orig; (void)vges_orig; (void)vgms_orig;
+  int origFlag = bias.origFlag;
+  // The reference takes vgb_orig from the instance's vgb member before it is recomputed, i.e. the
+  // previous load's value (:8026); in the limiter test below vgb therefore equals vgb_orig.
+  double vgb = vgb_orig;
+  vds = m.v[m_vds];
+  vgs = m.v[m_vgs];
+  vbs = m.v[m_vbs];
+  origFlag = (int)m.v[m_orig];
+  vbd = vbs - vds;
+  vgd = vgs - vds;
+  vgb = vgs - vbs;
+  vged = vges - vds;
+  vgmd = vgms - vds;
+  vgmb = vgms - vbs;
+  vdbd = vdbs - vds;
+  vbs_jct = vbs;
+  vbd_jct = vbd;
+  (void)vged; (void)vgmd;
+  double T0, T1, T2, T3, T4, T5, T6, T7, T8, T9, T10, T11, T12, T13, T14;
+  double dT0_dVg, dT0_dVd, dT0_dVb, dT1_dVg, dT1_dVd, dT1_dVb, dT2_dVg, dT2_dVd, dT2_dVb;
+  double dT3_dVg, dT3_dVd, dT3_dVb, dT4_dVd, dT5_dVg, dT5_dVd, dT5_dVb, dT6_dVg, dT6_dVd, dT6_dVb;
+  double dT8_dVg, dT8_dVd, dT8_dVb, dT9_dVg, dT9_dVd, dT9_dVb, dT10_dVg, dT10_dVd, dT10_dVb;
+  double tmp, tmp1, tmp2, tmp3, tmp4;
+  const double Aseff = P(Aseff), Pseff = P(Pseff), Adeff = P(Adeff), Pdeff = P(Pdeff), weffCJ = P(weffCJ);
+  (void)Pseff; (void)Pdeff;
+  const double gbs = m.v[m_gbs], cbs = m.v[m_cbs], gbd = m.v[m_gbd], cbd = m.v[m_cbd];
+  const int mode = vds >= 0.0 ? 1 : -1;
+  const double Vds = mode > 0 ? vds : -vds;
+  const double Vbs = mode > 0 ? vbs : vbd;
+  const double epssub = CONSTEPSSI;
+  const double phi = P(phi), sqrtPhi_p = P(sqrtPhi);
+  const double Vbseff = m.v[m_Vbseff], dVbseff_dVb = m.v[m_dVbseff_dVb];
+  const double Phis = phi - Vbseff;
+  const double dPhis_dVb = -1.0;
+  const double sqrtPhis = sqrt(Phis);
+  const double dsqrtPhis_dVb = -0.5 / sqrtPhis;
+  const double Vtm = P(vtm);
+  const double k1ox = P(k1ox);
+  const double coxe = P(coxe);
+  const double coxp = P(coxp);
+  const double dVth_dVb = m.v[m_dVth_dVb], dVth_dVd = m.v[m_dVth_dVd];
+  const double n = m.v[m_n], dn_dVb = m.v[m_dn_dVb], dn_dVd = m.v[m_dn_dVd];
+  const double von = m.v[m_von];
+  const double Vgs_eff = m.v[m_Vgs_eff], dVgs_eff_dVg = m.v[m_dVgs_eff_dVg];
+  const double Vgst = m.v[m_Vgst];
+  const double Abulk0 = m.v[m_Abulk0], dAbulk0_dVb = m.v[m_dAbulk0_dVb];
+  const double cdrain = m.v[m_cdrain], gds = m.v[m_gds], gm = m.v[m_gm], gmbs = m.v[m_gmbs];
+  const double csub = m.v[m_csub], gbbs = m.v[m_gbbs], gbgs = m.v[m_gbgs], gbds = m.v[m_gbds];
+  const double Igidl = m.v[m_Igidl], ggidld = m.v[m_ggidld], ggidlg = m.v[m_ggidlg], ggidlb = m.v[m_ggidlb];
+  const double Igisl = m.v[m_Igisl], ggisls = m.v[m_ggisls], ggislg = m.v[m_ggislg], ggislb = m.v[m_ggislb];
+  const double Igs = FULL ? m.v[m_Igs] : 0.0, gIgsg = FULL ? m.v[m_gIgsg] : 0.0, gIgss = FULL ? m.v[m_gIgss] : 0.0;
+  const double Igd = FULL ? m.v[m_Igd] : 0.0, gIgdg = FULL ? m.v[m_gIgdg] : 0.0, gIgdd = FULL ? m.v[m_gIgdd] : 0.0;
+  const double Igcs = FULL ? m.v[m_Igcs] : 0.0, gIgcsg = FULL ? m.v[m_gIgcsg] : 0.0;
+  const double gIgcsd = FULL ? m.v[m_gIgcsd] : 0.0, gIgcsb = FULL ? m.v[m_gIgcsb] : 0.0;
+  const double Igcd = FULL ? m.v[m_Igcd] : 0.0, gIgcdg = FULL ? m.v[m_gIgcdg] : 0.0;
+  const double gIgcdd = FULL ? m.v[m_gIgcdd] : 0.0, gIgcdb = FULL ? m.v[m_gIgcdb] : 0.0;
+  const double Igb = FULL ? m.v[m_Igb] : 0.0, gIgbg = FULL ? m.v[m_gIgbg] : 0.0;
+  const double gIgbd = FULL ? m.v[m_gIgbd] : 0.0, gIgbb = FULL ? m.v[m_gIgbb] : 0.0;
+  const double gIgbs = -(gIgbg + gIgbd + gIgbb);
+  const double gIgcss = -(gIgcsg + gIgcsd + gIgcsb);
+  const double gIgcds = -(gIgcdg + gIgcdd + gIgcdb);
+  double Coxeff, dCoxeff_dVg, Tcen, dTcen_dVg, Denomi, Vgsteff, dVgsteff_dVg, dVgsteff_dVd, dVgsteff_dVb;
+
+  // Intrinsic charges (:10707-11620): capMod 0, 1 or 2 (charge-thickness model).
+  double qgate = 0, qdrn = 0, qbulk = 0, qsrc = 0;
+  double cggb = 0, cgsb = 0, cgdb = 0, cdgb = 0, cdsb = 0, cddb = 0, cbgb = 0, cbsb = 0, cbdb = 0;
+  if ((P(xpart) < 0) || (!ChargeComputationNeeded)) {
+    // all zero
+  } else if (capMod == 0) {
+    // capMod = 0 (:10718-11012), the simple charge model BSIM3 shares.
+    xdc::CvCharges cv;
+    xdc::cv_simple(Vbseff, Vbs, phi, Phis, dPhis_dVb, sqrtPhis, dsqrtPhis_dVb, P(vfbcv), P(k1ox), Vgs_eff,
+                   dVgs_eff_dVg, coxe * P(weffCV) * P(leffCV) * nf, Abulk0, dAbulk0_dVb, P(abulkCVfactor), Vds,
+                   P(xpart), false, cv);
+    qgate = cv.qgate, qbulk = cv.qbulk, qdrn = cv.qdrn;
+    cggb = cv.cggb, cgsb = cv.cgsb, cgdb = cv.cgdb, cdgb = cv.cdgb, cdsb = cv.cdsb, cddb = cv.cddb;
+    cbgb = cv.cbgb, cbsb = cv.cbsb, cbdb = cv.cbdb;
+  } else {
+    double VbseffCV, dVbseffCV_dVb;
+    if (Vbseff < 0.0) {
+      VbseffCV = Vbseff;
+      dVbseffCV_dVb = 1.0;
+    } else {
+      VbseffCV = phi - Phis;
+      dVbseffCV_dVb = -dPhis_dVb;
+    }
+    const double CoxWL = coxe * P(weffCV) * P(leffCV) * nf;
+    if (P(cvchargeMod) == 0.0) {
+      const double noff = n * P(noff);
+      const double dnoff_dVd = P(noff) * dn_dVd;
+      const double dnoff_dVb = P(noff) * dn_dVb;
+      T0 = Vtm * noff;
+      const double voffcv = P(voffcv);
+      const double VgstNVt = (Vgst - voffcv) / T0;
+      if (VgstNVt > CONSTEXP_THRESHOLD) {
+        Vgsteff = Vgst - voffcv;
+        dVgsteff_dVg = dVgs_eff_dVg;
+        dVgsteff_dVd = -dVth_dVd;
+        dVgsteff_dVb = -dVth_dVb;
+      } else if (VgstNVt < -CONSTEXP_THRESHOLD) {
+        Vgsteff = T0 * log(1.0 + CONSTMIN_EXP);
+        dVgsteff_dVg = 0.0;
+        dVgsteff_dVd = Vgsteff / noff;
+        dVgsteff_dVb = dVgsteff_dVd * dnoff_dVb;
+        dVgsteff_dVd *= dnoff_dVd;
+      } else {
+        const double ExpVgst = exp(VgstNVt);
+        Vgsteff = T0 * log(1.0 + ExpVgst);
+        dVgsteff_dVg = ExpVgst / (1.0 + ExpVgst);
+        dVgsteff_dVd = -dVgsteff_dVg * (dVth_dVd + (Vgst - voffcv) / noff * dnoff_dVd) + Vgsteff / noff * dnoff_dVd;
+        dVgsteff_dVb = -dVgsteff_dVg * (dVth_dVb + (Vgst - voffcv) / noff * dnoff_dVb) + Vgsteff / noff * dnoff_dVb;
+        dVgsteff_dVg *= dVgs_eff_dVg;
+      }
+    } else {
+      const double mstarcv = P(mstarcv);
+      T0 = n * Vtm;
+      T1 = mstarcv * Vgst;
+      T2 = T1 / T0;
+      if (T2 > CONSTEXP_THRESHOLD) {
+        T10 = T1;
+        dT10_dVg = mstarcv * dVgs_eff_dVg;
+        dT10_dVd = -dVth_dVd * mstarcv;
+        dT10_dVb = -dVth_dVb * mstarcv;
+      } else if (T2 < -CONSTEXP_THRESHOLD) {
+        T10 = Vtm * log(1.0 + CONSTMIN_EXP);
+        dT10_dVg = 0.0;
+        dT10_dVd = T10 * dn_dVd;
+        dT10_dVb = T10 * dn_dVb;
+        T10 *= n;
+      } else {
+        const double ExpVgst = exp(T2);
+        T3 = Vtm * log(1.0 + ExpVgst);
+        T10 = n * T3;
+        dT10_dVg = mstarcv * ExpVgst / (1.0 + ExpVgst);
+        dT10_dVb = T3 * dn_dVb - dT10_dVg * (dVth_dVb + Vgst * dn_dVb / n);
+        dT10_dVd = T3 * dn_dVd - dT10_dVg * (dVth_dVd + Vgst * dn_dVd / n);
+        dT10_dVg *= dVgs_eff_dVg;
+      }
+      T1 = P(voffcbncv) - (1.0 - mstarcv) * Vgst;
+      T2 = T1 / T0;
+      if (T2 < -CONSTEXP_THRESHOLD) {
+        T3 = coxe * CONSTMIN_EXP / P(cdep0);
+        T9 = mstarcv + T3 * n;
+        dT9_dVg = 0.0;
+        dT9_dVd = dn_dVd * T3;
+        dT9_dVb = dn_dVb * T3;
+      } else if (T2 > CONSTEXP_THRESHOLD) {
+        T3 = coxe * CONSTMAX_EXP / P(cdep0);
+        T9 = mstarcv + T3 * n;
+        dT9_dVg = 0.0;
+        dT9_dVd = dn_dVd * T3;
+        dT9_dVb = dn_dVb * T3;
+      } else {
+        const double ExpVgst = exp(T2);
+        T3 = coxe / P(cdep0);
+        T4 = T3 * ExpVgst;
+        T5 = T1 * T4 / T0;
+        T9 = mstarcv + n * T4;
+        dT9_dVg = T3 * (mstarcv - 1.0) * ExpVgst / Vtm;
+        dT9_dVb = T4 * dn_dVb - dT9_dVg * dVth_dVb - T5 * dn_dVb;
+        dT9_dVd = T4 * dn_dVd - dT9_dVg * dVth_dVd - T5 * dn_dVd;
+        dT9_dVg *= dVgs_eff_dVg;
+      }
+      Vgsteff = T10 / T9;
+      T11 = T9 * T9;
+      dVgsteff_dVg = (T9 * dT10_dVg - T10 * dT9_dVg) / T11;
+      dVgsteff_dVd = (T9 * dT10_dVd - T10 * dT9_dVd) / T11;
+      dVgsteff_dVb = (T9 * dT10_dVb - T10 * dT9_dVb) / T11;
+    }
+    if (capMod == 1) {
+      // capMod = 1 (:11139-11319): accumulation and depletion charges Qac0 / Qsub0 with the
+      // zero-bias flat band, the inversion charge without the charge-thickness correction.
+      const double Vfb1 = P(vfbzb);
+      double V3 = Vfb1 - Vgs_eff + VbseffCV - CONSTDELTA_3;
+      if (Vfb1 <= 0.0)
+        T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * Vfb1);
+      else
+        T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * Vfb1);
+      T1 = 0.5 * (1.0 + V3 / T0);
+      const double Vfbeff = Vfb1 - 0.5 * (V3 + T0);
+      const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
+      const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
+      const double Qac0 = CoxWL * (Vfbeff - Vfb1);
+      const double dQac0_dVg = CoxWL * dVfbeff_dVg;
+      const double dQac0_dVb = CoxWL * dVfbeff_dVb;
+      const double k1ox1 = P(k1ox);
+      T0 = 0.5 * k1ox1;
+      T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
+      if (k1ox1 == 0.0) {
+        T1 = 0.0;
+        T2 = 0.0;
+      } else if (T3 < 0.0) {
+        T1 = T0 + T3 / k1ox1;
+        T2 = CoxWL;
+      } else {
+        T1 = sqrt(T0 * T0 + T3);
+        T2 = CoxWL * T0 / T1;
+      }
+      const double Qsub0 = CoxWL * k1ox1 * (T1 - T0);
+      const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg);
+      const double dQsub0_dVd = -T2 * dVgsteff_dVd;
+      const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb);
+      const double AbulkCV = Abulk0 * P(abulkCVfactor);
+      const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+      const double VdsatCV = Vgsteff / AbulkCV;
+      T0 = VdsatCV - Vds - CONSTDELTA_4;
+      dT0_dVg = 1.0 / AbulkCV;
+      dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
+      T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
+      dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
+      dT1_dVd = -T0 / T1;
+      dT1_dVb = dT1_dVg * dT0_dVb;
+      dT1_dVg *= dT0_dVg;
+      double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
+      if (T0 >= 0.0) {
+        VdseffCV = VdsatCV - 0.5 * (T0 + T1);
+        dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
+        dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
+        dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
+      } else {
+        T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
+        T4 = 1.0 - T3;
+        T5 = VdsatCV * T3 / (T1 - T0);
+        VdseffCV = VdsatCV * T4;
+        dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
+        dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
+        dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
+      }
+      if (Vds == 0.0) {  // the reference leaves dVdseffCV_dVd as computed
+        VdseffCV = 0.0;
+        dVdseffCV_dVg = 0.0;
+        dVdseffCV_dVb = 0.0;
+      }
+      T0 = AbulkCV * VdseffCV;
+      T1 = 12.0 * (Vgsteff - 0.5 * T0 + 1.0e-20);
+      T2 = VdseffCV / T1;
+      T3 = T0 * T2;
+      T4 = (1.0 - 12.0 * T2 * T2 * AbulkCV);
+      T5 = (6.0 * T0 * (4.0 * Vgsteff - T0) / (T1 * T1) - 0.5);
+      T6 = 12.0 * T2 * T2 * Vgsteff;
+      qgate = CoxWL * (Vgsteff - 0.5 * VdseffCV + T3);
+      double Cgg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+      const double Cgd1 = CoxWL * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd;
+      const double Cgb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb;
+      Cgg1 *= dVgsteff_dVg;
+      T7 = 1.0 - AbulkCV;
+      qbulk = CoxWL * T7 * (0.5 * VdseffCV - T3);
+      T4 = -T7 * (T4 - 1.0);
+      T5 = -T7 * T5;
+      T6 = -(T7 * T6 + (0.5 * VdseffCV - T3));
+      double Cbg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+      const double Cbd1 = CoxWL * T5 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd;
+      const double Cbb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb;
+      Cbg1 *= dVgsteff_dVg;
+      double Csg, Csd, Csb;
+      const double xpart = P(xpart);
+      if (xpart > 0.5) {  // 0/100
+        T1 = T1 + T1;
+        qsrc = -CoxWL * (0.5 * Vgsteff + 0.25 * T0 - T0 * T0 / T1);
+        T7 = (4.0 * Vgsteff - T0) / (T1 * T1);
+        T4 = -(0.5 + 24.0 * T0 * T0 / (T1 * T1));
+        T5 = -(0.25 * AbulkCV - 12.0 * AbulkCV * T0 * T7);
+        T6 = -(0.25 * VdseffCV - 12.0 * T0 * VdseffCV * T7);
+        Csg = CoxWL * (T4 + T5 * dVdseffCV_dVg);
+        Csd = CoxWL * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
+        Csb = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
+        Csg *= dVgsteff_dVg;
+      } else if (xpart < 0.5) {  // 40/60
+        T1 = T1 / 12.0;
+        T2 = 0.5 * CoxWL / (T1 * T1);
+        T3 = Vgsteff * (2.0 * T0 * T0 / 3.0 + Vgsteff * (Vgsteff - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
+        qsrc = -T2 * T3;
+        T7 = 4.0 / 3.0 * Vgsteff * (Vgsteff - T0) + 0.4 * T0 * T0;
+        T4 = -2.0 * qsrc / T1 - T2 * (Vgsteff * (3.0 * Vgsteff - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
+        T5 = (qsrc / T1 + T2 * T7) * AbulkCV;
+        T6 = (qsrc / T1 * VdseffCV + T2 * T7 * VdseffCV);
+        Csg = (T4 + T5 * dVdseffCV_dVg);
+        Csd = T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
+        Csb = (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
+        Csg *= dVgsteff_dVg;
+      } else {  // 50/50
+        qsrc = -0.5 * (qgate + qbulk);
+        Csg = -0.5 * (Cgg1 + Cbg1);
+        Csb = -0.5 * (Cgb1 + Cbb1);
+        Csd = -0.5 * (Cgd1 + Cbd1);
+      }
+      qgate += Qac0 + Qsub0;
+      qbulk -= (Qac0 + Qsub0);
+      qdrn = -(qgate + qbulk + qsrc);
+      const double Cgg = dQac0_dVg + dQsub0_dVg + Cgg1;
+      const double Cgd = dQsub0_dVd + Cgd1;
+      double Cgb = dQac0_dVb + dQsub0_dVb + Cgb1;
+      const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
+      const double Cbd = Cbd1 - dQsub0_dVd;
+      double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
+      Cgb *= dVbseff_dVb;
+      Cbb *= dVbseff_dVb;
+      Csb *= dVbseff_dVb;
+      cggb = Cgg;
+      cgsb = -(Cgg + Cgd + Cgb);
+      cgdb = Cgd;
+      cdgb = -(Cgg + Cbg + Csg);
+      cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
+      cddb = -(Cgd + Cbd + Csd);
+      cbgb = Cbg;
+      cbsb = -(Cbg + Cbd + Cbb);
+      cbdb = Cbd;
+    } else {
+    // capMod == 2
+    const double vfbzb = P(vfbzb);
+    double V3 = vfbzb - Vgs_eff + VbseffCV - CONSTDELTA_3;
+    if (vfbzb <= 0.0)
+      T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * vfbzb);
+    else
+      T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * vfbzb);
+    T1 = 0.5 * (1.0 + V3 / T0);
+    const double Vfbeff = vfbzb - 0.5 * (V3 + T0);
+    const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
+    const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
+    const double Cox = coxp;
+    double Tox = 1.0e8 * P(toxp);
+    T0 = (Vgs_eff - VbseffCV - vfbzb) / Tox;
+    dT0_dVg = dVgs_eff_dVg / Tox;
+    dT0_dVb = -dVbseffCV_dVb / Tox;
+    tmp = T0 * P(acde);
+    const double ldeb = P(ldeb);
+    double dTcen_dVb, dTcen_dVd;
+    if ((-CONSTEXP_THRESHOLD < tmp) && (tmp < CONSTEXP_THRESHOLD)) {
+      Tcen = ldeb * exp(tmp);
+      dTcen_dVg = P(acde) * Tcen;
+      dTcen_dVb = dTcen_dVg * dT0_dVb;
+      dTcen_dVg *= dT0_dVg;
+    } else if (tmp <= -CONSTEXP_THRESHOLD) {
+      Tcen = ldeb * CONSTMIN_EXP;
+      dTcen_dVg = dTcen_dVb = 0.0;
+    } else {
+      Tcen = ldeb * CONSTMAX_EXP;
+      dTcen_dVg = dTcen_dVb = 0.0;
+    }
+    const double LINK = 1.0e-3 * P(toxp);
+    V3 = ldeb - Tcen - LINK;
+    const double V4 = sqrt(V3 * V3 + 4.0 * LINK * ldeb);
+    Tcen = ldeb - 0.5 * (V3 + V4);
+    T1 = 0.5 * (1.0 + V3 / V4);
+    dTcen_dVg *= T1;
+    dTcen_dVb *= T1;
+    double Ccen = epssub / Tcen;
+    T2 = Cox / (Cox + Ccen);
+    Coxeff = T2 * Ccen;
+    T3 = -Ccen / Tcen;
+    dCoxeff_dVg = T2 * T2 * T3;
+    double dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
+    dCoxeff_dVg *= dTcen_dVg;
+    double CoxWLcen = CoxWL * Coxeff / coxe;
+    const double Qac0 = CoxWLcen * (Vfbeff - vfbzb);
+    double QovCox = Qac0 / Coxeff;
+    const double dQac0_dVg = CoxWLcen * dVfbeff_dVg + QovCox * dCoxeff_dVg;
+    const double dQac0_dVb = CoxWLcen * dVfbeff_dVb + QovCox * dCoxeff_dVb;
+    T0 = 0.5 * k1ox;
+    T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
+    if (k1ox == 0.0) {
+      T1 = 0.0;
+      T2 = 0.0;
+    } else if (T3 < 0.0) {
+      T1 = T0 + T3 / k1ox;
+      T2 = CoxWLcen;
+    } else {
+      T1 = sqrt(T0 * T0 + T3);
+      T2 = CoxWLcen * T0 / T1;
+    }
+    const double Qsub0 = CoxWLcen * k1ox * (T1 - T0);
+    QovCox = Qsub0 / Coxeff;
+    const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg) + QovCox * dCoxeff_dVg;
+    const double dQsub0_dVd = -T2 * dVgsteff_dVd;
+    const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb) + QovCox * dCoxeff_dVb;
+    if (k1ox <= 0.0) {
+      Denomi = 0.25 * P(moin) * Vtm;
+      T0 = 0.5 * sqrtPhi_p;
+    } else {
+      Denomi = P(moin) * Vtm * k1ox * k1ox;
+      T0 = k1ox * sqrtPhi_p;
+    }
+    T1 = 2.0 * T0 + Vgsteff;
+    const double DeltaPhi = Vtm * log(1.0 + T1 * Vgsteff / Denomi);
+    const double dDeltaPhi_dVg = 2.0 * Vtm * (T1 - T0) / (Denomi + T1 * Vgsteff);
+    T0 = Vgsteff - DeltaPhi - 0.001;
+    dT0_dVg = 1.0 - dDeltaPhi_dVg;
+    T1 = sqrt(T0 * T0 + Vgsteff * 0.004);
+    const double VgDP = 0.5 * (T0 + T1);
+    const double dVgDP_dVg = 0.5 * (dT0_dVg + (T0 * dT0_dVg + 0.002) / T1);
+    Tox += Tox;
+    T0 = (Vgsteff + P(vtfbphi2)) / Tox;
+    tmp = exp(P(bdos) * 0.7 * log(T0));
+    T1 = 1.0 + tmp;
+    T2 = P(bdos) * 0.7 * tmp / (T0 * Tox);
+    Tcen = P(ados) * 1.9e-9 / T1;
+    dTcen_dVg = -Tcen * T2 / T1;
+    dTcen_dVd = dTcen_dVg * dVgsteff_dVd;
+    dTcen_dVb = dTcen_dVg * dVgsteff_dVb;
+    dTcen_dVg *= dVgsteff_dVg;
+    Ccen = epssub / Tcen;
+    T0 = Cox / (Cox + Ccen);
+    Coxeff = T0 * Ccen;
+    T1 = -Ccen / Tcen;
+    dCoxeff_dVg = T0 * T0 * T1;
+    const double dCoxeff_dVd = dCoxeff_dVg * dTcen_dVd;
+    dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
+    dCoxeff_dVg *= dTcen_dVg;
+    CoxWLcen = CoxWL * Coxeff / coxe;
+    const double AbulkCV = Abulk0 * P(abulkCVfactor);
+    const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
+    const double VdsatCV = VgDP / AbulkCV;
+    T0 = VdsatCV - Vds - CONSTDELTA_4;
+    dT0_dVg = dVgDP_dVg / AbulkCV;
+    dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
+    dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
+    dT1_dVd = -T0 / T1;
+    dT1_dVb = dT1_dVg * dT0_dVb;
+    dT1_dVg *= dT0_dVg;
+    double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
+    if (T0 >= 0.0) {
+      VdseffCV = VdsatCV - 0.5 * (T0 + T1);
+      dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
+      dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
+      dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
+    } else {
+      T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
+      T4 = 1.0 - T3;
+      T5 = VdsatCV * T3 / (T1 - T0);
+      VdseffCV = VdsatCV * T4;
+      dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
+      dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
+      dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
+    }
+    if (Vds == 0.0) {
+      VdseffCV = 0.0;
+      dVdseffCV_dVg = 0.0;
+      dVdseffCV_dVb = 0.0;
+    }
+    T0 = AbulkCV * VdseffCV;
+    T1 = VgDP;
+    T2 = 12.0 * (T1 - 0.5 * T0 + 1.0e-20);
+    T3 = T0 / T2;
+    T4 = 1.0 - 12.0 * T3 * T3;
+    T5 = AbulkCV * (6.0 * T0 * (4.0 * T1 - T0) / (T2 * T2) - 0.5);
+    T6 = T5 * VdseffCV / AbulkCV;
+    qgate = CoxWLcen * (T1 - T0 * (0.5 - T3));
+    QovCox = qgate / Coxeff;
+    double Cgg1 = CoxWLcen * (T4 * dVgDP_dVg + T5 * dVdseffCV_dVg);
+    const double Cgd1 = CoxWLcen * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+    const double Cgb1 = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+    Cgg1 = Cgg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    T7 = 1.0 - AbulkCV;
+    T8 = T2 * T2;
+    T9 = 12.0 * T7 * T0 * T0 / (T8 * AbulkCV);
+    T10 = T9 * dVgDP_dVg;
+    T11 = -T7 * T5 / AbulkCV;
+    T12 = -(T9 * T1 / AbulkCV + VdseffCV * (0.5 - T0 / T2));
+    qbulk = CoxWLcen * T7 * (0.5 * VdseffCV - T0 * VdseffCV / T2);
+    QovCox = qbulk / Coxeff;
+    double Cbg1 = CoxWLcen * (T10 + T11 * dVdseffCV_dVg);
+    const double Cbd1 = CoxWLcen * T11 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+    const double Cbb1 = CoxWLcen * (T11 * dVdseffCV_dVb + T12 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+    Cbg1 = Cbg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    double Csg, Csd, Csb;
+    const double xpart = P(xpart);
+    if (xpart > 0.5) {
+      qsrc = -CoxWLcen * (T1 / 2.0 + T0 / 4.0 - 0.5 * T0 * T0 / T2);
+      QovCox = qsrc / Coxeff;
+      T2 += T2;
+      T3 = T2 * T2;
+      T7 = -(0.25 - 12.0 * T0 * (4.0 * T1 - T0) / T3);
+      T4 = -(0.5 + 24.0 * T0 * T0 / T3) * dVgDP_dVg;
+      T5 = T7 * AbulkCV;
+      T6 = T7 * VdseffCV;
+      Csg = CoxWLcen * (T4 + T5 * dVdseffCV_dVg);
+      Csd = CoxWLcen * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd + QovCox * dCoxeff_dVd;
+      Csb = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb + QovCox * dCoxeff_dVb;
+      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    } else if (xpart < 0.5) {
+      T2 = T2 / 12.0;
+      T3 = 0.5 * CoxWLcen / (T2 * T2);
+      T4 = T1 * (2.0 * T0 * T0 / 3.0 + T1 * (T1 - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
+      qsrc = -T3 * T4;
+      QovCox = qsrc / Coxeff;
+      T8 = 4.0 / 3.0 * T1 * (T1 - T0) + 0.4 * T0 * T0;
+      T5 = -2.0 * qsrc / T2 - T3 * (T1 * (3.0 * T1 - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
+      T6 = AbulkCV * (qsrc / T2 + T3 * T8);
+      T7 = T6 * VdseffCV / AbulkCV;
+      Csg = T5 * dVgDP_dVg + T6 * dVdseffCV_dVg;
+      Csd = Csg * dVgsteff_dVd + T6 * dVdseffCV_dVd + QovCox * dCoxeff_dVd;
+      Csb = Csg * dVgsteff_dVb + T6 * dVdseffCV_dVb + T7 * dAbulkCV_dVb + QovCox * dCoxeff_dVb;
+      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
+    } else {
+      qsrc = -0.5 * qgate;
+      Csg = -0.5 * Cgg1;
+      Csd = -0.5 * Cgd1;
+      Csb = -0.5 * Cgb1;
+    }
+    qgate += Qac0 + Qsub0 - qbulk;
+    qbulk -= (Qac0 + Qsub0);
+    qdrn = -(qgate + qbulk + qsrc);
+    const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
+    const double Cbd = Cbd1 - dQsub0_dVd;
+    double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
+    const double Cgg = Cgg1 - Cbg;
+    const double Cgd = Cgd1 - Cbd;
+    double Cgb = Cgb1 - Cbb;
+    Cgb *= dVbseff_dVb;
+    Cbb *= dVbseff_dVb;
+    Csb *= dVbseff_dVb;
+    cggb = Cgg;
+    cgsb = -(Cgg + Cgd + Cgb);
+    cgdb = Cgd;
+    cdgb = -(Cgg + Cbg + Csg);
+    cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
+    cddb = -(Cgd + Cbd + Csd);
+    cbgb = Cbg;
+    cbsb = -(Cbg + Cbd + Cbb);
+    cbdb = Cbd;
+    }
+  }
+
+  // Junction charges and capacitances (:11661-11810). Outside charge computation the reference
+  // keeps the previous load's junction values; they only feed Q and dQ/dx, which a DC solve does
+  // not use, and are zero here.
+  double qbs = 0.0, qbd = 0.0, capbs = 0.0, capbd = 0.0;
+  if (ChargeComputationNeeded) {
+    const double czbd = P(DunitAreaTempJctCap) * Adeff;
+    const double czbs = P(SunitAreaTempJctCap) * Aseff;
+    const double czbdsw = P(DunitLengthSidewallTempJctCap) * Pdeff;
+    const double czbdswg = P(DunitLengthGateSidewallTempJctCap) * weffCJ * nf;
+    const double czbssw = P(SunitLengthSidewallTempJctCap) * Pseff;
+    const double czbsswg = P(SunitLengthGateSidewallTempJctCap) * weffCJ * nf;
+    const double MJS = P(SbulkJctBotGradingCoeff), MJSWS = P(SbulkJctSideGradingCoeff);
+    const double MJSWGS = P(SbulkJctGateSideGradingCoeff);
+    const double MJD = P(DbulkJctBotGradingCoeff), MJSWD = P(DbulkJctSideGradingCoeff);
+    const double MJSWGD = P(DbulkJctGateSideGradingCoeff);
+    double arg, sarg;
+    if (vbs_jct == 0.0) {
+      qbs = 0.0;
+      capbs = czbs + czbssw + czbsswg;
+    } else if (vbs_jct < 0.0) {
+      if (czbs > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBS);
+        if (MJS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJS * log(arg));
+        qbs = P(PhiBS) * czbs * (1.0 - arg * sarg) / (1.0 - MJS);
+        capbs = czbs * sarg;
+      } else {
+        qbs = 0.0;
+        capbs = 0.0;
+      }
+      if (czbssw > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBSWS);
+        if (MJSWS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWS * log(arg));
+        qbs += P(PhiBSWS) * czbssw * (1.0 - arg * sarg) / (1.0 - MJSWS);
+        capbs += czbssw * sarg;
+      }
+      if (czbsswg > 0.0) {
+        arg = 1.0 - vbs_jct / P(PhiBSWGS);
+        if (MJSWGS == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWGS * log(arg));
+        qbs += P(PhiBSWGS) * czbsswg * (1.0 - arg * sarg) / (1.0 - MJSWGS);
+        capbs += czbsswg * sarg;
+      }
+    } else {
+      T0 = czbs + czbssw + czbsswg;
+      T1 = vbs_jct * (czbs * MJS / P(PhiBS) + czbssw * MJSWS / P(PhiBSWS) + czbsswg * MJSWGS / P(PhiBSWGS));
+      qbs = vbs_jct * (T0 + 0.5 * T1);
+      capbs = T0 + T1;
+    }
+    if (vbd_jct == 0.0) {
+      qbd = 0.0;
+      capbd = czbd + czbdsw + czbdswg;
+    } else if (vbd_jct < 0.0) {
+      if (czbd > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBD);
+        if (MJD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJD * log(arg));
+        qbd = P(PhiBD) * czbd * (1.0 - arg * sarg) / (1.0 - MJD);
+        capbd = czbd * sarg;
+      } else {
+        qbd = 0.0;
+        capbd = 0.0;
+      }
+      if (czbdsw > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBSWD);
+        if (MJSWD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWD * log(arg));
+        qbd += P(PhiBSWD) * czbdsw * (1.0 - arg * sarg) / (1.0 - MJSWD);
+        capbd += czbdsw * sarg;
+      }
+      if (czbdswg > 0.0) {
+        arg = 1.0 - vbd_jct / P(PhiBSWGD);
+        if (MJSWGD == 0.5)
+          sarg = 1.0 / sqrt(arg);
+        else
+          sarg = exp(-MJSWGD * log(arg));
+        qbd += P(PhiBSWGD) * czbdswg * (1.0 - arg * sarg) / (1.0 - MJSWGD);
+        capbd += czbdswg * sarg;
+      }
+    } else {
+      T0 = czbd + czbdsw + czbdswg;
+      T1 = vbd_jct * (czbd * MJD / P(PhiBD) + czbdsw * MJSWD / P(PhiBSWD) + czbdswg * MJSWGD / P(PhiBSWGD));
+      qbd = vbd_jct * (T0 + 0.5 * T1);
+      capbd = T0 + T1;
+    }
+  }
+
+  // Overlap capacitances (:11846-11890): constant for capMod 0, bias-dependent for 1 and 2.
+  const double vgdx = vgd, vgsx = vgs;
+  double cgdo, qgdo, cgso, qgso;
+  if (capMod == 0) {
+    cgdo = P(cgdo);
+    qgdo = P(cgdo) * vgdx;
+    cgso = P(cgso);
+    qgso = P(cgso) * vgsx;
+  } else {
+    T0 = vgdx + CONSTDELTA_1;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+    T2 = 0.5 * (T0 - T1);
+    T3 = P(weffCV) * P(cgdl);
+    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappad));
+    cgdo = P(cgdo) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+    qgdo = (P(cgdo) + T3) * vgdx - T3 * (T2 + 0.5 * P(ckappad) * (T4 - 1.0));
+    T0 = vgsx + CONSTDELTA_1;
+    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
+    T2 = 0.5 * (T0 - T1);
+    T3 = P(weffCV) * P(cgsl);
+    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappas));
+    cgso = P(cgso) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
+    qgso = (P(cgso) + T3) * vgsx - T3 * (T2 + 0.5 * P(ckappas) * (T4 - 1.0));
+  }
+  if (nf != 1.0) {
+    cgdo *= nf;
+    cgso *= nf;
+    qgdo *= nf;
+    qgso *= nf;
+  }
+
+  // Overlap and gate-bulk charge bookkeeping (setupCapacitors_oldDAE, trnqsMod = 0, :12624-12760).
+  const double cgbo = P(cgbo);
+  double dxpart, sxpart;
+  if (mode > 0) {
+    qdrn -= qgdo;
+    const double qgb = cgbo * vgb;
+    qgate += qgdo + qgso + qgb;
+    qbulk -= qgb;
+    qsrc = -(qgate + qbulk + qdrn);
+    sxpart = 0.6;
+    dxpart = 0.4;
+  } else {
+    qsrc = qdrn - qgso;
+    const double qgb = cgbo * vgb;
+    qgate += qgdo + qgso + qgb;
+    qbulk -= qgb;
+    qdrn = -(qgate + qbulk + qsrc);
+    sxpart = 0.4;
+    dxpart = 0.6;
+  }
+  (void)qsrc;
+
+  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = rgateMod = rbodyMod = 0).
+  double CAPcggb, CAPcgdb, CAPcgsb, CAPcgbb, CAPcdgb, CAPcsgb, CAPcbgb, CAPcddb, CAPcdsb, CAPcsdb, CAPcssb;
+  double CAPcdbb, CAPcsbb, CAPcbdb, CAPcbsb, CAPcbbb;
+  const double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
+  if (mode > 0) {
+    CAPcggb = (cggb + cgdo + cgso + cgbo);
+    CAPcgdb = (cgdb - cgdo);
+    CAPcgsb = (cgsb - cgso);
+    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+    CAPcdgb = (cdgb - cgdo);
+    CAPcsgb = -(cggb + cbgb + cdgb + cgso);
+    CAPcbgb = (cbgb - cgbo);
+    CAPcddb = (cddb + capbd + cgdo);
+    CAPcdsb = cdsb;
+    CAPcsdb = -(cgdb + cbdb + cddb);
+    CAPcssb = (capbs + cgso - (cgsb + cbsb + cdsb));
+    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+    CAPcbdb = (cbdb - capbd);
+    CAPcbsb = (cbsb - capbs);
+    CAPcbbb = -(CAPcbdb + CAPcbgb + CAPcbsb + CAPcbgmb);
+  } else {
+    CAPcggb = (cggb + cgdo + cgso + cgbo);
+    CAPcgdb = (cgsb - cgdo);
+    CAPcgsb = (cgdb - cgso);
+    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+    CAPcdgb = -(cggb + cbgb + cdgb + cgdo);
+    CAPcsgb = (cdgb - cgso);
+    CAPcbgb = (cbgb - cgbo);
+    CAPcddb = (capbd + cgdo - (cgsb + cbsb + cdsb));
+    CAPcdsb = -(cgdb + cbdb + cddb);
+    CAPcsdb = cdsb;
+    CAPcssb = (cddb + capbs + cgso);
+    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+    CAPcbdb = (cbsb - capbd);
+    CAPcbsb = (cbdb - capbs);
+    CAPcbbb = -(CAPcbgb + CAPcbdb + CAPcbsb + CAPcbgmb);
+  }
+
+  // Master::updateState: store and state (:16195-16242).
+  o.sto[s_vbd] = vbd;
+  o.sto[s_vbs] = vbs;
+  o.sto[s_vgs] = vgs;
+  o.sto[s_vds] = vds;
+  o.sto[s_vges] = vges;
+  o.sto[s_vgms] = vgms;
+  o.sto[s_vdes] = vdes;
+  o.sto[s_vses] = vses;
+  o.sto[s_vdbs] = vdbs;
+  o.sto[s_vsbs] = vsbs;
+  o.sto[s_vdbd] = vdbd;
+  o.sto[s_vged] = 0.0;
+  o.sto[s_vgmd] = 0.0;
+  o.sto[s_von] = von;
+  const double qg = qgate;
+  const double qd = qdrn - qbd;
+  const double qb = qbulk + qbd + qbs;
+  o.sta[t_qg] = qg;
+  o.sta[t_qd] = qd;
+  o.sta[t_qb] = qb;
+  o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
+  o.vgb = vgb;
+
+  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0.
+  const double gjbd = gbd, gjbs = gbs;
+  double Gmv, Gmbsv, FwdSum, RevSum, ceqdrn, ceqdrn_Jdxp, ceqbd, ceqbd_Jdxp, ceqbs, ceqbs_Jdxp;
+  double gbbdp, gbbsp, gbdpg, gbdpdp, gbdpb, gbdpsp, gbspg, gbspdp, gbspb, gbspsp;
+  if (mode >= 0) {
+    Gmv = gm;
+    Gmbsv = gmbs;
+    FwdSum = Gmv + Gmbsv;
+    RevSum = 0.0;
+    ceqdrn = dtype * cdrain;
+    ceqdrn_Jdxp = dtype * (-gds * (vds - vds_orig) - Gmv * (vgs - vgs_orig) - Gmbsv * (vbs - vbs_orig));
+    ceqbd = dtype * (csub + Igidl);
+    ceqbd_Jdxp = dtype * (-(gbds + ggidld) * (vds - vds_orig) - (gbgs + ggidlg) * (vgs - vgs_orig) -
+                          (gbbs + ggidlb) * (vbs - vbs_orig));
+    ceqbs = dtype * Igisl;
+    ceqbs_Jdxp = dtype * (+ggisls * (vds - vds_orig) - ggislg * (vgd - vgd_orig) - ggislb * (vbd - vbd_orig));
+    gbbdp = -(gbds);
+    gbbsp = gbds + gbgs + gbbs;
+    gbdpg = gbgs;
+    gbdpdp = gbds;
+    gbdpb = gbbs;
+    gbdpsp = -(gbdpg + gbdpdp + gbdpb);
+    gbspg = 0.0;
+    gbspdp = 0.0;
+    gbspb = 0.0;
+    gbspsp = 0.0;
+  } else {
+    Gmv = -gm;
+    Gmbsv = -gmbs;
+    FwdSum = 0.0;
+    RevSum = -(Gmv + Gmbsv);
+    ceqdrn = -dtype * cdrain;
+    ceqdrn_Jdxp = -dtype * (+gds * (vds - vds_orig) + Gmv * (vgd - vgd_orig) + Gmbsv * (vbd - vbd_orig));
+    ceqbs = dtype * (csub + Igisl);
+    ceqbs_Jdxp = dtype * (+(gbds + ggisls) * (vds - vds_orig) - (gbgs + ggislg) * (vgd - vgd_orig) -
+                          (gbbs + ggislb) * (vbd - vbd_orig));
+    ceqbd = dtype * Igidl;
+    ceqbd_Jdxp = dtype * (-ggidld * (vds - vds_orig) - ggidlg * (vgs - vgs_orig) - ggidlb * (vbs - vbs_orig));
+    gbbsp = -(gbds);
+    gbbdp = gbds + gbgs + gbbs;
+    gbdpg = 0.0;
+    gbdpsp = 0.0;
+    gbdpb = 0.0;
+    gbdpdp = 0.0;
+    gbspg = gbgs;
+    gbspsp = gbds;
+    gbspb = gbbs;
+    gbspdp = -(gbspg + gbspsp + gbspb);
+  }
+  // Gate-current totals (:13112-13170, mode >= 0; :13243-13300, mode < 0).
+  const double ceqgcrg = 0.0, ceqgcrg_Jdxp = 0.0;
+  double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0;
+  double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0;
+  double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
+  double gIdtotg = 0.0, gIdtotd = 0.0, gIdtots = 0.0, gIdtotb = 0.0;
+  double gIbtotg = 0.0, gIbtotd = 0.0, gIbtots = 0.0, gIbtotb = 0.0;
+  double gIgtotg = 0.0, gIgtotd = 0.0, gIgtots = 0.0, gIgtotb = 0.0;
+  if (mode >= 0) {
+    if (igcMod) {
+      gIstotg = gIgsg + gIgcsg;
+      gIstotd = gIgcsd;
+      gIstots = gIgss + gIgcss;
+      gIstotb = gIgcsb;
+      Istoteq = dtype * (Igs + Igcs);
+      Istoteq_Jdxp = dtype * (-gIstotg * (vgs - vgs_orig) - gIgcsd * (vds - vds_orig) - gIgcsb * (vbs - vbs_orig));
+      gIdtotg = gIgdg + gIgcdg;
+      gIdtotd = gIgdd + gIgcdd;
+      gIdtots = gIgcds;
+      gIdtotb = gIgcdb;
+      Idtoteq = dtype * (Igd + Igcd);
+      Idtoteq_Jdxp = dtype * (-gIgdg * (vgd - vgd_orig) - gIgcdg * (vgs - vgs_orig) - gIgcdd * (vds - vds_orig) -
+                              gIgcdb * (vbs - vbs_orig));
+    }
+    if (igbMod) {
+      gIbtotg = gIgbg;
+      gIbtotd = gIgbd;
+      gIbtots = gIgbs;
+      gIbtotb = gIgbb;
+      Ibtoteq = dtype * Igb;
+      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgs - vgs_orig) - gIgbd * (vds - vds_orig) - gIgbb * (vbs - vbs_orig));
+    }
+  } else {
+    if (igcMod) {
+      gIstotg = gIgsg + gIgcdg;
+      gIstotd = gIgcds;
+      gIstots = gIgss + gIgcdd;
+      gIstotb = gIgcdb;
+      Istoteq = dtype * (Igs + Igcd);
+      Istoteq_Jdxp = dtype * (-gIgsg * (vgs - vgs_orig) - gIgcdg * (vgd - vgd_orig) + gIgcdd * (vds - vds_orig) -
+                              gIgcdb * (vbd - vbd_orig));
+      gIdtotg = gIgdg + gIgcsg;
+      gIdtotd = gIgdd + gIgcss;
+      gIdtots = gIgcsd;
+      gIdtotb = gIgcsb;
+      Idtoteq = dtype * (Igd + Igcs);
+      Idtoteq_Jdxp = dtype * (-(gIgdg + gIgcsg) * (vgd - vgd_orig) + gIgcsd * (vds - vds_orig) -
+                              gIgcsb * (vbd - vbd_orig));
+    }
+    if (igbMod) {
+      gIbtotg = gIgbg;
+      gIbtotd = gIgbs;
+      gIbtots = gIgbd;
+      gIbtotb = gIgbb;
+      Ibtoteq = dtype * Igb;
+      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgd - vgd_orig) + gIgbd * (vds - vds_orig) - gIgbb * (vbd - vbd_orig));
+    }
+  }
+  if (igcMod != 0 || igbMod != 0) {
+    gIgtotg = gIstotg + gIdtotg + gIbtotg;
+    gIgtotd = gIstotd + gIdtotd + gIbtotd;
+    gIgtots = gIstots + gIdtots + gIbtots;
+    gIgtotb = gIstotb + gIdtotb + gIbtotb;
+    Igtoteq = Istoteq + Idtoteq + Ibtoteq;
+    Igtoteq_Jdxp = Istoteq_Jdxp + Idtoteq_Jdxp + Ibtoteq_Jdxp;
+  }
+  const double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
+  const double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
+  double ceqjs, ceqjs_Jdxp, ceqjd, ceqjd_Jdxp;
+  if (dtype > 0) {
+    ceqjs = (cbs);
+    ceqjs_Jdxp = (-gbs * (vbs_jct - vbs_jct_orig));
+    ceqjd = (cbd);
+    ceqjd_Jdxp = (-gbd * (vbd_jct - vbd_jct_orig));
+  } else {
+    ceqjs = -(cbs);
+    ceqjs_Jdxp = (gbs * (vbs_jct - vbs_jct_orig));
+    ceqjd = -(cbd);
+    ceqjd_Jdxp = (gbd * (vbd_jct - vbd_jct_orig));
+  }
+
+  // Master::loadDAEVectors (:16316-16564). Local order D, G, S, B.
+  const bool lim = fl.voltlim && !origFlag;
+  for (int k = 0; k < kNumVec; ++k) o.vec[k] = 0.0;
+  o.vec[0] += -(ceqjd - ceqbd - ceqdrn + Idtoteq) * M;
+  o.vec[1] -= -(-ceqgcrg + Igtoteq) * M;
+  o.vec[3] += -(ceqbd + ceqbs - ceqjd - ceqjs + Ibtoteq) * M;
+  o.vec[2] += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
+  if (SERIES) {
+    // Linear terminal resistor currents (:11901-11904, 16360-16370), where the node exists.
+    o.vecx[0] = 0.0;
+    o.vecx[1] = 0.0;
+    if (P(dExists) != 0.0) {
+      const double Idrain = P(drainConductance) * Vddp;
+      o.vecx[0] += -(-Idrain) * M;
+      o.vec[0] += -(Idrain)*M;
+    }
+    if (P(sExists) != 0.0) {
+      const double Isource = P(sourceConductance) * Vssp;
+      o.vecx[1] += -(-Isource) * M;
+      o.vec[2] += -(+Isource) * M;
+    }
+  }
+  if (lim) {
+    o.vec[8 + 0] += (ceqjd_Jdxp - ceqbd_Jdxp - ceqdrn_Jdxp + Idtoteq_Jdxp) * M;
+    o.vec[8 + 1] -= (-ceqgcrg_Jdxp + Igtoteq_Jdxp) * M;
+    o.vec[8 + 3] += (ceqbd_Jdxp + ceqbs_Jdxp - ceqjd_Jdxp - ceqjs_Jdxp + Ibtoteq_Jdxp) * M;
+    o.vec[8 + 2] += (ceqdrn_Jdxp - ceqbs_Jdxp + ceqjs_Jdxp + Istoteq_Jdxp) * M;
+  }
+  // auxChargeCalculations (:12216-12350).
+  double Qeqqg_Jdxp = 0.0, Qeqqd_Jdxp = 0.0, Qeqqb_Jdxp = 0.0;
+  if (ChargeComputationNeeded && !origFlag) {
+    Qeqqg_Jdxp = -CAPcggb * (vgb - vgb_orig) + CAPcgdb * (vbd - vbd_orig) + CAPcgsb * (vbs - vbs_orig);
+    Qeqqd_Jdxp = -CAPcdgb * (vgb - vgb_orig) - CAPcdgmb * (vgmb - vgmb_orig) +
+                 (CAPcddb + 0.0) * (vbd - vbd_orig) - 0.0 * (vbd_jct - vbd_jct_orig) + CAPcdsb * (vbs - vbs_orig);
+    Qeqqb_Jdxp = -CAPcbgb * (vgb - vgb_orig) - CAPcbgmb * (vgmb - vgmb_orig) + CAPcbdb * (vbd - vbd_orig) +
+                 CAPcbsb * (vbs - vbs_orig);
+  }
+  const double Qeqqgmid_Jdxp = 0.0, Qeqqgmid = 0.0;
+  double Qeqqg, Qeqqd, Qeqqb;
+  if (dtype > 0) {
+    Qeqqg = qg;
+    Qeqqd = qd;
+    Qeqqb = qb;
+  } else {
+    Qeqqg = -qg;
+    Qeqqd = -qd;
+    Qeqqb = -qb;
+  }
+  o.vec[4 + 0] += -(-Qeqqd) * M;
+  o.vec[4 + 1] -= -(Qeqqg) * M;
+  o.vec[4 + 3] += -(-Qeqqb) * M;
+  o.vec[4 + 2] += -(+Qeqqg + Qeqqb + Qeqqd + Qeqqgmid) * M;
+  if (lim) {
+    o.vec[12 + 0] += (-Qeqqd_Jdxp) * M;
+    o.vec[12 + 1] -= (Qeqqg_Jdxp) * M;
+    o.vec[12 + 3] += (-Qeqqb_Jdxp) * M;
+    o.vec[12 + 2] += (+Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqd_Jdxp + Qeqqgmid_Jdxp) * M;
+  }
+
+  // Master::loadDAEMatrices (:16577-17268). Rows/cols D=0 G=1 S=2 B=3.
+  for (int k = 0; k < kNumMat; ++k) {
+    o.jf[k] = 0.0;
+    o.jq[k] = 0.0;
+  }
+  const double gdpr = P(drainConductance), gspr = P(sourceConductance);
+  const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
+  const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
+  const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
+  const double Tq = 0.0;  // qdef * gtau with no NQS charge
+#define JF(r, c) o.jf[(r)*4 + (c)]
+#define JQ(r, c) o.jq[(r)*4 + (c)]
+  JF(1, 1) += (-ggtg + gIgtotg) * M;
+  JF(1, 0) += (-ggtd + gIgtotd) * M;
+  JF(1, 2) += (-ggts + gIgtots) * M;
+  JF(1, 3) += (-ggtb + gIgtotb) * M;
+  JF(0, 0) += (gdpr + gds + gbd + Tq * ddxpart_dVd - gdtotd + RevSum + gbdpdp + dxpart * ggtd - gIdtotd) * M;
+  if (SERIES) {
+    for (int k = 0; k < 6; ++k) o.jfx[k] = 0.0;
+  }
+  // The resistor couplings (D', D), (D, D'), (D, D) and the source's: their own slots with internal
+  // nodes, the collapsed (D, D) / (S, S) entry otherwise.
+#define JRES(k, r) (*(SERIES ? &o.jfx[k] : &JF(r, r)))
+  JRES(0, 0) -= (gdpr + gdtot) * M;
+  JF(0, 1) += (Gmv - gdtotg + gbdpg - gIdtotg + dxpart * ggtg + Tq * ddxpart_dVg) * M;
+  JF(0, 2) -= (gds + gdtots - dxpart * ggts + gIdtots - Tq * ddxpart_dVs + FwdSum - gbdpsp) * M;
+  JF(0, 3) -= (gjbd + gdtotb - Gmbsv - gbdpb + gIdtotb - Tq * ddxpart_dVb - dxpart * ggtb) * M;
+  JRES(1, 0) -= (gdpr - gdtotd) * M;
+  JRES(2, 0) += (gdpr + gdtot) * M;
+  JF(2, 0) -= (gds + gstotd + RevSum - gbspdp - Tq * dsxpart_dVd - sxpart * ggtd + gIstotd) * M;
+  JF(2, 1) += (-Gmv - gstotg + gbspg + sxpart * ggtg + Tq * dsxpart_dVg - gIstotg) * M;
+  JF(2, 2) += (gspr + gds + gbs + Tq * dsxpart_dVs - gstots + FwdSum + gbspsp + sxpart * ggts - gIstots) * M;
+  JRES(3, 2) -= (gspr + gstot) * M;
+  JF(2, 3) -= (gjbs + gstotb + Gmbsv - gbspb - sxpart * ggtb - Tq * dsxpart_dVb + gIstotb) * M;
+  JRES(4, 2) -= (gspr - gstots) * M;
+  JRES(5, 2) += (gspr + gstot) * M;
+#undef JRES
+  JF(3, 0) += (-gjbd + gbbdp - gIbtotd) * M;
+  JF(3, 1) += (-gbgs - gIbtotg) * M;
+  JF(3, 2) += (-gjbs + gbbsp - gIbtots) * M;
+  JF(3, 3) += (gjbd + gjbs - gbbs - gIbtotb) * M;
+  JF(0, 0) += (ggidld) * M;
+  JF(0, 1) += (ggidlg) * M;
+  JF(0, 2) -= ((ggidlg + ggidld + ggidlb)) * M;
+  JF(0, 3) += (ggidlb) * M;
+  JF(3, 0) -= (ggidld) * M;
+  JF(3, 1) -= (ggidlg) * M;
+  JF(3, 2) += ((ggidlg + ggidld + ggidlb)) * M;
+  JF(3, 3) -= (ggidlb) * M;
+  JF(2, 0) -= ((ggisls + ggislg + ggislb)) * M;
+  JF(2, 1) += (ggislg) * M;
+  JF(2, 2) += (ggisls) * M;
+  JF(2, 3) += (ggislb) * M;
+  JF(3, 0) += ((ggislg + ggisls + ggislb)) * M;
+  JF(3, 1) -= (ggislg) * M;
+  JF(3, 2) -= (ggisls) * M;
+  JF(3, 3) -= (ggislb) * M;
+  if (!(!fl.dcop && fl.init_tran && fl.newton_iter == 0)) {
+    JQ(1, 1) += (CAPcggb) * M;
+    JQ(1, 0) += (CAPcgdb) * M;
+    JQ(1, 2) += (CAPcgsb) * M;
+    JQ(1, 3) += (CAPcgbb) * M;
+    JQ(0, 0) += (CAPcddb) * M;
+    JQ(0, 1) += (+CAPcdgb) * M;
+    JQ(0, 2) -= (-CAPcdsb) * M;
+    JQ(0, 3) -= (-CAPcdbb) * M;
+    JQ(2, 0) -= (-CAPcsdb) * M;
+    JQ(2, 1) += (CAPcsgb) * M;
+    JQ(2, 2) += (CAPcssb) * M;
+    JQ(2, 3) -= (-CAPcsbb) * M;
+    JQ(3, 0) += (CAPcbdb) * M;
+    JQ(3, 1) += (CAPcbgb) * M;
+    JQ(3, 2) += (CAPcbsb) * M;
+    JQ(3, 3) += (CAPcbbb) * M;
+  }
+#undef JF
+#undef JQ
+}
+
+// V[4] = node voltages (D, G, S, B); sto_old = the store values the limiter compares against
+// (currSto on Newton step 0 of a transient step, nextSto otherwise); vgb_orig = the previous load's
+// vgb of this instance (0 before the first load), which the reference uses as the "original" vgb.
+// FULL = false compiles the load for the common card only — capMod 2, no gate tunnelling
+// (igcMod = igbMod = 0) — whatever the record says, so the default kernel carries none of the
+// other branches in its registers or its code; families whose cards use capMod 0/1 or the
+// tunnelling currents run the FULL = true instantiation.
+// SERIES = true: V holds (D', G, S', B) and Vx the external (D, S); the linear drain and source
+// resistances (rdsMod = 0, sheet resistance) load into vecx / jfx.
+// PART = 0: the whole evaluation; 1: the DC part only, which fills *mid; 2: the charge-and-stamp
+// part only, from *mid (the DC part of the same instance, same inputs).
+template <bool FULL = false, bool SERIES = false, int PART = 0, class RV>
+XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
+                      LoadOut &o, const double *Vx = nullptr, Mid *mid = nullptr) {
+  using namespace xdc;
+  if constexpr (PART == 2) {
+    bsim4_finish<FULL, SERIES>(P_, V, fl, vgb_orig, *mid, o, Vx);
+    return;
+  }
+  const double dtype = P(dtype);
+  const int mobMod = (int)P(mobMod);
+  const int dioMod = (int)P(dioMod);
+  const int tempMod = (int)P(tempMod);
+  const int capMod = FULL ? (int)P(capMod) : 2;
+  const double gmin = fl.gmin;
+  const double nf = P(nf);
+  const double vth0 = P(vth0);
+  const double M = P(mult);
+  const bool OFF = P(off) != 0.0;
+
+  const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
+
+  Bias bias;
+  bsim4_bias<SERIES>(P_, V, fl, Vx, bias);
+  const double Vddp = bias.Vddp, Vssp = bias.Vssp;
+  (void)Vddp; (void)Vssp;
+  double vds = bias.vds, vgs = bias.vgs, vbs = bias.vbs, vges = bias.vges, vgms = bias.vgms, vdbs = bias.vdbs;
+  double vsbs = bias.vsbs, vses = bias.vses, vdes = bias.vdes, vbd = bias.vbd, vdbd = bias.vdbd, vgd = bias.vgd;
+  double vged = bias.vged, vgmd = bias.vgmd, vgmb = bias.vgmb, vbs_jct = bias.vbs_jct, vbd_jct = bias.vbd_jct;
+  const double vbd_orig = bias.vbd_orig, vbs_orig = bias.vbs_orig, vgs_orig = bias.vgs_orig;
+  const double vds_orig = bias.vds_orig, vgd_orig = bias.vgd_orig, vges_orig = bias.vges_orig;
+  const double vgms_orig = bias.vgms_orig, vdes_orig = bias.vdes_orig, vses_orig = bias.vses_orig;
+  const double vdbs_orig = bias.vdbs_orig, vsbs_orig = bias.vsbs_orig, vdbd_orig = bias.vdbd_orig;
+  const double vged_orig = bias.vged_orig, vgmd_orig = bias.vgmd_orig, vbs_jct_orig = bias.vbs_jct_orig;
+  const double vbd_jct_orig = bias.vbd_jct_orig, vgmb_orig = bias.vgmb_orig;
+  (void)vdes_orig; (void)vses_orig; (void)vdbs_orig; (void)vsbs_orig; (void)vdbd_orig; (void)vged_orig;
+  (void)vgmd_orig; (void)vges_orig; (void)vgms_orig;
+  int origFlag = bias.origFlag;
+  // The reference takes vgb_orig from the instance's vgb member before it is recomputed, i.e. the
+  // previous load's value (:8026); in the limiter test below vgb therefore equals vgb_orig.
+  double vgb = vgb_orig;
   // Previous-iterate voltages for limiting (:8099-8166).
   double vbd_old, vbs_old, vgs_old, vds_old, von_local;
   if (fl.newton_iter == 0 && fl.dcop) {
@@ -1691,949 +2807,72 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   const double gIgcss = -(gIgcsg + gIgcsd + gIgcsb);
   const double gIgcds = -(gIgcdg + gIgcdd + gIgcdb);
 
-  // Intrinsic charges (:10707-11620): capMod 0, 1 or 2 (charge-thickness model).
-  double qgate = 0, qdrn = 0, qbulk = 0, qsrc = 0;
-  double cggb = 0, cgsb = 0, cgdb = 0, cdgb = 0, cdsb = 0, cddb = 0, cbgb = 0, cbsb = 0, cbdb = 0;
-  if ((P(xpart) < 0) || (!ChargeComputationNeeded)) {
-    // all zero
-  } else if (capMod == 0) {
-    // capMod = 0 (:10718-11012), the simple charge model BSIM3 shares.
-    xdc::CvCharges cv;
-    xdc::cv_simple(Vbseff, Vbs, phi, Phis, dPhis_dVb, sqrtPhis, dsqrtPhis_dVb, P(vfbcv), P(k1ox), Vgs_eff,
-                   dVgs_eff_dVg, coxe * P(weffCV) * P(leffCV) * nf, Abulk0, dAbulk0_dVb, P(abulkCVfactor), Vds,
-                   P(xpart), false, cv);
-    qgate = cv.qgate, qbulk = cv.qbulk, qdrn = cv.qdrn;
-    cggb = cv.cggb, cgsb = cv.cgsb, cgdb = cv.cgdb, cdgb = cv.cdgb, cdsb = cv.cdsb, cddb = cv.cddb;
-    cbgb = cv.cbgb, cbsb = cv.cbsb, cbdb = cv.cbdb;
-  } else {
-    double VbseffCV, dVbseffCV_dVb;
-    if (Vbseff < 0.0) {
-      VbseffCV = Vbseff;
-      dVbseffCV_dVb = 1.0;
-    } else {
-      VbseffCV = phi - Phis;
-      dVbseffCV_dVb = -dPhis_dVb;
-    }
-    const double CoxWL = coxe * P(weffCV) * P(leffCV) * nf;
-    if (P(cvchargeMod) == 0.0) {
-      const double noff = n * P(noff);
-      const double dnoff_dVd = P(noff) * dn_dVd;
-      const double dnoff_dVb = P(noff) * dn_dVb;
-      T0 = Vtm * noff;
-      const double voffcv = P(voffcv);
-      const double VgstNVt = (Vgst - voffcv) / T0;
-      if (VgstNVt > CONSTEXP_THRESHOLD) {
-        Vgsteff = Vgst - voffcv;
-        dVgsteff_dVg = dVgs_eff_dVg;
-        dVgsteff_dVd = -dVth_dVd;
-        dVgsteff_dVb = -dVth_dVb;
-      } else if (VgstNVt < -CONSTEXP_THRESHOLD) {
-        Vgsteff = T0 * log(1.0 + CONSTMIN_EXP);
-        dVgsteff_dVg = 0.0;
-        dVgsteff_dVd = Vgsteff / noff;
-        dVgsteff_dVb = dVgsteff_dVd * dnoff_dVb;
-        dVgsteff_dVd *= dnoff_dVd;
-      } else {
-        const double ExpVgst = exp(VgstNVt);
-        Vgsteff = T0 * log(1.0 + ExpVgst);
-        dVgsteff_dVg = ExpVgst / (1.0 + ExpVgst);
-        dVgsteff_dVd = -dVgsteff_dVg * (dVth_dVd + (Vgst - voffcv) / noff * dnoff_dVd) + Vgsteff / noff * dnoff_dVd;
-        dVgsteff_dVb = -dVgsteff_dVg * (dVth_dVb + (Vgst - voffcv) / noff * dnoff_dVb) + Vgsteff / noff * dnoff_dVb;
-        dVgsteff_dVg *= dVgs_eff_dVg;
-      }
-    } else {
-      const double mstarcv = P(mstarcv);
-      T0 = n * Vtm;
-      T1 = mstarcv * Vgst;
-      T2 = T1 / T0;
-      if (T2 > CONSTEXP_THRESHOLD) {
-        T10 = T1;
-        dT10_dVg = mstarcv * dVgs_eff_dVg;
-        dT10_dVd = -dVth_dVd * mstarcv;
-        dT10_dVb = -dVth_dVb * mstarcv;
-      } else if (T2 < -CONSTEXP_THRESHOLD) {
-        T10 = Vtm * log(1.0 + CONSTMIN_EXP);
-        dT10_dVg = 0.0;
-        dT10_dVd = T10 * dn_dVd;
-        dT10_dVb = T10 * dn_dVb;
-        T10 *= n;
-      } else {
-        const double ExpVgst = exp(T2);
-        T3 = Vtm * log(1.0 + ExpVgst);
-        T10 = n * T3;
-        dT10_dVg = mstarcv * ExpVgst / (1.0 + ExpVgst);
-        dT10_dVb = T3 * dn_dVb - dT10_dVg * (dVth_dVb + Vgst * dn_dVb / n);
-        dT10_dVd = T3 * dn_dVd - dT10_dVg * (dVth_dVd + Vgst * dn_dVd / n);
-        dT10_dVg *= dVgs_eff_dVg;
-      }
-      T1 = P(voffcbncv) - (1.0 - mstarcv) * Vgst;
-      T2 = T1 / T0;
-      if (T2 < -CONSTEXP_THRESHOLD) {
-        T3 = coxe * CONSTMIN_EXP / P(cdep0);
-        T9 = mstarcv + T3 * n;
-        dT9_dVg = 0.0;
-        dT9_dVd = dn_dVd * T3;
-        dT9_dVb = dn_dVb * T3;
-      } else if (T2 > CONSTEXP_THRESHOLD) {
-        T3 = coxe * CONSTMAX_EXP / P(cdep0);
-        T9 = mstarcv + T3 * n;
-        dT9_dVg = 0.0;
-        dT9_dVd = dn_dVd * T3;
-        dT9_dVb = dn_dVb * T3;
-      } else {
-        const double ExpVgst = exp(T2);
-        T3 = coxe / P(cdep0);
-        T4 = T3 * ExpVgst;
-        T5 = T1 * T4 / T0;
-        T9 = mstarcv + n * T4;
-        dT9_dVg = T3 * (mstarcv - 1.0) * ExpVgst / Vtm;
-        dT9_dVb = T4 * dn_dVb - dT9_dVg * dVth_dVb - T5 * dn_dVb;
-        dT9_dVd = T4 * dn_dVd - dT9_dVg * dVth_dVd - T5 * dn_dVd;
-        dT9_dVg *= dVgs_eff_dVg;
-      }
-      Vgsteff = T10 / T9;
-      T11 = T9 * T9;
-      dVgsteff_dVg = (T9 * dT10_dVg - T10 * dT9_dVg) / T11;
-      dVgsteff_dVd = (T9 * dT10_dVd - T10 * dT9_dVd) / T11;
-      dVgsteff_dVb = (T9 * dT10_dVb - T10 * dT9_dVb) / T11;
-    }
-    if (capMod == 1) {
-      // capMod = 1 (:11139-11319): accumulation and depletion charges Qac0 / Qsub0 with the
-      // zero-bias flat band, the inversion charge without the charge-thickness correction.
-      const double Vfb1 = P(vfbzb);
-      double V3 = Vfb1 - Vgs_eff + VbseffCV - CONSTDELTA_3;
-      if (Vfb1 <= 0.0)
-        T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * Vfb1);
-      else
-        T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * Vfb1);
-      T1 = 0.5 * (1.0 + V3 / T0);
-      const double Vfbeff = Vfb1 - 0.5 * (V3 + T0);
-      const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
-      const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
-      const double Qac0 = CoxWL * (Vfbeff - Vfb1);
-      const double dQac0_dVg = CoxWL * dVfbeff_dVg;
-      const double dQac0_dVb = CoxWL * dVfbeff_dVb;
-      const double k1ox1 = P(k1ox);
-      T0 = 0.5 * k1ox1;
-      T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
-      if (k1ox1 == 0.0) {
-        T1 = 0.0;
-        T2 = 0.0;
-      } else if (T3 < 0.0) {
-        T1 = T0 + T3 / k1ox1;
-        T2 = CoxWL;
-      } else {
-        T1 = sqrt(T0 * T0 + T3);
-        T2 = CoxWL * T0 / T1;
-      }
-      const double Qsub0 = CoxWL * k1ox1 * (T1 - T0);
-      const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg);
-      const double dQsub0_dVd = -T2 * dVgsteff_dVd;
-      const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb);
-      const double AbulkCV = Abulk0 * P(abulkCVfactor);
-      const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
-      const double VdsatCV = Vgsteff / AbulkCV;
-      T0 = VdsatCV - Vds - CONSTDELTA_4;
-      dT0_dVg = 1.0 / AbulkCV;
-      dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
-      T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
-      dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
-      dT1_dVd = -T0 / T1;
-      dT1_dVb = dT1_dVg * dT0_dVb;
-      dT1_dVg *= dT0_dVg;
-      double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
-      if (T0 >= 0.0) {
-        VdseffCV = VdsatCV - 0.5 * (T0 + T1);
-        dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
-        dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
-        dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
-      } else {
-        T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
-        T4 = 1.0 - T3;
-        T5 = VdsatCV * T3 / (T1 - T0);
-        VdseffCV = VdsatCV * T4;
-        dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
-        dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
-        dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
-      }
-      if (Vds == 0.0) {  // the reference leaves dVdseffCV_dVd as computed
-        VdseffCV = 0.0;
-        dVdseffCV_dVg = 0.0;
-        dVdseffCV_dVb = 0.0;
-      }
-      T0 = AbulkCV * VdseffCV;
-      T1 = 12.0 * (Vgsteff - 0.5 * T0 + 1.0e-20);
-      T2 = VdseffCV / T1;
-      T3 = T0 * T2;
-      T4 = (1.0 - 12.0 * T2 * T2 * AbulkCV);
-      T5 = (6.0 * T0 * (4.0 * Vgsteff - T0) / (T1 * T1) - 0.5);
-      T6 = 12.0 * T2 * T2 * Vgsteff;
-      qgate = CoxWL * (Vgsteff - 0.5 * VdseffCV + T3);
-      double Cgg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
-      const double Cgd1 = CoxWL * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd;
-      const double Cgb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb;
-      Cgg1 *= dVgsteff_dVg;
-      T7 = 1.0 - AbulkCV;
-      qbulk = CoxWL * T7 * (0.5 * VdseffCV - T3);
-      T4 = -T7 * (T4 - 1.0);
-      T5 = -T7 * T5;
-      T6 = -(T7 * T6 + (0.5 * VdseffCV - T3));
-      double Cbg1 = CoxWL * (T4 + T5 * dVdseffCV_dVg);
-      const double Cbd1 = CoxWL * T5 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd;
-      const double Cbb1 = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb;
-      Cbg1 *= dVgsteff_dVg;
-      double Csg, Csd, Csb;
-      const double xpart = P(xpart);
-      if (xpart > 0.5) {  // 0/100
-        T1 = T1 + T1;
-        qsrc = -CoxWL * (0.5 * Vgsteff + 0.25 * T0 - T0 * T0 / T1);
-        T7 = (4.0 * Vgsteff - T0) / (T1 * T1);
-        T4 = -(0.5 + 24.0 * T0 * T0 / (T1 * T1));
-        T5 = -(0.25 * AbulkCV - 12.0 * AbulkCV * T0 * T7);
-        T6 = -(0.25 * VdseffCV - 12.0 * T0 * VdseffCV * T7);
-        Csg = CoxWL * (T4 + T5 * dVdseffCV_dVg);
-        Csd = CoxWL * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
-        Csb = CoxWL * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
-        Csg *= dVgsteff_dVg;
-      } else if (xpart < 0.5) {  // 40/60
-        T1 = T1 / 12.0;
-        T2 = 0.5 * CoxWL / (T1 * T1);
-        T3 = Vgsteff * (2.0 * T0 * T0 / 3.0 + Vgsteff * (Vgsteff - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
-        qsrc = -T2 * T3;
-        T7 = 4.0 / 3.0 * Vgsteff * (Vgsteff - T0) + 0.4 * T0 * T0;
-        T4 = -2.0 * qsrc / T1 - T2 * (Vgsteff * (3.0 * Vgsteff - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
-        T5 = (qsrc / T1 + T2 * T7) * AbulkCV;
-        T6 = (qsrc / T1 * VdseffCV + T2 * T7 * VdseffCV);
-        Csg = (T4 + T5 * dVdseffCV_dVg);
-        Csd = T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd;
-        Csb = (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb;
-        Csg *= dVgsteff_dVg;
-      } else {  // 50/50
-        qsrc = -0.5 * (qgate + qbulk);
-        Csg = -0.5 * (Cgg1 + Cbg1);
-        Csb = -0.5 * (Cgb1 + Cbb1);
-        Csd = -0.5 * (Cgd1 + Cbd1);
-      }
-      qgate += Qac0 + Qsub0;
-      qbulk -= (Qac0 + Qsub0);
-      qdrn = -(qgate + qbulk + qsrc);
-      const double Cgg = dQac0_dVg + dQsub0_dVg + Cgg1;
-      const double Cgd = dQsub0_dVd + Cgd1;
-      double Cgb = dQac0_dVb + dQsub0_dVb + Cgb1;
-      const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
-      const double Cbd = Cbd1 - dQsub0_dVd;
-      double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
-      Cgb *= dVbseff_dVb;
-      Cbb *= dVbseff_dVb;
-      Csb *= dVbseff_dVb;
-      cggb = Cgg;
-      cgsb = -(Cgg + Cgd + Cgb);
-      cgdb = Cgd;
-      cdgb = -(Cgg + Cbg + Csg);
-      cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
-      cddb = -(Cgd + Cbd + Csd);
-      cbgb = Cbg;
-      cbsb = -(Cbg + Cbd + Cbb);
-      cbdb = Cbd;
-    } else {
-    // capMod == 2
-    const double vfbzb = P(vfbzb);
-    double V3 = vfbzb - Vgs_eff + VbseffCV - CONSTDELTA_3;
-    if (vfbzb <= 0.0)
-      T0 = sqrt(V3 * V3 - 4.0 * CONSTDELTA_3 * vfbzb);
-    else
-      T0 = sqrt(V3 * V3 + 4.0 * CONSTDELTA_3 * vfbzb);
-    T1 = 0.5 * (1.0 + V3 / T0);
-    const double Vfbeff = vfbzb - 0.5 * (V3 + T0);
-    const double dVfbeff_dVg = T1 * dVgs_eff_dVg;
-    const double dVfbeff_dVb = -T1 * dVbseffCV_dVb;
-    const double Cox = coxp;
-    double Tox = 1.0e8 * P(toxp);
-    T0 = (Vgs_eff - VbseffCV - vfbzb) / Tox;
-    dT0_dVg = dVgs_eff_dVg / Tox;
-    dT0_dVb = -dVbseffCV_dVb / Tox;
-    tmp = T0 * P(acde);
-    const double ldeb = P(ldeb);
-    double dTcen_dVb, dTcen_dVd;
-    if ((-CONSTEXP_THRESHOLD < tmp) && (tmp < CONSTEXP_THRESHOLD)) {
-      Tcen = ldeb * exp(tmp);
-      dTcen_dVg = P(acde) * Tcen;
-      dTcen_dVb = dTcen_dVg * dT0_dVb;
-      dTcen_dVg *= dT0_dVg;
-    } else if (tmp <= -CONSTEXP_THRESHOLD) {
-      Tcen = ldeb * CONSTMIN_EXP;
-      dTcen_dVg = dTcen_dVb = 0.0;
-    } else {
-      Tcen = ldeb * CONSTMAX_EXP;
-      dTcen_dVg = dTcen_dVb = 0.0;
-    }
-    const double LINK = 1.0e-3 * P(toxp);
-    V3 = ldeb - Tcen - LINK;
-    const double V4 = sqrt(V3 * V3 + 4.0 * LINK * ldeb);
-    Tcen = ldeb - 0.5 * (V3 + V4);
-    T1 = 0.5 * (1.0 + V3 / V4);
-    dTcen_dVg *= T1;
-    dTcen_dVb *= T1;
-    double Ccen = epssub / Tcen;
-    T2 = Cox / (Cox + Ccen);
-    Coxeff = T2 * Ccen;
-    T3 = -Ccen / Tcen;
-    dCoxeff_dVg = T2 * T2 * T3;
-    double dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
-    dCoxeff_dVg *= dTcen_dVg;
-    double CoxWLcen = CoxWL * Coxeff / coxe;
-    const double Qac0 = CoxWLcen * (Vfbeff - vfbzb);
-    double QovCox = Qac0 / Coxeff;
-    const double dQac0_dVg = CoxWLcen * dVfbeff_dVg + QovCox * dCoxeff_dVg;
-    const double dQac0_dVb = CoxWLcen * dVfbeff_dVb + QovCox * dCoxeff_dVb;
-    T0 = 0.5 * k1ox;
-    T3 = Vgs_eff - Vfbeff - VbseffCV - Vgsteff;
-    if (k1ox == 0.0) {
-      T1 = 0.0;
-      T2 = 0.0;
-    } else if (T3 < 0.0) {
-      T1 = T0 + T3 / k1ox;
-      T2 = CoxWLcen;
-    } else {
-      T1 = sqrt(T0 * T0 + T3);
-      T2 = CoxWLcen * T0 / T1;
-    }
-    const double Qsub0 = CoxWLcen * k1ox * (T1 - T0);
-    QovCox = Qsub0 / Coxeff;
-    const double dQsub0_dVg = T2 * (dVgs_eff_dVg - dVfbeff_dVg - dVgsteff_dVg) + QovCox * dCoxeff_dVg;
-    const double dQsub0_dVd = -T2 * dVgsteff_dVd;
-    const double dQsub0_dVb = -T2 * (dVfbeff_dVb + dVbseffCV_dVb + dVgsteff_dVb) + QovCox * dCoxeff_dVb;
-    if (k1ox <= 0.0) {
-      Denomi = 0.25 * P(moin) * Vtm;
-      T0 = 0.5 * sqrtPhi_p;
-    } else {
-      Denomi = P(moin) * Vtm * k1ox * k1ox;
-      T0 = k1ox * sqrtPhi_p;
-    }
-    T1 = 2.0 * T0 + Vgsteff;
-    const double DeltaPhi = Vtm * log(1.0 + T1 * Vgsteff / Denomi);
-    const double dDeltaPhi_dVg = 2.0 * Vtm * (T1 - T0) / (Denomi + T1 * Vgsteff);
-    T0 = Vgsteff - DeltaPhi - 0.001;
-    dT0_dVg = 1.0 - dDeltaPhi_dVg;
-    T1 = sqrt(T0 * T0 + Vgsteff * 0.004);
-    const double VgDP = 0.5 * (T0 + T1);
-    const double dVgDP_dVg = 0.5 * (dT0_dVg + (T0 * dT0_dVg + 0.002) / T1);
-    Tox += Tox;
-    T0 = (Vgsteff + P(vtfbphi2)) / Tox;
-    tmp = exp(P(bdos) * 0.7 * log(T0));
-    T1 = 1.0 + tmp;
-    T2 = P(bdos) * 0.7 * tmp / (T0 * Tox);
-    Tcen = P(ados) * 1.9e-9 / T1;
-    dTcen_dVg = -Tcen * T2 / T1;
-    dTcen_dVd = dTcen_dVg * dVgsteff_dVd;
-    dTcen_dVb = dTcen_dVg * dVgsteff_dVb;
-    dTcen_dVg *= dVgsteff_dVg;
-    Ccen = epssub / Tcen;
-    T0 = Cox / (Cox + Ccen);
-    Coxeff = T0 * Ccen;
-    T1 = -Ccen / Tcen;
-    dCoxeff_dVg = T0 * T0 * T1;
-    const double dCoxeff_dVd = dCoxeff_dVg * dTcen_dVd;
-    dCoxeff_dVb = dCoxeff_dVg * dTcen_dVb;
-    dCoxeff_dVg *= dTcen_dVg;
-    CoxWLcen = CoxWL * Coxeff / coxe;
-    const double AbulkCV = Abulk0 * P(abulkCVfactor);
-    const double dAbulkCV_dVb = P(abulkCVfactor) * dAbulk0_dVb;
-    const double VdsatCV = VgDP / AbulkCV;
-    T0 = VdsatCV - Vds - CONSTDELTA_4;
-    dT0_dVg = dVgDP_dVg / AbulkCV;
-    dT0_dVb = -VdsatCV * dAbulkCV_dVb / AbulkCV;
-    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_4 * VdsatCV);
-    dT1_dVg = (T0 + CONSTDELTA_4 + CONSTDELTA_4) / T1;
-    dT1_dVd = -T0 / T1;
-    dT1_dVb = dT1_dVg * dT0_dVb;
-    dT1_dVg *= dT0_dVg;
-    double VdseffCV, dVdseffCV_dVg, dVdseffCV_dVd, dVdseffCV_dVb;
-    if (T0 >= 0.0) {
-      VdseffCV = VdsatCV - 0.5 * (T0 + T1);
-      dVdseffCV_dVg = 0.5 * (dT0_dVg - dT1_dVg);
-      dVdseffCV_dVd = 0.5 * (1.0 - dT1_dVd);
-      dVdseffCV_dVb = 0.5 * (dT0_dVb - dT1_dVb);
-    } else {
-      T3 = (CONSTDELTA_4 + CONSTDELTA_4) / (T1 - T0);
-      T4 = 1.0 - T3;
-      T5 = VdsatCV * T3 / (T1 - T0);
-      VdseffCV = VdsatCV * T4;
-      dVdseffCV_dVg = dT0_dVg * T4 + T5 * (dT1_dVg - dT0_dVg);
-      dVdseffCV_dVd = T5 * (dT1_dVd + 1.0);
-      dVdseffCV_dVb = dT0_dVb * (T4 - T5) + T5 * dT1_dVb;
-    }
-    if (Vds == 0.0) {
-      VdseffCV = 0.0;
-      dVdseffCV_dVg = 0.0;
-      dVdseffCV_dVb = 0.0;
-    }
-    T0 = AbulkCV * VdseffCV;
-    T1 = VgDP;
-    T2 = 12.0 * (T1 - 0.5 * T0 + 1.0e-20);
-    T3 = T0 / T2;
-    T4 = 1.0 - 12.0 * T3 * T3;
-    T5 = AbulkCV * (6.0 * T0 * (4.0 * T1 - T0) / (T2 * T2) - 0.5);
-    T6 = T5 * VdseffCV / AbulkCV;
-    qgate = CoxWLcen * (T1 - T0 * (0.5 - T3));
-    QovCox = qgate / Coxeff;
-    double Cgg1 = CoxWLcen * (T4 * dVgDP_dVg + T5 * dVdseffCV_dVg);
-    const double Cgd1 = CoxWLcen * T5 * dVdseffCV_dVd + Cgg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
-    const double Cgb1 = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Cgg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
-    Cgg1 = Cgg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
-    T7 = 1.0 - AbulkCV;
-    T8 = T2 * T2;
-    T9 = 12.0 * T7 * T0 * T0 / (T8 * AbulkCV);
-    T10 = T9 * dVgDP_dVg;
-    T11 = -T7 * T5 / AbulkCV;
-    T12 = -(T9 * T1 / AbulkCV + VdseffCV * (0.5 - T0 / T2));
-    qbulk = CoxWLcen * T7 * (0.5 * VdseffCV - T0 * VdseffCV / T2);
-    QovCox = qbulk / Coxeff;
-    double Cbg1 = CoxWLcen * (T10 + T11 * dVdseffCV_dVg);
-    const double Cbd1 = CoxWLcen * T11 * dVdseffCV_dVd + Cbg1 * dVgsteff_dVd + QovCox * dCoxeff_dVd;
-    const double Cbb1 = CoxWLcen * (T11 * dVdseffCV_dVb + T12 * dAbulkCV_dVb) + Cbg1 * dVgsteff_dVb + QovCox * dCoxeff_dVb;
-    Cbg1 = Cbg1 * dVgsteff_dVg + QovCox * dCoxeff_dVg;
-    double Csg, Csd, Csb;
-    const double xpart = P(xpart);
-    if (xpart > 0.5) {
-      qsrc = -CoxWLcen * (T1 / 2.0 + T0 / 4.0 - 0.5 * T0 * T0 / T2);
-      QovCox = qsrc / Coxeff;
-      T2 += T2;
-      T3 = T2 * T2;
-      T7 = -(0.25 - 12.0 * T0 * (4.0 * T1 - T0) / T3);
-      T4 = -(0.5 + 24.0 * T0 * T0 / T3) * dVgDP_dVg;
-      T5 = T7 * AbulkCV;
-      T6 = T7 * VdseffCV;
-      Csg = CoxWLcen * (T4 + T5 * dVdseffCV_dVg);
-      Csd = CoxWLcen * T5 * dVdseffCV_dVd + Csg * dVgsteff_dVd + QovCox * dCoxeff_dVd;
-      Csb = CoxWLcen * (T5 * dVdseffCV_dVb + T6 * dAbulkCV_dVb) + Csg * dVgsteff_dVb + QovCox * dCoxeff_dVb;
-      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
-    } else if (xpart < 0.5) {
-      T2 = T2 / 12.0;
-      T3 = 0.5 * CoxWLcen / (T2 * T2);
-      T4 = T1 * (2.0 * T0 * T0 / 3.0 + T1 * (T1 - 4.0 * T0 / 3.0)) - 2.0 * T0 * T0 * T0 / 15.0;
-      qsrc = -T3 * T4;
-      QovCox = qsrc / Coxeff;
-      T8 = 4.0 / 3.0 * T1 * (T1 - T0) + 0.4 * T0 * T0;
-      T5 = -2.0 * qsrc / T2 - T3 * (T1 * (3.0 * T1 - 8.0 * T0 / 3.0) + 2.0 * T0 * T0 / 3.0);
-      T6 = AbulkCV * (qsrc / T2 + T3 * T8);
-      T7 = T6 * VdseffCV / AbulkCV;
-      Csg = T5 * dVgDP_dVg + T6 * dVdseffCV_dVg;
-      Csd = Csg * dVgsteff_dVd + T6 * dVdseffCV_dVd + QovCox * dCoxeff_dVd;
-      Csb = Csg * dVgsteff_dVb + T6 * dVdseffCV_dVb + T7 * dAbulkCV_dVb + QovCox * dCoxeff_dVb;
-      Csg = Csg * dVgsteff_dVg + QovCox * dCoxeff_dVg;
-    } else {
-      qsrc = -0.5 * qgate;
-      Csg = -0.5 * Cgg1;
-      Csd = -0.5 * Cgd1;
-      Csb = -0.5 * Cgb1;
-    }
-    qgate += Qac0 + Qsub0 - qbulk;
-    qbulk -= (Qac0 + Qsub0);
-    qdrn = -(qgate + qbulk + qsrc);
-    const double Cbg = Cbg1 - dQac0_dVg - dQsub0_dVg;
-    const double Cbd = Cbd1 - dQsub0_dVd;
-    double Cbb = Cbb1 - dQac0_dVb - dQsub0_dVb;
-    const double Cgg = Cgg1 - Cbg;
-    const double Cgd = Cgd1 - Cbd;
-    double Cgb = Cgb1 - Cbb;
-    Cgb *= dVbseff_dVb;
-    Cbb *= dVbseff_dVb;
-    Csb *= dVbseff_dVb;
-    cggb = Cgg;
-    cgsb = -(Cgg + Cgd + Cgb);
-    cgdb = Cgd;
-    cdgb = -(Cgg + Cbg + Csg);
-    cdsb = (Cgg + Cgd + Cgb + Cbg + Cbd + Cbb + Csg + Csd + Csb);
-    cddb = -(Cgd + Cbd + Csd);
-    cbgb = Cbg;
-    cbsb = -(Cbg + Cbd + Cbb);
-    cbdb = Cbd;
-    }
+  // Hand-off to the charge-and-stamp part.
+  Mid hm;
+  hm.v[m_vds] = vds;
+  hm.v[m_vgs] = vgs;
+  hm.v[m_vbs] = vbs;
+  hm.v[m_orig] = (double)origFlag;
+  hm.v[m_von] = von;
+  hm.v[m_gbs] = gbs;
+  hm.v[m_cbs] = cbs;
+  hm.v[m_gbd] = gbd;
+  hm.v[m_cbd] = cbd;
+  hm.v[m_cdrain] = cdrain;
+  hm.v[m_gds] = gds;
+  hm.v[m_gm] = gm;
+  hm.v[m_gmbs] = gmbs;
+  hm.v[m_csub] = csub;
+  hm.v[m_gbbs] = gbbs;
+  hm.v[m_gbgs] = gbgs;
+  hm.v[m_gbds] = gbds;
+  hm.v[m_Igidl] = Igidl;
+  hm.v[m_ggidld] = ggidld;
+  hm.v[m_ggidlg] = ggidlg;
+  hm.v[m_ggidlb] = ggidlb;
+  hm.v[m_Igisl] = Igisl;
+  hm.v[m_ggisls] = ggisls;
+  hm.v[m_ggislg] = ggislg;
+  hm.v[m_ggislb] = ggislb;
+  hm.v[m_Abulk0] = Abulk0;
+  hm.v[m_dAbulk0_dVb] = dAbulk0_dVb;
+  hm.v[m_Vbseff] = Vbseff;
+  hm.v[m_dVbseff_dVb] = dVbseff_dVb;
+  hm.v[m_Vgs_eff] = Vgs_eff;
+  hm.v[m_dVgs_eff_dVg] = dVgs_eff_dVg;
+  hm.v[m_Vgst] = Vgst;
+  hm.v[m_dVth_dVb] = dVth_dVb;
+  hm.v[m_dVth_dVd] = dVth_dVd;
+  hm.v[m_n] = n;
+  hm.v[m_dn_dVb] = dn_dVb;
+  hm.v[m_dn_dVd] = dn_dVd;
+  if constexpr (FULL) {
+    hm.v[m_Igs] = Igs;
+    hm.v[m_gIgsg] = gIgsg;
+    hm.v[m_gIgss] = gIgss;
+    hm.v[m_Igd] = Igd;
+    hm.v[m_gIgdg] = gIgdg;
+    hm.v[m_gIgdd] = gIgdd;
+    hm.v[m_Igcs] = Igcs;
+    hm.v[m_gIgcsg] = gIgcsg;
+    hm.v[m_gIgcsd] = gIgcsd;
+    hm.v[m_gIgcsb] = gIgcsb;
+    hm.v[m_Igcd] = Igcd;
+    hm.v[m_gIgcdg] = gIgcdg;
+    hm.v[m_gIgcdd] = gIgcdd;
+    hm.v[m_gIgcdb] = gIgcdb;
+    hm.v[m_Igb] = Igb;
+    hm.v[m_gIgbg] = gIgbg;
+    hm.v[m_gIgbd] = gIgbd;
+    hm.v[m_gIgbb] = gIgbb;
   }
-
-  // Junction charges and capacitances (:11661-11810). Outside charge computation the reference
-  // keeps the previous load's junction values; they only feed Q and dQ/dx, which a DC solve does
-  // not use, and are zero here.
-  double qbs = 0.0, qbd = 0.0, capbs = 0.0, capbd = 0.0;
-  if (ChargeComputationNeeded) {
-    const double czbd = P(DunitAreaTempJctCap) * Adeff;
-    const double czbs = P(SunitAreaTempJctCap) * Aseff;
-    const double czbdsw = P(DunitLengthSidewallTempJctCap) * Pdeff;
-    const double czbdswg = P(DunitLengthGateSidewallTempJctCap) * weffCJ * nf;
-    const double czbssw = P(SunitLengthSidewallTempJctCap) * Pseff;
-    const double czbsswg = P(SunitLengthGateSidewallTempJctCap) * weffCJ * nf;
-    const double MJS = P(SbulkJctBotGradingCoeff), MJSWS = P(SbulkJctSideGradingCoeff);
-    const double MJSWGS = P(SbulkJctGateSideGradingCoeff);
-    const double MJD = P(DbulkJctBotGradingCoeff), MJSWD = P(DbulkJctSideGradingCoeff);
-    const double MJSWGD = P(DbulkJctGateSideGradingCoeff);
-    double arg, sarg;
-    if (vbs_jct == 0.0) {
-      qbs = 0.0;
-      capbs = czbs + czbssw + czbsswg;
-    } else if (vbs_jct < 0.0) {
-      if (czbs > 0.0) {
-        arg = 1.0 - vbs_jct / P(PhiBS);
-        if (MJS == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJS * log(arg));
-        qbs = P(PhiBS) * czbs * (1.0 - arg * sarg) / (1.0 - MJS);
-        capbs = czbs * sarg;
-      } else {
-        qbs = 0.0;
-        capbs = 0.0;
-      }
-      if (czbssw > 0.0) {
-        arg = 1.0 - vbs_jct / P(PhiBSWS);
-        if (MJSWS == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJSWS * log(arg));
-        qbs += P(PhiBSWS) * czbssw * (1.0 - arg * sarg) / (1.0 - MJSWS);
-        capbs += czbssw * sarg;
-      }
-      if (czbsswg > 0.0) {
-        arg = 1.0 - vbs_jct / P(PhiBSWGS);
-        if (MJSWGS == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJSWGS * log(arg));
-        qbs += P(PhiBSWGS) * czbsswg * (1.0 - arg * sarg) / (1.0 - MJSWGS);
-        capbs += czbsswg * sarg;
-      }
-    } else {
-      T0 = czbs + czbssw + czbsswg;
-      T1 = vbs_jct * (czbs * MJS / P(PhiBS) + czbssw * MJSWS / P(PhiBSWS) + czbsswg * MJSWGS / P(PhiBSWGS));
-      qbs = vbs_jct * (T0 + 0.5 * T1);
-      capbs = T0 + T1;
-    }
-    if (vbd_jct == 0.0) {
-      qbd = 0.0;
-      capbd = czbd + czbdsw + czbdswg;
-    } else if (vbd_jct < 0.0) {
-      if (czbd > 0.0) {
-        arg = 1.0 - vbd_jct / P(PhiBD);
-        if (MJD == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJD * log(arg));
-        qbd = P(PhiBD) * czbd * (1.0 - arg * sarg) / (1.0 - MJD);
-        capbd = czbd * sarg;
-      } else {
-        qbd = 0.0;
-        capbd = 0.0;
-      }
-      if (czbdsw > 0.0) {
-        arg = 1.0 - vbd_jct / P(PhiBSWD);
-        if (MJSWD == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJSWD * log(arg));
-        qbd += P(PhiBSWD) * czbdsw * (1.0 - arg * sarg) / (1.0 - MJSWD);
-        capbd += czbdsw * sarg;
-      }
-      if (czbdswg > 0.0) {
-        arg = 1.0 - vbd_jct / P(PhiBSWGD);
-        if (MJSWGD == 0.5)
-          sarg = 1.0 / sqrt(arg);
-        else
-          sarg = exp(-MJSWGD * log(arg));
-        qbd += P(PhiBSWGD) * czbdswg * (1.0 - arg * sarg) / (1.0 - MJSWGD);
-        capbd += czbdswg * sarg;
-      }
-    } else {
-      T0 = czbd + czbdsw + czbdswg;
-      T1 = vbd_jct * (czbd * MJD / P(PhiBD) + czbdsw * MJSWD / P(PhiBSWD) + czbdswg * MJSWGD / P(PhiBSWGD));
-      qbd = vbd_jct * (T0 + 0.5 * T1);
-      capbd = T0 + T1;
-    }
+  (void)gIgbs; (void)gIgcss; (void)gIgcds;
+  if constexpr (PART == 1) {
+    *mid = hm;
+    return;
   }
-
-  // Overlap capacitances (:11846-11890): constant for capMod 0, bias-dependent for 1 and 2.
-  const double vgdx = vgd, vgsx = vgs;
-  double cgdo, qgdo, cgso, qgso;
-  if (capMod == 0) {
-    cgdo = P(cgdo);
-    qgdo = P(cgdo) * vgdx;
-    cgso = P(cgso);
-    qgso = P(cgso) * vgsx;
-  } else {
-    T0 = vgdx + CONSTDELTA_1;
-    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
-    T2 = 0.5 * (T0 - T1);
-    T3 = P(weffCV) * P(cgdl);
-    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappad));
-    cgdo = P(cgdo) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
-    qgdo = (P(cgdo) + T3) * vgdx - T3 * (T2 + 0.5 * P(ckappad) * (T4 - 1.0));
-    T0 = vgsx + CONSTDELTA_1;
-    T1 = sqrt(T0 * T0 + 4.0 * CONSTDELTA_1);
-    T2 = 0.5 * (T0 - T1);
-    T3 = P(weffCV) * P(cgsl);
-    T4 = sqrt(1.0 - 4.0 * T2 / P(ckappas));
-    cgso = P(cgso) + T3 - T3 * (1.0 - 1.0 / T4) * (0.5 - 0.5 * T0 / T1);
-    qgso = (P(cgso) + T3) * vgsx - T3 * (T2 + 0.5 * P(ckappas) * (T4 - 1.0));
-  }
-  if (nf != 1.0) {
-    cgdo *= nf;
-    cgso *= nf;
-    qgdo *= nf;
-    qgso *= nf;
-  }
-
-  // Overlap and gate-bulk charge bookkeeping (setupCapacitors_oldDAE, trnqsMod = 0, :12624-12760).
-  const double cgbo = P(cgbo);
-  double dxpart, sxpart;
-  if (mode > 0) {
-    qdrn -= qgdo;
-    const double qgb = cgbo * vgb;
-    qgate += qgdo + qgso + qgb;
-    qbulk -= qgb;
-    qsrc = -(qgate + qbulk + qdrn);
-    sxpart = 0.6;
-    dxpart = 0.4;
-  } else {
-    qsrc = qdrn - qgso;
-    const double qgb = cgbo * vgb;
-    qgate += qgdo + qgso + qgb;
-    qbulk -= qgb;
-    qdrn = -(qgate + qbulk + qsrc);
-    sxpart = 0.4;
-    dxpart = 0.6;
-  }
-  (void)qsrc;
-
-  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = rgateMod = rbodyMod = 0).
-  double CAPcggb, CAPcgdb, CAPcgsb, CAPcgbb, CAPcdgb, CAPcsgb, CAPcbgb, CAPcddb, CAPcdsb, CAPcsdb, CAPcssb;
-  double CAPcdbb, CAPcsbb, CAPcbdb, CAPcbsb, CAPcbbb;
-  const double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
-  if (mode > 0) {
-    CAPcggb = (cggb + cgdo + cgso + cgbo);
-    CAPcgdb = (cgdb - cgdo);
-    CAPcgsb = (cgsb - cgso);
-    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
-    CAPcdgb = (cdgb - cgdo);
-    CAPcsgb = -(cggb + cbgb + cdgb + cgso);
-    CAPcbgb = (cbgb - cgbo);
-    CAPcddb = (cddb + capbd + cgdo);
-    CAPcdsb = cdsb;
-    CAPcsdb = -(cgdb + cbdb + cddb);
-    CAPcssb = (capbs + cgso - (cgsb + cbsb + cdsb));
-    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
-    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
-    CAPcbdb = (cbdb - capbd);
-    CAPcbsb = (cbsb - capbs);
-    CAPcbbb = -(CAPcbdb + CAPcbgb + CAPcbsb + CAPcbgmb);
-  } else {
-    CAPcggb = (cggb + cgdo + cgso + cgbo);
-    CAPcgdb = (cgsb - cgdo);
-    CAPcgsb = (cgdb - cgso);
-    CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
-    CAPcdgb = -(cggb + cbgb + cdgb + cgdo);
-    CAPcsgb = (cdgb - cgso);
-    CAPcbgb = (cbgb - cgbo);
-    CAPcddb = (capbd + cgdo - (cgsb + cbsb + cdsb));
-    CAPcdsb = -(cgdb + cbdb + cddb);
-    CAPcsdb = cdsb;
-    CAPcssb = (cddb + capbs + cgso);
-    CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
-    CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
-    CAPcbdb = (cbsb - capbd);
-    CAPcbsb = (cbdb - capbs);
-    CAPcbbb = -(CAPcbgb + CAPcbdb + CAPcbsb + CAPcbgmb);
-  }
-
-  // Master::updateState: store and state (:16195-16242).
-  o.sto[s_vbd] = vbd;
-  o.sto[s_vbs] = vbs;
-  o.sto[s_vgs] = vgs;
-  o.sto[s_vds] = vds;
-  o.sto[s_vges] = vges;
-  o.sto[s_vgms] = vgms;
-  o.sto[s_vdes] = vdes;
-  o.sto[s_vses] = vses;
-  o.sto[s_vdbs] = vdbs;
-  o.sto[s_vsbs] = vsbs;
-  o.sto[s_vdbd] = vdbd;
-  o.sto[s_vged] = 0.0;
-  o.sto[s_vgmd] = 0.0;
-  o.sto[s_von] = von;
-  const double qg = qgate;
-  const double qd = qdrn - qbd;
-  const double qb = qbulk + qbd + qbs;
-  o.sta[t_qg] = qg;
-  o.sta[t_qd] = qd;
-  o.sta[t_qb] = qb;
-  o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
-  o.vgb = vgb;
-
-  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0.
-  const double gjbd = gbd, gjbs = gbs;
-  double Gmv, Gmbsv, FwdSum, RevSum, ceqdrn, ceqdrn_Jdxp, ceqbd, ceqbd_Jdxp, ceqbs, ceqbs_Jdxp;
-  double gbbdp, gbbsp, gbdpg, gbdpdp, gbdpb, gbdpsp, gbspg, gbspdp, gbspb, gbspsp;
-  if (mode >= 0) {
-    Gmv = gm;
-    Gmbsv = gmbs;
-    FwdSum = Gmv + Gmbsv;
-    RevSum = 0.0;
-    ceqdrn = dtype * cdrain;
-    ceqdrn_Jdxp = dtype * (-gds * (vds - vds_orig) - Gmv * (vgs - vgs_orig) - Gmbsv * (vbs - vbs_orig));
-    ceqbd = dtype * (csub + Igidl);
-    ceqbd_Jdxp = dtype * (-(gbds + ggidld) * (vds - vds_orig) - (gbgs + ggidlg) * (vgs - vgs_orig) -
-                          (gbbs + ggidlb) * (vbs - vbs_orig));
-    ceqbs = dtype * Igisl;
-    ceqbs_Jdxp = dtype * (+ggisls * (vds - vds_orig) - ggislg * (vgd - vgd_orig) - ggislb * (vbd - vbd_orig));
-    gbbdp = -(gbds);
-    gbbsp = gbds + gbgs + gbbs;
-    gbdpg = gbgs;
-    gbdpdp = gbds;
-    gbdpb = gbbs;
-    gbdpsp = -(gbdpg + gbdpdp + gbdpb);
-    gbspg = 0.0;
-    gbspdp = 0.0;
-    gbspb = 0.0;
-    gbspsp = 0.0;
-  } else {
-    Gmv = -gm;
-    Gmbsv = -gmbs;
-    FwdSum = 0.0;
-    RevSum = -(Gmv + Gmbsv);
-    ceqdrn = -dtype * cdrain;
-    ceqdrn_Jdxp = -dtype * (+gds * (vds - vds_orig) + Gmv * (vgd - vgd_orig) + Gmbsv * (vbd - vbd_orig));
-    ceqbs = dtype * (csub + Igisl);
-    ceqbs_Jdxp = dtype * (+(gbds + ggisls) * (vds - vds_orig) - (gbgs + ggislg) * (vgd - vgd_orig) -
-                          (gbbs + ggislb) * (vbd - vbd_orig));
-    ceqbd = dtype * Igidl;
-    ceqbd_Jdxp = dtype * (-ggidld * (vds - vds_orig) - ggidlg * (vgs - vgs_orig) - ggidlb * (vbs - vbs_orig));
-    gbbsp = -(gbds);
-    gbbdp = gbds + gbgs + gbbs;
-    gbdpg = 0.0;
-    gbdpsp = 0.0;
-    gbdpb = 0.0;
-    gbdpdp = 0.0;
-    gbspg = gbgs;
-    gbspsp = gbds;
-    gbspb = gbbs;
-    gbspdp = -(gbspg + gbspsp + gbspb);
-  }
-  // Gate-current totals (:13112-13170, mode >= 0; :13243-13300, mode < 0).
-  const double ceqgcrg = 0.0, ceqgcrg_Jdxp = 0.0;
-  double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0;
-  double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0;
-  double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
-  double gIdtotg = 0.0, gIdtotd = 0.0, gIdtots = 0.0, gIdtotb = 0.0;
-  double gIbtotg = 0.0, gIbtotd = 0.0, gIbtots = 0.0, gIbtotb = 0.0;
-  double gIgtotg = 0.0, gIgtotd = 0.0, gIgtots = 0.0, gIgtotb = 0.0;
-  if (mode >= 0) {
-    if (igcMod) {
-      gIstotg = gIgsg + gIgcsg;
-      gIstotd = gIgcsd;
-      gIstots = gIgss + gIgcss;
-      gIstotb = gIgcsb;
-      Istoteq = dtype * (Igs + Igcs);
-      Istoteq_Jdxp = dtype * (-gIstotg * (vgs - vgs_orig) - gIgcsd * (vds - vds_orig) - gIgcsb * (vbs - vbs_orig));
-      gIdtotg = gIgdg + gIgcdg;
-      gIdtotd = gIgdd + gIgcdd;
-      gIdtots = gIgcds;
-      gIdtotb = gIgcdb;
-      Idtoteq = dtype * (Igd + Igcd);
-      Idtoteq_Jdxp = dtype * (-gIgdg * (vgd - vgd_orig) - gIgcdg * (vgs - vgs_orig) - gIgcdd * (vds - vds_orig) -
-                              gIgcdb * (vbs - vbs_orig));
-    }
-    if (igbMod) {
-      gIbtotg = gIgbg;
-      gIbtotd = gIgbd;
-      gIbtots = gIgbs;
-      gIbtotb = gIgbb;
-      Ibtoteq = dtype * Igb;
-      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgs - vgs_orig) - gIgbd * (vds - vds_orig) - gIgbb * (vbs - vbs_orig));
-    }
-  } else {
-    if (igcMod) {
-      gIstotg = gIgsg + gIgcdg;
-      gIstotd = gIgcds;
-      gIstots = gIgss + gIgcdd;
-      gIstotb = gIgcdb;
-      Istoteq = dtype * (Igs + Igcd);
-      Istoteq_Jdxp = dtype * (-gIgsg * (vgs - vgs_orig) - gIgcdg * (vgd - vgd_orig) + gIgcdd * (vds - vds_orig) -
-                              gIgcdb * (vbd - vbd_orig));
-      gIdtotg = gIgdg + gIgcsg;
-      gIdtotd = gIgdd + gIgcss;
-      gIdtots = gIgcsd;
-      gIdtotb = gIgcsb;
-      Idtoteq = dtype * (Igd + Igcs);
-      Idtoteq_Jdxp = dtype * (-(gIgdg + gIgcsg) * (vgd - vgd_orig) + gIgcsd * (vds - vds_orig) -
-                              gIgcsb * (vbd - vbd_orig));
-    }
-    if (igbMod) {
-      gIbtotg = gIgbg;
-      gIbtotd = gIgbs;
-      gIbtots = gIgbd;
-      gIbtotb = gIgbb;
-      Ibtoteq = dtype * Igb;
-      Ibtoteq_Jdxp = dtype * (-gIgbg * (vgd - vgd_orig) + gIgbd * (vds - vds_orig) - gIgbb * (vbd - vbd_orig));
-    }
-  }
-  if (igcMod != 0 || igbMod != 0) {
-    gIgtotg = gIstotg + gIdtotg + gIbtotg;
-    gIgtotd = gIstotd + gIdtotd + gIbtotd;
-    gIgtots = gIstots + gIdtots + gIbtots;
-    gIgtotb = gIstotb + gIdtotb + gIbtotb;
-    Igtoteq = Istoteq + Idtoteq + Ibtoteq;
-    Igtoteq_Jdxp = Istoteq_Jdxp + Idtoteq_Jdxp + Ibtoteq_Jdxp;
-  }
-  const double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
-  const double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
-  double ceqjs, ceqjs_Jdxp, ceqjd, ceqjd_Jdxp;
-  if (dtype > 0) {
-    ceqjs = (cbs);
-    ceqjs_Jdxp = (-gbs * (vbs_jct - vbs_jct_orig));
-    ceqjd = (cbd);
-    ceqjd_Jdxp = (-gbd * (vbd_jct - vbd_jct_orig));
-  } else {
-    ceqjs = -(cbs);
-    ceqjs_Jdxp = (gbs * (vbs_jct - vbs_jct_orig));
-    ceqjd = -(cbd);
-    ceqjd_Jdxp = (gbd * (vbd_jct - vbd_jct_orig));
-  }
-
-  // Master::loadDAEVectors (:16316-16564). Local order D, G, S, B.
-  const bool lim = fl.voltlim && !origFlag;
-  for (int k = 0; k < kNumVec; ++k) o.vec[k] = 0.0;
-  o.vec[0] += -(ceqjd - ceqbd - ceqdrn + Idtoteq) * M;
-  o.vec[1] -= -(-ceqgcrg + Igtoteq) * M;
-  o.vec[3] += -(ceqbd + ceqbs - ceqjd - ceqjs + Ibtoteq) * M;
-  o.vec[2] += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
-  if (SERIES) {
-    // Linear terminal resistor currents (:11901-11904, 16360-16370), where the node exists.
-    o.vecx[0] = 0.0;
-    o.vecx[1] = 0.0;
-    if (P(dExists) != 0.0) {
-      const double Idrain = P(drainConductance) * Vddp;
-      o.vecx[0] += -(-Idrain) * M;
-      o.vec[0] += -(Idrain)*M;
-    }
-    if (P(sExists) != 0.0) {
-      const double Isource = P(sourceConductance) * Vssp;
-      o.vecx[1] += -(-Isource) * M;
-      o.vec[2] += -(+Isource) * M;
-    }
-  }
-  if (lim) {
-    o.vec[8 + 0] += (ceqjd_Jdxp - ceqbd_Jdxp - ceqdrn_Jdxp + Idtoteq_Jdxp) * M;
-    o.vec[8 + 1] -= (-ceqgcrg_Jdxp + Igtoteq_Jdxp) * M;
-    o.vec[8 + 3] += (ceqbd_Jdxp + ceqbs_Jdxp - ceqjd_Jdxp - ceqjs_Jdxp + Ibtoteq_Jdxp) * M;
-    o.vec[8 + 2] += (ceqdrn_Jdxp - ceqbs_Jdxp + ceqjs_Jdxp + Istoteq_Jdxp) * M;
-  }
-  // auxChargeCalculations (:12216-12350).
-  double Qeqqg_Jdxp = 0.0, Qeqqd_Jdxp = 0.0, Qeqqb_Jdxp = 0.0;
-  if (ChargeComputationNeeded && !origFlag) {
-    Qeqqg_Jdxp = -CAPcggb * (vgb - vgb_orig) + CAPcgdb * (vbd - vbd_orig) + CAPcgsb * (vbs - vbs_orig);
-    Qeqqd_Jdxp = -CAPcdgb * (vgb - vgb_orig) - CAPcdgmb * (vgmb - vgmb_orig) +
-                 (CAPcddb + 0.0) * (vbd - vbd_orig) - 0.0 * (vbd_jct - vbd_jct_orig) + CAPcdsb * (vbs - vbs_orig);
-    Qeqqb_Jdxp = -CAPcbgb * (vgb - vgb_orig) - CAPcbgmb * (vgmb - vgmb_orig) + CAPcbdb * (vbd - vbd_orig) +
-                 CAPcbsb * (vbs - vbs_orig);
-  }
-  const double Qeqqgmid_Jdxp = 0.0, Qeqqgmid = 0.0;
-  double Qeqqg, Qeqqd, Qeqqb;
-  if (dtype > 0) {
-    Qeqqg = qg;
-    Qeqqd = qd;
-    Qeqqb = qb;
-  } else {
-    Qeqqg = -qg;
-    Qeqqd = -qd;
-    Qeqqb = -qb;
-  }
-  o.vec[4 + 0] += -(-Qeqqd) * M;
-  o.vec[4 + 1] -= -(Qeqqg) * M;
-  o.vec[4 + 3] += -(-Qeqqb) * M;
-  o.vec[4 + 2] += -(+Qeqqg + Qeqqb + Qeqqd + Qeqqgmid) * M;
-  if (lim) {
-    o.vec[12 + 0] += (-Qeqqd_Jdxp) * M;
-    o.vec[12 + 1] -= (Qeqqg_Jdxp) * M;
-    o.vec[12 + 3] += (-Qeqqb_Jdxp) * M;
-    o.vec[12 + 2] += (+Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqd_Jdxp + Qeqqgmid_Jdxp) * M;
-  }
-
-  // Master::loadDAEMatrices (:16577-17268). Rows/cols D=0 G=1 S=2 B=3.
-  for (int k = 0; k < kNumMat; ++k) {
-    o.jf[k] = 0.0;
-    o.jq[k] = 0.0;
-  }
-  const double gdpr = P(drainConductance), gspr = P(sourceConductance);
-  const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
-  const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
-  const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
-  const double Tq = 0.0;  // qdef * gtau with no NQS charge
-#define JF(r, c) o.jf[(r)*4 + (c)]
-#define JQ(r, c) o.jq[(r)*4 + (c)]
-  JF(1, 1) += (-ggtg + gIgtotg) * M;
-  JF(1, 0) += (-ggtd + gIgtotd) * M;
-  JF(1, 2) += (-ggts + gIgtots) * M;
-  JF(1, 3) += (-ggtb + gIgtotb) * M;
-  JF(0, 0) += (gdpr + gds + gbd + Tq * ddxpart_dVd - gdtotd + RevSum + gbdpdp + dxpart * ggtd - gIdtotd) * M;
-  if (SERIES) {
-    for (int k = 0; k < 6; ++k) o.jfx[k] = 0.0;
-  }
-  // The resistor couplings (D', D), (D, D'), (D, D) and the source's: their own slots with internal
-  // nodes, the collapsed (D, D) / (S, S) entry otherwise.
-#define JRES(k, r) (*(SERIES ? &o.jfx[k] : &JF(r, r)))
-  JRES(0, 0) -= (gdpr + gdtot) * M;
-  JF(0, 1) += (Gmv - gdtotg + gbdpg - gIdtotg + dxpart * ggtg + Tq * ddxpart_dVg) * M;
-  JF(0, 2) -= (gds + gdtots - dxpart * ggts + gIdtots - Tq * ddxpart_dVs + FwdSum - gbdpsp) * M;
-  JF(0, 3) -= (gjbd + gdtotb - Gmbsv - gbdpb + gIdtotb - Tq * ddxpart_dVb - dxpart * ggtb) * M;
-  JRES(1, 0) -= (gdpr - gdtotd) * M;
-  JRES(2, 0) += (gdpr + gdtot) * M;
-  JF(2, 0) -= (gds + gstotd + RevSum - gbspdp - Tq * dsxpart_dVd - sxpart * ggtd + gIstotd) * M;
-  JF(2, 1) += (-Gmv - gstotg + gbspg + sxpart * ggtg + Tq * dsxpart_dVg - gIstotg) * M;
-  JF(2, 2) += (gspr + gds + gbs + Tq * dsxpart_dVs - gstots + FwdSum + gbspsp + sxpart * ggts - gIstots) * M;
-  JRES(3, 2) -= (gspr + gstot) * M;
-  JF(2, 3) -= (gjbs + gstotb + Gmbsv - gbspb - sxpart * ggtb - Tq * dsxpart_dVb + gIstotb) * M;
-  JRES(4, 2) -= (gspr - gstots) * M;
-  JRES(5, 2) += (gspr + gstot) * M;
-#undef JRES
-  JF(3, 0) += (-gjbd + gbbdp - gIbtotd) * M;
-  JF(3, 1) += (-gbgs - gIbtotg) * M;
-  JF(3, 2) += (-gjbs + gbbsp - gIbtots) * M;
-  JF(3, 3) += (gjbd + gjbs - gbbs - gIbtotb) * M;
-  JF(0, 0) += (ggidld) * M;
-  JF(0, 1) += (ggidlg) * M;
-  JF(0, 2) -= ((ggidlg + ggidld + ggidlb)) * M;
-  JF(0, 3) += (ggidlb) * M;
-  JF(3, 0) -= (ggidld) * M;
-  JF(3, 1) -= (ggidlg) * M;
-  JF(3, 2) += ((ggidlg + ggidld + ggidlb)) * M;
-  JF(3, 3) -= (ggidlb) * M;
-  JF(2, 0) -= ((ggisls + ggislg + ggislb)) * M;
-  JF(2, 1) += (ggislg) * M;
-  JF(2, 2) += (ggisls) * M;
-  JF(2, 3) += (ggislb) * M;
-  JF(3, 0) += ((ggislg + ggisls + ggislb)) * M;
-  JF(3, 1) -= (ggislg) * M;
-  JF(3, 2) -= (ggisls) * M;
-  JF(3, 3) -= (ggislb) * M;
-  if (!(!fl.dcop && fl.init_tran && fl.newton_iter == 0)) {
-    JQ(1, 1) += (CAPcggb) * M;
-    JQ(1, 0) += (CAPcgdb) * M;
-    JQ(1, 2) += (CAPcgsb) * M;
-    JQ(1, 3) += (CAPcgbb) * M;
-    JQ(0, 0) += (CAPcddb) * M;
-    JQ(0, 1) += (+CAPcdgb) * M;
-    JQ(0, 2) -= (-CAPcdsb) * M;
-    JQ(0, 3) -= (-CAPcdbb) * M;
-    JQ(2, 0) -= (-CAPcsdb) * M;
-    JQ(2, 1) += (CAPcsgb) * M;
-    JQ(2, 2) += (CAPcssb) * M;
-    JQ(2, 3) -= (-CAPcsbb) * M;
-    JQ(3, 0) += (CAPcbdb) * M;
-    JQ(3, 1) += (CAPcbgb) * M;
-    JQ(3, 2) += (CAPcbsb) * M;
-    JQ(3, 3) += (CAPcbbb) * M;
-  }
-#undef JF
-#undef JQ
-#undef P
+  bsim4_finish<FULL, SERIES>(P_, V, fl, vgb_orig, hm, o, Vx);
 }
+#undef P
 
 }  // namespace xb4

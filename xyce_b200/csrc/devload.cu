@@ -99,47 +99,25 @@ struct xd_ctx {
   bool series = false;
   int2 *d_ext = nullptr;
   int vec_rows = 4, mat_slots = xb4::kNumMat, stage_slots = xb4::kNumStage;
-  int resident_blocks[16] = {};  // per persistent launch shape: blocks resident on the whole device
+  int resident_blocks[32] = {};  // per persistent launch shape: blocks resident on the whole device
   // The last evaluation was xd_load_static_scratch: its staged stamps are in the library's static
   // array, so d_stage does not hold them and the calls that read d_stage refuse until the next
   // xd_update_state.
   bool stage_static = false;
+  // Hand-off state between the two kernels of a split evaluation (kNumMid slots per instance,
+  // slot-major); allocated for the BSIM4 families the split launch shapes evaluate.
+  double *d_mid = nullptr;
 };
 
 namespace {
 
-// One instance's evaluation and staging. SERIES: the family has internal drain / source nodes; ext
-// holds the external drain and source of each instance and the staging layout is the wide one
-// (6 vector rows, 22 matrix slots).
-template <bool FULL, bool SERIES>
-__device__ __forceinline__ void bsim4_eval_one(
-    int i, int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec,
-    const int4 *__restrict__ nodes, const double *__restrict__ sol, double *__restrict__ next_sta,
-    double *__restrict__ curr_sta, double *__restrict__ next_sto, const double *__restrict__ curr_sto,
-    double *__restrict__ vgb, double *__restrict__ stage, const xb4::LoadFlags &fl, const int2 *__restrict__ ext) {
-  const int4 nd = nodes[i];
-  double V[4];
-  V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
-  V[1] = nd.y >= 0 ? sol[nd.y] : 0.0;
-  V[2] = nd.z >= 0 ? sol[nd.z] : 0.0;
-  V[3] = nd.w >= 0 ? sol[nd.w] : 0.0;
-  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
-  double sto_old[xb4::kNumStore];
-#pragma unroll
-  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = 0.0;
-  sto_old[xb4::s_vbd] = so[(size_t)xb4::s_vbd * n + i];
-  sto_old[xb4::s_vbs] = so[(size_t)xb4::s_vbs * n + i];
-  sto_old[xb4::s_vgs] = so[(size_t)xb4::s_vgs * n + i];
-  sto_old[xb4::s_vds] = so[(size_t)xb4::s_vds * n + i];
-  sto_old[xb4::s_von] = so[(size_t)xb4::s_von * n + i];
-  xb4::RecPtr rp{tab + rec[i], nrec};
-  xb4::LoadOut o;
+// Writes one instance's evaluation results: the staged stamps (the 4-terminal layout, or with SERIES
+// the wide one: 6 vector rows, 22 matrix slots), the store and state entries, and vgb.
+template <bool SERIES>
+__device__ __forceinline__ void bsim4_write_one(int i, int n, const xb4::LoadOut &o, double *__restrict__ next_sta,
+                                                double *__restrict__ curr_sta, double *__restrict__ next_sto,
+                                                double *__restrict__ vgb, double *__restrict__ stage) {
   if (SERIES) {
-    const int2 ex = ext[i];
-    double Vx[2];
-    Vx[0] = ex.x >= 0 ? sol[ex.x] : 0.0;
-    Vx[1] = ex.y >= 0 ? sol[ex.y] : 0.0;
-    xb4::bsim4_load<FULL, true>(rp, V, sto_old, fl, vgb[i], o, Vx);
     // Wide layout: vector v, row r at (v * 6 + r); rows 4 and 5 (external D, S) carry F only.
 #pragma unroll
     for (int v = 0; v < 4; ++v)
@@ -155,7 +133,6 @@ __device__ __forceinline__ void bsim4_eval_one(
 #pragma unroll
     for (int k = 0; k < xb4::kNumMat; ++k) stage[(mq + k) * n + i] = o.jq[k];
   } else {
-    xb4::bsim4_load<FULL, false>(rp, V, sto_old, fl, vgb[i], o);
 #pragma unroll
     for (int k = 0; k < xb4::kNumVec; ++k) stage[(size_t)k * n + i] = o.vec[k];
 #pragma unroll
@@ -173,6 +150,100 @@ __device__ __forceinline__ void bsim4_eval_one(
     for (int k = 0; k < xb4::kNumState; ++k) curr_sta[(size_t)k * n + i] = o.sta[k];
   }
   vgb[i] = o.vgb;
+}
+
+// One instance's node voltages (D, G, S, B; ground reads 0 V) and, with SERIES, its external
+// drain and source voltages.
+template <bool SERIES>
+__device__ __forceinline__ void bsim4_gather_v(int i, const int4 *__restrict__ nodes, const int2 *__restrict__ ext,
+                                               const double *__restrict__ sol, double V[4], double Vx[2]) {
+  const int4 nd = nodes[i];
+  V[0] = nd.x >= 0 ? sol[nd.x] : 0.0;
+  V[1] = nd.y >= 0 ? sol[nd.y] : 0.0;
+  V[2] = nd.z >= 0 ? sol[nd.z] : 0.0;
+  V[3] = nd.w >= 0 ? sol[nd.w] : 0.0;
+  if (SERIES) {
+    const int2 ex = ext[i];
+    Vx[0] = ex.x >= 0 ? sol[ex.x] : 0.0;
+    Vx[1] = ex.y >= 0 ? sol[ex.y] : 0.0;
+  } else {
+    Vx[0] = Vx[1] = 0.0;
+  }
+}
+
+// The store values the limiter compares against (currSto on Newton step 0, nextSto otherwise).
+__device__ __forceinline__ void bsim4_sto_old(int i, int n, const double *__restrict__ next_sto,
+                                              const double *__restrict__ curr_sto, const xb4::LoadFlags &fl,
+                                              double sto_old[xb4::kNumStore]) {
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = 0.0;
+  sto_old[xb4::s_vbd] = so[(size_t)xb4::s_vbd * n + i];
+  sto_old[xb4::s_vbs] = so[(size_t)xb4::s_vbs * n + i];
+  sto_old[xb4::s_vgs] = so[(size_t)xb4::s_vgs * n + i];
+  sto_old[xb4::s_vds] = so[(size_t)xb4::s_vds * n + i];
+  sto_old[xb4::s_von] = so[(size_t)xb4::s_von * n + i];
+}
+
+// One instance's evaluation and staging. SERIES: the family has internal drain / source nodes; ext
+// holds the external drain and source of each instance and the staging layout is the wide one
+// (6 vector rows, 22 matrix slots).
+template <bool FULL, bool SERIES>
+__device__ __forceinline__ void bsim4_eval_one(
+    int i, int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec,
+    const int4 *__restrict__ nodes, const double *__restrict__ sol, double *__restrict__ next_sta,
+    double *__restrict__ curr_sta, double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    double *__restrict__ vgb, double *__restrict__ stage, const xb4::LoadFlags &fl, const int2 *__restrict__ ext) {
+  double V[4], Vx[2], sto_old[xb4::kNumStore];
+  bsim4_gather_v<SERIES>(i, nodes, ext, sol, V, Vx);
+  bsim4_sto_old(i, n, next_sto, curr_sto, fl, sto_old);
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load<FULL, SERIES>(rp, V, sto_old, fl, vgb[i], o, Vx);
+  bsim4_write_one<SERIES>(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
+}
+
+// Split evaluation, first kernel: the DC part of one instance (limiting, junction diodes, drain
+// current, GIDL / GISL, gate tunnelling); its hand-off state goes to mid, slot-major.
+template <int BLOCK, int MINB, bool FULL, bool SERIES>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_dc_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, const double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    const double *__restrict__ vgb, xb4::LoadFlags fl, const int2 *__restrict__ ext, double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[4], Vx[2], sto_old[xb4::kNumStore];
+  bsim4_gather_v<SERIES>(i, nodes, ext, sol, V, Vx);
+  bsim4_sto_old(i, n, next_sto, curr_sto, fl, sto_old);
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::Mid m;
+  xb4::bsim4_load<FULL, SERIES, 1>(rp, V, sto_old, fl, vgb[i], o, Vx, &m);
+  constexpr int nm = FULL ? xb4::kNumMidFull : xb4::kNumMid;
+#pragma unroll
+  for (int f = 0; f < nm; ++f) mid[(size_t)f * n + i] = m.v[f];
+}
+
+// Split evaluation, second kernel: charges, capacitances, store / state and the stamps of one
+// instance from the DC part's hand-off state; writes the same outputs as bsim4_eval_kernel.
+template <int BLOCK, int MINB, bool FULL, bool SERIES>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_charge_stamp_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, double *__restrict__ vgb, double *__restrict__ stage, xb4::LoadFlags fl,
+    const int2 *__restrict__ ext, const double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[4], Vx[2];
+  bsim4_gather_v<SERIES>(i, nodes, ext, sol, V, Vx);
+  xb4::Mid m;
+  constexpr int nm = FULL ? xb4::kNumMidFull : xb4::kNumMid;
+#pragma unroll
+  for (int f = 0; f < nm; ++f) m.v[f] = mid[(size_t)f * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load<FULL, SERIES, 2>(rp, V, nullptr, fl, vgb[i], o, Vx, &m);
+  bsim4_write_one<SERIES>(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
 }
 
 // One thread per instance. PERSIST: the grid is one wave of resident blocks that walks the
@@ -201,8 +272,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_eval_kernel(
 // MOSFET level 1: one thread per instance; reads the previous time point's Meyer state for
 // back-averaging. SERIES: the nodes are (D', G, S', B), ext the external (D, S), and the staging
 // is the wide layout.
-template <bool SERIES>
-__global__ void __launch_bounds__(128) mos1_eval_kernel(
+template <int BLOCK, int MINB, bool SERIES>
+__global__ void __launch_bounds__(BLOCK, MINB) mos1_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, const double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
@@ -482,8 +553,8 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(double *out, int iters) 
 // circuit and keeps the fastest.
 // BSIM3: one thread per instance. SERIES: internal drain / source nodes (ext = external D, S),
 // wide staging layout, as for BSIM4.
-template <bool SERIES>
-__global__ void __launch_bounds__(128) bsim3_eval_kernel(
+template <int BLOCK, int MINB, bool SERIES>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim3_eval_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
     const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
     double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ stage,
@@ -543,24 +614,40 @@ __global__ void __launch_bounds__(128) bsim3_eval_kernel(
 }
 
 struct EvalVariant {
+  int family;    // the model family the candidate evaluates
   int block, min_blocks;
-  bool full;     // compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
-  bool series;   // internal drain / source nodes, wide staging layout
+  bool full;     // BSIM4: compiled with every supported option (capMod 0/1, gate tunnelling), not only the common card
+  bool series;   // BSIM4: internal drain / source nodes, wide staging layout (BSIM3 / MOSFET1 take either layout)
   bool persist;  // one wave of resident blocks with a grid-stride loop
+  bool split;    // two kernels: the DC part (min_blocks), then charges and stamps (min_blocks2)
+  int min_blocks2;
 };
+constexpr int B4 = 4, B3 = 3, M1 = 1;  // kFamilyBsim4, kFamilyBsim3, kFamilyMos1
 constexpr EvalVariant kEvalVariants[] = {
-    {128, 1, false, false, false}, {128, 2, false, false, false}, {128, 3, false, false, false},
-    {128, 4, false, false, false}, {64, 4, false, false, false},  {256, 2, false, false, false},
-    {128, 2, true, false, false},  {128, 3, true, false, false},  {128, 2, true, true, false},
-    {128, 3, true, true, false},   {128, 3, false, false, true},  {128, 3, true, false, true}};
-constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8;
-// A variant computes a context's loads exactly if its staging layout is the context's and it is a
-// full one or the context's cards use only the common options.
+    {B4, 128, 1, false, false, false, false, 0}, {B4, 128, 2, false, false, false, false, 0},
+    {B4, 128, 3, false, false, false, false, 0}, {B4, 128, 4, false, false, false, false, 0},
+    {B4, 64, 4, false, false, false, false, 0},  {B4, 256, 2, false, false, false, false, 0},
+    {B4, 128, 2, true, false, false, false, 0},  {B4, 128, 3, true, false, false, false, 0},
+    {B4, 128, 2, true, true, false, false, 0},   {B4, 128, 3, true, true, false, false, 0},
+    {B4, 128, 3, false, false, true, false, 0},  {B4, 128, 3, true, false, true, false, 0},
+    {B4, 128, 3, false, false, false, true, 3},  {B4, 128, 4, false, false, false, true, 4},
+    {B4, 128, 5, false, false, false, true, 5},  {B4, 128, 4, false, false, false, true, 3},
+    {B3, 128, 1, false, false, false, false, 0}, {B3, 128, 2, false, false, false, false, 0},
+    {B3, 128, 3, false, false, false, false, 0}, {B3, 64, 4, false, false, false, false, 0},
+    {M1, 128, 1, false, false, false, false, 0}, {M1, 128, 4, false, false, false, false, 0},
+    {M1, 256, 2, false, false, false, false, 0}, {M1, 64, 8, false, false, false, false, 0}};
+constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8, kFirstBsim3Variant = 16, kFirstMos1Variant = 20;
+// A variant computes a context's loads exactly if it is for the context's family and, for BSIM4, its
+// staging layout is the context's and it is a full one or the context's cards use only the common
+// options; a split one also needs the context's hand-off buffer.
 bool variant_fits(const xd_ctx *ctx, int v) {
-  return kEvalVariants[v].series == ctx->series && (kEvalVariants[v].full || !ctx->needs_full);
+  const EvalVariant &e = kEvalVariants[v];
+  if (e.family != ctx->family) return false;
+  if (ctx->family != kFamilyBsim4) return true;
+  return e.series == ctx->series && (e.full || !ctx->needs_full) && (!e.split || ctx->d_mid != nullptr);
 }
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
-static_assert(kNumEvalVariants <= 16, "resident_blocks holds 16 launch shapes");
+static_assert(kNumEvalVariants <= 32, "resident_blocks holds 32 launch shapes");
 
 // The persistent launch shapes' kernels (for the occupancy query).
 const void *persistent_eval_kernel(int v) {
@@ -592,30 +679,73 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
                  double *curr_sta, double *next_sto, const double *curr_sto, double *stage, cudaStream_t st) {
   const int n = ctx->n;
   if (ctx->family == kFamilyMos1) {
-    if (ctx->series)
-      mos1_eval_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
-                                                              next_sta, curr_sta, next_sto, curr_sto, stage, fl,
-                                                              ctx->d_ext);
-    else
-      mos1_eval_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol,
-                                                               next_sta, curr_sta, next_sto, curr_sto, stage, fl,
-                                                               nullptr);
+    const int blk = kEvalVariants[v].block, grid = (n + blk - 1) / blk;
+#define XD_M1_ARGS(E) n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
+                      stage, fl, E
+#define XD_M1(B, M)                                                                         \
+  if (ctx->series)                                                                          \
+    mos1_eval_kernel<B, M, true><<<grid, blk, 0, st>>>(XD_M1_ARGS(ctx->d_ext));             \
+  else                                                                                      \
+    mos1_eval_kernel<B, M, false><<<grid, blk, 0, st>>>(XD_M1_ARGS(nullptr));
+    switch (v - kFirstMos1Variant) {
+      case 0: XD_M1(128, 1); break;
+      case 1: XD_M1(128, 4); break;
+      case 2: XD_M1(256, 2); break;
+      default: XD_M1(64, 8); break;
+    }
+#undef XD_M1
+#undef XD_M1_ARGS
     return;
   }
   if (ctx->family == kFamilyBsim3) {
-    if (ctx->series)
-      bsim3_eval_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes,
-                                                               sol, next_sta, curr_sta, next_sto, curr_sto, stage, fl,
-                                                               ctx->d_ext);
-    else
-      bsim3_eval_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes,
-                                                                sol, next_sta, curr_sta, next_sto, curr_sto, stage,
-                                                                fl, nullptr);
+    const int blk = kEvalVariants[v].block, grid = (n + blk - 1) / blk;
+#define XD_B3_ARGS(E) n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
+                      stage, fl, E
+#define XD_B3(B, M)                                                                         \
+  if (ctx->series)                                                                          \
+    bsim3_eval_kernel<B, M, true><<<grid, blk, 0, st>>>(XD_B3_ARGS(ctx->d_ext));            \
+  else                                                                                      \
+    bsim3_eval_kernel<B, M, false><<<grid, blk, 0, st>>>(XD_B3_ARGS(nullptr));
+    switch (v - kFirstBsim3Variant) {
+      case 0: XD_B3(128, 1); break;
+      case 1: XD_B3(128, 2); break;
+      case 2: XD_B3(128, 3); break;
+      default: XD_B3(64, 4); break;
+    }
+#undef XD_B3
+#undef XD_B3_ARGS
     return;
   }
   const int blk = kEvalVariants[v].block;
   int grid = (n + blk - 1) / blk;
   if (kEvalVariants[v].persist) grid = std::max(1, std::min(grid, ctx->resident_blocks[v]));
+  if (kEvalVariants[v].split) {
+#define XD_DC_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sto, curr_sto, ctx->d_vgb, fl, ctx->d_ext, \
+                   ctx->d_mid
+#define XD_CS_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, ctx->d_vgb, \
+                   stage, fl, ctx->d_ext, ctx->d_mid
+    switch (v) {
+      case 12:
+        bsim4_dc_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
+        bsim4_charge_stamp_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
+        break;
+      case 13:
+        bsim4_dc_kernel<128, 4, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
+        bsim4_charge_stamp_kernel<128, 4, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
+        break;
+      case 14:
+        bsim4_dc_kernel<128, 5, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
+        bsim4_charge_stamp_kernel<128, 5, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
+        break;
+      default:
+        bsim4_dc_kernel<128, 4, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
+        bsim4_charge_stamp_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
+        break;
+    }
+#undef XD_DC_ARGS
+#undef XD_CS_ARGS
+    return;
+  }
 #define XD_EVAL_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sta, curr_sta, next_sto, curr_sto, \
                      ctx->d_vgb, stage, fl, ctx->d_ext
   switch (v) {
@@ -630,7 +760,8 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
     case 8: bsim4_eval_kernel<128, 2, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
     case 9: bsim4_eval_kernel<128, 3, true, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
     case 10: bsim4_eval_kernel<128, 3, false, false, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
-    default: bsim4_eval_kernel<128, 3, true, false, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    case 11: bsim4_eval_kernel<128, 3, true, false, true><<<grid, blk, 0, st>>>(XD_EVAL_ARGS); break;
+    default: break;
   }
 #undef XD_EVAL_ARGS
 }
@@ -658,22 +789,30 @@ void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned
 // Times every launch shape on the circuit's own instances at a synthetic operating point (node
 // voltages spread over 0..1.2 V, transient flags) in scratch buffers, and returns the fastest.
 int autotune_eval(xd_ctx *ctx, int &best) {
-  best = ctx->series ? kFirstSeriesVariant : (ctx->needs_full ? kFirstFullVariant : 0);
+  best = ctx->family == kFamilyMos1    ? kFirstMos1Variant
+         : ctx->family == kFamilyBsim3 ? kFirstBsim3Variant
+         : ctx->series                 ? kFirstSeriesVariant
+                                       : (ctx->needs_full ? kFirstFullVariant : 0);
   const int n = ctx->n;
-  if (n < 4096 || ctx->family != kFamilyBsim4) return 0;
+  if (n < 4096) return 0;
+  // State and store blocks of the family's size (BSIM4 3 / 14, BSIM3 5 / 5, MOSFET1 8 / 5 slots).
+  const size_t nsta = ctx->family == kFamilyMos1 ? xm1::kNumState
+                      : ctx->family == kFamilyBsim3 ? xb3::kNumState : xb4::kNumState;
+  const size_t nsto = ctx->family == kFamilyMos1 ? xm1::kNumStore
+                      : ctx->family == kFamilyBsim3 ? xb3::kNumStore : xb4::kNumStore;
   double *sol = nullptr, *sta = nullptr, *sto = nullptr;
   cudaError_t ce;
   if ((ce = cudaMalloc(&sol, std::max(1, ctx->n_unknowns) * sizeof(double))) != cudaSuccess ||
-      (ce = cudaMalloc(&sta, (size_t)2 * xb4::kNumState * n * sizeof(double))) != cudaSuccess ||
-      (ce = cudaMalloc(&sto, (size_t)2 * xb4::kNumStore * n * sizeof(double))) != cudaSuccess) {
+      (ce = cudaMalloc(&sta, (size_t)2 * nsta * n * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMalloc(&sto, (size_t)2 * nsto * n * sizeof(double))) != cudaSuccess) {
     cudaFree(sol); cudaFree(sta); cudaFree(sto);
     return cuda_fail(ce, "autotune allocation");
   }
   std::vector<double> h(std::max(1, ctx->n_unknowns));
   for (size_t k = 0; k < h.size(); ++k) h[k] = 1.2 * (double)((k * 2654435761u) % 1000u) / 999.0;
   cudaMemcpy(sol, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
-  cudaMemset(sta, 0, (size_t)2 * xb4::kNumState * n * sizeof(double));
-  cudaMemset(sto, 0, (size_t)2 * xb4::kNumStore * n * sizeof(double));
+  cudaMemset(sta, 0, (size_t)2 * nsta * n * sizeof(double));
+  cudaMemset(sto, 0, (size_t)2 * nsto * n * sizeof(double));
   xb4::LoadFlags fl{};
   fl.transient = 1; fl.newton_iter = 1; fl.voltlim = 1; fl.gmin = 1e-12;
   cudaEvent_t e0, e1;
@@ -682,11 +821,11 @@ int autotune_eval(xd_ctx *ctx, int &best) {
   float best_ms = 1e30f;
   for (int v = 0; v < kNumEvalVariants; ++v) {
     if (!variant_fits(ctx, v)) continue;
-    launch_eval(v, ctx, fl, sol, sta, sta + (size_t)xb4::kNumState * n, sto, sto + (size_t)xb4::kNumStore * n,
+    launch_eval(v, ctx, fl, sol, sta, sta + (size_t)nsta * n, sto, sto + (size_t)nsto * n,
                 ctx->d_stage, 0);
     cudaEventRecord(e0, 0);
     for (int r = 0; r < 3; ++r)
-      launch_eval(v, ctx, fl, sol, sta, sta + (size_t)xb4::kNumState * n, sto, sto + (size_t)xb4::kNumStore * n,
+      launch_eval(v, ctx, fl, sol, sta, sta + (size_t)nsta * n, sto, sto + (size_t)nsto * n,
                   ctx->d_stage, 0);
     cudaEventRecord(e1, 0);
     cudaEventSynchronize(e1);
@@ -793,6 +932,7 @@ int xd_destroy(xd_ctx *ctx) {
   cudaFree(ctx->d_vgb);
   cudaFree(ctx->d_stage);
   cudaFree(ctx->d_ext);
+  cudaFree(ctx->d_mid);
   free_map(ctx->vmap);
   free_map(ctx->mmap);
   delete ctx;
@@ -966,6 +1106,9 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   if (series && ((ce = cudaMalloc(&ctx->d_ext, std::max(1, n) * sizeof(int2))) != cudaSuccess ||
                  (ce = cudaMemcpy(ctx->d_ext, ext.data(), n * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess))
     return cleanup(cuda_fail(ce, "xd_create allocation"));
+  if (family == kFamilyBsim4 && !series && !ctx->needs_full && n > 0 &&
+      (ce = cudaMalloc(&ctx->d_mid, (size_t)xb4::kNumMid * n * sizeof(double))) != cudaSuccess)
+    return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
   if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
   if ((rc = size_persistent_grids(ctx)) != 0) return cleanup(rc);
@@ -1081,7 +1224,8 @@ int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double
 int xd_launches_per_load(const xd_ctx *ctx) {
   if (!ctx) return -1;
   if (ctx->n == 0) return 0;
-  return 1 + (ctx->vmap.n_short > 0) + 2 * (ctx->vmap.n_long > 0) + (ctx->mmap.n_short > 0) +
+  const int eval = (ctx->family == kFamilyBsim4 && kEvalVariants[ctx->eval_variant].split) ? 2 : 1;
+  return eval + (ctx->vmap.n_short > 0) + 2 * (ctx->vmap.n_long > 0) + (ctx->mmap.n_short > 0) +
          2 * (ctx->mmap.n_long > 0);
 }
 
@@ -1106,13 +1250,18 @@ int xd_eval_variant_persistent(int v) {
   return kEvalVariants[v].persist ? 1 : 0;
 }
 
+int xd_eval_variant_split(int v) {
+  if (v < 0 || v >= kNumEvalVariants) return fail(-1, "bad variant query");
+  return kEvalVariants[v].split ? 1 : 0;
+}
+
 int xd_get_eval_variant(const xd_ctx *ctx) { return ctx ? ctx->eval_variant : -1; }
 
 int xd_set_eval_variant(xd_ctx *ctx, int v) {
   if (!ctx || v < 0 || v >= kNumEvalVariants) return fail(-1, "bad evaluation variant");
   if (!variant_fits(ctx, v))
-    return fail(-1, "this evaluation variant is compiled for capMod 2 without gate tunnelling, which the family's "
-                    "cards need");
+    return fail(-1, "this evaluation variant does not fit the family: it is compiled for capMod 2 without gate "
+                    "tunnelling, or for another staging layout (internal drain / source nodes)");
   ctx->eval_variant = v;
   return 0;
 }

@@ -62,6 +62,32 @@ int xd_tia_combine(xd_tia *t, const xd_tia_coef *coef, const double *d_x, const 
                    const double *d_b, const double *d_qn0, const double *d_fhist, double *d_jac,
                    double *d_rhs, double *d_q_tot, double *d_f_tot, void *stream);
 
+/* Fused device load and combine (no counterpart in the reference, where the device manager's loads
+ * and the integrator's combine are separate passes over memory: N_DEV_DeviceMgr.C:2117-2123,
+ * 2452-2461, 2256-2261, then N_TIA_OneStep.C:272-312, 470-497).
+ *
+ * xd_tia_fused_create binds a combine object and a MOSFET family built on the same pattern and
+ * device, and precomputes, per CSR entry and per row, where the family's contributions sit in its
+ * gather maps (set-up only; it allocates). xd_tia_load_combine then does, in one call, what
+ * xd_load_assign (into the family buffers d_fam_*) followed by xd_tia_combine (with those buffers
+ * as dfdx / dqdx / f / q and, when limiter != 0, fx / qx) does, with bit-identical jac, rhs, q_tot
+ * and f_tot: the evaluation kernel stages the stamps, and one pass over the rows forms every Newton
+ * matrix entry and residual straight from them, so the family's dF/dx and dQ/dx never go through
+ * memory (only the few entries with very many contributions, such as supply rails, are summed
+ * into d_fam_dfdx / d_fam_dqdx first). The family's F, Q and limiter vectors are stored into
+ * d_fam_f / d_fam_q / d_fam_fx / d_fam_qx as by xd_load_assign; d_fam_dfdx / d_fam_dqdx hold
+ * the family's sums only at those long entries afterwards. Buffers as for the two calls it
+ * replaces (d_fam_* zeroed once when allocated). */
+typedef struct xd_tia_fused xd_tia_fused;
+int xd_tia_fused_create(xd_tia *t, xd_ctx *family, xd_tia_fused **out);
+int xd_tia_fused_destroy(xd_tia_fused *f);
+int xd_tia_load_combine(xd_tia_fused *f, const xd_flags *flags, const xd_tia_coef *coef, const double *d_x,
+                        double *d_next_sta, double *d_curr_sta, double *d_next_sto, const double *d_curr_sto,
+                        double *d_fam_f, double *d_fam_q, double *d_fam_fx, double *d_fam_qx, double *d_fam_dfdx,
+                        double *d_fam_dqdx, const double *d_lin_dfdx, const double *d_lin_dqdx, int limiter,
+                        const double *d_b, const double *d_qn0, const double *d_fhist, double *d_jac,
+                        double *d_rhs, double *d_q_tot, double *d_f_tot, void *stream);
+
 /* Small dense direct solve of the Newton system J x = rhs (J in the pattern's CSR values), for
  * circuits of at most XD_DENSE_MAX_N unknowns; stands in for the reference's direct solve (KLU
  * through Amesos, src/LinearAlgebraServicesPKG/src/N_LAS_AmesosSolver.C:160, 305) where the

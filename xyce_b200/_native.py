@@ -104,6 +104,10 @@ SIGNATURES = {
     "xd_tia_create": (ctypes.c_int, [ctypes.POINTER(XdCsr), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "xd_tia_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
+    "xd_tia_fused_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_tia_fused_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_tia_load_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags), ctypes.POINTER(XdTiaCoef)] +
+                            [ctypes.c_void_p] * 13 + [ctypes.c_int] + [ctypes.c_void_p] * 8),
     "xd_tia_dense_solve": (ctypes.c_int, [ctypes.c_void_p] * 8),
     "xd_tia_dense_resolve": (ctypes.c_int, [ctypes.c_void_p] * 6),
     "xd_tia_dense_solve_fallback": (ctypes.c_int, [ctypes.c_void_p] * 8),

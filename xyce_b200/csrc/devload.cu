@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/xyce_devload.h"
+#include "../../include/xyce_tia.h"
 #include "bsim4_eval.cuh"
 #include "bsim4_setup.h"
 #include "bsim3.h"
@@ -441,8 +442,9 @@ __global__ void gather_combine_kernel(int n_long, const int *__restrict__ dst, c
 }
 
 template <int NOUT, bool ABS>
-int run_gather(const GatherMap &m, const double *stage, const OutSet<NOUT, ABS> &os, cudaStream_t st) {
-  if (m.n_short > 0) {
+int run_gather(const GatherMap &m, const double *stage, const OutSet<NOUT, ABS> &os, cudaStream_t st,
+               bool short_part = true) {
+  if (short_part && m.n_short > 0) {
     const int blk = 256;
     gather_short_kernel<NOUT, ABS><<<(m.n_short + blk - 1) / blk, blk, 0, st>>>(m.n_short, m.d_short_dst,
                                                                                m.d_short_ptr, m.d_src, stage, os);
@@ -1379,6 +1381,253 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
   OutSet<2, false> ms{{d_dfdx_vals, d_dqdx_vals}, {16 * n, 32 * n}};
   if ((rc = run_gather_static(ctx->mmap, stage, partial, ms, st))) return rc;
   ctx->stage_static = true;
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Fused load and combine. One Newton iterate's device load and the time-integration combine in
+// one pass over the CSR rows: the evaluation kernel stages the instances' stamps as usual, the
+// few entries with more than kLongThreshold contributions (supply rails) are summed by the chunked
+// gathers into the family's buffers, and one warp per row then forms, for every entry of the row,
+// the family's dF/dx and dQ/dx sum straight from the staged stamps (same sources, same order as
+// the gather kernels) and the Newton matrix entry from it, and for the row the family's F, Q and
+// limiter-vector sums and the residual, with the linear devices' terms, exactly as
+// tia_combine_kernel does from the family's stored sums. The family's dF/dx and dQ/dx are never
+// written to memory (except for the long entries) or read back; the results are bit-identical to
+// xd_load_assign followed by xd_tia_combine.
+
+int xd_tia_internal_pattern(const xd_tia *t, int *device, int *n_rows, int *nnz, const int **rowptr,
+                            const int **colind);
+
+struct xd_tia_fused {
+  xd_tia *tia = nullptr;
+  xd_ctx *fam = nullptr;
+  int device = 0, n_rows = 0, nnz = 0;
+  const int *d_rowptr = nullptr, *d_colind = nullptr;
+  int2 *d_ent = nullptr;   // per CSR entry: (first source in the matrix map, count); count -1 = long entry
+  int2 *d_vrow = nullptr;  // per row: (first source in the vector map, count); count -1 = long row
+};
+
+namespace {
+
+constexpr int kFusedWarps = 8;
+
+template <bool TRAN>
+__global__ void __launch_bounds__(32 * kFusedWarps) fused_combine_kernel(
+    int n_rows, const int *__restrict__ rowptr, const int *__restrict__ colind, xd_tia_coef c,
+    const double *__restrict__ x, const int2 *__restrict__ ent, const int *__restrict__ msrc,
+    const int2 *__restrict__ vrow, const int *__restrict__ vsrc, const double *__restrict__ stage, size_t mb_f,
+    size_t mb_q, size_t vb0, size_t vb1, size_t vb2, size_t vb3, const double *__restrict__ long_dfdx,
+    const double *__restrict__ long_dqdx, double *__restrict__ fam_f, double *__restrict__ fam_q,
+    double *__restrict__ fam_fx, double *__restrict__ fam_qx, const double *__restrict__ lin_f,
+    const double *__restrict__ lin_q, int limiter, const double *__restrict__ b, const double *__restrict__ qn0,
+    const double *__restrict__ fhist, double *__restrict__ jac, double *__restrict__ rhs,
+    double *__restrict__ q_tot, double *__restrict__ f_tot) {
+  const int row = blockIdx.x * kFusedWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n_rows) return;
+  const int beg = rowptr[row], end = rowptr[row + 1];
+  double af = 0.0, aq = 0.0;
+  bool has_diag = false;
+  for (int k = beg + lane; k < end; k += 32) {
+    const int2 e = ent[k];
+    double jf, jq = 0.0;
+    if (e.y < 0) {
+      jf = long_dfdx[k];
+      if (TRAN) jq = long_dqdx[k];
+    } else {
+      double sf = 0.0, sq = 0.0;
+      for (int s = e.x; s < e.x + e.y; ++s) {
+        const size_t src = (size_t)msrc[s];
+        sf += stage[mb_f + src];
+        if (TRAN) sq += stage[mb_q + src];
+      }
+      jf = sf;
+      jq = sq;
+    }
+    if (lin_f) {
+      const double g = lin_f[k];
+      jf += g;
+      af += g * x[colind[k]];
+    }
+    if (c.gshunt != 0.0 && colind[k] == row) {
+      jf += c.gshunt;
+      has_diag = true;
+    }
+    if (TRAN) {
+      if (lin_q) {
+        const double cq = lin_q[k];
+        jq += cq;
+        aq += cq * x[colind[k]];
+      }
+      jac[k] = c.qscale * jq + c.fscale * jf;
+    } else {
+      jac[k] = jf;
+    }
+  }
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    af += __shfl_down_sync(0xffffffffu, af, w);
+    aq += __shfl_down_sync(0xffffffffu, aq, w);
+  }
+  has_diag = __any_sync(0xffffffffu, has_diag);
+  if (lane == 0) {
+    // The family's vector sums for the row (the vector gather's order), kept in its buffers.
+    const int2 v = vrow[row];
+    double ff, fq, ffx, fqx;
+    if (v.y < 0) {
+      ff = fam_f[row];
+      fq = fam_q[row];
+      ffx = fam_fx[row];
+      fqx = fam_qx[row];
+    } else {
+      ff = fq = ffx = fqx = 0.0;
+      for (int s = v.x; s < v.x + v.y; ++s) {
+        const size_t src = (size_t)vsrc[s];
+        ff += stage[vb0 + src];
+        fq += stage[vb1 + src];
+        ffx += stage[vb2 + src];
+        fqx += stage[vb3 + src];
+      }
+      if (v.y > 0) {
+        fam_f[row] = ff;
+        fam_q[row] = fq;
+        fam_fx[row] = ffx;
+        fam_qx[row] = fqx;
+      } else {
+        // A row the family does not stamp: its buffers keep their (zero) values, as with the
+        // assigning load.
+        ff = fam_f[row];
+        fq = fam_q[row];
+        ffx = fam_fx[row];
+        fqx = fam_qx[row];
+      }
+    }
+    double F = ff + af;
+    if (has_diag) F += c.gshunt * x[row];
+    if (b) F -= b[row];
+    if (f_tot) f_tot[row] = F;
+    if (!TRAN) {
+      double r = -F;
+      if (limiter) r = r + ffx;
+      rhs[row] = r;
+      return;
+    }
+    const double Q = fq + aq;
+    if (q_tot) q_tot[row] = Q;
+    double r = (Q - qn0[row]) * c.inv_h + c.fscale * F;
+    if (c.hist_scale != 0.0) r = r + c.hist_scale * fhist[row];
+    r = -r;
+    if (limiter) r = r + c.qscale * fqx;
+    if (limiter) r = r + c.fscale * ffx;
+    rhs[row] = r;
+  }
+}
+
+// Per-target (first source, count) of a gather map over n_targets outputs: short targets get
+// their range in the map's source list, long ones count -1, the others (0, 0).
+int map_ranges(const GatherMap &m, int n_targets, std::vector<int2> &out) {
+  out.assign((size_t)n_targets, make_int2(0, 0));
+  std::vector<int> dst(m.n_short), ptr(m.n_short + 1), ldst(m.n_long);
+  if (m.n_short > 0) {
+    XD_CUDA(cudaMemcpy(dst.data(), m.d_short_dst, dst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    XD_CUDA(cudaMemcpy(ptr.data(), m.d_short_ptr, ptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  if (m.n_long > 0) XD_CUDA(cudaMemcpy(ldst.data(), m.d_long_dst, ldst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int t = 0; t < m.n_short; ++t) out[(size_t)dst[t]] = make_int2(ptr[t], ptr[t + 1] - ptr[t]);
+  for (int t = 0; t < m.n_long; ++t) out[(size_t)ldst[t]] = make_int2(0, -1);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xd_tia_fused_create(xd_tia *tia, xd_ctx *fam, xd_tia_fused **out) {
+  if (!tia || !fam || !out) return fail(-1, "null argument");
+  *out = nullptr;
+  int device, n_rows, nnz;
+  const int *rowptr, *colind;
+  int rc = xd_tia_internal_pattern(tia, &device, &n_rows, &nnz, &rowptr, &colind);
+  if (rc) return rc;
+  if (device != fam->device) return fail(-1, "the combine object and the family are on different devices");
+  if (n_rows != fam->n_unknowns || nnz != fam->nnz)
+    return fail(-1, "the combine object's pattern is not the family's pattern");
+  DeviceGuard g(device);
+  std::vector<int2> ent, vrow;
+  if ((rc = map_ranges(fam->mmap, nnz, ent)) != 0) return rc;
+  if ((rc = map_ranges(fam->vmap, n_rows, vrow)) != 0) return rc;
+  xd_tia_fused *f = new xd_tia_fused();
+  f->tia = tia;
+  f->fam = fam;
+  f->device = device;
+  f->n_rows = n_rows;
+  f->nnz = nnz;
+  f->d_rowptr = rowptr;
+  f->d_colind = colind;
+  cudaError_t ce;
+  if ((ce = cudaMalloc(&f->d_ent, std::max<size_t>(1, ent.size()) * sizeof(int2))) != cudaSuccess ||
+      (ce = cudaMemcpy(f->d_ent, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMalloc(&f->d_vrow, std::max<size_t>(1, vrow.size()) * sizeof(int2))) != cudaSuccess ||
+      (ce = cudaMemcpy(f->d_vrow, vrow.data(), vrow.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaFree(f->d_ent);
+    cudaFree(f->d_vrow);
+    delete f;
+    return cuda_fail(ce, "xd_tia_fused_create allocation");
+  }
+  *out = f;
+  return 0;
+}
+
+int xd_tia_fused_destroy(xd_tia_fused *f) {
+  if (!f) return 0;
+  DeviceGuard g(f->device);
+  cudaFree(f->d_ent);
+  cudaFree(f->d_vrow);
+  delete f;
+  return 0;
+}
+
+int xd_tia_load_combine(xd_tia_fused *fu, const xd_flags *flags, const xd_tia_coef *coef, const double *d_x,
+                        double *d_next_sta, double *d_curr_sta, double *d_next_sto, const double *d_curr_sto,
+                        double *d_fam_f, double *d_fam_q, double *d_fam_fx, double *d_fam_qx, double *d_fam_dfdx,
+                        double *d_fam_dqdx, const double *d_lin_dfdx, const double *d_lin_dqdx, int limiter,
+                        const double *d_b, const double *d_qn0, const double *d_fhist, double *d_jac,
+                        double *d_rhs, double *d_q_tot, double *d_f_tot, void *stream) {
+  if (!fu || !flags || !coef) return fail(-1, "null argument");
+  if (fu->n_rows == 0) return 0;
+  if (!d_x || !d_fam_f || !d_fam_q || !d_fam_fx || !d_fam_qx || !d_fam_dfdx || !d_fam_dqdx || !d_jac || !d_rhs)
+    return fail(-1, "null device buffer");
+  if (coef->mode != 0 && (!d_qn0 || (coef->hist_scale != 0.0 && !d_fhist)))
+    return fail(-1, "null device buffer for a time step");
+  xd_ctx *ctx = fu->fam;
+  int rc = xd_update_state(ctx, flags, d_x, d_next_sta, d_curr_sta, d_next_sto, d_curr_sto, stream);
+  if (rc) return rc;
+  DeviceGuard g(fu->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)ctx->n, r = (size_t)ctx->vec_rows;
+  const size_t mb = 4 * r * n, mm = (size_t)ctx->mat_slots * n;
+  if (ctx->n > 0) {
+    // Long entries and rows: the chunked gathers store the family's sums into its buffers.
+    OutSet<4, false> vs{{d_fam_f, d_fam_q, d_fam_fx, d_fam_qx}, {0, r * n, 2 * r * n, 3 * r * n}, 1};
+    if ((rc = run_gather(ctx->vmap, ctx->d_stage, vs, st, false))) return rc;
+    OutSet<2, false> ms{{d_fam_dfdx, d_fam_dqdx}, {mb, mb + mm}, 1};
+    if ((rc = run_gather(ctx->mmap, ctx->d_stage, ms, st, false))) return rc;
+  }
+  const int blocks = (fu->n_rows + kFusedWarps - 1) / kFusedWarps;
+#define XD_FUSED_ARGS                                                                                               \
+  fu->n_rows, fu->d_rowptr, fu->d_colind, *coef, d_x, fu->d_ent, ctx->mmap.d_src, fu->d_vrow, ctx->vmap.d_src,      \
+      ctx->d_stage, mb, mb + mm, (size_t)0, r * n, 2 * r * n, 3 * r * n, d_fam_dfdx, d_fam_dqdx, d_fam_f, d_fam_q,  \
+      d_fam_fx, d_fam_qx, d_lin_dfdx, d_lin_dqdx, limiter, d_b, d_qn0, d_fhist, d_jac, d_rhs, d_q_tot, d_f_tot
+  if (coef->mode != 0)
+    fused_combine_kernel<true><<<blocks, 32 * kFusedWarps, 0, st>>>(XD_FUSED_ARGS);
+  else
+    fused_combine_kernel<false><<<blocks, 32 * kFusedWarps, 0, st>>>(XD_FUSED_ARGS);
+#undef XD_FUSED_ARGS
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fused_combine_kernel launch");
   return 0;
 }
 

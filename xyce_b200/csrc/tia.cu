@@ -503,6 +503,18 @@ int cuda_err(cudaError_t e, const char *where) {
 
 }  // namespace
 
+// The pattern a combine object was created on (for the fused load-and-combine in devload.cu).
+int xd_tia_internal_pattern(const xd_tia *t, int *device, int *n_rows, int *nnz, const int **rowptr,
+                            const int **colind) {
+  if (!t) return xd_internal_fail(-1, "null combine object");
+  *device = t->device;
+  *n_rows = t->n_rows;
+  *nnz = t->nnz;
+  *rowptr = t->d_rowptr;
+  *colind = t->d_colind;
+  return 0;
+}
+
 extern "C" {
 
 int xd_tia_create(const xd_csr *pat, int cuda_device, xd_tia **out) {

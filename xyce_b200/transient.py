@@ -321,13 +321,11 @@ class TransientBase:
         torch = self.torch
         x_ref = self.x.clone()
         w = prm.rel_tol * x_ref.abs() + prm.abs_tol
-        self._load(flags_for_iter(0))
-        self._combine(mode, h, order, qn0, fhist)
+        self._load_and_combine(flags_for_iter(0), mode, h, order, qn0, fhist)
         for it in range(1, prm.max_iter + 1):
             dx = self._solve()
             w, wrms = self._update(dx, x_ref, w, prm)
-            self._load(flags_for_iter(it))
-            self._combine(mode, h, order, qn0, fhist)
+            self._load_and_combine(flags_for_iter(it), mode, h, order, qn0, fhist)
             max_rhs = self._residual_max()
             if not (math.isfinite(max_rhs) and math.isfinite(wrms)):
                 return -1
@@ -346,6 +344,11 @@ class TransientBase:
 
     def _residual_max(self):
         return float(self.rhs.abs().max())
+
+    def _load_and_combine(self, flags, mode, h=None, order=1, qn0=None, fhist=None):
+        """The device loads at self.x, then the combine (one fused pass where the backend has it)."""
+        self._load(flags)
+        self._combine(mode, h, order, qn0, fhist)
 
     def _history_here(self):
         """Q and F at the current point (after a load there) into q_tot / f_tot."""
@@ -512,7 +515,7 @@ class GpuTransient(TransientBase):
     """
 
     def __init__(self, c, family: MosfetDevice, rowptr, colind, device=0, solver="auto", gmin=1e-12,
-                 graphs=True, static_pivot=True):
+                 graphs=True, static_pivot=True, fused=True):
         import torch
 
         if solver == "auto":
@@ -534,6 +537,13 @@ class GpuTransient(TransientBase):
         h = ctypes.c_void_p()
         _native.check(lib.xd_tia_create(ctypes.byref(csr), int(device), ctypes.byref(h)), "xd_tia_create")
         self._tia = h
+        # Fused load and combine (xd_tia_load_combine): the Newton matrix and residual straight from
+        # the evaluation's staged stamps, bit-identical to xd_load_assign + xd_tia_combine.
+        self._fused = None
+        if fused:
+            hf = ctypes.c_void_p()
+            _native.check(lib.xd_tia_fused_create(h, family._h, ctypes.byref(hf)), "xd_tia_fused_create")
+            self._fused = hf
         T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=self.dev).contiguous()
         z = lambda k: torch.zeros(k, dtype=torch.float64, device=self.dev)
         self.lin_f, self.lin_q = T(self.lin.lin_f), T(self.lin.lin_q)
@@ -561,6 +571,9 @@ class GpuTransient(TransientBase):
         if getattr(self, "_slu", None) is not None and self._slu.value:
             self._lib.xd_slu_destroy(self._slu)
             self._slu = None
+        if getattr(self, "_fused", None) is not None and self._fused.value:
+            self._lib.xd_tia_fused_destroy(self._fused)
+            self._fused = None
         if getattr(self, "_tia", None) is not None and self._tia.value:
             self._lib.xd_tia_destroy(self._tia)
             self._tia = None
@@ -714,8 +727,7 @@ class GpuTransient(TransientBase):
             LU, piv, _ = torch.linalg.lu_factor_ex(self._dense.view(self.nu, self.nu))
             dx = torch.linalg.lu_solve(LU, piv, self.rhs.view(-1, 1)).view(-1)
         self._device_update(dx, self._g_xref, self._g_w, prm, self._g_norms)
-        self._load_raw(flags1)
-        self._combine(mode, h, order, qn0, fhist)
+        self._load_combine_raw(flags1, mode, h, order, qn0, fhist)
         self._device_residual_norm(self._g_norms)
         self._g_host.copy_(self._g_norms, non_blocking=True)
         return "small" if self._small else (LU, piv)
@@ -761,8 +773,7 @@ class GpuTransient(TransientBase):
         if f1 != f2:  # the iterations' flags differ beyond newton_iter >= 1: no single graph
             return super()._newton(prm, flags_for_iter, mode, h, order, qn0, fhist)
         torch = self.torch
-        self._load(flags_for_iter(0))
-        self._combine(mode, h, order, qn0, fhist)
+        self._load_and_combine(flags_for_iter(0), mode, h, order, qn0, fhist)
         graph, lu = self._graph_for(prm, f1, mode, h, order, qn0, fhist)  # loads and combine leave x as it was
         self._g_xref.copy_(self.x)
         self._g_w.copy_(prm.rel_tol * self._g_xref.abs() + prm.abs_tol)
@@ -896,6 +907,26 @@ class GpuTransient(TransientBase):
                                                p(self.curr_sta), p(self.next_sto), p(self.curr_sto), p(self.f),
                                                p(self.q), p(self.fx), p(self.qx), p(self.jf), p(self.jq),
                                                self._stream()), "xd_load_assign")
+
+    def _load_and_combine(self, flags, mode, h=None, order=1, qn0=None, fhist=None):
+        self._load_combine_raw(flags, mode, h, order, qn0, fhist)
+        self.stats.loads += 1
+
+    def _load_combine_raw(self, flags, mode, h=None, order=1, qn0=None, fhist=None):
+        if self._fused is None:
+            self._load_raw(flags)
+            self._combine(mode, h, order, qn0, fhist)
+            return
+        c = flags.to_c()
+        coef = tia_coef(mode, h, order, self.gshunt)
+        p = self._ptr
+        _native.check(self._lib.xd_tia_load_combine(self._fused, ctypes.byref(c), ctypes.byref(coef), p(self.x),
+                                                    p(self.next_sta), p(self.curr_sta), p(self.next_sto),
+                                                    p(self.curr_sto), p(self.f), p(self.q), p(self.fx), p(self.qx),
+                                                    p(self.jf), p(self.jq), p(self.lin_f), p(self.lin_q),
+                                                    1 if self.limiting else 0, p(self.b), p(qn0), p(fhist),
+                                                    p(self.jac), p(self.rhs), p(self.qtot), p(self.ftot),
+                                                    self._stream()), "xd_tia_load_combine")
 
     def _surrogate_load(self):
         self.surrogate.load(self.x, self.f, self.q, self.fx, self.qx, self._stream())

@@ -45,6 +45,9 @@
 #include <N_IO_CmdParse.h>
 #include <N_LAS_Matrix.h>
 #include <N_LAS_Vector.h>
+#ifdef XREF_GPU_BINDING
+#include "../xyce_b200/binding/N_DEV_GpuMosfetB4.h"
+#endif
 
 // The command-line parser lives in the reference's IO package, which is not compiled here. The
 // device code only asks it whether debug switches were given; these definitions answer "no".
@@ -191,10 +194,10 @@ extern "C" {
 //   model_nparams[m] number of (name, value) pairs for model m, concatenated in param_names/values
 //   inst_model[i]    model index of instance i; inst_nodes[4*i..] = D, G, S, B node ids (-1 = ground)
 //   inst_param_names / inst_param_values[i*n_inst_params + k]; NaN = not given
-void *xref_create(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
-                  const char **param_names, const double *param_values, int n_inst, const int *inst_model,
-                  const int *inst_nodes, int n_inst_params, const char **inst_param_names,
-                  const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
+static void *create_impl(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
+                         const char **param_names, const double *param_values, int n_inst, const int *inst_model,
+                         const int *inst_nodes, int n_inst_params, const char **inst_param_names,
+                         const double *inst_param_values, int n_nodes, char *errbuf, int errlen, bool gpu_binding) {
   RefCircuit *c = new RefCircuit();
   try {
     c->level = level;
@@ -202,7 +205,15 @@ void *xref_create(int level, int n_models, const int *model_is_pmos, const int *
     const XD::Configuration *cfg = XD::Configuration::findConfiguration(device_letter_for(level), level);
     if (!cfg) throw std::runtime_error("no configuration for level");
     XD::FactoryBlock fb(c->opts, c->ss, c->mld, c->ext, c->cp);
+#ifdef XREF_GPU_BINDING
+    if (gpu_binding) {
+      if (level != 14) throw std::runtime_error("the GPU binding is for BSIM4 (level 14)");
+      // The binding's device master in place of the reference's, from the same configuration.
+      c->dev = new XD::GpuMosfetB4::Master(*cfg, fb, c->ss, c->opts);
+    } else
+#endif
     c->dev = cfg->createDevice(fb);
+    (void)gpu_binding;
     int off = 0;
     for (int m = 0; m < n_models; ++m) {
       char name[64];
@@ -285,6 +296,26 @@ void *xref_create(int level, int n_models, const int *model_is_pmos, const int *
   return c;
 }
 
+void *xref_create(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
+                  const char **param_names, const double *param_values, int n_inst, const int *inst_model,
+                  const int *inst_nodes, int n_inst_params, const char **inst_param_names,
+                  const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
+  return create_impl(level, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst, inst_model,
+                     inst_nodes, n_inst_params, inst_param_names, inst_param_values, n_nodes, errbuf, errlen, false);
+}
+
+#ifdef XREF_GPU_BINDING
+// The same family with the GPU binding (xyce_b200/binding) as its device master: the harness's
+// Device calls then run through libxyce_b200.so on CUDA device 0.
+void *xref_create_gpu_binding(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
+                              const char **param_names, const double *param_values, int n_inst, const int *inst_model,
+                              const int *inst_nodes, int n_inst_params, const char **inst_param_names,
+                              const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
+  return create_impl(level, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst, inst_model,
+                     inst_nodes, n_inst_params, inst_param_names, inst_param_values, n_nodes, errbuf, errlen, true);
+}
+#endif
+
 void xref_destroy(void *h) { delete static_cast<RefCircuit *>(h); }
 
 int xref_num_unknowns(void *h) { return static_cast<RefCircuit *>(h)->n_unknowns; }
@@ -328,9 +359,9 @@ int xref_stamp(void *h, int i, int *rows, int *cols) {
 int xref_set_pattern(void *h, int n_rows, const int *rowptr, const int *colind) {
   RefCircuit *c = static_cast<RefCircuit *>(h);
   if (n_rows != c->n_unknowns + 1) return -1000000;
-  std::vector<int> rp(rowptr, rowptr + n_rows + 1);
-  c->dFdx = N_LAS_Matrix(rp);
-  c->dQdx = N_LAS_Matrix(rp);
+  std::vector<int> rp(rowptr, rowptr + n_rows + 1), ci(colind, colind + rowptr[n_rows]);
+  c->dFdx = N_LAS_Matrix(rp, ci);
+  c->dQdx = N_LAS_Matrix(rp, ci);
   bind_extern(*c);
   for (size_t i = 0; i < c->inst.size(); ++i) {
     XD::DeviceInstance *d = c->inst[i];

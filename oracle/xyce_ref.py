@@ -21,6 +21,9 @@ LIB_PATH = os.path.join(_HERE, "_ref", "libxyce_ref.so")
 LIB_OMP_PATH = os.path.join(_HERE, "_ref", "libxyce_ref_omp.so")
 # Serial build without the libm interposer (oracle/libm_perturb.C): the CPU baseline's timing.
 LIB_PLAIN_PATH = os.path.join(_HERE, "_ref", "libxyce_ref_plain.so")
+# The harness with the product's reference-side binding (xyce_b200/binding) as the BSIM4 device
+# master: the reference's Device calls run through libxyce_b200.so on the GPU.
+LIB_GPU_PATH = os.path.join(_HERE, "_ref", "libxyce_ref_gpu.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -38,25 +41,30 @@ class XrefFlags(ctypes.Structure):
 _LIBS: dict = {}
 
 
-def _path(omp: bool, plain: bool) -> str:
+def _path(omp: bool, plain: bool, gpu: bool = False) -> str:
+    if gpu:
+        return LIB_GPU_PATH
     return LIB_OMP_PATH if omp else (LIB_PLAIN_PATH if plain else LIB_PATH)
 
 
-def available(omp: bool = False, plain: bool = False) -> bool:
-    return os.path.exists(_path(omp, plain))
+def available(omp: bool = False, plain: bool = False, gpu: bool = False) -> bool:
+    return os.path.exists(_path(omp, plain, gpu))
 
 
-def load_library(omp: bool = False, plain: bool = False):
-    path = _path(omp, plain)
+def load_library(omp: bool = False, plain: bool = False, gpu: bool = False):
+    path = _path(omp, plain, gpu)
     if path in _LIBS:
         return _LIBS[path]
     if not os.path.exists(path):
         raise FileNotFoundError(f"oracle library not built: {path} (run make -C oracle)")
     lib = ctypes.CDLL(path)
+    create_args = [ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, _ip, _ip,
+                   ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     lib.xref_create.restype = ctypes.c_void_p
-    lib.xref_create.argtypes = [
-        ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, _ip, _ip,
-        ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    lib.xref_create.argtypes = create_args
+    if hasattr(lib, "xref_create_gpu_binding"):
+        lib.xref_create_gpu_binding.restype = ctypes.c_void_p
+        lib.xref_create_gpu_binding.argtypes = create_args
     lib.xref_destroy.argtypes = [ctypes.c_void_p]
     if hasattr(lib, "xref_set_perturbation"):
         lib.xref_set_perturbation.argtypes = [ctypes.c_int, ctypes.c_ulonglong]
@@ -112,8 +120,9 @@ class RefCircuit:
     inst_params: {NAME: float array [n]} (NaN = not given).
     """
 
-    def __init__(self, level, models, inst_model, inst_nodes, inst_params, n_nodes, omp=False, plain=False):
-        self.lib = load_library(omp, plain)
+    def __init__(self, level, models, inst_model, inst_nodes, inst_params, n_nodes, omp=False, plain=False,
+                 gpu_binding=False):
+        self.lib = load_library(omp, plain, gpu_binding)
         self.level = level
         is_pmos = np.array([1 if m[0] else 0 for m in models], dtype=np.int32)
         nparams = np.array([len(m[1]) for m in models], dtype=np.int32)
@@ -134,7 +143,8 @@ class RefCircuit:
             pvals[:, k] = np.asarray(inst_params[p], dtype=np.float64)
         pvals = np.ascontiguousarray(pvals)
         err = ctypes.create_string_buffer(512)
-        h = self.lib.xref_create(level, len(models), _iptr(is_pmos), _iptr(nparams), self._names, _dptr(vals), n,
+        create = self.lib.xref_create_gpu_binding if gpu_binding else self.lib.xref_create
+        h = create(level, len(models), _iptr(is_pmos), _iptr(nparams), self._names, _dptr(vals), n,
                                  _iptr(inst_model), _iptr(inst_nodes), len(pnames), self._pnames, _dptr(pvals),
                                  int(n_nodes), err, 512)
         if not h:

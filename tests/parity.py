@@ -64,12 +64,14 @@ class OracleRun:
     """The reference's own device objects for the circuit's MOSFETs, on the product's pattern."""
 
     def __init__(self, c: netlist.Circuit, cards, inst_model, inst_nodes, params, rowptr, colind, level=14,
-                 n_sta_slots=None):
+                 n_sta_slots=None, gpu_binding=False):
         self.c = c
         models = [(m.pmos, dict(m.params)) for m in cards]
         nu = c.n_unknowns
         # The reference numbers its internal nodes after the external unknowns, in instance order.
-        self.ref = xr.RefCircuit(level, models, inst_model, inst_nodes, params, nu - c.n_internal)
+        # gpu_binding: the reference's own device loop with the product's binding as the device master.
+        self.ref = xr.RefCircuit(level, models, inst_model, inst_nodes, params, nu - c.n_internal,
+                                 gpu_binding=gpu_binding)
         assert self.ref.n_unknowns == nu, "the oracle's internal nodes differ from the circuit's"
         n = inst_model.shape[0]
         # Oracle pattern: the product's pattern plus the ground row / column entries the stamps hit.

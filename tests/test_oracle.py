@@ -92,3 +92,19 @@ def test_finite_difference_jacobians_both_families(level):
             k = 3 * r + j  # row r of the 2 x (2 + ground) pattern
             assert fd_f[r] == pytest.approx(base.dfdx[k], rel=1e-5, abs=1e-12)
             assert fd_q[r] == pytest.approx(base.dqdx[k], rel=1e-5, abs=1e-22)
+
+
+def test_gpu_binding_library_loads_and_builds_the_reference_topology():
+    """The harness built with the product's BSIM4 binding as its device master loads without a GPU,
+    and creating a family through it registers the reference's own topology (the GPU is touched
+    only by the first load)."""
+    if not xr.available(gpu=True):
+        pytest.skip("binding harness not built (make -C oracle binding)")
+    lib = xr.load_library(gpu=True)
+    assert hasattr(lib, "xref_create_gpu_binding")
+    ref = xr.RefCircuit(14, [(False, {}), (True, {"RSH": 10.0})], np.array([0, 1]),
+                        np.array([[0, 1, -1, -1], [0, 1, 2, 2]]),
+                        {"L": np.array([0.18e-6] * 2), "W": np.array([1e-6] * 2), "NRD": np.array([np.nan, 2.0])}, 3,
+                        gpu_binding=True)
+    assert ref.n_unknowns == 4  # the PMOS instance's internal drain node
+    assert ref.n_state == 6 and ref.n_store == 28

@@ -62,6 +62,22 @@ int xd_tia_combine(xd_tia *t, const xd_tia_coef *coef, const double *d_x, const 
                    const double *d_b, const double *d_qn0, const double *d_fhist, double *d_jac,
                    double *d_rhs, double *d_q_tot, double *d_f_tot, void *stream);
 
+/* Independent voltage sources' values at an analysis time, evaluated on the device: stands in for
+ * the device manager's source update (DeviceMaster::updateSources -> PWLinData::updateSource,
+ * src/DeviceModelPKG/Core/src/N_DEV_SourceData.C:1371-1490) and the value the sources load into
+ * the branch rows (Vsrc::Master::updateState, N_DEV_Vsrc.C:941-960). Source k writes b[row[k]]:
+ * with transient != 0 (a transient step or its operating point) its piecewise-linear value at
+ * time t — n_pairs[k] (t, v) pairs in tv, all sources' pairs concatenated, delay td[k], repeat
+ * from time repeat[k] (negative or a null array: no repeat), computed with the reference's own
+ * arithmetic, so the values are bit-identical to its — and otherwise, or when it has no pairs,
+ * its DC value dc[k]. No other entry of d_b is written. xd_pwl_create copies the table to the
+ * device (set-up only); xd_pwl_eval is one kernel launch. */
+typedef struct xd_pwl xd_pwl;
+int xd_pwl_create(int n_src, const int *row, const int *n_pairs, const double *tv, const double *dc, const double *td,
+                  const double *repeat, int cuda_device, xd_pwl **out);
+int xd_pwl_destroy(xd_pwl *p);
+int xd_pwl_eval(xd_pwl *p, double t, int transient, double *d_b, void *stream);
+
 /* Fused device load and combine (no counterpart in the reference, where the device manager's loads
  * and the integrator's combine are separate passes over memory: N_DEV_DeviceMgr.C:2117-2123,
  * 2452-2461, 2256-2261, then N_TIA_OneStep.C:272-312, 470-497).

@@ -42,6 +42,10 @@
 #include <N_DEV_MOSFET1.h>
 #include <N_DEV_MOSFET_B3.h>
 #include <N_DEV_MOSFET_B4.h>
+#include <N_DEV_Resistor.h>
+#include <N_DEV_Capacitor.h>
+#include <N_DEV_Vsrc.h>
+#include <N_DEV_SourceData.h>
 #include <N_IO_CmdParse.h>
 #include <N_LAS_Matrix.h>
 #include <N_LAS_Vector.h>
@@ -89,9 +93,10 @@ struct RefCircuit {
   XD::Device *dev;
   std::vector<XD::DeviceInstance *> inst;
   int level;
+  int n_ext;  // external nodes per instance: 4 for the MOSFETs, 2 for resistors, capacitors, sources
   int n_nodes, n_unknowns, n_sta, n_sto;
   std::vector<int> int_lid_base, int_count, sta_base, sto_base, n_sta_inst;
-  std::vector<int> inst_lids;  // per instance: 4 external LIDs (ground mapped to n_unknowns)
+  std::vector<int> inst_lids;  // per instance: n_ext external LIDs (ground mapped to n_unknowns)
   N_LAS_Matrix dFdx, dQdx;
   N_LAS_Vector flagSol;
   // Views of the raw solver vectors for devices that index through N_LAS_Vector.
@@ -99,17 +104,18 @@ struct RefCircuit {
   std::vector<double> nextSol, currSol, lastSol, nextSta, currSta, lastSta, nextSto, currSto, lastSto,
       staDeriv, f, q, b, dfdxdvp, dqdxdvp, leadF, leadQ;
   std::string err;
-  RefCircuit() : dev(0), level(0), n_nodes(0), n_unknowns(0), n_sta(0), n_sto(0) {}
+  RefCircuit() : dev(0), level(0), n_ext(4), n_nodes(0), n_unknowns(0), n_sta(0), n_sto(0) {}
   ~RefCircuit() { delete dev; }
 };
 
-const char *device_letter_for(int level) { (void)level; return "m"; }
-
-void register_level(int level) {
-  static bool b1 = false, b3 = false, b4 = false;
-  if (level == 1 && !b1) { XD::MOSFET1::registerDevice(); b1 = true; }
-  if (level == 9 && !b3) { XD::MOSFET_B3::registerDevice(); b3 = true; }
-  if (level == 14 && !b4) { XD::MOSFET_B4::registerDevice(); b4 = true; }
+void register_device(const std::string &letter, int level) {
+  static bool b1 = false, b3 = false, b4 = false, r = false, cp = false, v = false;
+  if (letter == "m" && level == 1 && !b1) { XD::MOSFET1::registerDevice(); b1 = true; }
+  if (letter == "m" && level == 9 && !b3) { XD::MOSFET_B3::registerDevice(); b3 = true; }
+  if (letter == "m" && level == 14 && !b4) { XD::MOSFET_B4::registerDevice(); b4 = true; }
+  if (letter == "r" && !r) { XD::Resistor::registerDevice(); r = true; }
+  if (letter == "c" && !cp) { XD::Capacitor::registerDevice(); cp = true; }
+  if (letter == "v" && !v) { XD::Vsrc::registerDevice(); v = true; }
 }
 
 void bind_extern(RefCircuit &c) {
@@ -178,6 +184,7 @@ void do_load(RefCircuit &c) {
   std::fill(c.dqdxdvp.begin(), c.dqdxdvp.end(), 0.0);
   c.dFdx.put(0.0);
   c.dQdx.put(0.0);
+  c.dev->updateSources();  // the device manager refreshes the sources at the current time first
   c.dev->updateState(c.nextSol.data(), c.nextSta.data(), c.nextSto.data());
   c.dev->updateSecondaryState(c.staDeriv.data(), c.nextSto.data());
   c.dev->loadDAEVectors(c.nextSol.data(), c.f.data(), c.q.data(), c.b.data(), c.leadF.data(), c.leadQ.data());
@@ -194,15 +201,17 @@ extern "C" {
 //   model_nparams[m] number of (name, value) pairs for model m, concatenated in param_names/values
 //   inst_model[i]    model index of instance i; inst_nodes[4*i..] = D, G, S, B node ids (-1 = ground)
 //   inst_param_names / inst_param_values[i*n_inst_params + k]; NaN = not given
-static void *create_impl(int level, int n_models, const int *model_is_pmos, const int *model_nparams,
-                         const char **param_names, const double *param_values, int n_inst, const int *inst_model,
-                         const int *inst_nodes, int n_inst_params, const char **inst_param_names,
-                         const double *inst_param_values, int n_nodes, char *errbuf, int errlen, bool gpu_binding) {
+static void *create_impl(const char *letter, int level, int n_ext, int n_models, const int *model_is_pmos,
+                         const int *model_nparams, const char **param_names, const double *param_values, int n_inst,
+                         const int *inst_model, const int *inst_nodes, int n_inst_params,
+                         const char **inst_param_names, const double *inst_param_values, const int *pwl_count,
+                         const double *pwl_tv, int n_nodes, char *errbuf, int errlen, bool gpu_binding) {
   RefCircuit *c = new RefCircuit();
   try {
     c->level = level;
-    register_level(level);
-    const XD::Configuration *cfg = XD::Configuration::findConfiguration(device_letter_for(level), level);
+    c->n_ext = n_ext;
+    register_device(letter, level);
+    const XD::Configuration *cfg = XD::Configuration::findConfiguration(letter, level);
     if (!cfg) throw std::runtime_error("no configuration for level");
     XD::FactoryBlock fb(c->opts, c->ss, c->mld, c->ext, c->cp);
 #ifdef XREF_GPU_BINDING
@@ -230,12 +239,28 @@ static void *create_impl(int level, int n_models, const int *model_is_pmos, cons
       snprintf(name, sizeof(name), "m%d", i);
       snprintf(mname, sizeof(mname), "xmod%d", inst_model[i]);
       XD::InstanceBlock ib(name);
-      ib.setModelName(Xyce::Device::ModelName(mname));
+      if (n_models > 0) ib.setModelName(Xyce::Device::ModelName(mname));
       for (int k = 0; k < n_inst_params; ++k) {
         double v = inst_param_values[(size_t)i * n_inst_params + k];
         if (!std::isnan(v)) ib.params.push_back(XD::Param(inst_param_names[k], v, true));
       }
-      ib.numExtVars = 4;
+      if (std::string(letter) == "v") {
+        // The netlist parser marks every source specification as carrying a DC value
+        // (Vsrc::Instance, N_DEV_Vsrc.C:336-339).
+        ib.params.push_back(XD::Param("DCSOURCETYPE", (int)_DC_DATA, true));
+      }
+      if (pwl_count && pwl_count[i] > 0) {
+        // A piecewise-linear source: the type, the number of pairs, then T / V pairs in order, as
+        // the netlist parser hands them to the source (PWLinData, N_DEV_SourceData.C:1278-1312).
+        ib.params.push_back(XD::Param("TRANSIENTSOURCETYPE", (int)_PWL_DATA, true));
+        ib.params.push_back(XD::Param("NUM", pwl_count[i], true));
+        for (int k = 0; k < pwl_count[i]; ++k) {
+          ib.params.push_back(XD::Param("T", pwl_tv[2 * k], true));
+          ib.params.push_back(XD::Param("V", pwl_tv[2 * k + 1], true));
+        }
+        pwl_tv += 2 * pwl_count[i];
+      }
+      ib.numExtVars = n_ext;
       c->inst[i] = c->dev->addInstance(ib, fb);
       if (!c->inst[i]) throw std::runtime_error("addInstance failed");
     }
@@ -250,7 +275,7 @@ static void *create_impl(int level, int n_models, const int *model_is_pmos, cons
     }
     c->n_unknowns = next;
     const int gnd = next;
-    c->inst_lids.resize(4 * (size_t)n_inst);
+    c->inst_lids.resize((size_t)n_ext * n_inst);
     int sta = 0, sto = 0;
     c->sta_base.resize(n_inst);
     c->sto_base.resize(n_inst);
@@ -259,9 +284,9 @@ static void *create_impl(int level, int n_models, const int *model_is_pmos, cons
       XD::DeviceInstance *d = c->inst[i];
       std::vector<int> ext(d->getNumExtVars()), in(d->getNumIntVars());
       for (int k = 0; k < (int)ext.size(); ++k) {
-        int node = inst_nodes[4 * (size_t)i + k];
+        int node = inst_nodes[(size_t)n_ext * i + k];
         ext[k] = node < 0 ? gnd : node;
-        c->inst_lids[4 * (size_t)i + k] = ext[k];
+        c->inst_lids[(size_t)n_ext * i + k] = ext[k];
       }
       for (int k = 0; k < (int)in.size(); ++k) in[k] = c->int_lid_base[i] + k;
       d->registerLIDs(in, ext);
@@ -300,9 +325,26 @@ void *xref_create(int level, int n_models, const int *model_is_pmos, const int *
                   const char **param_names, const double *param_values, int n_inst, const int *inst_model,
                   const int *inst_nodes, int n_inst_params, const char **inst_param_names,
                   const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
-  return create_impl(level, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst, inst_model,
-                     inst_nodes, n_inst_params, inst_param_names, inst_param_values, n_nodes, errbuf, errlen, false);
+  return create_impl("m", level, 4, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst,
+                     inst_model, inst_nodes, n_inst_params, inst_param_names, inst_param_values, 0, 0, n_nodes, errbuf,
+                     errlen, false);
 }
+
+// Two-terminal linear devices with the reference's own code: letter "r" (resistors, instance
+// parameter R), "c" (capacitors, C) or "v" (independent voltage sources: DCV0, and with
+// pwl_count[i] > 0 a piecewise-linear transient value from pwl_tv's (t, v) pairs, the instances'
+// pairs concatenated). inst_nodes holds 2 nodes per instance (-1 = ground); a source's branch
+// current is its internal unknown, numbered after the n_nodes nodes in instance order.
+void *xref_create_linear(const char *letter, int n_inst, const int *inst_nodes, int n_inst_params,
+                         const char **inst_param_names, const double *inst_param_values, const int *pwl_count,
+                         const double *pwl_tv, int n_nodes, char *errbuf, int errlen) {
+  std::vector<int> inst_model(std::max(1, n_inst), 0);
+  return create_impl(letter, 1, 2, 0, 0, 0, 0, 0, n_inst, inst_model.data(), inst_nodes, n_inst_params,
+                     inst_param_names, inst_param_values, pwl_count, pwl_tv, n_nodes, errbuf, errlen, false);
+}
+
+// The analysis time the sources read (SolverState::currTime).
+void xref_set_time(void *h, double t) { static_cast<RefCircuit *>(h)->ss.currTime = t; }
 
 #ifdef XREF_GPU_BINDING
 // The same family with the GPU binding (xyce_b200/binding) as its device master: the harness's
@@ -311,8 +353,9 @@ void *xref_create_gpu_binding(int level, int n_models, const int *model_is_pmos,
                               const char **param_names, const double *param_values, int n_inst, const int *inst_model,
                               const int *inst_nodes, int n_inst_params, const char **inst_param_names,
                               const double *inst_param_values, int n_nodes, char *errbuf, int errlen) {
-  return create_impl(level, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst, inst_model,
-                     inst_nodes, n_inst_params, inst_param_names, inst_param_values, n_nodes, errbuf, errlen, true);
+  return create_impl("m", level, 4, n_models, model_is_pmos, model_nparams, param_names, param_values, n_inst,
+                     inst_model, inst_nodes, n_inst_params, inst_param_names, inst_param_values, 0, 0, n_nodes, errbuf,
+                     errlen, true);
 }
 #endif
 
@@ -342,7 +385,7 @@ int xref_stamp(void *h, int i, int *rows, int *cols) {
   XD::DeviceInstance *d = c->inst[i];
   const std::vector<std::vector<int> > &js = d->jacobianStamp();
   std::vector<int> lids;
-  for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[4 * (size_t)i + k]);
+  for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[(size_t)c->n_ext * i + k]);
   for (int k = 0; k < d->getNumIntVars(); ++k) lids.push_back(c->int_lid_base[i] + k);
   int n = 0;
   for (size_t r = 0; r < js.size(); ++r)
@@ -367,7 +410,7 @@ int xref_set_pattern(void *h, int n_rows, const int *rowptr, const int *colind) 
     XD::DeviceInstance *d = c->inst[i];
     const std::vector<std::vector<int> > &js = d->jacobianStamp();
     std::vector<int> lids;
-    for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[4 * i + k]);
+    for (int k = 0; k < d->getNumExtVars(); ++k) lids.push_back(c->inst_lids[(size_t)c->n_ext * i + k]);
     for (int k = 0; k < d->getNumIntVars(); ++k) lids.push_back(c->int_lid_base[i] + k);
     std::vector<std::vector<int> > jl(js.size());
     for (size_t r = 0; r < js.size(); ++r) {

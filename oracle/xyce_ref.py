@@ -66,6 +66,13 @@ def load_library(omp: bool = False, plain: bool = False, gpu: bool = False):
         lib.xref_create_gpu_binding.restype = ctypes.c_void_p
         lib.xref_create_gpu_binding.argtypes = create_args
     lib.xref_destroy.argtypes = [ctypes.c_void_p]
+    if hasattr(lib, "xref_create_linear"):
+        lib.xref_create_linear.restype = ctypes.c_void_p
+        lib.xref_create_linear.argtypes = [ctypes.c_char_p, ctypes.c_int, _ip, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_char_p), _dp, _ip, _dp, ctypes.c_int,
+                                           ctypes.c_char_p, ctypes.c_int]
+        lib.xref_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.xref_set_time.restype = None
     if hasattr(lib, "xref_set_perturbation"):
         lib.xref_set_perturbation.argtypes = [ctypes.c_int, ctypes.c_ulonglong]
         lib.xref_set_perturbation.restype = None
@@ -227,6 +234,50 @@ class RefCircuit:
 
     def time_loads(self, repetitions: int) -> float:
         return float(self.lib.xref_time_loads(self.h, int(repetitions)))
+
+
+class RefLinear(RefCircuit):
+    """The reference's resistors ("r", instance parameter R), capacitors ("c", C) or independent
+    voltage sources ("v", DCV0; pwl[i] = (times, values) for a piecewise-linear transient value) over
+    2-node instances (inst_nodes [n, 2], -1 = ground). A source's branch current is its internal
+    unknown, numbered after the n_nodes nodes in instance order."""
+
+    def __init__(self, letter, inst_nodes, inst_params, n_nodes, pwl=None):
+        self.lib = load_library()
+        self.level = 1
+        inst_nodes = np.ascontiguousarray(inst_nodes, dtype=np.int32).reshape(-1)
+        n = inst_nodes.shape[0] // 2
+        pnames = list(inst_params.keys())
+        self._pnames = (ctypes.c_char_p * max(1, len(pnames)))(*[p.encode() for p in pnames])
+        pvals = np.full((n, max(1, len(pnames))), math.nan)
+        for k, p in enumerate(pnames):
+            pvals[:, k] = np.asarray(inst_params[p], dtype=np.float64)
+        pvals = np.ascontiguousarray(pvals)
+        counts = np.zeros(max(1, n), dtype=np.int32)
+        tv = [0.0]
+        if pwl is not None:
+            tv = []
+            for i, p in enumerate(pwl):
+                if p is not None:
+                    counts[i] = len(p[0])
+                    for t, v in zip(p[0], p[1]):
+                        tv += [float(t), float(v)]
+        tv = np.ascontiguousarray(tv if tv else [0.0], dtype=np.float64)
+        err = ctypes.create_string_buffer(512)
+        h = self.lib.xref_create_linear(letter.encode(), n, _iptr(inst_nodes), len(pnames), self._pnames, _dptr(pvals),
+                                        _iptr(counts), _dptr(tv), int(n_nodes), err, 512)
+        if not h:
+            raise RuntimeError(f"oracle create failed: {err.value.decode()}")
+        self.h = ctypes.c_void_p(h)
+        self.n = n
+        self.n_nodes = int(n_nodes)
+        self.n_unknowns = self.lib.xref_num_unknowns(self.h)
+        self.n_state = self.lib.xref_num_state(self.h)
+        self.n_store = self.lib.xref_num_store(self.h)
+        self.nnz = None
+
+    def set_time(self, t: float):
+        self.lib.xref_set_time(self.h, float(t))
 
 
 def make_flags(**kw) -> XrefFlags:

@@ -104,6 +104,10 @@ SIGNATURES = {
     "xd_tia_create": (ctypes.c_int, [ctypes.POINTER(XdCsr), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "xd_tia_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_tia_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdTiaCoef)] + [ctypes.c_void_p] * 17),
+    "xd_pwl_create": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, _dp, _dp, _dp, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "xd_pwl_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "xd_pwl_eval": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "xd_tia_fused_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "xd_tia_fused_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_tia_load_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags), ctypes.POINTER(XdTiaCoef)] +

@@ -503,6 +503,98 @@ int cuda_err(cudaError_t e, const char *where) {
 
 }  // namespace
 
+// Independent voltage sources' values at an analysis time, on the device (PWLinData::updateSource,
+// src/DeviceModelPKG/Core/src/N_DEV_SourceData.C:1371-1490, restated with its own arithmetic, so the
+// values equal the reference's bit for bit; Vsrc::Master::updateState picks the transient value in a
+// transient or its operating point and the DC value otherwise, N_DEV_Vsrc.C:941-960).
+struct xd_pwl {
+  int device = 0, n = 0;
+  int *d_row = nullptr;     // b-vector row of each source
+  int *d_first = nullptr;   // [n + 1] first (t, v) pair of each source; no pairs = DC only
+  double *d_tv = nullptr;   // concatenated (t, v) pairs
+  double *d_par = nullptr;  // per source: DC value, delay TD, repeat time (negative: no repeat)
+};
+
+namespace {
+
+__global__ void pwl_eval_kernel(int n, const int *__restrict__ row, const int *__restrict__ first,
+                                const double *__restrict__ tv, const double *__restrict__ par, double t, int transient,
+                                double *__restrict__ b) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int f = first[k], num = first[k + 1] - f;
+  const double *T = tv + 2 * (size_t)f;  // T[2 i] = time i, T[2 i + 1] = value i
+  const double dc = par[3 * k], td = par[3 * k + 1], rep = par[3 * k + 2];
+  if (!transient || num == 0) {
+    b[row[k]] = dc;
+    return;
+  }
+  double time = t, time1, time2, v1, v2, value;
+  if (time >= td) {
+    time -= td;
+    const double tlast = T[2 * (num - 1)];
+    if (time <= tlast) {
+      int loc = num - 1;  // time == the last time: the segment that ends there
+      for (int i = 0; i < num; ++i)
+        if (time < T[2 * i]) {
+          loc = i;
+          break;
+        }
+      if (loc == 0) {
+        time1 = 0.0;
+        v1 = 0.0;
+      } else {
+        time1 = T[2 * (loc - 1)];
+        v1 = T[2 * (loc - 1) + 1];
+      }
+      time2 = T[2 * loc];
+      v2 = T[2 * loc + 1];
+    } else if (rep < 0.0) {
+      time1 = 0.0;
+      time2 = 1.0;
+      v1 = v2 = T[2 * (num - 1) + 1];
+    } else {
+      const double looptime = tlast - rep;
+      time -= tlast;
+      time -= looptime * floor(time / looptime);
+      time += rep;
+      int loc = num - 1;
+      for (int i = 0; i < num; ++i)
+        if (time < T[2 * i]) {
+          loc = i;
+          break;
+        }
+      if (time == rep) {
+        time1 = 0.0;
+        time2 = 1.0;
+        v1 = v2 = T[2 * (num - 1) + 1];
+      } else {
+        if (loc == 0) {
+          time1 = rep;
+          v1 = T[2 * (num - 1) + 1];
+        } else {
+          time1 = T[2 * (loc - 1)];
+          v1 = T[2 * (loc - 1) + 1];
+        }
+        time2 = T[2 * loc];
+        v2 = T[2 * loc + 1];
+      }
+    }
+    if (time1 == time2) {
+      value = v2;
+    } else {
+      const double length = time2 - time1;
+      value = (time2 - time) * v1 / length;
+      value += (-time1 + time) * v2 / length;
+    }
+  } else {
+    value = 0.0;
+  }
+  b[row[k]] = value;
+}
+
+}  // namespace
+
 // The pattern a combine object was created on (for the fused load-and-combine in devload.cu).
 int xd_tia_internal_pattern(const xd_tia *t, int *device, int *n_rows, int *nnz, const int **rowptr,
                             const int **colind) {
@@ -565,6 +657,68 @@ int xd_tia_destroy(xd_tia *t) {
   cudaFree(t->d_rowptr);
   cudaFree(t->d_colind);
   delete t;
+  return 0;
+}
+
+int xd_pwl_create(int n_src, const int *row, const int *n_pairs, const double *tv, const double *dc, const double *td,
+                  const double *repeat, int cuda_device, xd_pwl **out) {
+  if (!out || n_src < 0 || (n_src > 0 && (!row || !n_pairs || !dc))) return xd_internal_fail(-1, "null argument");
+  *out = nullptr;
+  std::vector<int> first(n_src + 1, 0);
+  std::vector<double> par(3 * (size_t)std::max(1, n_src), 0.0);
+  for (int k = 0; k < n_src; ++k) {
+    if (n_pairs[k] < 0) return xd_internal_fail(-1, "negative PWL pair count");
+    first[k + 1] = first[k] + n_pairs[k];
+    par[3 * k] = dc[k];
+    par[3 * k + 1] = td ? td[k] : 0.0;
+    par[3 * k + 2] = repeat ? repeat[k] : -1.0;
+  }
+  const size_t npairs = (size_t)first[n_src];
+  if (npairs > 0 && !tv) return xd_internal_fail(-1, "null PWL pairs");
+  for (int k = 0; k < n_src; ++k) {
+    // The reference's checks (PWLinData, N_DEV_SourceData.C:1314-1317).
+    if (n_pairs[k] > 0 && par[3 * k + 2] >= 0.0 && par[3 * k + 2] >= tv[2 * (size_t)(first[k + 1] - 1)])
+      return xd_internal_fail(-1, "PWL source's repeat value (R) must be >= 0 and < last value in Time-Voltage list");
+  }
+  cudaError_t ce = cudaSetDevice(cuda_device);
+  if (ce != cudaSuccess) return cuda_err(ce, "cudaSetDevice");
+  xd_pwl *p = new xd_pwl();
+  p->device = cuda_device;
+  p->n = n_src;
+  if ((ce = cudaMalloc(&p->d_row, std::max(1, n_src) * sizeof(int))) != cudaSuccess ||
+      (ce = cudaMalloc(&p->d_first, (n_src + 1) * sizeof(int))) != cudaSuccess ||
+      (ce = cudaMalloc(&p->d_tv, std::max<size_t>(1, 2 * npairs) * sizeof(double))) != cudaSuccess ||
+      (ce = cudaMalloc(&p->d_par, par.size() * sizeof(double))) != cudaSuccess ||
+      (n_src > 0 && (ce = cudaMemcpy(p->d_row, row, n_src * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) ||
+      (ce = cudaMemcpy(p->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (npairs > 0 && (ce = cudaMemcpy(p->d_tv, tv, 2 * npairs * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) ||
+      (ce = cudaMemcpy(p->d_par, par.data(), par.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    xd_pwl_destroy(p);
+    return cuda_err(ce, "xd_pwl_create");
+  }
+  *out = p;
+  return 0;
+}
+
+int xd_pwl_destroy(xd_pwl *p) {
+  if (!p) return 0;
+  Guard g(p->device);
+  cudaFree(p->d_row);
+  cudaFree(p->d_first);
+  cudaFree(p->d_tv);
+  cudaFree(p->d_par);
+  delete p;
+  return 0;
+}
+
+int xd_pwl_eval(xd_pwl *p, double t, int transient, double *d_b, void *stream) {
+  if (!p || !d_b) return xd_internal_fail(-1, "null argument");
+  if (p->n == 0) return 0;
+  Guard g(p->device);
+  pwl_eval_kernel<<<(p->n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(p->n, p->d_row, p->d_first, p->d_tv, p->d_par,
+                                                                       t, transient, d_b);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "pwl_eval_kernel launch");
   return 0;
 }
 

@@ -61,11 +61,16 @@ class NewtonParams:
 
 
 def pwl_value(times, values, t: float) -> float:
-    """PWLinData::updateSource without delay or repeat: linear between points, zero-valued start at
-    t = 0 when the first point is later, the last value after the last point."""
+    """PWLinData::updateSource without delay or repeat (N_DEV_SourceData.C:1371-1490), with its own
+    arithmetic: linear between points, zero-valued start at t = 0 when the first point is later,
+    the last value after the last point (formed as the reference forms it, from the segment
+    (0, v_last) - (1, v_last))."""
     n = len(times)
     if t > times[n - 1]:
-        return float(values[n - 1])
+        v = float(values[n - 1])
+        value = (1.0 - t) * v / 1.0
+        value += (-0.0 + t) * v / 1.0
+        return value
     loc = n - 1
     for i in range(n):
         if t < times[i]:
@@ -537,6 +542,19 @@ class GpuTransient(TransientBase):
         h = ctypes.c_void_p()
         _native.check(lib.xd_tia_create(ctypes.byref(csr), int(device), ctypes.byref(h)), "xd_tia_create")
         self._tia = h
+        # Source values at each time point on the device (xd_pwl_eval): the branch rows of b.
+        nv = c.n_vsrc
+        counts = np.array([0 if p is None else len(p[0]) for p in c.vsrc_pwl] + [0] * (nv - len(c.vsrc_pwl)),
+                          dtype=np.int32)[:nv]
+        tv = np.array([x for p in c.vsrc_pwl if p is not None for pair in zip(p[0], p[1]) for x in pair] or [0.0],
+                      dtype=np.float64)
+        rows = np.ascontiguousarray(self.lin.branch, dtype=np.int32)
+        dc = np.ascontiguousarray(c.vsrc_dc, dtype=np.float64)
+        hp = ctypes.c_void_p()
+        _native.check(lib.xd_pwl_create(nv, rows.ctypes.data_as(_native._ip), counts.ctypes.data_as(_native._ip),
+                                        tv.ctypes.data_as(_native._dp), dc.ctypes.data_as(_native._dp), None, None,
+                                        int(device), ctypes.byref(hp)), "xd_pwl_create")
+        self._pwl = hp
         # Fused load and combine (xd_tia_load_combine): the Newton matrix and residual straight from
         # the evaluation's staged stamps, bit-identical to xd_load_assign + xd_tia_combine.
         self._fused = None
@@ -571,6 +589,9 @@ class GpuTransient(TransientBase):
         if getattr(self, "_slu", None) is not None and self._slu.value:
             self._lib.xd_slu_destroy(self._slu)
             self._slu = None
+        if getattr(self, "_pwl", None) is not None and self._pwl.value:
+            self._lib.xd_pwl_destroy(self._pwl)
+            self._pwl = None
         if getattr(self, "_fused", None) is not None and self._fused.value:
             self._lib.xd_tia_fused_destroy(self._fused)
             self._fused = None
@@ -907,6 +928,10 @@ class GpuTransient(TransientBase):
                                                p(self.curr_sta), p(self.next_sto), p(self.curr_sto), p(self.f),
                                                p(self.q), p(self.fx), p(self.qx), p(self.jf), p(self.jq),
                                                self._stream()), "xd_load_assign")
+
+    def _set_sources(self, t):
+        _native.check(self._lib.xd_pwl_eval(self._pwl, 0.0 if t is None else float(t), 0 if t is None else 1,
+                                            self._ptr(self.b), self._stream()), "xd_pwl_eval")
 
     def _load_and_combine(self, flags, mode, h=None, order=1, qn0=None, fhist=None):
         self._load_combine_raw(flags, mode, h, order, qn0, fhist)

@@ -186,12 +186,13 @@ def batched_section(args, dev_id):
             "eval_launch_shape": shape}
 
 
-def placed_transient(args):
-    """The 100k-MOSFET gate netlist (placed wiring: a pin takes one of the 64 most recently opened
-    fan-out slots) through a transient on the GPU: device loads, combine and the cuSOLVER
-    refactorization of every Newton matrix on the device, one host factorization at the start.
-    Operating point from the logic-level starting iterate, then 0 - placed_ns at 10 ps steps with
-    the reference's transient Newton tolerances."""
+def placed_transient(args, n_mos=None, ns=None):
+    """A gate netlist with placed wiring (a pin takes one of the 64 most recently opened fan-out
+    slots; 100k MOSFETs and placed_ns by default, or n_mos MOSFETs for ns) through a transient on
+    the GPU: fused device loads and combine, and the refactorization of every Newton matrix on the
+    device, one host factorization at the start. Operating point from the logic-level starting
+    iterate, then 0 - ns at 10 ps steps with the reference's transient Newton tolerances; the
+    device state stays resident across the run."""
     import ctypes
 
     import torch
@@ -199,7 +200,9 @@ def placed_transient(args):
     from xyce_b200 import MosfetDevice, SolverFlags, netlist
     from xyce_b200.transient import GpuTransient, NewtonParams
 
-    c = netlist.random_logic(args.placed_mos, seed=args.seed, n_inputs=64, locality=64)
+    n_mos = args.placed_mos if n_mos is None else n_mos
+    ns = args.placed_ns if ns is None else ns
+    c = netlist.random_logic(n_mos, seed=args.seed, n_inputs=64, locality=64)
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, im, nd, params = netlist.mosfet_family(c, None)
     fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
@@ -212,7 +215,7 @@ def placed_transient(args):
     st = g.stats
     f0, h0, l0 = st.factorizations, st.host_factorizations, st.loads
     t0 = time.perf_counter()
-    _, w = g.run(args.placed_ns * 1e-9, 10e-12, params=NewtonParams.transient(),
+    _, w = g.run(ns * 1e-9, 10e-12, params=NewtonParams.transient(),
                  record=np.arange(0, c.n_nodes, 997))
     torch.cuda.synchronize()
     run_s = time.perf_counter() - t0
@@ -251,7 +254,7 @@ def placed_transient(args):
     res = {"workload": f"seeded INV/NAND2/NOR2 netlist with placed wiring (fan-out U{{1..4}}, a pin takes one of "
                        f"the 64 most recent open slots), {c.n_mos} BSIM4 MOSFETs, {c.res_nodes.shape[0]} R + "
                        f"{c.cap_nodes.shape[0]} C wire parasitics, 64 PWL inputs, {c.n_unknowns} unknowns, "
-                       f"{g.nnz} nnz; operating point, then 0-{args.placed_ns:g} ns at 10 ps steps, reference "
+                       f"{g.nnz} nnz; operating point, then 0-{ns:g} ns at 10 ps steps, reference "
                        f"transient Newton tolerances",
            "operating_point_s": dc_s, "operating_point_newton_iters": int(dc_its),
            "gpu_s_per_run": run_s, "steps": len(st.newton_iters), "failed_steps": st.failed_steps,
@@ -280,6 +283,8 @@ def transient_section(args):
     out = {}
     if args.placed_only:
         out["placed_netlist"] = placed_transient(args)
+        if args.scale_mos > 0:
+            out["scale_1m"] = placed_transient(args, args.scale_mos, args.scale_ns)
         return out
     # BSIM3 ring oscillator: operating point, 0.1 V kick on node 1, 0-20 ns at 10 ps steps.
     c = netlist.inverter_ring(101, vdd=1.8)
@@ -342,6 +347,10 @@ def transient_section(args):
         fam.close()
     if args.placed_mos > 0:
         out["placed_netlist"] = placed_transient(args)
+    if args.scale_mos > 0:
+        # The scale configuration's transient: ~1M BSIM4 MOSFETs with placed wiring and ~3M R/C,
+        # 2 ns, device-resident state.
+        out["scale_1m"] = placed_transient(args, args.scale_mos, args.scale_ns)
     out["warm_start_bsim4_gates"] = {
         "workload": f"seeded INV/NAND2/NOR2 netlist, {c.n_mos} BSIM4 MOSFETs, RC wires, 16 PWL inputs, "
                     f"{c.n_unknowns} unknowns, 0-1 ns at 10 ps, linear predictor on both paths",
@@ -369,6 +378,9 @@ def parse():
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     ap.add_argument("--placed-mos", type=int, default=100_000, help="MOSFETs of the placed-netlist transient (0: skip)")
     ap.add_argument("--placed-ns", type=float, default=1.0, help="length of the placed-netlist transient (ns)")
+    ap.add_argument("--scale-mos", type=int, default=0,
+                    help="MOSFETs of the scale transient (placed wiring; 0: skip; 1000000 for the scale configuration)")
+    ap.add_argument("--scale-ns", type=float, default=2.0, help="length of the scale transient (ns)")
     ap.add_argument("--placed-only", action="store_true",
                     help="transient section: only the placed-netlist transient (for profiling its solve)")
     return ap.parse_args()

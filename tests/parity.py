@@ -82,10 +82,19 @@ class OracleRun:
         cc = np.tile(nd, (1, 4)).reshape(-1)
         pairs.append(np.stack([rr, cc], 1))
         if c.n_internal:
-            # With internal nodes the reference's stamps reach beyond the terminal block: add them.
+            # With internal nodes the reference's stamps reach beyond the terminal block: add them,
+            # and check that the product's pattern holds every one of them that is not on ground
+            # (an entry the pattern lacked would drop out of the comparison unnoticed).
+            ref_pairs = []
             for i in range(n):
                 sr, sc = self.ref.stamp(i)
-                pairs.append(np.stack([np.asarray(sr, np.int64), np.asarray(sc, np.int64)], 1))
+                ref_pairs.append(np.stack([np.asarray(sr, np.int64), np.asarray(sc, np.int64)], 1))
+            pairs += ref_pairs
+            rp = np.concatenate(ref_pairs, 0)
+            rp = rp[(rp[:, 0] < g) & (rp[:, 1] < g)]
+            prow_ = np.repeat(np.arange(nu), np.diff(rowptr)).astype(np.int64)
+            have = np.isin(rp[:, 0] * (nu + 1) + rp[:, 1], prow_ * (nu + 1) + colind)
+            assert have.all(), f"the product's pattern lacks {int((~have).sum())} entries the reference stamps"
         pr = np.concatenate(pairs, 0)
         key = np.unique(pr[:, 0] * (nu + 1) + pr[:, 1])
         rows, cols = key // (nu + 1), (key % (nu + 1)).astype(np.int32)
@@ -104,6 +113,18 @@ class OracleRun:
         # reserves 12 and writes the first 5 without NQS); the product keeps only the written ones.
         self.n_sta_slots = self.ref.n_state // max(1, n) if n_sta_slots is None else n_sta_slots
         self.n_sto_slots = self.ref.n_store // max(1, n)
+        # sta_off[s, i]: the oracle's state entry of product slot s of instance i (-1: none).
+        self.sta_off = self.sta_base[None, :] + np.arange(self.n_sta_slots)[:, None]
+        if c.mos_internal is not None and c.mos_internal.shape[1] == 10:
+            # General topology: the product keeps (qb, qg, qd, qgmid, qbs, qbd); an instance
+            # registers qgmid only with rgateMod 3 and qbs / qbd only with rbodyMod
+            # (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5225).
+            rg3 = (c.mos_internal[:, 3] >= 0).astype(np.int64)
+            rb = c.mos_internal[:, 4] >= 0
+            self.n_sta_slots = 6
+            b = self.sta_base
+            self.sta_off = np.stack([b, b + 1, b + 2, np.where(rg3 == 1, b + 3, -1), np.where(rb, b + 3 + rg3, -1),
+                                     np.where(rb, b + 4 + rg3, -1)])
 
     def to_aos_sto(self, soa):
         """Product slot-major store block -> oracle per-instance layout."""
@@ -115,14 +136,16 @@ class OracleRun:
     def to_aos_sta(self, soa):
         out = np.zeros(max(1, self.ref.n_state))
         for s in range(self.n_sta_slots):
-            out[self.sta_base + s] = soa[s * self.n:(s + 1) * self.n]
+            has = self.sta_off[s] >= 0
+            out[self.sta_off[s][has]] = soa[s * self.n:(s + 1) * self.n][has]
         return out
 
     def from_aos_sto(self, aos):
         return np.concatenate([aos[self.sto_base + s] for s in range(self.n_sto_slots)])
 
     def from_aos_sta(self, aos):
-        return np.concatenate([aos[self.sta_base + s] for s in range(self.n_sta_slots)])
+        return np.concatenate([np.where(self.sta_off[s] >= 0, aos[np.maximum(self.sta_off[s], 0)], 0.0)
+                               for s in range(self.n_sta_slots)])
 
     def load(self, flags: SolverFlags, sol, next_sta_soa, curr_sta_soa, next_sto_soa, curr_sto_soa,
              perturb_seed=None):

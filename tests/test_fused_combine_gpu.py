@@ -44,7 +44,11 @@ def test_fused_load_combine_bitwise(mode, order, gshunt, limiter):
     T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), **f64)
     rng = np.random.default_rng(3)
     x = T(rng.uniform(-0.2, 1.4, nu))
-    lin_f, lin_q, b = T(lin.lin_f), T(lin.lin_q), T(lin.source_values(0.3e-9))
+    # b is per unknown: the sources' values on their branch rows, zero elsewhere.
+    bvec = np.zeros(nu)
+    bvec[lin.branch] = lin.source_values(0.3e-9)
+    lin_f, lin_q, b = T(lin.lin_f), T(lin.lin_q), T(bvec)
+    assert b.shape[0] == nu and lin_f.shape[0] == nnz
     qn0, fhist = T(rng.normal(0, 1e-15, nu)), T(rng.normal(0, 1e-4, nu))
     n = fam.n
     sets = []

@@ -1,0 +1,111 @@
+"""BSIM4's general topology: gate resistance (rgateMod 1-3), the body resistance network (rbodyMod
+1/2), bias-dependent source / drain resistance (rdsMod 1) and instance initial conditions (IC1-3),
+each with the internal nodes and branch currents the reference gives it
+(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C: nodes :3684-3769, registerLIDs :4996-5075,
+jacStamp :4641-4795, the loads :16303-16853 and :17102-17172).
+
+CPU: the library's stamp table and topology query against the reference's own instances (the
+oracle library): the same internal variables per instance, numbered the same way, and a pattern
+that holds every entry the reference's stamps touch. GPU: the load through the C ABI against the
+oracle over DC and transient flag sequences with limiting active, within the parity tolerance of
+the other BSIM4 tests, for each mode on its own and all of them mixed in one family.
+"""
+import numpy as np
+import pytest
+
+from oracle import xyce_ref as xr
+from xyce_b200 import ModelCard, SolverFlags, netlist
+from xyce_b200.device import GEN_INTERNAL, general_stamp, internal_nodes
+
+from tests.parity import OracleRun, family_inputs
+
+pytestmark = pytest.mark.skipif(not xr.available(), reason="oracle library not built")
+
+# Sheet resistance with squares on every instance keeps the reference from falling back to its
+# 1e3 S conductance (and from warning about it) where rdsMod 1 asks for S/D resistors.
+_RS = {"RSH": 20.0}
+BODY5 = {"RBPS0": 60.0, "RBPD0": 70.0, "RBSBX0": 120.0, "RBSBY0": 150.0, "RBDBX0": 110.0, "RBDBY0": 140.0,
+         "RBPBX0": 90.0, "RBPBY0": 80.0, "RBSDBXL": 0.1, "RBPBXW": -0.2}
+CASES = {
+    "rgate1": [ModelCard(False, {"RGATEMOD": 1, "RSHG": 5.0}), ModelCard(True, {"RGATEMOD": 1, "RSHG": 8.0})],
+    "rgate2": [ModelCard(False, {"RGATEMOD": 2, "XRCRG1": 14.0, "XRCRG2": 1.5}),
+               ModelCard(True, {"RGATEMOD": 2, "RSHG": 3.0})],
+    "rgate3": [ModelCard(False, {"RGATEMOD": 3, "RSHG": 4.0, "CAPMOD": 1}),
+               ModelCard(True, {"RGATEMOD": 3, "XRCRG1": 10.0})],
+    "rbody1": [ModelCard(False, {"RBODYMOD": 1, "RBDB": 40.0, "RBSB": 30.0}),
+               ModelCard(True, {"RBODYMOD": 1, "GBMIN": 1e-10})],
+    "rbody2": [ModelCard(False, {"RBODYMOD": 2, **BODY5}), ModelCard(True, {"RBODYMOD": 2, "RBPS0": 55.0,
+                                                                             "RBPD0": 65.0})],
+    "rds1": [ModelCard(False, {"RDSMOD": 1, "RDSW": 150.0, "RDW": 80.0, "RSW": 90.0, "RDWMIN": 5.0, "RSWMIN": 4.0,
+                               "PRWG": 0.1, "PRWB": 0.05, **_RS}),
+             ModelCard(True, {"RDSMOD": 1, "RDW": 120.0, "RSW": 100.0, **_RS})],
+    "mixed": [ModelCard(False, {"RGATEMOD": 3, "RBODYMOD": 1, "RDSMOD": 1, "IGCMOD": 1, "RDW": 60.0, "RSW": 70.0,
+                                **_RS}),
+              ModelCard(True, {"RGATEMOD": 2, "RBODYMOD": 2, "CAPMOD": 0, **BODY5})],
+}
+
+
+def _extra(case, n, rng):
+    extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5)} if case in ("rds1", "mixed") else {}
+    if case == "mixed":
+        # Instance overrides of the modes, and initial conditions on some instances.
+        extra["RGATEMOD"] = np.where(rng.random(n) < 0.2, 1.0, np.nan)
+        extra["RBODYMOD"] = np.where(rng.random(n) < 0.2, 0.0, np.nan)
+        extra["IC1"] = np.where(rng.random(n) < 0.1, 0.4, np.nan)
+        extra["IC2"] = np.where(rng.random(n) < 0.1, 0.9, np.nan)
+        extra["IC3"] = np.where(rng.random(n) < 0.1, -0.2, np.nan)
+    return extra
+
+
+def _circuit(case, n_mos=600, seed=21):
+    c = netlist.random_logic(n_mos, seed=seed)
+    extra = _extra(case, c.n_mos, np.random.default_rng(seed))
+    cards, im, nd, params = family_inputs(c, CASES[case], extra)
+    flags, general = internal_nodes(cards, im, nd, params, general=True)
+    assert general
+    return netlist.with_internal_nodes(c, flags), cards, extra, flags
+
+
+def test_general_stamp_table_matches_library():
+    assert np.array_equal(general_stamp(), netlist.GEN_STAMP)
+    assert GEN_INTERNAL == 10
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_topology_matches_reference_instances(case):
+    """The internal variables the library lists per instance are the ones the reference's instances
+    register (count and numbering), and the pattern holds every entry their stamps touch
+    (OracleRun asserts the latter)."""
+    c, cards, extra, flags = _circuit(case, n_mos=300)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards_, im, nd, params = family_inputs(c, cards, extra)
+    orc = OracleRun(c, cards_, im, nd, params, rowptr, colind)
+    assert orc.ref.n_unknowns == c.n_unknowns
+    counts = np.array([orc.ref.num_internal(i) for i in range(c.n_mos)])
+    assert np.array_equal(counts, flags.sum(1))
+    # State slots: 3 + qgmid (rgateMod 3) + qbs, qbd (rbodyMod) per instance.
+    assert orc.n_sta_slots == 6
+    assert int((orc.sta_off >= 0).sum()) == orc.ref.n_state
+
+
+def test_plain_family_refuses_nothing_and_needs_no_general_topology():
+    c = netlist.random_logic(200, seed=3)
+    cards, im, nd, params = family_inputs(c)
+    flags, general = internal_nodes(cards, im, nd, params, general=True)
+    assert not general and not flags.any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", list(CASES))
+def test_general_topology_parity(case):
+    pytest.importorskip("torch")
+    from tests.gpu_parity import run_sequence
+
+    c, cards, extra, flags = _circuit(case)
+    tran = [SolverFlags(newton_iter=1, voltlim=0), SolverFlags(newton_iter=1), SolverFlags(newton_iter=2),
+            SolverFlags(newton_iter=0, init_tran=1), SolverFlags(newton_iter=1, init_tran=1),
+            SolverFlags(newton_iter=3)]
+    dc = [SolverFlags(dcop=1, transient=0, newton_iter=0, init_jct=1), SolverFlags(dcop=1, transient=0, newton_iter=1),
+          SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=2)]
+    worst = run_sequence(c, cards, dc + tran, extra_params=extra, vrange=(-0.4, 1.6), seed=4)
+    print(case, int(flags.sum()), "internal variables; worst error / tolerance:", worst)

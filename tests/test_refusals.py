@@ -22,7 +22,14 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
 
 @pytest.mark.parametrize("level,cards,extra,match", [
     (3, NMOS_PMOS, None, "not implemented"),
-    (14, [ModelCard(False, {"RGATEMOD": 1}), ModelCard(True, {})], None, "rgateMod"),
+    # Gate resistance is loaded through the general topology: without its internal unknowns the
+    # family is refused, naming the field that carries them.
+    (14, [ModelCard(False, {"RGATEMOD": 1}), ModelCard(True, {})], None, "inst_internal_gen"),
+    (14, [ModelCard(False, {"RGATEMOD": 4}), ModelCard(True, {})], None, "rgateMod must be 0, 1, 2 or 3"),
+    (14, [ModelCard(False, {"RBODYMOD": 3}), ModelCard(True, {})], None, "rbodyMod must be 0, 1 or 2"),
+    (14, [ModelCard(False, {"RDSMOD": 2}), ModelCard(True, {})], None, "rdsMod must be 0 or 1"),
+    (14, [ModelCard(False, {"TRNQSMOD": 1}), ModelCard(True, {})], None, "trnqsMod"),
+    (14, NMOS_PMOS, {"IC3": 0.2}, "inst_internal_gen"),
     (14, [ModelCard(False, {"CAPMOD": 3}), ModelCard(True, {})], None, "capMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {"IGCMOD": 3}), ModelCard(True, {})], None, "igcMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {}), ModelCard(True, {"IGBMOD": 2})], None, "igbMod must be 0 or 1"),

@@ -34,7 +34,7 @@ class XdMosfetFamily(ctypes.Structure):
         ("model_param_names", _cpp), ("model_param_values", _dp), ("n_inst", ctypes.c_int),
         ("inst_model", _ip), ("inst_nodes", _ip), ("n_inst_params", ctypes.c_int),
         ("inst_param_names", _cpp), ("inst_param_values", _dp), ("temp_c", ctypes.c_double),
-        ("tnom_c", ctypes.c_double), ("inst_internal", _ip),
+        ("tnom_c", ctypes.c_double), ("inst_internal", _ip), ("inst_internal_gen", _ip),
     ]
 
 
@@ -89,10 +89,13 @@ SIGNATURES = {
     "xd_load": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),
     "xd_load_abs": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 7),
     "xd_copy_stamps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_num_stage_slots": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_launches_per_load": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_eval_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
     "xd_num_eval_variants": (ctypes.c_int, []),
     "xd_internal_nodes": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), _ip]),
+    "xd_internal_nodes_gen": (ctypes.c_int, [ctypes.POINTER(XdMosfetFamily), _ip]),
+    "xd_general_stamp": (ctypes.c_int, [_ip, _ip]),
     "xd_eval_variant_info": (ctypes.c_int, [ctypes.c_int, _ip, _ip]),
     "xd_eval_variant_persistent": (ctypes.c_int, [ctypes.c_int]),
     "xd_eval_variant_split": (ctypes.c_int, [ctypes.c_int]),

@@ -30,9 +30,19 @@ namespace {
 // The instances' own state and store LIDs (the reference keeps them in protected members of
 // DeviceInstance and offers no getter for the store's): a pointer to the base class member, named
 // through a derived class, reads them from any instance.
+// The same holds for the node LIDs: DeviceInstance::getDevLIDs is filled only by the numerical
+// Jacobian test (N_DEV_DeviceInstance.C:383-388), so the binding reads the external and internal
+// LID vectors registerLIDs stored.
 struct LidAccess : public DeviceInstance {
   static const std::vector<int> &sta(const DeviceInstance &d) { return d.*(&LidAccess::staLIDVec); }
   static const std::vector<int> &sto(const DeviceInstance &d) { return d.*(&LidAccess::stoLIDVec); }
+  // External LIDs (D, G, S, B), then the internal ones in the instance's registerLIDs order.
+  static std::vector<int> nodes(const DeviceInstance &d) {
+    std::vector<int> v = d.*(&LidAccess::extLIDVec);
+    const std::vector<int> &in = d.*(&LidAccess::intLIDVec);
+    v.insert(v.end(), in.begin(), in.end());
+    return v;
+  }
 };
 
 void check_cuda(cudaError_t e, const char *what) {
@@ -186,9 +196,9 @@ bool Master::setup() {
       const size_t col = std::find(inames.begin(), inames.end(), lines_[i].params[k].first) - inames.begin();
       ivals[(size_t)i * inames.size() + col] = lines_[i].params[k].second;
     }
-    const std::vector<int> &lids = insts[i]->getDevLIDs();  // D, G, S, B, then internal D', S'
+    const std::vector<int> lids = LidAccess::nodes(*insts[i]);  // D, G, S, B, then internal D', S'
+    if (lids.size() < 4) throw std::runtime_error("GPU MOSFET binding: instance without its four terminal LIDs");
     for (int k = 0; k < 4; ++k) nodes[4 * (size_t)i + k] = lids[k] == ground_ ? -1 : lids[k];
-    for (int k = 4; k < (int)lids.size() && k < 6; ++k) internal[2 * (size_t)i + (k - 4)] = lids[k];
   }
   std::vector<const char *> inptr;
   for (size_t k = 0; k < inames.size(); ++k) inptr.push_back(inames[k].c_str());
@@ -207,38 +217,69 @@ bool Master::setup() {
   fam.inst_param_values = ivals.data();
   fam.temp_c = getDeviceOptions().temp.getImmutableValue<double>() - CONSTCtoK;
   fam.tnom_c = getDeviceOptions().tnom - CONSTCtoK;
-  // Internal drain / source nodes: which instances the library expects them on must match the
-  // reference's topology (both follow the same rule).
-  std::vector<int> flags(2 * (size_t)n_);
+  // Internal variables: which instances the library expects them on must match the reference's
+  // topology (both follow the same rules). Gate / body resistance, rdsMod 1 and instance initial
+  // conditions take the general topology (10 internal variables per instance, registerLIDs
+  // order); otherwise only the drain / source ones can exist.
   fam.inst_internal = 0;
-  check_xd(xd_internal_nodes(&fam, flags.data()), "xd_internal_nodes");
+  fam.inst_internal_gen = 0;
+  std::vector<int> gflags((size_t)XD_GEN_INTERNAL * n_);
+  const int general = xd_internal_nodes_gen(&fam, gflags.data());
+  if (general < 0) check_xd(general, "xd_internal_nodes_gen");
+  std::vector<int> internal_gen(general ? (size_t)XD_GEN_INTERNAL * n_ : 0, -1);
   bool any = false;
   for (int i = 0; i < n_; ++i) {
-    const int got = (int)insts[i]->getDevLIDs().size() - 4;
-    const int want = flags[2 * (size_t)i] + flags[2 * (size_t)i + 1];
-    if (got != want) throw std::runtime_error("GPU MOSFET binding: internal nodes differ from the reference's topology");
-    int k = 4;
-    const std::vector<int> &lids = insts[i]->getDevLIDs();
-    internal[2 * (size_t)i] = flags[2 * (size_t)i] ? lids[k++] : -1;
-    internal[2 * (size_t)i + 1] = flags[2 * (size_t)i + 1] ? lids[k++] : -1;
+    const std::vector<int> lids = LidAccess::nodes(*insts[i]);
+    const int *fl = &gflags[(size_t)XD_GEN_INTERNAL * i];
+    int want = 0;
+    for (int k = 0; k < XD_GEN_INTERNAL; ++k) want += fl[k];
+    if ((int)lids.size() - 4 != want)
+      throw std::runtime_error("GPU MOSFET binding: internal nodes differ from the reference's topology");
+    int next = 4;
+    for (int k = 0; k < XD_GEN_INTERNAL; ++k) {
+      const int lid = fl[k] ? lids[next++] : -1;
+      if (general) internal_gen[(size_t)XD_GEN_INTERNAL * i + k] = lid;
+      if (!general && k < 2) internal[2 * (size_t)i + k] = lid;
+    }
     any = any || want > 0;
   }
-  fam.inst_internal = any ? internal.data() : 0;
+  if (general)
+    fam.inst_internal_gen = internal_gen.data();
+  else
+    fam.inst_internal = any ? internal.data() : 0;
   xd_csr pat;
   pat.n_rows = n_unknowns_;
   pat.rowptr = rowptr_.data();
   pat.colind = colind.data();
   check_cuda(cudaSetDevice(device_), "cudaSetDevice");
   check_xd(xd_create(&fam, &pat, device_, &ctx_), "xd_create");
-  // State / store permutation: slot s of instance i lives at the instance's s-th LID.
+  // State / store permutation: slot s of instance i lives at the instance's s-th LID. With the
+  // general topology the library keeps six state slots (qb, qg, qd, qgmid, qbs, qbd) and an
+  // instance registers qgmid only with rgateMod 3 and qbs / qbd only with rbodyMod
+  // (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5225): the slots it lacks get no LID (-1).
   const int nst = xd_num_state_slots(ctx_), nso = xd_num_store_slots(ctx_);
-  sta_lid_.resize((size_t)nst * n_);
+  sta_lid_.assign((size_t)nst * n_, -1);
   sto_lid_.resize((size_t)nso * n_);
   for (int i = 0; i < n_; ++i) {
     const std::vector<int> &st = LidAccess::sta(*insts[i]), &so = LidAccess::sto(*insts[i]);
-    if ((int)st.size() < nst || (int)so.size() < nso)
-      throw std::runtime_error("GPU MOSFET binding: state / store registration differs from the library's");
-    for (int s = 0; s < nst; ++s) sta_lid_[(size_t)s * n_ + i] = st[s];
+    if ((int)so.size() < nso)
+      throw std::runtime_error("GPU MOSFET binding: store registration differs from the library's");
+    if (general) {
+      const int *fl = &gflags[(size_t)XD_GEN_INTERNAL * i];
+      const bool rg3 = fl[3] != 0, rb = fl[4] != 0;
+      const int want = 3 + (rg3 ? 1 : 0) + (rb ? 2 : 0);
+      if ((int)st.size() != want)
+        throw std::runtime_error("GPU MOSFET binding: state registration differs from the library's");
+      int next = 0;
+      for (int s = 0; s < nst; ++s) {
+        const bool has = s < 3 || (s == 3 && rg3) || (s > 3 && rb);
+        sta_lid_[(size_t)s * n_ + i] = has ? st[next++] : -1;
+      }
+    } else {
+      if ((int)st.size() < nst)
+        throw std::runtime_error("GPU MOSFET binding: state registration differs from the library's");
+      for (int s = 0; s < nst; ++s) sta_lid_[(size_t)s * n_ + i] = st[s];
+    }
     for (int s = 0; s < nso; ++s) sto_lid_[(size_t)s * n_ + i] = so[s];
   }
   cudaStream_t st;
@@ -273,8 +314,9 @@ bool Master::updateState(double *solVec, double *staVec, double *stoVec) {
   cudaStream_t st = (cudaStream_t)stream_;
   std::copy(solVec, solVec + n_unknowns_, h_sol_.begin());
   for (size_t k = 0; k < sta_lid_.size(); ++k) {
-    h_sta_[0][k] = staVec[sta_lid_[k]];
-    h_sta_[1][k] = currSta[sta_lid_[k]];
+    const int lid = sta_lid_[k];
+    h_sta_[0][k] = lid >= 0 ? staVec[lid] : 0.0;
+    h_sta_[1][k] = lid >= 0 ? currSta[lid] : 0.0;
   }
   for (size_t k = 0; k < sto_lid_.size(); ++k) {
     h_sto_[0][k] = stoVec[sto_lid_[k]];
@@ -297,6 +339,7 @@ bool Master::updateState(double *solVec, double *staVec, double *stoVec) {
              "copy");
   check_cuda(cudaStreamSynchronize(st), "synchronize");
   for (size_t k = 0; k < sta_lid_.size(); ++k) {
+    if (sta_lid_[k] < 0) continue;
     staVec[sta_lid_[k]] = h_sta_[0][k];
     currSta[sta_lid_[k]] = h_sta_[1][k];
   }

@@ -40,6 +40,45 @@ enum { kNumVec = 16, kNumMat = 16, kNumStage = kNumVec + 2 * kNumMat };
 // the external drain and source, the matrices six more slots for the resistor couplings.
 enum { kSerVecRows = 6, kSerMat = kNumMat + 6, kSerStage = 4 * kSerVecRows + 2 * kSerMat };
 
+// General topology (rgateMod 1-3, rbodyMod 1/2, rdsMod 1, instance initial conditions, and the
+// sheet-resistance D' / S' nodes): the reference's full stamp over 14 local nodes — the four
+// terminals, the internal drain / source / gate / gate-mid / body / source-body / drain-body nodes
+// (registerLIDs order, N_DEV_MOSFET_B4.C:5018-5060) and the three initial-condition branch currents.
+// A node the instance does not have is the same unknown as the one it collapses onto (D' -> D,
+// S' -> S, G' and GM -> G, B' / SB / DB -> B); an absent branch current has no unknown.
+enum GenNode { g_D, g_G, g_S, g_B, g_DP, g_SP, g_GP, g_GM, g_BP, g_SB, g_DB, g_IBS, g_IDS, g_IGS, kGenNodes };
+// The stamp's (row, column) pairs in the reference's jacStamp order (:4641-4755): rows D, G, S, B,
+// D', S', G', GM, B', SB, DB, then the three initial-condition rows with their two couplings each.
+constexpr int kGenStamp[][2] = {
+    {g_D, g_D},   {g_D, g_DP},   {g_D, g_SP},   {g_D, g_GP},   {g_D, g_BP},
+    {g_G, g_G},   {g_G, g_DP},   {g_G, g_SP},   {g_G, g_GP},   {g_G, g_GM},   {g_G, g_BP},
+    {g_S, g_S},   {g_S, g_DP},   {g_S, g_SP},   {g_S, g_GP},   {g_S, g_BP},
+    {g_B, g_B},   {g_B, g_BP},   {g_B, g_SB},   {g_B, g_DB},
+    {g_DP, g_D},  {g_DP, g_DP},  {g_DP, g_SP},  {g_DP, g_GP},  {g_DP, g_GM},  {g_DP, g_BP},  {g_DP, g_DB},
+    {g_SP, g_S},  {g_SP, g_DP},  {g_SP, g_SP},  {g_SP, g_GP},  {g_SP, g_GM},  {g_SP, g_BP},  {g_SP, g_SB},
+    {g_GP, g_G},  {g_GP, g_DP},  {g_GP, g_SP},  {g_GP, g_GP},  {g_GP, g_GM},  {g_GP, g_BP},
+    {g_GM, g_G},  {g_GM, g_DP},  {g_GM, g_SP},  {g_GM, g_GP},  {g_GM, g_GM},  {g_GM, g_BP},
+    {g_BP, g_B},  {g_BP, g_DP},  {g_BP, g_SP},  {g_BP, g_GP},  {g_BP, g_GM},  {g_BP, g_BP},  {g_BP, g_SB},
+    {g_BP, g_DB},
+    {g_SB, g_B},  {g_SB, g_SP},  {g_SB, g_BP},  {g_SB, g_SB},
+    {g_DB, g_B},  {g_DB, g_DP},  {g_DB, g_BP},  {g_DB, g_DB},
+    {g_IBS, g_S}, {g_IBS, g_B},  {g_IBS, g_IBS}, {g_S, g_IBS}, {g_B, g_IBS},
+    {g_IDS, g_D}, {g_IDS, g_S},  {g_IDS, g_IDS}, {g_D, g_IDS}, {g_S, g_IDS},
+    {g_IGS, g_G}, {g_IGS, g_S},  {g_IGS, g_IGS}, {g_G, g_IGS}, {g_S, g_IGS}};
+constexpr int kGenSlots = sizeof(kGenStamp) / sizeof(kGenStamp[0]);
+static_assert(kGenSlots == 77, "the general stamp has 62 device entries and 15 initial-condition entries");
+// Slot of (row, col) in kGenStamp; -1 if the stamp has no such entry.
+constexpr int gen_slot(int r, int c) {
+  for (int k = 0; k < kGenSlots; ++k)
+    if (kGenStamp[k][0] == r && kGenStamp[k][1] == c) return k;
+  return -1;
+}
+// State slots of the general topology: the three intrinsic charges, then the gate-mid charge
+// (rgateMod 3) and the two junction charges (rbodyMod), in registerStateLIDs order (:5212-5225).
+enum GenState { gt_qb, gt_qg, gt_qd, gt_qgmid, gt_qbs, gt_qbd, kGenState };
+// Staging of one instance: 4 vectors x 14 rows, then dF/dx and dQ/dx over the 77 stamp slots.
+enum { kGenVecRows = kGenNodes, kGenStage = 4 * kGenVecRows + 2 * kGenSlots };
+
 struct LoadOut {
   double vec[kNumVec];
   double jf[kNumMat];
@@ -52,6 +91,12 @@ struct LoadOut {
   double sta[kNumState];
   bool write_curr_sta;    // first Newton step of the first transient step: also write currSta
   double vgb;             // this load's vgb (the next load's "vgb_orig")
+  // General topology: vectors gv[v * 14 + node] (F, Q, dF/dx*dVp, dQ/dx*dVp), the two matrices over
+  // the stamp slots, and the six state slots (zero where the instance has no such charge).
+  double gv[4 * kGenNodes];
+  double gf[kGenSlots];
+  double gq[kGenSlots];
+  double gsta[kGenState];
 };
 
 // Field-major record view: field f of this instance's record.
@@ -111,10 +156,15 @@ enum MidSlot {
   // Gate tunnelling currents (the full evaluation variants only).
   m_Igs = kNumMid, m_gIgsg, m_gIgss, m_Igd, m_gIgdg, m_gIgdd, m_Igcs, m_gIgcsg, m_gIgcsd, m_gIgcsb, m_Igcd,
   m_gIgcdg, m_gIgcdd, m_gIgcdb, m_Igb, m_gIgbg, m_gIgbd, m_gIgbb,
-  kNumMidFull
+  kNumMidFull,
+  // General topology: the limited gate, source / drain and body-network voltages, the gate
+  // resistance conductances (rgateMod 2/3) and the bias-dependent S/D conductances (rdsMod 1).
+  m_vges = kNumMidFull, m_vgms, m_vdes, m_vses, m_vdbs, m_vsbs, m_gcrg, m_gcrgg, m_gcrgd, m_gcrgs, m_gcrgb,
+  m_gstot, m_gstotd, m_gstotg, m_gstots, m_gstotb, m_gdtot, m_gdtotd, m_gdtotg, m_gdtots, m_gdtotb,
+  kNumMidGen
 };
 struct Mid {
-  double v[kNumMidFull];
+  double v[kNumMidGen];
 };
 
 #define P(x) P_(f_##x)
@@ -123,32 +173,42 @@ struct Mid {
 // initial-condition overrides applied (:7932-8097).
 struct Bias {
   double Vd, Vs, Vdp, Vsp, Vddp, Vssp;
+  // General topology: body-network drops, gate-resistor drops (unlimited, untyped: :7966-8004).
+  double Vdbb, Vdbbp, Vsbb, Vsbbp, Vbpb, Vgegp, Vgegm, Vgmgp;
   double vds, vgs, vbs, vges, vgms, vdbs, vsbs, vses, vdes, vbd, vdbd, vgd, vged, vgmd, vgmb, vbs_jct, vbd_jct;
   double vbd_orig, vbs_orig, vgs_orig, vds_orig, vgd_orig, vges_orig, vgms_orig, vdes_orig, vses_orig, vdbs_orig;
   double vsbs_orig, vdbd_orig, vged_orig, vgmd_orig, vbs_jct_orig, vbd_jct_orig, vgmb_orig;
   int origFlag;
 };
 
-template <bool SERIES, class RV>
-XD_HD void bsim4_bias(const RV &P_, const double V[4], const LoadFlags &fl, const double *Vx, Bias &b) {
+// V: with GEN the 14 local node values (GenNode order; collapsed nodes carry their representative's
+// value), else the 4 (D', G, S', B) with Vx the external (D, S) under SERIES.
+template <bool SERIES, bool GEN = false, class RV>
+XD_HD void bsim4_bias(const RV &P_, const double *V, const LoadFlags &fl, const double *Vx, Bias &b) {
   using namespace xdc;
   const double dtype = P(dtype);
   const double vth0 = P(vth0);
   const bool OFF = P(off) != 0.0;
-  // Node and branch voltages (:7932-8030), collapsed topology.
-  const double Vdp = V[0], Vge = V[1], Vsp = V[2], Vb = V[3];
-  const double Vd = SERIES ? Vx[0] : Vdp, Vs = SERIES ? Vx[1] : Vsp;
-  const double Vgp = Vge, Vbp = Vb, Vgm = Vge, Vdb = Vb, Vsb = Vb;
-  (void)Vgp; (void)Vbp; (void)Vgm; (void)Vdb; (void)Vsb;
+  const bool rbodyMod = GEN && P(rbodyMod) != 0.0;
+  // Node and branch voltages (:7932-8030).
+  double Vdp, Vge, Vsp, Vb, Vd, Vs, Vgp, Vbp, Vgm, Vdb, Vsb;
+  if (GEN) {
+    Vd = V[g_D]; Vs = V[g_S]; Vb = V[g_B]; Vsp = V[g_SP]; Vdp = V[g_DP];
+    Vgp = V[g_GP]; Vbp = V[g_BP]; Vge = V[g_G]; Vgm = V[g_GM]; Vdb = V[g_DB]; Vsb = V[g_SB];
+  } else {
+    Vdp = V[0]; Vge = V[1]; Vsp = V[2]; Vb = V[3];
+    Vd = SERIES ? Vx[0] : Vdp;
+    Vs = SERIES ? Vx[1] : Vsp;
+    Vgp = Vge; Vbp = Vb; Vgm = Vge; Vdb = Vb; Vsb = Vb;
+  }
   const double Vddp = Vd - Vdp, Vssp = Vs - Vsp;
-  (void)Vddp; (void)Vssp;
   double vds = dtype * (Vdp - Vsp);
-  double vgs = dtype * (Vge - Vsp);
-  double vbs = dtype * (Vb - Vsp);
+  double vgs = dtype * (Vgp - Vsp);
+  double vbs = dtype * (Vbp - Vsp);
   double vges = dtype * (Vge - Vsp);
-  double vgms = dtype * (Vge - Vsp);
-  double vdbs = dtype * (Vb - Vsp);
-  double vsbs = dtype * (Vb - Vsp);
+  double vgms = dtype * (Vgm - Vsp);
+  double vdbs = dtype * (Vdb - Vsp);
+  double vsbs = dtype * (Vsb - Vsp);
   double vses = dtype * (Vs - Vsp);
   double vdes = dtype * (Vd - Vsp);
   double vbd = vbs - vds;
@@ -157,8 +217,16 @@ XD_HD void bsim4_bias(const RV &P_, const double V[4], const LoadFlags &fl, cons
   double vged = vges - vds;
   double vgmd = vgms - vds;
   double vgmb = vgms - vbs;
-  double vbs_jct = vbs;
-  double vbd_jct = vbd;
+  double vbs_jct = (!rbodyMod) ? vbs : vsbs;
+  double vbd_jct = (!rbodyMod) ? vbd : vdbd;
+  b.Vdbb = Vdb - Vb;
+  b.Vdbbp = Vdb - Vbp;
+  b.Vsbb = Vsb - Vb;
+  b.Vsbbp = Vsb - Vbp;
+  b.Vbpb = Vbp - Vb;
+  b.Vgegp = Vge - Vgp;
+  b.Vgegm = Vge - Vgm;
+  b.Vgmgp = Vgm - Vgp;
   int origFlag = 1;
   const double vbd_orig = vbd, vbs_orig = vbs, vgs_orig = vgs, vds_orig = vds, vgd_orig = vgd;
   const double vges_orig = vges, vgms_orig = vgms, vdes_orig = vdes, vses_orig = vses, vdbs_orig = vdbs;
@@ -197,8 +265,8 @@ XD_HD void bsim4_bias(const RV &P_, const double V[4], const LoadFlags &fl, cons
 // Charge-and-stamp part of the evaluation: charges and capacitances, store and state, the F / Q /
 // limiter-vector stamps and the dF/dx, dQ/dx stamps (:10707-13855, 16195-17268), from the DC part's
 // hand-off state m.
-template <bool FULL = false, bool SERIES = false, class RV>
-XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, double vgb_orig, const Mid &m,
+template <bool FULL = false, bool SERIES = false, bool GEN = false, class RV>
+XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, double vgb_orig, const Mid &m,
                         LoadOut &o, const double *Vx) {
   using namespace xdc;
   const double dtype = P(dtype);
@@ -207,8 +275,11 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
   const double nf = P(nf);
   const double M = P(mult);
   const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
+  const int rgateMod = GEN ? (int)P(rgateMod) : 0;
+  const bool rbodyMod = GEN && P(rbodyMod) != 0.0;
+  const bool rdsMod = GEN && P(rdsMod) != 0.0;
   Bias bias;
-  bsim4_bias<SERIES>(P_, V, fl, Vx, bias);
+  bsim4_bias<SERIES, GEN>(P_, V, fl, Vx, bias);
   const double Vddp = bias.Vddp, Vssp = bias.Vssp;
   (void)Vddp; (void)Vssp;
   double vds = bias.vds, vgs = bias.vgs, vbs = bias.vbs, vges = bias.vges, vgms = bias.vgms, vdbs = bias.vdbs;
@@ -230,6 +301,14 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
   vgs = m.v[m_vgs];
   vbs = m.v[m_vbs];
   origFlag = (int)m.v[m_orig];
+  if (GEN) {
+    vges = m.v[m_vges];
+    vgms = m.v[m_vgms];
+    vdes = m.v[m_vdes];
+    vses = m.v[m_vses];
+    vdbs = m.v[m_vdbs];
+    vsbs = m.v[m_vsbs];
+  }
   vbd = vbs - vds;
   vgd = vgs - vds;
   vgb = vgs - vbs;
@@ -237,8 +316,8 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
   vgmd = vgms - vds;
   vgmb = vgms - vbs;
   vdbd = vdbs - vds;
-  vbs_jct = vbs;
-  vbd_jct = vbd;
+  vbs_jct = (!rbodyMod) ? vbs : vsbs;
+  vbd_jct = (!rbodyMod) ? vbd : vdbd;
   (void)vged; (void)vgmd;
   double T0, T1, T2, T3, T4, T5, T6, T7, T8, T9, T10, T11, T12, T13, T14;
   double dT0_dVg, dT0_dVd, dT0_dVb, dT1_dVg, dT1_dVd, dT1_dVb, dT2_dVg, dT2_dVd, dT2_dVb;
@@ -844,8 +923,21 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
     }
   }
 
-  // Overlap capacitances (:11846-11890): constant for capMod 0, bias-dependent for 1 and 2.
-  const double vgdx = vgd, vgsx = vgs;
+  // Overlap capacitances (:11812-11890): constant for capMod 0, bias-dependent for 1 and 2; with
+  // rgateMod 3 they sit between the gate-mid node and the drain / source.
+  const double vgdx = (rgateMod == 3) ? vgmd : vgd, vgsx = (rgateMod == 3) ? vgms : vgs;
+  // Gate resistor currents (:11824-11844).
+  double Igate = 0.0, IgateMid = 0.0;
+  if (GEN) {
+    if (rgateMod == 1) {
+      Igate = P(grgeltd) * (bias.Vgegp);
+    } else if (rgateMod == 2) {
+      Igate = (m.v[m_gcrg]) * (bias.Vgegp);
+    } else if (rgateMod == 3) {
+      Igate = P(grgeltd) * (bias.Vgegm);
+      IgateMid = m.v[m_gcrg] * (bias.Vgmgp);
+    }
+  }
   double cgdo, qgdo, cgso, qgso;
   if (capMod == 0) {
     cgdo = P(cgdo);
@@ -878,30 +970,140 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
   // Overlap and gate-bulk charge bookkeeping (setupCapacitors_oldDAE, trnqsMod = 0, :12624-12760).
   const double cgbo = P(cgbo);
   double dxpart, sxpart;
+  double qgmid = 0.0;  // rgateMod 3: the overlap and gate-bulk charge on the gate-mid node
   if (mode > 0) {
     qdrn -= qgdo;
-    const double qgb = cgbo * vgb;
-    qgate += qgdo + qgso + qgb;
-    qbulk -= qgb;
-    qsrc = -(qgate + qbulk + qdrn);
+    if (rgateMod == 3) {
+      const double qgmb = cgbo * vgmb;
+      qgmid = qgdo + qgso + qgmb;
+      qbulk -= qgmb;
+      qsrc = -(qgate + qgmid + qbulk + qdrn);
+    } else {
+      const double qgb = cgbo * vgb;
+      qgate += qgdo + qgso + qgb;
+      qbulk -= qgb;
+      qsrc = -(qgate + qbulk + qdrn);
+    }
     sxpart = 0.6;
     dxpart = 0.4;
   } else {
     qsrc = qdrn - qgso;
-    const double qgb = cgbo * vgb;
-    qgate += qgdo + qgso + qgb;
-    qbulk -= qgb;
-    qdrn = -(qgate + qbulk + qsrc);
+    if (rgateMod == 3) {
+      const double qgmb = cgbo * vgmb;
+      qgmid = qgdo + qgso + qgmb;
+      qbulk -= qgmb;
+      qdrn = -(qgate + qgmid + qbulk + qsrc);
+    } else {
+      const double qgb = cgbo * vgb;
+      qgate += qgdo + qgso + qgb;
+      qbulk -= qgb;
+      qdrn = -(qgate + qbulk + qsrc);
+    }
     sxpart = 0.4;
     dxpart = 0.6;
   }
   (void)qsrc;
 
-  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = rgateMod = rbodyMod = 0).
+  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = 0, :12357-12608).
   double CAPcggb, CAPcgdb, CAPcgsb, CAPcgbb, CAPcdgb, CAPcsgb, CAPcbgb, CAPcddb, CAPcdsb, CAPcsdb, CAPcssb;
   double CAPcdbb, CAPcsbb, CAPcbdb, CAPcbsb, CAPcbbb;
-  const double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
-  if (mode > 0) {
+  double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
+  double CAPcgmgmb = 0.0, CAPcgmdb = 0.0, CAPcgmsb = 0.0, CAPcgmbb = 0.0, CAPcdbdb = 0.0, CAPcsbsb = 0.0;
+  if (GEN) {
+    if (mode > 0) {
+      if (rgateMod == 3) {
+        CAPcgmgmb = (cgdo + cgso + cgbo);
+        CAPcgmdb = -cgdo;
+        CAPcgmsb = -cgso;
+        CAPcgmbb = -cgbo;
+        CAPcdgmb = CAPcgmdb;
+        CAPcsgmb = CAPcgmsb;
+        CAPcbgmb = CAPcgmbb;
+        CAPcggb = cggb;
+        CAPcgdb = cgdb;
+        CAPcgsb = cgsb;
+        CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+        CAPcdgb = cdgb;
+        CAPcsgb = -(cggb + cbgb + cdgb);
+        CAPcbgb = cbgb;
+      } else {
+        CAPcggb = (cggb + cgdo + cgso + cgbo);
+        CAPcgdb = (cgdb - cgdo);
+        CAPcgsb = (cgsb - cgso);
+        CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+        CAPcdgb = (cdgb - cgdo);
+        CAPcsgb = -(cggb + cbgb + cdgb + cgso);
+        CAPcbgb = (cbgb - cgbo);
+        CAPcdgmb = CAPcsgmb = CAPcbgmb = 0.0;
+      }
+      CAPcddb = (cddb + capbd + cgdo);
+      CAPcdsb = cdsb;
+      CAPcsdb = -(cgdb + cbdb + cddb);
+      CAPcssb = (capbs + cgso - (cgsb + cbsb + cdsb));
+      if (!rbodyMod) {
+        CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+        CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+        CAPcbdb = (cbdb - capbd);
+        CAPcbsb = (cbsb - capbs);
+        CAPcdbdb = 0.0;
+        CAPcsbsb = 0.0;
+      } else {
+        CAPcdbb = -(cddb + cdgb + cdsb);
+        CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb) + capbs;
+        CAPcbdb = cbdb;
+        CAPcbsb = cbsb;
+        CAPcdbdb = -capbd;
+        CAPcsbsb = -capbs;
+      }
+      CAPcbbb = -(CAPcbdb + CAPcbgb + CAPcbsb + CAPcbgmb);
+    } else {
+      if (rgateMod == 3) {
+        CAPcgmgmb = (cgdo + cgso + cgbo);
+        CAPcgmdb = -cgdo;
+        CAPcgmsb = -cgso;
+        CAPcgmbb = -cgbo;
+        CAPcdgmb = CAPcgmdb;
+        CAPcsgmb = CAPcgmsb;
+        CAPcbgmb = CAPcgmbb;
+        CAPcggb = cggb;
+        CAPcgdb = cgsb;
+        CAPcgsb = cgdb;
+        CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+        CAPcdgb = -(cggb + cbgb + cdgb);
+        CAPcsgb = cdgb;
+        CAPcbgb = cbgb;
+      } else {
+        CAPcggb = (cggb + cgdo + cgso + cgbo);
+        CAPcgdb = (cgsb - cgdo);
+        CAPcgsb = (cgdb - cgso);
+        CAPcgbb = -(CAPcggb + CAPcgdb + CAPcgsb);
+        CAPcdgb = -(cggb + cbgb + cdgb + cgdo);
+        CAPcsgb = (cdgb - cgso);
+        CAPcbgb = (cbgb - cgbo);
+        CAPcdgmb = CAPcsgmb = CAPcbgmb = 0.0;
+      }
+      CAPcddb = (capbd + cgdo - (cgsb + cbsb + cdsb));
+      CAPcdsb = -(cgdb + cbdb + cddb);
+      CAPcsdb = cdsb;
+      CAPcssb = (cddb + capbs + cgso);
+      if (!rbodyMod) {
+        CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb);
+        CAPcsbb = -(CAPcsgb + CAPcsdb + CAPcssb + CAPcsgmb);
+        CAPcbdb = (cbsb - capbd);
+        CAPcbsb = (cbdb - capbs);
+        CAPcdbdb = 0.0;
+        CAPcsbsb = 0.0;
+      } else {
+        CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdsb + CAPcdgmb) + capbd;
+        CAPcsbb = -(cddb + cdgb + cdsb);
+        CAPcbdb = cbsb;
+        CAPcbsb = cbdb;
+        CAPcdbdb = -capbd;
+        CAPcsbsb = -capbs;
+      }
+      CAPcbbb = -(CAPcbgb + CAPcbdb + CAPcbsb + CAPcbgmb);
+    }
+  } else if (mode > 0) {
     CAPcggb = (cggb + cgdo + cgso + cgbo);
     CAPcgdb = (cgdb - cgdo);
     CAPcgsb = (cgsb - cgso);
@@ -954,14 +1156,22 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
   o.sto[s_von] = von;
   const double qg = qgate;
   const double qd = qdrn - qbd;
-  const double qb = qbulk + qbd + qbs;
+  const double qb = (!rbodyMod) ? qbulk + qbd + qbs : qbulk;
   o.sta[t_qg] = qg;
   o.sta[t_qd] = qd;
   o.sta[t_qb] = qb;
+  if (GEN) {
+    o.gsta[gt_qb] = qb;
+    o.gsta[gt_qg] = qg;
+    o.gsta[gt_qd] = qd;
+    o.gsta[gt_qgmid] = (rgateMod == 3) ? qgmid : 0.0;
+    o.gsta[gt_qbs] = rbodyMod ? qbs : 0.0;
+    o.gsta[gt_qbd] = rbodyMod ? qbd : 0.0;
+  }
   o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
   o.vgb = vgb;
 
-  // setupFVectorVars (:13525-13855), rgateMod = rdsMod = 0.
+  // setupFVectorVars (:13525-13855).
   const double gjbd = gbd, gjbs = gbs;
   double Gmv, Gmbsv, FwdSum, RevSum, ceqdrn, ceqdrn_Jdxp, ceqbd, ceqbd_Jdxp, ceqbs, ceqbs_Jdxp;
   double gbbdp, gbbsp, gbdpg, gbdpdp, gbdpb, gbdpsp, gbspg, gbspdp, gbspb, gbspsp;
@@ -1011,7 +1221,7 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
     gbspdp = -(gbspg + gbspsp + gbspb);
   }
   // Gate-current totals (:13112-13170, mode >= 0; :13243-13300, mode < 0).
-  const double ceqgcrg = 0.0, ceqgcrg_Jdxp = 0.0;
+  double ceqgcrg = 0.0, ceqgcrg_Jdxp = 0.0;
   double Istoteq = 0.0, Idtoteq = 0.0, Ibtoteq = 0.0, Igtoteq = 0.0;
   double Istoteq_Jdxp = 0.0, Idtoteq_Jdxp = 0.0, Ibtoteq_Jdxp = 0.0, Igtoteq_Jdxp = 0.0;
   double gIstotg = 0.0, gIstotd = 0.0, gIstots = 0.0, gIstotb = 0.0;
@@ -1076,8 +1286,55 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
     Igtoteq = Istoteq + Idtoteq + Ibtoteq;
     Igtoteq_Jdxp = Istoteq_Jdxp + Idtoteq_Jdxp + Ibtoteq_Jdxp;
   }
-  const double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
-  const double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
+  // Gate resistance (rgateMod 2 / 3): the reference scales the DC part's derivatives by the
+  // gate-resistor drop in place and folds gcrg into gcrgg (:13637-13664, :13767-13795).
+  double gcrg = GEN ? m.v[m_gcrg] : 0.0, gcrgg = GEN ? m.v[m_gcrgg] : 0.0, gcrgd = GEN ? m.v[m_gcrgd] : 0.0;
+  double gcrgs = GEN ? m.v[m_gcrgs] : 0.0, gcrgb = GEN ? m.v[m_gcrgb] : 0.0;
+  if (GEN) {
+    double Tg = 0.0;
+    if (rgateMod == 2)
+      Tg = vges - vgs;
+    else if (rgateMod == 3)
+      Tg = vgms - vgs;
+    if (rgateMod > 1) {
+      if (mode >= 0) {
+        gcrgd = gcrgd * Tg;
+        gcrgg = gcrgg * Tg;
+        gcrgs = gcrgs * Tg;
+        gcrgb = gcrgb * Tg;
+        ceqgcrg = 0.0;
+        ceqgcrg_Jdxp = -(gcrgd * (vds - vds_orig) + gcrgg * (vgs - vgs_orig) + gcrgb * (vbs - vbs_orig));
+      } else {
+        const double tmp_gcrgd = gcrgd;
+        gcrgd = gcrgs * Tg;
+        gcrgg = gcrgg * Tg;
+        gcrgs = tmp_gcrgd * Tg;
+        gcrgb = gcrgb * Tg;
+        ceqgcrg = 0.0;
+        ceqgcrg_Jdxp = -(gcrgg * (vgd - vgd_orig) - gcrgs * (vds - vds_orig) + gcrgb * (vbd - vbd_orig));
+      }
+      gcrgg -= gcrg;
+    } else {
+      ceqgcrg = gcrg = gcrgd = gcrgg = gcrgs = gcrgb = 0.0;
+      ceqgcrg_Jdxp = 0.0;
+    }
+  }
+  // Bias-dependent S/D resistance (rdsMod 1, :13797-13820).
+  double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
+  double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
+  double ceqgstot = 0.0, ceqgstot_Jdxp = 0.0, ceqgdtot = 0.0, ceqgdtot_Jdxp = 0.0;
+  if (rdsMod) {
+    gstot = m.v[m_gstot]; gstotd = m.v[m_gstotd]; gstotg = m.v[m_gstotg]; gstots = m.v[m_gstots];
+    gstotb = m.v[m_gstotb];
+    gdtot = m.v[m_gdtot]; gdtotd = m.v[m_gdtotd]; gdtotg = m.v[m_gdtotg]; gdtots = m.v[m_gdtots];
+    gdtotb = m.v[m_gdtotb];
+    ceqgstot = 0.0;
+    ceqgstot_Jdxp = dtype * (gstotd * (vds - vds_orig) + gstotg * (vgs - vgs_orig) + gstotb * (vbs - vbs_orig));
+    gstots = gstots - gstot;
+    ceqgdtot = 0.0;
+    ceqgdtot_Jdxp = -dtype * (gdtotd * (vds - vds_orig) + gdtotg * (vgs - vgs_orig) + gdtotb * (vbs - vbs_orig));
+    gdtotd = gdtotd - gdtot;
+  }
   double ceqjs, ceqjs_Jdxp, ceqjd, ceqjd_Jdxp;
   if (dtype > 0) {
     ceqjs = (cbs);
@@ -1089,6 +1346,368 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
     ceqjs_Jdxp = (gbs * (vbs_jct - vbs_jct_orig));
     ceqjd = -(cbd);
     ceqjd_Jdxp = (gbd * (vbd_jct - vbd_jct_orig));
+    ceqgcrg = -ceqgcrg;
+    ceqgcrg_Jdxp = -ceqgcrg_Jdxp;
+  }
+  (void)ceqgstot; (void)ceqgdtot;
+
+  if constexpr (GEN) {
+    // ---- General topology: the reference's loads over the 14 local nodes ----
+    const bool lim = fl.voltlim && !origFlag;
+    // Terminal resistor and body-network currents (:11896-11917).
+    const double Idrain = rdsMod ? gdtot * Vddp : P(drainConductance) * Vddp;
+    const double Isource = rdsMod ? gstot * Vssp : P(sourceConductance) * Vssp;
+    double Idbb = 0.0, Idbbp = 0.0, Isbb = 0.0, Isbbp = 0.0, Ibpb = 0.0;
+    if (rbodyMod) {
+      Idbb = P(grbdb) * bias.Vdbb;
+      Idbbp = P(grbpd) * bias.Vdbbp;
+      Isbb = P(grbsb) * bias.Vsbb;
+      Isbbp = P(grbps) * bias.Vsbbp;
+      Ibpb = P(grbpb) * bias.Vbpb;
+    }
+    const double Igate_Jdxp = 0.0, IgateMid_Jdxp = 0.0;  // the reference leaves both at zero (:11826)
+#define GV(v, node) o.gv[(v)*kGenNodes + (node)]
+    for (int k = 0; k < 4 * kGenNodes; ++k) o.gv[k] = 0.0;
+    // Master::loadDAEVectors (:16316-16564).
+    GV(0, g_DP) += -(ceqjd - ceqbd - ceqdrn + Idtoteq) * M;
+    GV(0, g_GP) -= -(-ceqgcrg + Igtoteq) * M;
+    if (rgateMod == 1) {
+      GV(0, g_G) -= -(Igate) * M;
+      GV(0, g_GP) += -(Igate) * M;
+    } else if (rgateMod == 2) {
+      GV(0, g_G) -= -(Igate + ceqgcrg) * M;
+      GV(0, g_GP) += -(Igate) * M;
+    } else if (rgateMod == 3) {
+      GV(0, g_G) -= -(Igate) * M;
+      GV(0, g_GM) -= -(IgateMid - Igate + ceqgcrg) * M;
+      GV(0, g_GP) += -(IgateMid) * M;
+    }
+    if (!rbodyMod) {
+      GV(0, g_BP) += -(ceqbd + ceqbs - ceqjd - ceqjs + Ibtoteq) * M;
+      GV(0, g_SP) += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
+    } else {
+      GV(0, g_DB) -= -(ceqjd + Idbb + Idbbp) * M;
+      GV(0, g_BP) += -(ceqbd + ceqbs + Ibtoteq + Idbbp + Isbbp - Ibpb) * M;
+      GV(0, g_B) += -(Isbb + Idbb + Ibpb) * M;
+      GV(0, g_SB) -= -(ceqjs + Isbb + Isbbp) * M;
+      GV(0, g_SP) += -(ceqdrn - ceqbs + ceqjs + Istoteq) * M;
+    }
+    if (rdsMod) {
+      GV(0, g_D) += -(-ceqgdtot) * M;
+      GV(0, g_S) += -(ceqgstot) * M;
+      GV(0, g_DP) += -(ceqgdtot) * M;
+      GV(0, g_SP) += -(-ceqgstot) * M;
+    }
+    if (P(dExists) != 0.0) {
+      GV(0, g_D) += -(-Idrain) * M;
+      GV(0, g_DP) += -(Idrain) * M;
+    }
+    if (P(sExists) != 0.0) {
+      GV(0, g_S) += -(-Isource) * M;
+      GV(0, g_SP) += -(+Isource) * M;
+    }
+    // Instance initial conditions: a branch current enforcing the terminal voltage during the
+    // operating point (:16373-16401); not scaled by the multiplier.
+    if (fl.dcop && P(icVBSGiven) != 0.0) {
+      const double coef = V[g_IBS];
+      GV(0, g_B) += coef;
+      GV(0, g_S) += -coef;
+      GV(0, g_IBS) += (V[g_B] - V[g_S] - P(icVBS));
+    }
+    if (fl.dcop && P(icVDSGiven) != 0.0) {
+      const double coef = V[g_IDS];
+      GV(0, g_D) += coef;
+      GV(0, g_S) += -coef;
+      GV(0, g_IDS) += (V[g_D] - V[g_S] - P(icVDS));
+    }
+    if (fl.dcop && P(icVGSGiven) != 0.0) {
+      const double coef = V[g_IGS];
+      GV(0, g_G) += coef;
+      GV(0, g_S) += -coef;
+      GV(0, g_IGS) += (V[g_G] - V[g_S] - P(icVGS));
+    }
+    if (lim) {
+      GV(2, g_DP) += (ceqjd_Jdxp - ceqbd_Jdxp - ceqdrn_Jdxp + Idtoteq_Jdxp) * M;
+      GV(2, g_GP) -= (-ceqgcrg_Jdxp + Igtoteq_Jdxp) * M;
+      if (rgateMod == 1) {
+        GV(2, g_G) -= (Igate_Jdxp) * M;
+        GV(2, g_GP) += (Igate_Jdxp) * M;
+      } else if (rgateMod == 2) {
+        GV(2, g_G) -= (Igate_Jdxp + ceqgcrg_Jdxp) * M;
+        GV(2, g_GP) += (Igate_Jdxp) * M;
+      } else if (rgateMod == 3) {
+        GV(2, g_G) -= (Igate_Jdxp) * M;
+        GV(2, g_GM) -= (IgateMid_Jdxp - Igate_Jdxp + ceqgcrg_Jdxp) * M;
+        GV(2, g_GP) += (IgateMid_Jdxp) * M;
+      }
+      if (!rbodyMod) {
+        GV(2, g_BP) += (ceqbd_Jdxp + ceqbs_Jdxp - ceqjd_Jdxp - ceqjs_Jdxp + Ibtoteq_Jdxp) * M;
+        GV(2, g_SP) += (ceqdrn_Jdxp - ceqbs_Jdxp + ceqjs_Jdxp + Istoteq_Jdxp) * M;
+      } else {
+        GV(2, g_DB) -= (ceqjd_Jdxp) * M;
+        GV(2, g_BP) += (ceqbd_Jdxp + ceqbs_Jdxp + Ibtoteq_Jdxp) * M;
+        GV(2, g_SB) -= (ceqjs_Jdxp) * M;
+        GV(2, g_SP) += (ceqdrn_Jdxp - ceqbs_Jdxp + ceqjs_Jdxp + Istoteq_Jdxp) * M;
+      }
+      if (rdsMod) {
+        GV(2, g_D) -= (ceqgdtot_Jdxp) * M;
+        GV(2, g_S) += (ceqgstot_Jdxp) * M;
+        GV(2, g_DP) += (ceqgdtot_Jdxp) * M;
+        GV(2, g_SP) -= (ceqgstot_Jdxp) * M;
+      }
+    }
+    // auxChargeCalculations (:12216-12350).
+    double Qeqqg_Jdxp = 0.0, Qeqqd_Jdxp = 0.0, Qeqqb_Jdxp = 0.0, Qeqqgmid_Jdxp = 0.0;
+    double Qeqqjs_Jdxp = 0.0, Qeqqjd_Jdxp = 0.0;
+    if (ChargeComputationNeeded && !origFlag) {
+      Qeqqg_Jdxp = -CAPcggb * (vgb - vgb_orig) + CAPcgdb * (vbd - vbd_orig) + CAPcgsb * (vbs - vbs_orig);
+      Qeqqd_Jdxp = -CAPcdgb * (vgb - vgb_orig) - CAPcdgmb * (vgmb - vgmb_orig) +
+                   (CAPcddb + CAPcdbdb) * (vbd - vbd_orig) - CAPcdbdb * (vbd_jct - vbd_jct_orig) +
+                   CAPcdsb * (vbs - vbs_orig);
+      Qeqqb_Jdxp = -CAPcbgb * (vgb - vgb_orig) - CAPcbgmb * (vgmb - vgmb_orig) + CAPcbdb * (vbd - vbd_orig) +
+                   CAPcbsb * (vbs - vbs_orig);
+      if (rgateMod == 3)
+        Qeqqgmid_Jdxp = +CAPcgmdb * (vbd - vbd_orig) + CAPcgmsb * (vbs - vbs_orig) - CAPcgmgmb * (vgmb - vgmb_orig);
+      if (rbodyMod) {
+        Qeqqjs_Jdxp = CAPcsbsb * (vbs_jct - vbs_jct_orig);
+        Qeqqjd_Jdxp = CAPcdbdb * (vbd_jct - vbd_jct_orig);
+      }
+    }
+    const double sgn = dtype > 0 ? 1.0 : -1.0;
+    (void)sgn;
+    double Qeqqg, Qeqqd, Qeqqb, Qeqqgmid = 0.0, Qeqqjs = 0.0, Qeqqjd = 0.0;
+    if (dtype > 0) {
+      Qeqqg = qg;
+      Qeqqd = qd;
+      Qeqqb = qb;
+      if (rbodyMod) {
+        Qeqqjs = qbs;
+        Qeqqjd = qbd;
+      }
+      if (rgateMod == 3) Qeqqgmid = qgmid;
+    } else {
+      Qeqqg = -qg;
+      Qeqqd = -qd;
+      Qeqqb = -qb;
+      if (rbodyMod) {
+        Qeqqjs = -qbs;
+        Qeqqjd = -qbd;
+      }
+      if (rgateMod == 3) Qeqqgmid = -qgmid;
+    }
+    GV(1, g_DP) += -(-Qeqqd) * M;
+    GV(1, g_GP) -= -(Qeqqg) * M;
+    if (rgateMod == 3) GV(1, g_GM) -= -(+Qeqqgmid) * M;
+    if (!rbodyMod) {
+      GV(1, g_BP) += -(-Qeqqb) * M;
+      GV(1, g_SP) += -(+Qeqqg + Qeqqb + Qeqqd + Qeqqgmid) * M;
+    } else {
+      GV(1, g_DB) -= -(Qeqqjd) * M;
+      GV(1, g_BP) += -(-Qeqqb) * M;
+      GV(1, g_SB) -= -(Qeqqjs) * M;
+      GV(1, g_SP) += -(Qeqqd + Qeqqg + Qeqqb + Qeqqjd + Qeqqjs + Qeqqgmid) * M;
+    }
+    if (lim) {
+      GV(3, g_DP) += (-Qeqqd_Jdxp) * M;
+      GV(3, g_GP) -= (Qeqqg_Jdxp) * M;
+      if (rgateMod == 3) GV(3, g_GM) -= (+Qeqqgmid_Jdxp) * M;
+      if (!rbodyMod) {
+        GV(3, g_BP) += (-Qeqqb_Jdxp) * M;
+        GV(3, g_SP) += (+Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqd_Jdxp + Qeqqgmid_Jdxp) * M;
+      } else {
+        GV(3, g_DB) -= (Qeqqjd_Jdxp) * M;
+        GV(3, g_BP) += (-Qeqqb_Jdxp) * M;
+        GV(3, g_SB) -= (+Qeqqjs_Jdxp) * M;
+        GV(3, g_SP) += (+Qeqqd_Jdxp + Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqjd_Jdxp + Qeqqjs_Jdxp + Qeqqgmid_Jdxp) * M;
+      }
+    }
+#undef GV
+    // Master::loadDAEMatrices, pointer form (:16577-16853 and :17102-17172).
+    for (int k = 0; k < kGenSlots; ++k) {
+      o.gf[k] = 0.0;
+      o.gq[k] = 0.0;
+    }
+#define GF(r, c) o.gf[gen_slot(g_##r, g_##c)]
+#define GQ(r, c) o.gq[gen_slot(g_##r, g_##c)]
+    const double gjbd = !rbodyMod ? gbd : 0.0, gjbs = !rbodyMod ? gbs : 0.0;
+    const double gdpr = !rdsMod ? P(drainConductance) : 0.0, gspr = !rdsMod ? P(sourceConductance) : 0.0;
+    const double geltd = P(grgeltd);
+    const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
+    const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
+    const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
+    const double Tq = 0.0;  // qdef * gtau with no NQS charge
+    if (rgateMod == 1) {
+      GF(G, G) += (geltd) * M;
+      GF(G, GP) -= (geltd) * M;
+      GF(GP, G) -= (geltd) * M;
+      GF(GP, GP) += (+geltd - ggtg + gIgtotg) * M;
+      GF(GP, DP) += (-ggtd + gIgtotd) * M;
+      GF(GP, SP) += (-ggts + gIgtots) * M;
+      GF(GP, BP) += (-ggtb + gIgtotb) * M;
+    } else if (rgateMod == 2) {
+      GF(G, G) += (gcrg) * M;
+      GF(G, GP) += (gcrgg) * M;
+      GF(G, DP) += (gcrgd) * M;
+      GF(G, SP) += (gcrgs) * M;
+      GF(G, BP) += (gcrgb) * M;
+      GF(GP, G) -= (gcrg) * M;
+      GF(GP, GP) += (-gcrgg - ggtg + gIgtotg) * M;
+      GF(GP, DP) += (-gcrgd - ggtd + gIgtotd) * M;
+      GF(GP, SP) += (-gcrgs - ggts + gIgtots) * M;
+      GF(GP, BP) += (-gcrgb - ggtb + gIgtotb) * M;
+    } else if (rgateMod == 3) {
+      GF(G, G) += (geltd) * M;
+      GF(G, GM) -= (geltd) * M;
+      GF(GM, G) -= (geltd) * M;
+      GF(GM, GM) += (geltd + gcrg) * M;
+      GF(GM, DP) += (gcrgd) * M;
+      GF(GM, GP) += (gcrgg) * M;
+      GF(GM, SP) += (gcrgs) * M;
+      GF(GM, BP) += (gcrgb) * M;
+      GF(GP, GM) -= (gcrg) * M;
+      GF(GP, GP) += (-gcrgg - ggtg + gIgtotg) * M;
+      GF(GP, DP) += (-gcrgd - ggtd + gIgtotd) * M;
+      GF(GP, SP) += (-gcrgs - ggts + gIgtots) * M;
+      GF(GP, BP) += (-gcrgb - ggtb + gIgtotb) * M;
+    } else {
+      GF(GP, GP) += (-ggtg + gIgtotg) * M;
+      GF(GP, DP) += (-ggtd + gIgtotd) * M;
+      GF(GP, SP) += (-ggts + gIgtots) * M;
+      GF(GP, BP) += (-ggtb + gIgtotb) * M;
+    }
+    if (rdsMod) {
+      GF(D, GP) += (gdtotg) * M;
+      GF(D, SP) += (gdtots) * M;
+      GF(D, BP) += (gdtotb) * M;
+      GF(S, DP) += (gstotd) * M;
+      GF(S, GP) += (gstotg) * M;
+      GF(S, BP) += (gstotb) * M;
+    }
+    GF(DP, DP) += (gdpr + gds + gbd + Tq * ddxpart_dVd - gdtotd + RevSum + gbdpdp + dxpart * ggtd - gIdtotd) * M;
+    GF(DP, D) -= (gdpr + gdtot) * M;
+    GF(DP, GP) += (Gmv - gdtotg + gbdpg - gIdtotg + dxpart * ggtg + Tq * ddxpart_dVg) * M;
+    GF(DP, SP) -= (gds + gdtots - dxpart * ggts + gIdtots - Tq * ddxpart_dVs + FwdSum - gbdpsp) * M;
+    GF(DP, BP) -= (gjbd + gdtotb - Gmbsv - gbdpb + gIdtotb - Tq * ddxpart_dVb - dxpart * ggtb) * M;
+    GF(D, DP) -= (gdpr - gdtotd) * M;
+    GF(D, D) += (gdpr + gdtot) * M;
+    GF(SP, DP) -= (gds + gstotd + RevSum - gbspdp - Tq * dsxpart_dVd - sxpart * ggtd + gIstotd) * M;
+    GF(SP, GP) += (-Gmv - gstotg + gbspg + sxpart * ggtg + Tq * dsxpart_dVg - gIstotg) * M;
+    GF(SP, SP) += (gspr + gds + gbs + Tq * dsxpart_dVs - gstots + FwdSum + gbspsp + sxpart * ggts - gIstots) * M;
+    GF(SP, S) -= (gspr + gstot) * M;
+    GF(SP, BP) -= (gjbs + gstotb + Gmbsv - gbspb - sxpart * ggtb - Tq * dsxpart_dVb + gIstotb) * M;
+    GF(S, SP) -= (gspr - gstots) * M;
+    GF(S, S) += (gspr + gstot) * M;
+    GF(BP, DP) += (-gjbd + gbbdp - gIbtotd) * M;
+    GF(BP, GP) += (-gbgs - gIbtotg) * M;
+    GF(BP, SP) += (-gjbs + gbbsp - gIbtots) * M;
+    GF(BP, BP) += (gjbd + gjbs - gbbs - gIbtotb) * M;
+    GF(DP, DP) += (ggidld) * M;
+    GF(DP, GP) += (ggidlg) * M;
+    GF(DP, SP) -= ((ggidlg + ggidld + ggidlb)) * M;
+    GF(DP, BP) += (ggidlb) * M;
+    GF(BP, DP) -= (ggidld) * M;
+    GF(BP, GP) -= (ggidlg) * M;
+    GF(BP, SP) += ((ggidlg + ggidld + ggidlb)) * M;
+    GF(BP, BP) -= (ggidlb) * M;
+    GF(SP, DP) -= ((ggisls + ggislg + ggislb)) * M;
+    GF(SP, GP) += (ggislg) * M;
+    GF(SP, SP) += (ggisls) * M;
+    GF(SP, BP) += (ggislb) * M;
+    GF(BP, DP) += ((ggislg + ggisls + ggislb)) * M;
+    GF(BP, GP) -= (ggislg) * M;
+    GF(BP, SP) -= (ggisls) * M;
+    GF(BP, BP) -= (ggislb) * M;
+    if (rbodyMod) {
+      GF(DP, DB) += (-gbd) * M;
+      GF(SP, SB) -= (gbs) * M;
+      GF(DB, DP) += (-gbd) * M;
+      GF(DB, DB) += (gbd + P(grbpd) + P(grbdb)) * M;
+      GF(DB, BP) -= (P(grbpd)) * M;
+      GF(DB, B) -= (P(grbdb)) * M;
+      GF(BP, DB) -= (P(grbpd)) * M;
+      GF(BP, B) -= (P(grbpb)) * M;
+      GF(BP, SB) -= (P(grbps)) * M;
+      GF(BP, BP) += (P(grbpd) + P(grbps) + P(grbpb)) * M;
+      GF(SB, SP) += (-gbs) * M;
+      GF(SB, BP) -= (P(grbps)) * M;
+      GF(SB, B) -= (P(grbsb)) * M;
+      GF(SB, SB) += (gbs + P(grbps) + P(grbsb)) * M;
+      GF(B, DB) -= (P(grbdb)) * M;
+      GF(B, BP) -= (P(grbpb)) * M;
+      GF(B, SB) -= (P(grbsb)) * M;
+      GF(B, B) += (P(grbsb) + P(grbdb) + P(grbpb)) * M;
+    }
+    // Initial-condition rows (:16810-16853): the couplings during the operating point, the branch
+    // current's own diagonal (assigned, the row belongs to this instance alone) otherwise.
+    if (P(icVBSGiven) != 0.0) {
+      if (fl.dcop) {
+        GF(B, IBS) += 1.0;
+        GF(S, IBS) += -1.0;
+        GF(IBS, B) += 1.0;
+        GF(IBS, S) += -1.0;
+      } else {
+        GF(IBS, IBS) = 1.0;
+      }
+    }
+    if (P(icVDSGiven) != 0.0) {
+      if (fl.dcop) {
+        GF(D, IDS) += 1.0;
+        GF(S, IDS) += -1.0;
+        GF(IDS, D) += 1.0;
+        GF(IDS, S) += -1.0;
+      } else {
+        GF(IDS, IDS) = 1.0;
+      }
+    }
+    if (P(icVGSGiven) != 0.0) {
+      if (fl.dcop) {
+        GF(G, IGS) += 1.0;
+        GF(S, IGS) += -1.0;
+        GF(IGS, G) += 1.0;
+        GF(IGS, S) += -1.0;
+      } else {
+        GF(IGS, IGS) = 1.0;
+      }
+    }
+    if (!(!fl.dcop && fl.init_tran && fl.newton_iter == 0)) {
+      if (rgateMod == 3) {
+        GQ(GM, GM) += (+CAPcgmgmb) * M;
+        GQ(GM, DP) += (CAPcgmdb) * M;
+        GQ(GM, SP) += (CAPcgmsb) * M;
+        GQ(GM, BP) += (CAPcgmbb) * M;
+        GQ(DP, GM) += (CAPcdgmb) * M;
+        GQ(SP, GM) += (CAPcsgmb) * M;
+        GQ(BP, GM) += (CAPcbgmb) * M;
+      }
+      GQ(GP, GP) += (CAPcggb) * M;
+      GQ(GP, DP) += (CAPcgdb) * M;
+      GQ(GP, SP) += (CAPcgsb) * M;
+      GQ(GP, BP) += (CAPcgbb) * M;
+      GQ(DP, DP) += (CAPcddb) * M;
+      GQ(DP, GP) += (+CAPcdgb) * M;
+      GQ(DP, SP) -= (-CAPcdsb) * M;
+      GQ(DP, BP) -= (-CAPcdbb) * M;
+      GQ(SP, DP) -= (-CAPcsdb) * M;
+      GQ(SP, GP) += (CAPcsgb) * M;
+      GQ(SP, SP) += (CAPcssb) * M;
+      GQ(SP, BP) -= (-CAPcsbb) * M;
+      GQ(BP, DP) += (CAPcbdb) * M;
+      GQ(BP, GP) += (CAPcbgb) * M;
+      GQ(BP, SP) += (CAPcbsb) * M;
+      GQ(BP, BP) += (CAPcbbb) * M;
+      if (rbodyMod) {
+        GQ(DP, DB) += (CAPcdbdb) * M;
+        GQ(SP, SB) -= (-CAPcsbsb) * M;
+        GQ(DB, DP) += (CAPcdbdb) * M;
+        GQ(DB, DB) += (-CAPcdbdb) * M;
+        GQ(SB, SP) += (CAPcsbsb) * M;
+        GQ(SB, SB) += (-CAPcsbsb) * M;
+      }
+    }
+#undef GF
+#undef GQ
+    (void)Vx;
+    return;
   }
 
   // Master::loadDAEVectors (:16316-16564). Local order D, G, S, B.
@@ -1240,12 +1859,15 @@ XD_HD void bsim4_finish(const RV &P_, const double V[4], const LoadFlags &fl, do
 // resistances (rdsMod = 0, sheet resistance) load into vecx / jfx.
 // PART = 0: the whole evaluation; 1: the DC part only, which fills *mid; 2: the charge-and-stamp
 // part only, from *mid (the DC part of the same instance, same inputs).
-template <bool FULL = false, bool SERIES = false, int PART = 0, class RV>
-XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, const LoadFlags &fl, double vgb_orig,
+// GEN = true: the general topology; V holds the 14 local node values, sto_old all 14 store slots,
+// and the outputs go to gv / gf / gq / gsta (the variant is compiled FULL and without SERIES).
+template <bool FULL = false, bool SERIES = false, int PART = 0, bool GEN = false, class RV>
+XD_HD void bsim4_load(const RV &P_, const double *V, const double *sto_old, const LoadFlags &fl, double vgb_orig,
                       LoadOut &o, const double *Vx = nullptr, Mid *mid = nullptr) {
   using namespace xdc;
+  static_assert(!GEN || (FULL && !SERIES), "the general topology is evaluated by the full, non-series load");
   if constexpr (PART == 2) {
-    bsim4_finish<FULL, SERIES>(P_, V, fl, vgb_orig, *mid, o, Vx);
+    bsim4_finish<FULL, SERIES, GEN>(P_, V, fl, vgb_orig, *mid, o, Vx);
     return;
   }
   const double dtype = P(dtype);
@@ -1261,8 +1883,11 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
 
   const bool ChargeComputationNeeded = (fl.tranop || fl.acop || fl.transient);
 
+  const int rgateMod = GEN ? (int)P(rgateMod) : 0;
+  const bool rbodyMod = GEN && P(rbodyMod) != 0.0;
+  const bool rdsMod = GEN && P(rdsMod) != 0.0;
   Bias bias;
-  bsim4_bias<SERIES>(P_, V, fl, Vx, bias);
+  bsim4_bias<SERIES, GEN>(P_, V, fl, Vx, bias);
   const double Vddp = bias.Vddp, Vssp = bias.Vssp;
   (void)Vddp; (void)Vssp;
   double vds = bias.vds, vgs = bias.vgs, vbs = bias.vbs, vges = bias.vges, vgms = bias.vgms, vdbs = bias.vdbs;
@@ -1282,20 +1907,33 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   double vgb = vgb_orig;
   // Previous-iterate voltages for limiting (:8099-8166).
   double vbd_old, vbs_old, vgs_old, vds_old, von_local;
+  double vges_old = 0.0, vgms_old = 0.0, vdes_old = 0.0, vses_old = 0.0, vdbs_old = 0.0, vsbs_old = 0.0;
+  double vdbd_old = 0.0, vged_old = 0.0, vgmd_old = 0.0;
   if (fl.newton_iter == 0 && fl.dcop) {
     vbd_old = vbd;
     vbs_old = vbs;
     vgs_old = vgs;
     vds_old = vds;
     von_local = 0.0;
+    if (GEN) {
+      vges_old = vges; vgms_old = vgms; vdes_old = vdes; vses_old = vses; vdbs_old = vdbs; vsbs_old = vsbs;
+      vdbd_old = vdbd; vged_old = vged; vgmd_old = vgmd;
+    }
   } else {
     vbd_old = sto_old[s_vbd];
     vbs_old = sto_old[s_vbs];
     vgs_old = sto_old[s_vgs];
     vds_old = sto_old[s_vds];
     von_local = sto_old[s_von];
+    if (GEN) {
+      // vged / vgmd are never written by the load: their "old" values are whatever the store holds.
+      vges_old = sto_old[s_vges]; vgms_old = sto_old[s_vgms]; vdes_old = sto_old[s_vdes];
+      vses_old = sto_old[s_vses]; vdbs_old = sto_old[s_vdbs]; vsbs_old = sto_old[s_vsbs];
+      vdbd_old = sto_old[s_vdbd]; vged_old = sto_old[s_vged]; vgmd_old = sto_old[s_vgmd];
+    }
   }
   const double vgd_old = vgs_old - vds_old;
+  (void)vdbd_old;
 
   if (fl.voltlim && !(fl.init_fix && OFF)) {
     int Check = 0;
@@ -1305,18 +1943,62 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
         vds = vgs - vgd;
         vds = limvds(vds, vds_old);
         vgd = vgs - vds;
+        if (GEN) {
+          if (rgateMod == 3) {
+            vges = fetlim(vges, vges_old, von_local);
+            vgms = fetlim(vgms, vgms_old, von_local);
+          } else if ((rgateMod == 1) || (rgateMod == 2)) {
+            vges = fetlim(vges, vges_old, von_local);
+            vged = vges - vds;
+          }
+          if (rdsMod) {
+            vdes = limvds(vdes, vdes_old);
+            vses = -limvds(-vses, -vses_old);
+          }
+        }
       } else {
         vgd = fetlim(vgd, vgd_old, von_local);
         vds = vgs - vgd;
         vds = -limvds(-vds, -vds_old);
         vgs = vgd + vds;
+        if (GEN) {
+          if (rgateMod == 3) {
+            vged = fetlim(vged, vged_old, von_local);
+            vges = vged + vds;
+            vgmd = fetlim(vgmd, vgmd_old, von_local);
+            vgms = vgmd + vds;
+          }
+          if ((rgateMod == 1) || (rgateMod == 2)) {
+            vged = fetlim(vged, vged_old, von_local);
+            vges = vged + vds;
+          }
+          if (rdsMod) {
+            vdes = -limvds(-vdes, -vdes_old);
+            vses = limvds(vses, vses_old);
+          }
+        }
       }
       if (vds >= 0.0) {
         vbs = pnjlim(vbs, vbs_old, CONSTvt0, P(vcrit), &Check);
         vbd = vbs - vds;
+        if (rbodyMod) {
+          int Check1 = 0, Check2 = 0;
+          vdbs = pnjlim(vdbs, vdbs_old, CONSTvt0, P(vcrit), &Check1);
+          vdbd = vdbs - vds;
+          vsbs = pnjlim(vsbs, vsbs_old, CONSTvt0, P(vcrit), &Check2);
+        }
       } else {
         vbd = pnjlim(vbd, vbd_old, CONSTvt0, P(vcrit), &Check);
         vbs = vbd + vds;
+        if (rbodyMod) {
+          int Check1 = 0, Check2 = 0;
+          vdbd = pnjlim(vdbd, vdbd_old, CONSTvt0, P(vcrit), &Check1);
+          vdbs = vdbd + vds;
+          const double vsbd_old = vsbs_old - vds_old;
+          double vsbd = vsbs - vds;
+          vsbd = pnjlim(vsbd, vsbd_old, CONSTvt0, P(vcrit), &Check2);
+          vsbs = vsbd + vds;
+        }
       }
     }
     (void)Check;
@@ -1338,8 +2020,8 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   vgmd = vgms - vds;
   vgmb = vgms - vbs;
   vdbd = vdbs - vds;
-  vbs_jct = vbs;
-  vbd_jct = vbd;
+  vbs_jct = (!rbodyMod) ? vbs : vsbs;
+  vbd_jct = (!rbodyMod) ? vbd : vdbd;
 
   double T0, T1, T2, T3, T4, T5, T6, T7, T8, T9, T10, T11, T12, T13, T14;
   double dT0_dVg, dT0_dVd, dT0_dVb, dT1_dVg, dT1_dVd, dT1_dVb, dT2_dVg, dT2_dVd, dT2_dVb;
@@ -1815,7 +2497,9 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     dWeff_dVb *= T0;
   }
   double Rds, dRds_dVg, dRds_dVb;
-  {
+  if (rdsMod) {
+    Rds = dRds_dVg = dRds_dVb = 0.0;
+  } else {
     T0 = 1.0 + P(prwg) * Vgsteff;
     dT0_dVg = -P(prwg) / T0 / T0;
     T1 = P(prwb) * T9;
@@ -2410,7 +3094,102 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
   }
   double gds = Gds, gm = Gm, gmbs = Gmb;
 
-  // GIDL and GISL (:10063-10180). vgs_eff / vgd_eff here are the poly-depleted gate voltages.
+  // Gate resistance conductance for rgateMod 2 / 3 (:9954-9989; NQS, the other user, is refused).
+  double gcrg = 0.0, gcrgg = 0.0, gcrgd = 0.0, gcrgs = 0.0, gcrgb = 0.0;
+  if (GEN && rgateMod > 1) {
+    T9 = P(xrcrg2) * P(vtm);
+    T0 = T9 * beta;
+    dT0_dVd = (dbeta_dVd + dbeta_dVg * dVgsteff_dVd) * T9;
+    dT0_dVb = (dbeta_dVb + dbeta_dVg * dVgsteff_dVb) * T9;
+    dT0_dVg = dbeta_dVg * T9;
+    gcrg = P(xrcrg1) * (T0 + Ids);
+    gcrgd = P(xrcrg1) * (dT0_dVd + tmp1);
+    gcrgb = P(xrcrg1) * (dT0_dVb + tmp2) * dVbseff_dVb;
+    gcrgg = P(xrcrg1) * (dT0_dVg + tmp3) * dVgsteff_dVg;
+    if (nf != 1.0) {
+      gcrg *= nf;
+      gcrgg *= nf;
+      gcrgd *= nf;
+      gcrgb *= nf;
+    }
+    if (rgateMod == 2) {
+      T10 = P(grgeltd) * P(grgeltd);
+      T11 = P(grgeltd) + gcrg;
+      gcrg = P(grgeltd) * gcrg / T11;
+      T12 = T10 / T11 / T11;
+      gcrgg *= T12;
+      gcrgd *= T12;
+      gcrgb *= T12;
+    }
+    gcrgs = -(gcrgg + gcrgd + gcrgb);
+  }
+  // Bias-dependent external source / drain resistance, rdsMod = 1 (:9991-10061). It replaces the
+  // poly-depleted vgs_eff / vgd_eff that GIDL / GISL read below with the S/D-resistance ones, as the
+  // reference's shared members do.
+  double gstot = 0.0, gstotd = 0.0, gstotg = 0.0, gstots = 0.0, gstotb = 0.0;
+  double gdtot = 0.0, gdtotd = 0.0, gdtotg = 0.0, gdtots = 0.0, gdtotb = 0.0;
+  if (rdsMod) {
+    T0 = vgs - P(vfbsd);
+    T1 = sqrt(T0 * T0 + 1.0e-4);
+    vgs_eff = 0.5 * (T0 + T1);
+    dvgs_eff_dvg = vgs_eff / T1;
+    T0 = 1.0 + P(prwg) * vgs_eff;
+    double dT0_dvg = -P(prwg) / T0 / T0 * dvgs_eff_dvg;
+    T1 = -P(prwb) * vbs;
+    double dT1_dvb = -P(prwb);
+    T2 = 1.0 / T0 + T1;
+    T3 = T2 + sqrt(T2 * T2 + 0.01);
+    double dT3_dvg = T3 / (T3 - T2);
+    double dT3_dvb = dT3_dvg * dT1_dvb;
+    dT3_dvg *= dT0_dvg;
+    T4 = P(rs0) * 0.5;
+    const double Rs = P(rswmin) + T3 * T4;
+    const double dRs_dvg = T4 * dT3_dvg;
+    const double dRs_dvb = T4 * dT3_dvb;
+    T0 = 1.0 + P(sourceConductance) * Rs;
+    gstot = P(sourceConductance) / T0;
+    T0 = -gstot * gstot;
+    const double dgstot_dvd = 0.0;
+    const double dgstot_dvg = T0 * dRs_dvg;
+    const double dgstot_dvb = T0 * dRs_dvb;
+    const double dgstot_dvs = -(dgstot_dvg + dgstot_dvb + dgstot_dvd);
+    T0 = vgd - P(vfbsd);
+    T1 = sqrt(T0 * T0 + 1.0e-4);
+    vgd_eff = 0.5 * (T0 + T1);
+    dvgd_eff_dvg = vgd_eff / T1;
+    T0 = 1.0 + P(prwg) * vgd_eff;
+    dT0_dvg = -P(prwg) / T0 / T0 * dvgd_eff_dvg;
+    T1 = -P(prwb) * vbd;
+    dT1_dvb = -P(prwb);
+    T2 = 1.0 / T0 + T1;
+    T3 = T2 + sqrt(T2 * T2 + 0.01);
+    dT3_dvg = T3 / (T3 - T2);
+    dT3_dvb = dT3_dvg * dT1_dvb;
+    dT3_dvg *= dT0_dvg;
+    T4 = P(rd0) * 0.5;
+    const double Rd = P(rdwmin) + T3 * T4;
+    const double dRd_dvg = T4 * dT3_dvg;
+    const double dRd_dvb = T4 * dT3_dvb;
+    T0 = 1.0 + P(drainConductance) * Rd;
+    gdtot = P(drainConductance) / T0;
+    T0 = -gdtot * gdtot;
+    const double dgdtot_dvs = 0.0;
+    const double dgdtot_dvg = T0 * dRd_dvg;
+    const double dgdtot_dvb = T0 * dRd_dvb;
+    const double dgdtot_dvd = -(dgdtot_dvg + dgdtot_dvb + dgdtot_dvs);
+    gstotd = vses * dgstot_dvd;
+    gstotg = vses * dgstot_dvg;
+    gstots = vses * dgstot_dvs;
+    gstotb = vses * dgstot_dvb;
+    T2 = vdes - vds;
+    gdtotd = T2 * dgdtot_dvd;
+    gdtotg = T2 * dgdtot_dvg;
+    gdtots = T2 * dgdtot_dvs;
+    gdtotb = T2 * dgdtot_dvb;
+  }
+
+  // GIDL and GISL (:10063-10180). vgs_eff / vgd_eff here are the poly-depleted gate voltages
+  // (rdsMod 0) or the S/D-resistance ones (rdsMod 1).
   T0 = 3.0 * toxe;
   T1 = (vds - vgs_eff - P(egidl)) / T0;
   double Igidl, Ggidld, Ggidlg, Ggidlb;
@@ -2866,12 +3645,35 @@ XD_HD void bsim4_load(const RV &P_, const double V[4], const double *sto_old, co
     hm.v[m_gIgbd] = gIgbd;
     hm.v[m_gIgbb] = gIgbb;
   }
+  if constexpr (GEN) {
+    hm.v[m_vges] = vges;
+    hm.v[m_vgms] = vgms;
+    hm.v[m_vdes] = vdes;
+    hm.v[m_vses] = vses;
+    hm.v[m_vdbs] = vdbs;
+    hm.v[m_vsbs] = vsbs;
+    hm.v[m_gcrg] = gcrg;
+    hm.v[m_gcrgg] = gcrgg;
+    hm.v[m_gcrgd] = gcrgd;
+    hm.v[m_gcrgs] = gcrgs;
+    hm.v[m_gcrgb] = gcrgb;
+    hm.v[m_gstot] = gstot;
+    hm.v[m_gstotd] = gstotd;
+    hm.v[m_gstotg] = gstotg;
+    hm.v[m_gstots] = gstots;
+    hm.v[m_gstotb] = gstotb;
+    hm.v[m_gdtot] = gdtot;
+    hm.v[m_gdtotd] = gdtotd;
+    hm.v[m_gdtotg] = gdtotg;
+    hm.v[m_gdtots] = gdtots;
+    hm.v[m_gdtotb] = gdtotb;
+  }
   (void)gIgbs; (void)gIgcss; (void)gIgcds;
   if constexpr (PART == 1) {
     *mid = hm;
     return;
   }
-  bsim4_finish<FULL, SERIES>(P_, V, fl, vgb_orig, hm, o, Vx);
+  bsim4_finish<FULL, SERIES, GEN>(P_, V, fl, vgb_orig, hm, o, Vx);
 }
 #undef P
 

@@ -45,7 +45,10 @@
   F(vjdmFwd) F(vjdmRev) F(IVjsmFwd) F(IVjsmRev) F(IVjdmFwd) F(IVjdmRev) F(SslpFwd) F(SslpRev)     \
   F(DslpFwd) F(DslpRev) F(SjctTempRevSatCur) F(SswTempRevSatCur) F(SswgTempRevSatCur)            \
   F(DjctTempRevSatCur) F(DswTempRevSatCur) F(DswgTempRevSatCur) F(drainConductance)              \
-  F(sourceConductance) F(grgeltd) F(temp) F(off) F(dExists) F(sExists)
+  F(sourceConductance) F(grgeltd) F(temp) F(off) F(dExists) F(sExists)                           \
+  /* general topology: gate / body resistance modes, rdsMod 1 S/D resistance, body network */    \
+  F(rgateMod) F(rbodyMod) F(rd0) F(rdwmin) F(rs0) F(rswmin) F(grbpd) F(grbps) F(grbpb) F(grbsb)   \
+  F(grbdb) F(icVBS) F(icVDS) F(icVGS) F(icVBSGiven) F(icVDSGiven) F(icVGSGiven)
 
 namespace xb4 {
 enum Field {

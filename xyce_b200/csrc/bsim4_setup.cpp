@@ -95,7 +95,7 @@ struct InstParams {
   double drainArea = 0, sourceArea = 0, drainPerimeter = 0, sourcePerimeter = 0, drainSquares = 1.0,
          sourceSquares = 1.0, rbdb = 0, rbsb = 0, rbpb = 0, rbps = 0, rbpd = 0, delvto = 0, xgw = 0, ngcon = 0,
          mult = 1.0, off = 0, trnqsMod = 0, acnqsMod = 0, rbodyMod = 0, rgateMod = 0, geoMod = 0, rgeoMod = 0,
-         min = 0;
+         min = 0, icVDS = 0, icVGS = 0, icVBS = 0;
   std::set<std::string> given;
   bool g(const char *n) const { return given.count(n) != 0; }
 };
@@ -237,11 +237,11 @@ std::string process_model(const ModelSpec &spec, const SetupOptions &opts, Card 
 
   // Features outside the load kernel's scope are refused here rather than mis-evaluated.
   if (m.mtrlMod != 0) return "BSIM4 mtrlMod != 0 is not supported";
-  if (m.rdsMod != 0) return "BSIM4 rdsMod != 0 is not supported";
+  if (m.rdsMod != 0 && m.rdsMod != 1) return "BSIM4 rdsMod must be 0 or 1";
   if (m.igcMod < 0 || m.igcMod > 2) return "BSIM4 igcMod must be 0, 1 or 2";
   if (m.igbMod < 0 || m.igbMod > 1) return "BSIM4 igbMod must be 0 or 1";
-  if (m.rgateMod != 0) return "BSIM4 rgateMod != 0 is not supported";
-  if (m.rbodyMod != 0) return "BSIM4 rbodyMod != 0 is not supported";
+  if (m.rgateMod < 0 || m.rgateMod > 3 || m.rgateMod != (int)m.rgateMod) return "BSIM4 rgateMod must be 0, 1, 2 or 3";
+  if (m.rbodyMod < 0 || m.rbodyMod > 2 || m.rbodyMod != (int)m.rbodyMod) return "BSIM4 rbodyMod must be 0, 1 or 2";
   if (m.trnqsMod != 0 || m.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
   if (m.capMod < 0 || m.capMod > 2) return "BSIM4 capMod must be 0, 1 or 2";
   if (m.dioMod < 0 || m.dioMod > 2) return "BSIM4 dioMod must be 0, 1 or 2";
@@ -693,24 +693,31 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   InstParams ip = ipin;
   Card &m = ms.c;
   // Instance::Instance defaults for parameters not given on the instance line.
+  if (!ip.g("RBDB")) ip.rbdb = m.rbdb;
+  if (!ip.g("RBSB")) ip.rbsb = m.rbsb;
+  if (!ip.g("RBPB")) ip.rbpb = m.rbpb;
+  if (!ip.g("RBPS")) ip.rbps = m.rbps;
+  if (!ip.g("RBPD")) ip.rbpd = m.rbpd;
   if (!ip.g("XGW")) ip.xgw = m.xgw;
   if (!ip.g("NGCON")) ip.ngcon = m.ngcon;
   if (!ip.g("SD")) ip.sd = 2.0 * m.dmcg;
   if (!ip.g("TEMP")) ip.temp = opts.temp_c + CONSTCtoK;
   if (!ip.g("AD")) ip.drainArea = 0.0;
   if (!ip.g("AS")) ip.sourceArea = 0.0;
-  // Instance::processParams mode selection.
-  if (!ip.g("RBODYMOD")) ip.rbodyMod = m.rbodyMod;
-  if (!ip.g("RGATEMOD")) ip.rgateMod = m.rgateMod;
+  // Instance::processParams mode selection (:3618-3672): an instance value outside the range falls
+  // back to the model's.
+  if (!ip.g("RBODYMOD") || (ip.rbodyMod != 0 && ip.rbodyMod != 1 && ip.rbodyMod != 2)) ip.rbodyMod = m.rbodyMod;
+  if (!ip.g("RGATEMOD") || (ip.rgateMod != 0 && ip.rgateMod != 1 && ip.rgateMod != 2 && ip.rgateMod != 3))
+    ip.rgateMod = m.rgateMod;
   if (!ip.g("GEOMOD")) ip.geoMod = m.geoMod;
   if (!ip.g("RGEOMOD")) ip.rgeoMod = 0;
-  if (!ip.g("TRNQSMOD")) ip.trnqsMod = m.trnqsMod;
-  if (!ip.g("ACNQSMOD")) ip.acnqsMod = m.acnqsMod;
-  if (ip.rbodyMod != 0 || ip.rgateMod != 0 || ip.trnqsMod != 0 || ip.acnqsMod != 0)
-    return "BSIM4 instance rbodyMod/rgateMod/trnqsMod/acnqsMod != 0 is not supported";
-  if (ip.rgeoMod != 0 && m.sheetResistance > 0.0)
-    return "BSIM4 rgeoMod != 0 with RSH > 0 (geometry-derived source/drain resistance) is not supported";
-  if (ip.g("IC1") || ip.g("IC2") || ip.g("IC3")) return "BSIM4 instance initial conditions are not supported";
+  if (!ip.g("TRNQSMOD") || (ip.trnqsMod != 0 && ip.trnqsMod != 1)) ip.trnqsMod = m.trnqsMod;
+  if (!ip.g("ACNQSMOD") || (ip.acnqsMod != 0 && ip.acnqsMod != 1)) ip.acnqsMod = m.acnqsMod;
+  if (ip.trnqsMod != 0 || ip.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
+  // Geometry-derived source / drain resistance (RdseffGeo) applies where a sheet resistance or
+  // rdsMod asks for a resistance and the instance gives no squares.
+  if (ip.rgeoMod != 0 && (m.sheetResistance > 0.0 || m.rdsMod != 0) && (!ip.g("NRD") || !ip.g("NRS")))
+    return "BSIM4 rgeoMod != 0 without NRD / NRS (geometry-derived source/drain resistance) is not supported";
   const double temp = ip.temp;
   if (!ms.temp_done) {
     model_temperature(ms, temp);
@@ -806,6 +813,55 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   if (vbsc > p.vbm) vbsc = p.vbm;
   const double k2ox = k2 * toxe / m.toxm;
   const double vfbzb = p.vfbzbfactor + m.dtype * vth0;
+  // Body resistance network (:7218-7309): rbodyMod 2 scales the resistances with geometry; the
+  // conductances get gbmin added, and a resistance below 1 mOhm becomes 1e3 S.
+  double rbdb = ip.rbdb, rbsb = ip.rbsb, rbpb = ip.rbpb, rbps = ip.rbps, rbpd = ip.rbpd;
+  double grbdb = 0.0, grbpb = 0.0, grbps = 0.0, grbsb = 0.0, grbpd = 0.0;
+  {
+    const double lnl = log(p.leff * 1.0e6);
+    const double lnw = log(p.weff * 1.0e6);
+    const double lnnf = log(nf);
+    int bodymode = 5;
+    if ((!m.g("RBPS0")) || (!m.g("RBPD0")))
+      bodymode = 1;
+    else if ((!m.g("RBSBX0") && !m.g("RBSBY0")) || (!m.g("RBDBX0") && !m.g("RBDBY0")))
+      bodymode = 3;
+    if (ip.rbodyMod == 2) {
+      if (bodymode == 5) {
+        const double rbsbx = exp(log(m.rbsbx0) + m.rbsdbxl * lnl + m.rbsdbxw * lnw + m.rbsdbxnf * lnnf);
+        const double rbsby = exp(log(m.rbsby0) + m.rbsdbyl * lnl + m.rbsdbyw * lnw + m.rbsdbynf * lnnf);
+        rbsb = rbsbx * rbsby / (rbsbx + rbsby);
+        const double rbdbx = exp(log(m.rbdbx0) + m.rbsdbxl * lnl + m.rbsdbxw * lnw + m.rbsdbxnf * lnnf);
+        const double rbdby = exp(log(m.rbdby0) + m.rbsdbyl * lnl + m.rbsdbyw * lnw + m.rbsdbynf * lnnf);
+        rbdb = rbdbx * rbdby / (rbdbx + rbdby);
+      }
+      if ((bodymode == 3) || (bodymode == 5)) {
+        rbps = exp(log(m.rbps0) + m.rbpsl * lnl + m.rbpsw * lnw + m.rbpsnf * lnnf);
+        rbpd = exp(log(m.rbpd0) + m.rbpdl * lnl + m.rbpdw * lnw + m.rbpdnf * lnnf);
+      }
+      const double rbpbx = exp(log(m.rbpbx0) + m.rbpbxl * lnl + m.rbpbxw * lnw + m.rbpbxnf * lnnf);
+      const double rbpby = exp(log(m.rbpby0) + m.rbpbyl * lnl + m.rbpbyw * lnw + m.rbpbynf * lnnf);
+      rbpb = rbpbx * rbpby / (rbpbx + rbpby);
+    }
+    if ((ip.rbodyMod == 1) || ((ip.rbodyMod == 2) && (bodymode == 5))) {
+      grbdb = (rbdb < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbdb;
+      grbpb = (rbpb < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbpb;
+      grbps = (rbps < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbps;
+      grbsb = (rbsb < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbsb;
+      grbpd = (rbpd < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbpd;
+    }
+    if ((ip.rbodyMod == 2) && (bodymode == 3)) {
+      grbdb = grbsb = m.gbmin;
+      grbpb = (rbpb < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbpb;
+      grbps = (rbps < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbps;
+      grbpd = (rbpd < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbpd;
+    }
+    if ((ip.rbodyMod == 2) && (bodymode == 1)) {
+      grbdb = grbsb = m.gbmin;
+      grbps = grbpd = 1.0e3;
+      grbpb = (rbpb < 1.0e-3) ? 1.0e3 : m.gbmin + 1.0 / rbpb;
+    }
+  }
   double grgeltd = m.rshg * (ip.xgw + p.weffCJ / 3.0 / ip.ngcon) / (ip.ngcon * nf * (Lnew - m.xgl));
   if (grgeltd > 0.0)
     grgeltd = 1.0 / grgeltd;
@@ -840,20 +896,20 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
     Adeff = ip.drainArea;
   else
     pa_eff_geo(nf, geoMod, minSD, p.weffCJ, DMCGeff, DMCIeff, DMDGeff, dumPs, dumPd, dumAs, Adeff);
-  // Source / drain series resistance, rdsMod = 0 (:7378-7447): sheet resistance times the given
-  // number of squares; a zero product is replaced by 1e3 S. The internal node exists when the
-  // sheet resistance and the squares are both positive (:3684-3745).
+  // Source / drain series resistance (:7378-7447): sheet resistance times the given number of
+  // squares; no squares (rdsMod 1) or a zero product give 1e3 S. The internal node exists with
+  // rdsMod 1, or when the sheet resistance and the squares are both positive (:3684-3760).
   double sourceConductance = 0.0, drainConductance = 0.0;
-  if (ip.g("NRS")) {
-    sourceConductance = m.sheetResistance * ip.sourceSquares;
+  if (m.rdsMod != 0 || ip.g("NRS")) {
+    sourceConductance = ip.g("NRS") ? m.sheetResistance * ip.sourceSquares : 0.0;
     sourceConductance = (sourceConductance > 0.0) ? 1.0 / sourceConductance : 1.0e3;
   }
-  if (ip.g("NRD")) {
-    drainConductance = m.sheetResistance * ip.drainSquares;
+  if (m.rdsMod != 0 || ip.g("NRD")) {
+    drainConductance = ip.g("NRD") ? m.sheetResistance * ip.drainSquares : 0.0;
     drainConductance = (drainConductance > 0.0) ? 1.0 / drainConductance : 1.0e3;
   }
-  const bool dExists = m.sheetResistance > 0.0 && ip.g("NRD") && ip.drainSquares > 0.0;
-  const bool sExists = m.sheetResistance > 0.0 && ip.g("NRS") && ip.sourceSquares > 0.0;
+  const bool dExists = m.rdsMod != 0 || (m.sheetResistance > 0.0 && ip.g("NRD") && ip.drainSquares > 0.0);
+  const bool sExists = m.rdsMod != 0 || (m.sheetResistance > 0.0 && ip.g("NRS") && ip.sourceSquares > 0.0);
   double XExpBVS = 0, XExpBVD = 0, vjsmFwd = 0, vjsmRev = 0, vjdmFwd = 0, vjdmRev = 0;
   double IVjsmFwd = 0, IVjsmRev = 0, IVjdmFwd = 0, IVjdmRev = 0, SslpFwd = 0, SslpRev = 0, DslpFwd = 0, DslpRev = 0;
   const double Nvtms = ms.vtm * m.SjctEmissionCoeff;
@@ -1030,6 +1086,11 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   R(DswTempRevSatCur) = DswTempRevSatCur; R(DswgTempRevSatCur) = DswgTempRevSatCur;
   R(drainConductance) = drainConductance; R(sourceConductance) = sourceConductance; R(grgeltd) = grgeltd;
   R(dExists) = dExists ? 1.0 : 0.0; R(sExists) = sExists ? 1.0 : 0.0;
+  R(rgateMod) = ip.rgateMod; R(rbodyMod) = ip.rbodyMod; R(rd0) = p.rd0; R(rdwmin) = p.rdwmin; R(rs0) = p.rs0;
+  R(rswmin) = p.rswmin; R(grbpd) = grbpd; R(grbps) = grbps; R(grbpb) = grbpb; R(grbsb) = grbsb; R(grbdb) = grbdb;
+  R(icVBS) = ip.icVBS; R(icVDS) = ip.icVDS; R(icVGS) = ip.icVGS;
+  R(icVBSGiven) = ip.g("IC3") ? 1.0 : 0.0; R(icVDSGiven) = ip.g("IC1") ? 1.0 : 0.0;
+  R(icVGSGiven) = ip.g("IC2") ? 1.0 : 0.0;
   R(temp) = temp; R(off) = ip.off;
 #undef R
   return std::string();
@@ -1048,7 +1109,9 @@ bool set_inst_param(InstParams &ip, const std::string &name, double v) {
       {"M", &InstParams::mult}, {"TRNQSMOD", &InstParams::trnqsMod}, {"ACNQSMOD", &InstParams::acnqsMod},
       {"RBODYMOD", &InstParams::rbodyMod}, {"RGATEMOD", &InstParams::rgateMod}, {"GEOMOD", &InstParams::geoMod},
       {"RGEOMOD", &InstParams::rgeoMod}, {"MIN", &InstParams::min}, {"OFF", &InstParams::off}};
+  // The instance's initial conditions IC = (VDS, VGS, VBS) (:266-315).
   if (name == "IC1" || name == "IC2" || name == "IC3") {
+    (name == "IC1" ? ip.icVDS : name == "IC2" ? ip.icVGS : ip.icVBS) = v;
     ip.given.insert(name);
     return true;
   }

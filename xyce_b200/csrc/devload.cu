@@ -108,6 +108,12 @@ struct xd_ctx {
   // Hand-off state between the two kernels of a split evaluation (kNumMid slots per instance,
   // slot-major); allocated for the BSIM4 families the split launch shapes evaluate.
   double *d_mid = nullptr;
+  // General topology (BSIM4 gate / body resistance, rdsMod 1, instance initial conditions): each
+  // instance's 14 local nodes as unknowns (slot-major [node * n + i]; collapsed nodes carry their
+  // representative's unknown, ground and absent branch currents -1), 14 vector rows and 77 matrix
+  // slots of staging, and 6 state slots per instance.
+  bool gen = false;
+  int *d_gmap = nullptr;
 };
 
 namespace {
@@ -245,6 +251,48 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_charge_stamp_kernel(
   xb4::LoadOut o;
   xb4::bsim4_load<FULL, SERIES, 2>(rp, V, nullptr, fl, vgb[i], o, Vx, &m);
   bsim4_write_one<SERIES>(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
+}
+
+// General topology: one thread per instance over the 14 local nodes; the full store block is read
+// (the limiters of the gate, source / drain and body-network voltages compare against it) and the
+// six state slots written.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
+    double *__restrict__ stage, xb4::LoadFlags fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[xb4::kGenNodes], sto_old[xb4::kNumStore];
+#pragma unroll
+  for (int k = 0; k < xb4::kGenNodes; ++k) {
+    const int u = gmap[(size_t)k * n + i];
+    V[k] = u >= 0 ? sol[u] : 0.0;
+  }
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load<true, false, 0, true>(rp, V, sto_old, fl, vgb[i], o);
+#pragma unroll
+  for (int k = 0; k < 4 * xb4::kGenNodes; ++k) stage[(size_t)k * n + i] = o.gv[k];
+  const size_t mf = 4 * xb4::kGenNodes, mq = mf + xb4::kGenSlots;
+#pragma unroll
+  for (int k = 0; k < xb4::kGenSlots; ++k) stage[(mf + k) * n + i] = o.gf[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kGenSlots; ++k) stage[(mq + k) * n + i] = o.gq[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k)
+    if (k != xb4::s_vged && k != xb4::s_vgmd) next_sto[(size_t)k * n + i] = o.sto[k];
+#pragma unroll
+  for (int k = 0; k < xb4::kGenState; ++k) next_sta[(size_t)k * n + i] = o.gsta[k];
+  if (o.write_curr_sta) {
+#pragma unroll
+    for (int k = 0; k < xb4::kGenState; ++k) curr_sta[(size_t)k * n + i] = o.gsta[k];
+  }
+  vgb[i] = o.vgb;
 }
 
 // One thread per instance. PERSIST: the grid is one wave of resident blocks that walks the
@@ -623,6 +671,7 @@ struct EvalVariant {
   bool persist;  // one wave of resident blocks with a grid-stride loop
   bool split;    // two kernels: the DC part (min_blocks), then charges and stamps (min_blocks2)
   int min_blocks2;
+  bool gen;      // BSIM4 general topology (14 local nodes, 77 stamp slots)
 };
 constexpr int B4 = 4, B3 = 3, M1 = 1;  // kFamilyBsim4, kFamilyBsim3, kFamilyMos1
 constexpr EvalVariant kEvalVariants[] = {
@@ -637,8 +686,10 @@ constexpr EvalVariant kEvalVariants[] = {
     {B3, 128, 1, false, false, false, false, 0}, {B3, 128, 2, false, false, false, false, 0},
     {B3, 128, 3, false, false, false, false, 0}, {B3, 64, 4, false, false, false, false, 0},
     {M1, 128, 1, false, false, false, false, 0}, {M1, 128, 4, false, false, false, false, 0},
-    {M1, 256, 2, false, false, false, false, 0}, {M1, 64, 8, false, false, false, false, 0}};
+    {M1, 256, 2, false, false, false, false, 0}, {M1, 64, 8, false, false, false, false, 0},
+    {B4, 128, 1, true, false, false, false, 0, true}, {B4, 128, 2, true, false, false, false, 0, true}};
 constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8, kFirstBsim3Variant = 16, kFirstMos1Variant = 20;
+constexpr int kFirstGenVariant = 24;
 // A variant computes a context's loads exactly if it is for the context's family and, for BSIM4, its
 // staging layout is the context's and it is a full one or the context's cards use only the common
 // options; a split one also needs the context's hand-off buffer.
@@ -646,6 +697,7 @@ bool variant_fits(const xd_ctx *ctx, int v) {
   const EvalVariant &e = kEvalVariants[v];
   if (e.family != ctx->family) return false;
   if (ctx->family != kFamilyBsim4) return true;
+  if (e.gen || ctx->gen) return e.gen == ctx->gen;
   return e.series == ctx->series && (e.full || !ctx->needs_full) && (!e.split || ctx->d_mid != nullptr);
 }
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
@@ -720,6 +772,16 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
   }
   const int blk = kEvalVariants[v].block;
   int grid = (n + blk - 1) / blk;
+  if (kEvalVariants[v].gen) {
+#define XD_GEN_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_gmap, sol, next_sta, curr_sta, next_sto, curr_sto, \
+                    ctx->d_vgb, stage, fl
+    if (v == kFirstGenVariant)
+      bsim4_gen_kernel<128, 1><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
+    else
+      bsim4_gen_kernel<128, 2><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
+#undef XD_GEN_ARGS
+    return;
+  }
   if (kEvalVariants[v].persist) grid = std::max(1, std::min(grid, ctx->resident_blocks[v]));
   if (kEvalVariants[v].split) {
 #define XD_DC_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_nodes, sol, next_sto, curr_sto, ctx->d_vgb, fl, ctx->d_ext, \
@@ -788,18 +850,56 @@ void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned
   }
 }
 
+// General topology, per instance: which of the internal variables (D', S', G', GM, B', SB, DB and the
+// three initial-condition branch currents, registerLIDs order) it has (:3684-3769, 4996-5075).
+constexpr int kGenInternal = XD_GEN_INTERNAL;
+static_assert(kGenInternal == xb4::kGenNodes - 4, "the internal variables are the local nodes after D, G, S, B");
+void gen_flags(const xb4::RecordTable &rt, std::vector<unsigned char> &flags) {
+  const size_t nr = (size_t)rt.n_records, n = rt.inst_rec.size();
+  flags.assign((size_t)kGenInternal * n, 0);
+  auto f = [&](xb4::Field fld, size_t r) { return rt.tab[(size_t)fld * nr + r]; };
+  for (size_t i = 0; i < n; ++i) {
+    const size_t r = (size_t)rt.inst_rec[i];
+    const int rg = (int)f(xb4::f_rgateMod, r);
+    const bool rb = f(xb4::f_rbodyMod, r) != 0.0;
+    unsigned char *fl = &flags[(size_t)kGenInternal * i];
+    fl[0] = f(xb4::f_dExists, r) != 0.0;
+    fl[1] = f(xb4::f_sExists, r) != 0.0;
+    fl[2] = rg > 0;
+    fl[3] = rg == 3;
+    fl[4] = fl[5] = fl[6] = rb;
+    fl[7] = f(xb4::f_icVBSGiven, r) != 0.0;
+    fl[8] = f(xb4::f_icVDSGiven, r) != 0.0;
+    fl[9] = f(xb4::f_icVGSGiven, r) != 0.0;
+  }
+}
+// A BSIM4 family needs the general topology when a record uses gate or body resistance, rdsMod 1 or
+// an instance initial condition.
+bool family_needs_gen(const xb4::RecordTable &rt) {
+  const size_t nr = (size_t)rt.n_records;
+  auto f = [&](xb4::Field fld, size_t r) { return rt.tab[(size_t)fld * nr + r]; };
+  for (size_t r = 0; r < nr; ++r)
+    if (f(xb4::f_rgateMod, r) != 0.0 || f(xb4::f_rbodyMod, r) != 0.0 || f(xb4::f_rdsMod, r) != 0.0 ||
+        f(xb4::f_icVBSGiven, r) != 0.0 || f(xb4::f_icVDSGiven, r) != 0.0 || f(xb4::f_icVGSGiven, r) != 0.0)
+      return true;
+  return false;
+}
+
 // Times every launch shape on the circuit's own instances at a synthetic operating point (node
 // voltages spread over 0..1.2 V, transient flags) in scratch buffers, and returns the fastest.
 int autotune_eval(xd_ctx *ctx, int &best) {
   best = ctx->family == kFamilyMos1    ? kFirstMos1Variant
          : ctx->family == kFamilyBsim3 ? kFirstBsim3Variant
+         : ctx->gen                    ? kFirstGenVariant
          : ctx->series                 ? kFirstSeriesVariant
                                        : (ctx->needs_full ? kFirstFullVariant : 0);
   const int n = ctx->n;
   if (n < 4096) return 0;
-  // State and store blocks of the family's size (BSIM4 3 / 14, BSIM3 5 / 5, MOSFET1 8 / 5 slots).
+  // State and store blocks of the family's size (BSIM4 3 / 14 or, general topology, 6 / 14; BSIM3
+  // 5 / 5; MOSFET1 8 / 5 slots).
   const size_t nsta = ctx->family == kFamilyMos1 ? xm1::kNumState
-                      : ctx->family == kFamilyBsim3 ? xb3::kNumState : xb4::kNumState;
+                      : ctx->family == kFamilyBsim3 ? xb3::kNumState
+                      : ctx->gen ? (size_t)xb4::kGenState : (size_t)xb4::kNumState;
   const size_t nsto = ctx->family == kFamilyMos1 ? xm1::kNumStore
                       : ctx->family == kFamilyBsim3 ? xb3::kNumStore : xb4::kNumStore;
   double *sol = nullptr, *sta = nullptr, *sto = nullptr;
@@ -876,6 +976,42 @@ extern "C" {
 
 const char *xd_last_error(void) { return g_err.c_str(); }
 
+int xd_internal_nodes_gen(const xd_mosfet_family *fam, int *flags) {
+  g_err.clear();
+  if (!fam || !flags) return fail(-1, "null argument");
+  if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
+  if (fam->level != 14 && fam->level != 54) return fail(-1, "the general topology is BSIM4's (level 14 / 54)");
+  const int n = fam->n_inst;
+  std::vector<xb4::ModelSpec> models(fam->n_models);
+  size_t off = 0;
+  for (int m = 0; m < fam->n_models; ++m) {
+    models[m].pmos = fam->model_is_pmos[m] != 0;
+    for (int k = 0; k < fam->model_nparams[m]; ++k, ++off)
+      models[m].params.push_back({fam->model_param_names[off], fam->model_param_values[off]});
+  }
+  std::vector<std::string> ipn;
+  for (int k = 0; k < fam->n_inst_params; ++k) ipn.push_back(fam->inst_param_names[k]);
+  xb4::SetupOptions opts;
+  opts.temp_c = fam->temp_c;
+  opts.tnom_c = fam->tnom_c;
+  xb4::RecordTable rt;
+  const std::string e = xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
+  if (!e.empty()) return fail(-2, e);
+  std::vector<unsigned char> gf;
+  gen_flags(rt, gf);
+  for (size_t k = 0; k < gf.size(); ++k) flags[k] = gf[k];
+  return family_needs_gen(rt) ? 1 : 0;
+}
+
+int xd_general_stamp(int *rows, int *cols) {
+  if (!rows || !cols) return fail(-1, "null argument");
+  for (int k = 0; k < xb4::kGenSlots; ++k) {
+    rows[k] = xb4::kGenStamp[k][0];
+    cols[k] = xb4::kGenStamp[k][1];
+  }
+  return xb4::kGenSlots;
+}
+
 int xd_internal_nodes(const xd_mosfet_family *fam, int *flags) {
   g_err.clear();
   if (!fam || !flags) return fail(-1, "null argument");
@@ -916,6 +1052,7 @@ int xd_num_state_slots(const xd_ctx *ctx) {
   if (!ctx) return -1;
   return ctx->family == kFamilyMos1 ? (int)xm1::kNumState
          : ctx->family == kFamilyBsim3 ? (int)xb3::kNumState
+         : ctx->gen                    ? (int)xb4::kGenState
                                        : (int)xb4::kNumState;
 }
 int xd_num_store_slots(const xd_ctx *ctx) {
@@ -935,6 +1072,7 @@ int xd_destroy(xd_ctx *ctx) {
   cudaFree(ctx->d_stage);
   cudaFree(ctx->d_ext);
   cudaFree(ctx->d_mid);
+  cudaFree(ctx->d_gmap);
   free_map(ctx->vmap);
   free_map(ctx->mmap);
   delete ctx;
@@ -956,7 +1094,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     return fail(-2, "MOSFET level " + std::to_string(fam->level) +
                         " is not implemented (levels 1, 9, 49, 14, 54 are)");
   if (fam->n_inst < 0 || fam->n_models <= 0) return fail(-1, "bad instance or model count");
-  if ((long long)fam->n_inst * xb4::kSerStage >= (1LL << 31)) return fail(-1, "too many instances");
+  if ((long long)fam->n_inst * xb4::kGenStage >= (1LL << 31)) return fail(-1, "too many instances");
   if (pat->n_rows < 0 || !pat->rowptr || (pat->rowptr[pat->n_rows] > 0 && !pat->colind))
     return fail(-1, "bad CSR pattern");
   const int n = fam->n_inst;
@@ -980,11 +1118,22 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       : family == kFamilyBsim3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
                                : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
+  // General topology (BSIM4): the caller passed the 10 internal variables per instance, or the
+  // cards need them.
+  const bool gen = family == kFamilyBsim4 && (fam->inst_internal_gen != nullptr || family_needs_gen(rt));
+  if (gen && !fam->inst_internal_gen)
+    return fail(-1, "the instances use gate or body resistance, rdsMod 1 or initial conditions: pass their internal "
+                    "unknowns in inst_internal_gen (xd_internal_nodes_gen lists which instances have which)");
+  if (gen && fam->inst_internal)
+    return fail(-1, "pass the internal unknowns in inst_internal_gen only (it includes the drain and source ones)");
+  if (fam->inst_internal_gen && family != kFamilyBsim4)
+    return fail(-1, "inst_internal_gen is for BSIM4 families");
   // Internal drain / source nodes (series resistance): which instances have them.
   std::vector<unsigned char> dint(n, 0), sint(n, 0);
   bool series = false;
   internal_flags(family, rt, dint, sint);
-  for (int i = 0; i < n; ++i) series = series || dint[i] || sint[i];
+  if (!gen)
+    for (int i = 0; i < n; ++i) series = series || dint[i] || sint[i];
   if (series && !fam->inst_internal)
     return fail(-1, "instances have internal drain/source nodes (series resistance): pass their unknowns in "
                     "inst_internal (xd_internal_nodes lists which instances have them)");
@@ -1027,13 +1176,60 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     p = (int)(q - pat->colind);
     return true;
   };
-  const int vrows = series ? xb4::kSerVecRows : 4;
-  std::vector<int> vt, vs, mt, ms;
+  const int vrows = gen ? xb4::kGenVecRows : series ? xb4::kSerVecRows : 4;
+  std::vector<int> vt, vs, mt, ms, gmap;
+  if (gen) {
+    // Local node -> unknown (collapsed nodes onto their representative, -1 for ground and for
+    // absent branch currents), then the gather maps: per instance, vector rows in node order and
+    // matrix entries in stamp-slot order.
+    std::vector<unsigned char> gfl;
+    gen_flags(rt, gfl);
+    gmap.assign((size_t)xb4::kGenNodes * n, -1);
+    vt.reserve((size_t)xb4::kGenVecRows * n);
+    vs.reserve((size_t)xb4::kGenVecRows * n);
+    mt.reserve((size_t)xb4::kGenSlots * n);
+    ms.reserve((size_t)xb4::kGenSlots * n);
+    static const char *const kNames[kGenInternal] = {"drain'", "source'", "gate'", "gate-mid", "body'",
+                                                     "source-body", "drain-body", "IBS", "IDS", "IGS"};
+    for (int i = 0; i < n; ++i) {
+      int nd[xb4::kGenNodes];
+      for (int k = 0; k < 4; ++k) {
+        nd[k] = fam->inst_nodes[4 * (size_t)i + k];
+        if (nd[k] >= nu) return fail(-1, "instance node index beyond the pattern's unknowns");
+        if (nd[k] < 0) nd[k] = -1;
+      }
+      // Representatives of the collapsible nodes: D' -> D, S' -> S, G' / GM -> G, B' / SB / DB -> B.
+      const int rep[kGenInternal] = {nd[0], nd[2], nd[1], nd[1], nd[3], nd[3], nd[3], -1, -1, -1};
+      for (int k = 0; k < kGenInternal; ++k) {
+        const int u = fam->inst_internal_gen[(size_t)kGenInternal * i + k];
+        const bool has = gfl[(size_t)kGenInternal * i + k] != 0;
+        if (has && (u < 0 || u >= nu))
+          return fail(-1, "instance " + std::to_string(i) + " needs an internal " + kNames[k] +
+                              " unknown inside the pattern's unknowns");
+        if (!has && u >= 0)
+          return fail(-1, "instance " + std::to_string(i) + " has no internal " + kNames[k] + " variable");
+        nd[4 + k] = has ? u : rep[k];
+      }
+      for (int k = 0; k < xb4::kGenNodes; ++k) {
+        gmap[(size_t)k * n + i] = nd[k];
+        vt.push_back(nd[k]);
+        vs.push_back(k * n + i);
+      }
+      for (int k = 0; k < xb4::kGenSlots; ++k) {
+        int p;
+        if (!csr_pos(nd[xb4::kGenStamp[k][0]], nd[xb4::kGenStamp[k][1]], p))
+          return fail(-1, "CSR pattern lacks an entry the instance's general stamp touches");
+        mt.push_back(p);
+        ms.push_back(k * n + i);
+      }
+      nodes[i] = make_int4(nd[0], nd[1], nd[2], nd[3]);
+    }
+  }
   vt.reserve((size_t)vrows * n);
   vs.reserve((size_t)vrows * n);
   mt.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
   ms.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
-  for (int i = 0; i < n; ++i) {
+  for (int i = 0; !gen && i < n; ++i) {
     const int nd[4] = {nodes[i].x, nodes[i].y, nodes[i].z, nodes[i].w};
     for (int r = 0; r < 4; ++r) {
       vt.push_back(nd[r]);
@@ -1075,10 +1271,17 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   ctx->nnz = pat->rowptr[nu];
   ctx->n_rec = rt.n_records;
   ctx->series = series;
+  ctx->gen = gen;
   if (series) {
     ctx->vec_rows = xb4::kSerVecRows;
     ctx->mat_slots = xb4::kSerMat;
     ctx->stage_slots = xb4::kSerStage;
+  }
+  if (gen) {
+    ctx->vec_rows = xb4::kGenVecRows;
+    ctx->mat_slots = xb4::kGenSlots;
+    ctx->stage_slots = xb4::kGenStage;
+    ctx->needs_full = true;
   }
   if (family == kFamilyBsim4)
     for (int r = 0; r < rt.n_records; ++r)
@@ -1108,7 +1311,11 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   if (series && ((ce = cudaMalloc(&ctx->d_ext, std::max(1, n) * sizeof(int2))) != cudaSuccess ||
                  (ce = cudaMemcpy(ctx->d_ext, ext.data(), n * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess))
     return cleanup(cuda_fail(ce, "xd_create allocation"));
-  if (family == kFamilyBsim4 && !series && !ctx->needs_full && n > 0 &&
+  if (gen && ((ce = cudaMalloc(&ctx->d_gmap, std::max<size_t>(1, gmap.size()) * sizeof(int))) != cudaSuccess ||
+              (ce = cudaMemcpy(ctx->d_gmap, gmap.data(), gmap.size() * sizeof(int), cudaMemcpyHostToDevice)) !=
+                  cudaSuccess))
+    return cleanup(cuda_fail(ce, "xd_create allocation"));
+  if (family == kFamilyBsim4 && !series && !gen && !ctx->needs_full && n > 0 &&
       (ce = cudaMalloc(&ctx->d_mid, (size_t)xb4::kNumMid * n * sizeof(double))) != cudaSuccess)
     return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
@@ -1205,7 +1412,8 @@ int xd_load_vectors_staged(xd_ctx *ctx, const double *d_stage16, double *d_f, do
   if (!ctx) return fail(-1, "null context");
   if (ctx->n == 0) return 0;
   if (!d_stage16) return fail(-1, "null staged array");
-  if (ctx->series) return fail(-1, "staged vectors take the 4-terminal layout; this family has internal nodes");
+  if (ctx->series || ctx->gen)
+    return fail(-1, "staged vectors take the 4-terminal layout; this family has internal nodes");
   DeviceGuard g(ctx->device);
   const size_t n = (size_t)ctx->n;
   OutSet<4, false> os{{d_f, d_q, d_dfdxdvp, d_dqdxdvp}, {0, 4 * n, 8 * n, 12 * n}, assign ? 1 : 0};
@@ -1275,6 +1483,8 @@ int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream) {
   if (e != cudaSuccess) return cuda_fail(e, "fma_probe_kernel launch");
   return 0;
 }
+
+int xd_num_stage_slots(const xd_ctx *ctx) { return ctx ? ctx->stage_slots : -1; }
 
 int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream) {
   if (!ctx || !h_out) return fail(-1, "null argument");
@@ -1351,9 +1561,9 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
                            double *d_dfdxdvp, double *d_dqdxdvp, double *d_dfdx_vals, double *d_dqdx_vals,
                            void *stream) {
   if (!ctx || !flags) return fail(-1, "null argument");
-  if (ctx->series)
+  if (ctx->series || ctx->gen)
     return fail(-1, "xd_load_static_scratch: the static scratch holds the 4-terminal layout; this family has "
-                    "internal drain/source nodes");
+                    "internal nodes");
   if (ctx->n > XD_STATIC_MAX_INSTANCES)
     return fail(-1, "xd_load_static_scratch: " + std::to_string(ctx->n) + " instances exceed the static scratch "
                     "capacity of " + std::to_string(XD_STATIC_MAX_INSTANCES) + "; use xd_load");

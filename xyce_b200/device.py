@@ -123,23 +123,52 @@ def _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, t
     fam.temp_c = float(temp_c)
     fam.tnom_c = float(tnom_c)
     if inst_internal is not None:
-        internal = np.ascontiguousarray(np.asarray(inst_internal, dtype=np.int32).reshape(-1))
-        if internal.shape[0] != 2 * n:
-            raise _native.NativeError("inst_internal must have shape [n, 2]")
+        # [n, 2]: drain / source internal nodes; [n, 10]: the BSIM4 general topology's internal
+        # variables (GEN_INTERNAL order).
+        arr = np.asarray(inst_internal, dtype=np.int32)
+        internal = np.ascontiguousarray(arr.reshape(-1))
         keep.append(internal)
-        fam.inst_internal = internal.ctypes.data_as(_native._ip)
+        if arr.ndim == 2 and arr.shape == (n, GEN_INTERNAL):
+            fam.inst_internal_gen = internal.ctypes.data_as(_native._ip)
+        elif internal.shape[0] == 2 * n:
+            fam.inst_internal = internal.ctypes.data_as(_native._ip)
+        else:
+            raise _native.NativeError("inst_internal must have shape [n, 2] or [n, 10]")
     return fam, keep
 
 
-def internal_nodes(models, inst_model, inst_nodes, inst_params, level=14, temp_c=27.0, tnom_c=27.0):
-    """Which instances have an internal drain / source node ([n, 2] bool): the topology query the
-    reference's instances answer before their unknowns are numbered (``xd_internal_nodes``)."""
+# The BSIM4 general topology's internal variables per instance, in the reference's registerLIDs
+# order (N_DEV_MOSFET_B4.C:5018-5075); the columns of an [n, 10] ``inst_internal``.
+GEN_INTERNAL_NAMES = ("drain'", "source'", "gate'", "gate-mid", "body'", "source-body", "drain-body", "IBS", "IDS",
+                      "IGS")
+GEN_INTERNAL = len(GEN_INTERNAL_NAMES)
+
+
+def internal_nodes(models, inst_model, inst_nodes, inst_params, level=14, temp_c=27.0, tnom_c=27.0, general=False):
+    """Which instances have which internal variables: the topology query the reference's instances
+    answer before their unknowns are numbered. ``general=False``: [n, 2] bool, the internal drain /
+    source nodes (``xd_internal_nodes``). ``general=True`` (BSIM4): ([n, 10] bool in GEN_INTERNAL
+    order, whether the family needs the general topology) from ``xd_internal_nodes_gen``."""
     fam, keep = _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, tnom_c)
     n = int(np.asarray(inst_model).shape[0])
-    flags = np.zeros(2 * n, dtype=np.int32)
     lib = _native.load()
+    if general:
+        flags = np.zeros(GEN_INTERNAL * n, dtype=np.int32)
+        rc = lib.xd_internal_nodes_gen(ctypes.byref(fam), flags.ctypes.data_as(_native._ip))
+        _native.check(min(rc, 0), "xd_internal_nodes_gen")
+        return flags.reshape(n, GEN_INTERNAL).astype(bool), rc == 1
+    flags = np.zeros(2 * n, dtype=np.int32)
     _native.check(lib.xd_internal_nodes(ctypes.byref(fam), flags.ctypes.data_as(_native._ip)), "xd_internal_nodes")
     return flags.reshape(n, 2).astype(bool)
+
+
+def general_stamp():
+    """The general topology's 77 (row, col) local-node pairs (``xd_general_stamp``)."""
+    lib = _native.load()
+    rows, cols = np.zeros(128, dtype=np.int32), np.zeros(128, dtype=np.int32)
+    k = lib.xd_general_stamp(rows.ctypes.data_as(_native._ip), cols.ctypes.data_as(_native._ip))
+    _native.check(min(k, 0), "xd_general_stamp")
+    return np.stack([rows[:k], cols[:k]], 1)
 
 
 class MosfetDevice:
@@ -151,7 +180,8 @@ class MosfetDevice:
     inst_params:   dict name -> float array [n] (NaN = not given), e.g. L, W, NF, AD, DELVTO, M
     pattern:       (rowptr, colind) CSR pattern of the Jacobian over the unknowns
     inst_internal: int array [n, 2] internal drain / source unknowns (-1 = none), required when
-                   ``internal_nodes`` reports some
+                   ``internal_nodes`` reports some; or, for the BSIM4 general topology (gate / body
+                   resistance, rdsMod 1, instance ICs), [n, 10] in GEN_INTERNAL order
     """
 
     level = 14
@@ -220,10 +250,13 @@ class MosfetDevice:
                                             _ptr(dqdx), _stream_handle(stream)), "xd_load_abs")
 
     def copy_stamps(self, stream=None) -> np.ndarray:
-        out = np.zeros(48 * self.n, dtype=np.float64)
+        """The staged stamps, [slots, n] (48 slots for the 4-terminal layout, 68 with internal drain /
+        source nodes, 210 for the general topology)."""
+        slots = self._lib.xd_num_stage_slots(self._h)
+        out = np.zeros(slots * self.n, dtype=np.float64)
         _native.check(self._lib.xd_copy_stamps(self._h, ctypes.c_void_p(out.ctypes.data), _stream_handle(stream)),
                       "xd_copy_stamps")
-        return out.reshape(48, self.n)
+        return out.reshape(slots, self.n)
 
 
 class Bsim4Device(MosfetDevice):

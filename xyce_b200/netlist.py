@@ -40,9 +40,10 @@ class Circuit:
     vsrc_pwl: list = field(default_factory=list)  # per source: None or (times, values)
     vdd: float = 1.2
     meta: dict = field(default_factory=dict)
-    # Internal drain / source nodes of the MOSFETs (series resistance): [n_mos, 2] unknown indices,
-    # -1 where the node collapses onto the terminal. They come after the nodes and the source
-    # branches, in instance order, drain first (the reference's numbering of internal variables).
+    # Internal variables of the MOSFETs: [n_mos, 2] drain / source nodes (series resistance), or
+    # [n_mos, 10] for the BSIM4 general topology (D', S', G', GM, B', SB, DB and the IBS, IDS, IGS
+    # branch currents), unknown indices, -1 where the instance has none. They come after the nodes
+    # and the source branches, instance by instance in that order (the reference's numbering).
     mos_internal: np.ndarray | None = None
     n_internal: int = 0
 
@@ -78,6 +79,41 @@ def _pairs_2term(nodes: np.ndarray) -> np.ndarray:
     return np.stack([rows, cols], 1)
 
 
+# The BSIM4 general topology's stamp over its 14 local nodes (D, G, S, B, D', S', G', GM, B', SB, DB,
+# IBS, IDS, IGS = 0..13), in the reference's jacStamp order (N_DEV_MOSFET_B4.C:4641-4795); the
+# library reports the same table (xd_general_stamp).
+_D, _G, _S, _B, _DP, _SP, _GP, _GM, _BP, _SB, _DB, _IBS, _IDS, _IGS = range(14)
+GEN_STAMP = np.array(
+    [(_D, _D), (_D, _DP), (_D, _SP), (_D, _GP), (_D, _BP),
+     (_G, _G), (_G, _DP), (_G, _SP), (_G, _GP), (_G, _GM), (_G, _BP),
+     (_S, _S), (_S, _DP), (_S, _SP), (_S, _GP), (_S, _BP),
+     (_B, _B), (_B, _BP), (_B, _SB), (_B, _DB),
+     (_DP, _D), (_DP, _DP), (_DP, _SP), (_DP, _GP), (_DP, _GM), (_DP, _BP), (_DP, _DB),
+     (_SP, _S), (_SP, _DP), (_SP, _SP), (_SP, _GP), (_SP, _GM), (_SP, _BP), (_SP, _SB),
+     (_GP, _G), (_GP, _DP), (_GP, _SP), (_GP, _GP), (_GP, _GM), (_GP, _BP),
+     (_GM, _G), (_GM, _DP), (_GM, _SP), (_GM, _GP), (_GM, _GM), (_GM, _BP),
+     (_BP, _B), (_BP, _DP), (_BP, _SP), (_BP, _GP), (_BP, _GM), (_BP, _BP), (_BP, _SB), (_BP, _DB),
+     (_SB, _B), (_SB, _SP), (_SB, _BP), (_SB, _SB),
+     (_DB, _B), (_DB, _DP), (_DB, _BP), (_DB, _DB),
+     (_IBS, _S), (_IBS, _B), (_IBS, _IBS), (_S, _IBS), (_B, _IBS),
+     (_IDS, _D), (_IDS, _S), (_IDS, _IDS), (_D, _IDS), (_S, _IDS),
+     (_IGS, _G), (_IGS, _S), (_IGS, _IGS), (_G, _IGS), (_S, _IGS)], dtype=np.int64)
+
+
+def general_local_nodes(c: Circuit) -> np.ndarray:
+    """[n_mos, 14] unknown of each local node of the general topology: a node the instance does
+    not have is its terminal's unknown (D' -> D, S' -> S, G' and GM -> G, B' / SB / DB -> B), an
+    absent branch current -1, ground -1."""
+    nd = c.mos_nodes.astype(np.int64)
+    internal = c.mos_internal.astype(np.int64)
+    rep = nd[:, [0, 2, 1, 1, 3, 3, 3]]
+    loc = np.full((nd.shape[0], 14), -1, dtype=np.int64)
+    loc[:, :4] = nd
+    loc[:, 4:11] = np.where(internal[:, :7] >= 0, internal[:, :7], rep)
+    loc[:, 11:] = internal[:, 7:]
+    return loc
+
+
 def jacobian_pattern(c: Circuit):
     """CSR (rowptr, colind) over the unknowns: union of MOSFET 4x4, R/C 2x2 and V-source stamps."""
     parts = []
@@ -85,7 +121,12 @@ def jacobian_pattern(c: Circuit):
     r = np.repeat(m, 4, axis=1)
     cc = np.tile(m, (1, 4))
     parts.append(np.stack([r.reshape(-1), cc.reshape(-1)], 1))
-    if c.mos_internal is not None:
+    if c.mos_internal is not None and c.mos_internal.shape[1] == 10:
+        # The general topology's stamp after collapsing (pairs with ground or an absent branch
+        # current drop out below).
+        loc = general_local_nodes(c)
+        parts.append(np.stack([loc[:, GEN_STAMP[:, 0]].reshape(-1), loc[:, GEN_STAMP[:, 1]].reshape(-1)], 1))
+    elif c.mos_internal is not None:
         # Series resistances: (D', D), (D, D'), (D, D) and the source's.
         for k, col in ((0, 0), (1, 2)):
             has = c.mos_internal[:, k] >= 0
@@ -112,11 +153,13 @@ def jacobian_pattern(c: Circuit):
 
 
 def with_internal_nodes(c: Circuit, flags) -> Circuit:
-    """The circuit with an internal drain / source unknown for every True in flags ([n_mos, 2], from
-    ``device.internal_nodes``), numbered after all other unknowns in instance order, drain first."""
+    """The circuit with an internal unknown for every True in flags ([n_mos, 2] drain / source, or
+    [n_mos, 10] for the BSIM4 general topology, from ``device.internal_nodes``), numbered after all
+    other unknowns, instance by instance in column order."""
     import dataclasses
 
-    flags = np.asarray(flags, dtype=bool).reshape(-1, 2)
+    flags = np.asarray(flags, dtype=bool)
+    flags = flags.reshape(c.n_mos, -1)
     internal = np.full(flags.shape, -1, dtype=np.int64)
     base = c.n_nodes + c.n_vsrc
     order = np.flatnonzero(flags.reshape(-1))

@@ -64,9 +64,11 @@ def _tally(strict, key, got, ref):
 
 
 def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=3, n_sto=14, vspan=None,
-               strict=None):
+               strict=None, counts=None):
     """Compares one load of every output within the parity tolerance. With `strict` (a dict), also
-    counts per output how many entries pass at plain 1e-12 relative, without any floor."""
+    counts per output how many entries pass at plain 1e-12 relative, without any floor. `counts`
+    (output -> contributions per entry, tests.parity.stamp_counts) widens the abs-sum floor of
+    entries summed from very many instances to the summation-order bound."""
     report = {}
     keys = ["f", "dfdxdvp", "dfdx"] + (["q", "dqdxdvp", "dqdx"] if charges else [])
     for k in keys:
@@ -77,7 +79,8 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
             vec_scale = vspan * np.maximum(row_max(rowptr, r[m]), row_max(rowptr, g[m]))
         bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR,
                              rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail,
-                             sens=r["sens"][k] if "sens" in r else None, vec_scale=vec_scale)
+                             sens=r["sens"][k] if "sens" in r else None, vec_scale=vec_scale,
+                             nterms=None if counts is None else counts.get(k))
         report[k] = worst
         _tally(strict, k, g[k], r[k])
         assert bad == 0, (f"step {step} {flags}: {k} has {bad} entries out of tolerance (worst {worst:.3g}x); "

@@ -44,7 +44,10 @@ def test_reference_device_loop_through_gpu_binding(topology):
     elif topology == "general":
         cards = [ModelCard(False, {"RGATEMOD": 3, "RBODYMOD": 1, "RDSMOD": 1, "RSH": 20.0}),
                  ModelCard(True, {"RGATEMOD": 1, "RBODYMOD": 2, "RBPS0": 60.0, "RBPD0": 70.0})]
-        extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5), "IC2": np.where(np.arange(n) % 9 == 0, 0.8, np.nan)}
+        # Initial conditions on NMOS instances (drain / source nodes exist: the reference places the
+        # couplings in the branch currents' columns there).
+        ic = (np.arange(n) % 9 == 0) & (c.mos_type == netlist.NMOS)
+        extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5), "IC2": np.where(ic, 0.8, np.nan)}
     cards, im, nd, params = family_inputs(c, cards, extra)
     if topology == "series":
         c = netlist.with_internal_nodes(c, internal_nodes(cards, im, nd, params))

@@ -33,12 +33,16 @@ def test_fused_load_combine_bitwise(mode, order, gshunt, limiter):
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, im, nd, params = netlist.mosfet_family(c)
     nu, nnz = c.n_unknowns, int(rowptr[-1])
+    # Two fresh contexts: an evaluation advances the context's per-instance vgb memory (the next
+    # load's vgb_orig), so the fused call gets a context that has not loaded yet, as the unfused one.
     fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), nu)
+    fam2 = MosfetDevice(cards, im, nd, params, (rowptr, colind), nu)
+    assert lib.xd_set_eval_variant(fam2._h, lib.xd_get_eval_variant(fam._h)) == 0
     csr = _native.XdCsr(nu, rowptr.ctypes.data_as(_native._ip), colind.ctypes.data_as(_native._ip))
     tia = ctypes.c_void_p()
     _native.check(lib.xd_tia_create(ctypes.byref(csr), 0, ctypes.byref(tia)), "xd_tia_create")
     fused = ctypes.c_void_p()
-    _native.check(lib.xd_tia_fused_create(tia, fam._h, ctypes.byref(fused)), "xd_tia_fused_create")
+    _native.check(lib.xd_tia_fused_create(tia, fam2._h, ctypes.byref(fused)), "xd_tia_fused_create")
     lin = LinearDevices(c, rowptr, colind)
     f64 = dict(dtype=torch.float64, device="cuda")
     T = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), **f64)
@@ -85,6 +89,7 @@ def test_fused_load_combine_bitwise(mode, order, gshunt, limiter):
     lib.xd_tia_fused_destroy(fused)
     lib.xd_tia_destroy(tia)
     fam.close()
+    fam2.close()
 
 
 def test_fused_transient_matches_unfused_bitwise():

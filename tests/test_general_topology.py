@@ -45,21 +45,24 @@ CASES = {
 }
 
 
-def _extra(case, n, rng):
+def _extra(case, n, rng, nmos):
     extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5)} if case in ("rds1", "mixed") else {}
     if case == "mixed":
-        # Instance overrides of the modes, and initial conditions on some instances.
+        # Instance overrides of the modes, and initial conditions on some instances: on the NMOS
+        # ones, whose drain / source nodes exist (rdsMod 1), where the reference places the
+        # initial-condition couplings in the branch currents' columns (see
+        # test_reference_ic_coupling_placement for the instances where it does not).
         extra["RGATEMOD"] = np.where(rng.random(n) < 0.2, 1.0, np.nan)
         extra["RBODYMOD"] = np.where(rng.random(n) < 0.2, 0.0, np.nan)
-        extra["IC1"] = np.where(rng.random(n) < 0.1, 0.4, np.nan)
-        extra["IC2"] = np.where(rng.random(n) < 0.1, 0.9, np.nan)
-        extra["IC3"] = np.where(rng.random(n) < 0.1, -0.2, np.nan)
+        extra["IC1"] = np.where(nmos & (rng.random(n) < 0.2), 0.4, np.nan)
+        extra["IC2"] = np.where(nmos & (rng.random(n) < 0.2), 0.9, np.nan)
+        extra["IC3"] = np.where(nmos & (rng.random(n) < 0.2), -0.2, np.nan)
     return extra
 
 
 def _circuit(case, n_mos=600, seed=21):
     c = netlist.random_logic(n_mos, seed=seed)
-    extra = _extra(case, c.n_mos, np.random.default_rng(seed))
+    extra = _extra(case, c.n_mos, np.random.default_rng(seed), c.mos_type == netlist.NMOS)
     cards, im, nd, params = family_inputs(c, CASES[case], extra)
     flags, general = internal_nodes(cards, im, nd, params, general=True)
     assert general
@@ -109,3 +112,82 @@ def test_general_topology_parity(case):
           SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=2)]
     worst = run_sequence(c, cards, dc + tran, extra_params=extra, vrange=(-0.4, 1.6), seed=4)
     print(case, int(flags.sum()), "internal variables; worst error / tolerance:", worst)
+
+
+def _ic_placement(rgate, rbody, nrd, nrs, ics):
+    """Where the reference writes the initial-condition couplings of a 3-stage inverter ring whose
+    instances all use (rgateMod, rbodyMod, NRD given, NRS given) and the initial conditions `ics`:
+    the difference of its dF/dx in DC and in a time step (the couplings load only in DC, the branch
+    current's diagonal only in a step; the rest of dF/dx is the same) as {(row, col): value}, and
+    the same set placed in the branch currents' columns. Also the circuit and pattern."""
+    from xyce_b200.device import SolverFlags as _F  # noqa: F401
+
+    c0 = netlist.inverter_ring(3)
+    n = c0.n_mos
+    base = {"RGATEMOD": rgate, "RBODYMOD": rbody, "RSH": 10.0}
+    extra = {}
+    if nrd:
+        extra["NRD"] = np.full(n, 1.0)
+    if nrs:
+        extra["NRS"] = np.full(n, 1.0)
+    for name in ics:
+        extra[name] = np.full(n, 0.3)
+    cards, im, nd, params = family_inputs(c0, [ModelCard(False, dict(base)), ModelCard(True, dict(base))], extra)
+    flags, _ = internal_nodes(cards, im, nd, params, general=True)
+    c = netlist.with_internal_nodes(c0, flags)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    orc = OracleRun(c, cards, im, nd, params, rowptr, colind)
+    sol = np.random.default_rng(1).uniform(0.0, 1.0, c.n_unknowns)
+    z6, z14 = np.zeros(6 * n), np.zeros(14 * n)
+    dc = orc.load(SolverFlags(dcop=1, transient=0, newton_iter=1, voltlim=0), sol, z6, z6, z14, z14)
+    tr = orc.load(SolverFlags(newton_iter=1, voltlim=0), sol, z6, z6, z14, z14)
+    d = dc["dfdx"] - tr["dfdx"]
+    prow = np.repeat(np.arange(c.n_unknowns), np.diff(rowptr))
+    got = {(int(prow[k]), int(colind[k])): round(float(d[k])) for k in np.flatnonzero(np.abs(d) > 0.5)}
+    loc = netlist.general_local_nodes(c)
+    want = {}
+    for i in range(n):
+        for ic_node, term in ((11, 3), (12, 0), (13, 1)):  # (IBS, B), (IDS, D), (IGS, G)
+            if loc[i, ic_node] < 0:
+                continue
+            for r_, c_, v in ((loc[i, term], loc[i, ic_node], 1), (loc[i, 2], loc[i, ic_node], -1),
+                              (loc[i, ic_node], loc[i, term], 1), (loc[i, ic_node], loc[i, 2], -1),
+                              (loc[i, ic_node], loc[i, ic_node], -1)):
+                if r_ >= 0 and c_ >= 0:
+                    want[(int(r_), int(c_))] = want.get((int(r_), int(c_)), 0) + v
+    want = {k: v for k, v in want.items() if v != 0}
+    return got, want, c, orc, sol
+
+
+@pytest.mark.parametrize("rgate,rbody,nrd,nrs,ic,consistent", [
+    (1, 0, 0, 0, "IC1", True), (2, 0, 0, 1, "IC3", True), (0, 1, 1, 1, "IC2", True), (3, 1, 1, 1, "IC1", True),
+    (0, 1, 0, 1, "IC3", True), (3, 0, 0, 1, "IC2", True),
+    (0, 1, 0, 0, "IC1", False), (3, 0, 0, 0, "IC3", False), (1, 1, 1, 0, "IC2", False), (2, 1, 0, 1, "IC1", False)])
+def test_reference_ic_coupling_placement(rgate, rbody, nrd, nrs, ic, consistent):
+    """The reference places an initial condition's couplings in row D (IC1 = VDS) and row S (every
+    initial condition) in the branch current's column, except where that row absorbed its prime
+    node's row (no drain' / source') while gate-mid or body-network nodes exist (rgateMod 3 or
+    rbodyMod): there the coupling lands one column early, on the node before the branch current
+    (its Jacobian offsets, MOSFET_B4 registerJacLIDs :5313-5400 over jacStampMap's merged rows,
+    N_DEV_DeviceInstance.C:636-900). Its dF/dx is then not the derivative of its own F, which loads
+    the coupling at the branch current (:16373-16401); the finite difference below shows it. The
+    library places the couplings in the branch currents' columns always, so it equals the reference
+    in the consistent configurations, which the parity tests use."""
+    got, want, c, orc, sol = _ic_placement(rgate, rbody, nrd, nrs, [ic])
+    assert (got == want) == consistent, (got, want)
+    if not consistent:
+        # A coupling the reference's dF/dx misplaces, against a finite difference of its own F
+        # (linear in the branch current): F changes by the coupling in that row and column.
+        miss = [k for k, v in want.items() if got.get(k, 0) != v and k[0] != k[1]]
+        if not miss:
+            return
+        r_, c_ = miss[0]
+        n = c.n_mos
+        z6, z14 = np.zeros(6 * n), np.zeros(14 * n)
+        fl = SolverFlags(dcop=1, transient=0, newton_iter=1, voltlim=0)
+        x1 = sol.copy()
+        x1[c_] += 1.0
+        f0 = orc.load(fl, sol, z6, z6, z14, z14)["f"]
+        f1 = orc.load(fl, x1, z6, z6, z14, z14)["f"]
+        if c_ >= c.n_nodes + c.n_vsrc:  # a branch current: F is linear in it
+            assert f1[r_] - f0[r_] == pytest.approx(want[(r_, c_)], abs=1e-9)

@@ -242,6 +242,13 @@ def placed_transient(args, n_mos=None, ns=None):
         g._lib.xd_rf_solve(g._rf, ctypes.c_void_p(x.data_ptr()))
     torch.cuda.synchronize()
     solve_ms = (time.perf_counter() - t) * 1e3 / 3
+    # The same refactorization and solve through cuSOLVER's refactorization library (comparison).
+    ref_lib_ms = []
+    for _ in range(3):
+        t = time.perf_counter()
+        g._lib.xd_rf_refactor_library(g._rf, ctypes.c_void_p(g.jac.data_ptr()))
+        torch.cuda.synchronize()
+        ref_lib_ms.append((time.perf_counter() - t) * 1e3)
     x = g.rhs.clone()
     torch.cuda.synchronize()
     t = time.perf_counter()
@@ -251,6 +258,8 @@ def placed_transient(args, n_mos=None, ns=None):
     solve_lib_ms = (time.perf_counter() - t) * 1e3 / 3
     lev_l, lev_u = ctypes.c_int(), ctypes.c_int()
     g._lib.xd_rf_levels(g._rf, ctypes.byref(lev_l), ctypes.byref(lev_u))
+    nnz_f, nlev, nupd = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+    g._lib.xd_rf_stats(g._rf, ctypes.byref(nnz_f), ctypes.byref(nlev), ctypes.byref(nupd))
     res = {"workload": f"seeded INV/NAND2/NOR2 netlist with placed wiring (fan-out U{{1..4}}, a pin takes one of "
                        f"the 64 most recent open slots), {c.n_mos} BSIM4 MOSFETs, {c.res_nodes.shape[0]} R + "
                        f"{c.cap_nodes.shape[0]} C wire parasitics, 64 PWL inputs, {c.n_unknowns} unknowns, "
@@ -262,9 +271,10 @@ def placed_transient(args, n_mos=None, ns=None):
            "ms_per_newton_iteration": run_s * 1e3 / max(1, its),
            "matrices": st.factorizations - f0, "host_factorizations": st.host_factorizations - h0,
            "per_iteration_ms": {"device_loads_and_combine": ev[0].elapsed_time(ev[1]) / 5,
-                                "refactorization": min(ref_ms), "triangular_solves": solve_ms,
-                                "triangular_solves_cusolver": solve_lib_ms},
+                                "refactorization": min(ref_ms), "refactorization_cusolver": min(ref_lib_ms),
+                                "triangular_solves": solve_ms, "triangular_solves_cusolver": solve_lib_ms},
            "factor_levels": [lev_l.value, lev_u.value],
+           "factors": {"entries": nnz_f.value, "elimination_levels": nlev.value, "updates": nupd.value},
            "swing_v": [float(w.min()), float(w.max())]}
     g.close()
     fam.close()

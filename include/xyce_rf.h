@@ -28,18 +28,34 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
                  const int *colind_u, const double *vals_u, const int *p, const int *q, int cuda_device,
                  xd_rf **out);
 
-/* Refactors with new values of A (device, in A's pattern), keeping the pivot order. A zero pivot
- * in that order is an error (< 0); a small one is not detected here, so a caller that cannot
- * bound the growth checks the solution's residual (the transient driver refines and, failing
- * that, makes a new host factorization). */
+/* Refactors with new values of A (device, in A's pattern), keeping the pivot order: the library's
+ * own elimination (one thread block over the factors' dependency levels, a warp per row, each
+ * entry updated in a fixed order, so the factors do not depend on timing). A zero pivot in that
+ * order is an error (< 0, which synchronises the legacy default stream to read); a small one is
+ * not detected here, so a caller that cannot bound the growth checks the solution's residual
+ * (the transient driver refines and, failing that, makes a new host factorization). */
 int xd_rf_refactor(xd_rf *rf, const double *d_vals_a);
+
+/* The same refactorization through cuSOLVER's refactorization library (cusolverRfRefactor), for
+ * comparison; it is set up on the first call of this or xd_rf_solve_library, and its factors are
+ * separate from xd_rf_refactor's. */
+int xd_rf_refactor_library(xd_rf *rf, const double *d_vals_a);
+
+/* Size of the refactorization: entries of the bundled factors L - I + U, dependency levels of
+ * the elimination, and multiply-subtract updates per refactorization. */
+int xd_rf_stats(const xd_rf *rf, int *nnz_factors, int *elimination_levels, long long *updates);
+
+/* Copies the bundled factors' values (nnz_factors doubles, CSR over P A Q's indices, columns
+ * ascending in each row) to host memory. */
+int xd_rf_copy_factors(const xd_rf *rf, double *h_vals);
 
 /* Solves A x = b in place: d_x holds b on entry and x on return (device, length n). The forward
  * and back substitutions are the library's own kernels (one thread block walking the factors'
  * dependency levels, deterministic sums), ordered on the legacy default stream. */
 int xd_rf_solve(xd_rf *rf, double *d_x);
 
-/* The same solve through the refactorization library's own triangular solve (for comparison). */
+/* The solve through the refactorization library's own triangular solve, with its factors from
+ * xd_rf_refactor_library (for comparison). */
 int xd_rf_solve_library(xd_rf *rf, double *d_x);
 
 /* Dependency levels of the lower and upper factors: the number of sequential steps of each

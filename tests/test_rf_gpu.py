@@ -126,3 +126,81 @@ def test_triangular_solve_kernels_match_library_and_repeat_bitwise():
     assert np.max(np.abs(outs[0] - outs[2])) <= 1e-11 * np.max(np.abs(outs[2]))
     g.close()
     fam.close()
+
+
+def _diag_dominant(g, seed):
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(g.nu), np.diff(g.rowptr))
+    vals = rng.uniform(-1e-3, 1e-3, g.nnz)
+    vals[rows == g.colind] = rng.uniform(5e-3, 1e-2, int((rows == g.colind).sum()))
+    return vals
+
+
+def test_own_refactorization_matches_library_and_repeats_bitwise():
+    """The library's own refactorization (xd_rf_refactor: right-looking over pivot levels)
+    against cuSOLVER's (xd_rf_refactor_library) on a placed netlist's pattern with new values in
+    the kept pivot order: the same solution to rounding, backward error at rounding level, and
+    bit-identical factors when repeated."""
+    c = netlist.random_logic(20000, seed=5, locality=64)
+    g, fam = _pair(c, "rf")
+    vals = _diag_dominant(g, 1)
+    g.jac.copy_(torch.as_tensor(vals, device="cuda"))
+    g.rhs.copy_(torch.as_tensor(np.ones(g.nu), device="cuda"))
+    g._solve()  # host factorization of this matrix, refactorization set up
+    nnz_f, nlev, nupd = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+    _native.check(g._lib.xd_rf_stats(g._rf, ctypes.byref(nnz_f), ctypes.byref(nlev), ctypes.byref(nupd)), "xd_rf_stats")
+    vals2 = _diag_dominant(g, 2)
+    d2 = torch.as_tensor(vals2, device="cuda")
+    b = np.random.default_rng(3).standard_normal(g.nu)
+    A = sp.csr_matrix((vals2, g.colind, g.rowptr), shape=(g.nu, g.nu))
+    facs, xs = [], []
+    for fn, solve in (("xd_rf_refactor", "xd_rf_solve"), ("xd_rf_refactor", "xd_rf_solve"),
+                      ("xd_rf_refactor_library", "xd_rf_solve_library")):
+        torch.cuda.synchronize()
+        _native.check(getattr(g._lib, fn)(g._rf, ctypes.c_void_p(d2.data_ptr())), fn)
+        if fn == "xd_rf_refactor":
+            f = np.zeros(nnz_f.value)
+            _native.check(g._lib.xd_rf_copy_factors(g._rf, f.ctypes.data_as(_native._dp)), "xd_rf_copy_factors")
+            facs.append(f)
+        x = torch.as_tensor(b, device="cuda").clone()
+        torch.cuda.synchronize()
+        _native.check(getattr(g._lib, solve)(g._rf, ctypes.c_void_p(x.data_ptr())), solve)
+        torch.cuda.synchronize()
+        xs.append(x.cpu().numpy())
+    # New values in the kept pivot order: backward errors at rounding level, the same for both.
+    berrs = [np.max(np.abs(b - A @ x) / (abs(A) @ np.abs(x) + np.abs(b))) for x in xs]
+    assert max(berrs) < 1e-11, berrs
+    assert berrs[0] < 10 * berrs[2] + 1e-15, berrs
+    assert np.array_equal(facs[0], facs[1])
+    assert np.array_equal(xs[0], xs[1])
+    assert np.max(np.abs(xs[0] - xs[2])) <= 1e-11 * np.max(np.abs(xs[2]))
+    print(f"factors {nnz_f.value} entries, {nlev.value} elimination levels, {nupd.value} updates")
+    g.close()
+    fam.close()
+
+
+def test_own_refactorization_reports_a_zero_pivot():
+    """A matrix whose first pivot in the kept order is exactly zero: xd_rf_refactor returns an
+    error (the transient driver then factors afresh on the host) instead of factors with infinities."""
+    c = netlist.random_logic(2000, seed=8, locality=64)
+    g, fam = _pair(c, "rf")
+    vals = _diag_dominant(g, 4)
+    g.jac.copy_(torch.as_tensor(vals, device="cuda"))
+    g.rhs.copy_(torch.as_tensor(np.ones(g.nu), device="cuda"))
+    g._solve()
+    P, Q = g._rf_keep[9], g._rf_keep[10]
+    r, col = int(P[0]), int(Q[0])
+    k = g.rowptr[r] + int(np.flatnonzero(g.colind[g.rowptr[r]:g.rowptr[r + 1]] == col)[0])
+    bad = vals.copy()
+    bad[k] = 0.0
+    d = torch.as_tensor(bad, device="cuda")
+    torch.cuda.synchronize()
+    rc = g._lib.xd_rf_refactor(g._rf, ctypes.c_void_p(d.data_ptr()))
+    assert rc < 0
+    assert "zero pivot in row 0" in g._lib.xd_last_error().decode()
+    # The same object refactors a good matrix afterwards.
+    d.copy_(torch.as_tensor(vals, device="cuda"))
+    torch.cuda.synchronize()
+    assert g._lib.xd_rf_refactor(g._rf, ctypes.c_void_p(d.data_ptr())) == 0
+    g.close()
+    fam.close()

@@ -148,6 +148,9 @@ SIGNATURES = {
     "xd_rf_refactor": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "xd_rf_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "xd_rf_solve_library": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_rf_refactor_library": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "xd_rf_stats": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.POINTER(ctypes.c_longlong)]),
+    "xd_rf_copy_factors": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "xd_rf_levels": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip]),
     "xd_rf_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_mse_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libxyce_b200.so")
-SOURCES = ["devload.cu", "tia.cu", "mlp.cu", "rf.cpp", "sptrsv.cu", "bsim4_setup.cpp", "bsim3_setup.cpp",
+SOURCES = ["devload.cu", "tia.cu", "mlp.cu", "rf.cpp", "lu.cu", "sptrsv.cu", "bsim4_setup.cpp", "bsim3_setup.cpp",
            "mos1_setup.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
               "-Xcompiler", "-fPIC", "-shared"]

@@ -2,10 +2,10 @@
 //
 // Every Newton matrix of a circuit has the same sparsity pattern, so after one numeric
 // factorization P A Q = L U on the host (its pivot order and fill pattern), every later matrix is
-// refactored and solved on the GPU with that pattern (cuSOLVER's refactorization library), and
-// the values never leave the device. This is the library linear solve of the transient driver,
-// not part of the device-load path. The refactorization is cuSOLVER's; the triangular solves are
-// the library's own kernels (sptrsv.cu) on cuSOLVER's bundled factors.
+// refactored and solved on the GPU with that pattern, and the values never leave the device. The
+// refactorization (lu.cu) and the triangular solves (sptrsv.cu) are the library's own kernels.
+// cuSOLVER's refactorization library is kept only as a comparison (xd_rf_refactor_library,
+// xd_rf_solve_library), set up on first use.
 #include <cuda_runtime.h>
 #include <cusolverRf.h>
 
@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/xyce_rf.h"
+#include "lu.h"
 #include "sptrsv.h"
 
 int xd_internal_fail(int code, const std::string &msg);
@@ -22,8 +23,12 @@ struct xd_rf {
   int n = 0, nnz_a = 0;
   int *d_rowptr = nullptr, *d_colind = nullptr, *d_p = nullptr, *d_q = nullptr;
   double *d_temp = nullptr;
+  XdLu lu;        // the refactorization
+  XdSptrsv tri;   // the triangular solves, over lu's bundled factors
+  // The comparison library, created on first use from host copies of the set-up inputs.
   cusolverRfHandle_t h = nullptr;
-  XdSptrsv tri;
+  std::vector<int> ra, ca, rl, cl, ru, cu, hp, hq;
+  std::vector<double> va, vl, vu;
 };
 
 namespace {
@@ -41,6 +46,7 @@ void release(xd_rf *r) {
   if (!r) return;
   if (r->h) cusolverRfDestroy(r->h);
   xd_sptrsv_free(&r->tri);
+  xd_lu_free(&r->lu);
   cudaFree(r->d_rowptr);
   cudaFree(r->d_colind);
   cudaFree(r->d_p);
@@ -100,54 +106,42 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
     release(r);
     return cu_fail(e, "xd_rf_create upload");
   }
-  cusolverStatus_t st;
-  if ((st = cusolverRfCreate(&r->h)) != CUSOLVER_STATUS_SUCCESS) {
+  // Host copies for the comparison library (created on first use).
+  r->ra.assign(rowptr_a, rowptr_a + n + 1);
+  r->ca.assign(colind_a, colind_a + nnz_a);
+  r->va.assign(vals_a, vals_a + nnz_a);
+  r->rl.assign(rowptr_l, rowptr_l + n + 1);
+  r->cl.assign(colind_l, colind_l + nnz_l);
+  r->vl.assign(vals_l, vals_l + nnz_l);
+  r->ru.assign(rowptr_u, rowptr_u + n + 1);
+  r->cu.assign(colind_u, colind_u + nnz_u);
+  r->vu.assign(vals_u, vals_u + nnz_u);
+  r->hp.assign(p, p + n);
+  r->hq.assign(q, q + n);
+  int rc = xd_lu_init(&r->lu, n, nnz_a, rowptr_a, colind_a, rowptr_l, colind_l, rowptr_u, colind_u, p, q);
+  if (rc != 0) {
     release(r);
-    return rf_fail(st, "cusolverRfCreate");
+    return rc;
   }
-  if ((st = cusolverRfSetMatrixFormat(r->h, CUSOLVERRF_MATRIX_FORMAT_CSR, CUSOLVERRF_UNIT_DIAGONAL_STORED_L)) !=
-          CUSOLVER_STATUS_SUCCESS ||
-      (st = cusolverRfSetResetValuesFastMode(r->h, CUSOLVERRF_RESET_VALUES_FAST_MODE_ON)) != CUSOLVER_STATUS_SUCCESS) {
+  rc = xd_sptrsv_init(&r->tri, n, r->lu.nnz, r->lu.d_mp, r->lu.d_mi, p, q);
+  if (rc != 0) {
     release(r);
-    return rf_fail(st, "cusolverRf configuration");
+    return rc;
   }
-  // Refactorization algorithm 2 and triangular-solve algorithm 3 (both must precede the analysis):
-  // on the 200k-unknown placed netlist (2M factor entries, ~2,900 dependency levels in each of L
-  // and U) they take 14.9 and 18.8 ms on a B200 against 48.3 and 72.2 ms for the defaults (0, 1),
-  // with the same backward error (5e-14).
-  if ((st = cusolverRfSetAlgs(r->h, CUSOLVERRF_FACTORIZATION_ALG2, CUSOLVERRF_TRIANGULAR_SOLVE_ALG3)) !=
-      CUSOLVER_STATUS_SUCCESS) {
+  // The set-up factors A's own values.
+  double *d_a = nullptr;
+  if ((e = cudaMalloc(&d_a, sizeof(double) * (nnz_a > 0 ? nnz_a : 1))) != cudaSuccess ||
+      (e = cudaMemcpy(d_a, vals_a, sizeof(double) * nnz_a, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaFree(d_a);
     release(r);
-    return rf_fail(st, "cusolverRfSetAlgs");
+    return cu_fail(e, "xd_rf_create upload");
   }
-  // The set-up reads host copies; the library's signature is not const-qualified.
-  std::vector<int> ra(rowptr_a, rowptr_a + n + 1), ca(colind_a, colind_a + nnz_a);
-  std::vector<int> rl(rowptr_l, rowptr_l + n + 1), cl(colind_l, colind_l + nnz_l);
-  std::vector<int> ru(rowptr_u, rowptr_u + n + 1), cu(colind_u, colind_u + nnz_u);
-  std::vector<double> va(vals_a, vals_a + nnz_a), vl(vals_l, vals_l + nnz_l), vu(vals_u, vals_u + nnz_u);
-  std::vector<int> hp(p, p + n), hq(q, q + n);
-  if ((st = cusolverRfSetupHost(n, nnz_a, ra.data(), ca.data(), va.data(), nnz_l, rl.data(), cl.data(), vl.data(),
-                                nnz_u, ru.data(), cu.data(), vu.data(), hp.data(), hq.data(), r->h)) !=
-      CUSOLVER_STATUS_SUCCESS) {
-    release(r);
-    return rf_fail(st, "cusolverRfSetupHost");
-  }
-  if ((st = cusolverRfAnalyze(r->h)) != CUSOLVER_STATUS_SUCCESS) {
-    release(r);
-    return rf_fail(st, "cusolverRfAnalyze");
-  }
-  // The analysis is symbolic; the numeric factors come from a refactorization of A's values.
-  if ((st = cusolverRfRefactor(r->h)) != CUSOLVER_STATUS_SUCCESS) {
-    release(r);
-    return rf_fail(st, "cusolverRfRefactor");
-  }
-  int nnz_m = 0, *mp = nullptr, *mi = nullptr;
-  double *mx = nullptr;
-  if ((st = cusolverRfAccessBundledFactorsDevice(r->h, &nnz_m, &mp, &mi, &mx)) != CUSOLVER_STATUS_SUCCESS) {
-    release(r);
-    return rf_fail(st, "cusolverRfAccessBundledFactorsDevice");
-  }
-  int rc = xd_sptrsv_init(&r->tri, n, nnz_m, mp, mi, p, q);
+  int info = 0;
+  rc = xd_lu_refactor(&r->lu, d_a, 0);
+  if (rc == 0) rc = xd_lu_info(&r->lu, 0, &info);
+  cudaFree(d_a);
+  if (rc == 0 && info != 0)
+    rc = xd_internal_fail(-5, "zero pivot in row " + std::to_string(info - 1) + " of the refactorization");
   if (rc != 0) {
     release(r);
     return rc;
@@ -159,22 +153,18 @@ int xd_rf_create(int n, int nnz_a, const int *rowptr_a, const int *colind_a, con
 int xd_rf_refactor(xd_rf *r, const double *d_vals_a) {
   if (!r || !d_vals_a) return xd_internal_fail(-1, "null refactorization argument");
   cudaSetDevice(r->device);
-  cusolverStatus_t st = cusolverRfResetValues(r->n, r->nnz_a, r->d_rowptr, r->d_colind, const_cast<double *>(d_vals_a),
-                                              r->d_p, r->d_q, r->h);
-  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfResetValues");
-  st = cusolverRfRefactor(r->h);
-  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfRefactor");
-  return 0;
+  int rc = xd_lu_refactor(&r->lu, d_vals_a, 0);
+  int info = 0;
+  if (rc == 0) rc = xd_lu_info(&r->lu, 0, &info);
+  if (rc == 0 && info != 0)
+    return xd_internal_fail(-5, "zero pivot in row " + std::to_string(info - 1) + " of the refactorization");
+  return rc;
 }
 
 int xd_rf_solve(xd_rf *r, double *d_x) {
   if (!r || !d_x) return xd_internal_fail(-1, "null refactorization argument");
   cudaSetDevice(r->device);
-  int nnz_m = 0, *mp = nullptr, *mi = nullptr;
-  double *mx = nullptr;
-  cusolverStatus_t st = cusolverRfAccessBundledFactorsDevice(r->h, &nnz_m, &mp, &mi, &mx);
-  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfAccessBundledFactorsDevice");
-  return xd_sptrsv_solve(&r->tri, mx, d_x, 0);
+  return xd_sptrsv_solve(&r->tri, r->lu.d_mx, d_x, 0);
 }
 
 int xd_rf_levels(const xd_rf *r, int *levels_l, int *levels_u) {
@@ -184,9 +174,69 @@ int xd_rf_levels(const xd_rf *r, int *levels_l, int *levels_u) {
   return 0;
 }
 
+int xd_rf_stats(const xd_rf *r, int *nnz_factors, int *elimination_levels, long long *updates) {
+  if (!r || !nnz_factors || !elimination_levels || !updates) return xd_internal_fail(-1, "null argument");
+  *nnz_factors = r->lu.nnz;
+  *elimination_levels = r->lu.nlev;
+  *updates = r->lu.npairs;
+  return 0;
+}
+
+int xd_rf_copy_factors(const xd_rf *r, double *h_vals) {
+  if (!r || !h_vals) return xd_internal_fail(-1, "null argument");
+  cudaSetDevice(r->device);
+  cudaError_t e = cudaMemcpy(h_vals, r->lu.d_mx, sizeof(double) * r->lu.nnz, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cu_fail(e, "xd_rf_copy_factors");
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The comparison library's handle, set up on first use with the same inputs (algorithms 2 and 3:
+// on the 200k-unknown placed netlist they were the fastest of its choices).
+int library_handle(xd_rf *r) {
+  if (r->h) return 0;
+  cusolverStatus_t st;
+  if ((st = cusolverRfCreate(&r->h)) != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfCreate");
+  if ((st = cusolverRfSetMatrixFormat(r->h, CUSOLVERRF_MATRIX_FORMAT_CSR, CUSOLVERRF_UNIT_DIAGONAL_STORED_L)) !=
+          CUSOLVER_STATUS_SUCCESS ||
+      (st = cusolverRfSetResetValuesFastMode(r->h, CUSOLVERRF_RESET_VALUES_FAST_MODE_ON)) != CUSOLVER_STATUS_SUCCESS ||
+      (st = cusolverRfSetAlgs(r->h, CUSOLVERRF_FACTORIZATION_ALG2, CUSOLVERRF_TRIANGULAR_SOLVE_ALG3)) !=
+          CUSOLVER_STATUS_SUCCESS ||
+      (st = cusolverRfSetupHost(r->n, r->nnz_a, r->ra.data(), r->ca.data(), r->va.data(), (int)r->cl.size(),
+                                r->rl.data(), r->cl.data(), r->vl.data(), (int)r->cu.size(), r->ru.data(),
+                                r->cu.data(), r->vu.data(), r->hp.data(), r->hq.data(), r->h)) !=
+          CUSOLVER_STATUS_SUCCESS ||
+      (st = cusolverRfAnalyze(r->h)) != CUSOLVER_STATUS_SUCCESS || (st = cusolverRfRefactor(r->h)) != CUSOLVER_STATUS_SUCCESS) {
+    cusolverRfDestroy(r->h);
+    r->h = nullptr;
+    return rf_fail(st, "cusolverRf set-up");
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xd_rf_refactor_library(xd_rf *r, const double *d_vals_a) {
+  if (!r || !d_vals_a) return xd_internal_fail(-1, "null refactorization argument");
+  cudaSetDevice(r->device);
+  if (int rc = library_handle(r)) return rc;
+  cusolverStatus_t st = cusolverRfResetValues(r->n, r->nnz_a, r->d_rowptr, r->d_colind, const_cast<double *>(d_vals_a),
+                                              r->d_p, r->d_q, r->h);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfResetValues");
+  st = cusolverRfRefactor(r->h);
+  if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfRefactor");
+  return 0;
+}
+
 int xd_rf_solve_library(xd_rf *r, double *d_x) {
   if (!r || !d_x) return xd_internal_fail(-1, "null refactorization argument");
   cudaSetDevice(r->device);
+  if (int rc = library_handle(r)) return rc;
   cusolverStatus_t st = cusolverRfSolve(r->h, r->d_p, r->d_q, 1, r->d_temp, r->n, d_x, r->n);
   if (st != CUSOLVER_STATUS_SUCCESS) return rf_fail(st, "cusolverRfSolve");
   return 0;

@@ -76,7 +76,8 @@ def eval_shape(lib, h):
     blk, minb = ctypes.c_int(), ctypes.c_int()
     v = lib.xd_get_eval_variant(h)
     lib.xd_eval_variant_info(v, ctypes.byref(blk), ctypes.byref(minb))
-    return {"block": blk.value, "min_blocks_per_sm": minb.value, "persistent": lib.xd_eval_variant_persistent(v) == 1}
+    return {"variant": v, "block": blk.value, "min_blocks_per_sm": minb.value,
+            "persistent": lib.xd_eval_variant_persistent(v) == 1, "split": lib.xd_eval_variant_split(v) == 1}
 
 
 def other_families(c, rowptr, colind, sol, dev_id, args):
@@ -391,6 +392,8 @@ def parse():
     ap.add_argument("--scale-mos", type=int, default=0,
                     help="MOSFETs of the scale transient (placed wiring; 0: skip; 1000000 for the scale configuration)")
     ap.add_argument("--scale-ns", type=float, default=2.0, help="length of the scale transient (ns)")
+    ap.add_argument("--eval-variant", type=int, default=-1,
+                    help="pin the BSIM4 evaluation launch shape (xd_set_eval_variant; default: the autotuner's pick)")
     ap.add_argument("--placed-only", action="store_true",
                     help="transient section: only the placed-netlist transient (for profiling its solve)")
     return ap.parse_args()
@@ -576,6 +579,8 @@ def main():
     launches = lib.xd_launches_per_load(dev._h)
     import ctypes
 
+    if args.eval_variant >= 0:
+        _native.check(lib.xd_set_eval_variant(dev._h, args.eval_variant), "xd_set_eval_variant")
     shape = eval_shape(lib, dev._h)
     stream = torch.cuda.current_stream()
     f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")

@@ -1229,17 +1229,20 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   vs.reserve((size_t)vrows * n);
   mt.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
   ms.reserve((size_t)(series ? xb4::kSerMat : 16) * n);
+  // Each instance's vector rows in the order the family's loadDAEVectors adds them (BSIM4: D', G',
+  // B', S' then the external D, S, N_DEV_MOSFET_B4.C:16316-16370; BSIM3: D, S, B, D', S' with the
+  // gate's charge first, N_DEV_MOSFET_B3.C:9357-9366, 9554-9557; MOSFET1: D, G, S, B, D', S',
+  // N_DEV_MOSFET1.C:4222-4236): where two rows of an instance are the same unknown (bulk tied to
+  // source), the sum then adds them in the reference's order.
+  static const int kVecOrder[3][6] = {{0, 1, 3, 2, 4, 5}, {4, 5, 1, 3, 0, 2}, {4, 1, 5, 3, 0, 2}};
+  const int *vorder = kVecOrder[family == kFamilyBsim4 ? 0 : family == kFamilyBsim3 ? 1 : 2];
   for (int i = 0; !gen && i < n; ++i) {
     const int nd[4] = {nodes[i].x, nodes[i].y, nodes[i].z, nodes[i].w};
-    for (int r = 0; r < 4; ++r) {
-      vt.push_back(nd[r]);
+    for (int k = 0; k < 6; ++k) {
+      const int r = vorder[k];
+      if (r >= 4 && !series) continue;
+      vt.push_back(r < 4 ? nd[r] : (r == 4 ? ext[i].x : ext[i].y));
       vs.push_back(r * n + i);
-    }
-    if (series) {
-      vt.push_back(ext[i].x);
-      vs.push_back(4 * n + i);
-      vt.push_back(ext[i].y);
-      vs.push_back(5 * n + i);
     }
     for (int r = 0; r < 4; ++r)
       for (int c = 0; c < 4; ++c) {

@@ -271,6 +271,9 @@ def placed_transient(args, n_mos=None, ns=None):
            "newton_iters_per_step": float(np.mean(st.newton_iters)),
            "ms_per_newton_iteration": run_s * 1e3 / max(1, its),
            "matrices": st.factorizations - f0, "host_factorizations": st.host_factorizations - h0,
+           "solves": st.solves, "refinement_solves": st.refinements,
+           "first_solve_backward_error": {q: float(np.quantile(st.first_solve_berr, v)) for q, v in
+                                          (("median", 0.5), ("p90", 0.9), ("max", 1.0))} if st.first_solve_berr else None,
            "per_iteration_ms": {"device_loads_and_combine": ev[0].elapsed_time(ev[1]) / 5,
                                 "refactorization": min(ref_ms), "refactorization_cusolver": min(ref_lib_ms),
                                 "triangular_solves": solve_ms, "triangular_solves_cusolver": solve_lib_ms},

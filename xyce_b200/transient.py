@@ -147,6 +147,9 @@ class StepStats:
     static_pivot_fallbacks: int = 0
     chord_iters: list = field(default_factory=list)
     surrogate_error: list = field(default_factory=list)
+    solves: int = 0                 # triangular solves with the GPU refactorization's factors
+    refinements: int = 0            # of which iterative-refinement steps
+    first_solve_berr: list = field(default_factory=list)  # backward error after each first solve
 
 
 class TransientBase:
@@ -706,6 +709,7 @@ class GpuTransient(TransientBase):
         torch.cuda.current_stream(self.dev).synchronize()
         _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(x.data_ptr())), "xd_rf_solve")
         torch.cuda.synchronize(self.dev)
+        self.stats.solves += 1
         ab = b.abs()
         for k in range(max_refine + 1):
             if not bool(torch.isfinite(x).all()):
@@ -713,7 +717,10 @@ class GpuTransient(TransientBase):
             r = b - J @ x
             den = Ja @ x.abs() + ab
             err = torch.where(r == 0, torch.zeros_like(r), r.abs() / den.clamp_min(1e-300))
-            if float(err.max()) <= tol:
+            e = float(err.max())
+            if k == 0:
+                self.stats.first_solve_berr.append(e)
+            if e <= tol:
                 return x
             if k == max_refine:
                 return x if accept else None
@@ -721,6 +728,8 @@ class GpuTransient(TransientBase):
             torch.cuda.current_stream(self.dev).synchronize()
             _native.check(self._lib.xd_rf_solve(self._rf, ctypes.c_void_p(d.data_ptr())), "xd_rf_solve")
             torch.cuda.synchronize(self.dev)
+            self.stats.solves += 1
+            self.stats.refinements += 1
             x = x + d
         return None
 

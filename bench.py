@@ -40,10 +40,14 @@ UNIT = "loads/s"
 # node indices (16), record index (4), 5 store values (40), vgb (8); writes 48 stamp values (384),
 # 12 store (96), 3 state (24), vgb (8).
 EVAL_BYTES_PER_INST = 32 + 16 + 4 + 40 + 8 + 384 + 96 + 24 + 8
-# DRAM bytes per instance of one evaluation launch (dram__bytes_read.sum + dram__bytes_write.sum
-# of an ncu capture at 199,832 instances of the same generator, 90 + 326 B; traffic grows with
-# the instance count), for roofline.traffic.
+# DRAM bytes per instance of one evaluation (dram__bytes_read.sum + dram__bytes_write.sum), for
+# roofline.traffic. Fused kernel: one ncu capture at 199,832 instances of the same generator,
+# 90 + 326 B. Split kernels (the bias / DC stage, a 37-double hand-off per instance, then the
+# charge / stamp stage): one capture of both launches at 999,694 instances, the benchmark's own
+# size, 88.4 + 274.0 MB and 351.2 + 588.9 MB, i.e. 362 + 940 B; the hand-off adds 2 x 296 B to the
+# 612 algorithmic bytes.
 EVAL_DRAM_BYTES_PER_INST_NCU = 90 + 326
+SPLIT_DRAM_BYTES_PER_INST_NCU = 362 + 940
 # FP64 operations per instance of one evaluation (ncu thread-instruction counters of the same
 # capture: 2,621 DFMA (2 flops each) + 844 DMUL + 511 DADD per instance), for the evaluation
 # kernel's compute roofline against the FP64 FMA-pipe probe.
@@ -718,6 +722,10 @@ def main():
     hbm_peak, peak_src = measured_peaks()
     eval_achieved = EVAL_BYTES_PER_INST * n / (t_eval * 1e-3) / 1e9
     fp64_achieved = EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12
+    if shape["split"]:
+        eval_kernel, dram_per_inst = "bsim4_dc_kernel + bsim4_charge_stamp_kernel", SPLIT_DRAM_BYTES_PER_INST_NCU
+    else:
+        eval_kernel, dram_per_inst = "bsim4_eval_kernel", EVAL_DRAM_BYTES_PER_INST_NCU
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -728,13 +736,13 @@ def main():
                    "instances_per_gpu": n, "nnz": nnz, "parallelism": f"replicas x{world}",
                    "l2": "working set > 126 MB L2 (staging + maps + CSR values), no flush"},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "fp64", "kernel": "bsim4_eval_kernel", "achieved": fp64_achieved,
+        "roofline": {"bound": "fp64", "kernel": eval_kernel, "achieved": fp64_achieved,
                      "peak": fp64_peak_tflops, "unit": "TFLOP/s", "frac": fp64_achieved / fp64_peak_tflops,
-                     "traffic": EVAL_DRAM_BYTES_PER_INST_NCU * n,
+                     "traffic": dram_per_inst * n,
                      "note": f"binding bound: the FP64 pipe ({EVAL_FP64_FLOPS_PER_INST} FP64 flops per instance, "
                              "executed-instruction count); peak = the FP64 FMA probe timed in this run "
                              "(the measured-peaks file has no FP64 figure); traffic = ncu DRAM bytes per "
-                             f"instance ({EVAL_DRAM_BYTES_PER_INST_NCU} B) x instances",
+                             f"instance ({dram_per_inst} B) x instances",
                      "hbm": {"achieved": eval_achieved, "peak": hbm_peak, "unit": "GB/s",
                              "frac": eval_achieved / hbm_peak, "peak_source": peak_src,
                              "algorithmic_bytes_per_instance": EVAL_BYTES_PER_INST}},

@@ -294,7 +294,7 @@ def transient_section(args):
     the learned warm start against the plain GPU path (Newton iterations per step)."""
     import torch
 
-    from tests.transient_oracle import OracleTransient
+    from oracle.transient import OracleTransient
     from xyce_b200 import Bsim3Device, MosfetDevice, netlist, surrogate as S
     from xyce_b200.transient import GpuTransient, NewtonParams
 
@@ -478,7 +478,7 @@ def cpu_baseline(args, omp=False, sample=None, min_seconds=10.0):
     """Reference CPU load (oracle library = the reference's own device code) on a bounded sample.
     Serial: the plain build (no libm interposer) when present; omp: the OpenMP build."""
     from oracle import xyce_ref as xr
-    from tests.parity import OracleRun
+    from oracle.run import OracleRun
 
     sample = sample or args.cpu_sample
     c, rowptr, colind = build_workload(sample, args.seed, args.wire_segments)

@@ -10,7 +10,8 @@ import numpy as np
 import scipy.sparse as sp
 import torch
 
-from tests.parity import OracleRun, family_inputs
+from oracle.run import OracleRun
+from xyce_b200.netlist import mosfet_family as family_inputs
 from xyce_b200.device import SolverFlags
 from xyce_b200.transient import TransientBase
 

@@ -79,7 +79,7 @@ def test_batched_sweep_transient_waveforms_match_per_circuit_oracle_runs():
     abstol 1e-12. Newton tolerances are tight, so the merged system's shared convergence test
     cannot show in the waveforms."""
     from tests.parity import family_inputs
-    from tests.transient_oracle import OracleTransient
+    from oracle.transient import OracleTransient
     from xyce_b200 import ModelCard
     from xyce_b200.transient import GpuTransient, NewtonParams
 

@@ -69,7 +69,7 @@ def test_placed_netlist_transient_refactorization_matches_oracle():
     """A placed (locality-wired) BSIM4 gate netlist: operating point from the logic-level starting
     iterate, then 0.3 ns on the GPU refactorization path, against the same driver on the oracle's
     loads with a host LU; waveforms within reltol 1e-3 / abstol 1e-12."""
-    from tests.transient_oracle import OracleTransient
+    from oracle.transient import OracleTransient
 
     c = netlist.random_logic(2500, seed=4, n_inputs=16, locality=64)
     tight = NewtonParams(max_iter=40, rhs_tol=1e-9, delta_x_tol=1e-3, abs_tol=1e-9, rel_tol=1e-6,

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 from tests.parity import family_inputs  # noqa: E402
-from tests.transient_oracle import OracleTransient  # noqa: E402
+from oracle.transient import OracleTransient  # noqa: E402
 
 # Tight Newton tolerances for the comparisons: both sides converge far below the waveform bound,
 # so differences in iteration counts cannot show up as waveform differences.

@@ -1600,16 +1600,21 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------
-// Fused load and combine. One Newton iterate's device load and the time-integration combine in
-// one pass over the CSR rows: the evaluation kernel stages the instances' stamps as usual, the
-// few entries with more than kLongThreshold contributions (supply rails) are summed by the chunked
-// gathers into the family's buffers, and one warp per row then forms, for every entry of the row,
-// the family's dF/dx and dQ/dx sum straight from the staged stamps (same sources, same order as
-// the gather kernels) and the Newton matrix entry from it, and for the row the family's F, Q and
-// limiter-vector sums and the residual, with the linear devices' terms, exactly as
-// tia_combine_kernel does from the family's stored sums. The family's dF/dx and dQ/dx are never
-// written to memory (except for the long entries) or read back; the results are bit-identical to
-// xd_load_assign followed by xd_tia_combine.
+// Fused load and combine. One Newton iterate's device load and the time-integration combine
+// without the family's dF/dx and dQ/dx in between: the evaluation kernel stages the instances'
+// stamps as usual, the few entries with more than kLongThreshold contributions (supply-rail
+// couplings) are summed by the chunked gathers into the family's buffers, then
+//   * fused_entry_kernel, a thread per CSR entry, forms the family's dF/dx and dQ/dx sum straight
+//     from the staged stamps (same sources, same order as the gather kernels) and the Newton matrix
+//     entry from it with the linear devices' terms;
+//   * fused_row_kernel, a warp per row, forms the row's F, Q and limiter-vector sums and the
+//     residual, with the linear devices' terms summed in tia_combine_kernel's order, and the
+//     diagonal entry again where a gmin shunt is on.
+// The family's dF/dx and dQ/dx are never written to memory (except for the long entries) or read
+// back; the results are bit-identical to xd_load_assign followed by xd_tia_combine. Entries are
+// independent work items, so a row of 10^5 entries (a supply rail) costs no more than 10^5 short
+// rows: one warp per row walking such a row's staged sources (an index, a source list, then the
+// stamps, three dependent loads per entry) took ~6 ms at 200k unknowns.
 
 int xd_tia_internal_pattern(const xd_tia *t, int *device, int *n_rows, int *nnz, const int **rowptr,
                             const int **colind);
@@ -1621,16 +1626,67 @@ struct xd_tia_fused {
   const int *d_rowptr = nullptr, *d_colind = nullptr;
   int2 *d_ent = nullptr;   // per CSR entry: (first source in the matrix map, count); count -1 = long entry
   int2 *d_vrow = nullptr;  // per row: (first source in the vector map, count); count -1 = long row
+  int *d_diag = nullptr;   // per row: position of its diagonal entry, or -1
 };
 
 namespace {
 
 constexpr int kFusedWarps = 8;
+constexpr int kEntryBlock = 256;
+
+// The family's dF/dx and dQ/dx of CSR entry k: its staged sources summed in the matrix map's
+// order (as gather_short_kernel sums them), or the chunked gathers' sum for a long entry.
+template <bool TRAN>
+__device__ __forceinline__ void fused_entry_sums(int k, const int2 *__restrict__ ent, const int *__restrict__ msrc,
+                                                 const double *__restrict__ stage, size_t mb_f, size_t mb_q,
+                                                 const double *__restrict__ long_dfdx,
+                                                 const double *__restrict__ long_dqdx, double &jf, double &jq) {
+  const int2 e = ent[k];
+  if (e.y < 0) {
+    jf = long_dfdx[k];
+    jq = TRAN ? long_dqdx[k] : 0.0;
+    return;
+  }
+  double sf = 0.0, sq = 0.0;
+  for (int s = e.x; s < e.x + e.y; ++s) {
+    const size_t src = (size_t)msrc[s];
+    sf += stage[mb_f + src];
+    if (TRAN) sq += stage[mb_q + src];
+  }
+  jf = sf;
+  jq = sq;
+}
+
+// Newton matrix entry from the family's sums and the linear devices' constants, in
+// tia_combine_kernel's operation order (the gmin shunt, on diagonals only, by the row kernel).
+template <bool TRAN>
+__device__ __forceinline__ double fused_matrix_entry(int k, double jf, double jq, double shunt, const xd_tia_coef &c,
+                                                     const double *__restrict__ lin_f,
+                                                     const double *__restrict__ lin_q) {
+  if (lin_f) jf += lin_f[k];
+  if (shunt != 0.0) jf += shunt;
+  if (!TRAN) return jf;
+  if (lin_q) jq += lin_q[k];
+  return c.qscale * jq + c.fscale * jf;
+}
 
 template <bool TRAN>
-__global__ void __launch_bounds__(32 * kFusedWarps) fused_combine_kernel(
-    int n_rows, const int *__restrict__ rowptr, const int *__restrict__ colind, xd_tia_coef c,
-    const double *__restrict__ x, const int2 *__restrict__ ent, const int *__restrict__ msrc,
+__global__ void __launch_bounds__(kEntryBlock) fused_entry_kernel(
+    int nnz, xd_tia_coef c, const int2 *__restrict__ ent, const int *__restrict__ msrc,
+    const double *__restrict__ stage, size_t mb_f, size_t mb_q, const double *__restrict__ long_dfdx,
+    const double *__restrict__ long_dqdx, const double *__restrict__ lin_f, const double *__restrict__ lin_q,
+    double *__restrict__ jac) {
+  const int k = blockIdx.x * kEntryBlock + threadIdx.x;
+  if (k >= nnz) return;
+  double jf, jq;
+  fused_entry_sums<TRAN>(k, ent, msrc, stage, mb_f, mb_q, long_dfdx, long_dqdx, jf, jq);
+  jac[k] = fused_matrix_entry<TRAN>(k, jf, jq, 0.0, c, lin_f, lin_q);
+}
+
+template <bool TRAN>
+__global__ void __launch_bounds__(32 * kFusedWarps) fused_row_kernel(
+    int n_rows, const int *__restrict__ rowptr, const int *__restrict__ colind, const int *__restrict__ diag,
+    xd_tia_coef c, const double *__restrict__ x, const int2 *__restrict__ ent, const int *__restrict__ msrc,
     const int2 *__restrict__ vrow, const int *__restrict__ vsrc, const double *__restrict__ stage, size_t mb_f,
     size_t mb_q, size_t vb0, size_t vb1, size_t vb2, size_t vb3, const double *__restrict__ long_dfdx,
     const double *__restrict__ long_dqdx, double *__restrict__ fam_f, double *__restrict__ fam_q,
@@ -1642,42 +1698,14 @@ __global__ void __launch_bounds__(32 * kFusedWarps) fused_combine_kernel(
   const int lane = threadIdx.x & 31;
   if (row >= n_rows) return;
   const int beg = rowptr[row], end = rowptr[row + 1];
+  // The linear devices' currents and charges of the row, lane-strided then a shuffle tree, as
+  // tia_combine_kernel sums them.
   double af = 0.0, aq = 0.0;
-  bool has_diag = false;
-  for (int k = beg + lane; k < end; k += 32) {
-    const int2 e = ent[k];
-    double jf, jq = 0.0;
-    if (e.y < 0) {
-      jf = long_dfdx[k];
-      if (TRAN) jq = long_dqdx[k];
-    } else {
-      double sf = 0.0, sq = 0.0;
-      for (int s = e.x; s < e.x + e.y; ++s) {
-        const size_t src = (size_t)msrc[s];
-        sf += stage[mb_f + src];
-        if (TRAN) sq += stage[mb_q + src];
-      }
-      jf = sf;
-      jq = sq;
-    }
-    if (lin_f) {
-      const double g = lin_f[k];
-      jf += g;
-      af += g * x[colind[k]];
-    }
-    if (c.gshunt != 0.0 && colind[k] == row) {
-      jf += c.gshunt;
-      has_diag = true;
-    }
-    if (TRAN) {
-      if (lin_q) {
-        const double cq = lin_q[k];
-        jq += cq;
-        aq += cq * x[colind[k]];
-      }
-      jac[k] = c.qscale * jq + c.fscale * jf;
-    } else {
-      jac[k] = jf;
+  if (lin_f || (TRAN && lin_q)) {
+    for (int k = beg + lane; k < end; k += 32) {
+      const double xc = x[colind[k]];
+      if (lin_f) af += lin_f[k] * xc;
+      if (TRAN && lin_q) aq += lin_q[k] * xc;
     }
   }
 #pragma unroll
@@ -1685,58 +1713,64 @@ __global__ void __launch_bounds__(32 * kFusedWarps) fused_combine_kernel(
     af += __shfl_down_sync(0xffffffffu, af, w);
     aq += __shfl_down_sync(0xffffffffu, aq, w);
   }
-  has_diag = __any_sync(0xffffffffu, has_diag);
-  if (lane == 0) {
-    // The family's vector sums for the row (the vector gather's order), kept in its buffers.
-    const int2 v = vrow[row];
-    double ff, fq, ffx, fqx;
-    if (v.y < 0) {
+  if (lane != 0) return;
+  // The shunt goes on rows whose diagonal is in the pattern (the node rows): F and J together.
+  const int dk = diag[row];
+  const bool has_diag = c.gshunt != 0.0 && dk >= 0;
+  if (has_diag) {
+    double jf, jq;
+    fused_entry_sums<TRAN>(dk, ent, msrc, stage, mb_f, mb_q, long_dfdx, long_dqdx, jf, jq);
+    jac[dk] = fused_matrix_entry<TRAN>(dk, jf, jq, c.gshunt, c, lin_f, lin_q);
+  }
+  // The family's vector sums for the row (the vector gather's order), kept in its buffers.
+  const int2 v = vrow[row];
+  double ff, fq, ffx, fqx;
+  if (v.y < 0) {
+    ff = fam_f[row];
+    fq = fam_q[row];
+    ffx = fam_fx[row];
+    fqx = fam_qx[row];
+  } else {
+    ff = fq = ffx = fqx = 0.0;
+    for (int s = v.x; s < v.x + v.y; ++s) {
+      const size_t src = (size_t)vsrc[s];
+      ff += stage[vb0 + src];
+      fq += stage[vb1 + src];
+      ffx += stage[vb2 + src];
+      fqx += stage[vb3 + src];
+    }
+    if (v.y > 0) {
+      fam_f[row] = ff;
+      fam_q[row] = fq;
+      fam_fx[row] = ffx;
+      fam_qx[row] = fqx;
+    } else {
+      // A row the family does not stamp: its buffers keep their (zero) values, as with the
+      // assigning load.
       ff = fam_f[row];
       fq = fam_q[row];
       ffx = fam_fx[row];
       fqx = fam_qx[row];
-    } else {
-      ff = fq = ffx = fqx = 0.0;
-      for (int s = v.x; s < v.x + v.y; ++s) {
-        const size_t src = (size_t)vsrc[s];
-        ff += stage[vb0 + src];
-        fq += stage[vb1 + src];
-        ffx += stage[vb2 + src];
-        fqx += stage[vb3 + src];
-      }
-      if (v.y > 0) {
-        fam_f[row] = ff;
-        fam_q[row] = fq;
-        fam_fx[row] = ffx;
-        fam_qx[row] = fqx;
-      } else {
-        // A row the family does not stamp: its buffers keep their (zero) values, as with the
-        // assigning load.
-        ff = fam_f[row];
-        fq = fam_q[row];
-        ffx = fam_fx[row];
-        fqx = fam_qx[row];
-      }
     }
-    double F = ff + af;
-    if (has_diag) F += c.gshunt * x[row];
-    if (b) F -= b[row];
-    if (f_tot) f_tot[row] = F;
-    if (!TRAN) {
-      double r = -F;
-      if (limiter) r = r + ffx;
-      rhs[row] = r;
-      return;
-    }
-    const double Q = fq + aq;
-    if (q_tot) q_tot[row] = Q;
-    double r = (Q - qn0[row]) * c.inv_h + c.fscale * F;
-    if (c.hist_scale != 0.0) r = r + c.hist_scale * fhist[row];
-    r = -r;
-    if (limiter) r = r + c.qscale * fqx;
-    if (limiter) r = r + c.fscale * ffx;
-    rhs[row] = r;
   }
+  double F = ff + af;
+  if (has_diag) F += c.gshunt * x[row];
+  if (b) F -= b[row];
+  if (f_tot) f_tot[row] = F;
+  if (!TRAN) {
+    double r = -F;
+    if (limiter) r = r + ffx;
+    rhs[row] = r;
+    return;
+  }
+  const double Q = fq + aq;
+  if (q_tot) q_tot[row] = Q;
+  double r = (Q - qn0[row]) * c.inv_h + c.fscale * F;
+  if (c.hist_scale != 0.0) r = r + c.hist_scale * fhist[row];
+  r = -r;
+  if (limiter) r = r + c.qscale * fqx;
+  if (limiter) r = r + c.fscale * ffx;
+  rhs[row] = r;
 }
 
 // Per-target (first source, count) of a gather map over n_targets outputs: short targets get
@@ -1772,6 +1806,16 @@ int xd_tia_fused_create(xd_tia *tia, xd_ctx *fam, xd_tia_fused **out) {
   std::vector<int2> ent, vrow;
   if ((rc = map_ranges(fam->mmap, nnz, ent)) != 0) return rc;
   if ((rc = map_ranges(fam->vmap, n_rows, vrow)) != 0) return rc;
+  // Each row's diagonal position (the gmin shunt's entry), from the pattern.
+  std::vector<int> hp((size_t)n_rows + 1), hc((size_t)nnz), dpos((size_t)n_rows, -1);
+  XD_CUDA(cudaMemcpy(hp.data(), rowptr, hp.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  if (nnz > 0) XD_CUDA(cudaMemcpy(hc.data(), colind, hc.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int r = 0; r < n_rows; ++r)
+    for (int k = hp[r]; k < hp[r + 1]; ++k)
+      if (hc[k] == r) {
+        dpos[r] = k;
+        break;
+      }
   xd_tia_fused *f = new xd_tia_fused();
   f->tia = tia;
   f->fam = fam;
@@ -1784,9 +1828,12 @@ int xd_tia_fused_create(xd_tia *tia, xd_ctx *fam, xd_tia_fused **out) {
   if ((ce = cudaMalloc(&f->d_ent, std::max<size_t>(1, ent.size()) * sizeof(int2))) != cudaSuccess ||
       (ce = cudaMemcpy(f->d_ent, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (ce = cudaMalloc(&f->d_vrow, std::max<size_t>(1, vrow.size()) * sizeof(int2))) != cudaSuccess ||
-      (ce = cudaMemcpy(f->d_vrow, vrow.data(), vrow.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess) {
+      (ce = cudaMemcpy(f->d_vrow, vrow.data(), vrow.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMalloc(&f->d_diag, std::max<size_t>(1, dpos.size()) * sizeof(int))) != cudaSuccess ||
+      (ce = cudaMemcpy(f->d_diag, dpos.data(), dpos.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
     cudaFree(f->d_ent);
     cudaFree(f->d_vrow);
+    cudaFree(f->d_diag);
     delete f;
     return cuda_fail(ce, "xd_tia_fused_create allocation");
   }
@@ -1799,6 +1846,7 @@ int xd_tia_fused_destroy(xd_tia_fused *f) {
   DeviceGuard g(f->device);
   cudaFree(f->d_ent);
   cudaFree(f->d_vrow);
+  cudaFree(f->d_diag);
   delete f;
   return 0;
 }
@@ -1829,18 +1877,27 @@ int xd_tia_load_combine(xd_tia_fused *fu, const xd_flags *flags, const xd_tia_co
     OutSet<2, false> ms{{d_fam_dfdx, d_fam_dqdx}, {mb, mb + mm}, 1};
     if ((rc = run_gather(ctx->mmap, ctx->d_stage, ms, st, false))) return rc;
   }
-  const int blocks = (fu->n_rows + kFusedWarps - 1) / kFusedWarps;
-#define XD_FUSED_ARGS                                                                                               \
-  fu->n_rows, fu->d_rowptr, fu->d_colind, *coef, d_x, fu->d_ent, ctx->mmap.d_src, fu->d_vrow, ctx->vmap.d_src,      \
-      ctx->d_stage, mb, mb + mm, (size_t)0, r * n, 2 * r * n, 3 * r * n, d_fam_dfdx, d_fam_dqdx, d_fam_f, d_fam_q,  \
-      d_fam_fx, d_fam_qx, d_lin_dfdx, d_lin_dqdx, limiter, d_b, d_qn0, d_fhist, d_jac, d_rhs, d_q_tot, d_f_tot
-  if (coef->mode != 0)
-    fused_combine_kernel<true><<<blocks, 32 * kFusedWarps, 0, st>>>(XD_FUSED_ARGS);
-  else
-    fused_combine_kernel<false><<<blocks, 32 * kFusedWarps, 0, st>>>(XD_FUSED_ARGS);
-#undef XD_FUSED_ARGS
+  const int row_blocks = (fu->n_rows + kFusedWarps - 1) / kFusedWarps;
+  const int ent_blocks = (fu->nnz + kEntryBlock - 1) / kEntryBlock;
+#define XD_ENTRY_ARGS                                                                                               \
+  fu->nnz, *coef, fu->d_ent, ctx->mmap.d_src, ctx->d_stage, mb, mb + mm, d_fam_dfdx, d_fam_dqdx, d_lin_dfdx,         \
+      d_lin_dqdx, d_jac
+#define XD_ROW_ARGS                                                                                                 \
+  fu->n_rows, fu->d_rowptr, fu->d_colind, fu->d_diag, *coef, d_x, fu->d_ent, ctx->mmap.d_src, fu->d_vrow,            \
+      ctx->vmap.d_src, ctx->d_stage, mb, mb + mm, (size_t)0, r * n, 2 * r * n, 3 * r * n, d_fam_dfdx, d_fam_dqdx,    \
+      d_fam_f, d_fam_q, d_fam_fx, d_fam_qx, d_lin_dfdx, d_lin_dqdx, limiter, d_b, d_qn0, d_fhist, d_jac, d_rhs,      \
+      d_q_tot, d_f_tot
+  if (coef->mode != 0) {
+    if (ent_blocks > 0) fused_entry_kernel<true><<<ent_blocks, kEntryBlock, 0, st>>>(XD_ENTRY_ARGS);
+    fused_row_kernel<true><<<row_blocks, 32 * kFusedWarps, 0, st>>>(XD_ROW_ARGS);
+  } else {
+    if (ent_blocks > 0) fused_entry_kernel<false><<<ent_blocks, kEntryBlock, 0, st>>>(XD_ENTRY_ARGS);
+    fused_row_kernel<false><<<row_blocks, 32 * kFusedWarps, 0, st>>>(XD_ROW_ARGS);
+  }
+#undef XD_ENTRY_ARGS
+#undef XD_ROW_ARGS
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "fused_combine_kernel launch");
+  if (e != cudaSuccess) return cuda_fail(e, "fused load-and-combine launch");
   return 0;
 }
 

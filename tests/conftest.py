@@ -42,11 +42,13 @@ def pytest_terminal_summary(terminalreporter):
     rows = []
     terminalreporter.write_sep("-", "parity: entries within plain 1e-12 relative (rest needed a floor)")
     for test, strict in log:
-        for key, (tot, ok, idx) in sorted(strict.items()):
+        for key, (tot, ok, idx, cls) in sorted(strict.items()):
             rows.append({"test": test, "output": key, "entries": tot, "strict": ok, "needed_floor": tot - ok,
-                         "fraction_needed_floor": (tot - ok) / max(1, tot), "first_floor_indices": idx})
+                         "fraction_needed_floor": (tot - ok) / max(1, tot), "first_floor_indices": idx,
+                         "floor_needed": {"summation_order": cls[0], "cancellation": cls[1], "libm_ulp": cls[2]}})
             terminalreporter.write_line(f"{test} {key}: {ok}/{tot} strict, {tot - ok} needed a floor "
-                                        f"({(tot - ok) / max(1, tot):.2e})")
+                                        f"({(tot - ok) / max(1, tot):.2e}; summation order {cls[0]}, "
+                                        f"cancellation {cls[1]}, libm ulp {cls[2]})")
     path = os.environ.get("PARITY_REPORT")
     if path:
         with open(path, "w") as f:

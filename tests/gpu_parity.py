@@ -4,7 +4,8 @@ import os
 import numpy as np
 import torch
 
-from tests.parity import ABS_SUM_FLOOR, RTOL, OracleRun, compare, family_inputs, row_max, strict_split
+from tests.parity import (ABS_SUM_FLOOR, RTOL, OracleRun, compare, family_inputs, floor_classes, row_max,
+                          strict_split)
 from xyce_b200 import MosfetDevice, netlist
 
 
@@ -50,17 +51,20 @@ def log_strict(strict):
 STORE_WRITTEN = {14: [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13], 9: [0, 1, 2, 3, 4], 1: [0, 1, 2, 3, 4]}
 
 
-def _tally(strict, key, got, ref):
+def _tally(strict, key, got, ref, classes=(0, 0, 0)):
     """Adds (entries, entries within plain 1e-12 relative) of one output to `strict`, a dict of
-    [entries, strict passes, first few indices that needed a floor]."""
+    [entries, strict passes, first few indices that needed a floor, [summation-order,
+    cancellation, libm-ulp] counts of the floors those entries needed (tests.parity.floor_classes)]."""
     if strict is None:
         return
     tot, ok, idx = strict_split(got, ref)
-    t = strict.setdefault(key, [0, 0, []])
+    t = strict.setdefault(key, [0, 0, [], [0, 0, 0]])
     t[0] += tot
     t[1] += ok
     if len(t[2]) < 8:
         t[2].extend(int(i) for i in idx[:8 - len(t[2])])
+    for j in range(3):
+        t[3][j] += classes[j]
 
 
 def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=3, n_sto=14, vspan=None,
@@ -77,19 +81,18 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
         if vspan is not None and rowptr is not None and k in ("dfdxdvp", "dqdxdvp"):
             m = "dfdx" if k == "dfdxdvp" else "dqdx"
             vec_scale = vspan * np.maximum(row_max(rowptr, r[m]), row_max(rowptr, g[m]))
-        bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR,
-                             rowptr=rowptr if k in ("dfdx", "dqdx") else None, detail=detail,
-                             sens=r["sens"][k] if "sens" in r else None, vec_scale=vec_scale,
-                             nterms=None if counts is None else counts.get(k))
+        kw = dict(rowptr=rowptr if k in ("dfdx", "dqdx") else None, sens=r["sens"][k] if "sens" in r else None,
+                  vec_scale=vec_scale, nterms=None if counts is None else counts.get(k))
+        bad, worst = compare(k, g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR, detail=detail, **kw)
         report[k] = worst
-        _tally(strict, k, g[k], r[k])
+        _tally(strict, k, g[k], r[k], floor_classes(g[k], r[k], g["abs"][k], RTOL, ABS_SUM_FLOOR, **kw))
         assert bad == 0, (f"step {step} {flags}: {k} has {bad} entries out of tolerance (worst {worst:.3g}x); "
                           f"(name, index, gpu, ref, allowed): {detail}")
     gs = g["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]]
     rs = r["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]]
     ss = r["sens"]["next_sto"].reshape(n_sto, n)[STORE_WRITTEN[level]] if "sens" in r else None
     bad, worst = compare("sto", gs, rs, sens=ss)
-    _tally(strict, "next_sto", gs, rs)
+    _tally(strict, "next_sto", gs, rs, floor_classes(gs, rs, sens=ss))
     assert bad == 0, f"step {step}: store out of tolerance ({worst:.3g}x)"
     if charges:
         # Charges are sums of cancelling terms: the floor is 1e-14 of the instance's largest charge.
@@ -99,7 +102,10 @@ def check_step(step, flags, g, r, n, charges=True, rowptr=None, level=14, n_sta=
                              np.broadcast_to(scale, (n_sta, n)), RTOL, ABS_SUM_FLOOR, detail=detail,
                              sens=r["sens"]["next_sta"].reshape(n_sta, n) if "sens" in r else None)
         report["sta"] = worst
-        _tally(strict, "next_sta", g["next_sta"], r["next_sta"])
+        _tally(strict, "next_sta", g["next_sta"], r["next_sta"],
+               floor_classes(g["next_sta"].reshape(n_sta, n), r["next_sta"].reshape(n_sta, n),
+                             np.broadcast_to(scale, (n_sta, n)), RTOL, ABS_SUM_FLOOR,
+                             sens=r["sens"]["next_sta"].reshape(n_sta, n) if "sens" in r else None))
         assert bad == 0, f"step {step}: state out of tolerance ({worst:.3g}x): {detail}"
         if level in (9, 14) and flags.init_tran and flags.newton_iter == 0 and not flags.dcop:
             assert np.allclose(g["curr_sta"], g["next_sta"], rtol=0, atol=0)
@@ -145,3 +151,18 @@ def run_sequence(c, cards, seqs, vrange=(0.0, 1.2), seed=0, extra_params=None, c
     return worst
 
 
+
+
+# Waveform comparison. RELTOL is the configs' transient reltol; VNTOL the reference's default node
+# voltage tolerance (the absolute part of its per-point Newton weights, N_NLS_NLParams.C).
+WAVE_RELTOL, WAVE_VNTOL = 1e-3, 1e-6
+
+
+def waveform_errors(wg, wo):
+    """Worst error of waveforms wg against wo (points x nodes) as fractions of two bounds: per node,
+    reltol times the node's largest magnitude over the window; per point, reltol times the larger
+    of the two values there plus VNTOL. Both must be at most 1."""
+    err = np.abs(wg - wo)
+    scaled = float((err / (WAVE_RELTOL * np.abs(wo).max(axis=0, keepdims=True) + 1e-12)).max())
+    point = float((err / (WAVE_RELTOL * np.maximum(np.abs(wg), np.abs(wo)) + WAVE_VNTOL)).max())
+    return scaled, point

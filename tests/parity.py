@@ -80,6 +80,40 @@ def strict_split(got, ref, rtol=RTOL):
     return int(ok.size), int(np.count_nonzero(ok)), np.flatnonzero(~ok)
 
 
+def _allowances(got, ref, abs_sum, rtol, floor, rowptr, sens, vec_scale, nterms):
+    """compare()'s allowed error per entry, cumulatively by floor: plain relative; + the abs-sum
+    (summation-order) floor; + the row / vector-scale (cancellation) floor; + the libm sensitivity."""
+    a0 = rtol * np.maximum(np.abs(got), np.abs(ref))
+    a1 = a0
+    if abs_sum is not None:
+        fl = floor
+        if nterms is not None:
+            fl = np.maximum(floor, 2.0 * np.maximum(np.asarray(nterms, dtype=np.float64) - 1.0, 0.0) * 2.0 ** -53)
+        a1 = a1 + fl * np.asarray(abs_sum)
+    a2 = a1
+    if rowptr is not None:
+        a2 = a2 + ROW_FLOOR * row_scale(rowptr, got, ref)
+    if vec_scale is not None:
+        a2 = a2 + ROW_FLOOR * np.asarray(vec_scale)
+    a3 = a2
+    if sens is not None:
+        a3 = a3 + SENS_FACTOR * np.asarray(sens).reshape(a3.shape)
+    return a0, a1, a2, a3
+
+
+def floor_classes(got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, sens=None, vec_scale=None,
+                  nterms=None):
+    """Of the entries outside plain rtol relative: how many pass once the abs-sum floor is added
+    (summation order), how many need the row / vector-scale floor too (cancellation residue), and
+    how many the libm sensitivity as well (one-ulp conditioning)."""
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    d = np.abs(got - ref)
+    a0, a1, a2, a3 = _allowances(got, ref, abs_sum, rtol, floor, rowptr, sens, vec_scale, nterms)
+    return (int(np.count_nonzero((d > a0) & (d <= a1))), int(np.count_nonzero((d > a1) & (d <= a2))),
+            int(np.count_nonzero((d > a2) & (d <= a3))))
+
+
 def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr=None, detail=None, sens=None,
             vec_scale=None, nterms=None):
     """Returns (n_bad, worst ratio of |diff| to the allowed error). With rowptr (CSR values), adds
@@ -92,18 +126,7 @@ def compare(name, got, ref, abs_sum=None, rtol=RTOL, floor=ABS_SUM_FLOOR, rowptr
     got = np.asarray(got)
     ref = np.asarray(ref)
     d = np.abs(got - ref)
-    allow = rtol * np.maximum(np.abs(got), np.abs(ref))
-    if abs_sum is not None:
-        fl = floor
-        if nterms is not None:
-            fl = np.maximum(floor, 2.0 * np.maximum(np.asarray(nterms, dtype=np.float64) - 1.0, 0.0) * 2.0 ** -53)
-        allow = allow + fl * np.asarray(abs_sum)
-    if rowptr is not None:
-        allow = allow + ROW_FLOOR * row_scale(rowptr, got, ref)
-    if vec_scale is not None:
-        allow = allow + ROW_FLOOR * np.asarray(vec_scale)
-    if sens is not None:
-        allow = allow + SENS_FACTOR * np.asarray(sens).reshape(allow.shape)
+    allow = _allowances(got, ref, abs_sum, rtol, floor, rowptr, sens, vec_scale, nterms)[3]
     allow = np.maximum(allow, 1e-300)
     ratio = d / allow
     bad = int(np.count_nonzero(d > allow))

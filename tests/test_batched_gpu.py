@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-from tests.gpu_parity import GpuRun, check_step  # noqa: E402
+from tests.gpu_parity import GpuRun, check_step, waveform_errors  # noqa: E402
 from tests.parity import OracleRun  # noqa: E402
 
 
@@ -109,8 +109,7 @@ def test_batched_sweep_transient_waveforms_match_per_circuit_oracle_runs():
         to, wo = o.run(0.8e-9, 10e-12, params=tight, record=np.arange(ck.n_nodes))
         assert np.array_equal(tg, to)
         mine = wg[:, b.node_offset[k]:b.node_offset[k + 1]]
-        bound = 1e-3 * np.abs(wo).max(axis=0, keepdims=True) + 1e-12
-        worst[k] = float((np.abs(mine - wo) / bound).max())
-        assert worst[k] <= 1.0, (k, worst[k])
+        worst[k], point = waveform_errors(mine, wo)
+        assert worst[k] <= 1.0 and point <= 1.0, (k, worst[k], point)
         assert (wo.max(0) - wo.min(0)).max() > 0.5  # inputs switch inside the window
     print("batched sweep: worst waveform error / bound per circuit", worst)

@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
+from tests.gpu_parity import waveform_errors  # noqa: E402
 from tests.parity import family_inputs  # noqa: E402
 
 
@@ -86,11 +87,10 @@ def test_placed_netlist_transient_refactorization_matches_oracle():
         waves.append(s.run(0.3e-9, 10e-12, params=tight, record=rec))
     (tg, wg), (to, wo) = waves
     assert np.array_equal(tg, to)
-    bound = 1e-3 * np.abs(wo).max(axis=0, keepdims=True) + 1e-12
-    worst = float((np.abs(wg - wo) / bound).max())
-    assert worst <= 1.0, worst
+    worst, point = waveform_errors(wg, wo)
+    assert worst <= 1.0 and point <= 1.0, (worst, point)
     assert g.stats.host_factorizations < g.stats.factorizations // 4, g.stats
-    print("placed netlist: worst error / bound", worst, "host factorizations", g.stats.host_factorizations,
+    print("placed netlist: worst error / bound", worst, "per point", point, "host factorizations", g.stats.host_factorizations,
           "of", g.stats.factorizations)
     g.close()
     fam.close()

@@ -67,8 +67,9 @@ def test_oracle_parity_at_benchmark_size(case):
     dev.close()
     log_strict(strict)
     print(f"{case}: {n} instances, evaluation variant {variant}, worst error / tolerance {worst}")
-    for key, (tot, ok, idx) in strict.items():
+    for key, (tot, ok, idx, cls) in strict.items():
         frac = (tot - ok) / max(1, tot)
-        print(f"  {key}: {ok}/{tot} within plain 1e-12 relative, {tot - ok} needed a floor ({frac:.2e})")
+        print(f"  {key}: {ok}/{tot} within plain 1e-12 relative, {tot - ok} needed a floor ({frac:.2e}: "
+              f"summation order {cls[0]}, cancellation {cls[1]}, libm ulp {cls[2]})")
         limit = MAX_FLOOR_FRACTION.get(key, DEFAULT_MAX_FLOOR_FRACTION)
         assert frac <= limit, f"{key}: {frac:.3g} of the entries needed a tolerance floor"

@@ -84,18 +84,19 @@ typedef struct xd_mosfet_family {
                                             or -1 where the node collapses onto D / S; null if
                                             no instance has one (see xd_internal_nodes)        */
   const int *inst_internal_gen;          /* BSIM4 general topology: [XD_GEN_INTERNAL*n_inst]
-                                            the unknowns of D', S', G', GM, B', SB, DB, IBS,
-                                            IDS, IGS per instance, -1 where absent (see
+                                            the unknowns of D', S', G', GM, B', SB, DB, Q,
+                                            IBS, IDS, IGS per instance, -1 where absent (see
                                             xd_internal_nodes_gen); null otherwise. Required
-                                            when the cards use rgateMod, rbodyMod, rdsMod 1 or
-                                            instance ICs; then inst_internal must be null      */
+                                            when the cards use rgateMod, rbodyMod, rdsMod 1,
+                                            trnqsMod 1 or instance ICs; then inst_internal
+                                            must be null                                      */
 } xd_mosfet_family;
 
 /* Internal variables per instance of the BSIM4 general topology, in the reference's registerLIDs
- * order (N_DEV_MOSFET_B4.C:5018-5075): drain', source', gate' (rgateMod 1-3), gate-mid (rgateMod 3),
- * body', source-body, drain-body (rbodyMod 1/2), then the branch currents of the initial
- * conditions IC3 = VBS, IC1 = VDS, IC2 = VGS. */
-#define XD_GEN_INTERNAL 10
+ * order (N_DEV_MOSFET_B4.C:5018-5099): drain', source', gate' (rgateMod 1-3), gate-mid (rgateMod 3),
+ * body', source-body, drain-body (rbodyMod 1/2), the NQS charge (trnqsMod 1), then the branch
+ * currents of the initial conditions IC3 = VBS, IC1 = VDS, IC2 = VGS. */
+#define XD_GEN_INTERNAL 11
 
 /* Jacobian sparsity pattern over the unknowns (host memory, read during xd_create only).
  * Column indices must be sorted within each row and must include every entry the family's
@@ -131,9 +132,10 @@ int xd_internal_nodes(const xd_mosfet_family *family, int *flags);
 int xd_internal_nodes_gen(const xd_mosfet_family *family, int *flags);
 
 /* The general topology's stamp: rows[k], cols[k] (local nodes D=0, G, S, B, D', S', G', GM, B', SB,
- * DB, IBS, IDS, IGS = 13) of its 77 Jacobian entries, in the reference's jacStamp order
- * (N_DEV_MOSFET_B4.C:4641-4795); returns the count. The pattern must hold every entry whose two
- * nodes are unknowns after collapsing. Host-only. */
+ * DB, Q, IBS, IDS, IGS = 14) of its 85 Jacobian entries, in the reference's jacStamp order
+ * (N_DEV_MOSFET_B4.C:4641-4795) with the charge node's columns of rows D', S', G' last; returns the
+ * count. The pattern must hold every entry whose two nodes are unknowns after collapsing.
+ * Host-only. */
 int xd_general_stamp(int *rows, int *cols);
 
 /* Releases all device memory of the context. */
@@ -143,9 +145,10 @@ int xd_destroy(xd_ctx *ctx);
 const char *xd_last_error(void);
 
 int xd_num_instances(const xd_ctx *ctx);
-int xd_num_state_slots(const xd_ctx *ctx); /* per instance: 3 for BSIM4 (qb, qg, qd); 6 with the
-                                              general topology (then qgmid, qbs, qbd, zero where
-                                              the instance has no such charge)                  */
+int xd_num_state_slots(const xd_ctx *ctx); /* per instance: 3 for BSIM4 (qb, qg, qd); 8 with the
+                                              general topology (then qgmid, qbs, qbd, qcheq,
+                                              qcdump, zero where the instance has no such
+                                              charge)                                           */
 int xd_num_store_slots(const xd_ctx *ctx); /* per instance: 14 for BSIM4 */
 
 /* Evaluates every instance at the solution d_sol. Reads the previous iterate's limited
@@ -200,11 +203,11 @@ int xd_load_abs(xd_ctx *ctx, double *d_f, double *d_q, double *d_dfdxdvp, double
  * as 4x4 row-major terminal blocks. A family with internal drain / source nodes has the wide
  * layout, [68 * n_inst]: each vector takes 6 rows (D', G, S', B, then the external D and S,
  * F only), dF/dx and dQ/dx take 22 slots each (the 4x4 block on D', G, S', B, then (D', D),
- * (D, D'), (D, D), (S', S), (S, S'), (S, S)). The general topology's layout is [210 * n_inst]:
- * each vector 14 rows (the local nodes of xd_general_stamp), then dF/dx and dQ/dx over its 77
+ * (D, D'), (D, D), (S', S), (S, S'), (S, S)). The general topology's layout is [230 * n_inst]:
+ * each vector 15 rows (the local nodes of xd_general_stamp), then dF/dx and dQ/dx over its 85
  * stamp slots. xd_num_stage_slots gives the count. Synchronises the stream. */
 int xd_copy_stamps(xd_ctx *ctx, double *h_out, void *stream);
-int xd_num_stage_slots(const xd_ctx *ctx); /* staged values per instance: 48, 68 or 210 */
+int xd_num_stage_slots(const xd_ctx *ctx); /* staged values per instance: 48, 68 or 230 */
 
 /* Diagnostics. xd_launches_per_load: kernels one xd_load enqueues (eval + gathers).
  * xd_probe_fp64_fma: runs `blocks` x 256 threads, each doing `iters` x 64 independent-chain

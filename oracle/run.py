@@ -89,16 +89,18 @@ class OracleRun:
         self.n_sto_slots = self.ref.n_store // max(1, n)
         # sta_off[s, i]: the oracle's state entry of product slot s of instance i (-1: none).
         self.sta_off = self.sta_base[None, :] + np.arange(self.n_sta_slots)[:, None]
-        if c.mos_internal is not None and c.mos_internal.shape[1] == 10:
-            # General topology: the product keeps (qb, qg, qd, qgmid, qbs, qbd); an instance
-            # registers qgmid only with rgateMod 3 and qbs / qbd only with rbodyMod
-            # (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5225).
+        if c.mos_internal is not None and c.mos_internal.shape[1] == netlist.GEN_NODES - 4:
+            # General topology: the product keeps (qb, qg, qd, qgmid, qbs, qbd, qcheq, qcdump); an
+            # instance registers qgmid only with rgateMod 3, qbs / qbd only with rbodyMod and
+            # qcheq / qcdump only with trnqsMod (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5238).
             rg3 = (c.mos_internal[:, 3] >= 0).astype(np.int64)
             rb = c.mos_internal[:, 4] >= 0
-            self.n_sta_slots = 6
+            nq = c.mos_internal[:, 7] >= 0
+            self.n_sta_slots = 8
             b = self.sta_base
+            q0 = b + 3 + rg3 + 2 * rb.astype(np.int64)
             self.sta_off = np.stack([b, b + 1, b + 2, np.where(rg3 == 1, b + 3, -1), np.where(rb, b + 3 + rg3, -1),
-                                     np.where(rb, b + 4 + rg3, -1)])
+                                     np.where(rb, b + 4 + rg3, -1), np.where(nq, q0, -1), np.where(nq, q0 + 1, -1)])
 
     def to_aos_sto(self, soa):
         """Product slot-major store block -> oracle per-instance layout."""

@@ -10,8 +10,8 @@ on the binding, which runs them through libxyce_b200.so. The outputs, in the ref
 vectors and matrices, must equal the product's direct C-ABI load bit for bit (the binding only
 permutes and adds into zeroed outputs) and match the reference's CPU load within the parity
 tolerance, over a transient and DC flag sequence with limiting active, with and without internal
-drain / source nodes, and with the general topology (gate and body resistance, rdsMod 1, instance
-initial conditions).
+drain / source nodes, and with the general topology (gate and body resistance, rdsMod 1, the NQS
+charge node, instance initial conditions).
 """
 import numpy as np
 import pytest
@@ -43,7 +43,7 @@ def test_reference_device_loop_through_gpu_binding(topology):
         extra = {"NRD": np.full(n, 2.0), "NRS": np.where(np.arange(n) % 3 == 0, np.nan, 1.5)}
     elif topology == "general":
         cards = [ModelCard(False, {"RGATEMOD": 3, "RBODYMOD": 1, "RDSMOD": 1, "RSH": 20.0}),
-                 ModelCard(True, {"RGATEMOD": 1, "RBODYMOD": 2, "RBPS0": 60.0, "RBPD0": 70.0})]
+                 ModelCard(True, {"RGATEMOD": 1, "RBODYMOD": 2, "RBPS0": 60.0, "RBPD0": 70.0, "TRNQSMOD": 1})]
         # Initial conditions on NMOS instances (drain / source nodes exist: the reference places the
         # couplings in the branch currents' columns there).
         ic = (np.arange(n) % 9 == 0) & (c.mos_type == netlist.NMOS)

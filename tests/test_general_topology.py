@@ -1,8 +1,10 @@
 """BSIM4's general topology: gate resistance (rgateMod 1-3), the body resistance network (rbodyMod
-1/2), bias-dependent source / drain resistance (rdsMod 1) and instance initial conditions (IC1-3),
-each with the internal nodes and branch currents the reference gives it
-(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C: nodes :3684-3769, registerLIDs :4996-5075,
-jacStamp :4641-4795, the loads :16303-16853 and :17102-17172).
+1/2), bias-dependent source / drain resistance (rdsMod 1), the transient NQS charge model
+(trnqsMod 1: a charge node, the charge partition by qdrn / qcheq) and instance initial conditions
+(IC1-3), each with the internal nodes and branch currents the reference gives it
+(src/DeviceModelPKG/OpenModels/src/N_DEV_MOSFET_B4.C: nodes :3684-3769, registerLIDs :4996-5099,
+jacStamp :4641-4795, NQS :11626-11637, 12616-13045, 12216-12322, the loads :16303-16853 and
+:17102-17187).
 
 CPU: the library's stamp table and topology query against the reference's own instances (the
 oracle library): the same internal variables per instance, numbered the same way, and a pattern
@@ -42,11 +44,21 @@ CASES = {
     "mixed": [ModelCard(False, {"RGATEMOD": 3, "RBODYMOD": 1, "RDSMOD": 1, "IGCMOD": 1, "RDW": 60.0, "RSW": 70.0,
                                 **_RS}),
               ModelCard(True, {"RGATEMOD": 2, "RBODYMOD": 2, "CAPMOD": 0, **BODY5})],
+    "nqs": [ModelCard(False, {"TRNQSMOD": 1}), ModelCard(True, {"TRNQSMOD": 1, "XRCRG1": 10.0, "XPART": 0.5})],
+    # NQS with the gate-resistance modes that scale gcrg in place (the NQS conductances take the
+    # unscaled values) and with the body network's extra state slots before the NQS ones.
+    "nqs_rgate": [ModelCard(False, {"TRNQSMOD": 1, "RGATEMOD": 2, "XPART": 1.0}),
+                  ModelCard(True, {"TRNQSMOD": 1, "RGATEMOD": 3, "RBODYMOD": 1, "CAPMOD": 1, "RSHG": 4.0})],
+    # Instances switching NQS off (and on) against their model's setting.
+    "nqs_mixed": [ModelCard(False, {"TRNQSMOD": 1, "RDSMOD": 1, "RDW": 60.0, "RSW": 70.0, **_RS}),
+                  ModelCard(True, {"RGATEMOD": 1, "RSHG": 8.0, "CAPMOD": 0})],
 }
 
 
 def _extra(case, n, rng, nmos):
-    extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5)} if case in ("rds1", "mixed") else {}
+    extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5)} if case in ("rds1", "mixed", "nqs_mixed") else {}
+    if case == "nqs_mixed":
+        extra["TRNQSMOD"] = np.where(rng.random(n) < 0.3, np.where(nmos, 0.0, 1.0), np.nan)
     if case == "mixed":
         # Instance overrides of the modes, and initial conditions on some instances: on the NMOS
         # ones, whose drain / source nodes exist (rdsMod 1), where the reference places the
@@ -71,7 +83,7 @@ def _circuit(case, n_mos=600, seed=21):
 
 def test_general_stamp_table_matches_library():
     assert np.array_equal(general_stamp(), netlist.GEN_STAMP)
-    assert GEN_INTERNAL == 10
+    assert GEN_INTERNAL == 11 and netlist.GEN_NODES == 15 and general_stamp().shape[0] == 85
 
 
 @pytest.mark.parametrize("case", list(CASES))
@@ -86,8 +98,8 @@ def test_topology_matches_reference_instances(case):
     assert orc.ref.n_unknowns == c.n_unknowns
     counts = np.array([orc.ref.num_internal(i) for i in range(c.n_mos)])
     assert np.array_equal(counts, flags.sum(1))
-    # State slots: 3 + qgmid (rgateMod 3) + qbs, qbd (rbodyMod) per instance.
-    assert orc.n_sta_slots == 6
+    # State slots: 3 + qgmid (rgateMod 3) + qbs, qbd (rbodyMod) + qcheq, qcdump (trnqsMod).
+    assert orc.n_sta_slots == 8
     assert int((orc.sta_off >= 0).sum()) == orc.ref.n_state
 
 
@@ -138,16 +150,16 @@ def _ic_placement(rgate, rbody, nrd, nrs, ics):
     rowptr, colind = netlist.jacobian_pattern(c)
     orc = OracleRun(c, cards, im, nd, params, rowptr, colind)
     sol = np.random.default_rng(1).uniform(0.0, 1.0, c.n_unknowns)
-    z6, z14 = np.zeros(6 * n), np.zeros(14 * n)
-    dc = orc.load(SolverFlags(dcop=1, transient=0, newton_iter=1, voltlim=0), sol, z6, z6, z14, z14)
-    tr = orc.load(SolverFlags(newton_iter=1, voltlim=0), sol, z6, z6, z14, z14)
+    z8, z14 = np.zeros(8 * n), np.zeros(14 * n)
+    dc = orc.load(SolverFlags(dcop=1, transient=0, newton_iter=1, voltlim=0), sol, z8, z8, z14, z14)
+    tr = orc.load(SolverFlags(newton_iter=1, voltlim=0), sol, z8, z8, z14, z14)
     d = dc["dfdx"] - tr["dfdx"]
     prow = np.repeat(np.arange(c.n_unknowns), np.diff(rowptr))
     got = {(int(prow[k]), int(colind[k])): round(float(d[k])) for k in np.flatnonzero(np.abs(d) > 0.5)}
     loc = netlist.general_local_nodes(c)
     want = {}
     for i in range(n):
-        for ic_node, term in ((11, 3), (12, 0), (13, 1)):  # (IBS, B), (IDS, D), (IGS, G)
+        for ic_node, term in ((12, 3), (13, 0), (14, 1)):  # (IBS, B), (IDS, D), (IGS, G)
             if loc[i, ic_node] < 0:
                 continue
             for r_, c_, v in ((loc[i, term], loc[i, ic_node], 1), (loc[i, 2], loc[i, ic_node], -1),
@@ -183,11 +195,11 @@ def test_reference_ic_coupling_placement(rgate, rbody, nrd, nrs, ic, consistent)
             return
         r_, c_ = miss[0]
         n = c.n_mos
-        z6, z14 = np.zeros(6 * n), np.zeros(14 * n)
+        z8, z14 = np.zeros(8 * n), np.zeros(14 * n)
         fl = SolverFlags(dcop=1, transient=0, newton_iter=1, voltlim=0)
         x1 = sol.copy()
         x1[c_] += 1.0
-        f0 = orc.load(fl, sol, z6, z6, z14, z14)["f"]
-        f1 = orc.load(fl, x1, z6, z6, z14, z14)["f"]
+        f0 = orc.load(fl, sol, z8, z8, z14, z14)["f"]
+        f1 = orc.load(fl, x1, z8, z8, z14, z14)["f"]
         if c_ >= c.n_nodes + c.n_vsrc:  # a branch current: F is linear in it
             assert f1[r_] - f0[r_] == pytest.approx(want[(r_, c_)], abs=1e-9)

@@ -28,7 +28,9 @@ NMOS_PMOS = [ModelCard(False, {}), ModelCard(True, {})]
     (14, [ModelCard(False, {"RGATEMOD": 4}), ModelCard(True, {})], None, "rgateMod must be 0, 1, 2 or 3"),
     (14, [ModelCard(False, {"RBODYMOD": 3}), ModelCard(True, {})], None, "rbodyMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {"RDSMOD": 2}), ModelCard(True, {})], None, "rdsMod must be 0 or 1"),
-    (14, [ModelCard(False, {"TRNQSMOD": 1}), ModelCard(True, {})], None, "trnqsMod"),
+    # The NQS charge node is a general-topology internal variable too.
+    (14, [ModelCard(False, {"TRNQSMOD": 1}), ModelCard(True, {})], None, "inst_internal_gen"),
+    (14, [ModelCard(False, {"TRNQSMOD": 2}), ModelCard(True, {})], None, "trnqsMod must be 0 or 1"),
     (14, NMOS_PMOS, {"IC3": 0.2}, "inst_internal_gen"),
     (14, [ModelCard(False, {"CAPMOD": 3}), ModelCard(True, {})], None, "capMod must be 0, 1 or 2"),
     (14, [ModelCard(False, {"IGCMOD": 3}), ModelCard(True, {})], None, "igcMod must be 0, 1 or 2"),

@@ -218,9 +218,9 @@ bool Master::setup() {
   fam.temp_c = getDeviceOptions().temp.getImmutableValue<double>() - CONSTCtoK;
   fam.tnom_c = getDeviceOptions().tnom - CONSTCtoK;
   // Internal variables: which instances the library expects them on must match the reference's
-  // topology (both follow the same rules). Gate / body resistance, rdsMod 1 and instance initial
-  // conditions take the general topology (10 internal variables per instance, registerLIDs
-  // order); otherwise only the drain / source ones can exist.
+  // topology (both follow the same rules). Gate / body resistance, rdsMod 1, the NQS charge node
+  // and instance initial conditions take the general topology (XD_GEN_INTERNAL internal variables
+  // per instance, registerLIDs order); otherwise only the drain / source ones can exist.
   fam.inst_internal = 0;
   fam.inst_internal_gen = 0;
   std::vector<int> gflags((size_t)XD_GEN_INTERNAL * n_);
@@ -254,9 +254,10 @@ bool Master::setup() {
   check_cuda(cudaSetDevice(device_), "cudaSetDevice");
   check_xd(xd_create(&fam, &pat, device_, &ctx_), "xd_create");
   // State / store permutation: slot s of instance i lives at the instance's s-th LID. With the
-  // general topology the library keeps six state slots (qb, qg, qd, qgmid, qbs, qbd) and an
-  // instance registers qgmid only with rgateMod 3 and qbs / qbd only with rbodyMod
-  // (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5225): the slots it lacks get no LID (-1).
+  // general topology the library keeps eight state slots (qb, qg, qd, qgmid, qbs, qbd, qcheq,
+  // qcdump) and an instance registers qgmid only with rgateMod 3, qbs / qbd only with rbodyMod and
+  // qcheq / qcdump only with trnqsMod (registerStateLIDs, N_DEV_MOSFET_B4.C:5212-5238): the slots
+  // it lacks get no LID (-1).
   const int nst = xd_num_state_slots(ctx_), nso = xd_num_store_slots(ctx_);
   sta_lid_.assign((size_t)nst * n_, -1);
   sto_lid_.resize((size_t)nso * n_);
@@ -266,13 +267,13 @@ bool Master::setup() {
       throw std::runtime_error("GPU MOSFET binding: store registration differs from the library's");
     if (general) {
       const int *fl = &gflags[(size_t)XD_GEN_INTERNAL * i];
-      const bool rg3 = fl[3] != 0, rb = fl[4] != 0;
-      const int want = 3 + (rg3 ? 1 : 0) + (rb ? 2 : 0);
+      const bool rg3 = fl[3] != 0, rb = fl[4] != 0, nqs = fl[7] != 0;
+      const int want = 3 + (rg3 ? 1 : 0) + (rb ? 2 : 0) + (nqs ? 2 : 0);
       if ((int)st.size() != want)
         throw std::runtime_error("GPU MOSFET binding: state registration differs from the library's");
       int next = 0;
       for (int s = 0; s < nst; ++s) {
-        const bool has = s < 3 || (s == 3 && rg3) || (s > 3 && rb);
+        const bool has = s < 3 || (s == 3 && rg3) || ((s == 4 || s == 5) && rb) || (s > 5 && nqs);
         sta_lid_[(size_t)s * n_ + i] = has ? st[next++] : -1;
       }
     } else {

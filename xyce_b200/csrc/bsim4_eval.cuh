@@ -40,15 +40,19 @@ enum { kNumVec = 16, kNumMat = 16, kNumStage = kNumVec + 2 * kNumMat };
 // the external drain and source, the matrices six more slots for the resistor couplings.
 enum { kSerVecRows = 6, kSerMat = kNumMat + 6, kSerStage = 4 * kSerVecRows + 2 * kSerMat };
 
-// General topology (rgateMod 1-3, rbodyMod 1/2, rdsMod 1, instance initial conditions, and the
-// sheet-resistance D' / S' nodes): the reference's full stamp over 14 local nodes — the four
-// terminals, the internal drain / source / gate / gate-mid / body / source-body / drain-body nodes
-// (registerLIDs order, N_DEV_MOSFET_B4.C:5018-5060) and the three initial-condition branch currents.
-// A node the instance does not have is the same unknown as the one it collapses onto (D' -> D,
-// S' -> S, G' and GM -> G, B' / SB / DB -> B); an absent branch current has no unknown.
-enum GenNode { g_D, g_G, g_S, g_B, g_DP, g_SP, g_GP, g_GM, g_BP, g_SB, g_DB, g_IBS, g_IDS, g_IGS, kGenNodes };
+// General topology (rgateMod 1-3, rbodyMod 1/2, rdsMod 1, trnqsMod 1, instance initial conditions,
+// and the sheet-resistance D' / S' nodes): the reference's full stamp over 15 local nodes — the
+// four terminals, the internal drain / source / gate / gate-mid / body / source-body / drain-body
+// nodes, the NQS charge node (registerLIDs order, N_DEV_MOSFET_B4.C:5018-5079) and the three
+// initial-condition branch currents. A node the instance does not have is the same unknown as the
+// one it collapses onto (D' -> D, S' -> S, G' and GM -> G, B' / SB / DB -> B); an absent charge node
+// or branch current has no unknown.
+enum GenNode {
+  g_D, g_G, g_S, g_B, g_DP, g_SP, g_GP, g_GM, g_BP, g_SB, g_DB, g_Q, g_IBS, g_IDS, g_IGS, kGenNodes
+};
 // The stamp's (row, column) pairs in the reference's jacStamp order (:4641-4755): rows D, G, S, B,
-// D', S', G', GM, B', SB, DB, then the three initial-condition rows with their two couplings each.
+// D', S', G', GM, B', SB, DB, the charge row, then the three initial-condition rows with their two
+// couplings each; the charge node's columns in rows D', S', G' last.
 constexpr int kGenStamp[][2] = {
     {g_D, g_D},   {g_D, g_DP},   {g_D, g_SP},   {g_D, g_GP},   {g_D, g_BP},
     {g_G, g_G},   {g_G, g_DP},   {g_G, g_SP},   {g_G, g_GP},   {g_G, g_GM},   {g_G, g_BP},
@@ -62,21 +66,31 @@ constexpr int kGenStamp[][2] = {
     {g_BP, g_DB},
     {g_SB, g_B},  {g_SB, g_SP},  {g_SB, g_BP},  {g_SB, g_SB},
     {g_DB, g_B},  {g_DB, g_DP},  {g_DB, g_BP},  {g_DB, g_DB},
+    {g_Q, g_DP},  {g_Q, g_SP},   {g_Q, g_GP},   {g_Q, g_BP},   {g_Q, g_Q},
     {g_IBS, g_S}, {g_IBS, g_B},  {g_IBS, g_IBS}, {g_S, g_IBS}, {g_B, g_IBS},
     {g_IDS, g_D}, {g_IDS, g_S},  {g_IDS, g_IDS}, {g_D, g_IDS}, {g_S, g_IDS},
-    {g_IGS, g_G}, {g_IGS, g_S},  {g_IGS, g_IGS}, {g_G, g_IGS}, {g_S, g_IGS}};
+    {g_IGS, g_G}, {g_IGS, g_S},  {g_IGS, g_IGS}, {g_G, g_IGS}, {g_S, g_IGS},
+    {g_DP, g_Q},  {g_SP, g_Q},   {g_GP, g_Q}};
 constexpr int kGenSlots = sizeof(kGenStamp) / sizeof(kGenStamp[0]);
-static_assert(kGenSlots == 77, "the general stamp has 62 device entries and 15 initial-condition entries");
+static_assert(kGenSlots == 85, "the general stamp has 62 device entries, 8 NQS entries and 15 initial-condition entries");
 // Slot of (row, col) in kGenStamp; -1 if the stamp has no such entry.
 constexpr int gen_slot(int r, int c) {
   for (int k = 0; k < kGenSlots; ++k)
     if (kGenStamp[k][0] == r && kGenStamp[k][1] == c) return k;
   return -1;
 }
+// The slot of (R, C) as a compile-time constant: a stamp statement whose entry is not in the table
+// does not compile.
+template <int R, int C>
+struct GenSlotOf {
+  static constexpr int value = gen_slot(R, C);
+  static_assert(value >= 0, "the general stamp has no such entry");
+};
 // State slots of the general topology: the three intrinsic charges, then the gate-mid charge
-// (rgateMod 3) and the two junction charges (rbodyMod), in registerStateLIDs order (:5212-5225).
-enum GenState { gt_qb, gt_qg, gt_qd, gt_qgmid, gt_qbs, gt_qbd, kGenState };
-// Staging of one instance: 4 vectors x 14 rows, then dF/dx and dQ/dx over the 77 stamp slots.
+// (rgateMod 3), the two junction charges (rbodyMod) and the NQS charges qcheq, qcdump (trnqsMod),
+// in registerStateLIDs order (:5212-5238).
+enum GenState { gt_qb, gt_qg, gt_qd, gt_qgmid, gt_qbs, gt_qbd, gt_qcheq, gt_qcdump, kGenState };
+// Staging of one instance: 4 vectors x 15 rows, then dF/dx and dQ/dx over the 85 stamp slots.
 enum { kGenVecRows = kGenNodes, kGenStage = 4 * kGenVecRows + 2 * kGenSlots };
 
 struct LoadOut {
@@ -91,8 +105,8 @@ struct LoadOut {
   double sta[kNumState];
   bool write_curr_sta;    // first Newton step of the first transient step: also write currSta
   double vgb;             // this load's vgb (the next load's "vgb_orig")
-  // General topology: vectors gv[v * 14 + node] (F, Q, dF/dx*dVp, dQ/dx*dVp), the two matrices over
-  // the stamp slots, and the six state slots (zero where the instance has no such charge).
+  // General topology: vectors gv[v * 15 + node] (F, Q, dF/dx*dVp, dQ/dx*dVp), the two matrices over
+  // the stamp slots, and the eight state slots (zero where the instance has no such charge).
   double gv[4 * kGenNodes];
   double gf[kGenSlots];
   double gq[kGenSlots];
@@ -178,6 +192,7 @@ struct Bias {
   double vds, vgs, vbs, vges, vgms, vdbs, vsbs, vses, vdes, vbd, vdbd, vgd, vged, vgmd, vgmb, vbs_jct, vbd_jct;
   double vbd_orig, vbs_orig, vgs_orig, vds_orig, vgd_orig, vges_orig, vgms_orig, vdes_orig, vses_orig, vdbs_orig;
   double vsbs_orig, vdbd_orig, vged_orig, vgmd_orig, vbs_jct_orig, vbd_jct_orig, vgmb_orig;
+  double qdef;  // NQS: the charge node's value, typed (:7950-7986); zero without trnqsMod
   int origFlag;
 };
 
@@ -250,6 +265,9 @@ XD_HD void bsim4_bias(const RV &P_, const double *V, const LoadFlags &fl, const 
     vds = vgs = vbs = vges = vgms = 0.0;
     vds = vsbs = vdes = vses = 0.0;
   }
+  // NQS: the charge node's value (:7950-7986), zeroed with the voltages of an OFF device (:8096).
+  b.qdef = (GEN && P(trnqsMod) != 0.0) ? dtype * V[g_Q] : 0.0;
+  if ((fl.init_fix || fl.init_jct) && OFF) b.qdef = 0.0;
   b.Vd = Vd; b.Vs = Vs; b.Vdp = Vdp; b.Vsp = Vsp; b.Vddp = Vddp; b.Vssp = Vssp;
   b.vds = vds; b.vgs = vgs; b.vbs = vbs; b.vges = vges; b.vgms = vgms; b.vdbs = vdbs; b.vsbs = vsbs;
   b.vses = vses; b.vdes = vdes; b.vbd = vbd; b.vdbd = vdbd; b.vgd = vgd; b.vged = vged; b.vgmd = vgmd;
@@ -825,6 +843,23 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
     }
   }
 
+  // NQS (:11626-11637): the channel charge the charge node carries, its capacitances and the
+  // relaxation conductance gtau = gcrg / (Cox W L) x 1e-9 (from the DC part's unscaled gcrg).
+  const bool trnqsMod = GEN && P(trnqsMod) != 0.0;
+  constexpr double ScalingFactor = 1.0e-9;
+  const double qdef = bias.qdef;
+  double qchqs = 0.0, cqgb = 0.0, cqdb = 0.0, cqsb = 0.0, cqbb = 0.0, gtau = 0.0, CoxWL = 0.0;
+  if (trnqsMod) {
+    qchqs = -(qbulk + qgate);
+    cqgb = -(cggb + cbgb);
+    cqdb = -(cgdb + cbdb);
+    cqsb = -(cgsb + cbsb);
+    cqbb = -(cqgb + cqdb + cqsb);
+    CoxWL = P(coxe) * P(weffCV) * nf * P(leffCV);
+    gtau = m.v[m_gcrg] / CoxWL * ScalingFactor;
+  }
+  double qcheq = qchqs;
+
   // Junction charges and capacitances (:11661-11810). Outside charge computation the reference
   // keeps the previous load's junction values; they only feed Q and dQ/dx, which a DC solve does
   // not use, and are zero here.
@@ -967,11 +1002,80 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
     qgso *= nf;
   }
 
-  // Overlap and gate-bulk charge bookkeeping (setupCapacitors_oldDAE, trnqsMod = 0, :12624-12760).
+  // Overlap and gate-bulk charge bookkeeping and the charge partition (setupCapacitors_oldDAE,
+  // :12616-13045). With NQS the intrinsic charge is the charge node's: the terminal charges keep
+  // only the overlap and gate-bulk parts, and the partition dxpart / sxpart follows qdrn / qcheq.
   const double cgbo = P(cgbo);
   double dxpart, sxpart;
+  double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
+  double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
+  double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0, gqdef = 0.0;
   double qgmid = 0.0;  // rgateMod 3: the overlap and gate-bulk charge on the gate-mid node
-  if (mode > 0) {
+  // The integration coefficient of the old DAE form; zero on the first Newton step out of the
+  // operating point (:12618-12629).
+  const double ag0 = (!fl.dcop && fl.init_tran && fl.newton_iter == 0) ? 0.0 : fl.pdt;
+  if (trnqsMod) {
+    qcheq = qchqs;
+    const double T0q = qdef * ScalingFactor / CoxWL;
+    const double gcg = m.v[m_gcrgg], gcd = m.v[m_gcrgd], gcs = m.v[m_gcrgs], gcb = m.v[m_gcrgb];
+    ggtg = T0q * gcg;
+    ggtd = T0q * (mode > 0 ? gcd : gcs);
+    ggts = T0q * (mode > 0 ? gcs : gcd);
+    ggtb = T0q * gcb;
+    gqdef = ScalingFactor * ag0;
+    const double xpart = P(xpart);
+    if (mode > 0) {
+      if (fabs(qcheq) <= 1.0e-5 * CoxWL) {
+        dxpart = (xpart < 0.5) ? 0.4 : (xpart > 0.5) ? 0.0 : 0.5;
+      } else {
+        dxpart = qdrn / qcheq;
+        const double Cdd = cddb, Csd = -(cgdb + cddb + cbdb);
+        ddxpart_dVd = (Cdd - dxpart * (Cdd + Csd)) / qcheq;
+        const double Cdg = cdgb, Csg = -(cggb + cdgb + cbgb);
+        ddxpart_dVg = (Cdg - dxpart * (Cdg + Csg)) / qcheq;
+        const double Cds = cdsb, Css = -(cgsb + cdsb + cbsb);
+        ddxpart_dVs = (Cds - dxpart * (Cds + Css)) / qcheq;
+        ddxpart_dVb = -(ddxpart_dVd + ddxpart_dVg + ddxpart_dVs);
+      }
+      sxpart = 1.0 - dxpart;
+      dsxpart_dVd = -ddxpart_dVd;
+      dsxpart_dVg = -ddxpart_dVg;
+      dsxpart_dVs = -ddxpart_dVs;
+      dsxpart_dVb = -(dsxpart_dVd + dsxpart_dVg + dsxpart_dVs);
+    } else {
+      if (fabs(qcheq) <= 1.0e-5 * CoxWL) {
+        sxpart = (xpart < 0.5) ? 0.4 : (xpart > 0.5) ? 0.0 : 0.5;
+      } else {
+        sxpart = qdrn / qcheq;
+        const double Css = cddb, Cds = -(cgdb + cddb + cbdb);
+        dsxpart_dVs = (Css - sxpart * (Css + Cds)) / qcheq;
+        const double Csg = cdgb, Cdg = -(cggb + cdgb + cbgb);
+        dsxpart_dVg = (Csg - sxpart * (Csg + Cdg)) / qcheq;
+        const double Csd = cdsb, Cdd = -(cgsb + cdsb + cbsb);
+        dsxpart_dVd = (Csd - sxpart * (Csd + Cdd)) / qcheq;
+        dsxpart_dVb = -(dsxpart_dVd + dsxpart_dVg + dsxpart_dVs);
+      }
+      dxpart = 1.0 - sxpart;
+      ddxpart_dVd = -dsxpart_dVd;
+      ddxpart_dVg = -dsxpart_dVg;
+      ddxpart_dVs = -dsxpart_dVs;
+      ddxpart_dVb = -(ddxpart_dVd + ddxpart_dVg + ddxpart_dVs);
+    }
+    if (rgateMod == 3) {
+      const double qgmb = cgbo * vgmb;
+      qgmid = qgdo + qgso + qgmb;
+      qgate = 0.0;
+      qbulk = -qgmb;
+      qdrn = -qgdo;
+      qsrc = (mode > 0) ? -(qgmid + qbulk + qdrn) : -qgso;
+    } else {
+      const double qgb = cgbo * vgb;
+      qgate = qgdo + qgso + qgb;
+      qbulk = -qgb;
+      qdrn = -qgdo;
+      qsrc = (mode > 0) ? -(qgate + qbulk + qdrn) : -qgso;
+    }
+  } else if (mode > 0) {
     qdrn -= qgdo;
     if (rgateMod == 3) {
       const double qgmb = cgbo * vgmb;
@@ -1002,14 +1106,58 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
     sxpart = 0.4;
     dxpart = 0.6;
   }
-  (void)qsrc;
+  (void)qsrc; (void)ag0;
 
-  // Capacitance matrix entries (setupCapacitors_newDAE, trnqsMod = 0, :12357-12608).
+  // Capacitance matrix entries (setupCapacitors_newDAE, :12357-12608).
   double CAPcggb, CAPcgdb, CAPcgsb, CAPcgbb, CAPcdgb, CAPcsgb, CAPcbgb, CAPcddb, CAPcdsb, CAPcsdb, CAPcssb;
   double CAPcdbb, CAPcsbb, CAPcbdb, CAPcbsb, CAPcbbb;
   double CAPcdgmb = 0.0, CAPcsgmb = 0.0, CAPcbgmb = 0.0;
   double CAPcgmgmb = 0.0, CAPcgmdb = 0.0, CAPcgmsb = 0.0, CAPcgmbb = 0.0, CAPcdbdb = 0.0, CAPcsbsb = 0.0;
-  if (GEN) {
+  double CAPcqgb = 0.0, CAPcqdb = 0.0, CAPcqsb = 0.0, CAPcqbb = 0.0;
+  if (trnqsMod) {
+    // NQS: the intrinsic capacitances sit on the charge node's row; the terminals keep the overlap
+    // and junction parts (the trnqsMod != 0 branches of :12423-12480 and :12543-12600).
+    CAPcqgb = cqgb;
+    CAPcqdb = (mode > 0) ? cqdb : cqsb;
+    CAPcqsb = (mode > 0) ? cqsb : cqdb;
+    CAPcqbb = cqbb;
+    if (rgateMod == 3) {
+      CAPcgmgmb = (cgdo + cgso + cgbo);
+      CAPcgmdb = -cgdo;
+      CAPcgmsb = -cgso;
+      CAPcgmbb = -cgbo;
+      CAPcdgmb = CAPcgmdb;
+      CAPcsgmb = CAPcgmsb;
+      CAPcbgmb = CAPcgmbb;
+      CAPcdgb = CAPcsgb = CAPcbgb = 0.0;
+      CAPcggb = CAPcgdb = CAPcgsb = CAPcgbb = 0.0;
+    } else {
+      CAPcggb = (cgdo + cgso + cgbo);
+      CAPcgdb = -cgdo;
+      CAPcgsb = -cgso;
+      CAPcgbb = -cgbo;
+      CAPcdgb = CAPcgdb;
+      CAPcsgb = CAPcgsb;
+      CAPcbgb = CAPcgbb;
+      CAPcdgmb = CAPcsgmb = CAPcbgmb = 0.0;
+    }
+    CAPcddb = (capbd + cgdo);
+    CAPcdsb = CAPcsdb = 0.0;
+    CAPcssb = (capbs + cgso);
+    if (!rbodyMod) {
+      CAPcdbb = -(CAPcdgb + CAPcddb + CAPcdgmb);
+      CAPcsbb = -(CAPcsgb + CAPcssb + CAPcsgmb);
+      CAPcbdb = -capbd;
+      CAPcbsb = -capbs;
+      CAPcdbdb = 0.0;
+      CAPcsbsb = 0.0;
+    } else {
+      CAPcdbb = CAPcsbb = CAPcbdb = CAPcbsb = 0.0;
+      CAPcdbdb = -capbd;
+      CAPcsbsb = -capbs;
+    }
+    CAPcbbb = -(CAPcbdb + CAPcbgb + CAPcbsb + CAPcbgmb);
+  } else if (GEN) {
     if (mode > 0) {
       if (rgateMod == 3) {
         CAPcgmgmb = (cgdo + cgso + cgbo);
@@ -1167,6 +1315,8 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
     o.gsta[gt_qgmid] = (rgateMod == 3) ? qgmid : 0.0;
     o.gsta[gt_qbs] = rbodyMod ? qbs : 0.0;
     o.gsta[gt_qbd] = rbodyMod ? qbd : 0.0;
+    o.gsta[gt_qcheq] = trnqsMod ? qcheq : 0.0;
+    o.gsta[gt_qcdump] = trnqsMod ? qdef * ScalingFactor : 0.0;
   }
   o.write_curr_sta = (!fl.dcop) && fl.init_tran && fl.newton_iter == 0;
   o.vgb = vgb;
@@ -1473,6 +1623,25 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
         Qeqqjd_Jdxp = CAPcdbdb * (vbd_jct - vbd_jct_orig);
       }
     }
+    // NQS (:12232-12244, 12300-12322): the charge-node terms of the limiter vectors; outside charge
+    // computation the partition is the fixed 40/60 one and gtau is formed again from gcrg as the
+    // F-vector set-up left it (zero unless rgateMod 2 / 3).
+    double Qqcheq_Jdxp = 0.0;
+    if (trnqsMod) {
+      if (ChargeComputationNeeded) {
+        const double T0n = ggtg * (vgb - vgb_orig) - ggtd * (vbd - vbd_orig) - ggts * (vbs - vbs_orig);
+        Qeqqg_Jdxp += T0n;
+        const double T1n = qdef * gtau;
+        Qeqqd_Jdxp -= dxpart * T0n + T1n * (ddxpart_dVg * (vgb - vgb_orig) - ddxpart_dVd * (vbd - vbd_orig) -
+                                            ddxpart_dVs * (vbs - vbs_orig));
+        Qqcheq_Jdxp = -(CAPcqgb * (vgb - vgb_orig) - CAPcqdb * (vbd - vbd_orig) - CAPcqsb * (vbs - vbs_orig)) + T0n;
+      } else {
+        sxpart = (1.0 - (dxpart = (mode > 0) ? 0.4 : 0.6));
+        ddxpart_dVd = ddxpart_dVg = ddxpart_dVb = ddxpart_dVs = 0.0;
+        dsxpart_dVd = dsxpart_dVg = dsxpart_dVb = dsxpart_dVs = 0.0;
+        gtau = gcrg / CoxWL * ScalingFactor;
+      }
+    }
     const double sgn = dtype > 0 ? 1.0 : -1.0;
     (void)sgn;
     double Qeqqg, Qeqqd, Qeqqb, Qeqqgmid = 0.0, Qeqqjs = 0.0, Qeqqjd = 0.0;
@@ -1507,6 +1676,10 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
       GV(1, g_SB) -= -(Qeqqjs) * M;
       GV(1, g_SP) += -(Qeqqd + Qeqqg + Qeqqb + Qeqqjd + Qeqqjs + Qeqqgmid) * M;
     }
+    if (trnqsMod) {
+      const double Qqdef = dtype > 0 ? qdef : -qdef, Qqcheq = dtype > 0 ? qcheq : -qcheq;
+      GV(1, g_Q) += -(Qqcheq - Qqdef) * M;
+    }
     if (lim) {
       GV(3, g_DP) += (-Qeqqd_Jdxp) * M;
       GV(3, g_GP) -= (Qeqqg_Jdxp) * M;
@@ -1520,6 +1693,7 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
         GV(3, g_SB) -= (+Qeqqjs_Jdxp) * M;
         GV(3, g_SP) += (+Qeqqd_Jdxp + Qeqqg_Jdxp + Qeqqb_Jdxp + Qeqqjd_Jdxp + Qeqqjs_Jdxp + Qeqqgmid_Jdxp) * M;
       }
+      if (trnqsMod) GV(3, g_Q) += (Qqcheq_Jdxp) * M;
     }
 #undef GV
     // Master::loadDAEMatrices, pointer form (:16577-16853 and :17102-17172).
@@ -1527,15 +1701,12 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
       o.gf[k] = 0.0;
       o.gq[k] = 0.0;
     }
-#define GF(r, c) o.gf[gen_slot(g_##r, g_##c)]
-#define GQ(r, c) o.gq[gen_slot(g_##r, g_##c)]
+#define GF(r, c) o.gf[GenSlotOf<g_##r, g_##c>::value]
+#define GQ(r, c) o.gq[GenSlotOf<g_##r, g_##c>::value]
     const double gjbd = !rbodyMod ? gbd : 0.0, gjbs = !rbodyMod ? gbs : 0.0;
     const double gdpr = !rdsMod ? P(drainConductance) : 0.0, gspr = !rdsMod ? P(sourceConductance) : 0.0;
     const double geltd = P(grgeltd);
-    const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
-    const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
-    const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
-    const double Tq = 0.0;  // qdef * gtau with no NQS charge
+    const double Tq = qdef * gtau;  // :16606
     if (rgateMod == 1) {
       GF(G, G) += (geltd) * M;
       GF(G, GP) -= (geltd) * M;
@@ -1637,6 +1808,16 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
       GF(B, SB) -= (P(grbsb)) * M;
       GF(B, B) += (P(grbsb) + P(grbdb) + P(grbpb)) * M;
     }
+    if (trnqsMod) {  // :16796-16807
+      GF(Q, Q) += (gqdef + gtau) * M;
+      GF(Q, GP) += (ggtg) * M;
+      GF(Q, DP) += (ggtd) * M;
+      GF(Q, SP) += (ggts) * M;
+      GF(Q, BP) += (ggtb) * M;
+      GF(DP, Q) += (dxpart * gtau) * M;
+      GF(SP, Q) += (sxpart * gtau) * M;
+      GF(GP, Q) -= (gtau) * M;
+    }
     // Initial-condition rows (:16810-16853): the couplings during the operating point, the branch
     // current's own diagonal (assigned, the row belongs to this instance alone) otherwise.
     if (P(icVBSGiven) != 0.0) {
@@ -1702,6 +1883,12 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
         GQ(DB, DB) += (-CAPcdbdb) * M;
         GQ(SB, SP) += (CAPcsbsb) * M;
         GQ(SB, SB) += (-CAPcsbsb) * M;
+      }
+      if (trnqsMod) {  // :17181-17187
+        GQ(Q, GP) += (-CAPcqgb) * M;
+        GQ(Q, DP) += (-CAPcqdb) * M;
+        GQ(Q, SP) += (-CAPcqsb) * M;
+        GQ(Q, BP) += (-CAPcqbb) * M;
       }
     }
 #undef GF
@@ -1775,10 +1962,8 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
     o.jq[k] = 0.0;
   }
   const double gdpr = P(drainConductance), gspr = P(sourceConductance);
-  const double ggtg = 0.0, ggtd = 0.0, ggts = 0.0, ggtb = 0.0;
-  const double ddxpart_dVd = 0.0, ddxpart_dVg = 0.0, ddxpart_dVb = 0.0, ddxpart_dVs = 0.0;
-  const double dsxpart_dVd = 0.0, dsxpart_dVg = 0.0, dsxpart_dVb = 0.0, dsxpart_dVs = 0.0;
-  const double Tq = 0.0;  // qdef * gtau with no NQS charge
+  // No NQS charge on this path: ggt*, the partition's derivatives and Tq = qdef * gtau are zero.
+  const double Tq = qdef * gtau;
 #define JF(r, c) o.jf[(r)*4 + (c)]
 #define JQ(r, c) o.jq[(r)*4 + (c)]
   JF(1, 1) += (-ggtg + gIgtotg) * M;
@@ -3094,9 +3279,9 @@ XD_HD void bsim4_load(const RV &P_, const double *V, const double *sto_old, cons
   }
   double gds = Gds, gm = Gm, gmbs = Gmb;
 
-  // Gate resistance conductance for rgateMod 2 / 3 (:9954-9989; NQS, the other user, is refused).
+  // Gate resistance conductance for rgateMod 2 / 3 and the NQS time constant (:9954-9989).
   double gcrg = 0.0, gcrgg = 0.0, gcrgd = 0.0, gcrgs = 0.0, gcrgb = 0.0;
-  if (GEN && rgateMod > 1) {
+  if (GEN && (rgateMod > 1 || P(trnqsMod) != 0.0)) {
     T9 = P(xrcrg2) * P(vtm);
     T0 = T9 * beta;
     dT0_dVd = (dbeta_dVd + dbeta_dVg * dVgsteff_dVd) * T9;

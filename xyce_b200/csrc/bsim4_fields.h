@@ -46,9 +46,9 @@
   F(DslpFwd) F(DslpRev) F(SjctTempRevSatCur) F(SswTempRevSatCur) F(SswgTempRevSatCur)            \
   F(DjctTempRevSatCur) F(DswTempRevSatCur) F(DswgTempRevSatCur) F(drainConductance)              \
   F(sourceConductance) F(grgeltd) F(temp) F(off) F(dExists) F(sExists)                           \
-  /* general topology: gate / body resistance modes, rdsMod 1 S/D resistance, body network */    \
+  /* general topology: gate / body resistance modes, rdsMod 1 S/D resistance, body network, NQS */ \
   F(rgateMod) F(rbodyMod) F(rd0) F(rdwmin) F(rs0) F(rswmin) F(grbpd) F(grbps) F(grbpb) F(grbsb)   \
-  F(grbdb) F(icVBS) F(icVDS) F(icVGS) F(icVBSGiven) F(icVDSGiven) F(icVGSGiven)
+  F(grbdb) F(icVBS) F(icVDS) F(icVGS) F(icVBSGiven) F(icVDSGiven) F(icVGSGiven) F(trnqsMod)
 
 namespace xb4 {
 enum Field {

@@ -242,7 +242,11 @@ std::string process_model(const ModelSpec &spec, const SetupOptions &opts, Card 
   if (m.igbMod < 0 || m.igbMod > 1) return "BSIM4 igbMod must be 0 or 1";
   if (m.rgateMod < 0 || m.rgateMod > 3 || m.rgateMod != (int)m.rgateMod) return "BSIM4 rgateMod must be 0, 1, 2 or 3";
   if (m.rbodyMod < 0 || m.rbodyMod > 2 || m.rbodyMod != (int)m.rbodyMod) return "BSIM4 rbodyMod must be 0, 1 or 2";
-  if (m.trnqsMod != 0 || m.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
+  // The transient NQS charge model (trnqsMod 1) adds the charge node; acnqsMod only sets the AC
+  // small-signal time constant (taunet, N_DEV_MOSFET_B4.C:11639-11642), which no DC or transient
+  // load reads.
+  if (m.trnqsMod != 0 && m.trnqsMod != 1) return "BSIM4 trnqsMod must be 0 or 1";
+  if (m.acnqsMod != 0 && m.acnqsMod != 1) return "BSIM4 acnqsMod must be 0 or 1";
   if (m.capMod < 0 || m.capMod > 2) return "BSIM4 capMod must be 0, 1 or 2";
   if (m.dioMod < 0 || m.dioMod > 2) return "BSIM4 dioMod must be 0, 1 or 2";
   if (m.mobMod < 0 || m.mobMod > 2) return "BSIM4 mobMod must be 0, 1 or 2";
@@ -713,7 +717,6 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   if (!ip.g("RGEOMOD")) ip.rgeoMod = 0;
   if (!ip.g("TRNQSMOD") || (ip.trnqsMod != 0 && ip.trnqsMod != 1)) ip.trnqsMod = m.trnqsMod;
   if (!ip.g("ACNQSMOD") || (ip.acnqsMod != 0 && ip.acnqsMod != 1)) ip.acnqsMod = m.acnqsMod;
-  if (ip.trnqsMod != 0 || ip.acnqsMod != 0) return "BSIM4 trnqsMod/acnqsMod != 0 is not supported";
   // Geometry-derived source / drain resistance (RdseffGeo) applies where a sheet resistance or
   // rdsMod asks for a resistance and the instance gives no squares.
   if (ip.rgeoMod != 0 && (m.sheetResistance > 0.0 || m.rdsMod != 0) && (!ip.g("NRD") || !ip.g("NRS")))
@@ -1090,7 +1093,7 @@ std::string instance_record(ModelState &ms, const InstParams &ipin, const SetupO
   R(rswmin) = p.rswmin; R(grbpd) = grbpd; R(grbps) = grbps; R(grbpb) = grbpb; R(grbsb) = grbsb; R(grbdb) = grbdb;
   R(icVBS) = ip.icVBS; R(icVDS) = ip.icVDS; R(icVGS) = ip.icVGS;
   R(icVBSGiven) = ip.g("IC3") ? 1.0 : 0.0; R(icVDSGiven) = ip.g("IC1") ? 1.0 : 0.0;
-  R(icVGSGiven) = ip.g("IC2") ? 1.0 : 0.0;
+  R(icVGSGiven) = ip.g("IC2") ? 1.0 : 0.0; R(trnqsMod) = ip.trnqsMod;
   R(temp) = temp; R(off) = ip.off;
 #undef R
   return std::string();

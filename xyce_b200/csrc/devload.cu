@@ -109,9 +109,9 @@ struct xd_ctx {
   // slot-major); allocated for the BSIM4 families the split launch shapes evaluate.
   double *d_mid = nullptr;
   // General topology (BSIM4 gate / body resistance, rdsMod 1, instance initial conditions): each
-  // instance's 14 local nodes as unknowns (slot-major [node * n + i]; collapsed nodes carry their
-  // representative's unknown, ground and absent branch currents -1), 14 vector rows and 77 matrix
-  // slots of staging, and 6 state slots per instance.
+  // instance's 15 local nodes as unknowns (slot-major [node * n + i]; collapsed nodes carry their
+  // representative's unknown, ground, an absent charge node and absent branch currents -1), 15
+  // vector rows and 85 matrix slots of staging, and 8 state slots per instance.
   bool gen = false;
   int *d_gmap = nullptr;
 };
@@ -253,9 +253,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_charge_stamp_kernel(
   bsim4_write_one<SERIES>(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
 }
 
-// General topology: one thread per instance over the 14 local nodes; the full store block is read
+// General topology: one thread per instance over the 15 local nodes; the full store block is read
 // (the limiters of the gate, source / drain and body-network voltages compare against it) and the
-// six state slots written.
+// eight state slots written.
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_kernel(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
@@ -671,7 +671,7 @@ struct EvalVariant {
   bool persist;  // one wave of resident blocks with a grid-stride loop
   bool split;    // two kernels: the DC part (min_blocks), then charges and stamps (min_blocks2)
   int min_blocks2;
-  bool gen;      // BSIM4 general topology (14 local nodes, 77 stamp slots)
+  bool gen;      // BSIM4 general topology (15 local nodes, 85 stamp slots)
 };
 constexpr int B4 = 4, B3 = 3, M1 = 1;  // kFamilyBsim4, kFamilyBsim3, kFamilyMos1
 constexpr EvalVariant kEvalVariants[] = {
@@ -850,8 +850,9 @@ void internal_flags(int family, const xb4::RecordTable &rt, std::vector<unsigned
   }
 }
 
-// General topology, per instance: which of the internal variables (D', S', G', GM, B', SB, DB and the
-// three initial-condition branch currents, registerLIDs order) it has (:3684-3769, 4996-5075).
+// General topology, per instance: which of the internal variables (D', S', G', GM, B', SB, DB, the
+// NQS charge and the three initial-condition branch currents, registerLIDs order) it has
+// (:3684-3769, 4996-5099).
 constexpr int kGenInternal = XD_GEN_INTERNAL;
 static_assert(kGenInternal == xb4::kGenNodes - 4, "the internal variables are the local nodes after D, G, S, B");
 void gen_flags(const xb4::RecordTable &rt, std::vector<unsigned char> &flags) {
@@ -868,19 +869,21 @@ void gen_flags(const xb4::RecordTable &rt, std::vector<unsigned char> &flags) {
     fl[2] = rg > 0;
     fl[3] = rg == 3;
     fl[4] = fl[5] = fl[6] = rb;
-    fl[7] = f(xb4::f_icVBSGiven, r) != 0.0;
-    fl[8] = f(xb4::f_icVDSGiven, r) != 0.0;
-    fl[9] = f(xb4::f_icVGSGiven, r) != 0.0;
+    fl[7] = f(xb4::f_trnqsMod, r) != 0.0;
+    fl[8] = f(xb4::f_icVBSGiven, r) != 0.0;
+    fl[9] = f(xb4::f_icVDSGiven, r) != 0.0;
+    fl[10] = f(xb4::f_icVGSGiven, r) != 0.0;
   }
 }
-// A BSIM4 family needs the general topology when a record uses gate or body resistance, rdsMod 1 or
-// an instance initial condition.
+// A BSIM4 family needs the general topology when a record uses gate or body resistance, rdsMod 1,
+// the NQS charge node or an instance initial condition.
 bool family_needs_gen(const xb4::RecordTable &rt) {
   const size_t nr = (size_t)rt.n_records;
   auto f = [&](xb4::Field fld, size_t r) { return rt.tab[(size_t)fld * nr + r]; };
   for (size_t r = 0; r < nr; ++r)
     if (f(xb4::f_rgateMod, r) != 0.0 || f(xb4::f_rbodyMod, r) != 0.0 || f(xb4::f_rdsMod, r) != 0.0 ||
-        f(xb4::f_icVBSGiven, r) != 0.0 || f(xb4::f_icVDSGiven, r) != 0.0 || f(xb4::f_icVGSGiven, r) != 0.0)
+        f(xb4::f_trnqsMod, r) != 0.0 || f(xb4::f_icVBSGiven, r) != 0.0 || f(xb4::f_icVDSGiven, r) != 0.0 ||
+        f(xb4::f_icVGSGiven, r) != 0.0)
       return true;
   return false;
 }
@@ -1118,7 +1121,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
       : family == kFamilyBsim3 ? xb3::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt)
                                : xb4::build_records(models, n, fam->inst_model, ipn, fam->inst_param_values, opts, rt);
   if (!e.empty()) return fail(-2, e);
-  // General topology (BSIM4): the caller passed the 10 internal variables per instance, or the
+  // General topology (BSIM4): the caller passed the 11 internal variables per instance, or the
   // cards need them.
   const bool gen = family == kFamilyBsim4 && (fam->inst_internal_gen != nullptr || family_needs_gen(rt));
   if (gen && !fam->inst_internal_gen)
@@ -1190,7 +1193,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
     mt.reserve((size_t)xb4::kGenSlots * n);
     ms.reserve((size_t)xb4::kGenSlots * n);
     static const char *const kNames[kGenInternal] = {"drain'", "source'", "gate'", "gate-mid", "body'",
-                                                     "source-body", "drain-body", "IBS", "IDS", "IGS"};
+                                                     "source-body", "drain-body", "charge", "IBS", "IDS", "IGS"};
     for (int i = 0; i < n; ++i) {
       int nd[xb4::kGenNodes];
       for (int k = 0; k < 4; ++k) {
@@ -1199,7 +1202,7 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
         if (nd[k] < 0) nd[k] = -1;
       }
       // Representatives of the collapsible nodes: D' -> D, S' -> S, G' / GM -> G, B' / SB / DB -> B.
-      const int rep[kGenInternal] = {nd[0], nd[2], nd[1], nd[1], nd[3], nd[3], nd[3], -1, -1, -1};
+      const int rep[kGenInternal] = {nd[0], nd[2], nd[1], nd[1], nd[3], nd[3], nd[3], -1, -1, -1, -1};
       for (int k = 0; k < kGenInternal; ++k) {
         const int u = fam->inst_internal_gen[(size_t)kGenInternal * i + k];
         const bool has = gfl[(size_t)kGenInternal * i + k] != 0;

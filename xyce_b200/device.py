@@ -123,7 +123,7 @@ def _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, t
     fam.temp_c = float(temp_c)
     fam.tnom_c = float(tnom_c)
     if inst_internal is not None:
-        # [n, 2]: drain / source internal nodes; [n, 10]: the BSIM4 general topology's internal
+        # [n, 2]: drain / source internal nodes; [n, 11]: the BSIM4 general topology's internal
         # variables (GEN_INTERNAL order).
         arr = np.asarray(inst_internal, dtype=np.int32)
         internal = np.ascontiguousarray(arr.reshape(-1))
@@ -133,21 +133,21 @@ def _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, t
         elif internal.shape[0] == 2 * n:
             fam.inst_internal = internal.ctypes.data_as(_native._ip)
         else:
-            raise _native.NativeError("inst_internal must have shape [n, 2] or [n, 10]")
+            raise _native.NativeError(f"inst_internal must have shape [n, 2] or [n, {GEN_INTERNAL}]")
     return fam, keep
 
 
 # The BSIM4 general topology's internal variables per instance, in the reference's registerLIDs
-# order (N_DEV_MOSFET_B4.C:5018-5075); the columns of an [n, 10] ``inst_internal``.
-GEN_INTERNAL_NAMES = ("drain'", "source'", "gate'", "gate-mid", "body'", "source-body", "drain-body", "IBS", "IDS",
-                      "IGS")
+# order (N_DEV_MOSFET_B4.C:5018-5099); the columns of an [n, 11] ``inst_internal``.
+GEN_INTERNAL_NAMES = ("drain'", "source'", "gate'", "gate-mid", "body'", "source-body", "drain-body", "charge",
+                      "IBS", "IDS", "IGS")
 GEN_INTERNAL = len(GEN_INTERNAL_NAMES)
 
 
 def internal_nodes(models, inst_model, inst_nodes, inst_params, level=14, temp_c=27.0, tnom_c=27.0, general=False):
     """Which instances have which internal variables: the topology query the reference's instances
     answer before their unknowns are numbered. ``general=False``: [n, 2] bool, the internal drain /
-    source nodes (``xd_internal_nodes``). ``general=True`` (BSIM4): ([n, 10] bool in GEN_INTERNAL
+    source nodes (``xd_internal_nodes``). ``general=True`` (BSIM4): ([n, 11] bool in GEN_INTERNAL
     order, whether the family needs the general topology) from ``xd_internal_nodes_gen``."""
     fam, keep = _family_struct(models, inst_model, inst_nodes, inst_params, level, temp_c, tnom_c)
     n = int(np.asarray(inst_model).shape[0])
@@ -163,7 +163,7 @@ def internal_nodes(models, inst_model, inst_nodes, inst_params, level=14, temp_c
 
 
 def general_stamp():
-    """The general topology's 77 (row, col) local-node pairs (``xd_general_stamp``)."""
+    """The general topology's 85 (row, col) local-node pairs (``xd_general_stamp``)."""
     lib = _native.load()
     rows, cols = np.zeros(128, dtype=np.int32), np.zeros(128, dtype=np.int32)
     k = lib.xd_general_stamp(rows.ctypes.data_as(_native._ip), cols.ctypes.data_as(_native._ip))
@@ -181,7 +181,7 @@ class MosfetDevice:
     pattern:       (rowptr, colind) CSR pattern of the Jacobian over the unknowns
     inst_internal: int array [n, 2] internal drain / source unknowns (-1 = none), required when
                    ``internal_nodes`` reports some; or, for the BSIM4 general topology (gate / body
-                   resistance, rdsMod 1, instance ICs), [n, 10] in GEN_INTERNAL order
+                   resistance, rdsMod 1, NQS, instance ICs), [n, 11] in GEN_INTERNAL order
     """
 
     level = 14
@@ -251,7 +251,7 @@ class MosfetDevice:
 
     def copy_stamps(self, stream=None) -> np.ndarray:
         """The staged stamps, [slots, n] (48 slots for the 4-terminal layout, 68 with internal drain /
-        source nodes, 210 for the general topology)."""
+        source nodes, 230 for the general topology)."""
         slots = self._lib.xd_num_stage_slots(self._h)
         out = np.zeros(slots * self.n, dtype=np.float64)
         _native.check(self._lib.xd_copy_stamps(self._h, ctypes.c_void_p(out.ctypes.data), _stream_handle(stream)),

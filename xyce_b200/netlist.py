@@ -41,8 +41,8 @@ class Circuit:
     vdd: float = 1.2
     meta: dict = field(default_factory=dict)
     # Internal variables of the MOSFETs: [n_mos, 2] drain / source nodes (series resistance), or
-    # [n_mos, 10] for the BSIM4 general topology (D', S', G', GM, B', SB, DB and the IBS, IDS, IGS
-    # branch currents), unknown indices, -1 where the instance has none. They come after the nodes
+    # [n_mos, 11] for the BSIM4 general topology (D', S', G', GM, B', SB, DB, the NQS charge Q and
+    # the IBS, IDS, IGS branch currents), unknown indices, -1 where the instance has none. They come after the nodes
     # and the source branches, instance by instance in that order (the reference's numbering).
     mos_internal: np.ndarray | None = None
     n_internal: int = 0
@@ -79,10 +79,12 @@ def _pairs_2term(nodes: np.ndarray) -> np.ndarray:
     return np.stack([rows, cols], 1)
 
 
-# The BSIM4 general topology's stamp over its 14 local nodes (D, G, S, B, D', S', G', GM, B', SB, DB,
-# IBS, IDS, IGS = 0..13), in the reference's jacStamp order (N_DEV_MOSFET_B4.C:4641-4795); the
-# library reports the same table (xd_general_stamp).
-_D, _G, _S, _B, _DP, _SP, _GP, _GM, _BP, _SB, _DB, _IBS, _IDS, _IGS = range(14)
+# The BSIM4 general topology's stamp over its 15 local nodes (D, G, S, B, D', S', G', GM, B', SB, DB,
+# Q, IBS, IDS, IGS = 0..14), in the reference's jacStamp order (N_DEV_MOSFET_B4.C:4641-4795), the
+# charge node's columns of rows D', S', G' last; the library reports the same table
+# (xd_general_stamp).
+_D, _G, _S, _B, _DP, _SP, _GP, _GM, _BP, _SB, _DB, _Q, _IBS, _IDS, _IGS = range(15)
+GEN_NODES = 15
 GEN_STAMP = np.array(
     [(_D, _D), (_D, _DP), (_D, _SP), (_D, _GP), (_D, _BP),
      (_G, _G), (_G, _DP), (_G, _SP), (_G, _GP), (_G, _GM), (_G, _BP),
@@ -95,19 +97,21 @@ GEN_STAMP = np.array(
      (_BP, _B), (_BP, _DP), (_BP, _SP), (_BP, _GP), (_BP, _GM), (_BP, _BP), (_BP, _SB), (_BP, _DB),
      (_SB, _B), (_SB, _SP), (_SB, _BP), (_SB, _SB),
      (_DB, _B), (_DB, _DP), (_DB, _BP), (_DB, _DB),
+     (_Q, _DP), (_Q, _SP), (_Q, _GP), (_Q, _BP), (_Q, _Q),
      (_IBS, _S), (_IBS, _B), (_IBS, _IBS), (_S, _IBS), (_B, _IBS),
      (_IDS, _D), (_IDS, _S), (_IDS, _IDS), (_D, _IDS), (_S, _IDS),
-     (_IGS, _G), (_IGS, _S), (_IGS, _IGS), (_G, _IGS), (_S, _IGS)], dtype=np.int64)
+     (_IGS, _G), (_IGS, _S), (_IGS, _IGS), (_G, _IGS), (_S, _IGS),
+     (_DP, _Q), (_SP, _Q), (_GP, _Q)], dtype=np.int64)
 
 
 def general_local_nodes(c: Circuit) -> np.ndarray:
-    """[n_mos, 14] unknown of each local node of the general topology: a node the instance does
+    """[n_mos, 15] unknown of each local node of the general topology: a node the instance does
     not have is its terminal's unknown (D' -> D, S' -> S, G' and GM -> G, B' / SB / DB -> B), an
-    absent branch current -1, ground -1."""
+    absent charge node or branch current -1, ground -1."""
     nd = c.mos_nodes.astype(np.int64)
     internal = c.mos_internal.astype(np.int64)
     rep = nd[:, [0, 2, 1, 1, 3, 3, 3]]
-    loc = np.full((nd.shape[0], 14), -1, dtype=np.int64)
+    loc = np.full((nd.shape[0], GEN_NODES), -1, dtype=np.int64)
     loc[:, :4] = nd
     loc[:, 4:11] = np.where(internal[:, :7] >= 0, internal[:, :7], rep)
     loc[:, 11:] = internal[:, 7:]
@@ -121,7 +125,7 @@ def jacobian_pattern(c: Circuit):
     r = np.repeat(m, 4, axis=1)
     cc = np.tile(m, (1, 4))
     parts.append(np.stack([r.reshape(-1), cc.reshape(-1)], 1))
-    if c.mos_internal is not None and c.mos_internal.shape[1] == 10:
+    if c.mos_internal is not None and c.mos_internal.shape[1] == GEN_NODES - 4:
         # The general topology's stamp after collapsing (pairs with ground or an absent branch
         # current drop out below).
         loc = general_local_nodes(c)
@@ -154,7 +158,7 @@ def jacobian_pattern(c: Circuit):
 
 def with_internal_nodes(c: Circuit, flags) -> Circuit:
     """The circuit with an internal unknown for every True in flags ([n_mos, 2] drain / source, or
-    [n_mos, 10] for the BSIM4 general topology, from ``device.internal_nodes``), numbered after all
+    [n_mos, 11] for the BSIM4 general topology, from ``device.internal_nodes``), numbered after all
     other unknowns, instance by instance in column order."""
     import dataclasses
 

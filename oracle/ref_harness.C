@@ -64,6 +64,20 @@ std::string CmdParse::getArgumentValue(const std::string &) const { return std::
 
 namespace XD = Xyce::Device;
 
+// Access to BSIM4's private Jacobian-stamp map (an explicit instantiation may name a private
+// member), for the NQS offset repair in xref_set_pattern.
+namespace {
+template <class Tag, typename Tag::type M>
+struct XrefMember {
+  friend typename Tag::type xref_member(Tag) { return M; }
+};
+struct B4JacMap2 {
+  typedef std::vector<std::vector<int> > XD::MOSFET_B4::Instance::*type;
+  friend type xref_member(B4JacMap2);
+};
+template struct XrefMember<B4JacMap2, &XD::MOSFET_B4::Instance::jacMap2>;
+}  // namespace
+
 extern "C" {
 // Mirrors the reference SolverState / DeviceOptions fields the MOSFET loads read.
 typedef struct xref_flags {
@@ -423,7 +437,22 @@ int xref_set_pattern(void *h, int n_rows, const int *rowptr, const int *colind) 
         jl[r].push_back((int)(p - b));
       }
     }
+    // BSIM4 with trnqsMod: the reference reads the gate'-charge offset as jacMap2[1][6]
+    // (N_DEV_MOSFET_B4.C:5396), the gate row's map, one past its end unless IC2 gave that row a
+    // seventh column; the entry it means is jacMap2[6][6] (the gate' row's charge column, the
+    // pattern of the rows around it). Out of range the read is undefined (it crashed the
+    // process), so the harness gives the gate row's map that entry for the call and takes it away
+    // after: the reference's own code then registers the gate'-charge offset the stamp names.
+    std::vector<std::vector<int> > *m2 = 0;
+    if (XD::MOSFET_B4::Instance *b4 = dynamic_cast<XD::MOSFET_B4::Instance *>(d)) {
+      std::vector<std::vector<int> > &map2 = b4->*xref_member(B4JacMap2());
+      if (map2.size() > 6 && map2[6].size() == 7 && map2[1].size() == 6) {
+        map2[1].push_back(map2[6][6]);
+        m2 = &map2;
+      }
+    }
     d->registerJacLIDs(jl);
+    if (m2) (*m2)[1].pop_back();
     d->setupPointers();
   }
   return 0;

@@ -205,9 +205,9 @@ def test_load_is_deterministic():
 def test_unsupported_card_is_refused():
     c = netlist.inverter_ring(5)
     rowptr, colind = netlist.jacobian_pattern(c)
-    cards, im, nd, params = family_inputs(c, [ModelCard(False, {"TRNQSMOD": 1}), ModelCard(True, {})])
+    cards, im, nd, params = family_inputs(c, [ModelCard(False, {"MTRLMOD": 1}), ModelCard(True, {})])
     from xyce_b200._native import NativeError
-    with pytest.raises(NativeError, match="trnqsMod"):
+    with pytest.raises(NativeError, match="mtrlMod"):
         Bsim4Device(cards, im, nd, params, (rowptr, colind), c.n_unknowns)
 
 

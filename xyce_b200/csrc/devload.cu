@@ -1125,7 +1125,8 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
   // cards need them.
   const bool gen = family == kFamilyBsim4 && (fam->inst_internal_gen != nullptr || family_needs_gen(rt));
   if (gen && !fam->inst_internal_gen)
-    return fail(-1, "the instances use gate or body resistance, rdsMod 1 or initial conditions: pass their internal "
+    return fail(-1, "the instances use gate or body resistance, rdsMod 1, the NQS charge node or initial conditions: "
+                    "pass their internal "
                     "unknowns in inst_internal_gen (xd_internal_nodes_gen lists which instances have which)");
   if (gen && fam->inst_internal)
     return fail(-1, "pass the internal unknowns in inst_internal_gen only (it includes the drain and source ones)");

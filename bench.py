@@ -130,6 +130,79 @@ def other_families(c, rowptr, colind, sol, dev_id, args):
     return out
 
 
+def general_family(args, dev_id, n_mos=200_000):
+    """Load throughput of BSIM4's general topology: a seeded gate netlist whose NMOS cards use gate
+    resistance with a gate-mid node (rgateMod 3), the body network (rbodyMod 1), bias-dependent S/D
+    resistance (rdsMod 1) and the NQS charge node, and whose PMOS cards use rgateMod 2 with the
+    five-resistor body network (rbodyMod 2): 15 local nodes and 85 stamp entries per instance.
+    xd_load_assign with transient flags and limiting on, every evaluation launch shape that fits
+    (fused and split) timed over 10 steps after 3 warm-up steps, and the autotuner's pick."""
+    import ctypes
+
+    import torch
+
+    from xyce_b200 import ModelCard, MosfetDevice, SolverFlags, _native, netlist
+    from xyce_b200.device import internal_nodes
+
+    lib = _native.load()
+    c = netlist.random_logic(n_mos, seed=args.seed + 7)
+    n = c.n_mos
+    cards = [ModelCard(False, {"RGATEMOD": 3, "RBODYMOD": 1, "RDSMOD": 1, "TRNQSMOD": 1, "RSH": 20.0}),
+             ModelCard(True, {"RGATEMOD": 2, "RBODYMOD": 2, "RBPS0": 60.0, "RBPD0": 70.0})]
+    extra = {"NRD": np.full(n, 2.0), "NRS": np.full(n, 1.5)}
+    cards, im, nd, params = netlist.mosfet_family(c, cards, extra)
+    flags, general = internal_nodes(cards, im, nd, params, general=True)
+    assert general
+    c = netlist.with_internal_nodes(c, flags)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    nu, nnz = c.n_unknowns, int(rowptr[-1])
+    fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), nu, device=dev_id, level=14,
+                       inst_internal=c.mos_internal)
+    f64 = dict(dtype=torch.float64, device=f"cuda:{dev_id}")
+    sol = torch.as_tensor(np.random.default_rng(args.seed).uniform(0.0, 1.2, nu), **f64)
+    sta = [torch.zeros(fam.n_state, **f64) for _ in range(2)]
+    sto = [torch.zeros(fam.n_store, **f64) for _ in range(2)]
+    bufs = [torch.zeros(nu, **f64) for _ in range(4)] + [torch.zeros(nnz, **f64) for _ in range(2)]
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    fam.load(SolverFlags(newton_iter=1, voltlim=0), sol, sta[0], sta[1], sto[0], sto[1], *bufs)
+    picked = lib.xd_get_eval_variant(fam._h)
+
+    def time_steps():
+        fl = SolverFlags(newton_iter=1).to_c()
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+        def step():
+            _native.check(lib.xd_load_assign(fam._h, ctypes.byref(fl), p(sol), p(sta[0]), p(sta[1]), p(sto[0]),
+                                             p(sto[1]), *[p(b) for b in bufs], st), "xd_load_assign")
+
+        for _ in range(3):
+            step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(10):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 10
+
+    shapes = {}
+    for v in range(lib.xd_num_eval_variants()):
+        if lib.xd_eval_variant_general(v) == 1 and lib.xd_set_eval_variant(fam._h, v) == 0:
+            blk, minb = ctypes.c_int(), ctypes.c_int()
+            lib.xd_eval_variant_info(v, ctypes.byref(blk), ctypes.byref(minb))
+            key = f"{'split' if lib.xd_eval_variant_split(v) == 1 else 'fused'} {blk.value}x{minb.value}"
+            shapes[key] = time_steps()
+    lib.xd_set_eval_variant(fam._h, picked)
+    ms = time_steps()
+    fam.close()
+    return {"workload": f"seeded INV/NAND2/NOR2 netlist, {n} BSIM4 MOSFETs with the general topology (NMOS rgateMod 3, "
+                        f"rbodyMod 1, rdsMod 1, trnqsMod 1; PMOS rgateMod 2, rbodyMod 2), {int(flags.sum())} internal "
+                        f"unknowns, {nnz} Jacobian nnz",
+            "ms_per_step": ms, "loads_per_s": n / (ms * 1e-3), "eval_variant": picked,
+            "ms_per_step_by_launch_shape": shapes}
+
+
 def batched_section(args, dev_id):
     """The batched Monte-Carlo sweep: 256 circuits (sizes log-uniform 1k-20k MOSFETs, per-circuit
     DELVTO ~ N(0, 30 mV) and TOXE x U[0.98, 1.02]) merged into one block-diagonal system, every
@@ -299,7 +372,7 @@ def transient_section(args):
     import torch
 
     from oracle.transient import OracleTransient
-    from xyce_b200 import Bsim3Device, MosfetDevice, netlist, surrogate as S
+    from xyce_b200 import Bsim3Device, MosfetDevice, SolverFlags, netlist, surrogate as S
     from xyce_b200.transient import GpuTransient, NewtonParams
 
     out = {}
@@ -341,30 +414,47 @@ def transient_section(args):
         "cpu_newton_iters_per_step": float(np.mean(c_st.newton_iters)), "steps": len(g_st.newton_iters),
         "node1_swing_v": [float(g_w[:, 0].min()), float(g_w[:, 0].max())]}
     fam.close()
-    # Learned warm start on a BSIM4 gate netlist.
+    # Learned warm start on the placed gate netlist (the placed-netlist transient's circuit).
     t0 = time.perf_counter()
     sur = S.BsimSurrogate(seed=0)
     rep = sur.train(n_samples=args.surrogate_samples // 2, epochs=8)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    c = netlist.random_logic(1200, seed=7, n_inputs=16)
+    n_ws = args.placed_mos if args.placed_mos > 0 else 100_000
+    c = netlist.random_logic(n_ws, seed=args.seed, n_inputs=64, locality=64)
     rowptr, colind = netlist.jacobian_pattern(c)
     cards, im, nd, params = netlist.mosfet_family(c, None)
     res, waves = {}, {}
     for mode in ("plain", "warm_start"):
         fam = MosfetDevice(cards, im, nd, params, (rowptr, colind), c.n_unknowns, level=14)
-        g = GpuTransient(c, fam, rowptr, colind)
+        g = GpuTransient(c, fam, rowptr, colind, solver="rf")
         g.predictor = "linear"
         if mode == "warm_start":
             g.surrogate = S.SurrogateLoads(sur, fam, c.mos_type, c.mos_nodes, c.mos_w, c.mos_l)
-        g.dcop()
+        g.dcop(x0=netlist.logic_initial_guess(c))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, waves[mode] = g.run(1e-9, 10e-12, params=NewtonParams.transient(), record=np.arange(c.n_nodes))
+        _, waves[mode] = g.run(args.placed_ns * 1e-9, 10e-12, params=NewtonParams.transient(),
+                               record=np.arange(0, c.n_nodes, 97))
         torch.cuda.synchronize()
+        st = g.stats
         res[mode] = {"s_per_run": time.perf_counter() - t0,
-                     "exact_newton_iters_per_step": float(np.mean(g.stats.newton_iters)),
-                     "factorizations": g.stats.factorizations, "surrogate_loads": g.stats.surrogate_loads}
+                     "exact_newton_iters_per_step": float(np.mean(st.newton_iters)),
+                     "chord_iters_per_step": float(np.mean(st.chord_iters)) if st.chord_iters else 0.0,
+                     "matrices": st.factorizations, "surrogate_loads": st.surrogate_loads}
+        if mode == "warm_start":
+            # One surrogate load against one exact FP64 load of the same instances, at the final point.
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            fl = SolverFlags(newton_iter=1, pdt=1e11, gmin=g.gmin)
+            e[0].record()
+            for _ in range(5):
+                g._surrogate_load()
+            e[1].record()
+            for _ in range(5):
+                g._load_raw(fl)
+            e[2].record()
+            torch.cuda.synchronize()
+            res["load_ms"] = {"surrogate": e[0].elapsed_time(e[1]) / 5, "exact_fp64": e[1].elapsed_time(e[2]) / 5}
         g.close()
         fam.close()
     if args.placed_mos > 0:
@@ -373,10 +463,10 @@ def transient_section(args):
         # The scale configuration's transient: ~1M BSIM4 MOSFETs with placed wiring and ~3M R/C,
         # 2 ns, device-resident state.
         out["scale_1m"] = placed_transient(args, args.scale_mos, args.scale_ns)
-    out["warm_start_bsim4_gates"] = {
-        "workload": f"seeded INV/NAND2/NOR2 netlist, {c.n_mos} BSIM4 MOSFETs, RC wires, 16 PWL inputs, "
-                    f"{c.n_unknowns} unknowns, 0-1 ns at 10 ps, linear predictor on both paths",
-        "plain": res["plain"], "warm_start": res["warm_start"],
+    out["warm_start_placed"] = {
+        "workload": f"the placed netlist: {c.n_mos} BSIM4 MOSFETs, {c.n_unknowns} unknowns, operating point, "
+                    f"0-{args.placed_ns:g} ns at 10 ps, linear predictor on both paths, GPU refactorization",
+        "plain": res["plain"], "warm_start": res["warm_start"], "load_ms": res["load_ms"],
         "max_waveform_difference_v": float(np.abs(waves["plain"] - waves["warm_start"]).max()),
         "surrogate": {"train_s": train_s, "samples": 2 * (args.surrogate_samples // 2),
                       "heldout_rel_error_median_p95": {t: {k: [round(v["rel_median"], 4), round(v["rel_p95"], 4)]
@@ -397,7 +487,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-transient", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
+    ap.add_argument("--surrogate-samples", type=int, default=20_000_000,
+                    help="surrogate training samples in all (half per device type)")
     ap.add_argument("--placed-mos", type=int, default=100_000, help="MOSFETs of the placed-netlist transient (0: skip)")
     ap.add_argument("--placed-ns", type=float, default=1.0, help="length of the placed-netlist transient (ns)")
     ap.add_argument("--scale-mos", type=int, default=0,
@@ -713,6 +804,18 @@ def main():
     e2e_ms = e0.elapsed_time(e1) / args.steps
     _, e2e_ms = replica_totals(dist, n, e2e_ms, f"cuda:{dev_id}")
     e2e_value = n_all / (e2e_ms * 1e-3)
+    # The link the end-to-end step is bound by: the same device-to-host copies of one step's
+    # outputs, alone (no load, no host-to-device traffic), from the same buffers.
+    d_set, h_set = sets[0][0], sets[0][1]
+    e0.record(s_copy)
+    for _ in range(3):
+        with torch.cuda.stream(s_copy):
+            for key in ("f", "q", "fx", "qx", "jf", "jq", "sta_n", "sto_n"):
+                h_set[key].copy_(d_set[key], non_blocking=True)
+    e1.record(s_copy)
+    torch.cuda.synchronize()
+    d2h_alone_gbs = d2h * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    d2h_e2e_gbs = d2h / (e2e_ms * 1e-3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -755,13 +858,16 @@ def main():
         "fp64": {"probe_peak_tflops": fp64_peak_tflops, "flops_per_instance": EVAL_FP64_FLOPS_PER_INST,
                  "eval_achieved_tflops": EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12,
                  "eval_frac": EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12 / fp64_peak_tflops},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "link": {"bound": "device-to-host copy", "achieved_gbs": d2h_e2e_gbs,
+                         "copies_alone_gbs": d2h_alone_gbs, "frac": d2h_e2e_gbs / d2h_alone_gbs}},
         "clocks": clk.summary(),
     }
     if cpu is not None:
         result["cpu_baseline"] = cpu
     if rank == 0 and world == 1 and not args.no_batched:
         result["other_families"] = other_families(c, rowptr, colind, sol, dev_id, args)
+        result["other_families"]["bsim4_general_topology"] = general_family(args, dev_id)
         result["batched"] = batched_section(args, dev_id)
     if rank == 0 and world == 1 and not args.no_transient:
         from oracle import xyce_ref as xr

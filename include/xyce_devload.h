@@ -234,6 +234,9 @@ int xd_eval_variant_persistent(int v);
  * kernel is smaller than the fused one (fewer registers, a smaller instruction footprint). Its
  * results are bit-identical to the fused candidates'. 0 otherwise, < 0 for a bad v. */
 int xd_eval_variant_split(int v);
+/* 1 when candidate v evaluates BSIM4's general topology (the only candidates a general-topology
+ * family fits), 0 otherwise, < 0 for a bad v. */
+int xd_eval_variant_general(int v);
 int xd_get_eval_variant(const xd_ctx *ctx);
 int xd_set_eval_variant(xd_ctx *ctx, int v);
 int xd_probe_fp64_fma(double *d_out, int blocks, int iters, void *stream);

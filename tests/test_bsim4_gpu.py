@@ -258,7 +258,8 @@ def test_split_evaluation_equals_fused_bitwise():
            SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=1)]
     rng = np.random.default_rng(9)
     sols = [rng.uniform(-0.3, 1.5, c.n_unknowns) for _ in seq]
-    split = [v for v in range(lib.xd_num_eval_variants()) if lib.xd_eval_variant_split(v) == 1]
+    split = [v for v in range(lib.xd_num_eval_variants())
+             if lib.xd_eval_variant_split(v) == 1 and lib.xd_eval_variant_general(v) == 0]
     assert split
     outs = {}
     for v in [10] + split:

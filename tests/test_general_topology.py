@@ -203,3 +203,47 @@ def test_reference_ic_coupling_placement(rgate, rbody, nrd, nrs, ic, consistent)
         f1 = orc.load(fl, x1, z8, z8, z14, z14)["f"]
         if c_ >= c.n_nodes + c.n_vsrc:  # a branch current: F is linear in it
             assert f1[r_] - f0[r_] == pytest.approx(want[(r_, c_)], abs=1e-9)
+
+
+@pytest.mark.gpu
+def test_general_launch_shapes_equal_bitwise():
+    """Every launch shape of the general topology — fused, and split into the DC part and the
+    charge-and-stamp part handing the general state over through the context's buffer — gives the
+    same loads bit for bit over a flag sequence that takes each path of the hand-off (limiting off
+    and on, the first transient step, junction initialisation, a DC load), NQS instances included."""
+    pytest.importorskip("torch")
+    from tests.gpu_parity import GpuRun
+    from xyce_b200 import MosfetDevice, _native
+
+    lib = _native.load()
+    c, cards, extra, flags = _circuit("nqs_rgate", n_mos=3000, seed=5)
+    rowptr, colind = netlist.jacobian_pattern(c)
+    cards_, im, nd, params = family_inputs(c, cards, extra)
+    n = im.shape[0]
+    seq = [SolverFlags(newton_iter=1, voltlim=0), SolverFlags(newton_iter=0, init_tran=1),
+           SolverFlags(newton_iter=2), SolverFlags(dcop=1, transient=0, newton_iter=0, init_jct=1),
+           SolverFlags(dcop=1, transient=0, tranop=1, newton_iter=1)]
+    rng = np.random.default_rng(3)
+    sols = [rng.uniform(-0.3, 1.5, c.n_unknowns) for _ in seq]
+    shapes = [v for v in range(lib.xd_num_eval_variants()) if lib.xd_eval_variant_general(v) == 1]
+    assert any(lib.xd_eval_variant_split(v) == 1 for v in shapes)
+    outs = {}
+    for v in shapes:
+        dev = MosfetDevice(cards_, im, nd, params, (rowptr, colind), c.n_unknowns, inst_internal=c.mos_internal)
+        assert dev._lib.xd_set_eval_variant(dev._h, v) == 0
+        gpu = GpuRun(dev, int(rowptr[-1]), c.n_unknowns)
+        ns = dev.n_state_slots
+        sta_n, sta_c, sto_n, sto_c = np.zeros(ns * n), np.zeros(ns * n), np.zeros(14 * n), np.zeros(14 * n)
+        res = []
+        for fl, sol in zip(seq, sols):
+            g = gpu.load(fl, sol, sta_n, sta_c, sto_n, sto_c)
+            res.append(g)
+            sta_n, sta_c, sto_n = g["next_sta"], g["curr_sta"], g["next_sto"]
+        outs[v] = res
+        dev.close()
+    ref = outs[shapes[0]]
+    for v in shapes[1:]:
+        for step, (a, b) in enumerate(zip(ref, outs[v])):
+            for k in a:
+                if k != "abs":
+                    assert np.array_equal(a[k], b[k], equal_nan=True), (v, step, k)

@@ -99,6 +99,7 @@ SIGNATURES = {
     "xd_eval_variant_info": (ctypes.c_int, [ctypes.c_int, _ip, _ip]),
     "xd_eval_variant_persistent": (ctypes.c_int, [ctypes.c_int]),
     "xd_eval_variant_split": (ctypes.c_int, [ctypes.c_int]),
+    "xd_eval_variant_general": (ctypes.c_int, [ctypes.c_int]),
     "xd_get_eval_variant": (ctypes.c_int, [ctypes.c_void_p]),
     "xd_set_eval_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "xd_load_static_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XdFlags)] + [ctypes.c_void_p] * 12),

@@ -253,29 +253,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_charge_stamp_kernel(
   bsim4_write_one<SERIES>(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
 }
 
-// General topology: one thread per instance over the 15 local nodes; the full store block is read
-// (the limiters of the gate, source / drain and body-network voltages compare against it) and the
-// eight state slots written.
-template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_kernel(
-    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
-    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
-    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
-    double *__restrict__ stage, xb4::LoadFlags fl) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double V[xb4::kGenNodes], sto_old[xb4::kNumStore];
+// General topology: the 15 local nodes' values of instance i (absent nodes and ground read 0 V).
+__device__ __forceinline__ void bsim4_gen_gather(int i, int n, const int *__restrict__ gmap,
+                                                 const double *__restrict__ sol, double *V) {
 #pragma unroll
   for (int k = 0; k < xb4::kGenNodes; ++k) {
     const int u = gmap[(size_t)k * n + i];
     V[k] = u >= 0 ? sol[u] : 0.0;
   }
-  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
-#pragma unroll
-  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
-  xb4::RecPtr rp{tab + rec[i], nrec};
-  xb4::LoadOut o;
-  xb4::bsim4_load<true, false, 0, true>(rp, V, sto_old, fl, vgb[i], o);
+}
+
+// General topology: one instance's staged stamps (15 vector rows x 4, 85 dF/dx and 85 dQ/dx
+// slots), store (vged / vgmd kept from the input), eight state slots and carried vgb.
+__device__ __forceinline__ void bsim4_gen_write(int i, int n, const xb4::LoadOut &o, double *__restrict__ next_sta,
+                                                double *__restrict__ curr_sta, double *__restrict__ next_sto,
+                                                double *__restrict__ vgb, double *__restrict__ stage) {
 #pragma unroll
   for (int k = 0; k < 4 * xb4::kGenNodes; ++k) stage[(size_t)k * n + i] = o.gv[k];
   const size_t mf = 4 * xb4::kGenNodes, mq = mf + xb4::kGenSlots;
@@ -293,6 +285,70 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_kernel(
     for (int k = 0; k < xb4::kGenState; ++k) curr_sta[(size_t)k * n + i] = o.gsta[k];
   }
   vgb[i] = o.vgb;
+}
+
+// General topology: one thread per instance over the 15 local nodes; the full store block is read
+// (the limiters of the gate, source / drain and body-network voltages compare against it) and the
+// eight state slots written.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, const double *__restrict__ curr_sto, double *__restrict__ vgb,
+    double *__restrict__ stage, xb4::LoadFlags fl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[xb4::kGenNodes], sto_old[xb4::kNumStore];
+  bsim4_gen_gather(i, n, gmap, sol, V);
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load<true, false, 0, true>(rp, V, sto_old, fl, vgb[i], o);
+  bsim4_gen_write(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
+}
+
+// General topology, split like bsim4_dc_kernel / bsim4_charge_stamp_kernel: the DC part writes the
+// general hand-off state (kNumMidGen doubles per instance, slot-major), the charge-and-stamp part
+// reads it; together they load what bsim4_gen_kernel loads, bit for bit.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_dc_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
+    const double *__restrict__ sol, const double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    const double *__restrict__ vgb, xb4::LoadFlags fl, double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[xb4::kGenNodes], sto_old[xb4::kNumStore];
+  bsim4_gen_gather(i, n, gmap, sol, V);
+  const double *so = (fl.newton_iter == 0) ? curr_sto : next_sto;
+#pragma unroll
+  for (int k = 0; k < xb4::kNumStore; ++k) sto_old[k] = so[(size_t)k * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::Mid m;
+  xb4::bsim4_load<true, false, 1, true>(rp, V, sto_old, fl, vgb[i], o, nullptr, &m);
+#pragma unroll
+  for (int f = 0; f < xb4::kNumMidGen; ++f) mid[(size_t)f * n + i] = m.v[f];
+}
+
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_gen_cs_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int *__restrict__ gmap,
+    const double *__restrict__ sol, double *__restrict__ next_sta, double *__restrict__ curr_sta,
+    double *__restrict__ next_sto, double *__restrict__ vgb, double *__restrict__ stage, xb4::LoadFlags fl,
+    const double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double V[xb4::kGenNodes];
+  bsim4_gen_gather(i, n, gmap, sol, V);
+  xb4::Mid m;
+#pragma unroll
+  for (int f = 0; f < xb4::kNumMidGen; ++f) m.v[f] = mid[(size_t)f * n + i];
+  xb4::RecPtr rp{tab + rec[i], nrec};
+  xb4::LoadOut o;
+  xb4::bsim4_load<true, false, 2, true>(rp, V, nullptr, fl, vgb[i], o, nullptr, &m);
+  bsim4_gen_write(i, n, o, next_sta, curr_sta, next_sto, vgb, stage);
 }
 
 // One thread per instance. PERSIST: the grid is one wave of resident blocks that walks the
@@ -671,7 +727,7 @@ struct EvalVariant {
   bool persist;  // one wave of resident blocks with a grid-stride loop
   bool split;    // two kernels: the DC part (min_blocks), then charges and stamps (min_blocks2)
   int min_blocks2;
-  bool gen;      // BSIM4 general topology (15 local nodes, 85 stamp slots)
+  bool gen;      // BSIM4 general topology (15 local nodes, 85 stamp slots; split: the general hand-off)
 };
 constexpr int B4 = 4, B3 = 3, M1 = 1;  // kFamilyBsim4, kFamilyBsim3, kFamilyMos1
 constexpr EvalVariant kEvalVariants[] = {
@@ -687,7 +743,8 @@ constexpr EvalVariant kEvalVariants[] = {
     {B3, 128, 3, false, false, false, false, 0}, {B3, 64, 4, false, false, false, false, 0},
     {M1, 128, 1, false, false, false, false, 0}, {M1, 128, 4, false, false, false, false, 0},
     {M1, 256, 2, false, false, false, false, 0}, {M1, 64, 8, false, false, false, false, 0},
-    {B4, 128, 1, true, false, false, false, 0, true}, {B4, 128, 2, true, false, false, false, 0, true}};
+    {B4, 128, 1, true, false, false, false, 0, true}, {B4, 128, 2, true, false, false, false, 0, true},
+    {B4, 128, 2, true, false, false, true, 2, true},  {B4, 128, 3, true, false, false, true, 3, true}};
 constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8, kFirstBsim3Variant = 16, kFirstMos1Variant = 20;
 constexpr int kFirstGenVariant = 24;
 // A variant computes a context's loads exactly if it is for the context's family and, for BSIM4, its
@@ -697,7 +754,7 @@ bool variant_fits(const xd_ctx *ctx, int v) {
   const EvalVariant &e = kEvalVariants[v];
   if (e.family != ctx->family) return false;
   if (ctx->family != kFamilyBsim4) return true;
-  if (e.gen || ctx->gen) return e.gen == ctx->gen;
+  if (e.gen || ctx->gen) return e.gen == ctx->gen && (!e.split || ctx->d_mid != nullptr);
   return e.series == ctx->series && (e.full || !ctx->needs_full) && (!e.split || ctx->d_mid != nullptr);
 }
 constexpr int kNumEvalVariants = sizeof(kEvalVariants) / sizeof(kEvalVariants[0]);
@@ -775,11 +832,29 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
   if (kEvalVariants[v].gen) {
 #define XD_GEN_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_gmap, sol, next_sta, curr_sta, next_sto, curr_sto, \
                     ctx->d_vgb, stage, fl
-    if (v == kFirstGenVariant)
-      bsim4_gen_kernel<128, 1><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
-    else
-      bsim4_gen_kernel<128, 2><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
+#define XD_GEN_DC_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_gmap, sol, next_sto, curr_sto, ctx->d_vgb, fl, \
+                       ctx->d_mid
+#define XD_GEN_CS_ARGS n, ctx->d_tab, ctx->n_rec, ctx->d_rec, ctx->d_gmap, sol, next_sta, curr_sta, next_sto, \
+                       ctx->d_vgb, stage, fl, ctx->d_mid
+    switch (v - kFirstGenVariant) {
+      case 0:
+        bsim4_gen_kernel<128, 1><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
+        break;
+      case 1:
+        bsim4_gen_kernel<128, 2><<<grid, blk, 0, st>>>(XD_GEN_ARGS);
+        break;
+      case 2:
+        bsim4_gen_dc_kernel<128, 2><<<grid, blk, 0, st>>>(XD_GEN_DC_ARGS);
+        bsim4_gen_cs_kernel<128, 2><<<grid, blk, 0, st>>>(XD_GEN_CS_ARGS);
+        break;
+      default:
+        bsim4_gen_dc_kernel<128, 3><<<grid, blk, 0, st>>>(XD_GEN_DC_ARGS);
+        bsim4_gen_cs_kernel<128, 3><<<grid, blk, 0, st>>>(XD_GEN_CS_ARGS);
+        break;
+    }
 #undef XD_GEN_ARGS
+#undef XD_GEN_DC_ARGS
+#undef XD_GEN_CS_ARGS
     return;
   }
   if (kEvalVariants[v].persist) grid = std::max(1, std::min(grid, ctx->resident_blocks[v]));
@@ -1322,8 +1397,11 @@ int xd_create(const xd_mosfet_family *fam, const xd_csr *pat, int cuda_device, x
               (ce = cudaMemcpy(ctx->d_gmap, gmap.data(), gmap.size() * sizeof(int), cudaMemcpyHostToDevice)) !=
                   cudaSuccess))
     return cleanup(cuda_fail(ce, "xd_create allocation"));
+  // Hand-off state of the split evaluation: the common card's, or the general topology's.
   if (family == kFamilyBsim4 && !series && !gen && !ctx->needs_full && n > 0 &&
       (ce = cudaMalloc(&ctx->d_mid, (size_t)xb4::kNumMid * n * sizeof(double))) != cudaSuccess)
+    return cleanup(cuda_fail(ce, "xd_create allocation"));
+  if (gen && n > 0 && (ce = cudaMalloc(&ctx->d_mid, (size_t)xb4::kNumMidGen * n * sizeof(double))) != cudaSuccess)
     return cleanup(cuda_fail(ce, "xd_create allocation"));
   if ((rc = build_map(vt, vs, nu, ctx->vmap)) != 0) return cleanup(rc);
   if ((rc = build_map(mt, ms, ctx->nnz, ctx->mmap)) != 0) return cleanup(rc);
@@ -1470,6 +1548,11 @@ int xd_eval_variant_persistent(int v) {
 int xd_eval_variant_split(int v) {
   if (v < 0 || v >= kNumEvalVariants) return fail(-1, "bad variant query");
   return kEvalVariants[v].split ? 1 : 0;
+}
+
+int xd_eval_variant_general(int v) {
+  if (v < 0 || v >= kNumEvalVariants) return fail(-1, "bad variant query");
+  return kEvalVariants[v].gen ? 1 : 0;
 }
 
 int xd_get_eval_variant(const xd_ctx *ctx) { return ctx ? ctx->eval_variant : -1; }

@@ -17,7 +17,6 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
-#include <mutex>
 #include <vector>
 
 #include "../../include/xyce_devload.h"
@@ -1602,23 +1601,17 @@ constexpr size_t kStaticStage = (size_t)XD_STATIC_MAX_INSTANCES * xb4::kNumStage
 constexpr size_t kStaticPartial = (size_t)4 * XD_STATIC_MAX_INSTANCES;
 static __device__ __align__(256) double g_static_scratch[kStaticStage + kStaticPartial];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mu;
-double *g_static_ptr[kMaxDevices] = {nullptr};
-
-// Device address of g_static_scratch on the current device (resolved once per device). In host
-// code the symbol names a host-side stand-in, never a device address, so kernels only ever get
-// the address cudaGetSymbolAddress returns.
+// Device address of g_static_scratch on the current device. In host code the symbol names a
+// host-side stand-in, never a device address, so kernels only ever get the address
+// cudaGetSymbolAddress returns. Resolved on every call (it allocates nothing and costs little
+// next to the evaluation): an address kept from an earlier call would dangle once the device's
+// primary context had been reset and created again.
 int static_scratch_on(int dev, double **out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(-1, "device ordinal out of range for static scratch");
-  std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_ptr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
-    g_static_ptr[dev] = static_cast<double *>(p);
-  }
-  *out = g_static_ptr[dev];
+  (void)dev;
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+  *out = static_cast<double *>(p);
   return 0;
 }
 

@@ -196,7 +196,7 @@ struct Bias {
   int origFlag;
 };
 
-// V: with GEN the 14 local node values (GenNode order; collapsed nodes carry their representative's
+// V: with GEN the 15 local node values (GenNode order; collapsed nodes carry their representative's
 // value), else the 4 (D', G, S', B) with Vx the external (D, S) under SERIES.
 template <bool SERIES, bool GEN = false, class RV>
 XD_HD void bsim4_bias(const RV &P_, const double *V, const LoadFlags &fl, const double *Vx, Bias &b) {
@@ -1502,7 +1502,7 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
   (void)ceqgstot; (void)ceqgdtot;
 
   if constexpr (GEN) {
-    // ---- General topology: the reference's loads over the 14 local nodes ----
+    // ---- General topology: the reference's loads over the 15 local nodes ----
     const bool lim = fl.voltlim && !origFlag;
     // Terminal resistor and body-network currents (:11896-11917).
     const double Idrain = rdsMod ? gdtot * Vddp : P(drainConductance) * Vddp;
@@ -2044,7 +2044,7 @@ XD_HD void bsim4_finish(const RV &P_, const double *V, const LoadFlags &fl, doub
 // resistances (rdsMod = 0, sheet resistance) load into vecx / jfx.
 // PART = 0: the whole evaluation; 1: the DC part only, which fills *mid; 2: the charge-and-stamp
 // part only, from *mid (the DC part of the same instance, same inputs).
-// GEN = true: the general topology; V holds the 14 local node values, sto_old all 14 store slots,
+// GEN = true: the general topology; V holds the 15 local node values, sto_old all 14 store slots,
 // and the outputs go to gv / gf / gq / gsta (the variant is compiled FULL and without SERIES).
 template <bool FULL = false, bool SERIES = false, int PART = 0, bool GEN = false, class RV>
 XD_HD void bsim4_load(const RV &P_, const double *V, const double *sto_old, const LoadFlags &fl, double vgb_orig,

@@ -147,8 +147,10 @@ def test_gate_tunnelling_family_refuses_variants_without_it():
     dev.close()
     # 6, 7 and 11 are the full ones; 8, 9 are for internal nodes; 10 is a persistent common one;
     # 12-15 split the common evaluation into two kernels; 16-23 are for BSIM3 and MOSFET1; 24-27
-    # for the general topology (24, 25 fused, 26, 27 split).
-    assert ok == [False] * 6 + [True] * 2 + [False] * 2 + [False] + [True] + [False] * 4 + [False] * 8 + [False] * 4
+    # for the general topology (24, 25 fused, 26, 27 split); 28, 29 split the common evaluation with
+    # the DC part at 112 registers in 96- or 64-thread blocks.
+    assert ok == ([False] * 6 + [True] * 2 + [False] * 2 + [False] + [True] + [False] * 4 + [False] * 8 + [False] * 4
+                  + [False] * 2)
 
 
 @pytest.mark.parametrize("variant", ["all", "mixed"])

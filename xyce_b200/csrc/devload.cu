@@ -211,13 +211,14 @@ __device__ __forceinline__ void bsim4_eval_one(
 
 // Split evaluation, first kernel: the DC part of one instance (limiting, junction diodes, drain
 // current, GIDL / GISL, gate tunnelling); its hand-off state goes to mid, slot-major.
-template <int BLOCK, int MINB, bool FULL, bool SERIES>
-__global__ void __launch_bounds__(BLOCK, MINB) bsim4_dc_kernel(
-    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
-    const double *__restrict__ sol, const double *__restrict__ next_sto, const double *__restrict__ curr_sto,
-    const double *__restrict__ vgb, xb4::LoadFlags fl, const int2 *__restrict__ ext, double *__restrict__ mid) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Split evaluation, first kernel's body: the DC part of instance i into the hand-off buffer.
+template <bool FULL, bool SERIES>
+__device__ __forceinline__ void bsim4_dc_one(int i, int n, const double *__restrict__ tab, int nrec,
+                                             const int *__restrict__ rec, const int4 *__restrict__ nodes,
+                                             const double *__restrict__ sol, const double *__restrict__ next_sto,
+                                             const double *__restrict__ curr_sto, const double *__restrict__ vgb,
+                                             const xb4::LoadFlags &fl, const int2 *__restrict__ ext,
+                                             double *__restrict__ mid) {
   double V[4], Vx[2], sto_old[xb4::kNumStore];
   bsim4_gather_v<SERIES>(i, nodes, ext, sol, V, Vx);
   bsim4_sto_old(i, n, next_sto, curr_sto, fl, sto_old);
@@ -228,6 +229,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_dc_kernel(
   constexpr int nm = FULL ? xb4::kNumMidFull : xb4::kNumMid;
 #pragma unroll
   for (int f = 0; f < nm; ++f) mid[(size_t)f * n + i] = m.v[f];
+}
+
+template <int BLOCK, int MINB, bool FULL, bool SERIES>
+__global__ void __launch_bounds__(BLOCK, MINB) bsim4_dc_kernel(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, const double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    const double *__restrict__ vgb, xb4::LoadFlags fl, const int2 *__restrict__ ext, double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bsim4_dc_one<FULL, SERIES>(i, n, tab, nrec, rec, nodes, sol, next_sto, curr_sto, vgb, fl, ext, mid);
+}
+
+// The same DC part under an explicit register budget instead of launch bounds: 112 registers a
+// thread let 18 warps reside per SM (six 96-thread or nine 64-thread blocks) where 128 x 4 holds 16.
+template <int REGS>
+__global__ void __maxnreg__(REGS) bsim4_dc_kernel_regs(
+    int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,
+    const double *__restrict__ sol, const double *__restrict__ next_sto, const double *__restrict__ curr_sto,
+    const double *__restrict__ vgb, xb4::LoadFlags fl, const int2 *__restrict__ ext, double *__restrict__ mid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bsim4_dc_one<false, false>(i, n, tab, nrec, rec, nodes, sol, next_sto, curr_sto, vgb, fl, ext, mid);
 }
 
 // Split evaluation, second kernel: charges, capacitances, store / state and the stamps of one
@@ -743,7 +766,8 @@ constexpr EvalVariant kEvalVariants[] = {
     {M1, 128, 1, false, false, false, false, 0}, {M1, 128, 4, false, false, false, false, 0},
     {M1, 256, 2, false, false, false, false, 0}, {M1, 64, 8, false, false, false, false, 0},
     {B4, 128, 1, true, false, false, false, 0, true}, {B4, 128, 2, true, false, false, false, 0, true},
-    {B4, 128, 2, true, false, false, true, 2, true},  {B4, 128, 3, true, false, false, true, 3, true}};
+    {B4, 128, 2, true, false, false, true, 2, true},  {B4, 128, 3, true, false, false, true, 3, true},
+    {B4, 96, 6, false, false, false, true, 4},        {B4, 64, 9, false, false, false, true, 4}};
 constexpr int kFirstFullVariant = 6, kFirstSeriesVariant = 8, kFirstBsim3Variant = 16, kFirstMos1Variant = 20;
 constexpr int kFirstGenVariant = 24;
 // A variant computes a context's loads exactly if it is for the context's family and, for BSIM4, its
@@ -875,10 +899,18 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
         bsim4_dc_kernel<128, 5, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
         bsim4_charge_stamp_kernel<128, 5, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
         break;
-      default:
+      case 15:
         bsim4_dc_kernel<128, 4, false, false><<<grid, blk, 0, st>>>(XD_DC_ARGS);
         bsim4_charge_stamp_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
         break;
+      default: {
+        // The DC part at 112 registers in 96- or 64-thread blocks (18 resident warps per SM), the
+        // charge / stamp part in 128 x 4.
+        const int grid128 = (n + 127) / 128;
+        bsim4_dc_kernel_regs<112><<<grid, blk, 0, st>>>(XD_DC_ARGS);
+        bsim4_charge_stamp_kernel<128, 4, false, false><<<grid128, 128, 0, st>>>(XD_CS_ARGS);
+        break;
+      }
     }
 #undef XD_DC_ARGS
 #undef XD_CS_ARGS

@@ -18,7 +18,9 @@
 //     end, so no row of level l can have reused the slot), others are read from global memory.
 // Levels of short rows are solved a thread per row, others a warp per row; levels with more rows
 // or entries than a staging slot holds are read from global memory directly. Every sum is reduced
-// in a fixed order, so results do not depend on the timing.
+// in a fixed order, so results do not depend on the timing. In a staged level the short rows (at
+// most kShortRow entries, ordered first by the set-up) are solved a thread each while the warps the
+// short rows leave free solve the longer rows a warp each.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,7 +47,8 @@ constexpr int kSlotRows = 256;          // rows per staged level
 constexpr int kSlotEnts = 2048;         // entries per staged level
 constexpr int kWindow = 1 << 11;        // solved values kept in shared memory
 constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are summed by the whole block
-constexpr int kThreadRowEnts = 4;       // levels averaging at most this many entries a row: a thread a row
+constexpr int kThreadRowEnts = 4;       // unstaged levels averaging at most this many entries a row: a thread a row
+constexpr int kShortRow = 8;            // staged levels: rows of at most this many entries a thread each, longer a warp
 
 constexpr int kEntsPerThread = kSlotEnts / kThreads;
 static_assert(kSlotEnts % kThreads == 0, "a staged level's entries split evenly over the threads");
@@ -56,6 +59,7 @@ struct Smem {
   double xv[kSlots][kSlotEnts];  // solved values of the entries' columns that were final when staged
   int pos[kSlots][kSlotEnts];
   int cut[kSlots];               // columns at positions below cut[s] have their value in xv
+  int nshort[kSlots];            // the level's short rows (they come first)
   double rhs[kSlots][kSlotRows];
   double diag[kSlots][kSlotRows];
   int dst[kSlots][kSlotRows];
@@ -77,7 +81,8 @@ __device__ __forceinline__ void cp_async_wait_ahead() {
 }
 
 // One triangle in level order. meta[l] = (first position, end position, first entry, end entry);
-// lstart[l] = the first of level l's rows longer than kBlockRow entries (they come last).
+// lstart[2l] = the first of level l's rows longer than kBlockRow entries (they come last);
+// lstart[2l + 1] = the first of its rows longer than kShortRow entries (the short ones come first).
 struct Tri {
   const int4 *meta;
   const int *lstart;
@@ -114,6 +119,7 @@ __device__ __forceinline__ bool staged(const int4 &m) { return m.y - m.x <= kSlo
 // waiting for a load.
 struct PosAhead {
   int p[kEntsPerThread];
+  int ls;  // thread 0: the level's first row longer than kShortRow entries
 };
 
 __device__ __forceinline__ PosAhead load_pos(int l, const int4 &m, const Tri &t, int tid) {
@@ -124,6 +130,7 @@ __device__ __forceinline__ PosAhead load_pos(int l, const int4 &m, const Tri &t,
     const int k = tid + q * kThreads;
     a.p[q] = (st && k < m.w - m.z) ? t.epos[m.z + k] : -1;
   }
+  a.ls = (st && tid == 0) ? t.lstart[2 * l + 1] : 0;
   return a;
 }
 
@@ -149,7 +156,10 @@ __device__ __forceinline__ void stage_level(int l, const int4 &m, const PosAhead
         if (pa.p[q] < cut) cp_async8(&sm.xv[s][k], t.out + pa.p[q]);
       }
     }
-    if (tid == 0) sm.cut[s] = cut;
+    if (tid == 0) {
+      sm.cut[s] = cut;
+      sm.nshort[s] = pa.ls - m.x;
+    }
   }
   cp_async_commit();
 }
@@ -179,18 +189,19 @@ __global__ void __launch_bounds__(kThreads) level_solve_kernel(Tri t) {
   auto step = [&](int l, int4 &cur, int4 &ahp, int4 &ahq, PosAhead &pa) {
     const int b = cur.x, e = cur.y, lo = e - kWindow;
     const bool by_thread = cur.w - cur.z <= kThreadRowEnts * (e - b);
-    if (staged(cur) && by_thread) {
-      const int s = l % kSlots, eb = cur.z;
-      for (int r = tid; r < e - b; r += kThreads) {
+    if (staged(cur)) {
+      // Short rows (the first ns) a thread each; longer ones a warp each, on the warps after those
+      // the short rows occupy, at the same time.
+      const int s = l % kSlots, eb = cur.z, ns = sm.nshort[s];
+      for (int r = tid; r < ns; r += kThreads) {
         const int kb = sm.eptr[s][r] - eb, ke = sm.eptr[s][r + 1] - eb;
         double acc = 0.0;
         for (int k = kb; k < ke; ++k) acc += sm.val[s][k] * staged_solved(sm, s, k, lo, t.out);
         const double v = UPPER ? (sm.rhs[s][r] - acc) / sm.diag[s][r] : sm.rhs[s][r] - acc;
         publish<UPPER>(b + r, v, sm.dst[s][r], sm, t);
       }
-    } else if (staged(cur)) {
-      const int s = l % kSlots, eb = cur.z;
-      for (int r = warp; r < e - b; r += kWarps) {
+      const int w0 = min(kWarps - 1, (ns + 31) >> 5);
+      for (int r = ns + warp - w0; warp >= w0 && r < e - b; r += kWarps - w0) {
         const int kb = sm.eptr[s][r] - eb, ke = sm.eptr[s][r + 1] - eb;
         double acc = 0.0;
         for (int k = kb + lane; k < ke; k += 32) acc += sm.val[s][k] * staged_solved(sm, s, k, lo, t.out);
@@ -204,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) level_solve_kernel(Tri t) {
     } else {
       // Unstaged level: rows from global memory, one thread or one warp each; very long rows by
       // the block.
-      const int m = t.lstart[l];
+      const int m = t.lstart[2 * l];
       if (by_thread) {
         for (int r = b + tid; r < m; r += kThreads) {
           const int kb = t.eptr[r], ke = t.eptr[r + 1];
@@ -307,15 +318,19 @@ void build_tri(int n, const std::vector<int> &mp, const std::vector<int> &mi, bo
     lev[r] = d;
     nlev = std::max(nlev, d + 1);
   }
-  // Buckets (level, long): a level's rows longer than kBlockRow entries come after its others.
+  // Buckets (level, length class): within a level the rows of at most kShortRow entries first, then
+  // the longer ones, the rows longer than kBlockRow entries last.
   auto len = [&](int r) {
     int c = 0;
     for (int k = mp[r]; k < mp[r + 1]; ++k) c += (upper ? (mi[k] > r) : (mi[k] < r)) ? 1 : 0;
     return c;
   };
   std::vector<int> bucket(n);
-  for (int r = 0; r < n; ++r) bucket[r] = 2 * lev[r] + (len(r) > kBlockRow ? 1 : 0);
-  std::vector<int> start(2 * (size_t)nlev + 1, 0);
+  for (int r = 0; r < n; ++r) {
+    const int c = len(r);
+    bucket[r] = 3 * lev[r] + (c > kBlockRow ? 2 : c > kShortRow ? 1 : 0);
+  }
+  std::vector<int> start(3 * (size_t)nlev + 1, 0);
   for (int r = 0; r < n; ++r) ++start[bucket[r] + 1];
   for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
   h.rows.assign(n, 0);
@@ -339,11 +354,12 @@ void build_tri(int n, const std::vector<int> &mp, const std::vector<int> &mi, bo
   h.epos.resize(h.src.size());
   for (size_t k = 0; k < h.src.size(); ++k) h.epos[k] = h.pos[mi[h.src[k]]];
   h.meta.assign(nlev, make_int4(0, 0, 0, 0));
-  h.lstart.assign(nlev, 0);
+  h.lstart.assign(2 * (size_t)nlev, 0);
   for (int l = 0; l < nlev; ++l) {
-    const int b = start[2 * l], e = start[2 * l + 2];
+    const int b = start[3 * l], e = start[3 * l + 3];
     h.meta[l] = make_int4(b, e, h.eptr[b], h.eptr[e]);
-    h.lstart[l] = start[2 * l + 1];
+    h.lstart[2 * l] = start[3 * l + 2];
+    h.lstart[2 * l + 1] = start[3 * l + 1];
   }
 }
 

@@ -43,8 +43,8 @@ constexpr int kThreads = XD_SPTRSV_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kAhead = 2;               // levels staged ahead of the one being solved
 constexpr int kSlots = kAhead + 1;      // staging slots (a level uses slot level % kSlots)
-constexpr int kSlotRows = 256;          // rows per staged level
-constexpr int kSlotEnts = 2048;         // entries per staged level
+constexpr int kSlotRows = 384;          // rows per staged level
+constexpr int kSlotEnts = 3072;         // entries per staged level
 constexpr int kWindow = 1 << 11;        // solved values kept in shared memory
 constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are summed by the whole block
 constexpr int kThreadRowEnts = 4;       // unstaged levels averaging at most this many entries a row: a thread a row
@@ -66,6 +66,7 @@ struct Smem {
   int eptr[kSlots][kSlotRows + 1];
   double red[2][kWarps];
 };
+static_assert(sizeof(Smem) <= 227 * 1024, "the staging fits one block's shared memory");
 
 __device__ __forceinline__ void cp_async4(void *s, const void *g) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(s);

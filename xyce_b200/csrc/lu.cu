@@ -4,7 +4,9 @@
 // the pivot order and the fill. Every later matrix is refactored here, on the device, by
 // right-looking elimination of P A Q over "pivot levels": pivot k is applied once every pivot that
 // changes its row (k' with L(k, k') != 0) or its column (k' with U(k', k) != 0) has been, so all
-// pivots of one level apply together. Applying a level is two steps:
+// pivots of one level apply together. Applying a level is two steps (in the single-block runs the
+// updates come first and form their L factors on the spot, the divisions follow in the next
+// level's step; see lu_levels_block_kernel):
 //   1. divisions: for each pivot k of the level and each row i below it with L(i, k) != 0,
 //      L(i, k) = M[i][k] / U(k, k) (final: every pivot that changes M[i][k] is in an earlier level);
 //   2. updates: M[i][j] -= L(i, k) * U(k, j) for every such i and every U(k, j) != 0, j > k,
@@ -46,24 +48,48 @@ __global__ void lu_scatter_kernel(int nnz_a, const int *__restrict__ a2m, const 
 
 __device__ __forceinline__ void lu_divide(int2 dv, double *mx) { mx[dv.x] = mx[dv.x] / mx[dv.y]; }
 
-__device__ __forceinline__ void lu_update(int4 ds, const int2 *__restrict__ pairs, double *mx) {
+// A destination's updates with the level's L factors already stored (after its division step).
+// ds = (destination, L(i, k), U(k, j), U(k, k)) for one update; (destination, first pair, count,
+// -1) for more, pairs (L(i, k), U(k, j), U(k, k), 0) in increasing k.
+__device__ __forceinline__ void lu_update(int4 ds, const int4 *__restrict__ pairs, double *mx) {
   double acc = mx[ds.x];
-  if (ds.w == 1) {
+  if (ds.w >= 0) {
     acc = acc - mx[ds.y] * mx[ds.z];
   } else {
-    for (int p = ds.y; p < ds.y + ds.w; ++p) {
-      const int2 lu = pairs[p];
+    for (int p = ds.y; p < ds.y + ds.z; ++p) {
+      const int4 lu = pairs[p];
       acc = acc - mx[lu.x] * mx[lu.y];
     }
   }
   mx[ds.x] = acc;
 }
 
-// Levels [l0, l1) in one block. Each thread loads the index entry of its first item of the next
-// step before the barrier that precedes it, so the barrier's wait covers that load's latency.
+// The same updates before the level's divisions: each L factor formed on the spot from the
+// undivided column entry and the pivot, the division the division step makes, so the same value.
+__device__ __forceinline__ void lu_update_divide(int4 ds, const int4 *__restrict__ pairs, double *mx) {
+  double acc = mx[ds.x];
+  if (ds.w >= 0) {
+    acc = acc - (mx[ds.y] / mx[ds.w]) * mx[ds.z];
+  } else {
+    for (int p = ds.y; p < ds.y + ds.z; ++p) {
+      const int4 lu = pairs[p];
+      acc = acc - (mx[lu.x] / mx[lu.z]) * mx[lu.y];
+    }
+  }
+  mx[ds.x] = acc;
+}
+
+// Levels [l0, l1) in one block, one barrier per level: step l applies level l's updates, forming
+// their L factors on the spot (lu_update_divide), together with level l - 1's divisions, which
+// store those factors. The two never touch one entry: level l's updates read column entries and
+// pivots of level l's pivots and U rows of them and write entries of later pivots' columns, while
+// level l - 1's divisions write its own columns' L entries (a level-l update reading one of those
+// as U(k, j), or writing one, would make a pivot of level l - 1 depend on one of level l). After
+// the last step the run's last level is divided. Each thread loads the index entries of its first
+// items of the next step before the barrier that precedes it, so the barrier's wait covers them.
 __global__ void __launch_bounds__(kLuThreads, 1) lu_levels_block_kernel(
     int l0, int l1, const int *__restrict__ lev_div, const int *__restrict__ lev_dst, const int2 *__restrict__ div,
-    const int4 *__restrict__ dst, const int2 *__restrict__ pairs, double *mx) {
+    const int4 *__restrict__ dst, const int4 *__restrict__ pairs, double *mx) {
   __shared__ int s_div[kSegmentLevels + 1], s_dst[kSegmentLevels + 1];
   const int nl = l1 - l0;
   for (int l = threadIdx.x; l <= nl; l += kLuThreads) {
@@ -72,26 +98,34 @@ __global__ void __launch_bounds__(kLuThreads, 1) lu_levels_block_kernel(
   }
   __syncthreads();
   const int tid = threadIdx.x;
-  int2 dv_next = make_int2(0, 0);
-  if (s_div[0] + tid < s_div[1]) dv_next = div[s_div[0] + tid];
+  int4 ds_next = make_int4(0, 0, 0, 0);
+  if (s_dst[0] + tid < s_dst[1]) ds_next = dst[s_dst[0] + tid];
+  int2 dv_next = make_int2(0, 0);  // the first division of the level before the current one
   for (int l = 0; l < nl; ++l) {
-    // Divisions of level l.
-    const int db = s_div[l], de = s_div[l + 1];
-    int4 ds_next = make_int4(0, 0, 0, 0);
-    if (s_dst[l] + tid < s_dst[l + 1]) ds_next = dst[s_dst[l] + tid];
-    if (db + tid < de) {
-      lu_divide(dv_next, mx);
-      for (int t = db + tid + kLuThreads; t < de; t += kLuThreads) lu_divide(div[t], mx);
-    }
-    __syncthreads();
-    // Updates of level l.
     const int ub = s_dst[l], ue = s_dst[l + 1];
-    if (l + 1 < nl && s_div[l + 1] + tid < s_div[l + 2]) dv_next = div[s_div[l + 1] + tid];
+    const int4 ds = ds_next;
+    const int2 dv = dv_next;
+    // The next step's first items: level l + 1's update, level l's division.
+    if (l + 1 < nl && s_dst[l + 1] + tid < s_dst[l + 2]) ds_next = dst[s_dst[l + 1] + tid];
+    if (s_div[l] + tid < s_div[l + 1]) dv_next = div[s_div[l] + tid];
     if (ub + tid < ue) {
-      lu_update(ds_next, pairs, mx);
-      for (int d = ub + tid + kLuThreads; d < ue; d += kLuThreads) lu_update(dst[d], pairs, mx);
+      lu_update_divide(ds, pairs, mx);
+      for (int d = ub + tid + kLuThreads; d < ue; d += kLuThreads) lu_update_divide(dst[d], pairs, mx);
+    }
+    if (l > 0) {
+      const int db = s_div[l - 1], de = s_div[l];
+      if (db + tid < de) {
+        lu_divide(dv, mx);
+        for (int t = db + tid + kLuThreads; t < de; t += kLuThreads) lu_divide(div[t], mx);
+      }
     }
     __syncthreads();
+  }
+  // The last level's divisions.
+  const int db = s_div[nl - 1], de = s_div[nl];
+  if (db + tid < de) {
+    lu_divide(dv_next, mx);
+    for (int t = db + tid + kLuThreads; t < de; t += kLuThreads) lu_divide(div[t], mx);
   }
 }
 
@@ -100,7 +134,7 @@ __global__ void lu_divide_grid_kernel(int b, int e, const int2 *__restrict__ div
   const int t = b + blockIdx.x * blockDim.x + threadIdx.x;
   if (t < e) lu_divide(div[t], mx);
 }
-__global__ void lu_update_grid_kernel(int b, int e, const int4 *__restrict__ dst, const int2 *__restrict__ pairs,
+__global__ void lu_update_grid_kernel(int b, int e, const int4 *__restrict__ dst, const int4 *__restrict__ pairs,
                                       double *mx) {
   const int d = b + blockIdx.x * blockDim.x + threadIdx.x;
   if (d < e) lu_update(dst[d], pairs, mx);
@@ -220,12 +254,12 @@ int xd_lu_init(XdLu *lu, int n, int nnz_a, const int *rowptr_a, const int *colin
   // updates are collected in a map from its position to its pairs, in the level's pivot order
   // (increasing k within the level).
   std::vector<int> lev_div(1, 0), lev_dst(1, 0);
-  std::vector<int2> div, pairs;
-  std::vector<int4> dst;
+  std::vector<int2> div;
+  std::vector<int4> dst, pairs;
   std::vector<long long> lev_work(1, 0);  // divisions plus updates up to each level
   std::vector<int> slot(nnz, -1);   // destination position -> index in this level's list
   std::vector<int> touched;
-  std::vector<std::vector<int2>> lists;
+  std::vector<std::vector<int4>> lists;
   for (int l = 0; l < nlev; ++l) {
     touched.clear();
     lists.clear();
@@ -245,7 +279,7 @@ int xd_lu_init(XdLu *lu, int n, int nnz_a, const int *rowptr_a, const int *colin
             touched.push_back(dpos);
             lists.emplace_back();
           }
-          lists[slot[dpos]].push_back(make_int2(lpos, u));
+          lists[slot[dpos]].push_back(make_int4(lpos, u, diag[k], 0));
         }
       }
     }
@@ -253,11 +287,11 @@ int xd_lu_init(XdLu *lu, int n, int nnz_a, const int *rowptr_a, const int *colin
     // each destination's pairs are already in increasing k.
     long long work = 0;
     for (size_t d = 0; d < touched.size(); ++d) {
-      const std::vector<int2> &ls = lists[d];
+      const std::vector<int4> &ls = lists[d];
       if (ls.size() == 1) {
-        dst.push_back(make_int4(touched[d], ls[0].x, ls[0].y, 1));
+        dst.push_back(make_int4(touched[d], ls[0].x, ls[0].y, ls[0].z));
       } else {
-        dst.push_back(make_int4(touched[d], (int)pairs.size(), 0, (int)ls.size()));
+        dst.push_back(make_int4(touched[d], (int)pairs.size(), (int)ls.size(), -1));
         pairs.insert(pairs.end(), ls.begin(), ls.end());
       }
       work += (long long)ls.size();
@@ -289,7 +323,7 @@ int xd_lu_init(XdLu *lu, int n, int nnz_a, const int *rowptr_a, const int *colin
   }
   long long npairs = (long long)pairs.size();
   for (const int4 &d : dst)
-    if (d.w == 1) ++npairs;
+    if (d.w >= 0) ++npairs;
   lu->n = n;
   lu->nnz = nnz;
   lu->nnz_a = nnz_a;

@@ -25,10 +25,10 @@ struct XdLu {
   std::vector<int> lev_div, lev_dst;     // [nlev + 1] ranges of divisions / destinations (host)
   int *d_lev_div = nullptr, *d_lev_dst = nullptr;
   int2 *d_div = nullptr;                 // [ndiv] (position of L(i, k), position of U(k, k))
-  // [ndst] (destination M[i][j], a, b, count): with one update (L(i, k), U(k, j)) = (a, b) inline,
-  // with more, its pairs start at a in d_pairs.
+  // [ndst] with one update (destination M[i][j], position of L(i, k), of U(k, j), of U(k, k)); with
+  // more, (destination, first pair in d_pairs, count, -1).
   int4 *d_dst = nullptr;
-  int2 *d_pairs = nullptr;               // [npairs - inline ones] (position of L(i, k), of U(k, j))
+  int4 *d_pairs = nullptr;               // [npairs - inline ones] (L(i, k), U(k, j), U(k, k), 0) positions
   long long npairs = 0;
   // Launch plan: consecutive light levels run in one single-block launch; a level with more work
   // than one block turns over quickly runs as its own grid-wide launches.

@@ -830,7 +830,9 @@ def main():
     eval_achieved = EVAL_BYTES_PER_INST * n / (t_eval * 1e-3) / 1e9
     fp64_achieved = EVAL_FP64_FLOPS_PER_INST * n / (t_eval * 1e-3) / 1e12
     if shape["split"]:
-        eval_kernel, dram_per_inst = "bsim4_dc_kernel + bsim4_charge_stamp_kernel", SPLIT_DRAM_BYTES_PER_INST_NCU
+        # The DC part under a register budget (bsim4_dc_kernel_regs) runs in 64- or 96-thread blocks.
+        dc = "bsim4_dc_kernel" if shape["block"] == 128 else "bsim4_dc_kernel_regs"
+        eval_kernel, dram_per_inst = f"{dc} + bsim4_charge_stamp_kernel", SPLIT_DRAM_BYTES_PER_INST_NCU
     else:
         eval_kernel, dram_per_inst = "bsim4_eval_kernel", EVAL_DRAM_BYTES_PER_INST_NCU
     result = {

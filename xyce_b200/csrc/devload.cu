@@ -241,8 +241,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) bsim4_dc_kernel(
   bsim4_dc_one<FULL, SERIES>(i, n, tab, nrec, rec, nodes, sol, next_sto, curr_sto, vgb, fl, ext, mid);
 }
 
-// The same DC part under an explicit register budget instead of launch bounds: 112 registers a
-// thread let 18 warps reside per SM (six 96-thread or nine 64-thread blocks) where 128 x 4 holds 16.
+// The same DC part under an explicit register budget instead of launch bounds (112 registers a
+// thread, in 64- or 96-thread blocks): an autotuner candidate that times within noise of 128 x 4
+// on the scale circuit (the register file still holds 16 of its warps per SM).
 template <int REGS>
 __global__ void __maxnreg__(REGS) bsim4_dc_kernel_regs(
     int n, const double *__restrict__ tab, int nrec, const int *__restrict__ rec, const int4 *__restrict__ nodes,

@@ -905,8 +905,9 @@ void launch_eval(int v, const xd_ctx *ctx, const xb4::LoadFlags &fl, const doubl
         bsim4_charge_stamp_kernel<128, 3, false, false><<<grid, blk, 0, st>>>(XD_CS_ARGS);
         break;
       default: {
-        // The DC part at 112 registers in 96- or 64-thread blocks (18 resident warps per SM), the
-        // charge / stamp part in 128 x 4.
+        // The DC part under a 112-register budget in 96- or 64-thread blocks, the charge / stamp
+        // part in 128 x 4. Each sub-partition's register file still holds 4 warps at that budget (16
+        // per SM): the budget changes the schedule and the spills, not the occupancy.
         const int grid128 = (n + 127) / 128;
         bsim4_dc_kernel_regs<112><<<grid, blk, 0, st>>>(XD_DC_ARGS);
         bsim4_charge_stamp_kernel<128, 4, false, false><<<grid128, 128, 0, st>>>(XD_CS_ARGS);

@@ -25,6 +25,7 @@
 #include "bsim4_setup.h"
 #include "bsim3.h"
 #include "mos1.h"
+#include "tia_long.h"
 
 namespace {
 
@@ -466,6 +467,32 @@ struct OutSet {
   int assign = 0;     // 1: store the family's sum (=) instead of adding it (+=)
 };
 
+// acc[o] += the staged values stage[base[o] + src[k]] for k in [b, e), in k order. The sources are
+// read kGatherBatch at a time, all their loads issued before the first add, so that a target with
+// many sources (a node row of the vector map) waits for one round of loads per batch instead of one
+// per source; the adds keep the sequential order.
+constexpr int kGatherBatch = 4;
+template <int NOUT, bool ABS>
+__device__ __forceinline__ void sum_sources(int b, int e, const int *__restrict__ src,
+                                            const double *__restrict__ stage, const size_t *base, double *acc) {
+  for (int k = b; k < e; k += kGatherBatch) {
+    size_t s[kGatherBatch];
+#pragma unroll
+    for (int j = 0; j < kGatherBatch; ++j) s[j] = k + j < e ? (size_t)src[k + j] : 0;
+    double v[kGatherBatch][NOUT];
+#pragma unroll
+    for (int j = 0; j < kGatherBatch; ++j)
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) v[j][o] = k + j < e ? stage[base[o] + s[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < kGatherBatch; ++j)
+      if (k + j < e) {
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) acc[o] += ABS ? fabs(v[j][o]) : v[j][o];
+      }
+  }
+}
+
 template <int NOUT, bool ABS>
 __global__ void gather_short_kernel(int nt, const int *__restrict__ dst, const int *__restrict__ ptr,
                                     const int *__restrict__ src, const double *__restrict__ stage,
@@ -476,14 +503,7 @@ __global__ void gather_short_kernel(int nt, const int *__restrict__ dst, const i
   double acc[NOUT];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
-  for (int k = b; k < e; ++k) {
-    const size_t s = (size_t)src[k];
-#pragma unroll
-    for (int o = 0; o < NOUT; ++o) {
-      const double v = stage[os.base[o] + s];
-      acc[o] += ABS ? fabs(v) : v;
-    }
-  }
+  sum_sources<NOUT, ABS>(b, e, src, stage, os.base, acc);
   const int d = dst[t];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o)
@@ -536,34 +556,44 @@ __global__ void __launch_bounds__(kChunkBlock) gather_chunk_kernel(const int *__
   }
 }
 
+// One block per long entry: threads take the entry's chunk partials with a fixed stride, then a
+// fixed tree (a single warp walking ~1,000 partials of a supply rail's entry was a serial tail of
+// the gather).
+constexpr int kCombineBlock = 256;
 template <int NOUT, bool ABS>
-__global__ void gather_combine_kernel(int n_long, const int *__restrict__ dst, const int *__restrict__ first_chunk,
-                                      const double *__restrict__ partial, int n_chunks, OutSet<NOUT, ABS> os) {
-  const int t = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  const int lane = threadIdx.x & 31;
-  if (t >= n_long) return;
+__global__ void __launch_bounds__(kCombineBlock) gather_combine_kernel(int n_long, const int *__restrict__ dst,
+                                                                       const int *__restrict__ first_chunk,
+                                                                       const double *__restrict__ partial,
+                                                                       int n_chunks, OutSet<NOUT, ABS> os) {
+  __shared__ double red[NOUT][kCombineBlock];
+  const int t = blockIdx.x, tid = threadIdx.x;
   const int b = first_chunk[t], e = first_chunk[t + 1];
   double acc[NOUT];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o) acc[o] = 0.0;
-  for (int k = b + lane; k < e; k += 32) {
+  for (int k = b + tid; k < e; k += kCombineBlock) {
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) acc[o] += partial[(size_t)o * n_chunks + k];
   }
 #pragma unroll
-  for (int w = 16; w > 0; w >>= 1) {
+  for (int o = 0; o < NOUT; ++o) red[o][tid] = acc[o];
+  __syncthreads();
+  for (int w = kCombineBlock / 2; w > 0; w >>= 1) {
+    if (tid < w) {
 #pragma unroll
-    for (int o = 0; o < NOUT; ++o) acc[o] += __shfl_down_sync(0xffffffffu, acc[o], w);
+      for (int o = 0; o < NOUT; ++o) red[o][tid] += red[o][tid + w];
+    }
+    __syncthreads();
   }
-  if (lane == 0) {
+  if (tid == 0) {
     const int d = dst[t];
 #pragma unroll
     for (int o = 0; o < NOUT; ++o)
       if (os.out[o]) {
         if (os.assign)
-          os.out[o][d] = acc[o];
+          os.out[o][d] = red[o][0];
         else
-          os.out[o][d] += acc[o];
+          os.out[o][d] += red[o][0];
       }
   }
 }
@@ -579,8 +609,7 @@ int run_gather(const GatherMap &m, const double *stage, const OutSet<NOUT, ABS> 
   if (m.n_long > 0) {
     gather_chunk_kernel<NOUT, ABS><<<m.n_chunks, kChunkBlock, 0, st>>>(m.d_chunk_begin, m.d_src, stage, m.d_partial,
                                                                        m.n_chunks, os);
-    const int warps = 8;
-    gather_combine_kernel<NOUT, ABS><<<(m.n_long + warps - 1) / warps, 32 * warps, 0, st>>>(
+    gather_combine_kernel<NOUT, ABS><<<m.n_long, kCombineBlock, 0, st>>>(
         m.n_long, m.d_long_dst, m.d_long_chunk, m.d_partial, m.n_chunks, os);
   }
   cudaError_t e = cudaGetLastError();
@@ -1660,8 +1689,7 @@ int run_gather_static(const GatherMap &m, const double *stage, double *partial, 
   if (m.n_long > 0) {
     gather_chunk_kernel<NOUT, false><<<m.n_chunks, kChunkBlock, 0, st>>>(m.d_chunk_begin, m.d_src, stage, partial,
                                                                          m.n_chunks, os);
-    const int warps = 8;
-    gather_combine_kernel<NOUT, false><<<(m.n_long + warps - 1) / warps, 32 * warps, 0, st>>>(
+    gather_combine_kernel<NOUT, false><<<m.n_long, kCombineBlock, 0, st>>>(
         m.n_long, m.d_long_dst, m.d_long_chunk, partial, m.n_chunks, os);
   }
   cudaError_t e = cudaGetLastError();
@@ -1721,11 +1749,14 @@ int xd_load_static_scratch(xd_ctx *ctx, const xd_flags *flags, const double *d_s
 //   * fused_entry_kernel, a thread per CSR entry, forms the family's dF/dx and dQ/dx sum straight
 //     from the staged stamps (same sources, same order as the gather kernels) and the Newton matrix
 //     entry from it with the linear devices' terms;
-//   * fused_row_kernel, a warp per row, forms the row's F, Q and limiter-vector sums and the
-//     residual, with the linear devices' terms summed in tia_combine_kernel's order, and the
+//   * the vector gather forms the family's F, Q and limiter-vector sums (a thread per row), and
+//     fused_row_kernel, a warp per row, the residual from them, with the linear devices' terms
+//     summed in tia_combine_kernel's order (a long row's from its chunk sums, tia_long.h), and the
 //     diagonal entry again where a gmin shunt is on.
 // The family's dF/dx and dQ/dx are never written to memory (except for the long entries) or read
-// back; the results are bit-identical to xd_load_assign followed by xd_tia_combine. Entries are
+// back; the results are bit-identical to xd_load_assign followed by xd_tia_combine. (The row
+// kernel summing the row's vector sources on one lane, instead of the thread-per-row gather, took
+// 0.34 against 0.28 ms for the separate load and combine at 200k unknowns.) Entries are
 // independent work items, so a row of 10^5 entries (a supply rail) costs no more than 10^5 short
 // rows: one warp per row walking such a row's staged sources (an index, a source list, then the
 // stamps, three dependent loads per entry) took ~6 ms at 200k unknowns.
@@ -1739,8 +1770,8 @@ struct xd_tia_fused {
   int device = 0, n_rows = 0, nnz = 0;
   const int *d_rowptr = nullptr, *d_colind = nullptr;
   int2 *d_ent = nullptr;   // per CSR entry: (first source in the matrix map, count); count -1 = long entry
-  int2 *d_vrow = nullptr;  // per row: (first source in the vector map, count); count -1 = long row
   int *d_diag = nullptr;   // per row: position of its diagonal entry, or -1
+  XdLongRows lrows;        // the combine object's long rows (tia_long.h)
 };
 
 namespace {
@@ -1761,14 +1792,11 @@ __device__ __forceinline__ void fused_entry_sums(int k, const int2 *__restrict__
     jq = TRAN ? long_dqdx[k] : 0.0;
     return;
   }
-  double sf = 0.0, sq = 0.0;
-  for (int s = e.x; s < e.x + e.y; ++s) {
-    const size_t src = (size_t)msrc[s];
-    sf += stage[mb_f + src];
-    if (TRAN) sq += stage[mb_q + src];
-  }
-  jf = sf;
-  jq = sq;
+  double acc[2] = {0.0, 0.0};
+  const size_t base[2] = {mb_f, mb_q};
+  sum_sources<TRAN ? 2 : 1, false>(e.x, e.x + e.y, msrc, stage, base, acc);
+  jf = acc[0];
+  jq = acc[1];
 }
 
 // Newton matrix entry from the family's sums and the linear devices' constants, in
@@ -1801,31 +1829,35 @@ template <bool TRAN>
 __global__ void __launch_bounds__(32 * kFusedWarps) fused_row_kernel(
     int n_rows, const int *__restrict__ rowptr, const int *__restrict__ colind, const int *__restrict__ diag,
     xd_tia_coef c, const double *__restrict__ x, const int2 *__restrict__ ent, const int *__restrict__ msrc,
-    const int2 *__restrict__ vrow, const int *__restrict__ vsrc, const double *__restrict__ stage, size_t mb_f,
-    size_t mb_q, size_t vb0, size_t vb1, size_t vb2, size_t vb3, const double *__restrict__ long_dfdx,
-    const double *__restrict__ long_dqdx, double *__restrict__ fam_f, double *__restrict__ fam_q,
-    double *__restrict__ fam_fx, double *__restrict__ fam_qx, const double *__restrict__ lin_f,
+    const double *__restrict__ stage, size_t mb_f, size_t mb_q, const double *__restrict__ long_dfdx,
+    const double *__restrict__ long_dqdx, const double *__restrict__ fam_f, const double *__restrict__ fam_q,
+    const double *__restrict__ fam_fx, const double *__restrict__ fam_qx, const double *__restrict__ lin_f,
     const double *__restrict__ lin_q, int limiter, const double *__restrict__ b, const double *__restrict__ qn0,
     const double *__restrict__ fhist, double *__restrict__ jac, double *__restrict__ rhs,
-    double *__restrict__ q_tot, double *__restrict__ f_tot) {
+    double *__restrict__ q_tot, double *__restrict__ f_tot, XdLongRows L) {
   const int row = blockIdx.x * kFusedWarps + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n_rows) return;
   const int beg = rowptr[row], end = rowptr[row + 1];
   // The linear devices' currents and charges of the row, lane-strided then a shuffle tree, as
-  // tia_combine_kernel sums them.
+  // tia_combine_kernel sums them; a long row's from its chunk sums, as there.
   double af = 0.0, aq = 0.0;
-  if (lin_f || (TRAN && lin_q)) {
+  if (end - beg > kLongRowEntries) {
+    bool hd;
+    long_row_sums(L, long_row_index(L, row), lane, af, aq, hd);
+  } else if (lin_f || (TRAN && lin_q)) {
     for (int k = beg + lane; k < end; k += 32) {
       const double xc = x[colind[k]];
       if (lin_f) af += lin_f[k] * xc;
       if (TRAN && lin_q) aq += lin_q[k] * xc;
     }
   }
+  if (end - beg <= kLongRowEntries) {
 #pragma unroll
-  for (int w = 16; w > 0; w >>= 1) {
-    af += __shfl_down_sync(0xffffffffu, af, w);
-    aq += __shfl_down_sync(0xffffffffu, aq, w);
+    for (int w = 16; w > 0; w >>= 1) {
+      af += __shfl_down_sync(0xffffffffu, af, w);
+      aq += __shfl_down_sync(0xffffffffu, aq, w);
+    }
   }
   if (lane != 0) return;
   // The shunt goes on rows whose diagonal is in the pattern (the node rows): F and J together.
@@ -1836,37 +1868,9 @@ __global__ void __launch_bounds__(32 * kFusedWarps) fused_row_kernel(
     fused_entry_sums<TRAN>(dk, ent, msrc, stage, mb_f, mb_q, long_dfdx, long_dqdx, jf, jq);
     jac[dk] = fused_matrix_entry<TRAN>(dk, jf, jq, c.gshunt, c, lin_f, lin_q);
   }
-  // The family's vector sums for the row (the vector gather's order), kept in its buffers.
-  const int2 v = vrow[row];
-  double ff, fq, ffx, fqx;
-  if (v.y < 0) {
-    ff = fam_f[row];
-    fq = fam_q[row];
-    ffx = fam_fx[row];
-    fqx = fam_qx[row];
-  } else {
-    ff = fq = ffx = fqx = 0.0;
-    for (int s = v.x; s < v.x + v.y; ++s) {
-      const size_t src = (size_t)vsrc[s];
-      ff += stage[vb0 + src];
-      fq += stage[vb1 + src];
-      ffx += stage[vb2 + src];
-      fqx += stage[vb3 + src];
-    }
-    if (v.y > 0) {
-      fam_f[row] = ff;
-      fam_q[row] = fq;
-      fam_fx[row] = ffx;
-      fam_qx[row] = fqx;
-    } else {
-      // A row the family does not stamp: its buffers keep their (zero) values, as with the
-      // assigning load.
-      ff = fam_f[row];
-      fq = fam_q[row];
-      ffx = fam_fx[row];
-      fqx = fam_qx[row];
-    }
-  }
+  // The family's vector sums for the row, from the vector gather (rows it does not stamp keep
+  // their zero values, as with the assigning load).
+  const double ff = fam_f[row], fq = fam_q[row], ffx = fam_fx[row], fqx = fam_qx[row];
   double F = ff + af;
   if (has_diag) F += c.gshunt * x[row];
   if (b) F -= b[row];
@@ -1917,9 +1921,8 @@ int xd_tia_fused_create(xd_tia *tia, xd_ctx *fam, xd_tia_fused **out) {
   if (n_rows != fam->n_unknowns || nnz != fam->nnz)
     return fail(-1, "the combine object's pattern is not the family's pattern");
   DeviceGuard g(device);
-  std::vector<int2> ent, vrow;
+  std::vector<int2> ent;
   if ((rc = map_ranges(fam->mmap, nnz, ent)) != 0) return rc;
-  if ((rc = map_ranges(fam->vmap, n_rows, vrow)) != 0) return rc;
   // Each row's diagonal position (the gmin shunt's entry), from the pattern.
   std::vector<int> hp((size_t)n_rows + 1), hc((size_t)nnz), dpos((size_t)n_rows, -1);
   XD_CUDA(cudaMemcpy(hp.data(), rowptr, hp.size() * sizeof(int), cudaMemcpyDeviceToHost));
@@ -1938,15 +1941,13 @@ int xd_tia_fused_create(xd_tia *tia, xd_ctx *fam, xd_tia_fused **out) {
   f->nnz = nnz;
   f->d_rowptr = rowptr;
   f->d_colind = colind;
+  xd_tia_internal_long_rows(tia, &f->lrows);
   cudaError_t ce;
   if ((ce = cudaMalloc(&f->d_ent, std::max<size_t>(1, ent.size()) * sizeof(int2))) != cudaSuccess ||
       (ce = cudaMemcpy(f->d_ent, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess ||
-      (ce = cudaMalloc(&f->d_vrow, std::max<size_t>(1, vrow.size()) * sizeof(int2))) != cudaSuccess ||
-      (ce = cudaMemcpy(f->d_vrow, vrow.data(), vrow.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (ce = cudaMalloc(&f->d_diag, std::max<size_t>(1, dpos.size()) * sizeof(int))) != cudaSuccess ||
       (ce = cudaMemcpy(f->d_diag, dpos.data(), dpos.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
     cudaFree(f->d_ent);
-    cudaFree(f->d_vrow);
     cudaFree(f->d_diag);
     delete f;
     return cuda_fail(ce, "xd_tia_fused_create allocation");
@@ -1959,7 +1960,6 @@ int xd_tia_fused_destroy(xd_tia_fused *f) {
   if (!f) return 0;
   DeviceGuard g(f->device);
   cudaFree(f->d_ent);
-  cudaFree(f->d_vrow);
   cudaFree(f->d_diag);
   delete f;
   return 0;
@@ -1985,22 +1985,25 @@ int xd_tia_load_combine(xd_tia_fused *fu, const xd_flags *flags, const xd_tia_co
   const size_t n = (size_t)ctx->n, r = (size_t)ctx->vec_rows;
   const size_t mb = 4 * r * n, mm = (size_t)ctx->mat_slots * n;
   if (ctx->n > 0) {
-    // Long entries and rows: the chunked gathers store the family's sums into its buffers.
+    // The family's vector sums (all rows, a thread per row), and its long matrix entries' sums
+    // (chunked) into its buffers.
     OutSet<4, false> vs{{d_fam_f, d_fam_q, d_fam_fx, d_fam_qx}, {0, r * n, 2 * r * n, 3 * r * n}, 1};
-    if ((rc = run_gather(ctx->vmap, ctx->d_stage, vs, st, false))) return rc;
+    if ((rc = run_gather(ctx->vmap, ctx->d_stage, vs, st))) return rc;
     OutSet<2, false> ms{{d_fam_dfdx, d_fam_dqdx}, {mb, mb + mm}, 1};
     if ((rc = run_gather(ctx->mmap, ctx->d_stage, ms, st, false))) return rc;
   }
+  // Long rows: their chunks' linear-device sums (their matrix entries come from the entry kernel).
+  if ((rc = xd_tia_internal_long_chunks(fu->tia, coef, d_x, nullptr, nullptr, d_lin_dfdx, d_lin_dqdx, nullptr, st)))
+    return rc;
   const int row_blocks = (fu->n_rows + kFusedWarps - 1) / kFusedWarps;
   const int ent_blocks = (fu->nnz + kEntryBlock - 1) / kEntryBlock;
 #define XD_ENTRY_ARGS                                                                                               \
   fu->nnz, *coef, fu->d_ent, ctx->mmap.d_src, ctx->d_stage, mb, mb + mm, d_fam_dfdx, d_fam_dqdx, d_lin_dfdx,         \
       d_lin_dqdx, d_jac
 #define XD_ROW_ARGS                                                                                                 \
-  fu->n_rows, fu->d_rowptr, fu->d_colind, fu->d_diag, *coef, d_x, fu->d_ent, ctx->mmap.d_src, fu->d_vrow,            \
-      ctx->vmap.d_src, ctx->d_stage, mb, mb + mm, (size_t)0, r * n, 2 * r * n, 3 * r * n, d_fam_dfdx, d_fam_dqdx,    \
-      d_fam_f, d_fam_q, d_fam_fx, d_fam_qx, d_lin_dfdx, d_lin_dqdx, limiter, d_b, d_qn0, d_fhist, d_jac, d_rhs,      \
-      d_q_tot, d_f_tot
+  fu->n_rows, fu->d_rowptr, fu->d_colind, fu->d_diag, *coef, d_x, fu->d_ent, ctx->mmap.d_src, ctx->d_stage, mb,   \
+      mb + mm, d_fam_dfdx, d_fam_dqdx, d_fam_f, d_fam_q, d_fam_fx, d_fam_qx, d_lin_dfdx, d_lin_dqdx, limiter, d_b,   \
+      d_qn0, d_fhist, d_jac, d_rhs, d_q_tot, d_f_tot, fu->lrows
   if (coef->mode != 0) {
     if (ent_blocks > 0) fused_entry_kernel<true><<<ent_blocks, kEntryBlock, 0, st>>>(XD_ENTRY_ARGS);
     fused_row_kernel<true><<<row_blocks, 32 * kFusedWarps, 0, st>>>(XD_ROW_ARGS);

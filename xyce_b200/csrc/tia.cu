@@ -7,7 +7,9 @@
 // residual's operations in the reference's order: ((Q - Q_n) / h + f F) + g F_hist, negated, then
 // the limiter corrections (1/h) dQdxdVp and f dFdxdVp added.
 // One warp per row: lanes take the row's entries with a fixed stride, and the per-row sums of the
-// linear devices' F and Q use a fixed shuffle tree, so the results do not vary between runs.
+// linear devices' F and Q use a fixed shuffle tree, so the results do not vary between runs. Rows
+// of more than kLongRowEntries entries (the supply rail's) are cut into chunks first, a block per
+// chunk, and their warp adds the chunk sums (tia_long.h).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +19,7 @@
 #include <vector>
 
 #include "../../include/xyce_tia.h"
+#include "tia_long.h"
 
 int xd_internal_fail(int code, const std::string &msg);
 
@@ -26,6 +29,12 @@ struct xd_tia {
   int nnz = 0;
   int *d_rowptr = nullptr;
   int *d_colind = nullptr;
+  // Long rows (tia_long.h): the rows, each one's first chunk, the chunks' entry ranges and rows,
+  // the chunk sums and diagonal flags.
+  int n_lrows = 0, n_lchunks = 0;
+  int *d_lrow = nullptr, *d_lfirst = nullptr, *d_lchunk_row = nullptr, *d_ldiag = nullptr;
+  int2 *d_lchunk = nullptr;
+  double *d_lpart = nullptr;
 };
 
 struct xd_slu {
@@ -48,7 +57,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) tia_combine_kernel(
     const double *__restrict__ q, const double *__restrict__ fx, const double *__restrict__ qx,
     const double *__restrict__ b, const double *__restrict__ qn0,
     const double *__restrict__ fhist, double *__restrict__ jac, double *__restrict__ rhs,
-    double *__restrict__ q_tot, double *__restrict__ f_tot) {
+    double *__restrict__ q_tot, double *__restrict__ f_tot, XdLongRows L) {
   const int row = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n_rows) return;
@@ -56,7 +65,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) tia_combine_kernel(
   const bool tran = c.mode != 0;
   double af = 0.0, aq = 0.0;
   bool has_diag = false;
-  for (int k = beg + lane; k < end; k += 32) {
+  // A long row's entries and chunk sums come from long_row_chunk_kernel.
+  const bool long_row = end - beg > kLongRowEntries;
+  if (long_row) long_row_sums(L, long_row_index(L, row), lane, af, aq, has_diag);
+  for (int k = beg + lane; !long_row && k < end; k += 32) {
     double jf = dfdx[k];
     if (lin_f) {
       const double g = lin_f[k];
@@ -79,13 +91,15 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) tia_combine_kernel(
       jac[k] = jf;
     }
   }
+  if (!long_row) {
 #pragma unroll
-  for (int w = 16; w > 0; w >>= 1) {
-    af += __shfl_down_sync(0xffffffffu, af, w);
-    aq += __shfl_down_sync(0xffffffffu, aq, w);
+    for (int w = 16; w > 0; w >>= 1) {
+      af += __shfl_down_sync(0xffffffffu, af, w);
+      aq += __shfl_down_sync(0xffffffffu, aq, w);
+    }
+    // The shunt goes on rows whose diagonal is in the pattern (the node rows): F and J together.
+    has_diag = __any_sync(0xffffffffu, has_diag);
   }
-  // The shunt goes on rows whose diagonal is in the pattern (the node rows): F and J together.
-  has_diag = __any_sync(0xffffffffu, has_diag);
   if (lane == 0) {
     double F = f[row] + af;
     if (has_diag) F += c.gshunt * x[row];
@@ -593,7 +607,145 @@ __global__ void pwl_eval_kernel(int n, const int *__restrict__ row, const int *_
   b[row[k]] = value;
 }
 
+// One chunk of a long row (tia_long.h) per block: with JAC, the chunk's Newton matrix entries as
+// tia_combine_kernel forms them; always the chunk's linear-device F and Q sums (threads take
+// entries with a fixed stride, then a fixed tree) and whether it holds the row's diagonal (with a
+// gmin shunt on).
+template <bool JAC>
+__global__ void __launch_bounds__(kLongBlock) long_row_chunk_kernel(
+    int n_chunks, const int2 *__restrict__ chunk, const int *__restrict__ chunk_row, const int *__restrict__ colind,
+    xd_tia_coef c, const double *__restrict__ x, const double *__restrict__ dfdx, const double *__restrict__ dqdx,
+    const double *__restrict__ lin_f, const double *__restrict__ lin_q, double *__restrict__ jac,
+    double *__restrict__ part, int *__restrict__ diag) {
+  __shared__ double red[2][kLongBlock];
+  __shared__ int hd;
+  const int ch = blockIdx.x, tid = threadIdx.x;
+  const int2 rg = chunk[ch];
+  const int row = chunk_row[ch];
+  const bool tran = c.mode != 0;
+  if (tid == 0) hd = 0;
+  __syncthreads();
+  double af = 0.0, aq = 0.0;
+  bool has = false;
+  for (int k = rg.x + tid; k < rg.y; k += kLongBlock) {
+    const int col = colind[k];
+    double jf = JAC ? dfdx[k] : 0.0;
+    if (lin_f) {
+      const double g = lin_f[k];
+      if (JAC) jf += g;
+      af += g * x[col];
+    }
+    if (c.gshunt != 0.0 && col == row) {
+      if (JAC) jf += c.gshunt;
+      has = true;
+    }
+    if (tran) {
+      double jq = JAC ? dqdx[k] : 0.0;
+      if (lin_q) {
+        const double cq = lin_q[k];
+        if (JAC) jq += cq;
+        aq += cq * x[col];
+      }
+      if (JAC) jac[k] = c.qscale * jq + c.fscale * jf;
+    } else if (JAC) {
+      jac[k] = jf;
+    }
+  }
+  if (has) hd = 1;
+  red[0][tid] = af;
+  red[1][tid] = aq;
+  __syncthreads();
+  for (int w = kLongBlock / 2; w > 0; w >>= 1) {
+    if (tid < w) {
+      red[0][tid] += red[0][tid + w];
+      red[1][tid] += red[1][tid + w];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    part[ch] = red[0][0];
+    part[n_chunks + ch] = red[1][0];
+    diag[ch] = hd;
+  }
+}
+
+void free_long_rows(xd_tia *t) {
+  cudaFree(t->d_lrow);
+  cudaFree(t->d_lfirst);
+  cudaFree(t->d_lchunk_row);
+  cudaFree(t->d_ldiag);
+  cudaFree(t->d_lchunk);
+  cudaFree(t->d_lpart);
+  t->d_lrow = t->d_lfirst = t->d_lchunk_row = t->d_ldiag = nullptr;
+  t->d_lchunk = nullptr;
+  t->d_lpart = nullptr;
+  t->n_lrows = t->n_lchunks = 0;
+}
+
+// The long rows of the pattern and their chunks (kLongChunk consecutive entries, the last one of a
+// row shorter), uploaded.
+cudaError_t setup_long_rows(xd_tia *t, const int *rowptr) {
+  std::vector<int> lrow, lfirst(1, 0), crow;
+  std::vector<int2> chunk;
+  for (int r = 0; r < t->n_rows; ++r) {
+    const int b = rowptr[r], e = rowptr[r + 1];
+    if (e - b <= kLongRowEntries) continue;
+    lrow.push_back(r);
+    for (int k = b; k < e; k += kLongChunk) {
+      chunk.push_back(make_int2(k, std::min(e, k + kLongChunk)));
+      crow.push_back(r);
+    }
+    lfirst.push_back((int)chunk.size());
+  }
+  if (lrow.empty()) return cudaSuccess;
+  const size_t nr = lrow.size(), nc = chunk.size();
+  cudaError_t e;
+  if ((e = cudaMalloc(&t->d_lrow, nr * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&t->d_lfirst, (nr + 1) * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&t->d_lchunk_row, nc * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&t->d_ldiag, nc * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&t->d_lchunk, nc * sizeof(int2))) != cudaSuccess ||
+      (e = cudaMalloc(&t->d_lpart, 2 * nc * sizeof(double))) != cudaSuccess ||
+      (e = cudaMemcpy(t->d_lrow, lrow.data(), nr * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(t->d_lfirst, lfirst.data(), (nr + 1) * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(t->d_lchunk_row, crow.data(), nc * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(t->d_lchunk, chunk.data(), nc * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return e;
+  t->n_lrows = (int)nr;
+  t->n_lchunks = (int)nc;
+  return cudaSuccess;
+}
+
 }  // namespace
+
+int xd_tia_internal_long_rows(const xd_tia *t, XdLongRows *out) {
+  if (!t || !out) return xd_internal_fail(-1, "null combine object");
+  out->n_rows = t->n_lrows;
+  out->n_chunks = t->n_lchunks;
+  out->row = t->d_lrow;
+  out->first = t->d_lfirst;
+  out->part = t->d_lpart;
+  out->diag = t->d_ldiag;
+  return 0;
+}
+
+int xd_tia_internal_long_chunks(xd_tia *t, const xd_tia_coef *c, const double *x, const double *dfdx,
+                                const double *dqdx, const double *lin_f, const double *lin_q, double *jac,
+                                cudaStream_t st) {
+  if (!t || !c) return xd_internal_fail(-1, "null argument");
+  if (t->n_lchunks == 0) return 0;
+  if (jac)
+    long_row_chunk_kernel<true><<<t->n_lchunks, kLongBlock, 0, st>>>(t->n_lchunks, t->d_lchunk, t->d_lchunk_row,
+                                                                     t->d_colind, *c, x, dfdx, dqdx, lin_f, lin_q,
+                                                                     jac, t->d_lpart, t->d_ldiag);
+  else
+    long_row_chunk_kernel<false><<<t->n_lchunks, kLongBlock, 0, st>>>(t->n_lchunks, t->d_lchunk, t->d_lchunk_row,
+                                                                      t->d_colind, *c, x, dfdx, dqdx, lin_f, lin_q,
+                                                                      jac, t->d_lpart, t->d_ldiag);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(e, "long_row_chunk_kernel launch");
+  return 0;
+}
 
 // The pattern a combine object was created on (for the fused load-and-combine in devload.cu).
 int xd_tia_internal_pattern(const xd_tia *t, int *device, int *n_rows, int *nnz, const int **rowptr,
@@ -637,10 +789,18 @@ int xd_tia_create(const xd_csr *pat, int cuda_device, xd_tia **out) {
     delete t;
     return cuda_err(e, "xd_tia_create upload");
   }
+  if ((e = setup_long_rows(t, pat->rowptr)) != cudaSuccess) {
+    free_long_rows(t);
+    cudaFree(t->d_rowptr);
+    cudaFree(t->d_colind);
+    delete t;
+    return cuda_err(e, "xd_tia_create long rows");
+  }
   if (pat->n_rows <= XD_DENSE_MAX_N && dense_smem_bytes(pat->n_rows) > 48 * 1024) {
     e = cudaFuncSetAttribute(dense_factor_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)dense_smem_bytes(pat->n_rows));
     if (e != cudaSuccess) {
+      free_long_rows(t);
       cudaFree(t->d_rowptr);
       cudaFree(t->d_colind);
       delete t;
@@ -654,6 +814,7 @@ int xd_tia_create(const xd_csr *pat, int cuda_device, xd_tia **out) {
 int xd_tia_destroy(xd_tia *t) {
   if (!t) return 0;
   Guard g(t->device);
+  free_long_rows(t);
   cudaFree(t->d_rowptr);
   cudaFree(t->d_colind);
   delete t;
@@ -733,10 +894,15 @@ int xd_tia_combine(xd_tia *t, const xd_tia_coef *coef, const double *d_x, const 
   if (coef->mode != 0 && (!d_dqdx || !d_q || !d_qn0 || (coef->hist_scale != 0.0 && !d_fhist)))
     return xd_internal_fail(-1, "null device buffer for a time step");
   Guard g(t->device);
+  int rc = xd_tia_internal_long_chunks(t, coef, d_x, d_dfdx, d_dqdx, d_lin_dfdx, d_lin_dqdx, d_jac,
+                                       (cudaStream_t)stream);
+  if (rc) return rc;
+  XdLongRows L;
+  xd_tia_internal_long_rows(t, &L);
   const int blocks = (t->n_rows + kWarpsPerBlock - 1) / kWarpsPerBlock;
   tia_combine_kernel<<<blocks, 32 * kWarpsPerBlock, 0, (cudaStream_t)stream>>>(
       t->n_rows, t->d_rowptr, t->d_colind, *coef, d_x, d_dfdx, d_dqdx, d_lin_dfdx, d_lin_dqdx, d_f, d_q, d_dfdxdvp,
-      d_dqdxdvp, d_b, d_qn0, d_fhist, d_jac, d_rhs, d_q_tot, d_f_tot);
+      d_dqdxdvp, d_b, d_qn0, d_fhist, d_jac, d_rhs, d_q_tot, d_f_tot, L);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_err(e, "tia_combine_kernel launch");
   return 0;

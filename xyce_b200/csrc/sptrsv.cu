@@ -21,6 +21,11 @@
 // in a fixed order, so results do not depend on the timing. In a staged level the short rows (at
 // most kShortRow entries, ordered first by the set-up) are solved a thread each while the warps the
 // short rows leave free solve the longer rows a warp each.
+// Thin levels (at most kChainShort short and kChainLong longer rows) are most of the lower
+// triangle's levels (median two rows), and a block step (staging, barrier) costs far more than
+// their rows. Runs of consecutive thin levels that fit one staging slot are staged as one step,
+// which warp 0 solves level by level with a warp barrier between levels; each row is summed as in
+// any other staged level, so the results are the same bits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,6 +54,10 @@ constexpr int kWindow = 1 << 11;        // solved values kept in shared memory
 constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are summed by the whole block
 constexpr int kThreadRowEnts = 4;       // unstaged levels averaging at most this many entries a row: a thread a row
 constexpr int kShortRow = 8;            // staged levels: rows of at most this many entries a thread each, longer a warp
+constexpr int kChainShort = 32;         // a thin level: at most this many short rows ...
+constexpr int kChainLong = 4;           // ... and this many longer ones
+constexpr int kMaxSub = 32;             // thin levels per run
+constexpr int kSubInts = 2 * kMaxSub + 2;  // a run's record: count, (first row, first long row) per level, end
 
 constexpr int kEntsPerThread = kSlotEnts / kThreads;
 static_assert(kSlotEnts % kThreads == 0, "a staged level's entries split evenly over the threads");
@@ -60,6 +69,8 @@ struct Smem {
   int pos[kSlots][kSlotEnts];
   int cut[kSlots];               // columns at positions below cut[s] have their value in xv
   int nshort[kSlots];            // the level's short rows (they come first)
+  int chain[kSlots];             // 1: the step is a run of thin levels, described by sub
+  int sub[kSlots][kSubInts];
   double rhs[kSlots][kSlotRows];
   double diag[kSlots][kSlotRows];
   int dst[kSlots][kSlotRows];
@@ -96,7 +107,9 @@ struct Tri {
   double *out;       // [n] solved values by position
   double *next_rhs;  // lower: the upper triangle's right-hand side (by its positions)
   double *x;         // upper: the solution
-  int nlev;
+  int nlev;          // steps
+  const int *chain;  // [nlev] offset of the step's run record in sub, or -1
+  const int *sub;    // run records (rows relative to the step's first position), padded by kSubInts
 };
 
 __device__ __forceinline__ double solved(int p, int lo, const Smem &sm, const double *out) {
@@ -121,6 +134,7 @@ __device__ __forceinline__ bool staged(const int4 &m) { return m.y - m.x <= kSlo
 struct PosAhead {
   int p[kEntsPerThread];
   int ls;  // thread 0: the level's first row longer than kShortRow entries
+  int ch;  // the step's run record offset, or -1
 };
 
 __device__ __forceinline__ PosAhead load_pos(int l, const int4 &m, const Tri &t, int tid) {
@@ -132,6 +146,7 @@ __device__ __forceinline__ PosAhead load_pos(int l, const int4 &m, const Tri &t,
     a.p[q] = (st && k < m.w - m.z) ? t.epos[m.z + k] : -1;
   }
   a.ls = (st && tid == 0) ? t.lstart[2 * l + 1] : 0;
+  a.ch = st ? t.chain[l] : -1;
   return a;
 }
 
@@ -157,9 +172,12 @@ __device__ __forceinline__ void stage_level(int l, const int4 &m, const PosAhead
         if (pa.p[q] < cut) cp_async8(&sm.xv[s][k], t.out + pa.p[q]);
       }
     }
+    if (pa.ch >= 0)
+      for (int k = tid; k < kSubInts; k += kThreads) cp_async4(&sm.sub[s][k], t.sub + pa.ch + k);
     if (tid == 0) {
       sm.cut[s] = cut;
       sm.nshort[s] = pa.ls - m.x;
+      sm.chain[s] = pa.ch >= 0;
     }
   }
   cp_async_commit();
@@ -191,18 +209,15 @@ __global__ void __launch_bounds__(kThreads) level_solve_kernel(Tri t) {
     const int b = cur.x, e = cur.y, lo = e - kWindow;
     const bool by_thread = cur.w - cur.z <= kThreadRowEnts * (e - b);
     if (staged(cur)) {
-      // Short rows (the first ns) a thread each; longer ones a warp each, on the warps after those
-      // the short rows occupy, at the same time.
-      const int s = l % kSlots, eb = cur.z, ns = sm.nshort[s];
-      for (int r = tid; r < ns; r += kThreads) {
+      const int s = l % kSlots, eb = cur.z;
+      auto short_row = [&](int r) {
         const int kb = sm.eptr[s][r] - eb, ke = sm.eptr[s][r + 1] - eb;
         double acc = 0.0;
         for (int k = kb; k < ke; ++k) acc += sm.val[s][k] * staged_solved(sm, s, k, lo, t.out);
         const double v = UPPER ? (sm.rhs[s][r] - acc) / sm.diag[s][r] : sm.rhs[s][r] - acc;
         publish<UPPER>(b + r, v, sm.dst[s][r], sm, t);
-      }
-      const int w0 = min(kWarps - 1, (ns + 31) >> 5);
-      for (int r = ns + warp - w0; warp >= w0 && r < e - b; r += kWarps - w0) {
+      };
+      auto warp_row = [&](int r) {
         const int kb = sm.eptr[s][r] - eb, ke = sm.eptr[s][r + 1] - eb;
         double acc = 0.0;
         for (int k = kb + lane; k < ke; k += 32) acc += sm.val[s][k] * staged_solved(sm, s, k, lo, t.out);
@@ -212,6 +227,26 @@ __global__ void __launch_bounds__(kThreads) level_solve_kernel(Tri t) {
           const double v = UPPER ? (sm.rhs[s][r] - acc) / sm.diag[s][r] : sm.rhs[s][r] - acc;
           publish<UPPER>(b + r, v, sm.dst[s][r], sm, t);
         }
+      };
+      if (sm.chain[s]) {
+        // A run of thin levels: warp 0 solves them in order.
+        if (warp == 0) {
+          const int *sb = sm.sub[s];
+          const int nsub = sb[0];
+          for (int j = 0; j < nsub; ++j) {
+            const int rb = sb[1 + 2 * j], rs = sb[2 + 2 * j], re = sb[3 + 2 * j];
+            for (int r = rb + lane; r < rs; r += 32) short_row(r);
+            for (int r = rs; r < re; ++r) warp_row(r);
+            __syncwarp();
+          }
+        }
+      } else {
+        // Short rows (the first ns) a thread each; longer ones a warp each, on the warps after
+        // those the short rows occupy, at the same time.
+        const int ns = sm.nshort[s];
+        for (int r = tid; r < ns; r += kThreads) short_row(r);
+        const int w0 = min(kWarps - 1, (ns + 31) >> 5);
+        for (int r = ns + warp - w0; warp >= w0 && r < e - b; r += kWarps - w0) warp_row(r);
       }
     } else {
       // Unstaged level: rows from global memory, one thread or one warp each; very long rows by
@@ -302,8 +337,9 @@ int cu_err(cudaError_t e, const char *where) {
 // One triangle's level order: rows by dependency depth (ascending row index within a level),
 // each row's entries of this triangle, the level metadata.
 struct HostTri {
-  std::vector<int> rows, pos, eptr, epos, src, lstart;
-  std::vector<int4> meta;
+  std::vector<int> rows, pos, eptr, epos, src, lstart, chain, sub;
+  std::vector<int4> meta;  // per step
+  int nlev = 0;            // dependency levels
 };
 
 void build_tri(int n, const std::vector<int> &mp, const std::vector<int> &mi, bool upper, HostTri &h) {
@@ -354,14 +390,50 @@ void build_tri(int n, const std::vector<int> &mp, const std::vector<int> &mi, bo
   }
   h.epos.resize(h.src.size());
   for (size_t k = 0; k < h.src.size(); ++k) h.epos[k] = h.pos[mi[h.src[k]]];
-  h.meta.assign(nlev, make_int4(0, 0, 0, 0));
-  h.lstart.assign(2 * (size_t)nlev, 0);
-  for (int l = 0; l < nlev; ++l) {
-    const int b = start[3 * l], e = start[3 * l + 3];
-    h.meta[l] = make_int4(b, e, h.eptr[b], h.eptr[e]);
-    h.lstart[2 * l] = start[3 * l + 2];
-    h.lstart[2 * l + 1] = start[3 * l + 1];
+  // Steps: a level, or a run of 2..kMaxSub consecutive thin levels that fits one staging slot. A
+  // run's record in sub: the level count, then per level its first row and first long row
+  // (relative to the run's first position), then the run's row count.
+  h.nlev = nlev;
+  h.meta.clear();
+  h.lstart.clear();
+  h.chain.clear();
+  h.sub.clear();
+  auto thin = [&](int l) {
+    return start[3 * l + 1] - start[3 * l] <= kChainShort && start[3 * l + 3] - start[3 * l + 1] <= kChainLong;
+  };
+  for (int l = 0; l < nlev;) {
+    int l2 = l, rows = 0, ents = 0;
+    while (l2 < nlev && l2 - l < kMaxSub && thin(l2)) {
+      const int b = start[3 * l2], e = start[3 * l2 + 3];
+      const int r2 = rows + (e - b), e2 = ents + (h.eptr[e] - h.eptr[b]);
+      if (r2 > kSlotRows || e2 > kSlotEnts) break;
+      rows = r2;
+      ents = e2;
+      ++l2;
+    }
+    if (l2 - l >= 2) {
+      const int b = start[3 * l], e = start[3 * l2];
+      h.meta.push_back(make_int4(b, e, h.eptr[b], h.eptr[e]));
+      h.lstart.push_back(e);
+      h.lstart.push_back(b);
+      h.chain.push_back((int)h.sub.size());
+      h.sub.push_back(l2 - l);
+      for (int k = l; k < l2; ++k) {
+        h.sub.push_back(start[3 * k] - b);
+        h.sub.push_back(start[3 * k + 1] - b);
+      }
+      h.sub.push_back(e - b);
+      l = l2;
+    } else {
+      const int b = start[3 * l], e = start[3 * l + 3];
+      h.meta.push_back(make_int4(b, e, h.eptr[b], h.eptr[e]));
+      h.lstart.push_back(start[3 * l + 2]);
+      h.lstart.push_back(start[3 * l + 1]);
+      h.chain.push_back(-1);
+      ++l;
+    }
   }
+  h.sub.resize(h.sub.size() + kSubInts, 0);  // the staging copies kSubInts ints from a record's offset
 }
 
 template <class T>
@@ -403,12 +475,16 @@ int xd_sptrsv_init(XdSptrsv *s, int n, int nnz_m, const int *d_mp, const int *d_
   s->n = n;
   s->nnz[0] = (int)lo.src.size();
   s->nnz[1] = (int)up.src.size();
-  s->nlev[0] = (int)lo.meta.size();
-  s->nlev[1] = (int)up.meta.size();
+  s->nlev[0] = lo.nlev;
+  s->nlev[1] = up.nlev;
+  s->nstep[0] = (int)lo.meta.size();
+  s->nstep[1] = (int)up.meta.size();
   int rc;
   if ((rc = upload(&s->d_meta[0], lo.meta)) || (rc = upload(&s->d_meta[1], up.meta)) ||
       (rc = upload(&s->d_eptr[0], lo.eptr)) || (rc = upload(&s->d_eptr[1], up.eptr)) ||
       (rc = upload(&s->d_lstart[0], lo.lstart)) || (rc = upload(&s->d_lstart[1], up.lstart)) ||
+      (rc = upload(&s->d_chain[0], lo.chain)) || (rc = upload(&s->d_chain[1], up.chain)) ||
+      (rc = upload(&s->d_sub[0], lo.sub)) || (rc = upload(&s->d_sub[1], up.sub)) ||
       (rc = upload(&s->d_epos[0], lo.epos)) || (rc = upload(&s->d_epos[1], up.epos)) ||
       (rc = upload(&s->d_src[0], lo.src)) || (rc = upload(&s->d_src[1], up.src)) ||
       (rc = upload(&s->d_dst[0], ldst)) || (rc = upload(&s->d_dst[1], udst)) || (rc = upload(&s->d_dsrc, dsrc)) ||
@@ -431,6 +507,9 @@ void xd_sptrsv_free(XdSptrsv *s) {
     cudaFree(s->d_eptr[u]);
     cudaFree(s->d_lstart[u]);
     s->d_lstart[u] = nullptr;
+    cudaFree(s->d_chain[u]);
+    cudaFree(s->d_sub[u]);
+    s->d_chain[u] = s->d_sub[u] = nullptr;
     cudaFree(s->d_epos[u]);
     cudaFree(s->d_src[u]);
     cudaFree(s->d_dst[u]);
@@ -455,9 +534,9 @@ int xd_sptrsv_solve(XdSptrsv *s, const double *d_mx, double *d_x, cudaStream_t s
   gather_kernel<<<blocks, 256, 0, st>>>(s->nnz[0], s->d_src[0], s->d_val[0], s->nnz[1], s->d_src[1], s->d_val[1], n,
                                         s->d_dsrc, diag, s->d_bsrc, d_x, rhs_l, d_mx);
   Tri lo{s->d_meta[0], s->d_lstart[0], s->d_eptr[0], s->d_epos[0], s->d_val[0], rhs_l, nullptr,
-         s->d_dst[0], out_l, rhs_u, nullptr, s->nlev[0]};
+         s->d_dst[0], out_l, rhs_u, nullptr, s->nstep[0], s->d_chain[0], s->d_sub[0]};
   Tri up{s->d_meta[1], s->d_lstart[1], s->d_eptr[1], s->d_epos[1], s->d_val[1], rhs_u, diag,
-         s->d_dst[1], out_u, nullptr, d_x, s->nlev[1]};
+         s->d_dst[1], out_u, nullptr, d_x, s->nstep[1], s->d_chain[1], s->d_sub[1]};
   level_solve_kernel<false><<<1, kThreads, sizeof(Smem), st>>>(lo);
   level_solve_kernel<true><<<1, kThreads, sizeof(Smem), st>>>(up);
   cudaError_t e = cudaGetLastError();

@@ -7,10 +7,13 @@
 // Both triangles of P A Q = L U renumbered in dependency-level order ([0] lower, [1] upper).
 struct XdSptrsv {
   int n = 0;
-  int nlev[2] = {0, 0};
+  int nlev[2] = {0, 0};                   // dependency levels of each triangle
+  int nstep[2] = {0, 0};                  // the kernel's steps: levels, with runs of thin levels as one
   int nnz[2] = {0, 0};                    // strictly lower / strictly upper entries
   int4 *d_meta[2] = {nullptr, nullptr};   // per level: first and end position, first and end entry
   int *d_lstart[2] = {nullptr, nullptr};  // per level: first row summed by the whole block
+  int *d_chain[2] = {nullptr, nullptr};   // per step: offset of its thin-level run in d_sub, or -1
+  int *d_sub[2] = {nullptr, nullptr};     // the runs' level boundaries (see sptrsv.cu)
   int *d_eptr[2] = {nullptr, nullptr};    // [n+1] entry range of each position
   int *d_epos[2] = {nullptr, nullptr};    // [nnz] each entry's column as a position
   int *d_src[2] = {nullptr, nullptr};     // [nnz] each entry's index in the bundled factors

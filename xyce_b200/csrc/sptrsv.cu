@@ -24,8 +24,9 @@
 // Thin levels (at most kChainShort short and kChainLong longer rows) are most of the lower
 // triangle's levels (median two rows), and a block step (staging, barrier) costs far more than
 // their rows. Runs of consecutive thin levels that fit one staging slot are staged as one step,
-// which warp 0 solves level by level with a warp barrier between levels; each row is summed as in
-// any other staged level, so the results are the same bits.
+// which the first kChainLong warps solve level by level (short rows a thread each, longer rows a
+// warp each) with a barrier of those warps alone between levels; each row is summed as in any
+// other staged level, so the results are the same bits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,7 +56,8 @@ constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are s
 constexpr int kThreadRowEnts = 4;       // unstaged levels averaging at most this many entries a row: a thread a row
 constexpr int kShortRow = 8;            // staged levels: rows of at most this many entries a thread each, longer a warp
 constexpr int kChainShort = 32;         // a thin level: at most this many short rows ...
-constexpr int kChainLong = 4;           // ... and this many longer ones
+constexpr int kChainLong = 4;           // ... and this many longer ones (a warp each)
+constexpr int kChainThreads = 32 * kChainLong;
 constexpr int kMaxSub = 32;             // thin levels per run
 constexpr int kSubInts = 2 * kMaxSub + 2;  // a run's record: count, (first row, first long row) per level, end
 
@@ -229,15 +231,16 @@ __global__ void __launch_bounds__(kThreads) level_solve_kernel(Tri t) {
         }
       };
       if (sm.chain[s]) {
-        // A run of thin levels: warp 0 solves them in order.
-        if (warp == 0) {
+        // A run of thin levels: the first kChainLong warps solve them in order, named barrier 1
+        // (theirs alone) between levels.
+        if (warp < kChainLong) {
           const int *sb = sm.sub[s];
           const int nsub = sb[0];
           for (int j = 0; j < nsub; ++j) {
             const int rb = sb[1 + 2 * j], rs = sb[2 + 2 * j], re = sb[3 + 2 * j];
-            for (int r = rb + lane; r < rs; r += 32) short_row(r);
-            for (int r = rs; r < re; ++r) warp_row(r);
-            __syncwarp();
+            for (int r = rb + tid; r < rs; r += kChainThreads) short_row(r);
+            for (int r = rs + warp; r < re; r += kChainLong) warp_row(r);
+            asm volatile("bar.sync 1, %0;" ::"n"(kChainThreads) : "memory");
           }
         }
       } else {

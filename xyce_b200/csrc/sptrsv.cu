@@ -55,8 +55,8 @@ constexpr int kWindow = 1 << 11;        // solved values kept in shared memory
 constexpr int kBlockRow = 2048;         // in unstaged levels, longer rows are summed by the whole block
 constexpr int kThreadRowEnts = 4;       // unstaged levels averaging at most this many entries a row: a thread a row
 constexpr int kShortRow = 8;            // staged levels: rows of at most this many entries a thread each, longer a warp
-constexpr int kChainShort = 64;         // a thin level: at most this many short rows ...
-constexpr int kChainLong = 8;           // ... and this many longer ones (a warp each)
+constexpr int kChainShort = 128;        // a thin level: at most this many short rows ...
+constexpr int kChainLong = 16;          // ... and this many longer ones (a warp each)
 constexpr int kChainThreads = 32 * kChainLong;
 constexpr int kMaxSub = 32;             // thin levels per run
 constexpr int kSubInts = 2 * kMaxSub + 2;  // a run's record: count, (first row, first long row) per level, end

@@ -54,8 +54,9 @@ int xd_tia_destroy(xd_tia *t);
  *   f_tot[i] = F_i and q_tot[i] = Q_i when those pointers are non-null.
  * dfdx / dqdx / f / q hold the nonlinear devices' loads (for instance from xd_load_assign);
  * lin_* may be null (no linear devices), b may be null (no sources); in mode 0 dqdx, lin_dqdx,
- * qn0 and fhist are not read. Row sums use a fixed lane split and a fixed reduction tree, so the
- * results are bit-identical from run to run. */
+ * qn0 and fhist are not read. Row sums use a fixed lane split and a fixed reduction tree (rows of
+ * more than 1,024 entries, such as a supply rail's: fixed 1,024-entry chunks, a block each, then a
+ * fixed tree over the chunks), so the results are bit-identical from run to run. */
 int xd_tia_combine(xd_tia *t, const xd_tia_coef *coef, const double *d_x, const double *d_dfdx,
                    const double *d_dqdx, const double *d_lin_dfdx, const double *d_lin_dqdx,
                    const double *d_f, const double *d_q, const double *d_dfdxdvp, const double *d_dqdxdvp,
@@ -91,7 +92,8 @@ int xd_pwl_eval(xd_pwl *p, double t, int transient, double *d_b, void *stream);
  * matrix entry and residual straight from them, so the family's dF/dx and dQ/dx never go through
  * memory (only the few entries with very many contributions, such as supply rails, are summed
  * into d_fam_dfdx / d_fam_dqdx first). The family's F, Q and limiter vectors are stored into
- * d_fam_f / d_fam_q / d_fam_fx / d_fam_qx as by xd_load_assign; d_fam_dfdx / d_fam_dqdx hold
+ * d_fam_f / d_fam_q / d_fam_fx / d_fam_qx as by xd_load_assign (by the same vector gather, before
+ * the row pass reads them); d_fam_dfdx / d_fam_dqdx hold
  * the family's sums only at those long entries afterwards. Buffers as for the two calls it
  * replaces (d_fam_* zeroed once when allocated). */
 typedef struct xd_tia_fused xd_tia_fused;
